@@ -1,0 +1,347 @@
+"""Throughput of the CHNS time step on B200 (Mcell-steps/s), with roofline, CPU baseline and end-to-end legs.
+
+Workload: the rising bubble of BASELINE config 2 on its 192x384 grid -- no-slip top/bottom, free-slip sides,
+density and viscosity ratio 10, split_icpcg pressure (rho_ref = min density), WENO5 phase advection, seeded
+interface modes 2-8 -- run in the reference's R0-unit parameterisation (testcase 26: lx=4, ly=8, R=1,
+Re=12.374, Ca=0.0202, Cn=0.04, Pe=150, g=1, dt=5e-5).  The literal unit-square mapping of config 2
+diverges on the reference itself after ~30 steps, so a bounded trajectory on the same grid is timed.
+Inputs are synthetic (seeded numpy), FP64 ("plain" form).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on stdout (rank 0).  For N > 1 the driver launches one process per GPU (torchrun); every rank
+advances its own replica (the 2D step does not shard without changing the preconditioner), value is the
+aggregate over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+# Algorithmic bytes per cell per pressure-PCG iteration of the split scheme, FP64 (SpMV 16, x/r update 48,
+# forward sweep 24, backward sweep 24, p update 24): every distinct array read once and written once.
+PCG_BYTES_PER_CELL_IT = 136.0
+RESTART_FIELDS = ("c", "c_prev", "c_prev2", "p", "p_prev", "u", "v", "u_prev", "v_prev", "e_prev", "hu_prev",
+                  "hv_prev")
+
+
+def workload_cfg() -> dict:
+    return dict(
+        name="rising_bubble_192x384_split_icpcg", mode="coupled", nx=192, ny=384, ghost=3, lx=4.0, ly=8.0,
+        periodic_x=False, periodic_y=False, v_bc_left_type="neumann", v_bc_left_value=0.0,
+        v_bc_right_type="neumann", v_bc_right_value=0.0, interface_center_x=2.0, interface_center_y=2.0,
+        interface_radius=1.0, re=12.374368670764582, ca=0.02020305007471719, cn=0.04, pe=150.0,
+        density_ratio=10.0, viscosity_ratio=10.0, body_force_y=-1.0, dt=5e-5, pressure_scheme="split_icpcg",
+        poisson_iterations=2000, pressure_tolerance=1e-10, ch_inner_iterations=500, ch_tolerance=1e-10,
+        momentum_iterations=200, momentum_tolerance=1e-10, surface_tension_multiplier=1.0)
+
+
+def initial_state(cfg: dict, seed: int = 2) -> dict:
+    """Seeded perturbed bubble: R(theta) = R + sum_{k=2..8} a_k cos(k theta + phi_k), a_k = 0.02 U(-1,1)
+    (0.005 in the unit-square units of config 2), c = 1/2 - 1/2 tanh((r - R(theta)) / (2 sqrt 2 Cn))."""
+    rng = np.random.default_rng(seed)
+    nx, ny, g = cfg["nx"], cfg["ny"], cfg["ghost"]
+    dx, dy = cfg["lx"] / nx, cfg["ly"] / ny
+    x = (np.arange(nx) + 0.5) * dx - cfg["interface_center_x"]
+    y = (np.arange(ny) + 0.5) * dy - cfg["interface_center_y"]
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    r, th = np.hypot(X, Y), np.arctan2(Y, X)
+    R = np.full_like(r, cfg["interface_radius"])
+    for k in range(2, 9):
+        R += 0.02 * rng.uniform(-1, 1) * np.cos(k * th + rng.uniform(0, 2 * np.pi))
+    c = 0.5 - 0.5 * np.tanh((r - R) / (2.0 * math.sqrt(2.0) * cfg["cn"]))
+    cell = np.zeros((nx + 2 * g, ny + 2 * g))
+    cell[g:-g, g:-g] = c
+    state = {n: np.zeros((nx + 2 * g + (1 if n in ("u", "u_prev", "hu_prev") else 0),
+                          ny + 2 * g + (1 if n in ("v", "v_prev", "hv_prev") else 0))) for n in RESTART_FIELDS}
+    for n in ("c", "c_prev", "c_prev2"):
+        state[n] = cell.copy()
+    return state
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+        return False
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return None, 0, 1, 0
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return dist, rank, world, local
+
+
+def reduce_max(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+
+        torch.cuda.synchronize()
+        dist.barrier()
+
+
+def cpu_reference_run(cfg, state, first_step, count):
+    """Steps of the reference build (oracle/_ref, the reference's own C++ sources) on the host: seconds."""
+    from oracle.oracle import OracleSolver, available, with_defaults
+
+    impl = "reference" if available("reference") else "port"
+    s = OracleSolver(with_defaults(cfg), impl)
+    s.initialize()
+    for n, a in state.items():
+        s.set_field(n, a)
+    s.refresh_derived()
+    return s.time_steps(first_step, count), impl
+
+
+def run_ours(args):
+    import torch
+
+    import ding_nsch_core_solver_b200 as dn
+
+    dist, rank, world, local = dist_setup(args.gpus)
+    device = local if dist is not None else 0
+    torch.cuda.set_device(device)
+    cfg = workload_cfg()
+    state = initial_state(cfg)
+    n_cells = cfg["nx"] * cfg["ny"]
+
+    solver = dn.Solver(cfg, device=device)
+
+    def inject(st):
+        for n, a in st.items():
+            solver.set_field(n, a)
+        solver.refresh_derived()
+
+    inject(state)
+    solver.set_initial_mass(solver.compute_mass("c"))
+    stream = torch.cuda.ExternalStream(solver.stream(), device=device)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # 512 MB > 126 MB L2
+
+    step = 0
+    for _ in range(args.warmup):
+        solver.step(step)
+        step += 1
+    barrier(dist)
+
+    # ---- device-resident timed region: K steps, L2 flushed between steps (outside the timed windows)
+    times, pcg_ms, pcg_its, reports, phases = [], [], [], [], []
+    launches0 = solver.kernel_launches()
+    with ClockSampler(device) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rep = solver.step(step)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            ph = solver.phase_times_ms()
+            phases.append(ph)
+            pcg_ms.append(ph[4])
+            pcg_its.append(ph[7])
+            reports.append(rep)
+            step += 1
+    launches = solver.kernel_launches() - launches0
+    total_ms = sum(times)
+    total_ms = reduce_max(dist, total_ms)
+    value = n_cells * args.steps * world / (total_ms * 1e-3) / 1e6
+
+    # ---- end-to-end through the C-ABI with host buffers: restart-field upload, step, download, per step
+    host = {n: solver.get_field(n) for n in RESTART_FIELDS}
+    pinned = {n: torch.from_numpy(a).pin_memory().numpy() for n, a in host.items()}
+    h2d = sum(a.nbytes for a in pinned.values())
+    barrier(dist)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        inject(pinned)
+        solver.step(step)
+        for n in RESTART_FIELDS:
+            solver.get_field(n, out=pinned[n])
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        step += 1
+    e2e_ms = reduce_max(dist, e2e_ms)
+    e2e_value = n_cells * args.steps * world / (e2e_ms * 1e-3) / 1e6
+
+    # ---- roofline of the dominant kernel (the pressure PCG), bytes per launch / launch time
+    peak, peak_kind = hbm_peak()
+    bytes_per_launch = PCG_BYTES_PER_CELL_IT * n_cells * statistics.mean(pcg_its)
+    achieved = bytes_per_launch / (statistics.mean(pcg_ms) * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
+                "kernel": "k_pcg<5,0> (pressure ICC-PCG, persistent, one launch per solve)",
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "kernel_ms_mean": statistics.mean(pcg_ms)}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sample = max(1, args.cpu_sample_steps)
+        sec, impl = cpu_reference_run(cfg, state, 0, sample)
+        cpu = {"value": round(n_cells * sample / sec / 1e6, 6), "unit": "Mcell-steps/s", "cores": 1,
+               "kind": "reference" if impl == "reference" else "port",
+               "sample": f"{sample} steps (steps 0-{sample - 1}) of the same 192x384 workload from the same "
+                         f"seeded state; the reference step is single-threaded",
+               "seconds": round(sec, 3)}
+
+    if rank == 0:
+        mean_rep = {k: statistics.mean(r[k] for r in reports) for k in ("pressure_iterations", "ch_iterations",
+                                                                       "momentum_iterations")}
+        line = {
+            "metric": "Mcell-steps/s (plain FP64 step; mixed form not built yet)",
+            "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rising bubble 192x384 split_icpcg, R0-unit parameters of testcase 26, seeded "
+                                   "interface modes 2-8", "grid": [192, 384], "pressure_scheme": "split_icpcg",
+                       "pressure_tolerance": 1e-10, "ch_tolerance": 1e-10, "precision": "fp64",
+                       "l2": "flushed (512 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+            "iterations_mean": mean_rep,
+            "phase_ms_mean": {k: round(statistics.mean(p[i] for p in phases), 4) for i, k in enumerate(
+                ("ch", "momentum", "pressure", "correction", "pressure_pcg_kernel", "ch_pcg_kernel",
+                 "bicgstab_kernel"))},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": h2d},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        barrier(dist)
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import available
+
+    cfg = workload_cfg()
+    state = initial_state(cfg)
+    n_cells = cfg["nx"] * cfg["ny"]
+    if not (available("reference") or available("port")):
+        print(json.dumps({"impl": "reference", "unavailable": "CPU reference build missing (make -C oracle)"}))
+        return
+    if args.warmup > 0:
+        cpu_reference_run(cfg, state, 0, 1)  # one warm-up step (page-in, allocator)
+    sec, impl = cpu_reference_run(cfg, state, 0, args.steps)
+    value = n_cells * args.steps / sec / 1e6
+    cpu = {"value": round(value, 6), "unit": "Mcell-steps/s", "cores": 1, "kind": impl,
+           "sample": f"{args.steps} steps of the 192x384 workload; the reference step is single-threaded, so one "
+                     f"host thread is all it can use"}
+    print(json.dumps({
+        "impl": "reference", "metric": "Mcell-steps/s (plain FP64 step; mixed form not built yet)",
+        "value": round(value, 6), "unit": "Mcell-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "rising bubble 192x384 split_icpcg, R0-unit parameters of testcase 26, seeded "
+                               "interface modes 2-8", "grid": [192, 384]},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(value, 6), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

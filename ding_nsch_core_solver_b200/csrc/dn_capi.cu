@@ -1,0 +1,1381 @@
+// dn_capi.cu -- host side of libdn_cuda: handle, device state, the time-step driver and the C-ABI.
+//
+// The driver replays Solver::advance_one_timestep (src/core/coupled/solver.cpp:224-283) as a sequence of
+// kernels on one stream; the three linear solves run as persistent cooperative kernels (dn_krylov.cuh,
+// dn_momentum.cuh).  There is no CPU fallback: every numeric step runs on the GPU, and a missing or
+// failing device reports an error status.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dn_common.cuh"
+#include "dn_fields.cuh"
+#include "dn_krylov.cuh"
+#include "dn_momentum.cuh"
+
+using namespace dn;
+
+namespace {
+
+constexpr double kSqrt2 = 1.4142135623730950488;
+constexpr int kHostScal = 8192;  // pinned host scratch (doubles): scalars and reduction partials
+
+// ---------------------------------------------------------------------------------------------------
+// Pressure system (build_pressure_linear_system, pressure.cpp:123-196) into 5 slots W,S,C,N,E + rhs
+// ---------------------------------------------------------------------------------------------------
+__device__ double split_divergence(const Fv &pe, const Fv &rm, const Grid &G, int i, int j, double rho_ref) {
+  // liu_split_explicit_divergence, operators.cpp:424-444
+  const bool eo = G.px || i < G.nx - 1, wo = G.px || i > 0, no = G.py || j < G.ny - 1, so = G.py || j > 0;
+  const double fe = eo ? (1.0 - rho_ref / xface(rm, G, i + 1, j)) * gfx(pe, G, i + 1, j) : 0.0;
+  const double fw = wo ? (1.0 - rho_ref / xface(rm, G, i, j)) * gfx(pe, G, i, j) : 0.0;
+  const double fn = no ? (1.0 - rho_ref / yface(rm, G, i, j + 1)) * gfy(pe, G, i, j + 1) : 0.0;
+  const double fs = so ? (1.0 - rho_ref / yface(rm, G, i, j)) * gfy(pe, G, i, j) : 0.0;
+  return (fe - fw) / G.dx + (fn - fs) / G.dy;
+}
+
+__global__ void k_p_assemble(Grid G, BCSet bc, Fv rm, Fv us, Fv vs, Fv pe, int split, double rho_ref, double dt,
+                             double *a, double *rhs) {
+  const long long n = (long long)G.nx * G.ny;
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int i = (int)(r / G.ny), j = (int)(r % G.ny);
+  const double dx = G.dx, dy = G.dy;
+  const bool he = G.px || i < G.nx - 1, hw = G.px || i > 0, hn = G.py || j < G.ny - 1, hs = G.py || j > 0;
+  const double ce = split ? 1.0 / (dx * dx) : 1.0 / (xface(rm, G, i + 1, j) * dx * dx);
+  const double cw = split ? 1.0 / (dx * dx) : 1.0 / (xface(rm, G, i, j) * dx * dx);
+  const double cn = split ? 1.0 / (dy * dy) : 1.0 / (yface(rm, G, i, j + 1) * dy * dy);
+  const double cs = split ? 1.0 / (dy * dy) : 1.0 / (yface(rm, G, i, j) * dy * dy);
+  double diag = 0.0;
+  double rv = split ? -(split_divergence(pe, rm, G, i, j, rho_ref) + rho_ref * div_cell(us, vs, G, i, j) / dt)
+                    : -div_cell(us, vs, G, i, j) / dt;
+  auto boundary = [&](int side, double coeff, double spacing) {
+    const BCSide &b = bc.p[side];
+    if (b.type == DN_BC_DIRICHLET) {
+      diag += 2.0 * coeff;
+      rv += 2.0 * coeff * b.value;
+    } else {
+      rv += coeff * b.value * spacing;
+    }
+  };
+  double aE = 0.0, aW = 0.0, aN = 0.0, aS = 0.0;
+  if (he) {
+    diag += ce;
+    aE = 0.0 + -ce;
+  } else {
+    boundary(DN_RIGHT, ce, dx);
+  }
+  if (hw) {
+    diag += cw;
+    aW = 0.0 + -cw;
+  } else {
+    boundary(DN_LEFT, cw, dx);
+  }
+  if (hn) {
+    diag += cn;
+    aN = 0.0 + -cn;
+  } else {
+    boundary(DN_TOP, cn, dy);
+  }
+  if (hs) {
+    diag += cs;
+    aS = 0.0 + -cs;
+  } else {
+    boundary(DN_BOTTOM, cs, dy);
+  }
+  auto keep = [](double v) { return fabs(v) < 1.0e-18 ? 0.0 : v; };
+  a[0 * n + r] = keep(aW);
+  a[1 * n + r] = keep(aS);
+  a[2 * n + r] = 0.0 + diag;
+  a[3 * n + r] = keep(aN);
+  a[4 * n + r] = keep(aE);
+  rhs[r] = rv;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// CH operator A = alpha0 I - beta1 L + beta2 L^2 (build_laplacian_matrix / multiply /
+// build_cahn_hilliard_operator, ch_sparse_krylov.hpp:135-233) with std::map accumulation semantics.
+// ---------------------------------------------------------------------------------------------------
+struct SmallMap {
+  long long col[16];
+  double val[16];
+  int cnt;
+  __device__ void clear() { cnt = 0; }
+  __device__ void add(long long c, double v) {
+    for (int k = 0; k < cnt; ++k)
+      if (col[k] == c) {
+        val[k] += v;
+        return;
+      }
+    col[cnt] = c;
+    val[cnt] = 0.0 + v;
+    ++cnt;
+  }
+  __device__ void sort() {
+    for (int a = 1; a < cnt; ++a) {
+      long long c = col[a];
+      double v = val[a];
+      int b = a - 1;
+      while (b >= 0 && col[b] > c) {
+        col[b + 1] = col[b];
+        val[b + 1] = val[b];
+        --b;
+      }
+      col[b + 1] = c;
+      val[b + 1] = v;
+    }
+  }
+  __device__ void drop_tiny() {  // finalize_row_maps, ch_sparse_krylov.hpp:116
+    int w = 0;
+    for (int k = 0; k < cnt; ++k)
+      if (!(fabs(val[k]) < 1.0e-18)) {
+        col[w] = col[k];
+        val[w] = val[k];
+        ++w;
+      }
+    cnt = w;
+  }
+};
+
+__device__ void laplacian_row(int i, int j, const Grid &G, SmallMap &m) {
+  const int nx = G.nx, ny = G.ny;
+  const double inv_dx2 = 1.0 / (G.dx * G.dx), inv_dy2 = 1.0 / (G.dy * G.dy);
+  const long long row = (long long)i * ny + j;
+  double diag = 0.0;
+  m.clear();
+  if (G.px || i > 0) {
+    const int iw = (G.px && i == 0) ? nx - 1 : i - 1;
+    m.add((long long)iw * ny + j, inv_dx2);
+    diag -= inv_dx2;
+  }
+  if (G.px || i < nx - 1) {
+    const int ie = (G.px && i == nx - 1) ? 0 : i + 1;
+    m.add((long long)ie * ny + j, inv_dx2);
+    diag -= inv_dx2;
+  }
+  if (G.py || j > 0) {
+    const int js = (G.py && j == 0) ? ny - 1 : j - 1;
+    m.add((long long)i * ny + js, inv_dy2);
+    diag -= inv_dy2;
+  }
+  if (G.py || j < ny - 1) {
+    const int jn = (G.py && j == ny - 1) ? 0 : j + 1;
+    m.add((long long)i * ny + jn, inv_dy2);
+    diag -= inv_dy2;
+  }
+  m.add(row, diag);
+  m.sort();
+  m.drop_tiny();
+}
+
+__global__ void k_ch_matrix(Grid G, double alpha0, double beta1, double beta2, double *a13, int *status) {
+  const long long n = (long long)G.nx * G.ny;
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int i = (int)(r / G.ny), j = (int)(r % G.ny);
+  SmallMap L, Lm, L2, A;
+  laplacian_row(i, j, G, L);
+  L2.clear();
+  for (int p = 0; p < L.cnt; ++p) {
+    const long long mid = L.col[p];
+    laplacian_row((int)(mid / G.ny), (int)(mid % G.ny), G, Lm);
+    for (int q = 0; q < Lm.cnt; ++q) L2.add(Lm.col[q], L.val[p] * Lm.val[q]);
+  }
+  L2.sort();
+  L2.drop_tiny();
+  A.clear();
+  A.add(r, alpha0);
+  for (int p = 0; p < L.cnt; ++p) A.add(L.col[p], -beta1 * L.val[p]);
+  for (int p = 0; p < L2.cnt; ++p) A.add(L2.col[p], beta2 * L2.val[p]);
+  A.drop_tiny();
+  for (int s = 0; s < 13; ++s) a13[(size_t)s * n + r] = 0.0;
+  for (int p = 0; p < A.cnt; ++p) {
+    int slot = -1;
+    for (int s = 0; s < 13; ++s)
+      if (slot_col<13>(i, j, s, G.nx, G.ny, G.px, G.py) == A.col[p]) {
+        slot = s;
+        break;
+      }
+    if (slot < 0) {
+      atomicExch(status, 1);  // column outside the 13-point stencil (grid too small)
+      continue;
+    }
+    a13[(size_t)slot * n + r] = A.val[p];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Initial conditions (initialize_phase / initialize_velocity, solver.cpp:115-221)
+// ---------------------------------------------------------------------------------------------------
+struct InitParams {
+  int mode, phase_initializer, velocity_profile, invert_phase, couette;
+  double cn, lx, ly, cx, cy, radius, amplitude, wavenumber, slot_w, slot_d, advect_u, advect_v;
+  double rcx, rcy, omega, ub, ut;
+};
+
+__device__ double sd_box(double x, double y, double cx, double cy, double hx, double hy) {
+  const double qx = fabs(x - cx) - hx, qy = fabs(y - cy) - hy;
+  const double ox = fmax(qx, 0.0), oy = fmax(qy, 0.0);
+  return hypot(ox, oy) + fmin(fmax(qx, qy), 0.0);
+}
+
+__global__ void k_init_phase(Fv c, Grid G, InitParams P) {
+  DN_FOR_INTERIOR(c);
+  const double x = ((double)i + 0.5) * G.dx, y = ((double)j + 0.5) * G.dy;
+  double value = 1.0;
+  if (P.phase_initializer == 1) {
+    const double shw = 0.5 * P.slot_w, st = P.cy + P.radius, sb = st - P.slot_d;
+    const double scy = 0.5 * (st + sb), shh = 0.5 * (st - sb);
+    const double sm = fmax(2.0 * kSqrt2 * P.cn, 1.0e-12);
+    const double dsd = hypot(x - P.cx, y - P.cy) - P.radius;
+    const double shape = fmax(dsd, -sd_box(x, y, P.cx, scy, shw, shh));
+    value = 0.5 - 0.5 * tanh(shape / sm);
+    c.at(i, j) = P.invert_phase ? (1.0 - value) : value;
+    return;
+  }
+  if (P.mode == DN_MODE_SINGLE_PHASE) {
+    c.at(i, j) = P.invert_phase ? 0.0 : 1.0;
+    return;
+  }
+  if (P.mode != DN_MODE_ADVECTION_ONLY) {
+    if (P.radius > 0.0) {
+      const double rx = x - P.cx, ry = y - P.cy;
+      const double r = sqrt(rx * rx + ry * ry);
+      value = 0.5 - 0.5 * tanh((r - P.radius) / (2.0 * kSqrt2 * P.cn));
+    } else {
+      const double y0 = P.cy + P.amplitude * cos(2.0 * M_PI * P.wavenumber * x / fmax(P.lx, 1.0e-12));
+      value = 0.5 - 0.5 * tanh((y - y0) / (2.0 * kSqrt2 * P.cn));
+    }
+  }
+  c.at(i, j) = P.invert_phase ? (1.0 - value) : value;
+}
+
+__global__ void k_init_u(Fv u, Grid G, InitParams P, int full) {
+  const long long nxg = u.nx + 2 * u.g, nyg = u.ny + 2 * u.g;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxg * nyg) return;
+  const int i = (int)(t / nyg) - u.g, j = (int)(t % nyg) - u.g;
+  if (P.velocity_profile == 1) {
+    const double y = ((double)j + 0.5) * G.dy;
+    u.at(i, j) = -P.omega * (y - P.rcy);
+    return;
+  }
+  if (i < 0 || i >= u.nx || j < 0 || j >= u.ny || !full) return;
+  if (P.couette) {
+    const double y = ((double)j + 0.5) * G.dy;
+    u.at(i, j) = P.ub + (P.ut - P.ub) * y / fmax(P.ly, 1.0e-30);
+  } else {
+    u.at(i, j) = P.advect_u;
+  }
+}
+__global__ void k_init_v(Fv v, Grid G, InitParams P) {
+  const long long nxg = v.nx + 2 * v.g, nyg = v.ny + 2 * v.g;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nxg * nyg) return;
+  const int i = (int)(t / nyg) - v.g, j = (int)(t % nyg) - v.g;
+  if (P.velocity_profile == 1) {
+    const double x = ((double)i + 0.5) * G.dx;
+    v.at(i, j) = P.omega * (x - P.rcx);
+    return;
+  }
+  if (i < 0 || i >= v.nx || j < 0 || j >= v.ny) return;
+  v.at(i, j) = P.advect_v;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------
+// Handle
+// ---------------------------------------------------------------------------------------------------
+struct dn_handle {
+  dn_config cfg;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  Grid G;
+  BCSet bc;
+  bool has_dirichlet = false;
+  Fv f[DN_F_COUNT];
+  // ghosted work fields
+  Fv mob, lap, bih, mu_t, afx, afy, arhs, dfx, dfy, ddiv, E_new, cmid, mm, pe, urhs, vrhs, hu, hv, sm_c, sm_u, sm_v;
+  // compact Krylov vectors
+  long long n = 0;
+  double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *y = nullptr, *p0 = nullptr, *p1 = nullptr,
+         *ap = nullptr;
+  // pressure operator + factor
+  double *a5 = nullptr, *l5 = nullptr, *d5 = nullptr, *dinv5 = nullptr;
+  bool p_factor_valid = false;
+  int p_factor_kind = 0;
+  // CH operator + factor
+  double *a13 = nullptr, *l13 = nullptr, *d13 = nullptr, *dinv13 = nullptr;
+  double ch_alpha0 = -1.0;
+  int ch_prec = kPrecLDLT;  // kPrecLDLT or kPrecDiag
+  // momentum
+  long long nm = 0;
+  MomLayout ml;
+  double *mcoef = nullptr;
+  long long *mtgt = nullptr;
+  double *mb = nullptr, *mx = nullptr, *mr = nullptr, *mrhat = nullptr, *mp0 = nullptr, *mp1 = nullptr, *mv0 = nullptr,
+         *mv1 = nullptr, *mphat = nullptr, *ms = nullptr, *mshat = nullptr, *mt = nullptr, *mupd = nullptr,
+         *mdinv = nullptr;
+  // synchronisation + scratch
+  unsigned int *bar_count = nullptr, *bar_gen = nullptr, *prog = nullptr;
+  int *status = nullptr;
+  double *partials = nullptr;
+  double *scal = nullptr;       // device scalars
+  double *host_scal = nullptr;  // pinned
+  int max_coop_blocks = 0;
+  int nsweep = 0;
+  double initial_mass = 0.0;
+  long long launches = 0;
+  std::string err;
+  std::vector<void *> allocations;
+  cudaEvent_t ev[5] = {};
+  cudaEvent_t kev[2] = {};
+  double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ch, momentum, pressure, correction, pressure PCG kernel,
+                                                 // CH PCG kernel, BiCGSTAB kernel, pressure PCG iterations
+  int step = 0;  // step index of the step in progress (split extrapolation, operators.cpp:416)
+};
+
+namespace {
+
+dn_status fail(dn_handle *h, dn_status s, const std::string &msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+#define DN_CUDA(h, call)                                                                        \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return fail(h, DN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define DN_TRY(expr)              \
+  do {                            \
+    dn_status s_ = (expr);        \
+    if (s_ != DN_OK) return s_;   \
+  } while (0)
+
+template <typename T>
+dn_status dalloc(dn_handle *h, T **p, size_t count) {
+  void *q = nullptr;
+  DN_CUDA(h, cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+  DN_CUDA(h, cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), h->stream));
+  h->allocations.push_back(q);
+  *p = static_cast<T *>(q);
+  return DN_OK;
+}
+
+dn_status falloc(dn_handle *h, Fv &f, int nx, int ny, double init) {
+  f.nx = nx;
+  f.ny = ny;
+  f.g = h->cfg.ghost;
+  DN_TRY(dalloc(h, &f.d, f.size()));
+  if (init != 0.0) {
+    const long long n = (long long)f.size();
+    k_fill<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(f.d, init, n);
+    h->launches++;
+  }
+  return DN_OK;
+}
+
+inline unsigned blocks_for(long long n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+dn_status check_launch(dn_handle *h, const char *what) {
+  h->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, DN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return DN_OK;
+}
+
+bool is_uish(int id) { return id == DN_F_U || id == DN_F_U_PREV || id == DN_F_U_STAR || id == DN_F_SFX_U || id == DN_F_HU_PREV; }
+bool is_vish(int id) { return id == DN_F_V || id == DN_F_V_PREV || id == DN_F_V_STAR || id == DN_F_SFY_V || id == DN_F_HV_PREV; }
+
+// ---- boundary conditions
+dn_status bc(dn_handle *h, const Fv &f, int kind) {
+  const BCSet &B = h->bc;
+  BCSide L{}, R{}, Bt{}, T{};
+  if (kind == kBCPressure) {
+    L = B.p[0]; R = B.p[1]; Bt = B.p[2]; T = B.p[3];
+  } else if (kind == kBCU) {
+    L = B.u[0]; R = B.u[1]; Bt = B.u[2]; T = B.u[3];
+    k_bc_faces_u<<<blocks_for(f.ny), 256, 0, h->stream>>>(f, h->G, L, R);
+    DN_TRY(check_launch(h, "k_bc_faces_u"));
+  } else if (kind == kBCV) {
+    L = B.v[0]; R = B.v[1]; Bt = B.v[2]; T = B.v[3];
+    k_bc_faces_v<<<blocks_for(f.nx), 256, 0, h->stream>>>(f, h->G, Bt, T);
+    DN_TRY(check_launch(h, "k_bc_faces_v"));
+  }
+  const long long nghost = 2LL * f.g * f.ny + 2LL * f.g * (f.nx + 2 * f.g);
+  k_bc_ghosts<<<blocks_for(nghost), 256, 0, h->stream>>>(f, h->G, kind, L, R, Bt, T);
+  return check_launch(h, "k_bc_ghosts");
+}
+
+dn_status copy_field(dn_handle *h, const Fv &dst, const Fv &src) {
+  DN_CUDA(h, cudaMemcpyAsync(dst.d, src.d, src.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  return DN_OK;
+}
+
+dn_status fill_field(dn_handle *h, const Fv &f, double v) {
+  k_fill<<<blocks_for((long long)f.size()), 256, 0, h->stream>>>(f.d, v, (long long)f.size());
+  return check_launch(h, "k_fill");
+}
+
+// mean of a field's interior into h->scal[slot] (device)
+dn_status field_mean(dn_handle *h, const Fv &f, int slot) {
+  const int nb = 128;
+  k_field_sum<<<nb, 256, 0, h->stream>>>(f, 1.0, h->partials);
+  DN_TRY(check_launch(h, "k_field_sum"));
+  k_finish_mean<<<1, 32, 0, h->stream>>>(h->partials, nb, (double)f.nx * f.ny, h->scal + slot);
+  return check_launch(h, "k_finish_mean");
+}
+dn_status subtract_mean(dn_handle *h, const Fv &f) {
+  DN_TRY(field_mean(h, f, 0));
+  k_add_scalar_interior<<<blocks_for((long long)f.nx * f.ny), 256, 0, h->stream>>>(f, h->scal);
+  return check_launch(h, "k_add_scalar_interior");
+}
+
+dn_status read_scalars(dn_handle *h, int count, double *out) {
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->scal + 8, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(out, h->host_scal, count * sizeof(double));
+  return DN_OK;
+}
+
+dn_status read_status(dn_handle *h, int *status) {
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 32, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(status, h->host_scal + 32, sizeof(int));
+  return DN_OK;
+}
+
+dn_status reset_sync(dn_handle *h) {
+  DN_CUDA(h, cudaMemsetAsync(h->bar_count, 0, sizeof(unsigned int), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(h->prog, 0, 2 * (size_t)kMaxBlocks * 8 * sizeof(unsigned int), h->stream));
+  return DN_OK;
+}
+
+dn_status dev_status_to_dn(dn_handle *h, int st) {
+  switch (st) {
+  case kDevOk: return DN_OK;
+  case kDevTimeout: return fail(h, DN_ERR_TIMEOUT, "device wait timed out (grid barrier or wavefront flag)");
+  case kDevPcgBreakdownRz0: return fail(h, DN_ERR_PCG_BREAKDOWN, "pcg preconditioner breakdown: non-positive r^T M^{-1} r");
+  case kDevPcgBreakdownPap: return fail(h, DN_ERR_PCG_BREAKDOWN, "pcg breakdown: p^T A p is invalid");
+  case kDevPcgBreakdownRz: return fail(h, DN_ERR_PCG_BREAKDOWN, "pcg preconditioner breakdown: non-positive new r^T M^{-1} r");
+  case kDevBicgRho: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid rho");
+  case kDevBicgRhatV: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid r_hat^T A M^{-1} p");
+  case kDevBicgTT: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid t^T t");
+  case kDevBicgOmega: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid omega");
+  default: return fail(h, DN_ERR_CUDA, "unknown device status");
+  }
+}
+
+// ---- persistent PCG launch
+template <int S, int SWEEP>
+dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *dinv, int prec, int project, int max_it,
+                  double tol, double out[4]) {
+  PcgArgs P;
+  P.A = SpOp{a, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  P.l = l;
+  P.dinv = dinv;
+  P.prec = prec;
+  P.b = h->b;
+  P.x = h->x;
+  P.r = h->r;
+  P.z = h->z;
+  P.y = h->y;
+  P.p0 = h->p0;
+  P.p1 = h->p1;
+  P.ap = h->ap;
+  P.project = project;
+  P.max_it = max_it;
+  P.tol = tol;
+  P.bar_count = h->bar_count;
+  P.bar_gen = h->bar_gen;
+  P.status = h->status;
+  P.prog_f = h->prog;
+  P.prog_b = h->prog + kMaxBlocks * 8;
+  P.partials = h->partials;
+  P.out = h->scal + 8;
+  P.nsweep = h->nsweep;
+  DN_TRY(reset_sync(h));
+  int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(h->nsweep, (h->n + 2047) / 2048));
+  blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
+  if (SWEEP == 0 && (long long)blocks * (kBlock / 32) < h->nsweep)
+    return fail(h, DN_ERR_UNSUPPORTED, "grid too wide for the co-resident wavefront warps");
+  void *args[] = {&P};
+  cudaEventRecord(h->kev[0], h->stream);
+  DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_pcg<S, SWEEP>, dim3(blocks), dim3(kBlock), args, 0, h->stream));
+  cudaEventRecord(h->kev[1], h->stream);
+  h->launches++;
+  int st = 0;
+  DN_TRY(read_status(h, &st));
+  if (st != kDevOk) return dev_status_to_dn(h, st);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+  h->phase_ms[S == 5 ? 4 : 5] += ms;
+  return read_scalars(h, 4, out);
+}
+
+dn_status run_bicgstab(dn_handle *h, double out[4]) {
+  BicgArgs P;
+  P.n = h->nm;
+  P.coef = h->mcoef;
+  P.tgt = h->mtgt;
+  P.b = h->mb;
+  P.x = h->mx;
+  P.r = h->mr;
+  P.rhat = h->mrhat;
+  P.p0 = h->mp0;
+  P.p1 = h->mp1;
+  P.v0 = h->mv0;
+  P.v1 = h->mv1;
+  P.phat = h->mphat;
+  P.s = h->ms;
+  P.shat = h->mshat;
+  P.t = h->mt;
+  P.upd = h->mupd;
+  P.dinv = h->mdinv;
+  P.max_it = h->cfg.momentum_iterations;
+  P.tol = h->cfg.momentum_tolerance;
+  P.use_rel = 0;  // momentum.cpp:470-472: absolute tolerance
+  P.bar_count = h->bar_count;
+  P.bar_gen = h->bar_gen;
+  P.status = h->status;
+  P.partials = h->partials;
+  P.out = h->scal + 8;
+  k_mom_dinv<<<blocks_for(h->nm), 256, 0, h->stream>>>(P);
+  DN_TRY(check_launch(h, "k_mom_dinv"));
+  DN_TRY(reset_sync(h));
+  int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(1, (h->nm + 2047) / 2048));
+  blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
+  void *args[] = {&P};
+  cudaEventRecord(h->kev[0], h->stream);
+  DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(blocks), dim3(kBlock), args, 0, h->stream));
+  cudaEventRecord(h->kev[1], h->stream);
+  h->launches++;
+  int st = 0;
+  DN_TRY(read_status(h, &st));
+  if (st != kDevOk) return dev_status_to_dn(h, st);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+  h->phase_ms[6] += ms;
+  return read_scalars(h, 4, out);
+}
+
+bool solve_ch(const dn_config &c) {
+  return c.mode != DN_MODE_ADVECTION_ONLY && !(c.mode == DN_MODE_SINGLE_PHASE || c.freeze_ch);
+}
+bool compute_mu(const dn_config &c) { return c.mode != DN_MODE_ADVECTION_ONLY && c.mode != DN_MODE_SINGLE_PHASE; }
+bool use_split(const dn_config &c) {
+  return c.pressure_scheme == DN_P_SPLIT_ICPCG || c.pressure_scheme == DN_P_SPLIT_ILDLT_PCG;
+}
+double rho_ref_of(const dn_config &c) { return std::min(1.0, c.density_ratio); }
+
+// ---------------------------------------------------------------------------------------------------
+// Step pieces
+// ---------------------------------------------------------------------------------------------------
+#define LAUNCH_INTERIOR(kernel, F, ...)                                                           \
+  do {                                                                                            \
+    kernel<<<blocks_for((long long)(F).nx * (F).ny), 256, 0, h->stream>>>(__VA_ARGS__);           \
+    DN_TRY(check_launch(h, #kernel));                                                             \
+  } while (0)
+
+dn_status materials(dn_handle *h, const Fv &c, const Fv &rho, const Fv &eta) {
+  LAUNCH_INTERIOR(k_materials, c, c, rho, eta, h->cfg.density_ratio, h->cfg.viscosity_ratio);
+  DN_TRY(bc(h, rho, kBCScalar));
+  return bc(h, eta, kBCScalar);
+}
+
+dn_status midpoint(dn_handle *h) {
+  Fv *f = h->f;
+  LAUNCH_INTERIOR(k_midpoint, f[DN_F_RHO_MID], f[DN_F_RHO_PREV], f[DN_F_RHO], f[DN_F_ETA_PREV], f[DN_F_ETA],
+                  f[DN_F_RHO_MID], f[DN_F_ETA_MID]);
+  DN_TRY(bc(h, f[DN_F_RHO_MID], kBCScalar));
+  return bc(h, f[DN_F_ETA_MID], kBCScalar);
+}
+
+dn_status chem(dn_handle *h, const Fv &c, const Fv &mu) {
+  LAUNCH_INTERIOR(k_chem, mu, c, mu, h->G, h->cfg.cn);
+  return bc(h, mu, kBCScalar);
+}
+
+dn_status refresh_mu(dn_handle *h) {
+  if (compute_mu(h->cfg)) return chem(h, h->f[DN_F_C], h->f[DN_F_MU]);
+  DN_TRY(fill_field(h, h->f[DN_F_MU], 0.0));
+  return bc(h, h->f[DN_F_MU], kBCScalar);
+}
+
+dn_status clear_surface_force(dn_handle *h) {
+  Fv *f = h->f;
+  for (int id : {DN_F_SFX_CELL, DN_F_SFY_CELL, DN_F_SFX_U, DN_F_SFY_V}) DN_TRY(fill_field(h, f[id], 0.0));
+  DN_TRY(bc(h, f[DN_F_SFX_CELL], kBCScalar));
+  DN_TRY(bc(h, f[DN_F_SFY_CELL], kBCScalar));
+  DN_TRY(bc(h, f[DN_F_SFX_U], kBCU));
+  return bc(h, f[DN_F_SFY_V], kBCV);
+}
+
+dn_status smooth(dn_handle *h, const Fv &f, const Fv &scratch, int kind) {
+  const double nw = h->cfg.surface_tension_smoothing_weight, cw = 1.0 - 4.0 * nw;
+  for (int pass = 0; pass < h->cfg.surface_tension_smoothing_passes; ++pass) {
+    DN_TRY(bc(h, f, kind));
+    LAUNCH_INTERIOR(k_smooth, scratch, f, scratch, cw, nw);
+    DN_TRY(bc(h, scratch, kind));
+    DN_TRY(copy_field(h, f, scratch));
+  }
+  return DN_OK;
+}
+
+// update_surface_tension_force, phase_field.cpp:179-256
+dn_status surface_force(dn_handle *h, const Fv &c_old, const Fv &c_new) {
+  const dn_config &cfg = h->cfg;
+  if (cfg.surface_tension_multiplier == 0.0 || !compute_mu(cfg)) return clear_surface_force(h);
+  Fv *f = h->f;
+  DN_TRY(copy_field(h, h->cmid, c_new));
+  LAUNCH_INTERIOR(k_cmid, h->cmid, c_old, c_new, h->cmid);
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  DN_TRY(fill_field(h, h->mm, 0.0));
+  DN_TRY(chem(h, h->cmid, h->mm));
+  const double scale = cfg.surface_tension_multiplier / (cfg.re * cfg.ca);
+  LAUNCH_INTERIOR(k_sf_cell, f[DN_F_SFX_CELL], h->mm, h->cmid, f[DN_F_SFX_CELL], f[DN_F_SFY_CELL], h->G, scale);
+  DN_TRY(bc(h, f[DN_F_SFX_CELL], kBCScalar));
+  DN_TRY(bc(h, f[DN_F_SFY_CELL], kBCScalar));
+  LAUNCH_INTERIOR(k_sf_u, f[DN_F_SFX_U], h->mm, h->cmid, f[DN_F_SFX_U], h->G, scale);
+  LAUNCH_INTERIOR(k_sf_v, f[DN_F_SFY_V], h->mm, h->cmid, f[DN_F_SFY_V], h->G, scale);
+  DN_TRY(bc(h, f[DN_F_SFX_U], kBCU));
+  DN_TRY(bc(h, f[DN_F_SFY_V], kBCV));
+  if (cfg.surface_tension_smoothing_passes <= 0 || cfg.surface_tension_smoothing_weight <= 0.0) return DN_OK;
+  DN_TRY(smooth(h, f[DN_F_SFX_CELL], h->sm_c, kBCScalar));
+  DN_TRY(smooth(h, f[DN_F_SFY_CELL], h->sm_c, kBCScalar));
+  DN_TRY(smooth(h, f[DN_F_SFX_U], h->sm_u, kBCU));
+  return smooth(h, f[DN_F_SFY_V], h->sm_v, kBCV);
+}
+
+// build_phase_explicit_operator, phase_field.cpp:354-396 -> h->E_new
+dn_status phase_explicit(dn_handle *h, const Fv &c, const Fv &u, const Fv &v) {
+  const dn_config &cfg = h->cfg;
+  LAUNCH_INTERIOR(k_mob_lap, h->mob, c, h->mob, h->lap, h->G);
+  DN_TRY(bc(h, h->mob, kBCScalar));
+  DN_TRY(bc(h, h->lap, kBCScalar));
+  LAUNCH_INTERIOR(k_lap, h->bih, h->lap, h->bih, h->G);
+  DN_TRY(bc(h, h->bih, kBCScalar));
+  DN_TRY(chem(h, c, h->mu_t));
+  LAUNCH_INTERIOR(k_adv_flux_x, h->afx, c, u, h->afx);
+  LAUNCH_INTERIOR(k_adv_flux_y, h->afy, c, v, h->afy);
+  DN_TRY(bc(h, h->afx, kBCU));
+  DN_TRY(bc(h, h->afy, kBCV));
+  LAUNCH_INTERIOR(k_flux_div, h->arhs, h->afx, h->afy, h->arhs, h->G, 1);
+  DN_TRY(bc(h, h->arhs, kBCScalar));
+  LAUNCH_INTERIOR(k_diff_flux_x, h->dfx, h->mu_t, h->mob, h->dfx, h->G);
+  LAUNCH_INTERIOR(k_diff_flux_y, h->dfy, h->mu_t, h->mob, h->dfy, h->G);
+  DN_TRY(bc(h, h->dfx, kBCU));
+  DN_TRY(bc(h, h->dfy, kBCV));
+  LAUNCH_INTERIOR(k_flux_div, h->ddiv, h->dfx, h->dfy, h->ddiv, h->G, 0);
+  DN_TRY(bc(h, h->ddiv, kBCScalar));
+  const double a1 = cfg.cn > 0.0 ? (3.0 * kSqrt2 / (16.0 * cfg.cn)) : 0.0;
+  const double a2 = cfg.cn > 0.0 ? (3.0 * kSqrt2 * cfg.cn / 4.0) : 0.0;
+  LAUNCH_INTERIOR(k_explicit, h->E_new, h->ddiv, h->lap, h->bih, h->arhs, h->E_new, a1, a2, cfg.pe);
+  return bc(h, h->E_new, kBCScalar);
+}
+
+// ensure_ch_linear_system, phase_field.cpp:130-142 (+ build_preconditioner, ch_sparse_krylov.hpp:434-442)
+dn_status ensure_ch_system(dn_handle *h, double alpha0) {
+  if (std::fabs(alpha0 - h->ch_alpha0) <= 1.0e-14 * std::max(1.0, std::fabs(alpha0))) return DN_OK;
+  const dn_config &cfg = h->cfg;
+  const double a1 = cfg.cn > 0.0 ? (3.0 * kSqrt2 / (16.0 * cfg.cn)) : 0.0;
+  const double a2 = cfg.cn > 0.0 ? (3.0 * kSqrt2 * cfg.cn / 4.0) : 0.0;
+  const double beta1 = a1 / cfg.pe, beta2 = a2 / cfg.pe;
+  DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+  k_ch_matrix<<<blocks_for(h->n, 128), 128, 0, h->stream>>>(h->G, alpha0, beta1, beta2, h->a13, h->status);
+  DN_TRY(check_launch(h, "k_ch_matrix"));
+  int st = 0;
+  DN_TRY(read_status(h, &st));
+  if (st) return fail(h, DN_ERR_UNSUPPORTED, "grid too small for the 13-point CH stencil");
+  Factor F{h->l13, h->d13, h->dinv13, 0.0};
+  k_factor<13><<<1, 1024, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, F, kPrecLDLT,
+                                           h->status);
+  DN_TRY(check_launch(h, "k_factor<13>"));
+  DN_TRY(read_status(h, &st));
+  if (st == kDevFactorFailed) {
+    h->ch_prec = kPrecDiag;
+    k_diag_inverse<13><<<blocks_for(h->n), 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py},
+                                                              h->dinv13);
+    DN_TRY(check_launch(h, "k_diag_inverse"));
+  } else {
+    h->ch_prec = kPrecLDLT;
+  }
+  h->ch_alpha0 = alpha0;
+  return DN_OK;
+}
+
+// solve_phase_linear_system_eq25, phase_field.cpp:437-503; b = rhs, x = initial guess (compact).  On exit x
+// holds the solution.
+dn_status ch_linear_solve(dn_handle *h, double alpha0, dn_report *rep, double *iter_res, double *eq_res) {
+  DN_TRY(ensure_ch_system(h, alpha0));
+  double out[4];
+  rep->ch_preconditioner = (h->ch_prec == kPrecLDLT) ? 1 : 0;
+  dn_status s;
+  if (h->ch_prec == kPrecLDLT)
+    s = run_pcg<13, 1>(h, h->a13, h->l13, h->dinv13, kPrecLDLT, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance, out);
+  else
+    s = run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance, out);
+  if (s == DN_ERR_PCG_BREAKDOWN) {
+    // phase_field.cpp:468-473: retry with the diagonal preconditioner from the current iterate
+    h->ch_prec = kPrecDiag;
+    k_diag_inverse<13><<<blocks_for(h->n), 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py},
+                                                              h->dinv13);
+    DN_TRY(check_launch(h, "k_diag_inverse"));
+    rep->ch_preconditioner = 2;
+    s = run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance, out);
+  }
+  DN_TRY(s);
+  rep->ch_iterations = (int)out[0];
+  *iter_res = out[3];
+  // equation residual ||b - A x|| / ||b||
+  const int nb = 128;
+  k_residual_partials<13><<<nb, 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, h->b,
+                                                      h->x, h->partials);
+  DN_TRY(check_launch(h, "k_residual_partials"));
+  std::vector<double> part(2 * nb);
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 64, h->partials, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  double rs = 0.0, bs = 0.0;
+  for (int k = 0; k < nb; ++k) {
+    rs += h->host_scal[64 + 2 * k];
+    bs += h->host_scal[64 + 2 * k + 1];
+  }
+  *eq_res = std::sqrt(rs / std::max(bs, 1.0e-30));
+  return DN_OK;
+}
+
+// solve_cahn_hilliard_semi_implicit, phase_field.cpp:667-708
+dn_status ch_semi_implicit(dn_handle *h, int step, dn_report *rep) {
+  Fv *f = h->f;
+  DN_TRY(phase_explicit(h, f[DN_F_C], f[DN_F_U], f[DN_F_V]));
+  const double dt = h->cfg.dt;
+  const double alpha0 = (step == 0) ? (1.0 / dt) : (3.0 / (2.0 * dt));
+  LAUNCH_INTERIOR(k_ch_rhs, h->E_new, f[DN_F_C_PREV], f[DN_F_C_PREV2], h->E_new, f[DN_F_E_PREV], h->b, h->x, f[DN_F_C],
+                  step, dt);
+  double iter_res = 0.0, eq_res = 0.0;
+  DN_TRY(ch_linear_solve(h, alpha0, rep, &iter_res, &eq_res));
+  LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_C], h->x, f[DN_F_C]);
+  DN_TRY(bc(h, f[DN_F_C], kBCScalar));
+  DN_TRY(chem(h, f[DN_F_C], f[DN_F_MU]));
+  rep->ch_equation_residual = eq_res;
+  rep->ch_residual = iter_res;
+  return copy_field(h, f[DN_F_E_PREV], h->E_new);
+}
+
+dn_status phase(dn_handle *h, int step, dn_report *rep) {
+  Fv *f = h->f;
+  if (solve_ch(h->cfg)) {
+    DN_TRY(ch_semi_implicit(h, step, rep));
+    DN_TRY(materials(h, f[DN_F_C], f[DN_F_RHO], f[DN_F_ETA]));
+    DN_TRY(midpoint(h));
+    DN_TRY(surface_force(h, f[DN_F_C_PREV], f[DN_F_C]));
+    rep->coupling_iterations = 1;
+    return DN_OK;
+  }
+  DN_TRY(materials(h, f[DN_F_C], f[DN_F_RHO], f[DN_F_ETA]));
+  DN_TRY(midpoint(h));
+  DN_TRY(refresh_mu(h));
+  DN_TRY(surface_force(h, f[DN_F_C_PREV], f[DN_F_C]));
+  rep->ch_iterations = 0;
+  rep->ch_preconditioner = -1;
+  rep->ch_equation_residual = 0.0;
+  rep->ch_residual = 0.0;
+  rep->coupling_iterations = 0;
+  return DN_OK;
+}
+
+// compute_momentum_fluxes + solve_momentum_predictor, momentum.cpp:55-502
+dn_status momentum(dn_handle *h, int step, dn_report *rep) {
+  Fv *f = h->f;
+  const dn_config &cfg = h->cfg;
+  DN_TRY(fill_field(h, h->hu, 0.0));
+  DN_TRY(fill_field(h, h->hv, 0.0));
+  LAUNCH_INTERIOR(k_mom_flux_u, h->hu, f[DN_F_U], f[DN_F_V], h->hu, h->G);
+  LAUNCH_INTERIOR(k_mom_flux_v, h->hv, f[DN_F_U], f[DN_F_V], h->hv, h->G);
+  DN_TRY(bc(h, h->hu, kBCU));
+  DN_TRY(bc(h, h->hv, kBCV));
+  const double alpha = 0.5 * cfg.dt / cfg.re;
+  LAUNCH_INTERIOR(k_mom_rhs_u, h->urhs, f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hu, f[DN_F_HU_PREV],
+                  f[DN_F_SFX_U], h->urhs, h->G, step, cfg.dt, alpha, cfg.body_force_x);
+  LAUNCH_INTERIOR(k_mom_rhs_v, h->vrhs, f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hv, f[DN_F_HV_PREV],
+                  f[DN_F_SFY_V], h->vrhs, h->G, step, cfg.dt, alpha, cfg.body_force_y);
+  k_mom_assemble<<<blocks_for(h->nm, 128), 128, 0, h->stream>>>(h->ml, h->G, h->bc, f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID],
+                                                           f[DN_F_ETA], h->urhs, h->vrhs, alpha, h->mcoef, h->mtgt, h->mb,
+                                                           h->mx);
+  DN_TRY(check_launch(h, "k_mom_assemble"));
+  double out[4];
+  DN_TRY(run_bicgstab(h, out));
+  rep->momentum_iterations = (int)out[0];
+  rep->momentum_residual = out[1];
+  DN_TRY(copy_field(h, f[DN_F_U_STAR], f[DN_F_U]));
+  DN_TRY(copy_field(h, f[DN_F_V_STAR], f[DN_F_V]));
+  k_mom_scatter<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, h->mx, f[DN_F_U_STAR], f[DN_F_V_STAR]);
+  DN_TRY(check_launch(h, "k_mom_scatter"));
+  DN_TRY(bc(h, f[DN_F_U_STAR], kBCU));
+  DN_TRY(bc(h, f[DN_F_V_STAR], kBCV));
+  DN_TRY(copy_field(h, f[DN_F_HU_PREV], h->hu));
+  return copy_field(h, f[DN_F_HV_PREV], h->hv);
+}
+
+dn_status split_extrapolation(dn_handle *h, int step) {
+  Fv *f = h->f;
+  LAUNCH_INTERIOR(k_p_ext, h->pe, f[DN_F_P], f[DN_F_P_PREV], h->pe, step == 0 ? 1 : 0);
+  return bc(h, h->pe, kBCPressure);
+}
+
+// solve_pressure_correction_{icpcg,ildlt_pcg,liu_split_icpcg,liu_split_ildlt_pcg}, pressure.cpp:302-365, 470-491
+dn_status pressure(dn_handle *h, int step, dn_report *rep) {
+  Fv *f = h->f;
+  const dn_config &cfg = h->cfg;
+  if (cfg.pressure_scheme == DN_P_JACOBI)
+    return fail(h, DN_ERR_UNSUPPORTED, "pressure_scheme jacobi is not implemented by the CUDA backend");
+  const bool split = use_split(cfg);
+  const bool icc = cfg.pressure_scheme == DN_P_ICPCG || cfg.pressure_scheme == DN_P_SPLIT_ICPCG;
+  DN_TRY(fill_field(h, f[DN_F_P_CORR], 0.0));
+  DN_TRY(bc(h, f[DN_F_P_CORR], kBCPressure));
+  const double rho_ref = split ? rho_ref_of(cfg) : 1.0;
+  if (split) DN_TRY(split_extrapolation(h, step));
+  k_p_assemble<<<blocks_for(h->n), 256, 0, h->stream>>>(h->G, h->bc, f[DN_F_RHO_MID], f[DN_F_U_STAR], f[DN_F_V_STAR],
+                                                       h->pe, split ? 1 : 0, rho_ref, cfg.dt, h->a5, h->b);
+  DN_TRY(check_launch(h, "k_p_assemble"));
+  if (!h->has_dirichlet) {  // regularize_pressure_linear_system, pressure.cpp:198-212
+    const int nb = 128;
+    k_vec_sum<<<nb, 256, 0, h->stream>>>(h->b, h->n, h->partials);
+    DN_TRY(check_launch(h, "k_vec_sum"));
+    k_finish_mean<<<1, 32, 0, h->stream>>>(h->partials, nb, (double)h->n, h->scal);
+    DN_TRY(check_launch(h, "k_finish_mean"));
+    k_vec_sub_scalar<<<blocks_for(h->n), 256, 0, h->stream>>>(h->b, h->n, h->scal);
+    DN_TRY(check_launch(h, "k_vec_sub_scalar"));
+  }
+  // The split operator is constant, so its factor is built once; the variable one every step.
+  const int kind = icc ? kPrecICC : kPrecLDLT;
+  if (!(split && h->p_factor_valid && h->p_factor_kind == kind)) {
+    DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    Factor F{h->l5, h->d5, h->dinv5, 0.0};
+    k_factor<5><<<1, 1024, 0, h->stream>>>(SpOp{h->a5, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, F, kind,
+                                            h->status);
+    DN_TRY(check_launch(h, "k_factor<5>"));
+    int st = 0;
+    DN_TRY(read_status(h, &st));
+    if (st == kDevFactorFailed) {
+      h->p_factor_valid = false;
+      return fail(h, icc ? DN_ERR_ICC_FAILED : DN_ERR_ILDLT_FAILED,
+                  icc ? "ICC preconditioner construction failed" : "ILDLT preconditioner construction failed");
+    }
+    h->p_factor_valid = split;
+    h->p_factor_kind = kind;
+  }
+  DN_CUDA(h, cudaMemsetAsync(h->x, 0, h->n * sizeof(double), h->stream));
+  double out[4];
+  DN_TRY((run_pcg<5, 0>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
+                        cfg.pressure_tolerance, out)));
+  rep->pressure_iterations = (int)out[0];
+  rep->pressure_residual = out[2];
+  h->phase_ms[7] = out[0];
+  LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], h->x, f[DN_F_P_CORR]);
+  if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
+  return bc(h, f[DN_F_P_CORR], kBCPressure);
+}
+
+// apply_pressure_velocity_correction, operators.cpp:480-534
+dn_status correct(dn_handle *h, int step, dn_report *rep) {
+  Fv *f = h->f;
+  const dn_config &cfg = h->cfg;
+  k_boundary_speed<<<1, 256, 0, h->stream>>>(f[DN_F_U_STAR], f[DN_F_V_STAR], h->G, h->scal + 16);
+  DN_TRY(check_launch(h, "k_boundary_speed"));
+  const bool split = use_split(cfg);
+  const double rho_ref = split ? rho_ref_of(cfg) : 1.0;
+  if (split) DN_TRY(split_extrapolation(h, step));
+  LAUNCH_INTERIOR(k_correct_u, f[DN_F_U], f[DN_F_U], f[DN_F_U_STAR], f[DN_F_RHO_MID], f[DN_F_P_CORR], h->pe, h->G,
+                  split ? 1 : 0, rho_ref, cfg.dt);
+  LAUNCH_INTERIOR(k_correct_v, f[DN_F_V], f[DN_F_V], f[DN_F_V_STAR], f[DN_F_RHO_MID], f[DN_F_P_CORR], h->pe, h->G,
+                  split ? 1 : 0, rho_ref, cfg.dt);
+  DN_TRY(bc(h, f[DN_F_U], kBCU));
+  DN_TRY(bc(h, f[DN_F_V], kBCV));
+  k_boundary_speed<<<1, 256, 0, h->stream>>>(f[DN_F_U], f[DN_F_V], h->G, h->scal + 17);
+  DN_TRY(check_launch(h, "k_boundary_speed"));
+  DN_TRY(copy_field(h, f[DN_F_P_PREV], f[DN_F_P]));
+  LAUNCH_INTERIOR(k_copy_interior, f[DN_F_P], f[DN_F_P], f[DN_F_P_CORR]);
+  if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P]));
+  DN_TRY(bc(h, f[DN_F_P], kBCPressure));
+  double bs[2];
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->scal + 16, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(bs, h->host_scal, sizeof bs);
+  rep->boundary_speed_pre = bs[0];
+  rep->boundary_speed_post = bs[1];
+  return DN_OK;
+}
+
+dn_status begin_step(dn_handle *h) {
+  Fv *f = h->f;
+  DN_TRY(copy_field(h, f[DN_F_C_PREV2], f[DN_F_C_PREV]));
+  DN_TRY(copy_field(h, f[DN_F_C_PREV], f[DN_F_C]));
+  DN_TRY(copy_field(h, f[DN_F_RHO_PREV], f[DN_F_RHO]));
+  DN_TRY(copy_field(h, f[DN_F_ETA_PREV], f[DN_F_ETA]));
+  DN_TRY(copy_field(h, f[DN_F_U_PREV], f[DN_F_U]));
+  return copy_field(h, f[DN_F_V_PREV], f[DN_F_V]);
+}
+
+}  // namespace
+
+// ===================================================================================================
+// C-ABI
+// ===================================================================================================
+extern "C" {
+
+const char *dn_status_string(dn_status s) {
+  switch (s) {
+  case DN_OK: return "ok";
+  case DN_ERR_INVALID_ARGUMENT: return "invalid argument";
+  case DN_ERR_CONFIG: return "invalid configuration";
+  case DN_ERR_CUDA: return "CUDA error";
+  case DN_ERR_ICC_FAILED: return "ICC preconditioner construction failed";
+  case DN_ERR_ILDLT_FAILED: return "ILDLT preconditioner construction failed";
+  case DN_ERR_PCG_BREAKDOWN: return "pcg breakdown";
+  case DN_ERR_BICGSTAB_BREAKDOWN: return "bicgstab breakdown";
+  case DN_ERR_TIMEOUT: return "device wait timed out";
+  case DN_ERR_NONFINITE: return "non-finite diagnostic detected";
+  case DN_ERR_UNSUPPORTED: return "unsupported configuration";
+  }
+  return "unknown status";
+}
+
+const char *dn_last_error(const dn_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
+  if (!cfg || !out) return DN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  dn_handle *h = new dn_handle();
+  h->cfg = *cfg;
+  const dn_config &c = h->cfg;
+  auto bad = [&](dn_status s, const std::string &m) {
+    h->err = m;
+    *out = h;
+    return s;
+  };
+  if (c.nx < 8 || c.ny < 8) return bad(DN_ERR_UNSUPPORTED, "the CUDA backend needs nx, ny >= 8");
+  if (c.ghost < 3) return bad(DN_ERR_UNSUPPORTED, "ghost must be >= 3 (WENO5 stencil)");
+  if ((long long)c.nx * c.ny > (1LL << 30)) return bad(DN_ERR_UNSUPPORTED, "grid too large");
+  if (c.mode == DN_MODE_ADVECTION_ONLY)
+    return bad(DN_ERR_UNSUPPORTED, "mode advection_only is not implemented by the CUDA backend");
+  // validate_boundary_configuration, operators.cpp:11-34
+  static const char *names[4] = {"left", "right", "bottom", "top"};
+  for (int s = 0; s < 4; ++s) {
+    const int periodic = (s < 2) ? c.periodic_x : c.periodic_y;
+    if (!periodic) continue;
+    if (c.p_bc[s].type != DN_BC_UNSET)
+      return bad(DN_ERR_CONFIG, std::string("pressure_bc_") + names[s] + " cannot be set when the direction is periodic");
+    if (c.u_bc[s].type != DN_BC_UNSET)
+      return bad(DN_ERR_CONFIG, std::string("u_bc_") + names[s] + " cannot be set when the direction is periodic");
+    if (c.v_bc[s].type != DN_BC_UNSET)
+      return bad(DN_ERR_CONFIG, std::string("v_bc_") + names[s] + " cannot be set when the direction is periodic");
+  }
+  if (c.surface_tension_smoothing_passes < 0)
+    return bad(DN_ERR_CONFIG, "surface_tension_smoothing_passes must be non-negative");
+  if (c.surface_tension_smoothing_weight < 0.0 || c.surface_tension_smoothing_weight > 0.25)
+    return bad(DN_ERR_CONFIG, "surface_tension_smoothing_weight must lie in [0, 0.25]");
+  if (c.precision != DN_PRECISION_FP64)
+    return bad(DN_ERR_UNSUPPORTED, "precision mixed is not available in this build");
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bad(DN_ERR_CUDA, "no CUDA device available");
+  if (device < 0) cudaGetDevice(&device);
+  h->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return bad(DN_ERR_CUDA, "cudaSetDevice failed");
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  h->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
+  for (auto &e : h->ev) cudaEventCreate(&e);
+  for (auto &e : h->kev) cudaEventCreate(&e);
+
+  // grid and effective BCs (operators.cpp:36-112)
+  h->G.nx = c.nx;
+  h->G.ny = c.ny;
+  h->G.g = c.ghost;
+  h->G.px = c.periodic_x;
+  h->G.py = c.periodic_y;
+  h->G.dx = c.lx / std::max((double)c.nx, 1.0);
+  h->G.dy = c.ly / std::max((double)c.ny, 1.0);
+  for (int s = 0; s < 4; ++s) {
+    h->bc.p[s] = c.p_bc[s].type != DN_BC_UNSET ? BCSide{c.p_bc[s].type, c.p_bc[s].value} : BCSide{DN_BC_NEUMANN, 0.0};
+    h->bc.v[s] = c.v_bc[s].type != DN_BC_UNSET ? BCSide{c.v_bc[s].type, c.v_bc[s].value} : BCSide{DN_BC_DIRICHLET, 0.0};
+    if (c.u_bc[s].type != DN_BC_UNSET) {
+      h->bc.u[s] = BCSide{c.u_bc[s].type, c.u_bc[s].value};
+    } else {
+      double v = 0.0;
+      if (s == DN_BOTTOM) v = c.bottom_wall_velocity_x;
+      if (s == DN_TOP) v = c.top_wall_velocity_x;
+      h->bc.u[s] = BCSide{DN_BC_DIRICHLET, v};
+    }
+  }
+  h->has_dirichlet = (!c.periodic_x && (h->bc.p[0].type == DN_BC_DIRICHLET || h->bc.p[1].type == DN_BC_DIRICHLET)) ||
+                     (!c.periodic_y && (h->bc.p[2].type == DN_BC_DIRICHLET || h->bc.p[3].type == DN_BC_DIRICHLET));
+
+  dn_status s = DN_OK;
+  auto A = [&](dn_status st) {
+    if (s == DN_OK) s = st;
+  };
+  const int nx = c.nx, ny = c.ny;
+  for (int k = 0; k < DN_F_COUNT; ++k) {
+    const bool one = k == DN_F_RHO || k == DN_F_ETA || k == DN_F_RHO_PREV || k == DN_F_ETA_PREV ||
+                     k == DN_F_RHO_MID || k == DN_F_ETA_MID;
+    A(falloc(h, h->f[k], is_uish(k) ? nx + 1 : nx, is_vish(k) ? ny + 1 : ny, one ? 1.0 : 0.0));
+  }
+  for (Fv *w : {&h->mob, &h->lap, &h->bih, &h->mu_t, &h->arhs, &h->ddiv, &h->E_new, &h->cmid, &h->mm, &h->pe, &h->sm_c})
+    A(falloc(h, *w, nx, ny, 0.0));
+  for (Fv *w : {&h->afx, &h->dfx, &h->urhs, &h->hu, &h->sm_u}) A(falloc(h, *w, nx + 1, ny, 0.0));
+  for (Fv *w : {&h->afy, &h->dfy, &h->vrhs, &h->hv, &h->sm_v}) A(falloc(h, *w, nx, ny + 1, 0.0));
+  h->n = (long long)nx * ny;
+  for (double **p : {&h->b, &h->x, &h->r, &h->z, &h->y, &h->p0, &h->p1, &h->ap, &h->d5, &h->dinv5, &h->d13, &h->dinv13})
+    A(dalloc(h, p, h->n));
+  A(dalloc(h, &h->a5, 5 * h->n));
+  A(dalloc(h, &h->l5, 5 * h->n));
+  A(dalloc(h, &h->a13, 13 * h->n));
+  A(dalloc(h, &h->l13, 13 * h->n));
+  h->ml = MomLayout{nx, ny, c.periodic_x, c.periodic_y, (long long)(nx + 1) * ny, (long long)nx * (ny + 1)};
+  h->nm = h->ml.nu + h->ml.nv;
+  A(dalloc(h, &h->mcoef, 9 * h->nm));
+  A(dalloc(h, &h->mtgt, 9 * h->nm));
+  for (double **p : {&h->mb, &h->mx, &h->mr, &h->mrhat, &h->mp0, &h->mp1, &h->mv0, &h->mv1, &h->mphat, &h->ms, &h->mshat,
+                     &h->mt, &h->mupd, &h->mdinv})
+    A(dalloc(h, p, h->nm));
+  A(dalloc(h, &h->bar_count, 1));
+  A(dalloc(h, &h->bar_gen, 1));
+  A(dalloc(h, &h->status, 1));
+  A(dalloc(h, &h->prog, 2 * (size_t)kMaxBlocks * 8));
+  A(dalloc(h, &h->partials, 2 * (size_t)kMaxBlocks * 8));
+  A(dalloc(h, &h->scal, 64));
+  if (s == DN_OK && cudaMallocHost(&h->host_scal, kHostScal * sizeof(double)) != cudaSuccess) s = DN_ERR_CUDA;
+  if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+  h->nsweep = (nx + 31) / 32;
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg<5, 0>, kBlock, 0);
+  int occ2 = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg<13, 1>, kBlock, 0);
+  int occ3 = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_bicgstab, kBlock, 0);
+  occ = std::min(occ, std::min(occ2, occ3));
+  h->max_coop_blocks = std::min(kMaxBlocks, std::max(1, occ) * h->num_sms);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bad(DN_ERR_CUDA, "initial synchronisation failed");
+  *out = h;
+  return DN_OK;
+}
+
+dn_status dn_destroy(dn_handle *h) {
+  if (!h) return DN_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void *p : h->allocations) cudaFree(p);
+  if (h->host_scal) cudaFreeHost(h->host_scal);
+  for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : h->kev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return DN_OK;
+}
+
+dn_status dn_initialize(dn_handle *h) {
+  if (!h || !h->stream) return DN_ERR_INVALID_ARGUMENT;
+  const dn_config &c = h->cfg;
+  Fv *f = h->f;
+  InitParams P{};
+  P.mode = c.mode;
+  P.phase_initializer = c.phase_initializer;
+  P.velocity_profile = c.velocity_profile;
+  P.invert_phase = c.invert_phase;
+  P.cn = c.cn;
+  P.lx = c.lx;
+  P.ly = c.ly;
+  P.cx = c.interface_center_x;
+  P.cy = c.interface_center_y;
+  P.radius = c.interface_radius;
+  P.amplitude = c.interface_amplitude;
+  P.wavenumber = c.interface_wavenumber;
+  P.slot_w = c.zalesak_slot_width;
+  P.slot_d = c.zalesak_slot_depth;
+  P.advect_u = c.advect_u;
+  P.advect_v = c.advect_v;
+  P.rcx = c.rotation_center_x;
+  P.rcy = c.rotation_center_y;
+  P.omega = c.angular_velocity;
+  P.ub = h->bc.u[DN_BOTTOM].value;
+  P.ut = h->bc.u[DN_TOP].value;
+  P.couette = !c.periodic_y && h->bc.u[DN_BOTTOM].type == DN_BC_DIRICHLET && h->bc.u[DN_TOP].type == DN_BC_DIRICHLET &&
+              (std::fabs(P.ut) > 0.0 || std::fabs(P.ub) > 0.0);
+  LAUNCH_INTERIOR(k_init_phase, f[DN_F_C], f[DN_F_C], h->G, P);
+  k_init_u<<<blocks_for((long long)f[DN_F_U].size()), 256, 0, h->stream>>>(f[DN_F_U], h->G, P, 1);
+  DN_TRY(check_launch(h, "k_init_u"));
+  k_init_v<<<blocks_for((long long)f[DN_F_V].size()), 256, 0, h->stream>>>(f[DN_F_V], h->G, P);
+  DN_TRY(check_launch(h, "k_init_v"));
+  if (c.velocity_profile != 1) {
+    DN_TRY(bc(h, f[DN_F_U], kBCU));
+    DN_TRY(bc(h, f[DN_F_V], kBCV));
+  }
+  DN_TRY(bc(h, f[DN_F_C], kBCScalar));
+  DN_TRY(copy_field(h, f[DN_F_C_PREV], f[DN_F_C]));
+  DN_TRY(copy_field(h, f[DN_F_C_PREV2], f[DN_F_C]));
+  DN_TRY(copy_field(h, f[DN_F_U_PREV], f[DN_F_U]));
+  DN_TRY(copy_field(h, f[DN_F_V_PREV], f[DN_F_V]));
+  DN_TRY(materials(h, f[DN_F_C], f[DN_F_RHO], f[DN_F_ETA]));
+  DN_TRY(copy_field(h, f[DN_F_RHO_PREV], f[DN_F_RHO]));
+  DN_TRY(copy_field(h, f[DN_F_ETA_PREV], f[DN_F_ETA]));
+  DN_TRY(copy_field(h, f[DN_F_RHO_MID], f[DN_F_RHO]));
+  DN_TRY(copy_field(h, f[DN_F_ETA_MID], f[DN_F_ETA]));
+  DN_TRY(refresh_mu(h));
+  DN_TRY(clear_surface_force(h));
+  double m = 0.0;
+  DN_TRY(dn_compute_mass(h, DN_F_C, &m));
+  h->initial_mass = m;
+  DN_TRY(fill_field(h, f[DN_F_P], 0.0));
+  DN_TRY(bc(h, f[DN_F_P], kBCPressure));
+  DN_TRY(copy_field(h, f[DN_F_P_PREV], f[DN_F_P]));
+  DN_TRY(fill_field(h, f[DN_F_E_PREV], 0.0));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+dn_status dn_set_field(dn_handle *h, int field, const double *host, size_t count) {
+  if (!h || !host || field < 0 || field >= DN_F_COUNT) return DN_ERR_INVALID_ARGUMENT;
+  if (count != h->f[field].size()) return fail(h, DN_ERR_INVALID_ARGUMENT, "field size mismatch");
+  DN_CUDA(h, cudaMemcpyAsync(h->f[field].d, host, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+dn_status dn_get_field(dn_handle *h, int field, double *host, size_t count) {
+  if (!h || !host || field < 0 || field >= DN_F_COUNT) return DN_ERR_INVALID_ARGUMENT;
+  if (count != h->f[field].size()) return fail(h, DN_ERR_INVALID_ARGUMENT, "field size mismatch");
+  DN_CUDA(h, cudaMemcpyAsync(host, h->f[field].d, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+dn_status dn_field_device_ptr(dn_handle *h, int field, double **dev_ptr, size_t *count) {
+  if (!h || field < 0 || field >= DN_F_COUNT) return DN_ERR_INVALID_ARGUMENT;
+  if (dev_ptr) *dev_ptr = h->f[field].d;
+  if (count) *count = h->f[field].size();
+  return DN_OK;
+}
+
+void dn_set_initial_mass(dn_handle *h, double mass) {
+  if (h) h->initial_mass = mass;
+}
+
+dn_status dn_refresh_derived(dn_handle *h) {
+  if (!h) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  DN_TRY(bc(h, f[DN_F_C], kBCScalar));
+  DN_TRY(bc(h, f[DN_F_C_PREV], kBCScalar));
+  DN_TRY(bc(h, f[DN_F_C_PREV2], kBCScalar));
+  DN_TRY(bc(h, f[DN_F_P], kBCPressure));
+  DN_TRY(bc(h, f[DN_F_P_PREV], kBCPressure));
+  DN_TRY(bc(h, f[DN_F_U], kBCU));
+  DN_TRY(bc(h, f[DN_F_V], kBCV));
+  DN_TRY(bc(h, f[DN_F_U_PREV], kBCU));
+  DN_TRY(bc(h, f[DN_F_V_PREV], kBCV));
+  DN_TRY(materials(h, f[DN_F_C], f[DN_F_RHO], f[DN_F_ETA]));
+  DN_TRY(materials(h, f[DN_F_C_PREV], f[DN_F_RHO_PREV], f[DN_F_ETA_PREV]));
+  DN_TRY(midpoint(h));
+  DN_TRY(refresh_mu(h));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+dn_status dn_begin_step(dn_handle *h, int step) {
+  if (!h) return DN_ERR_INVALID_ARGUMENT;
+  h->step = step;
+  return begin_step(h);
+}
+
+dn_status dn_phase(dn_handle *h, int step, dn_report *rep) {
+  if (!h || !rep) return DN_ERR_INVALID_ARGUMENT;
+  return phase(h, step, rep);
+}
+
+dn_status dn_momentum(dn_handle *h, int step, dn_report *rep) {
+  if (!h || !rep) return DN_ERR_INVALID_ARGUMENT;
+  return momentum(h, step, rep);
+}
+
+dn_status dn_pressure(dn_handle *h, dn_report *rep) {
+  if (!h || !rep) return DN_ERR_INVALID_ARGUMENT;
+  return pressure(h, h->step, rep);
+}
+
+dn_status dn_correct(dn_handle *h, dn_report *rep) {
+  if (!h || !rep) return DN_ERR_INVALID_ARGUMENT;
+  return correct(h, h->step, rep);
+}
+
+dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
+  if (!h) return DN_ERR_INVALID_ARGUMENT;
+  dn_report local;
+  if (!rep) rep = &local;
+  std::memset(rep, 0, sizeof(*rep));
+  rep->ch_preconditioner = -1;
+  h->step = step;
+  for (int k = 4; k < 8; ++k) h->phase_ms[k] = 0.0;
+  cudaEventRecord(h->ev[0], h->stream);
+  DN_TRY(begin_step(h));
+  DN_TRY(phase(h, step, rep));
+  cudaEventRecord(h->ev[1], h->stream);
+  DN_TRY(momentum(h, step, rep));
+  cudaEventRecord(h->ev[2], h->stream);
+  DN_TRY(pressure(h, step, rep));
+  cudaEventRecord(h->ev[3], h->stream);
+  DN_TRY(correct(h, step, rep));
+  cudaEventRecord(h->ev[4], h->stream);
+  DN_CUDA(h, cudaEventSynchronize(h->ev[4]));
+  for (int k = 0; k < 4; ++k) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, h->ev[k], h->ev[k + 1]);
+    h->phase_ms[k] = ms;
+  }
+  return DN_OK;
+}
+
+dn_status dn_ch_linear_solve(dn_handle *h, const double *rhs_field, double alpha0, double *c_state,
+                             double *iterate_residual, double *equation_residual, int *iterations) {
+  if (!h || !rhs_field || !c_state) return DN_ERR_INVALID_ARGUMENT;
+  // stage rhs and c_state through the work fields (cell-field layout)
+  const size_t cnt = h->E_new.size();
+  DN_CUDA(h, cudaMemcpyAsync(h->E_new.d, rhs_field, cnt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(h->cmid.d, c_state, cnt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  LAUNCH_INTERIOR(k_gather_compact, h->E_new, h->E_new, h->b);
+  LAUNCH_INTERIOR(k_gather_compact, h->cmid, h->cmid, h->x);
+  dn_report rep{};
+  double it = 0.0, eq = 0.0;
+  DN_TRY(ch_linear_solve(h, alpha0, &rep, &it, &eq));
+  LAUNCH_INTERIOR(k_scatter_compact, h->cmid, h->x, h->cmid);
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  DN_CUDA(h, cudaMemcpyAsync(c_state, h->cmid.d, cnt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (iterate_residual) *iterate_residual = it;
+  if (equation_residual) *equation_residual = eq;
+  if (iterations) *iterations = rep.ch_iterations;
+  return DN_OK;
+}
+
+dn_status dn_pressure_solve(dn_handle *h, int step, const double *u_star, const double *v_star, const double *rho_mid,
+                            const double *p, const double *p_prev, double *p_corr, int *iterations,
+                            double *relative_residual) {
+  if (!h || !u_star || !v_star || !rho_mid || !p || !p_prev || !p_corr) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  auto up = [&](int id, const double *src) -> dn_status {
+    DN_CUDA(h, cudaMemcpyAsync(f[id].d, src, f[id].size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    return DN_OK;
+  };
+  DN_TRY(up(DN_F_U_STAR, u_star));
+  DN_TRY(up(DN_F_V_STAR, v_star));
+  DN_TRY(up(DN_F_RHO_MID, rho_mid));
+  DN_TRY(up(DN_F_P, p));
+  DN_TRY(up(DN_F_P_PREV, p_prev));
+  dn_report rep{};
+  DN_TRY(pressure(h, step, &rep));
+  DN_CUDA(h, cudaMemcpyAsync(p_corr, f[DN_F_P_CORR].d, f[DN_F_P_CORR].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                             h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (iterations) *iterations = rep.pressure_iterations;
+  if (relative_residual) *relative_residual = rep.pressure_residual;
+  return DN_OK;
+}
+
+dn_status dn_compute_mass(dn_handle *h, int field, double *mass) {
+  if (!h || !mass || field < 0 || field >= DN_F_COUNT) return DN_ERR_INVALID_ARGUMENT;
+  const int nb = 128;
+  const Fv &f = h->f[field];
+  k_field_sum<<<nb, 256, 0, h->stream>>>(f, h->G.dx * h->G.dy, h->partials);
+  DN_TRY(check_launch(h, "k_field_sum"));
+  k_finish_mean<<<1, 32, 0, h->stream>>>(h->partials, nb, 1.0, h->scal + 8);
+  DN_TRY(check_launch(h, "k_finish_mean"));
+  return read_scalars(h, 1, mass);
+}
+
+dn_status dn_diagnostics(dn_handle *h, dn_diag *d) {
+  if (!h || !d) return DN_ERR_INVALID_ARGUMENT;
+  const int nb = 128;
+  Fv *f = h->f;
+  k_diag_partials<<<nb, 256, 0, h->stream>>>(f[DN_F_C], f[DN_F_U], f[DN_F_V], f[DN_F_MU], f[DN_F_RHO], f[DN_F_ETA], h->G,
+                                             h->cfg.cn, h->partials);
+  DN_TRY(check_launch(h, "k_diag_partials"));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->partials, (size_t)nb * kNDiag * sizeof(double), cudaMemcpyDeviceToHost,
+                             h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  const int ops[kNDiag] = {0, 0, 1, 1, 1, 0, 2, 1, 2, 1, 0, 1, 1, 1};
+  double a[kNDiag];
+  for (int k = 0; k < kNDiag; ++k) {
+    a[k] = ops[k] == 0 ? 0.0 : (ops[k] == 1 ? -INFINITY : INFINITY);
+    for (int b = 0; b < nb; ++b) {
+      const double v = h->host_scal[b * kNDiag + k];
+      a[k] = ops[k] == 0 ? a[k] + v : (ops[k] == 1 ? std::max(a[k], v) : std::min(a[k], v));
+    }
+  }
+  const dn_config &c = h->cfg;
+  std::memset(d, 0, sizeof(*d));
+  d->mass = a[0];
+  d->mass_drift = std::fabs(a[0] - h->initial_mass);
+  d->divergence_l2 = std::sqrt(a[1] / (double)(c.nx * c.ny));
+  d->max_divergence = std::max(0.0, a[2]);
+  d->max_abs_mu = std::max(0.0, a[3]);
+  d->max_velocity = std::max(0.0, a[4]);
+  d->kinetic_energy = a[5];
+  d->rho_min = a[6];
+  d->rho_max = std::max(0.0, a[7]);
+  d->eta_min = a[8];
+  d->eta_max = std::max(0.0, a[9]);
+  d->total_free_energy = a[10];
+  // populate_timestep_limits, diagnostics.cpp:48-112
+  const double h_ = std::min(h->G.dx, h->G.dy), tiny = 1.0e-30;
+  const double mar = std::max(0.0, a[11]);
+  d->dt_limit_advective = mar > tiny ? 0.5 / mar : INFINITY;
+  d->dt_limit_capillary = INFINITY;
+  d->dt_limit_ch_explicit = INFINITY;
+  if (solve_ch(c)) {
+    const double rs = std::max(d->rho_max, tiny);
+    d->dt_limit_capillary = 0.5 * std::sqrt(std::max(c.re * c.ca * h_ * h_ * h_ / rs, 0.0));
+    const double mob = std::max(0.0, a[12]), wpp = std::max(0.0, a[13]);
+    if (mob > tiny) {
+      const double coeff = 6.0 * kSqrt2 * mob * wpp / std::max(c.pe * c.cn, tiny);
+      d->dt_limit_ch_explicit = coeff > tiny ? 0.25 * h_ * h_ / coeff : INFINITY;
+    }
+  }
+  d->dt_limit_active = d->dt_limit_advective;
+  if (d->dt_limit_capillary < d->dt_limit_active) d->dt_limit_active = d->dt_limit_capillary;
+  if (d->dt_limit_ch_explicit < d->dt_limit_active) d->dt_limit_active = d->dt_limit_ch_explicit;
+  d->dt_limit_ratio = (!std::isfinite(d->dt_limit_active) || d->dt_limit_active <= tiny) ? 0.0 : c.dt / d->dt_limit_active;
+  if (!std::isfinite(d->mass_drift) || !std::isfinite(d->divergence_l2) || !std::isfinite(d->max_velocity) ||
+      !std::isfinite(d->max_abs_mu))
+    return fail(h, DN_ERR_NONFINITE, "non-finite diagnostic detected");
+  return DN_OK;
+}
+
+dn_status dn_synchronize(dn_handle *h) {
+  if (!h) return DN_ERR_INVALID_ARGUMENT;
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+void *dn_stream(dn_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+dn_status dn_last_phase_times(dn_handle *h, double *out) {
+  if (!h || !out) return DN_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 8; ++k) out[k] = h->phase_ms[k];
+  return DN_OK;
+}
+
+long long dn_kernel_launches(const dn_handle *h) { return h ? h->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,503 @@
+// dn_fields.cuh -- stencil / pointwise kernels of the CHNS step on ghosted Field2D-layout arrays.
+//
+// Each kernel restates one loop of the reference (file:line cited) with the reference's operand order;
+// with --fmad=false these kernels reproduce the reference's doubles bit for bit.  One thread per cell;
+// the whole step is HBM/L2 bound and these kernels are a few percent of it (the Krylov solves dominate).
+#pragma once
+
+#include "dn_common.cuh"
+
+namespace dn {
+
+#define DN_FOR_INTERIOR(F)                                                          \
+  const long long _n = (long long)(F).nx * (F).ny;                                  \
+  const long long _t = (long long)blockIdx.x * blockDim.x + threadIdx.x;            \
+  if (_t >= _n) return;                                                             \
+  const int i = (int)(_t / (F).ny), j = (int)(_t % (F).ny);
+
+// ------------------------------------------------------------------------------------------------------
+// Boundary conditions (operators.cpp:130-289).  The reference fills x-ghost layers for interior j and then
+// y-ghost layers for every i; here every ghost cell is computed from interior values in one pass, which
+// gives the same value everywhere except the corner cells that are >= 2 cells outside in both directions
+// (the reference copies a not-yet-refreshed x-ghost there).  No stencil of the step reads those corners.
+// ------------------------------------------------------------------------------------------------------
+enum BCKind { kBCScalar = 0, kBCPressure = 1, kBCU = 2, kBCV = 3 };
+
+// u boundary faces, operators.cpp:189-200
+__global__ void k_bc_faces_u(Fv f, Grid G, BCSide left, BCSide right) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= f.ny) return;
+  if (G.px) {
+    f.at(f.nx - 1, j) = f.at(0, j);
+  } else {
+    f.at(0, j) = (left.type == DN_BC_DIRICHLET) ? left.value : f.at(1, j) + left.value * G.dx;
+    f.at(f.nx - 1, j) = (right.type == DN_BC_DIRICHLET) ? right.value : f.at(f.nx - 2, j) + right.value * G.dx;
+  }
+}
+// v boundary faces, operators.cpp:245-256
+__global__ void k_bc_faces_v(Fv f, Grid G, BCSide bottom, BCSide top) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= f.nx) return;
+  if (G.py) {
+    f.at(i, f.ny - 1) = f.at(i, 0);
+  } else {
+    f.at(i, 0) = (bottom.type == DN_BC_DIRICHLET) ? bottom.value : f.at(i, 1) + bottom.value * G.dy;
+    f.at(i, f.ny - 1) = (top.type == DN_BC_DIRICHLET) ? top.value : f.at(i, f.ny - 2) + top.value * G.dy;
+  }
+}
+
+// x-direction ghost value at (i, j), j interior, i outside [0, nx').
+__device__ __forceinline__ double bc_xval(const Fv &f, const Grid &G, int kind, const BCSide &L, const BCSide &R,
+                                          int i, int j) {
+  const int nx = f.nx;
+  if (i >= 0 && i < nx) return f.at(i, j);
+  const bool left = i < 0;
+  const int g = left ? -i : i - (nx - 1);
+  if (G.px) {
+    if (kind == kBCU) return left ? f.at(nx - g - 1, j) : f.at(g, j);
+    return left ? f.at(nx - g, j) : f.at(g - 1, j);
+  }
+  if (kind == kBCScalar) return left ? f.at(0, j) : f.at(nx - 1, j);
+  const BCSide &b = left ? L : R;
+  if (kind == kBCU) {
+    const double off = 2.0 * (double)g * b.value * G.dx;
+    const double in = left ? f.at(g, j) : f.at(nx - 1 - g, j);
+    return (b.type == DN_BC_DIRICHLET) ? 2.0 * b.value - in : in + off;
+  }
+  // pressure and v: cell-centred in x
+  const double off = 2.0 * ((double)g - 0.5) * b.value * G.dx;
+  const double in = left ? f.at(g - 1, j) : f.at(nx - g, j);
+  return (b.type == DN_BC_DIRICHLET) ? 2.0 * b.value - in : in + off;
+}
+
+__global__ void k_bc_ghosts(Fv f, Grid G, int kind, BCSide L, BCSide R, BCSide B, BCSide T) {
+  const int gw = f.g, nx = f.nx, ny = f.ny;
+  const long long nxg = 2LL * gw * ny;               // x-ghost strips, interior j
+  const long long nyg = 2LL * gw * (nx + 2 * gw);    // y-ghost strips, all i
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nxg) {
+    const int j = (int)(t % ny);
+    const int k = (int)(t / ny);  // 0..2g-1
+    const int i = (k < gw) ? -(k + 1) : nx - 1 + (k - gw + 1);
+    f.at(i, j) = bc_xval(f, G, kind, L, R, i, j);
+    return;
+  }
+  t -= nxg;
+  if (t >= nyg) return;
+  const int i = (int)(t % (nx + 2 * gw)) - gw;
+  const int k = (int)(t / (nx + 2 * gw));
+  const bool bottom = k < gw;
+  const int g = bottom ? k + 1 : k - gw + 1;
+  const int j = bottom ? -g : ny - 1 + g;
+  double val;
+  if (G.py) {
+    if (kind == kBCV)
+      val = bottom ? bc_xval(f, G, kind, L, R, i, ny - g - 1) : bc_xval(f, G, kind, L, R, i, g);
+    else
+      val = bottom ? bc_xval(f, G, kind, L, R, i, ny - g) : bc_xval(f, G, kind, L, R, i, g - 1);
+  } else if (kind == kBCScalar) {
+    val = bottom ? bc_xval(f, G, kind, L, R, i, 0) : bc_xval(f, G, kind, L, R, i, ny - 1);
+  } else {
+    const BCSide &b = bottom ? B : T;
+    if (kind == kBCV) {
+      const double off = 2.0 * (double)g * b.value * G.dy;
+      const double in = bottom ? bc_xval(f, G, kind, L, R, i, g) : bc_xval(f, G, kind, L, R, i, ny - 1 - g);
+      val = (b.type == DN_BC_DIRICHLET) ? 2.0 * b.value - in : in + off;
+    } else {
+      const double off = 2.0 * ((double)g - 0.5) * b.value * G.dy;
+      const double in = bottom ? bc_xval(f, G, kind, L, R, i, g - 1) : bc_xval(f, G, kind, L, R, i, ny - g);
+      val = (b.type == DN_BC_DIRICHLET) ? 2.0 * b.value - in : in + off;
+    }
+  }
+  f.at(i, j) = val;
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Face / corner interpolation (operators.cpp:328-398)
+// ------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double xface(const Fv &f, const Grid &G, int i, int j) {
+  if (i <= 0) return G.px ? 0.5 * (f.at(G.nx - 1, j) + f.at(0, j)) : f.at(0, j);
+  if (i >= G.nx) return G.px ? 0.5 * (f.at(G.nx - 1, j) + f.at(0, j)) : f.at(G.nx - 1, j);
+  return 0.5 * (f.at(i - 1, j) + f.at(i, j));
+}
+__device__ __forceinline__ double yface(const Fv &f, const Grid &G, int i, int j) {
+  if (j <= 0) return G.py ? 0.5 * (f.at(i, G.ny - 1) + f.at(i, 0)) : f.at(i, 0);
+  if (j >= G.ny) return G.py ? 0.5 * (f.at(i, G.ny - 1) + f.at(i, 0)) : f.at(i, G.ny - 1);
+  return 0.5 * (f.at(i, j - 1) + f.at(i, j));
+}
+__device__ __forceinline__ double corner(const Fv &f, int i, int j) {
+  return 0.25 * (f.at(i, j) + f.at(i - 1, j) + f.at(i, j - 1) + f.at(i - 1, j - 1));
+}
+__device__ __forceinline__ double lapc(const Fv &f, const Grid &G, int i, int j) {
+  return (f.at(i + 1, j) - 2.0 * f.at(i, j) + f.at(i - 1, j)) / (G.dx * G.dx) +
+         (f.at(i, j + 1) - 2.0 * f.at(i, j) + f.at(i, j - 1)) / (G.dy * G.dy);
+}
+__device__ __forceinline__ double gfx(const Fv &f, const Grid &G, int i, int j) {
+  return (f.at(i, j) - f.at(i - 1, j)) / G.dx;
+}
+__device__ __forceinline__ double gfy(const Fv &f, const Grid &G, int i, int j) {
+  return (f.at(i, j) - f.at(i, j - 1)) / G.dy;
+}
+__device__ __forceinline__ double div_cell(const Fv &u, const Fv &v, const Grid &G, int i, int j) {
+  return (u.at(i + 1, j) - u.at(i, j)) / G.dx + (v.at(i, j + 1) - v.at(i, j)) / G.dy;
+}
+__device__ __forceinline__ double sq(double v) { return v * v; }
+
+// ------------------------------------------------------------------------------------------------------
+// Pointwise / stencil kernels
+// ------------------------------------------------------------------------------------------------------
+__global__ void k_copy(double *dst, const double *src, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = src[t];
+}
+__global__ void k_fill(double *dst, double v, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = v;
+}
+__global__ void k_copy_interior(Fv dst, Fv src) {
+  DN_FOR_INTERIOR(dst);
+  dst.at(i, j) = src.at(i, j);
+}
+__global__ void k_add_scalar_interior(Fv f, const double *sub) {
+  DN_FOR_INTERIOR(f);
+  f.at(i, j) -= *sub;
+}
+
+// update_materials_from_phase, phase_field.cpp:57-66
+__global__ void k_materials(Fv c, Fv rho, Fv eta, double dr, double vr) {
+  DN_FOR_INTERIOR(c);
+  const double cc = c.at(i, j);
+  rho.at(i, j) = cc + (1.0 - cc) * dr;
+  eta.at(i, j) = cc + (1.0 - cc) * vr;
+}
+// update_midpoint_materials, phase_field.cpp:70-79
+__global__ void k_midpoint(Fv rp, Fv r, Fv ep, Fv e, Fv rm, Fv em) {
+  DN_FOR_INTERIOR(rm);
+  rm.at(i, j) = 0.5 * (rp.at(i, j) + r.at(i, j));
+  em.at(i, j) = 0.5 * (ep.at(i, j) + e.at(i, j));
+}
+// update_chemical_potential, phase_field.cpp:97-109 (input already carries its scalar BC ghosts)
+__global__ void k_chem(Fv c, Fv mu, Grid G, double cn) {
+  DN_FOR_INTERIOR(mu);
+  const double alpha = 6.0 * 1.4142135623730950488;  // 6*sqrt(2), correctly rounded like std::sqrt
+  const double cc = c.at(i, j);
+  const double dw = 0.5 * cc * (1.0 - cc) * (1.0 - 2.0 * cc);
+  mu.at(i, j) = alpha * (dw / cn - cn * lapc(c, G, i, j));
+}
+// mobility and laplacian, phase_field.cpp:367-372
+__global__ void k_mob_lap(Fv c, Fv mob, Fv lap, Grid G) {
+  DN_FOR_INTERIOR(mob);
+  const double cc = c.at(i, j);
+  mob.at(i, j) = fmax(0.0, cc * (1.0 - cc));
+  lap.at(i, j) = lapc(c, G, i, j);
+}
+__global__ void k_lap(Fv in, Fv out, Grid G) {
+  DN_FOR_INTERIOR(out);
+  out.at(i, j) = lapc(in, G, i, j);
+}
+
+// weno5_left, phase_field.cpp:144-157
+__device__ __forceinline__ double weno5_left(double v1, double v2, double v3, double v4, double v5) {
+  const double eps = 1.0e-6;
+  const double q0 = (2.0 * v1 - 7.0 * v2 + 11.0 * v3) / 6.0;
+  const double q1 = (-v2 + 5.0 * v3 + 2.0 * v4) / 6.0;
+  const double q2 = (2.0 * v3 + 5.0 * v4 - v5) / 6.0;
+  const double b0 = 13.0 / 12.0 * sq(v1 - 2.0 * v2 + v3) + 0.25 * sq(v1 - 4.0 * v2 + 3.0 * v3);
+  const double b1 = 13.0 / 12.0 * sq(v2 - 2.0 * v3 + v4) + 0.25 * sq(v2 - v4);
+  const double b2 = 13.0 / 12.0 * sq(v3 - 2.0 * v4 + v5) + 0.25 * sq(3.0 * v3 - 4.0 * v4 + v5);
+  const double a0 = 0.1 / sq(eps + b0);
+  const double a1 = 0.6 / sq(eps + b1);
+  const double a2 = 0.3 / sq(eps + b2);
+  const double sum = a0 + a1 + a2;
+  return (a0 * q0 + a1 * q1 + a2 * q2) / sum;
+}
+
+// advective face fluxes with WENO5 face values, phase_field.cpp:163-177, 288-300
+__global__ void k_adv_flux_x(Fv c, Fv ua, Fv fx) {
+  DN_FOR_INTERIOR(fx);
+  const double uu = ua.at(i, j);
+  const double face = (uu >= 0.0) ? weno5_left(c.at(i - 3, j), c.at(i - 2, j), c.at(i - 1, j), c.at(i, j), c.at(i + 1, j))
+                                  : weno5_left(c.at(i + 2, j), c.at(i + 1, j), c.at(i, j), c.at(i - 1, j), c.at(i - 2, j));
+  fx.at(i, j) = uu * face;
+}
+__global__ void k_adv_flux_y(Fv c, Fv va, Fv fy) {
+  DN_FOR_INTERIOR(fy);
+  const double vv = va.at(i, j);
+  const double face = (vv >= 0.0) ? weno5_left(c.at(i, j - 3), c.at(i, j - 2), c.at(i, j - 1), c.at(i, j), c.at(i, j + 1))
+                                  : weno5_left(c.at(i, j + 2), c.at(i, j + 1), c.at(i, j), c.at(i, j - 1), c.at(i, j - 2));
+  fy.at(i, j) = vv * face;
+}
+// diffusive face fluxes, phase_field.cpp:315-341
+__global__ void k_diff_flux_x(Fv mu, Fv mob, Fv fx, Grid G) {
+  DN_FOR_INTERIOR(fx);
+  const double m = xface(mob, G, i, j);
+  fx.at(i, j) = m * gfx(mu, G, i, j);
+}
+__global__ void k_diff_flux_y(Fv mu, Fv mob, Fv fy, Grid G) {
+  DN_FOR_INTERIOR(fy);
+  const double m = yface(mob, G, i, j);
+  fy.at(i, j) = m * gfy(mu, G, i, j);
+}
+// adv_rhs (phase_field.cpp:304-309) and diffusion divergence (:345-350)
+__global__ void k_flux_div(Fv fx, Fv fy, Fv out, Grid G, int negate) {
+  DN_FOR_INTERIOR(out);
+  if (negate)
+    out.at(i, j) = -(fx.at(i + 1, j) - fx.at(i, j)) / G.dx - (fy.at(i, j + 1) - fy.at(i, j)) / G.dy;
+  else
+    out.at(i, j) = (fx.at(i + 1, j) - fx.at(i, j)) / G.dx + (fy.at(i, j + 1) - fy.at(i, j)) / G.dy;
+}
+// explicit operator, phase_field.cpp:386-394
+__global__ void k_explicit(Fv ddiv, Fv lap, Fv bih, Fv arhs, Fv E, double a1, double a2, double pe) {
+  DN_FOR_INTERIOR(E);
+  E.at(i, j) = ddiv.at(i, j) / pe - (a1 * lap.at(i, j) - a2 * bih.at(i, j)) / pe + arhs.at(i, j);
+}
+// BDF1/BDF2 + AB2 right-hand side, phase_field.cpp:679-690; written straight into the compact Krylov rhs
+__global__ void k_ch_rhs(Fv cp, Fv cp2, Fv E, Fv Ep, double *rhs, double *x0, Fv c, int step, double dt) {
+  DN_FOR_INTERIOR(E);
+  double v;
+  if (step == 0)
+    v = cp.at(i, j) / dt + E.at(i, j);
+  else
+    v = (4.0 * cp.at(i, j) - cp2.at(i, j)) / (2.0 * dt) + 2.0 * E.at(i, j) - Ep.at(i, j);
+  const long long r = (long long)i * E.ny + j;
+  rhs[r] = v;
+  x0[r] = c.at(i, j);
+}
+__global__ void k_scatter_compact(const double *x, Fv f) {
+  DN_FOR_INTERIOR(f);
+  f.at(i, j) = x[(long long)i * f.ny + j];
+}
+__global__ void k_gather_compact(Fv f, double *x) {
+  DN_FOR_INTERIOR(f);
+  x[(long long)i * f.ny + j] = f.at(i, j);
+}
+
+// c_mid, phase_field.cpp:185-191
+__global__ void k_cmid(Fv co, Fv cn_, Fv cm) {
+  DN_FOR_INTERIOR(cm);
+  cm.at(i, j) = 0.5 * (co.at(i, j) + cn_.at(i, j));
+}
+// face surface-tension forces, phase_field.cpp:206-226
+__global__ void k_sf_u(Fv mm, Fv cm, Fv fxu, Grid G, double scale) {
+  DN_FOR_INTERIOR(fxu);
+  const int nx = G.nx;
+  const double mf = (i <= 0) ? 0.5 * (mm.at(nx - 1, j) + mm.at(0, j))
+                             : (i >= nx ? 0.5 * (mm.at(nx - 1, j) + mm.at(0, j)) : 0.5 * (mm.at(i - 1, j) + mm.at(i, j)));
+  fxu.at(i, j) = scale * mf * gfx(cm, G, i, j);
+}
+__global__ void k_sf_v(Fv mm, Fv cm, Fv fyv, Grid G, double scale) {
+  DN_FOR_INTERIOR(fyv);
+  const int ny = G.ny;
+  const double mf = (j <= 0) ? 0.5 * (mm.at(i, ny - 1) + mm.at(i, 0))
+                             : (j >= ny ? 0.5 * (mm.at(i, ny - 1) + mm.at(i, 0)) : 0.5 * (mm.at(i, j - 1) + mm.at(i, j)));
+  fyv.at(i, j) = scale * mf * gfy(cm, G, i, j);
+}
+// cell surface-tension forces, phase_field.cpp:197-202
+__global__ void k_sf_cell(Fv mm, Fv cm, Fv fxc, Fv fyc, Grid G, double scale) {
+  DN_FOR_INTERIOR(fxc);
+  fxc.at(i, j) = scale * mm.at(i, j) * ((cm.at(i + 1, j) - cm.at(i - 1, j)) / (2.0 * G.dx));
+  fyc.at(i, j) = scale * mm.at(i, j) * ((cm.at(i, j + 1) - cm.at(i, j - 1)) / (2.0 * G.dy));
+}
+// smoothing pass, phase_field.cpp:234-249
+__global__ void k_smooth(Fv f, Fv out, double cw, double nw) {
+  DN_FOR_INTERIOR(out);
+  out.at(i, j) = cw * f.at(i, j) + nw * (f.at(i - 1, j) + f.at(i + 1, j) + f.at(i, j - 1) + f.at(i, j + 1));
+}
+
+// centred momentum convection, momentum.cpp:55-85
+__global__ void k_mom_flux_u(Fv u, Fv v, Fv hu, Grid G) {
+  DN_FOR_INTERIOR(hu);
+  const double uf = u.at(i, j);
+  const double dudx = (u.at(i + 1, j) - u.at(i - 1, j)) / (2.0 * G.dx);
+  const double dudy = (u.at(i, j + 1) - u.at(i, j - 1)) / (2.0 * G.dy);
+  const double vf = 0.25 * (v.at(i - 1, j) + v.at(i, j) + v.at(i - 1, j + 1) + v.at(i, j + 1));
+  hu.at(i, j) = uf * dudx + vf * dudy;
+}
+__global__ void k_mom_flux_v(Fv u, Fv v, Fv hv, Grid G) {
+  DN_FOR_INTERIOR(hv);
+  const double vf = v.at(i, j);
+  const double dvdx = (v.at(i + 1, j) - v.at(i - 1, j)) / (2.0 * G.dx);
+  const double dvdy = (v.at(i, j + 1) - v.at(i, j - 1)) / (2.0 * G.dy);
+  const double uf = 0.25 * (u.at(i, j - 1) + u.at(i, j) + u.at(i + 1, j - 1) + u.at(i + 1, j));
+  hv.at(i, j) = uf * dvdx + vf * dvdy;
+}
+
+// viscous stress divergence, momentum.cpp:91-155
+__device__ __forceinline__ double visc_u(const Fv &u, const Fv &v, const Fv &eta, const Grid &G, int i, int j) {
+  const double eta_e = xface(eta, G, i + 1, j), eta_w = xface(eta, G, i, j);
+  const double dudx_e = (u.at(i + 1, j) - u.at(i, j)) / G.dx;
+  const double dudx_w = (u.at(i, j) - u.at(i - 1, j)) / G.dx;
+  const double normal = (2.0 * eta_e * dudx_e - 2.0 * eta_w * dudx_w) / G.dx;
+  const double eta_n = corner(eta, i, j + 1), eta_s = corner(eta, i, j);
+  const double dudy_n = (u.at(i, j + 1) - u.at(i, j)) / G.dy;
+  const double dudy_s = (u.at(i, j) - u.at(i, j - 1)) / G.dy;
+  const double shear_self = (eta_n * dudy_n - eta_s * dudy_s) / G.dy;
+  const double self = normal + shear_self;
+  const double dvdx_n = (v.at(i, j + 1) - v.at(i - 1, j + 1)) / G.dx;
+  const double dvdx_s = (v.at(i, j) - v.at(i - 1, j)) / G.dx;
+  const double cross = (eta_n * dvdx_n - eta_s * dvdx_s) / G.dy;
+  return self + cross;
+}
+__device__ __forceinline__ double visc_v(const Fv &u, const Fv &v, const Fv &eta, const Grid &G, int i, int j) {
+  const double eta_e = corner(eta, i + 1, j), eta_w = corner(eta, i, j);
+  const double dvdx_e = (v.at(i + 1, j) - v.at(i, j)) / G.dx;
+  const double dvdx_w = (v.at(i, j) - v.at(i - 1, j)) / G.dx;
+  const double shear_self = (eta_e * dvdx_e - eta_w * dvdx_w) / G.dx;
+  const double eta_n = yface(eta, G, i, j + 1), eta_s = yface(eta, G, i, j);
+  const double dvdy_n = (v.at(i, j + 1) - v.at(i, j)) / G.dy;
+  const double dvdy_s = (v.at(i, j) - v.at(i, j - 1)) / G.dy;
+  const double normal = (2.0 * eta_n * dvdy_n - 2.0 * eta_s * dvdy_s) / G.dy;
+  const double self = shear_self + normal;
+  const double dudy_e = (u.at(i + 1, j) - u.at(i + 1, j - 1)) / G.dy;
+  const double dudy_w = (u.at(i, j) - u.at(i, j - 1)) / G.dy;
+  const double cross = (eta_e * dudy_e - eta_w * dudy_w) / G.dx;
+  return self + cross;
+}
+
+// split extrapolation p~ = 2p^n - p^{n-1} (p^n at step 0), operators.cpp:413-422
+__global__ void k_p_ext(Fv p, Fv pp, Fv pe, int first) {
+  DN_FOR_INTERIOR(pe);
+  pe.at(i, j) = first ? p.at(i, j) : (2.0 * p.at(i, j) - pp.at(i, j));
+}
+
+// velocity correction, operators.cpp:490-516
+__global__ void k_correct_u(Fv u, Fv us, Fv rm, Fv pc, Fv pe, Grid G, int split, double rho_ref, double dt) {
+  DN_FOR_INTERIOR(u);
+  const double se = split ? (1.0 / xface(rm, G, i, j) - 1.0 / rho_ref) * gfx(pe, G, i, j) : 0.0;
+  const double si = split ? gfx(pc, G, i, j) / rho_ref : gfx(pc, G, i, j) / xface(rm, G, i, j);
+  u.at(i, j) = us.at(i, j) - dt * (si + se);
+}
+__global__ void k_correct_v(Fv v, Fv vs, Fv rm, Fv pc, Fv pe, Grid G, int split, double rho_ref, double dt) {
+  DN_FOR_INTERIOR(v);
+  const double se = split ? (1.0 / yface(rm, G, i, j) - 1.0 / rho_ref) * gfy(pe, G, i, j) : 0.0;
+  const double si = split ? gfy(pc, G, i, j) / rho_ref : gfy(pc, G, i, j) / yface(rm, G, i, j);
+  v.at(i, j) = vs.at(i, j) - dt * (si + se);
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Reductions used outside the Krylov kernels (two-stage, deterministic)
+// ------------------------------------------------------------------------------------------------------
+enum RedOp { kRedSum = 0, kRedMax = 1, kRedMin = 2 };
+
+// Stage 1: per-block partials of up to 4 interior reductions of a cell field (value index selects the
+// quantity).  Used for means and the diagnostics.
+__device__ __forceinline__ double red_identity(int op) { return op == kRedSum ? 0.0 : (op == kRedMax ? -INFINITY : INFINITY); }
+__device__ __forceinline__ double red_combine(int op, double a, double b) {
+  return op == kRedSum ? a + b : (op == kRedMax ? fmax(a, b) : fmin(a, b));
+}
+
+__global__ void k_reduce_final(const double *partials, int nparts, int nvals, const int *ops, double *out) {
+  // one warp per value
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w >= nvals) return;
+  const int op = ops[w];
+  double s = red_identity(op);
+  for (int b = lane; b < nparts; b += 32) s = red_combine(op, s, partials[(size_t)b * nvals + w]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s = red_combine(op, s, __shfl_xor_sync(0xffffffffu, s, o));
+  if (lane == 0) out[w] = s;
+}
+
+// Interior sum of a field (for subtract_mean, operators.cpp:447-460, and compute_mass, diagnostics.cpp:24-32).
+__global__ void k_field_sum(Fv f, double scale, double *partials) {
+  __shared__ double sh[8 * 32];
+  const long long n = (long long)f.nx * f.ny;
+  double v[1] = {0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / f.ny), j = (int)(t % f.ny);
+    v[0] += f.at(i, j) * scale;
+  }
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+__global__ void k_vec_sum(const double *x, long long n, double *partials) {
+  __shared__ double sh[8 * 32];
+  double v[1] = {0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    v[0] += x[t];
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+__global__ void k_finish_mean(const double *partials, int nparts, double count, double *out) {
+  const int lane = threadIdx.x;
+  double s = 0.0;
+  for (int b = lane; b < nparts; b += 32) s += partials[b];
+  s = warp_sum(s);
+  if (lane == 0) out[0] = s / count;
+}
+__global__ void k_vec_sub_scalar(double *x, long long n, const double *sub) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) x[t] -= *sub;
+}
+
+// periodic_boundary_speed_stat, operators.cpp:463-478 (single CTA)
+__global__ void k_boundary_speed(Fv u, Fv v, Grid G, double *out) {
+  double m = 0.0;
+  if (G.px)
+    for (int j = threadIdx.x; j < u.ny; j += blockDim.x) m = fmax(m, fmax(fabs(u.at(0, j)), fabs(u.at(G.nx, j))));
+  if (G.py)
+    for (int i = threadIdx.x; i < v.nx; i += blockDim.x) m = fmax(m, fmax(fabs(v.at(i, 0)), fabs(v.at(i, G.ny))));
+  __shared__ double sh[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, sh[w]);
+    *out = r;
+  }
+}
+
+// Diagnostics, diagnostics.cpp:24-167: per-block partials of
+//   0 mass  1 div_sq  2 div_max  3 mu_max  4 vel_max  5 ke  6 rho_min  7 rho_max  8 eta_min  9 eta_max
+//   10 free energy  11 max advective rate  12 mobility max  13 |W''| max
+constexpr int kNDiag = 14;
+__global__ void k_diag_partials(Fv c, Fv u, Fv v, Fv mu, Fv rho, Fv eta, Grid G, double cn, double *partials) {
+  double a[kNDiag];
+  const int ops[kNDiag] = {0, 0, 1, 1, 1, 0, 2, 1, 2, 1, 0, 1, 1, 1};
+#pragma unroll
+  for (int k = 0; k < kNDiag; ++k) a[k] = red_identity(ops[k]);
+  const long long n = (long long)G.nx * G.ny;
+  const double alpha = 6.0 * 1.4142135623730950488;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / G.ny), j = (int)(t % G.ny);
+    const double cc = c.at(i, j);
+    a[0] += cc * G.dx * G.dy;
+    const double dv = div_cell(u, v, G, i, j);
+    const double uc = 0.5 * (u.at(i, j) + u.at(i + 1, j)), vc = 0.5 * (v.at(i, j) + v.at(i, j + 1));
+    a[1] += dv * dv;
+    a[2] = fmax(a[2], fabs(dv));
+    a[3] = fmax(a[3], fabs(mu.at(i, j)));
+    a[4] = fmax(a[4], sqrt(uc * uc + vc * vc));
+    a[5] += 0.5 * rho.at(i, j) * (uc * uc + vc * vc) * G.dx * G.dy;
+    a[6] = fmin(a[6], rho.at(i, j));
+    a[7] = fmax(a[7], rho.at(i, j));
+    a[8] = fmin(a[8], eta.at(i, j));
+    a[9] = fmax(a[9], eta.at(i, j));
+    const double bulk = 0.25 * cc * cc * sq(1.0 - cc) / cn;
+    const double gx = (c.at(i + 1, j) - c.at(i - 1, j)) / (2.0 * G.dx);
+    const double gy = (c.at(i, j + 1) - c.at(i, j - 1)) / (2.0 * G.dy);
+    a[10] += alpha * (bulk + 0.5 * cn * (sq(gx) + sq(gy))) * G.dx * G.dy;
+    a[11] = fmax(a[11], fabs(uc) / fmax(G.dx, 1.0e-30) + fabs(vc) / fmax(G.dy, 1.0e-30));
+    a[12] = fmax(a[12], fmax(0.0, cc * (1.0 - cc)));
+    a[13] = fmax(a[13], fabs(0.5 - 3.0 * cc + 3.0 * cc * cc));
+  }
+  __shared__ double sh[kNDiag][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kNDiag; ++k) {
+    double s = a[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = red_combine(ops[k], s, __shfl_xor_sync(0xffffffffu, s, o));
+    if (lane == 0) sh[k][w] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNDiag) {
+    const int k = threadIdx.x;
+    double s = red_identity(ops[k]);
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) s = red_combine(ops[k], s, sh[k][ww]);
+    partials[(size_t)blockIdx.x * kNDiag + k] = s;
+  }
+}
+
+}  // namespace dn

@@ -1,0 +1,664 @@
+// dn_krylov.cuh -- sparse operators, incomplete factorizations and the persistent PCG / BiCGSTAB kernels.
+//
+// Matrices are stored by stencil slot: a[s*n + r] is the coefficient of row r (= i*ny + j) at the slot's
+// offset, with periodic wrap; 0 means "absent" (the reference drops |a| < 1e-18 entries,
+// ch_sparse_krylov.hpp:116).  The 5-point slots are W,S,C,N,E; the 13-point slots are the offsets of
+// L^2 in lexicographic (di, dj) order, so that for interior rows slot order equals the reference's CSR
+// column order and slot s mirrors to slot S-1-s.
+//
+// The PCG kernel is persistent: one cooperative launch runs the whole solve (all iterations) with bounded
+// grid barriers between phases.  The ICC(0)/ILDLT(0) triangular solves of the 5-point pressure operator
+// run as a register/shuffle-pipelined anti-diagonal wavefront: lane t of a sweep warp owns x-line
+// i = 32k + t and marches along j; the value of line i-1 arrives from lane t-1 by warp shuffle one step
+// earlier, and across warps through the y array plus a monotonic progress flag.  This applies exactly the
+// reference's incomplete factors (same preconditioner, same iteration counts up to round-off).
+#pragma once
+
+#include "dn_common.cuh"
+
+namespace dn {
+
+// ---------------------------------------------------------------------------------------------------
+// Stencils
+// ---------------------------------------------------------------------------------------------------
+template <int S>
+struct Stencil;
+template <>
+struct Stencil<5> {
+  static constexpr int n = 5;
+  static constexpr int center = 2;
+  __host__ __device__ static constexpr int di(int s) { return s == 0 ? -1 : (s == 4 ? 1 : 0); }
+  __host__ __device__ static constexpr int dj(int s) { return s == 1 ? -1 : (s == 3 ? 1 : 0); }
+};
+template <>
+struct Stencil<13> {
+  static constexpr int n = 13;
+  static constexpr int center = 6;
+  __host__ __device__ static constexpr int di(int s) {
+    return s == 0 ? -2 : (s <= 3 ? -1 : (s <= 8 ? 0 : (s <= 11 ? 1 : 2)));
+  }
+  __host__ __device__ static constexpr int dj(int s) {
+    return s == 0 ? 0 : (s <= 3 ? s - 2 : (s <= 8 ? s - 6 : (s <= 11 ? s - 10 : 0)));
+  }
+};
+
+// Column of slot s in row (i, j), or -1 when the neighbour lies outside a non-periodic boundary.
+template <int S>
+__device__ __forceinline__ long long slot_col(int i, int j, int s, int nx, int ny, int px, int py) {
+  int ii = i + Stencil<S>::di(s), jj = j + Stencil<S>::dj(s);
+  if (ii < 0 || ii >= nx) {
+    if (!px) return -1;
+    ii = (ii + nx) % nx;
+  }
+  if (jj < 0 || jj >= ny) {
+    if (!py) return -1;
+    jj = (jj + ny) % ny;
+  }
+  return (long long)ii * ny + jj;
+}
+
+struct SpOp {
+  const double *a;  // [S][n]
+  int n, nx, ny, px, py;
+};
+
+template <int S>
+__device__ __forceinline__ double spmv_row(const SpOp &A, const double *x, int i, int j) {
+  const long long r = (long long)i * A.ny + j;
+  double sum = 0.0;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const double a = A.a[(size_t)s * A.n + r];
+    if (a != 0.0) {
+      const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+      sum += a * x[c];
+    }
+  }
+  return sum;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Incomplete factorizations (try_build_incomplete_ldlt / try_build_incomplete_cholesky,
+// ch_sparse_krylov.hpp:252-419).  Level-scheduled, one CTA: rows of one level are independent.
+//   5-point: level(i, j) = i + j (valid for every periodicity).
+//   13-point: level(i, j) = 2i + j when y is not periodic; with periodic y the 13-point dependency graph
+//   is a single chain (row (i,0) depends on (i-1,ny-1)), so rows are processed in order.
+// ---------------------------------------------------------------------------------------------------
+struct Factor {
+  double *l;     // [S][n]: L at lower slots, 0 elsewhere
+  double *d;     // [n]: d (ICC) or D (LDLT)
+  double *dinv;  // [n]: 1 / max(d, floor)
+  double floor;
+};
+
+template <int S>
+__device__ __forceinline__ int num_levels(int nx, int ny, int py) {
+  if (S == 5) return nx + ny - 1;
+  return py ? nx * ny : 2 * (nx - 1) + ny;
+}
+template <int S>
+__device__ __forceinline__ void level_range(int lev, int nx, int ny, int py, int &i0, int &i1) {
+  if (S == 5) {
+    i0 = max(0, lev - (ny - 1));
+    i1 = min(nx - 1, lev);
+  } else if (py) {
+    i0 = i1 = -1;
+  } else {
+    i0 = max(0, (lev - (ny - 1) + 1) / 2);
+    i1 = min(nx - 1, lev / 2);
+  }
+}
+template <int S>
+__device__ __forceinline__ void level_row(int lev, int i, int ny, int py, int &ri, int &rj) {
+  if (S == 13 && py) {
+    ri = lev / ny;
+    rj = lev % ny;
+  } else {
+    ri = i;
+    rj = (S == 5) ? lev - i : lev - 2 * i;
+  }
+}
+
+// Sorted lower slots of row (i, j): fills slots[] (ascending column), returns the count.
+template <int S>
+__device__ __forceinline__ int lower_slots(const SpOp &A, int i, int j, int *slots, long long *cols) {
+  const long long r = (long long)i * A.ny + j;
+  int cnt = 0;
+  for (int s = 0; s < S; ++s) {
+    if (fabs(A.a[(size_t)s * A.n + r]) < 1.0e-18) continue;
+    const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+    if (c < 0 || c >= r) continue;
+    int p = cnt++;
+    while (p > 0 && cols[p - 1] > c) {
+      cols[p] = cols[p - 1];
+      slots[p] = slots[p - 1];
+      --p;
+    }
+    cols[p] = c;
+    slots[p] = s;
+  }
+  return cnt;
+}
+
+// L value of row c at column k (0 when k is not a lower entry of row c).
+template <int S>
+__device__ __forceinline__ double find_lower(const SpOp &A, const Factor &F, long long c, long long k) {
+  const int ci = (int)(c / A.ny), cj = (int)(c % A.ny);
+  for (int s = 0; s < S; ++s) {
+    if (slot_col<S>(ci, cj, s, A.nx, A.ny, A.px, A.py) == k) {
+      if (fabs(A.a[(size_t)s * A.n + c]) < 1.0e-18 || k >= c) return 0.0;
+      return F.l[(size_t)s * A.n + c];
+    }
+  }
+  return 0.0;
+}
+
+// kind: 1 = ILDLT, 2 = ICC.  status: set to kDevFactorFailed on a pivot below the floor.
+template <int S>
+__global__ void k_factor(SpOp A, Factor F, int kind, int *status) {
+  __shared__ double shmax[32];
+  __shared__ double sh_floor;
+  // max |diag| (ch_sparse_krylov.hpp:258-263 / 343-348)
+  double m = 0.0;
+  for (long long r = threadIdx.x; r < A.n; r += blockDim.x) {
+    m = fmax(m, fabs(A.a[(size_t)Stencil<S>::center * A.n + r]));
+    for (int s = 0; s < S; ++s) F.l[(size_t)s * A.n + r] = 0.0;
+  }
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) shmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mm = fmax(mm, shmax[w]);
+    sh_floor = (kind == 2) ? sqrt(fmax(1.0, mm) * 1.0e-12) : fmax(1.0, mm) * 1.0e-12;
+  }
+  __syncthreads();
+  const double floor = sh_floor;
+  const double floor_sq = floor * floor;
+  const int nlev = num_levels<S>(A.nx, A.ny, A.py);
+  const bool seq = (S == 13 && A.py);
+  for (int lev = 0; lev < nlev; ++lev) {
+    int i0, i1;
+    level_range<S>(lev, A.nx, A.ny, A.py, i0, i1);
+    if (seq) {
+      i0 = 0;
+      i1 = 0;
+    }
+    for (int ii = i0 + (int)threadIdx.x; ii <= i1; ii += blockDim.x) {
+      int i, j;
+      level_row<S>(lev, ii, A.ny, A.py, i, j);
+      const long long r = (long long)i * A.ny + j;
+      int slots[S];
+      long long cols[S];
+      const int cnt = lower_slots<S>(A, i, j, slots, cols);
+      for (int p = 0; p < cnt; ++p) {
+        const long long c = cols[p];
+        double sum = A.a[(size_t)slots[p] * A.n + r];
+        for (int q = 0; q < p; ++q) {
+          const long long k = cols[q];
+          if (k >= c) break;
+          const double l_ck = find_lower<S>(A, F, c, k);
+          if (l_ck != 0.0) {
+            if (kind == 2)
+              sum -= F.l[(size_t)slots[q] * A.n + r] * l_ck;
+            else
+              sum -= F.l[(size_t)slots[q] * A.n + r] * F.d[k] * l_ck;
+          }
+        }
+        const double denom = fmax(F.d[c], floor);
+        F.l[(size_t)slots[p] * A.n + r] = sum / denom;
+      }
+      double d = A.a[(size_t)Stencil<S>::center * A.n + r];
+      for (int p = 0; p < cnt; ++p) {
+        const double lv = F.l[(size_t)slots[p] * A.n + r];
+        if (kind == 2)
+          d -= lv * lv;
+        else
+          d -= lv * lv * F.d[cols[p]];
+      }
+      if (kind == 2) {
+        if (!isfinite(d) || d <= floor_sq) {
+          atomicExch(status, kDevFactorFailed);
+          d = floor_sq * 4.0;
+        }
+        d = sqrt(d);
+      } else if (!isfinite(d) || d <= floor) {
+        atomicExch(status, kDevFactorFailed);
+        d = floor * 2.0;
+      }
+      F.d[r] = d;
+      F.dinv[r] = 1.0 / fmax(d, floor);
+    }
+    __syncthreads();
+  }
+}
+
+// Diagonal preconditioner (build_diagonal_preconditioner, ch_sparse_krylov.hpp:421-432).
+template <int S>
+__global__ void k_diag_inverse(SpOp A, double *dinv) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.n) return;
+  dinv[r] = 1.0 / fmax(fabs(A.a[(size_t)Stencil<S>::center * A.n + r]), 1.0e-30);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Persistent PCG (solve_preconditioned_cg, ch_sparse_krylov.hpp:515-660)
+// ---------------------------------------------------------------------------------------------------
+enum PrecKind { kPrecDiag = 0, kPrecLDLT = 1, kPrecICC = 2 };
+
+struct PcgArgs {
+  SpOp A;
+  const double *l;     // factor slots [S][n]
+  const double *dinv;  // [n]
+  int prec;            // PrecKind
+  const double *b;
+  double *x, *r, *z, *y, *p0, *p1, *ap;
+  int project;  // mean projection of x, r, z, p (pressure null space, pressure.cpp:225-239)
+  int max_it;
+  double tol;
+  // synchronisation
+  unsigned int *bar_count;
+  unsigned int *bar_gen;
+  int *status;
+  unsigned int *prog_f, *prog_b;  // per sweep warp progress, monotonic across applications
+  double *partials;
+  double *out;  // [0] iterations [1] abs residual [2] rel residual [3] iterate residual
+  int nsweep;   // sweep warps (ceil(nx/32)) for the 5-point wavefront
+};
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned int *p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Warp-uniform bounded wait until *flag >= target; returns the observed value (or 0 on timeout).
+__device__ __forceinline__ unsigned int wait_flag(const unsigned int *flag, unsigned int target, int *status) {
+  unsigned int v = 0;
+  const int lane = threadIdx.x & 31;
+  long long spins = 0;
+  while (true) {
+    if (lane == 0) v = ld_acquire(flag);
+    v = __shfl_sync(0xffffffffu, v, 0);
+    if (v >= target) return v;
+    if (++spins > kSpinLimit || *(volatile int *)status != kDevOk) {
+      if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
+      return 0;
+    }
+    __nanosleep(20);
+  }
+}
+
+constexpr int kPub = 16;  // columns between progress publications of a sweep warp
+
+// Forward sweep of the 5-point factor for sweep warp k.  Reads r (minus the pending mean m_r; when
+// projecting, writes the projected residual back), writes y.  ICC: y = (r - sum L y) / d.  LDLT: y = r - sum L y.
+__device__ void fwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r) {
+  const int lane = threadIdx.x & 31;
+  const int nx = P.A.nx, ny = P.A.ny, n = P.A.n;
+  const int i = 32 * k + lane;
+  const bool valid = i < nx;
+  const unsigned int base = epoch * (unsigned int)(ny + 1);
+  const double *lW = P.l, *lS = P.l + n, *lN = P.l + 3 * (size_t)n, *lE = P.l + 4 * (size_t)n;
+  double y_prev = 0.0, y_first = 0.0, y_step = 0.0;
+  unsigned int avail = 0;
+  for (int s = 0; s < ny + 31; ++s) {
+    const int j = s - lane;
+    double y_up = __shfl_up_sync(0xffffffffu, y_step, 1);
+    if (k > 0 && s < ny) {
+      if ((unsigned int)s >= avail) {
+        const unsigned int v = wait_flag(&P.prog_f[k - 1], base + (unsigned int)s + 1u, P.status);
+        if (v == 0) return;
+        avail = v - base;
+      }
+      if (lane == 0) y_up = __ldcg(&P.y[(size_t)(i - 1) * ny + s]);
+    }
+    if (valid && j >= 0 && j < ny) {
+      const size_t idx = (size_t)i * ny + j;
+      double rv = __ldcg(&P.r[idx]);
+      if (P.project) {
+        rv = rv - m_r;
+        P.r[idx] = rv;
+      }
+      double sum = rv;
+      if (P.A.px && i == nx - 1) sum -= __ldg(&lE[idx]) * __ldcg(&P.y[j]);
+      if (i > 0) sum -= __ldg(&lW[idx]) * y_up;
+      if (P.A.py && j == ny - 1) sum -= __ldg(&lN[idx]) * y_first;
+      if (j > 0) sum -= __ldg(&lS[idx]) * y_prev;
+      const double yv = (P.prec == kPrecICC) ? sum * __ldg(&P.dinv[idx]) : sum;
+      P.y[idx] = yv;
+      y_prev = yv;
+      if (j == 0) y_first = yv;
+      y_step = yv;
+    }
+    const int done = s - 30;  // columns finished by lane 31
+    if (done > 0 && (done % kPub == 0 || done == ny)) {
+      __syncwarp();
+      if (lane == 31) {
+        __threadfence();
+        st_release(&P.prog_f[k], base + (unsigned int)done);
+      }
+    }
+  }
+}
+
+// Backward sweep for sweep warp k (lines nx-1-32k-t, marching j downward).  Accumulates sum z,
+// sum r.z and sum r into acc[0..2].  ICC: z = (y - sum L^T z) / d.  LDLT: z = y / D - sum L^T z.
+__device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double (&acc)[3]) {
+  const int lane = threadIdx.x & 31;
+  const int nx = P.A.nx, ny = P.A.ny, n = P.A.n;
+  const int i = nx - 1 - (32 * k + lane);
+  const bool valid = i >= 0;
+  const unsigned int base = epoch * (unsigned int)(ny + 1);
+  const double *lW = P.l, *lS = P.l + n, *lN = P.l + 3 * (size_t)n, *lE = P.l + 4 * (size_t)n;
+  // the whole forward sweep must be finished (its last warp publishes ny columns last)
+  if (k == 0) {
+    if (wait_flag(&P.prog_f[P.nsweep - 1], base + (unsigned int)ny, P.status) == 0) return;
+  }
+  double z_prev = 0.0, z_first = 0.0, z_step = 0.0;
+  unsigned int avail = 0;
+  for (int s = 0; s < ny + 31; ++s) {
+    const int j = ny - 1 - (s - lane);
+    double z_dn = __shfl_up_sync(0xffffffffu, z_step, 1);
+    if (k > 0 && s < ny) {
+      if ((unsigned int)s >= avail) {
+        const unsigned int v = wait_flag(&P.prog_b[k - 1], base + (unsigned int)s + 1u, P.status);
+        if (v == 0) return;
+        avail = v - base;
+      }
+      if (lane == 0) z_dn = __ldcg(&P.z[(size_t)(i + 1) * ny + (ny - 1 - s)]);
+    }
+    if (valid && j >= 0 && j < ny) {
+      const size_t idx = (size_t)i * ny + j;
+      const double yv = __ldcg(&P.y[idx]);
+      double sum = (P.prec == kPrecICC) ? yv : yv * __ldg(&P.dinv[idx]);
+      if (j + 1 < ny) sum -= __ldg(&lS[idx + 1]) * z_prev;
+      if (P.A.py && j == 0) sum -= __ldg(&lN[(size_t)i * ny + ny - 1]) * z_first;
+      if (i + 1 < nx) sum -= __ldg(&lW[idx + ny]) * z_dn;
+      if (P.A.px && i == 0) {
+        const size_t e = (size_t)(nx - 1) * ny + j;
+        sum -= __ldg(&lE[e]) * __ldcg(&P.z[e]);
+      }
+      const double zv = (P.prec == kPrecICC) ? sum * __ldg(&P.dinv[idx]) : sum;
+      P.z[idx] = zv;
+      z_prev = zv;
+      if (j == ny - 1) z_first = zv;
+      z_step = zv;
+      const double rv = __ldcg(&P.r[idx]);
+      acc[0] += zv;
+      acc[1] += rv * zv;
+      acc[2] += rv;
+    }
+    const int done = s - 30;
+    if (done > 0 && (done % kPub == 0 || done == ny)) {
+      __syncwarp();
+      if (lane == 31) {
+        __threadfence();
+        st_release(&P.prog_b[k], base + (unsigned int)done);
+      }
+    }
+  }
+}
+
+// Level-scheduled forward+backward application of a general slot factor by one CTA (13-point CH
+// operator; also handles periodic y, where the 13-point graph is a chain).  Accumulates like bwd5.
+template <int S>
+__device__ void apply_levels(const PcgArgs &P, double (&acc)[3]) {
+  const SpOp &A = P.A;
+  const int n = A.n;
+  const bool seq = (S == 13 && A.py);
+  const int nlev = num_levels<S>(A.nx, A.ny, A.py);
+  // forward: y_r = r_r - sum_{lower} L y  (ICC divides by d)
+  for (int lev = 0; lev < nlev; ++lev) {
+    int i0, i1;
+    level_range<S>(lev, A.nx, A.ny, A.py, i0, i1);
+    if (seq) i0 = i1 = 0;
+    for (int ii = i0 + (int)threadIdx.x; ii <= i1; ii += blockDim.x) {
+      int i, j;
+      level_row<S>(lev, ii, A.ny, A.py, i, j);
+      const long long r = (long long)i * A.ny + j;
+      int slots[S];
+      long long cols[S];
+      const int cnt = lower_slots<S>(A, i, j, slots, cols);
+      double sum = P.r[r];
+      for (int p = 0; p < cnt; ++p) sum -= P.l[(size_t)slots[p] * n + r] * P.y[cols[p]];
+      P.y[r] = (P.prec == kPrecICC) ? sum * P.dinv[r] : sum;
+    }
+    if (!seq) __syncthreads();
+  }
+  __syncthreads();
+  // backward: z_r = y_r (/D) - sum_{c > r, L_cr != 0} L_cr z_c, ascending c (lower_transpose order)
+  for (int lev = nlev - 1; lev >= 0; --lev) {
+    int i0, i1;
+    level_range<S>(lev, A.nx, A.ny, A.py, i0, i1);
+    if (seq) i0 = i1 = 0;
+    for (int ii = i0 + (int)threadIdx.x; ii <= i1; ii += blockDim.x) {
+      int i, j;
+      level_row<S>(lev, ii, A.ny, A.py, i, j);
+      const long long r = (long long)i * A.ny + j;
+      // upper neighbours c of r: slot s of r with col c > r; L_cr sits in row c at the mirrored slot
+      int slots[S];
+      long long cols[S];
+      int cnt = 0;
+      for (int s = 0; s < S; ++s) {
+        const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+        if (c <= r) continue;
+        const double lcr = P.l[(size_t)(S - 1 - s) * n + c];
+        if (lcr == 0.0) continue;
+        int p = cnt++;
+        while (p > 0 && cols[p - 1] > c) {
+          cols[p] = cols[p - 1];
+          slots[p] = slots[p - 1];
+          --p;
+        }
+        cols[p] = c;
+        slots[p] = s;
+      }
+      double sum = (P.prec == kPrecICC) ? P.y[r] : P.y[r] * P.dinv[r];
+      for (int p = 0; p < cnt; ++p) sum -= P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
+      const double zv = (P.prec == kPrecICC) ? sum * P.dinv[r] : sum;
+      P.z[r] = zv;
+      const double rv = P.r[r];
+      acc[0] += zv;
+      acc[1] += rv * zv;
+      acc[2] += rv;
+    }
+    if (!seq) __syncthreads();
+  }
+}
+
+// One persistent launch runs the whole PCG.  SWEEP: 0 = 5-point pipelined wavefront, 1 = level-scheduled
+// slot factor (CTA 0), 2 = diagonal.
+template <int S, int SWEEP>
+__global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
+  __shared__ double sh[8 * 32 + 8];
+  const GridBarrier bar{P.bar_count, P.bar_gen, P.status, gridDim.x};
+  int parity = 0;
+  const SpOp &A = P.A;
+  const int n = A.n, ny = A.ny;
+  const double dn_ = (double)n;
+  const long long per = (n + gridDim.x - 1) / gridDim.x;
+  const long long lo = (long long)blockIdx.x * per, hi = min((long long)n, lo + per);
+  const int warp = threadIdx.x >> 5;
+  const int nwarps_cta = blockDim.x >> 5;
+
+  // ---- r = b - A x0, project r, initial residual (ch_sparse_krylov.hpp:531-558)
+  double v3[3] = {0.0, 0.0, 0.0};
+  for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+    const int i = (int)(r / ny), j = (int)(r % ny);
+    const double rr = P.b[r] - spmv_row<S>(A, P.x, i, j);
+    P.r[r] = rr;
+    v3[0] += rr;
+    v3[1] += rr * rr;
+    v3[2] += P.b[r] * P.b[r];
+  }
+  if (!grid_sum<3>(v3, P.partials, parity, sh, bar)) return;
+  double m_r = P.project ? v3[0] / dn_ : 0.0;
+  double rn2 = P.project ? fmax(v3[1] - v3[0] * v3[0] / dn_, 0.0) : v3[1];
+  const double rhs_norm = sqrt(fmax(v3[2], 0.0));
+  double absr = sqrt(fmax(rn2, 0.0));
+  double relr = absr / fmax(rhs_norm, 1.0e-30);
+  int iterations = 0;
+  double iter_res = 0.0;
+  if (relr < P.tol || absr < P.tol) {  // x stays x0 (the reference projects r only)
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      P.out[0] = 0;
+      P.out[1] = absr;
+      P.out[2] = relr;
+      P.out[3] = 0.0;
+    }
+    return;
+  }
+
+  unsigned int epoch = 0;
+  auto precondition = [&](double m_r_now, double (&acc)[3]) -> bool {
+    acc[0] = acc[1] = acc[2] = 0.0;
+    ++epoch;
+    if (SWEEP == 0) {
+      // sweep warp k lives in CTA k % G, warp k / G
+      for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta) {
+        fwd5(P, k, epoch, m_r_now);
+      }
+      for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta) {
+        bwd5(P, k, epoch, acc);
+      }
+    } else if (SWEEP == 1) {
+      if (P.project) {  // level-scheduled path: project r first (pointwise, own range)
+        for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) P.r[r] = P.r[r] - m_r_now;
+        if (!bar.sync()) return false;
+      }
+      if (blockIdx.x == 0) apply_levels<S>(P, acc);
+    } else {
+      for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+        double rv = P.r[r];
+        if (P.project) {
+          rv = rv - m_r_now;
+          P.r[r] = rv;
+        }
+        const double zv = P.dinv[r] * rv;
+        P.z[r] = zv;
+        acc[0] += zv;
+        acc[1] += rv * zv;
+        acc[2] += rv;
+      }
+    }
+    return grid_sum<3>(acc, P.partials, parity, sh, bar);
+  };
+
+  double acc[3];
+  if (!precondition(m_r, acc)) return;
+  double m_z = P.project ? acc[0] / dn_ : 0.0;
+  double rz_old = P.project ? acc[1] - m_z * acc[2] : acc[1];
+  if (!isfinite(rz_old) || rz_old <= 0.0) {
+    if (threadIdx.x == 0) atomicCAS(P.status, kDevOk, kDevPcgBreakdownRz0);
+    return;
+  }
+  double beta = 0.0;
+  double m_x = 0.0;
+  double *p_old = P.p0, *p_new = P.p1;
+  bool first = true;
+  const int limit = P.max_it > 1 ? P.max_it : 1;
+  for (int it = 0; it < limit; ++it) {
+    // ---- P1: p = z - m_z + beta p_old ; Ap = A p  (p at neighbours formed on the fly)
+    double v[3] = {0.0, 0.0, 0.0};
+    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+      const int i = (int)(r / ny), j = (int)(r % ny);
+      double apv = 0.0;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const double a = A.a[(size_t)s * n + r];
+        if (a != 0.0) {
+          const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+          const double pc = first ? (P.z[c] - m_z) : (P.z[c] - m_z) + beta * p_old[c];
+          apv += a * pc;
+        }
+      }
+      const double pr = first ? (P.z[r] - m_z) : (P.z[r] - m_z) + beta * p_old[r];
+      p_new[r] = pr;
+      P.ap[r] = apv;
+      v[0] += pr;
+      v[1] += pr * apv;
+      v[2] += apv;
+    }
+    if (!grid_sum<3>(v, P.partials, parity, sh, bar)) return;
+    const double m_p = P.project ? v[0] / dn_ : 0.0;
+    const double pap = P.project ? v[1] - m_p * v[2] : v[1];
+    if (!isfinite(pap) || fabs(pap) < 1.0e-30) {
+      if (threadIdx.x == 0) atomicCAS(P.status, kDevOk, kDevPcgBreakdownPap);
+      return;
+    }
+    const double alpha = rz_old / pap;
+    // ---- P2: x += alpha p ; r -= alpha Ap ; norms (ch_sparse_krylov.hpp:592-610)
+    double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+      const double pp = p_new[r] - m_p;
+      p_new[r] = pp;
+      const double delta = alpha * pp;
+      const double xv = (P.x[r] - m_x) + delta;
+      P.x[r] = xv;
+      const double rv = P.r[r] - alpha * P.ap[r];
+      P.r[r] = rv;
+      w[0] += delta * delta;
+      w[1] += xv * xv;
+      w[2] += xv;
+      w[3] += rv;
+      w[4] += rv * rv;
+    }
+    if (!grid_sum<5>(w, P.partials, parity, sh, bar)) return;
+    m_x = P.project ? w[2] / dn_ : 0.0;
+    m_r = P.project ? w[3] / dn_ : 0.0;
+    rn2 = P.project ? fmax(w[4] - w[3] * w[3] / dn_, 0.0) : w[4];
+    iterations = it + 1;
+    iter_res = sqrt(w[0] / fmax(w[1], 1.0e-30));
+    absr = sqrt(fmax(rn2, 0.0));
+    relr = absr / fmax(rhs_norm, 1.0e-30);
+    if (relr < P.tol || absr < P.tol) break;
+    // ---- z = M^{-1} r, project z, r.z (ch_sparse_krylov.hpp:626-635)
+    if (!precondition(m_r, acc)) return;
+    m_z = P.project ? acc[0] / dn_ : 0.0;
+    const double rz_new = P.project ? acc[1] - m_z * acc[2] : acc[1];
+    if (!isfinite(rz_new) || rz_new <= 0.0) {
+      if (threadIdx.x == 0) atomicCAS(P.status, kDevOk, kDevPcgBreakdownRz);
+      return;
+    }
+    beta = rz_new / rz_old;
+    rz_old = rz_new;
+    double *t = p_old;
+    p_old = p_new;
+    p_new = t;
+    first = false;
+  }
+  // pending projection of x
+  if (P.project && m_x != 0.0) {
+    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) P.x[r] = P.x[r] - m_x;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.out[0] = (double)iterations;
+    P.out[1] = absr;
+    P.out[2] = relr;
+    P.out[3] = iter_res;
+  }
+}
+
+// Equation residual of the CH solve, phase_field.cpp:484-502: partial sums of (b - A x)^2 and b^2.
+template <int S>
+__global__ void k_residual_partials(SpOp A, const double *b, const double *x, double *partials) {
+  __shared__ double sh[8 * 32];
+  double v[2] = {0.0, 0.0};
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(r / A.ny), j = (int)(r % A.ny);
+    const double d = b[r] - spmv_row<S>(A, x, i, j);
+    v[0] += d * d;
+    v[1] += b[r] * b[r];
+  }
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x * 2] = v[0];
+    partials[blockIdx.x * 2 + 1] = v[1];
+  }
+}
+
+}  // namespace dn

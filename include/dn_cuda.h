@@ -1,0 +1,184 @@
+/*
+ * dn_cuda.h -- C-ABI of the B200 (sm_100a) CHNS time-step library, libdn_cuda.so.
+ *
+ * The library replaces, as a drop-in backend, the hot path of Hygc0627/ding_nsch_core_solver's coupled
+ * solver: one time step on the 2D MAC grid (Cahn-Hilliard implicit solve, momentum predictor, pressure
+ * correction).  Every entry point is `extern "C"`, takes plain pointers and sizes, returns a dn_status and
+ * never throws or aborts.  A handle owns its device memory and one CUDA stream; calls on one handle must
+ * be serialised by the caller, different handles are independent.
+ *
+ * Field arrays exchanged with the host use the reference's Field2D layout (src/core/base/field.hpp:9-36):
+ * FP64, (nx'+2g) x (ny'+2g) values with j (the y index) contiguous, where nx' = nx+1 for u-type fields,
+ * ny' = ny+1 for v-type fields, and g = ghost (3).
+ */
+#ifndef DN_CUDA_H
+#define DN_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Messages (dn_status_string) mirror the reference's std::runtime_error texts. */
+typedef enum {
+  DN_OK = 0,
+  DN_ERR_INVALID_ARGUMENT = 1,   /* bad size / pointer / config value                                  */
+  DN_ERR_CONFIG = 2,             /* config.cpp:49-208 parse errors, operators.cpp:11-34 BC validation  */
+  DN_ERR_CUDA = 3,               /* a CUDA runtime call failed                                           */
+  DN_ERR_ICC_FAILED = 4,         /* pressure.cpp:36-38  "ICC preconditioner construction failed"       */
+  DN_ERR_ILDLT_FAILED = 5,       /* pressure.cpp:44-46  "ILDLT preconditioner construction failed"     */
+  DN_ERR_PCG_BREAKDOWN = 6,      /* ch_sparse_krylov.hpp:566-568, 588-590, 631-633                      */
+  DN_ERR_BICGSTAB_BREAKDOWN = 7, /* ch_sparse_krylov.hpp:887-938                                       */
+  DN_ERR_TIMEOUT = 8,            /* a device-side wait (grid barrier / wavefront flag) gave up         */
+  DN_ERR_NONFINITE = 9,          /* solver.cpp:355-364 "non-finite diagnostic detected"                */
+  DN_ERR_UNSUPPORTED = 10        /* a config the CUDA path does not implement (see message)            */
+} dn_status;
+
+typedef enum { DN_BC_UNSET = 0, DN_BC_DIRICHLET = 1, DN_BC_NEUMANN = 2 } dn_bc_type;          /* config.hpp:24-28 */
+typedef enum { DN_LEFT = 0, DN_RIGHT = 1, DN_BOTTOM = 2, DN_TOP = 3 } dn_side;                 /* config.hpp:17-22 */
+typedef enum { DN_MODE_COUPLED = 0, DN_MODE_SINGLE_PHASE = 1, DN_MODE_ADVECTION_ONLY = 2 } dn_mode;
+/* pressure_scheme (pressure.cpp:1031-1071; reference aliases liu_/paper_ fold onto these; the new config
+ * values cuda_icpcg / cuda_ildlt_pcg / cuda_split_icpcg / cuda_split_ildlt_pcg select the same schemes). */
+typedef enum {
+  DN_P_JACOBI = 0,
+  DN_P_ICPCG = 1,
+  DN_P_ILDLT_PCG = 2,
+  DN_P_SPLIT_ICPCG = 3,
+  DN_P_SPLIT_ILDLT_PCG = 4
+} dn_pressure_scheme;
+/* arithmetic of the Krylov inner loops: plain FP64, or FP32 inner solves wrapped in FP64 defect correction */
+typedef enum { DN_PRECISION_FP64 = 0, DN_PRECISION_MIXED = 1 } dn_precision;
+
+typedef struct {
+  int type; /* dn_bc_type */
+  double value;
+} dn_bc;
+
+/* Numeric image of ding::Config (config.hpp:35-136), keys the time step reads. */
+typedef struct {
+  int nx, ny, ghost;
+  int mode;            /* dn_mode */
+  int freeze_ch;
+  int pressure_scheme; /* dn_pressure_scheme */
+  int phase_initializer; /* 0 default, 1 zalesak_disk */
+  int velocity_profile;  /* 0 default, 1 solid_body_rotation */
+  int invert_phase;
+  int periodic_x, periodic_y;
+  int ch_inner_iterations, momentum_iterations, poisson_iterations;
+  int surface_tension_smoothing_passes;
+  double dt, lx, ly, re, ca, pe, cn, density_ratio, viscosity_ratio;
+  double surface_tension_multiplier, surface_tension_smoothing_weight;
+  double ch_tolerance, pressure_tolerance, momentum_tolerance;
+  double body_force_x, body_force_y;
+  double interface_center_x, interface_center_y, interface_radius, interface_amplitude, interface_wavenumber;
+  double zalesak_slot_width, zalesak_slot_depth;
+  double advect_u, advect_v, rotation_center_x, rotation_center_y, angular_velocity;
+  double top_wall_velocity_x, bottom_wall_velocity_x;
+  dn_bc p_bc[4], u_bc[4], v_bc[4]; /* indexed by dn_side */
+  int precision;                   /* dn_precision */
+  double mixed_inner_tolerance;    /* relative tolerance of each FP32 inner solve (mixed form) */
+} dn_config;
+
+/* Fields (Solver members, src/core/coupled/solver.hpp:64-91). */
+typedef enum {
+  DN_F_C = 0, DN_F_C_PREV, DN_F_C_PREV2, DN_F_MU, DN_F_RHO, DN_F_ETA, DN_F_RHO_PREV, DN_F_ETA_PREV,
+  DN_F_RHO_MID, DN_F_ETA_MID, DN_F_P, DN_F_P_PREV, DN_F_P_CORR, DN_F_U, DN_F_V, DN_F_U_PREV, DN_F_V_PREV,
+  DN_F_U_STAR, DN_F_V_STAR, DN_F_SFX_CELL, DN_F_SFY_CELL, DN_F_SFX_U, DN_F_SFY_V, DN_F_E_PREV,
+  DN_F_HU_PREV, DN_F_HV_PREV, DN_F_COUNT
+} dn_field;
+
+/* What one step (or one backend call) reports: Solver::last_* members (solver.hpp:93-108). */
+typedef struct {
+  int ch_iterations, momentum_iterations, pressure_iterations, coupling_iterations;
+  int ch_preconditioner; /* 0 diagonal, 1 ILDLT, 2 diagonal fallback after a breakdown, -1 not used */
+  double ch_residual, ch_equation_residual, momentum_residual, pressure_residual;
+  double boundary_speed_pre, boundary_speed_post;
+  int refinement_cycles; /* mixed form: outer FP64 defect-correction cycles of the pressure solve */
+} dn_report;
+
+/* Diagnostics (src/core/base/diagnostics.hpp; computed as in diagnostics.cpp:114-167). */
+typedef struct {
+  double mass, mass_drift, divergence_l2, max_divergence, max_abs_mu, max_velocity, kinetic_energy;
+  double total_free_energy, rho_min, rho_max, eta_min, eta_max;
+  double dt_limit_advective, dt_limit_capillary, dt_limit_ch_explicit, dt_limit_active, dt_limit_ratio;
+} dn_diag;
+
+typedef struct dn_handle dn_handle;
+
+/* ---- configuration ------------------------------------------------------------------------------- */
+/* Defaults of struct Config (config.hpp:35-136). */
+void dn_config_default(dn_config *cfg);
+/* Parse a reference case file (`key = value`, `#` comments) -- replaces ding::load_config (config.cpp:49-208).
+ * Accepts the reference's pressure_scheme spellings and the new cuda_* values.  `err` may be NULL. */
+dn_status dn_config_parse(const char *text, dn_config *cfg, char *err, size_t err_len);
+
+/* ---- lifetime ------------------------------------------------------------------------------------ */
+/* Replaces ding::Solver::Solver (solver.cpp:25-57): allocates every field on `device` (-1 = current). */
+dn_status dn_create(const dn_config *cfg, int device, dn_handle **out);
+dn_status dn_destroy(dn_handle *h);
+const char *dn_status_string(dn_status s);
+/* Message of the last failure on this handle (reference wording where one exists). */
+const char *dn_last_error(const dn_handle *h);
+
+/* ---- state ----------------------------------------------------------------------------------------- */
+/* Solver::initialize (solver.cpp:69-113) on the device: built-in phase / velocity initialisers. */
+dn_status dn_initialize(dn_handle *h);
+/* Host <-> device copy of one Field2D-layout field (`count` doubles, checked against the field size). */
+dn_status dn_set_field(dn_handle *h, int field, const double *host, size_t count);
+dn_status dn_get_field(dn_handle *h, int field, double *host, size_t count);
+/* Device-pointer access for callers that keep their own device buffers (same layout). */
+dn_status dn_field_device_ptr(dn_handle *h, int field, double **dev_ptr, size_t *count);
+void dn_set_initial_mass(dn_handle *h, double mass);
+/* After injecting c, c_prev, p, p_prev, u, v, E_prev, H_prev with dn_set_field, rebuild the derived fields
+ * exactly as a restart does (io.cpp:412-436): BC ghosts, rho/eta (n and n-1), midpoint materials, mu. */
+dn_status dn_refresh_derived(dn_handle *h);
+
+/* ---- the time step and its phases (each replaces the cited reference member) ------------------------ */
+/* Solver::advance_one_timestep (solver.cpp:224-283). */
+dn_status dn_step(dn_handle *h, int step, dn_report *rep);
+/* history copies at the start of advance_one_timestep (solver.cpp:225-231) */
+dn_status dn_begin_step(dn_handle *h, int step);
+/* Solver::advance_phase_state (phase_field.cpp:258-281): CH solve, materials, surface force */
+dn_status dn_phase(dn_handle *h, int step, dn_report *rep);
+/* compute_momentum_fluxes + solve_momentum_predictor (momentum.cpp:55-85, 157-502) */
+dn_status dn_momentum(dn_handle *h, int step, dn_report *rep);
+/* Solver::solve_pressure_correction (pressure.cpp:1031-1089) for the configured scheme */
+dn_status dn_pressure(dn_handle *h, dn_report *rep);
+/* Solver::apply_pressure_velocity_correction (operators.cpp:480-534) */
+dn_status dn_correct(dn_handle *h, dn_report *rep);
+
+/* ---- backend entry points with host buffers (what a reference-side binding calls) ------------------ */
+/* CH backend: replaces Solver::solve_phase_linear_system_eq25 (phase_field.cpp:437-503) for
+ * ch_solver = cuda_sparse_pcg.  rhs_field, c_state: Field2D layout (nx x ny cell field); c_state in/out. */
+dn_status dn_ch_linear_solve(dn_handle *h, const double *rhs_field, double alpha0, double *c_state,
+                             double *iterate_residual, double *equation_residual, int *iterations);
+/* Pressure backend: replaces Solver::solve_pressure_correction_{icpcg,ildlt_pcg,liu_split_icpcg,
+ * liu_split_ildlt_pcg} (pressure.cpp:302-365, 470-491).  Inputs u_star, v_star, rho_mid, p, p_prev
+ * (Field2D layout), step index (split extrapolation); output p_corr (Field2D, ghosts filled). */
+dn_status dn_pressure_solve(dn_handle *h, int step, const double *u_star, const double *v_star,
+                            const double *rho_mid, const double *p, const double *p_prev, double *p_corr,
+                            int *iterations, double *relative_residual);
+
+/* ---- diagnostics ------------------------------------------------------------------------------------ */
+/* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
+dn_status dn_diagnostics(dn_handle *h, dn_diag *out);
+/* Solver::compute_mass (diagnostics.cpp:24-32), FP64 on the device. */
+dn_status dn_compute_mass(dn_handle *h, int field, double *mass);
+
+/* ---- timing / introspection ---------------------------------------------------------------------------- */
+/* Block until the handle's stream is idle. */
+dn_status dn_synchronize(dn_handle *h);
+/* The handle's CUDA stream (cudaStream_t) for event timing by the caller. */
+void *dn_stream(dn_handle *h);
+/* Device-side times (CUDA events) of the last dn_step, milliseconds: [0] CH phase, [1] momentum phase,
+ * [2] pressure phase, [3] correction phase, [4] pressure PCG kernel, [5] CH PCG kernel(s), [6] momentum
+ * BiCGSTAB kernel, [7] pressure PCG iterations.  `out` holds 8 doubles. */
+dn_status dn_last_phase_times(dn_handle *h, double *out);
+/* Number of this library's kernels launched since the handle was created. */
+long long dn_kernel_launches(const dn_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -2063,6 +2063,25 @@ int orc_ch_linear_solve(orc_solver *s, const double *rhs_field, double alpha0, d
   GUARD_END
 }
 
+/* restart-load rebuild of the derived fields, io.cpp:412-436 */
+int orc_refresh_derived(orc_solver *s) {
+  GUARD_BEGIN
+  bc_scalar(s, &s->f[ORC_F_C]);
+  bc_scalar(s, &s->f[ORC_F_C_PREV]);
+  bc_scalar(s, &s->f[ORC_F_C_PREV2]);
+  bc_pressure(s, &s->f[ORC_F_P]);
+  bc_pressure(s, &s->f[ORC_F_P_PREV]);
+  bc_u(s, &s->f[ORC_F_U]);
+  bc_v(s, &s->f[ORC_F_V]);
+  bc_u(s, &s->f[ORC_F_U_PREV]);
+  bc_v(s, &s->f[ORC_F_V_PREV]);
+  update_materials(s);
+  materials_from(s, &s->f[ORC_F_C_PREV], &s->f[ORC_F_RHO_PREV], &s->f[ORC_F_ETA_PREV]);
+  update_midpoint(s);
+  refresh_mu(s);
+  GUARD_END
+}
+
 void orc_get_report(const orc_solver *s, orc_report *r) { *r = s->rep; }
 
 double orc_compute_mass(orc_solver *s, int field_id) { return mass_of(s, &s->f[field_id]); }

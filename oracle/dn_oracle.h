@@ -99,6 +99,7 @@ int orc_momentum(orc_solver *s, int step);         /* momentum.cpp:55-85 + 157-5
 int orc_pressure(orc_solver *s);                   /* solve_pressure_correction, pressure.cpp:1031-1089 */
 int orc_correct(orc_solver *s);                    /* apply_pressure_velocity_correction, operators.cpp:480-534 */
 int orc_finish_step(orc_solver *s);                /* refresh mu, solver.cpp:274 */
+int orc_refresh_derived(orc_solver *s);            /* restart-load rebuild of derived fields, io.cpp:412-436 */
 int orc_ch_linear_solve(orc_solver *s, const double *rhs_field, double alpha0, double *c_state,
                         double *iterate_residual, double *equation_residual); /* phase_field.cpp:437-503 */
 void orc_get_report(const orc_solver *s, orc_report *r);

@@ -200,7 +200,7 @@ def _load(impl: str):
         "field": (dp, [vp, C.c_int, ip, ip, ip]), "set_initial_mass": (None, [vp, C.c_double]),
         "initialize": (C.c_int, [vp]), "step": (C.c_int, [vp, C.c_int]), "begin_step": (C.c_int, [vp, C.c_int]),
         "phase": (C.c_int, [vp, C.c_int]), "momentum": (C.c_int, [vp, C.c_int]), "pressure": (C.c_int, [vp]),
-        "correct": (C.c_int, [vp]), "finish_step": (C.c_int, [vp]),
+        "correct": (C.c_int, [vp]), "finish_step": (C.c_int, [vp]), "refresh_derived": (C.c_int, [vp]),
         "ch_linear_solve": (C.c_int, [vp, dp, C.c_double, dp, dp, dp]),
         "get_report": (None, [vp, C.POINTER(Report)]), "diagnostics": (None, [vp, C.POINTER(Diag)]),
         "compute_mass": (C.c_double, [vp, C.c_int]),
@@ -288,6 +288,10 @@ class OracleSolver:
 
     def finish_step(self):
         self._check(self._f["finish_step"](self._h))
+
+    def refresh_derived(self):
+        """Rebuild BC ghosts, materials and mu from the state fields, as a restart load does (io.cpp:412-436)."""
+        self._check(self._f["refresh_derived"](self._h))
 
     def ch_linear_solve(self, rhs: np.ndarray, alpha0: float, c_state: np.ndarray):
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)

@@ -236,6 +236,26 @@ int ref_finish_step(void *hp) {
   return guarded(h, [&] { h->solver->refresh_chemical_potential_for_current_phase(); });
 }
 
+int ref_refresh_derived(void *hp) {
+  auto *h = static_cast<RefHandle *>(hp);
+  return guarded(h, [&] {
+    ding::Solver &s = *h->solver;
+    s.apply_scalar_bc(s.c_);
+    s.apply_scalar_bc(s.c_previous_step_);
+    s.apply_scalar_bc(s.c_two_steps_back_);
+    s.apply_pressure_bc(s.pressure_);
+    s.apply_pressure_bc(s.pressure_previous_step_);
+    s.apply_u_velocity_bc(s.u_);
+    s.apply_v_bc(s.v_);
+    s.apply_u_velocity_bc(s.u_previous_step_);
+    s.apply_v_bc(s.v_previous_step_);
+    s.update_materials();
+    s.update_materials_from_phase(s.c_previous_step_, s.rho_previous_step_, s.eta_previous_step_);
+    s.update_midpoint_materials();
+    s.refresh_chemical_potential_for_current_phase();
+  });
+}
+
 int ref_ch_linear_solve(void *hp, const double *rhs_field, double alpha0, double *c_state, double *iterate_residual,
                         double *equation_residual) {
   auto *h = static_cast<RefHandle *>(hp);

@@ -1,0 +1,254 @@
+"""Parity of the CUDA time step (libdn_cuda through its C-ABI) with the CPU oracle.
+
+Each case injects the same seeded FP64 state into the oracle (the C restatement of the reference, itself
+pinned bit for bit to the reference build and its golden run) and into the GPU handle, advances both, and
+compares c, mu, u, v, p after every phase / step.  Tolerance: relative L2 error <= 1e-10 per step (the
+plain-form bar), and equal Krylov iteration counts.
+"""
+import csv
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSolver, parse_cfg, with_defaults
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1.0e-10
+COMPARE = ("c", "mu", "u", "v", "p")
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def interior(a, g, extra_x=0, extra_y=0):
+    return a[g:a.shape[0] - g, g:a.shape[1] - g]
+
+
+@pytest.fixture(scope="module")
+def dn():
+    import ding_nsch_core_solver_b200 as m
+
+    m.load()
+    return m
+
+
+def unit(**kw):
+    base = dict(nx=32, ny=32, ghost=3, dt=1.0e-3, periodic_x=True, periodic_y=True, poisson_iterations=5000,
+                pressure_tolerance=1.0e-10, momentum_iterations=200, momentum_tolerance=1.0e-10,
+                density_ratio=10.0, viscosity_ratio=5.0, ch_inner_iterations=200, ch_tolerance=1e-10)
+    base.update(kw)
+    return with_defaults(base)
+
+
+CASES = {
+    "periodic_icpcg": unit(pressure_scheme="icpcg"),
+    "periodic_split_icpcg": unit(pressure_scheme="split_icpcg"),
+    "periodic_ildlt": unit(pressure_scheme="ildlt_pcg"),
+    "walls_split_ildlt": unit(nx=40, ny=56, periodic_x=False, periodic_y=False, pressure_scheme="split_ildlt_pcg",
+                              body_force_y=-0.98, dt=1e-4),
+    "walls_split_icpcg_wide": unit(nx=96, ny=48, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
+                                   body_force_y=-0.98, dt=1e-4),
+    "channel_x_icpcg": unit(nx=48, ny=32, periodic_x=True, periodic_y=False, pressure_scheme="icpcg",
+                            top_wall_velocity_x=0.5, bottom_wall_velocity_x=-0.5, dt=1e-4),
+    "channel_y_split": unit(nx=32, ny=40, periodic_x=False, periodic_y=True, pressure_scheme="split_icpcg", dt=1e-4),
+    "mixed_bcs_icpcg": unit(nx=36, ny=44, periodic_x=False, periodic_y=False, pressure_scheme="icpcg", dt=1e-4,
+                            u_bc_left_type="dirichlet", u_bc_left_value=-0.1, u_bc_right_type="neumann",
+                            u_bc_right_value=0.05, v_bc_left_type="neumann", v_bc_right_type="neumann",
+                            v_bc_top_type="neumann", v_bc_top_value=0.02, pressure_bc_top_type="dirichlet",
+                            pressure_bc_top_value=0.3),
+    "smoothing_split": unit(nx=40, ny=40, pressure_scheme="split_icpcg", surface_tension_smoothing_passes=2,
+                            surface_tension_smoothing_weight=0.1, dt=1e-4),
+    "freeze_ch": unit(freeze_ch=True, pressure_scheme="icpcg", surface_tension_multiplier=0.0),
+    "single_phase": unit(mode="single_phase", pressure_scheme="icpcg", density_ratio=3.0),
+    "many_lines_split": unit(nx=130, ny=24, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
+                             dt=1e-4, body_force_y=-1.0),
+}
+
+
+def seeded_pair(dn, cfg, seed, amp=0.02):
+    """Oracle and GPU solver holding the same seeded state (every field copied from the oracle)."""
+    orc = OracleSolver(cfg, "port")
+    orc.initialize()
+    rng = np.random.default_rng(seed)
+    g = cfg["ghost"]
+    if cfg["mode"] == "coupled":
+        f = orc.field("c")
+        f[g:-g, g:-g] += amp * rng.standard_normal(f[g:-g, g:-g].shape)
+    for name, a in (("u", 0.05), ("v", 0.05), ("p", 0.1)):
+        f = orc.field(name)
+        f[g:-g, g:-g] += a * rng.standard_normal(f[g:-g, g:-g].shape)
+    orc.refresh_derived()  # BC ghosts, materials and mu of the perturbed state, as a restart load builds them
+    gpu = dn.Solver(cfg)
+    from ding_nsch_core_solver_b200.capi import FIELDS
+
+    for name in FIELDS:
+        gpu.set_field(name, orc.field(name))
+    gpu.set_initial_mass(0.0)
+    orc.set_initial_mass(0.0)
+    return orc, gpu
+
+
+def assert_fields_close(orc, gpu, names, where, tol=TOL):
+    g = orc.cfg["ghost"]
+    for name in names:
+        a = interior(gpu.get_field(name), g)
+        b = interior(orc.field(name), g)
+        err = rel_l2(a, b)
+        assert err <= tol, f"{where}: {name} rel-L2 {err:.3e} > {tol:.0e}"
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_step_parity(dn, name):
+    cfg = CASES[name]
+    orc, gpu = seeded_pair(dn, cfg, seed=11)
+    for k in range(3):
+        orc.step(k)
+        rep = gpu.step(k)
+        ro = orc.report()
+        assert_fields_close(orc, gpu, COMPARE, f"{name} step {k}")
+        assert rep["pressure_iterations"] == ro["pressure_iterations"], (k, rep, ro)
+        assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
+        assert rep["momentum_iterations"] == ro["momentum_iterations"], (k, rep, ro)
+        assert rep["ch_preconditioner"] == ro["ch_preconditioner"]
+        assert math.isclose(rep["pressure_residual"], ro["pressure_residual"], rel_tol=1e-3, abs_tol=1e-14)
+
+
+def test_phase_by_phase_parity(dn):
+    """Every phase entry point on its own (the per-backend boundary)."""
+    cfg = CASES["walls_split_ildlt"]
+    orc, gpu = seeded_pair(dn, cfg, seed=5)
+    for k in range(2):
+        orc.begin_step(k)
+        gpu.begin_step(k)
+        orc.phase(k)
+        gpu.phase(k)
+        assert_fields_close(orc, gpu, ("c", "mu", "rho", "eta", "rho_mid", "sfx_u", "sfy_v", "e_prev"), f"phase {k}")
+        orc.momentum(k)
+        gpu.momentum(k)
+        assert_fields_close(orc, gpu, ("u_star", "v_star", "hu_prev", "hv_prev"), f"momentum {k}")
+        orc.pressure()
+        gpu.pressure()
+        assert_fields_close(orc, gpu, ("p_corr",), f"pressure {k}")
+        orc.correct()
+        gpu.correct()
+        assert_fields_close(orc, gpu, ("u", "v", "p", "p_prev"), f"correct {k}")
+
+
+def test_stencil_kernels_bitwise(dn):
+    """With --fmad=false the explicit stencil phase reproduces the reference's doubles exactly: compare the CH
+    explicit operator stored as E_prev after one phase, and the surface forces."""
+    cfg = CASES["walls_split_icpcg_wide"]
+    orc, gpu = seeded_pair(dn, cfg, seed=3)
+    orc.begin_step(1)
+    gpu.begin_step(1)
+    orc.phase(1)
+    gpu.phase(1)
+    g = cfg["ghost"]
+    np.testing.assert_array_equal(interior(gpu.get_field("e_prev"), g), interior(orc.field("e_prev"), g))
+
+
+def test_boundary_ghost_rules(dn):
+    """Ghost values of the configurable-BC case (core_solver_unit_tests.cpp:149-215) equal the oracle's on every
+    ghost cell that a stencil can read.  Excluded: corner cells outside in both directions and more than one
+    cell out in either, which the reference fills from a not yet refreshed x-ghost and no stencil reads."""
+    cfg = unit(periodic_x=False, periodic_y=False, u_bc_left_type="dirichlet", u_bc_left_value=-0.5,
+               u_bc_right_type="neumann", u_bc_right_value=0.25, u_bc_bottom_type="neumann",
+               u_bc_bottom_value=0.1, u_bc_top_type="dirichlet", u_bc_top_value=1.5, v_bc_left_type="neumann",
+               v_bc_left_value=-0.2, v_bc_right_type="dirichlet", v_bc_right_value=0.7,
+               v_bc_bottom_type="dirichlet", v_bc_bottom_value=-1.2, v_bc_top_type="neumann", v_bc_top_value=0.3,
+               pressure_bc_left_type="dirichlet", pressure_bc_left_value=2.0, pressure_bc_right_type="neumann",
+               pressure_bc_right_value=0.4, pressure_bc_bottom_type="neumann", pressure_bc_bottom_value=-0.1,
+               pressure_bc_top_type="dirichlet", pressure_bc_top_value=-3.0, pressure_scheme="icpcg", dt=1e-4)
+    orc, gpu = seeded_pair(dn, cfg, seed=2)
+    orc.step(0)
+    gpu.step(0)
+    g = cfg["ghost"]
+    for name in ("c", "mu", "p", "u", "v", "u_star", "v_star", "p_corr"):
+        a, b = gpu.get_field(name), orc.field(name)
+        mask = np.ones_like(a, dtype=bool)
+        nxg, nyg = a.shape
+        for i in range(nxg):
+            for j in range(nyg):
+                di = max(g - i, i - (nxg - 1 - g), 0)
+                dj = max(g - j, j - (nyg - 1 - g), 0)
+                if di >= 1 and dj >= 1 and max(di, dj) >= 2:
+                    mask[i, j] = False
+        err = np.max(np.abs(a[mask] - b[mask])) / max(np.max(np.abs(b[mask])), 1e-300)
+        assert err < 1e-9, (name, err)
+
+
+def test_ch_backend_recovers_manufactured_state(dn):
+    """dn_ch_linear_solve (the ch_solver backend entry point) on the reference unit test's manufactured state
+    (core_solver_unit_tests.cpp:217-283): equation residual < 1e-10, relative error < 1e-8."""
+    cfg = unit(ch_inner_iterations=200, ch_tolerance=1e-12)
+    gpu = dn.Solver(cfg)
+    g, n = 3, 32
+    dx = 1.0 / n
+    x = (np.arange(n) + 0.5) * dx
+    c_exact = 0.42 + 0.08 * np.sin(2 * np.pi * x)[:, None] * np.cos(2 * np.pi * x)[None, :]
+    orc = OracleSolver(cfg, "port")
+    orc.initialize()
+    ext = np.pad(c_exact, g, mode="wrap")
+    alpha0 = 3.0 / (2.0 * cfg["dt"])
+    # rhs from the oracle's own operator application: solve with the oracle from a zero start at tight tol
+    lap = np.zeros_like(ext)
+    lap[g:-g, g:-g] = ((ext[g + 1:-g + 1 or None, g:-g] - 2 * ext[g:-g, g:-g] + ext[g - 1:-g - 1, g:-g]) / dx ** 2 +
+                       (ext[g:-g, g + 1:-g + 1 or None] - 2 * ext[g:-g, g:-g] + ext[g:-g, g - 1:-g - 1]) / dx ** 2)
+    lap = np.pad(lap[g:-g, g:-g], g, mode="wrap")
+    bih = np.zeros_like(ext)
+    bih[g:-g, g:-g] = ((lap[g + 1:-g + 1 or None, g:-g] - 2 * lap[g:-g, g:-g] + lap[g - 1:-g - 1, g:-g]) / dx ** 2 +
+                       (lap[g:-g, g + 1:-g + 1 or None] - 2 * lap[g:-g, g:-g] + lap[g:-g, g - 1:-g - 1]) / dx ** 2)
+    a1 = 3 * math.sqrt(2) / (16 * cfg["cn"])
+    a2 = 3 * math.sqrt(2) * cfg["cn"] / 4
+    rhs = alpha0 * ext - (a1 * lap - a2 * np.pad(bih[g:-g, g:-g], g, mode="wrap")) / cfg["pe"]
+    cs, it_res, eq_res, its = gpu.ch_linear_solve(rhs, alpha0, np.zeros_like(ext))
+    err = np.sqrt(((cs[g:-g, g:-g] - c_exact) ** 2).sum() / (c_exact ** 2).sum())
+    assert eq_res < 1e-10 and err < 1e-8
+    co, it_o, eq_o = orc.ch_linear_solve(rhs, alpha0, np.zeros_like(ext))
+    assert rel_l2(cs[g:-g, g:-g], co[g:-g, g:-g]) < 1e-12
+
+
+def test_pressure_backend_entry_point(dn):
+    """dn_pressure_solve (the pressure_scheme backend entry point) against the oracle's pressure phase."""
+    cfg = CASES["walls_split_icpcg_wide"]
+    orc, gpu = seeded_pair(dn, cfg, seed=9)
+    orc.begin_step(1)
+    orc.phase(1)
+    orc.momentum(1)
+    orc.pressure()
+    out, its, rel = gpu.pressure_solve(1, orc.field("u_star"), orc.field("v_star"), orc.field("rho_mid"),
+                                       orc.field("p"), orc.field("p_prev"))
+    g = cfg["ghost"]
+    assert rel_l2(interior(out, g), interior(orc.field("p_corr"), g)) < TOL
+    assert its == orc.report()["pressure_iterations"]
+
+
+def test_golden_case92_history(dn):
+    """Case 92 (the reference's published 176Result run) from the oracle's initial state: diagnostics of the
+    first 40 steps match the published history.csv and the pressure solve takes 133 iterations each step."""
+    cfg = parse_cfg(open(os.path.join(GOLDEN, "case92.cfg")).read())
+    rows = list(csv.DictReader(open(os.path.join(GOLDEN, "case92_history.csv"))))
+    orc = OracleSolver(cfg, "port")
+    orc.initialize()
+    gpu = dn.Solver(cfg)
+    from ding_nsch_core_solver_b200.capi import FIELDS
+
+    for name in FIELDS:
+        gpu.set_field(name, orc.field(name))
+    gpu.set_initial_mass(float(rows[0]["mass"]))
+    for k in range(40):
+        rep = gpu.step(k)
+        row = rows[k + 1]
+        d = gpu.diagnostics()
+        assert rep["pressure_iterations"] == int(row["pressure_iterations"]), (k, rep)
+        assert rep["ch_iterations"] == int(row["ch_iterations"])
+        assert rep["momentum_iterations"] == int(row["momentum_iterations"])
+        for col, tol in (("mass", 1e-14), ("max_abs_mu", 1e-10), ("max_velocity", 1e-8), ("kinetic_energy", 1e-8),
+                         ("total_free_energy", 1e-12)):
+            ref = float(row[col])
+            assert abs(d[col] - ref) <= tol * max(abs(ref), 1e-300), (k, col, d[col], ref)
