@@ -14,7 +14,6 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdn_cuda.so")
 SOURCES = ["dn_capi.cu", "dn_config.cpp"]
-HEADERS = ["dn_common.cuh", "dn_fields.cuh", "dn_krylov.cuh", "dn_momentum.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
          "-Xcompiler", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include")]
@@ -24,8 +23,8 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "dn_cuda.h"),
-                                                                   os.path.abspath(__file__)]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "dn_cuda.h"),
+                                                                  os.path.abspath(__file__)]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

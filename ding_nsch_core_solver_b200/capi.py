@@ -117,6 +117,7 @@ def load():
         "dn_stream": (VP, [H]),
         "dn_last_phase_times": (I, [H, DP]),
         "dn_kernel_launches": (C.c_longlong, [H]),
+        "dn_profile_counters": (I, [H, DP, I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -285,9 +286,14 @@ class Solver:
 
     def phase_times_ms(self) -> list:
         """[ch, momentum, pressure, correction] phase ms, then [pressure PCG kernel, CH PCG kernel, BiCGSTAB kernel]
-        ms and the pressure PCG iteration count, all from the last step."""
-        out = (C.c_double * 8)()
+        ms, the pressure PCG iteration count, and the pressure PCG kernel's split [SpMV, update, sweeps] ms."""
+        out = (C.c_double * 11)()
         self._check(self._lib.dn_last_phase_times(self._h, out))
+        return list(out)
+
+    def profile_counters(self, count: int = 64) -> list:
+        out = (C.c_double * count)()
+        self._check(self._lib.dn_profile_counters(self._h, out, count))
         return list(out)
 
     def kernel_launches(self) -> int:

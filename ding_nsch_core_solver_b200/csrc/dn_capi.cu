@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -328,9 +329,16 @@ struct dn_handle {
   int *status = nullptr;
   double *partials = nullptr;
   double *scal = nullptr;       // device scalars
+  double *prof = nullptr;       // device profiling counters of the last pressure solve (64 doubles)
   double *host_scal = nullptr;  // pinned
   int max_coop_blocks = 0;
   int nsweep = 0;
+  // staged wavefront (non-periodic x): hand-over lines and launch shape
+  double *bnd_f = nullptr, *bnd_b = nullptr, *wline0 = nullptr, *zlast = nullptr;
+  int sw5 = 0;                 // sweep warps per CTA, 0 = staged path unavailable
+  int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3>
+  size_t sw5_warp_smem[2] = {0, 0};  // per sweep warp, [constant operator, variable operator]
+  int smem_optin = 0;
   double initial_mass = 0.0;
   long long launches = 0;
   std::string err;
@@ -340,9 +348,19 @@ struct dn_handle {
   double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ch, momentum, pressure, correction, pressure PCG kernel,
                                                  // CH PCG kernel, BiCGSTAB kernel, pressure PCG iterations
   int step = 0;  // step index of the step in progress (split extrapolation, operators.cpp:416)
+  double pcg_split_ms[3] = {0, 0, 0};  // pressure PCG, in-kernel: [P1 SpMV+barrier, P2 update+barrier, sweeps]
 };
 
 namespace {
+
+bool solve_ch(const dn_config &c) {
+  return c.mode != DN_MODE_ADVECTION_ONLY && !(c.mode == DN_MODE_SINGLE_PHASE || c.freeze_ch);
+}
+bool compute_mu(const dn_config &c) { return c.mode != DN_MODE_ADVECTION_ONLY && c.mode != DN_MODE_SINGLE_PHASE; }
+bool use_split(const dn_config &c) {
+  return c.pressure_scheme == DN_P_SPLIT_ICPCG || c.pressure_scheme == DN_P_SPLIT_ILDLT_PCG;
+}
+double rho_ref_of(const dn_config &c) { return std::min(1.0, c.density_ratio); }
 
 dn_status fail(dn_handle *h, dn_status s, const std::string &msg) {
   if (h) h->err = msg;
@@ -504,14 +522,56 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   P.partials = h->partials;
   P.out = h->scal + 8;
   P.nsweep = h->nsweep;
-  DN_TRY(reset_sync(h));
+  P.warp_smem = 0;
+  size_t dyn_smem = 0;
   int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(h->nsweep, (h->n + 2047) / 2048));
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
+  if (SWEEP == 3) {
+    const dn_config &c = h->cfg;
+    const bool var = !use_split(c);
+    Sweep5 &W = P.s5;
+    W.nx = h->G.nx;
+    W.ny = h->G.ny;
+    W.n = (int)h->n;
+    W.px = h->G.px;
+    W.py = h->G.py;
+    W.prec = prec;
+    W.varcoef = var ? 1 : 0;
+    W.aW = a;
+    W.aS = a + h->n;
+    W.aN = a + 3 * h->n;
+    W.aE = a + 4 * h->n;
+    W.cx = -(1.0 / (h->G.dx * h->G.dx));
+    W.cy = -(1.0 / (h->G.dy * h->G.dy));
+    W.dinv = dinv;
+    W.r = h->r;
+    W.y = h->y;
+    W.z = h->z;
+    W.bnd_f = h->bnd_f;
+    W.bnd_b = h->bnd_b;
+    W.wline0 = h->wline0;
+    W.zlast = h->zlast;
+    W.prog_f = h->prog;
+    W.prog_b = h->prog + kMaxBlocks * 8;
+    W.nsweep = h->nsweep;
+    W.sw = h->sw5;
+    W.status = h->status;
+    P.warp_smem = (int)h->sw5_warp_smem[var ? 1 : 0];
+    W.warp_smem = P.warp_smem;
+    W.prof = h->prof;
+    dyn_smem = 64 + (size_t)h->sw5 * P.warp_smem;
+    const int sweep_ctas = (h->nsweep + h->sw5 - 1) / h->sw5;
+    blocks = std::max(blocks, sweep_ctas);
+    blocks = std::min(blocks, h->sw5_blocks_max);
+    if (blocks < sweep_ctas) return fail(h, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
+  }
+  DN_TRY(reset_sync(h));
   if (SWEEP == 0 && (long long)blocks * (kBlock / 32) < h->nsweep)
     return fail(h, DN_ERR_UNSUPPORTED, "grid too wide for the co-resident wavefront warps");
   void *args[] = {&P};
   cudaEventRecord(h->kev[0], h->stream);
-  DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_pcg<S, SWEEP>, dim3(blocks), dim3(kBlock), args, 0, h->stream));
+  DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_pcg<S, SWEEP>, dim3(blocks), dim3(kBlock), args, dyn_smem,
+                                         h->stream));
   cudaEventRecord(h->kev[1], h->stream);
   h->launches++;
   int st = 0;
@@ -520,7 +580,15 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
   h->phase_ms[S == 5 ? 4 : 5] += ms;
-  return read_scalars(h, 4, out);
+  double tmp[7];
+  DN_TRY(read_scalars(h, 7, tmp));
+  for (int k = 0; k < 4; ++k) out[k] = tmp[k];
+  if (S == 5) {
+    h->pcg_split_ms[0] = tmp[4];
+    h->pcg_split_ms[1] = tmp[5];
+    h->pcg_split_ms[2] = tmp[6];
+  }
+  return DN_OK;
 }
 
 dn_status run_bicgstab(dn_handle *h, double out[4]) {
@@ -569,14 +637,6 @@ dn_status run_bicgstab(dn_handle *h, double out[4]) {
   return read_scalars(h, 4, out);
 }
 
-bool solve_ch(const dn_config &c) {
-  return c.mode != DN_MODE_ADVECTION_ONLY && !(c.mode == DN_MODE_SINGLE_PHASE || c.freeze_ch);
-}
-bool compute_mu(const dn_config &c) { return c.mode != DN_MODE_ADVECTION_ONLY && c.mode != DN_MODE_SINGLE_PHASE; }
-bool use_split(const dn_config &c) {
-  return c.pressure_scheme == DN_P_SPLIT_ICPCG || c.pressure_scheme == DN_P_SPLIT_ILDLT_PCG;
-}
-double rho_ref_of(const dn_config &c) { return std::min(1.0, c.density_ratio); }
 
 // ---------------------------------------------------------------------------------------------------
 // Step pieces
@@ -877,8 +937,13 @@ dn_status pressure(dn_handle *h, int step, dn_report *rep) {
   }
   DN_CUDA(h, cudaMemsetAsync(h->x, 0, h->n * sizeof(double), h->stream));
   double out[4];
-  DN_TRY((run_pcg<5, 0>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
-                        cfg.pressure_tolerance, out)));
+  if (h->sw5 > 0 && !h->G.px && h->nsweep >= 1) {
+    DN_TRY((run_pcg<5, 3>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
+                          cfg.pressure_tolerance, out)));
+  } else {
+    DN_TRY((run_pcg<5, 0>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
+                          cfg.pressure_tolerance, out)));
+  }
   rep->pressure_iterations = (int)out[0];
   rep->pressure_residual = out[2];
   h->phase_ms[7] = out[0];
@@ -1057,9 +1122,37 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   A(dalloc(h, &h->prog, 2 * (size_t)kMaxBlocks * 8));
   A(dalloc(h, &h->partials, 2 * (size_t)kMaxBlocks * 8));
   A(dalloc(h, &h->scal, 64));
+  A(dalloc(h, &h->prof, 64));
   if (s == DN_OK && cudaMallocHost(&h->host_scal, kHostScal * sizeof(double)) != cudaSuccess) s = DN_ERR_CUDA;
   if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
   h->nsweep = (nx + 31) / 32;
+  A(dalloc(h, &h->bnd_f, (size_t)h->nsweep * ny));
+  A(dalloc(h, &h->bnd_b, (size_t)h->nsweep * ny));
+  A(dalloc(h, &h->wline0, ny));
+  A(dalloc(h, &h->zlast, ny));
+  if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+  {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    h->smem_optin = optin;
+    auto round16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    h->sw5_warp_smem[0] = round16(sweep_warp_smem(2, ny));
+    h->sw5_warp_smem[1] = round16(sweep_warp_smem(4, ny));
+    const size_t per = h->sw5_warp_smem[use_split(c) ? 0 : 1];
+    const size_t budget = (size_t)optin > 64 + 2304 ? (size_t)optin - 64 - 2304 : 0;  // minus static smem
+    int sw = (int)std::min<size_t>(8, budget / per);
+    sw = std::min(sw, h->nsweep);
+    if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
+    h->sw5 = sw;
+    if (sw > 0) {
+      const size_t dyn = 64 + (size_t)sw * per;
+      cudaFuncSetAttribute(k_pcg<5, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+      int occ5 = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k_pcg<5, 3>, kBlock, dyn);
+      h->sw5_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * h->num_sms);
+      if (h->sw5_blocks_max == 0) h->sw5 = 0;
+    }
+  }
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg<5, 0>, kBlock, 0);
   int occ2 = 0;
@@ -1373,9 +1466,17 @@ void *dn_stream(dn_handle *h) { return h ? (void *)h->stream : nullptr; }
 dn_status dn_last_phase_times(dn_handle *h, double *out) {
   if (!h || !out) return DN_ERR_INVALID_ARGUMENT;
   for (int k = 0; k < 8; ++k) out[k] = h->phase_ms[k];
+  for (int k = 0; k < 3; ++k) out[8 + k] = h->pcg_split_ms[k];
   return DN_OK;
 }
 
 long long dn_kernel_launches(const dn_handle *h) { return h ? h->launches : 0; }
+
+dn_status dn_profile_counters(dn_handle *h, double *out, int count) {
+  if (!h || !out || count < 0 || count > 64) return DN_ERR_INVALID_ARGUMENT;
+  DN_CUDA(h, cudaMemcpyAsync(out, h->prof, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
 
 }  // extern "C"

@@ -31,6 +31,14 @@ enum DevStatus : int {
   kDevFactorFailed = 9,      // incomplete factorization hit the pivot floor
 };
 
+enum PrecKind { kPrecDiag = 0, kPrecLDLT = 1, kPrecICC = 2 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Bounded spin: ~2^22 polls with a short sleep, i.e. well under a few seconds, then give up.
 constexpr long long kSpinLimit = 1ll << 22;
 
@@ -119,11 +127,12 @@ struct GridBarrier {
       } else {
         long long spins = 0;
         while (*gen == my_gen) {
-          if (++spins > kSpinLimit || *status != kDevOk) {
+          ++spins;
+          if ((spins & 1023) == 0 && (spins > kSpinLimit || *status != kDevOk)) {
             atomicCAS((int *)status, kDevOk, kDevTimeout);
             break;
           }
-          __nanosleep(64);
+          if (spins > 64) __nanosleep(32);
         }
       }
       __threadfence();

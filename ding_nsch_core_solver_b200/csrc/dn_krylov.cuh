@@ -15,6 +15,7 @@
 #pragma once
 
 #include "dn_common.cuh"
+#include "dn_wavefront.cuh"
 
 namespace dn {
 
@@ -244,8 +245,6 @@ __global__ void k_diag_inverse(SpOp A, double *dinv) {
 // ---------------------------------------------------------------------------------------------------
 // Persistent PCG (solve_preconditioned_cg, ch_sparse_krylov.hpp:515-660)
 // ---------------------------------------------------------------------------------------------------
-enum PrecKind { kPrecDiag = 0, kPrecLDLT = 1, kPrecICC = 2 };
-
 struct PcgArgs {
   SpOp A;
   const double *l;     // factor slots [S][n]
@@ -264,6 +263,8 @@ struct PcgArgs {
   double *partials;
   double *out;  // [0] iterations [1] abs residual [2] rel residual [3] iterate residual
   int nsweep;   // sweep warps (ceil(nx/32)) for the 5-point wavefront
+  Sweep5 s5;    // staged wavefront (SWEEP 3)
+  int warp_smem;  // shared-memory bytes per sweep warp (SWEEP 3)
 };
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
@@ -284,11 +285,11 @@ __device__ __forceinline__ unsigned int wait_flag(const unsigned int *flag, unsi
     if (lane == 0) v = ld_acquire(flag);
     v = __shfl_sync(0xffffffffu, v, 0);
     if (v >= target) return v;
-    if (++spins > kSpinLimit || *(volatile int *)status != kDevOk) {
+    ++spins;
+    if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
       if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
       return 0;
     }
-    __nanosleep(20);
   }
 }
 
@@ -318,11 +319,7 @@ __device__ void fwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r) {
     }
     if (valid && j >= 0 && j < ny) {
       const size_t idx = (size_t)i * ny + j;
-      double rv = __ldcg(&P.r[idx]);
-      if (P.project) {
-        rv = rv - m_r;
-        P.r[idx] = rv;
-      }
+      const double rv = __ldcg(&P.r[idx]) - m_r;
       double sum = rv;
       if (P.A.px && i == nx - 1) sum -= __ldg(&lE[idx]) * __ldcg(&P.y[j]);
       if (i > 0) sum -= __ldg(&lW[idx]) * y_up;
@@ -347,7 +344,7 @@ __device__ void fwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r) {
 
 // Backward sweep for sweep warp k (lines nx-1-32k-t, marching j downward).  Accumulates sum z,
 // sum r.z and sum r into acc[0..2].  ICC: z = (y - sum L^T z) / d.  LDLT: z = y / D - sum L^T z.
-__device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double (&acc)[3]) {
+__device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
   const int nx = P.A.nx, ny = P.A.ny, n = P.A.n;
   const int i = nx - 1 - (32 * k + lane);
@@ -387,7 +384,7 @@ __device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double (&acc)[
       z_prev = zv;
       if (j == ny - 1) z_first = zv;
       z_step = zv;
-      const double rv = __ldcg(&P.r[idx]);
+      const double rv = __ldcg(&P.r[idx]) - m_r;
       acc[0] += zv;
       acc[1] += rv * zv;
       acc[2] += rv;
@@ -406,7 +403,7 @@ __device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double (&acc)[
 // Level-scheduled forward+backward application of a general slot factor by one CTA (13-point CH
 // operator; also handles periodic y, where the 13-point graph is a chain).  Accumulates like bwd5.
 template <int S>
-__device__ void apply_levels(const PcgArgs &P, double (&acc)[3]) {
+__device__ void apply_levels(const PcgArgs &P, double m_r, double (&acc)[3]) {
   const SpOp &A = P.A;
   const int n = A.n;
   const bool seq = (S == 13 && A.py);
@@ -423,7 +420,7 @@ __device__ void apply_levels(const PcgArgs &P, double (&acc)[3]) {
       int slots[S];
       long long cols[S];
       const int cnt = lower_slots<S>(A, i, j, slots, cols);
-      double sum = P.r[r];
+      double sum = P.r[r] - m_r;
       for (int p = 0; p < cnt; ++p) sum -= P.l[(size_t)slots[p] * n + r] * P.y[cols[p]];
       P.y[r] = (P.prec == kPrecICC) ? sum * P.dinv[r] : sum;
     }
@@ -461,7 +458,7 @@ __device__ void apply_levels(const PcgArgs &P, double (&acc)[3]) {
       for (int p = 0; p < cnt; ++p) sum -= P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
       const double zv = (P.prec == kPrecICC) ? sum * P.dinv[r] : sum;
       P.z[r] = zv;
-      const double rv = P.r[r];
+      const double rv = P.r[r] - m_r;
       acc[0] += zv;
       acc[1] += rv * zv;
       acc[2] += rv;
@@ -470,11 +467,15 @@ __device__ void apply_levels(const PcgArgs &P, double (&acc)[3]) {
   }
 }
 
-// One persistent launch runs the whole PCG.  SWEEP: 0 = 5-point pipelined wavefront, 1 = level-scheduled
-// slot factor (CTA 0), 2 = diagonal.
+// One persistent launch runs the whole PCG.  SWEEP: 0 = 5-point pipelined wavefront on global memory,
+// 1 = level-scheduled slot factor (CTA 0), 2 = diagonal, 3 = 5-point wavefront staged through shared memory.
+// The residual r is kept unprojected in memory; the mean of the latest update (m_r) is subtracted on the
+// fly by the preconditioner and folded in by the next update, which equals projecting r after every
+// update (pressure.cpp:225-239 applied in ch_sparse_krylov.hpp:602-605).
 template <int S, int SWEEP>
 __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   __shared__ double sh[8 * 32 + 8];
+  extern __shared__ __align__(16) char dsm[];
   const GridBarrier bar{P.bar_count, P.bar_gen, P.status, gridDim.x};
   int parity = 0;
   const SpOp &A = P.A;
@@ -484,8 +485,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   const long long lo = (long long)blockIdx.x * per, hi = min((long long)n, lo + per);
   const int warp = threadIdx.x >> 5;
   const int nwarps_cta = blockDim.x >> 5;
+  unsigned int *cnt_cta = (unsigned int *)dsm;
+  if (SWEEP == 3) {
+    if (threadIdx.x < 16) cnt_cta[threadIdx.x] = 0u;
+    __syncthreads();
+  }
 
-  // ---- r = b - A x0, project r, initial residual (ch_sparse_krylov.hpp:531-558)
+  // ---- r = b - A x0, initial residual (ch_sparse_krylov.hpp:531-558)
   double v3[3] = {0.0, 0.0, 0.0};
   for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
     const int i = (int)(r / ny), j = (int)(r % ny);
@@ -514,30 +520,42 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   }
 
   unsigned int epoch = 0;
+  // acc[0] = sum z, acc[1] = r.z (= r^T M^-1 r), acc[2] = sum of the projected r
   auto precondition = [&](double m_r_now, double (&acc)[3]) -> bool {
     acc[0] = acc[1] = acc[2] = 0.0;
     ++epoch;
     if (SWEEP == 0) {
-      // sweep warp k lives in CTA k % G, warp k / G
-      for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta) {
+      for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta)
         fwd5(P, k, epoch, m_r_now);
-      }
-      for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta) {
-        bwd5(P, k, epoch, acc);
+      for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta)
+        bwd5(P, k, epoch, m_r_now, acc);
+    } else if (SWEEP == 3) {
+      const int k = blockIdx.x * P.s5.sw + warp;
+      if (warp < P.s5.sw && k < P.nsweep) {
+        char *mine = dsm + 64 + (size_t)warp * P.warp_smem;
+        if (P.prec == kPrecICC) {
+          if (P.s5.varcoef) {
+            fwd5_staged<true, true>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<true, true>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+          } else {
+            fwd5_staged<true, false>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<true, false>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+          }
+        } else {
+          if (P.s5.varcoef) {
+            fwd5_staged<false, true>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<false, true>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+          } else {
+            fwd5_staged<false, false>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<false, false>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+          }
+        }
       }
     } else if (SWEEP == 1) {
-      if (P.project) {  // level-scheduled path: project r first (pointwise, own range)
-        for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) P.r[r] = P.r[r] - m_r_now;
-        if (!bar.sync()) return false;
-      }
-      if (blockIdx.x == 0) apply_levels<S>(P, acc);
+      if (blockIdx.x == 0) apply_levels<S>(P, m_r_now, acc);
     } else {
       for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
-        double rv = P.r[r];
-        if (P.project) {
-          rv = rv - m_r_now;
-          P.r[r] = rv;
-        }
+        const double rv = P.r[r] - m_r_now;
         const double zv = P.dinv[r] * rv;
         P.z[r] = zv;
         acc[0] += zv;
@@ -549,7 +567,9 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   };
 
   double acc[3];
+  unsigned long long t_p1 = 0, t_p2 = 0, t_pc = 0, t0 = global_ns();
   if (!precondition(m_r, acc)) return;
+  t_pc += global_ns() - t0;
   double m_z = P.project ? acc[0] / dn_ : 0.0;
   double rz_old = P.project ? acc[1] - m_z * acc[2] : acc[1];
   if (!isfinite(rz_old) || rz_old <= 0.0) {
@@ -563,6 +583,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   const int limit = P.max_it > 1 ? P.max_it : 1;
   for (int it = 0; it < limit; ++it) {
     // ---- P1: p = z - m_z + beta p_old ; Ap = A p  (p at neighbours formed on the fly)
+    t0 = global_ns();
     double v[3] = {0.0, 0.0, 0.0};
     for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
       const int i = (int)(r / ny), j = (int)(r % ny);
@@ -591,6 +612,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
       return;
     }
     const double alpha = rz_old / pap;
+    const unsigned long long t1 = global_ns();
+    t_p1 += t1 - t0;
     // ---- P2: x += alpha p ; r -= alpha Ap ; norms (ch_sparse_krylov.hpp:592-610)
     double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
@@ -599,7 +622,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
       const double delta = alpha * pp;
       const double xv = (P.x[r] - m_x) + delta;
       P.x[r] = xv;
-      const double rv = P.r[r] - alpha * P.ap[r];
+      const double rv = (P.r[r] - m_r) - alpha * P.ap[r];
       P.r[r] = rv;
       w[0] += delta * delta;
       w[1] += xv * xv;
@@ -608,6 +631,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
       w[4] += rv * rv;
     }
     if (!grid_sum<5>(w, P.partials, parity, sh, bar)) return;
+    const unsigned long long t2 = global_ns();
+    t_p2 += t2 - t1;
     m_x = P.project ? w[2] / dn_ : 0.0;
     m_r = P.project ? w[3] / dn_ : 0.0;
     rn2 = P.project ? fmax(w[4] - w[3] * w[3] / dn_, 0.0) : w[4];
@@ -618,6 +643,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
     if (relr < P.tol || absr < P.tol) break;
     // ---- z = M^{-1} r, project z, r.z (ch_sparse_krylov.hpp:626-635)
     if (!precondition(m_r, acc)) return;
+    t_pc += global_ns() - t2;
     m_z = P.project ? acc[0] / dn_ : 0.0;
     const double rz_new = P.project ? acc[1] - m_z * acc[2] : acc[1];
     if (!isfinite(rz_new) || rz_new <= 0.0) {
@@ -640,6 +666,9 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
     P.out[1] = absr;
     P.out[2] = relr;
     P.out[3] = iter_res;
+    P.out[4] = (double)t_p1 * 1e-6;
+    P.out[5] = (double)t_p2 * 1e-6;
+    P.out[6] = (double)t_pc * 1e-6;
   }
 }
 

@@ -173,8 +173,13 @@ dn_status dn_synchronize(dn_handle *h);
 void *dn_stream(dn_handle *h);
 /* Device-side times (CUDA events) of the last dn_step, milliseconds: [0] CH phase, [1] momentum phase,
  * [2] pressure phase, [3] correction phase, [4] pressure PCG kernel, [5] CH PCG kernel(s), [6] momentum
- * BiCGSTAB kernel, [7] pressure PCG iterations.  `out` holds 8 doubles. */
+ * BiCGSTAB kernel, [7] pressure PCG iterations, then the pressure PCG kernel's own split (device clock):
+ * [8] SpMV + dot phases, [9] update phases, [10] preconditioner sweeps.  `out` holds 11 doubles. */
 dn_status dn_last_phase_times(dn_handle *h, double *out);
+/* Device-clock profiling counters of the last pressure solve's wavefront (ns), 4 per sweep warp k:
+ * [4k] forward sweep, [4k+1] waits for the neighbouring warp, [4k+2] waits for staged inputs,
+ * [4k+3] backward sweep.  `count` <= 64. */
+dn_status dn_profile_counters(dn_handle *h, double *out, int count);
 /* Number of this library's kernels launched since the handle was created. */
 long long dn_kernel_launches(const dn_handle *h);
 
