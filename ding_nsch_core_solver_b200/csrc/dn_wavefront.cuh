@@ -21,9 +21,10 @@
 
 namespace dn {
 
-constexpr int kRing = 128;  // ring columns per staged array
-constexpr int kChunk = 32;  // columns per cp.async chunk
+constexpr int kRing = 64;   // ring columns per staged array
+constexpr int kChunk = 8;   // columns per cp.async chunk (= one hand-over group of steps)
 constexpr int kHand = 8;    // columns per boundary publication
+constexpr int kAhead = 3;   // chunks staged ahead of the one being consumed
 
 struct Sweep5 {
   int nx, ny, n, px, py;
@@ -74,6 +75,7 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_ahead() { asm volatile("cp.async.wait_group 3;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void st_global_if(double *p, double v, bool pred) {
@@ -99,22 +101,22 @@ __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, u
   }
 }
 
-// Stage columns [c0, c0+32) of 32 lines starting at line i0 of array `src` into ring slot columns.
+// Stage columns [c0, c0+kChunk) of 32 lines starting at line i0 of array `src` into ring slot columns.
 __device__ __forceinline__ void stage_chunk(double *ring, const double *src, int i0, int nlines, int ny, int c0,
                                            bool vec16) {
   const int lane = threadIdx.x & 31;
   if (c0 >= ny || c0 < 0) return;
   const int ncol = min(kChunk, ny - c0);
   if (vec16) {
-    // 32 lines x 16 pieces of 16 bytes; lanes 0-15 cover one line, 16-31 the next
-    for (int p = lane; p < 32 * (kChunk / 2); p += 32) {
-      const int line = p >> 4, pc = (p & 15) * 2;
+    constexpr int per_line = kChunk / 2;  // 16-byte pieces per line
+    for (int p = lane; p < 32 * per_line; p += 32) {
+      const int line = p / per_line, pc = (p % per_line) * 2;
       if (line < nlines && pc < ncol)
         cp_async16(&ring[line * kRing + ((c0 + pc) & (kRing - 1))], &src[(size_t)(i0 + line) * ny + c0 + pc]);
     }
   } else {
     for (int p = lane; p < 32 * kChunk; p += 32) {
-      const int line = p >> 5, pc = p & 31;
+      const int line = p / kChunk, pc = p % kChunk;
       if (line < nlines && pc < ncol)
         cp_async8(&ring[line * kRing + ((c0 + pc) & (kRing - 1))], &src[(size_t)(i0 + line) * ny + c0 + pc]);
     }
@@ -179,8 +181,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   };
   const unsigned long long t_begin = global_ns();
   unsigned long long t_wait = 0;
-  stage(0);
-  stage(1);
+  for (int c = 0; c < kAhead; ++c) stage(c);
   double w_prev = 0.0, w_first = 0.0, w_step = 0.0, bvals = 0.0;
   double rz = 0.0, rsum = 0.0;
   unsigned int avail = 0;
@@ -190,13 +191,11 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   const double *rows = ring_s + lane * kRing;
   double *ydst = yout + (size_t)i * ny;
   for (int q = 0; q < nchunk; ++q) {
-    stage(q + 2);
-    cp_async_wait2();
+    stage(q + kAhead);
+    cp_async_wait_ahead();
     __syncwarp();
-#pragma unroll 1
-    for (int g = 0; g < kChunk; g += kHand) {
-      const int s0 = q * kChunk + g;
-      if (s0 >= total) break;
+    {
+      const int s0 = q * kChunk;
       // hand-over values of line i0-1 for columns [s0, s0+kHand), held by lanes 0..kHand-1
       if (k > 0 && s0 < ny) {
         const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
@@ -372,7 +371,7 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
     } else {
       const int hi = ny - kChunk * c;
       for (int p = lane; p < 32 * kChunk; p += 32) {
-        const int line = p >> 5, pc = p & 31;
+        const int line = p / kChunk, pc = p % kChunk;
         if (line < nlines && pc < hi) {
           const size_t gi = (size_t)(i0 + line) * ny + pc;
           const int sidx = line * kRing + (pc & (kRing - 1));
@@ -389,8 +388,7 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
   };
   __syncwarp();  // y of these lines was written by this warp's forward sweep
   const unsigned long long t_begin = global_ns();
-  stage(0);
-  stage(1);
+  for (int c = 0; c < kAhead; ++c) stage(c);
   double z_prev = 0.0, z_first = 0.0, z_step = 0.0, bvals = 0.0, zsum = 0.0;
   unsigned int avail = 0;
   const double *rowy = ring_y + lane * kRing;
@@ -399,13 +397,11 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
   const double *rowe = ring_e + lane * kRing;
   double *zdst = zout + (size_t)i * ny;
   for (int q = 0; q < nchunk; ++q) {
-    stage(q + 2);
-    cp_async_wait2();
+    stage(q + kAhead);
+    cp_async_wait_ahead();
     __syncwarp();
-#pragma unroll 1
-    for (int g = 0; g < kChunk; g += kHand) {
-      const int s0 = q * kChunk + g;
-      if (s0 >= total) break;
+    {
+      const int s0 = q * kChunk;
       if (k + 1 < nsweep && s0 < ny) {
         const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
         if (avail + base < need) {
