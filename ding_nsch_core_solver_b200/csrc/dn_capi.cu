@@ -9,9 +9,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1476,6 +1478,413 @@ dn_status dn_profile_counters(dn_handle *h, double *out, int count) {
   if (!h || !out || count < 0 || count > 64) return DN_ERR_INVALID_ARGUMENT;
   DN_CUDA(h, cudaMemcpyAsync(out, h->prof, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------
+// Allocation-free pressure solve: dn_pressure_solve_static.
+//
+// Some callers cannot allocate device memory when they need a pressure solve: a host framework whose
+// caching pool has already reserved the GPU's memory, a real-time loop that may not stall on cudaMalloc
+// (which synchronises the device), or a caller that holds nothing but raw device pointers and no handle
+// lifetime.  This variant of the pressure PCG runs on the caller's device buffers and stream and keeps
+// every intermediate (operator, factor, Krylov vectors, hand-over lines, reduction partials, barrier
+// words) in one fixed file-scope device array, so it calls no allocator at all.  The array is part of the
+// library's device image: every GPU that loads the library holds DN_STATIC_SCRATCH_BYTES of it until the
+// process exits.  All calls share it, so calls that overlap in time on one device (two host threads, or
+// two streams) race on it; the caller serialises them.
+// ---------------------------------------------------------------------------------------------------
+static __device__ __align__(256) double g_pressure_scratch[DN_STATIC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+
+// Per device: the device address of g_pressure_scratch (the name is only a host-side stand-in) and the
+// launch limits of the PCG kernels, resolved once with that device current.
+struct StaticDevice {
+  bool ready;
+  char *base;
+  int num_sms;
+  int smem_optin;
+  int max_coop_blocks;
+  int pcg3_static_smem;
+};
+std::mutex g_static_mu;
+StaticDevice g_static_dev[kStaticMaxDevices];
+
+dn_status static_fail(char *err, size_t err_len, dn_status s, const char *fmt, ...) {
+  if (err && err_len) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, err_len, fmt, ap);
+    va_end(ap);
+  }
+  return s;
+}
+
+#define DN_SCUDA(call)                                                                                   \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) return static_fail(err, err_len, DN_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define DN_SLAUNCH(what)                                                                                 \
+  do {                                                                                                   \
+    cudaError_t e_ = cudaGetLastError();                                                                 \
+    if (e_ != cudaSuccess) return static_fail(err, err_len, DN_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e_)); \
+  } while (0)
+
+// Byte offsets of the sub-buffers inside the scratch array, each on a 256-byte boundary.
+struct StaticLayout {
+  size_t bar_count, bar_gen, status, prog, partials, scal, prof;
+  size_t b, x, r, z, y, p0, p1, ap, a5, l5, d5, dinv5, pe, bnd_f, bnd_b, wline0, zlast;
+  size_t total;
+};
+
+StaticLayout static_layout(int nx, int ny, int g) {
+  StaticLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return at;
+  };
+  const size_t n = (size_t)nx * ny, nsweep = (size_t)(nx + 31) / 32;
+  L.bar_count = take(sizeof(unsigned int));
+  L.bar_gen = take(sizeof(unsigned int));
+  L.status = take(sizeof(int));
+  L.prog = take(2 * (size_t)kMaxBlocks * 8 * sizeof(unsigned int));
+  L.partials = take(2 * (size_t)kMaxBlocks * 8 * sizeof(double));
+  L.scal = take(64 * sizeof(double));
+  L.prof = take(64 * sizeof(double));
+  for (size_t *v : {&L.b, &L.x, &L.r, &L.z, &L.y, &L.p0, &L.p1, &L.ap}) *v = take(n * sizeof(double));
+  L.a5 = take(5 * n * sizeof(double));
+  L.l5 = take(5 * n * sizeof(double));
+  L.d5 = take(n * sizeof(double));
+  L.dinv5 = take(n * sizeof(double));
+  L.pe = take((size_t)(nx + 2 * g) * (ny + 2 * g) * sizeof(double));
+  L.bnd_f = take(nsweep * ny * sizeof(double));
+  L.bnd_b = take(nsweep * ny * sizeof(double));
+  L.wline0 = take((size_t)ny * sizeof(double));
+  L.zlast = take((size_t)ny * sizeof(double));
+  L.total = off;
+  return L;
+}
+
+// Set-up of the current device (first call on it): resolve the array's device address and the launch
+// limits.  Occupancy queries and attribute calls allocate nothing.
+dn_status static_setup(int device, StaticDevice *out, char *err, size_t err_len) {
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  StaticDevice &d = g_static_dev[device];
+  if (!d.ready) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_pressure_scratch);
+    if (e != cudaSuccess)
+      return static_fail(err, err_len, DN_ERR_CUDA, "cudaGetSymbolAddress(g_pressure_scratch): %s",
+                         cudaGetErrorString(e));
+    StaticDevice t{};
+    t.base = static_cast<char *>(ptr);
+    DN_SCUDA(cudaDeviceGetAttribute(&t.num_sms, cudaDevAttrMultiProcessorCount, device));
+    DN_SCUDA(cudaDeviceGetAttribute(&t.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa{};
+    DN_SCUDA(cudaFuncGetAttributes(&fa, k_pcg<5, 3>));
+    t.pcg3_static_smem = (int)fa.sharedSizeBytes;
+    // the same co-residency bound as a handle's (all persistent kernels of the library)
+    int occ = 0, occ2 = 0, occ3 = 0;
+    DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg<5, 0>, kBlock, 0));
+    DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg<13, 1>, kBlock, 0));
+    DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_bicgstab, kBlock, 0));
+    occ = std::min(occ, std::min(occ2, occ3));
+    t.max_coop_blocks = std::min(kMaxBlocks, std::max(1, occ) * t.num_sms);
+    t.ready = true;
+    d = t;
+  }
+  *out = d;
+  return DN_OK;
+}
+
+dn_status static_device_status(int st, char *err, size_t err_len) {
+  switch (st) {
+  case kDevOk: return DN_OK;
+  case kDevTimeout:
+    return static_fail(err, err_len, DN_ERR_TIMEOUT, "device wait timed out (grid barrier or wavefront flag)");
+  case kDevPcgBreakdownRz0:
+    return static_fail(err, err_len, DN_ERR_PCG_BREAKDOWN, "pcg preconditioner breakdown: non-positive r^T M^{-1} r");
+  case kDevPcgBreakdownPap:
+    return static_fail(err, err_len, DN_ERR_PCG_BREAKDOWN, "pcg breakdown: p^T A p is invalid");
+  case kDevPcgBreakdownRz:
+    return static_fail(err, err_len, DN_ERR_PCG_BREAKDOWN,
+                       "pcg preconditioner breakdown: non-positive new r^T M^{-1} r");
+  default: return static_fail(err, err_len, DN_ERR_CUDA, "unknown device status %d", st);
+  }
+}
+
+dn_status static_read(void *host, const void *dev, size_t bytes, cudaStream_t st, char *err, size_t err_len) {
+  DN_SCUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st));
+  DN_SCUDA(cudaStreamSynchronize(st));
+  return DN_OK;
+}
+
+dn_status static_bc_pressure(const Fv &f, const Grid &G, const BCSet &B, cudaStream_t st, char *err,
+                             size_t err_len) {
+  const long long nghost = 2LL * f.g * f.ny + 2LL * f.g * (f.nx + 2 * f.g);
+  k_bc_ghosts<<<blocks_for(nghost), 256, 0, st>>>(f, G, kBCPressure, B.p[0], B.p[1], B.p[2], B.p[3]);
+  DN_SLAUNCH("k_bc_ghosts");
+  return DN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double *u_star, const double *v_star,
+                                   const double *rho_mid, const double *p, const double *p_prev, double *p_corr,
+                                   void *stream, int *iterations, double *relative_residual, char *err,
+                                   size_t err_len) {
+  if (err && err_len) err[0] = '\0';
+  if (!cfg || !u_star || !v_star || !rho_mid || !p || !p_prev || !p_corr)
+    return static_fail(err, err_len, DN_ERR_INVALID_ARGUMENT, "null pointer argument");
+  const dn_config &c = *cfg;
+  if (c.nx < 8 || c.ny < 8) return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "the CUDA backend needs nx, ny >= 8");
+  if (c.ghost < 3) return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "ghost must be >= 3 (WENO5 stencil)");
+  if (c.pressure_scheme == DN_P_JACOBI)
+    return static_fail(err, err_len, DN_ERR_UNSUPPORTED,
+                       "pressure_scheme jacobi is not implemented by the CUDA backend");
+  if (c.pressure_scheme < DN_P_ICPCG || c.pressure_scheme > DN_P_SPLIT_ILDLT_PCG)
+    return static_fail(err, err_len, DN_ERR_CONFIG, "unknown pressure_scheme %d", c.pressure_scheme);
+  if (c.precision != DN_PRECISION_FP64)
+    return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "precision mixed is not available in this build");
+  static const char *names[4] = {"left", "right", "bottom", "top"};
+  for (int s = 0; s < 4; ++s) {  // validate_boundary_configuration, operators.cpp:11-34 (pressure and velocity)
+    const int periodic = (s < 2) ? c.periodic_x : c.periodic_y;
+    if (periodic && (c.p_bc[s].type != DN_BC_UNSET || c.u_bc[s].type != DN_BC_UNSET || c.v_bc[s].type != DN_BC_UNSET))
+      return static_fail(err, err_len, DN_ERR_CONFIG, "boundary conditions on side %s cannot be set when the direction is periodic",
+                         names[s]);
+  }
+  if ((long long)c.nx * c.ny > (1LL << 30)) return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "grid too large");
+  const StaticLayout L = static_layout(c.nx, c.ny, c.ghost);
+  if (L.total > (size_t)DN_STATIC_SCRATCH_BYTES)
+    return static_fail(err, err_len, DN_ERR_UNSUPPORTED,
+                       "grid %d x %d needs %zu bytes of scratch; the static scratch array holds %zu bytes", c.nx,
+                       c.ny, L.total, (size_t)DN_STATIC_SCRATCH_BYTES);
+
+  int device = 0;
+  DN_SCUDA(cudaGetDevice(&device));
+  if (device < 0 || device >= kStaticMaxDevices)
+    return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "device ordinal %d beyond the set-up table", device);
+  StaticDevice D{};
+  {
+    const dn_status s = static_setup(device, &D, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  // grid and effective pressure BCs (operators.cpp:36-112), as a handle derives them
+  Grid G;
+  G.nx = c.nx;
+  G.ny = c.ny;
+  G.g = c.ghost;
+  G.px = c.periodic_x;
+  G.py = c.periodic_y;
+  G.dx = c.lx / std::max((double)c.nx, 1.0);
+  G.dy = c.ly / std::max((double)c.ny, 1.0);
+  BCSet B{};
+  for (int s = 0; s < 4; ++s)
+    B.p[s] = c.p_bc[s].type != DN_BC_UNSET ? BCSide{c.p_bc[s].type, c.p_bc[s].value} : BCSide{DN_BC_NEUMANN, 0.0};
+  const bool has_dirichlet = (!c.periodic_x && (B.p[0].type == DN_BC_DIRICHLET || B.p[1].type == DN_BC_DIRICHLET)) ||
+                             (!c.periodic_y && (B.p[2].type == DN_BC_DIRICHLET || B.p[3].type == DN_BC_DIRICHLET));
+  const bool split = c.pressure_scheme == DN_P_SPLIT_ICPCG || c.pressure_scheme == DN_P_SPLIT_ILDLT_PCG;
+  const bool icc = c.pressure_scheme == DN_P_ICPCG || c.pressure_scheme == DN_P_SPLIT_ICPCG;
+  const int kind = icc ? kPrecICC : kPrecLDLT;
+  const double rho_ref = split ? std::min(1.0, c.density_ratio) : 1.0;
+  const int nx = c.nx, ny = c.ny, g = c.ghost;
+  const long long n = (long long)nx * ny;
+  const int nsweep = (nx + 31) / 32;
+
+  // caller's fields (read only, except p_corr) and the scratch sub-buffers
+  Fv f_us{const_cast<double *>(u_star), nx + 1, ny, g};
+  Fv f_vs{const_cast<double *>(v_star), nx, ny + 1, g};
+  Fv f_rm{const_cast<double *>(rho_mid), nx, ny, g};
+  Fv f_p{const_cast<double *>(p), nx, ny, g};
+  Fv f_pp{const_cast<double *>(p_prev), nx, ny, g};
+  Fv f_pc{p_corr, nx, ny, g};
+  char *base = D.base;
+  auto dptr = [&](size_t off) { return reinterpret_cast<double *>(base + off); };
+  auto uptr = [&](size_t off) { return reinterpret_cast<unsigned int *>(base + off); };
+  Fv f_pe{dptr(L.pe), nx, ny, g};
+  double *b = dptr(L.b), *x = dptr(L.x), *a5 = dptr(L.a5), *partials = dptr(L.partials), *scal = dptr(L.scal);
+  int *status = reinterpret_cast<int *>(base + L.status);
+
+  // Every call starts from a cleared array: barrier words, status, progress counters, the iterate x and
+  // the hand-over lines all have to begin at zero, and clearing the whole used prefix costs a few us.
+  DN_SCUDA(cudaMemsetAsync(base, 0, L.total, st));
+
+  // solve_pressure_correction_{icpcg,ildlt_pcg,liu_split_icpcg,liu_split_ildlt_pcg}, pressure.cpp:302-365
+  k_fill<<<blocks_for((long long)f_pc.size()), 256, 0, st>>>(f_pc.d, 0.0, (long long)f_pc.size());
+  DN_SLAUNCH("k_fill");
+  {
+    const dn_status s = static_bc_pressure(f_pc, G, B, st, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  if (split) {  // extrapolated pressure p~ = 2p - p_prev (p at step 0), operators.cpp:416
+    k_p_ext<<<blocks_for(n), 256, 0, st>>>(f_p, f_pp, f_pe, step == 0 ? 1 : 0);
+    DN_SLAUNCH("k_p_ext");
+    const dn_status s = static_bc_pressure(f_pe, G, B, st, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  k_p_assemble<<<blocks_for(n), 256, 0, st>>>(G, B, f_rm, f_us, f_vs, f_pe, split ? 1 : 0, rho_ref, c.dt, a5, b);
+  DN_SLAUNCH("k_p_assemble");
+  if (!has_dirichlet) {  // regularize_pressure_linear_system, pressure.cpp:198-212
+    const int nb = 128;
+    k_vec_sum<<<nb, 256, 0, st>>>(b, n, partials);
+    DN_SLAUNCH("k_vec_sum");
+    k_finish_mean<<<1, 32, 0, st>>>(partials, nb, (double)n, scal);
+    DN_SLAUNCH("k_finish_mean");
+    k_vec_sub_scalar<<<blocks_for(n), 256, 0, st>>>(b, n, scal);
+    DN_SLAUNCH("k_vec_sub_scalar");
+  }
+  const SpOp A{a5, (int)n, nx, ny, G.px, G.py};
+  k_factor<5><<<1, 1024, 0, st>>>(A, Factor{dptr(L.l5), dptr(L.d5), dptr(L.dinv5), 0.0}, kind, status);
+  DN_SLAUNCH("k_factor<5>");
+  int dev_st = 0;
+  {
+    const dn_status s = static_read(&dev_st, status, sizeof(int), st, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  if (dev_st == kDevFactorFailed)
+    return static_fail(err, err_len, icc ? DN_ERR_ICC_FAILED : DN_ERR_ILDLT_FAILED,
+                       icc ? "ICC preconditioner construction failed" : "ILDLT preconditioner construction failed");
+  if (dev_st != kDevOk) return static_device_status(dev_st, err, err_len);
+
+  // the persistent PCG kernel, launched with the shape a handle would use for this grid
+  PcgArgs P;
+  P.A = A;
+  P.l = dptr(L.l5);
+  P.dinv = dptr(L.dinv5);
+  P.prec = kind;
+  P.b = b;
+  P.x = x;
+  P.r = dptr(L.r);
+  P.z = dptr(L.z);
+  P.y = dptr(L.y);
+  P.p0 = dptr(L.p0);
+  P.p1 = dptr(L.p1);
+  P.ap = dptr(L.ap);
+  P.project = has_dirichlet ? 0 : 1;
+  P.max_it = c.poisson_iterations;
+  P.tol = c.pressure_tolerance;
+  P.bar_count = uptr(L.bar_count);
+  P.bar_gen = uptr(L.bar_gen);
+  P.status = status;
+  P.prog_f = uptr(L.prog);
+  P.prog_b = uptr(L.prog) + kMaxBlocks * 8;
+  P.partials = partials;
+  P.out = scal + 8;
+  P.nsweep = nsweep;
+  P.warp_smem = 0;
+  int blocks = (int)std::min<long long>(D.num_sms, std::max<long long>(nsweep, (n + 2047) / 2048));
+  blocks = std::max(1, std::min(blocks, D.max_coop_blocks));
+  // staged wavefront: sweep warps per CTA from the shared-memory budget, as dn_create chooses them
+  int sw = 0, sw_blocks_max = 0;
+  size_t warp_smem = 0;
+  if (!G.px) {
+    const size_t per = (sweep_warp_smem(split ? 2 : 4, ny) + 15) & ~(size_t)15;
+    const size_t budget = (size_t)D.smem_optin > 64 + 2304 ? (size_t)D.smem_optin - 64 - 2304 : 0;
+    sw = (int)std::min<size_t>(8, budget / per);
+    sw = std::min(sw, nsweep);
+    if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
+    if (sw > 0) {
+      const size_t dyn = 64 + (size_t)sw * per;
+      if (dyn + (size_t)D.pcg3_static_smem > (size_t)D.smem_optin) {
+        sw = 0;
+      } else {
+        // raise the kernel's dynamic shared-memory limit to the device maximum: never below what any
+        // handle on this device launches it with
+        DN_SCUDA(cudaFuncSetAttribute(k_pcg<5, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      D.smem_optin - D.pcg3_static_smem));
+        int occ5 = 0;
+        DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k_pcg<5, 3>, kBlock, dyn));
+        sw_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * D.num_sms);
+        if (sw_blocks_max == 0) sw = 0;
+        warp_smem = per;
+      }
+    }
+  }
+  void *args[] = {&P};
+  if (sw > 0) {
+    Sweep5 &W = P.s5;
+    W.nx = nx;
+    W.ny = ny;
+    W.n = (int)n;
+    W.px = G.px;
+    W.py = G.py;
+    W.prec = kind;
+    W.varcoef = split ? 0 : 1;
+    W.aW = a5;
+    W.aS = a5 + n;
+    W.aN = a5 + 3 * n;
+    W.aE = a5 + 4 * n;
+    W.cx = -(1.0 / (G.dx * G.dx));
+    W.cy = -(1.0 / (G.dy * G.dy));
+    W.dinv = P.dinv;
+    W.r = P.r;
+    W.y = P.y;
+    W.z = P.z;
+    W.bnd_f = dptr(L.bnd_f);
+    W.bnd_b = dptr(L.bnd_b);
+    W.wline0 = dptr(L.wline0);
+    W.zlast = dptr(L.zlast);
+    W.prog_f = P.prog_f;
+    W.prog_b = P.prog_b;
+    W.nsweep = nsweep;
+    W.sw = sw;
+    W.status = status;
+    P.warp_smem = (int)warp_smem;
+    W.warp_smem = P.warp_smem;
+    W.prof = dptr(L.prof);
+    const int sweep_ctas = (nsweep + sw - 1) / sw;
+    blocks = std::max(blocks, sweep_ctas);
+    blocks = std::min(blocks, sw_blocks_max);
+    if (blocks < sweep_ctas)
+      return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
+    DN_SCUDA(cudaLaunchCooperativeKernel((const void *)k_pcg<5, 3>, dim3(blocks), dim3(kBlock), args,
+                                         64 + (size_t)sw * warp_smem, st));
+  } else {
+    if ((long long)blocks * (kBlock / 32) < nsweep)
+      return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "grid too wide for the co-resident wavefront warps");
+    DN_SCUDA(cudaLaunchCooperativeKernel((const void *)k_pcg<5, 0>, dim3(blocks), dim3(kBlock), args, 0, st));
+  }
+  {
+    const dn_status s = static_read(&dev_st, status, sizeof(int), st, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  if (dev_st != kDevOk) return static_device_status(dev_st, err, err_len);
+  double out[4];
+  {
+    const dn_status s = static_read(out, scal + 8, sizeof(out), st, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  k_scatter_compact<<<blocks_for(n), 256, 0, st>>>(x, f_pc);
+  DN_SLAUNCH("k_scatter_compact");
+  if (!has_dirichlet) {  // remove the mean of the correction (pressure.cpp:317, 338, 361)
+    const int nb = 128;
+    k_field_sum<<<nb, 256, 0, st>>>(f_pc, 1.0, partials);
+    DN_SLAUNCH("k_field_sum");
+    k_finish_mean<<<1, 32, 0, st>>>(partials, nb, (double)n, scal);
+    DN_SLAUNCH("k_finish_mean");
+    k_add_scalar_interior<<<blocks_for(n), 256, 0, st>>>(f_pc, scal);
+    DN_SLAUNCH("k_add_scalar_interior");
+  }
+  {
+    const dn_status s = static_bc_pressure(f_pc, G, B, st, err, err_len);
+    if (s != DN_OK) return s;
+  }
+  DN_SCUDA(cudaStreamSynchronize(st));
+  if (iterations) *iterations = (int)out[0];
+  if (relative_residual) *relative_residual = out[2];
   return DN_OK;
 }
 

@@ -160,6 +160,24 @@ dn_status dn_pressure_solve(dn_handle *h, int step, const double *u_star, const 
                             const double *rho_mid, const double *p, const double *p_prev, double *p_corr,
                             int *iterations, double *relative_residual);
 
+/* Size of the fixed device array that dn_pressure_solve_static works in (16 MiB; the grid's operator,
+ * factor, Krylov vectors and sync words need about 165 bytes per cell, so up to about 100,000 cells). */
+#define DN_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)
+/* No counterpart in the reference.  The pressure solve of dn_pressure_solve for callers that cannot
+ * allocate device memory at the point of the solve (a caching pool that already holds the GPU's memory,
+ * a loop that must not stall on cudaMalloc, code holding only raw device pointers and no handle).  No
+ * handle and no allocation: inputs u_star, v_star, rho_mid, p, p_prev and the output p_corr are the
+ * caller's DEVICE buffers in Field2D layout for `cfg`'s grid; the work runs on `stream` (a cudaStream_t,
+ * NULL for the default stream), which is synchronised before return.  Scratch lives in one static device
+ * array of DN_STATIC_SCRATCH_BYTES that every GPU loading the library holds until exit; grids that need
+ * more return DN_ERR_UNSUPPORTED.  The first call on a device (with that device current) resolves the
+ * array's address; make it before any stream capture.  All calls share the array, so calls overlapping
+ * in time on one device race.  On error a message goes to `err` (`err_len` bytes, may be NULL). */
+dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double *u_star, const double *v_star,
+                                   const double *rho_mid, const double *p, const double *p_prev, double *p_corr,
+                                   void *stream, int *iterations, double *relative_residual, char *err,
+                                   size_t err_len);
+
 /* ---- diagnostics ------------------------------------------------------------------------------------ */
 /* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
 dn_status dn_diagnostics(dn_handle *h, dn_diag *out);
