@@ -1,17 +1,17 @@
 """Throughput of the CHNS time step on B200 (Mcell-steps/s), with roofline, CPU baseline and end-to-end legs.
 
-Workload: the rising bubble of BASELINE config 2 on its 192x384 grid -- no-slip top/bottom, free-slip sides,
-density and viscosity ratio 10, split_icpcg pressure (rho_ref = min density), WENO5 phase advection, seeded
-interface modes 2-8 -- run in the reference's R0-unit parameterisation (testcase 26: lx=4, ly=8, R=1,
-Re=12.374, Ca=0.0202, Cn=0.04, Pe=150, g=1, dt=5e-5).  The literal unit-square mapping of config 2
-diverges on the reference itself after ~30 steps, so a bounded trajectory on the same grid is timed.
-Inputs are synthetic (seeded numpy), FP64 ("plain" form).
+Workload: the 192x384 rising bubble -- no-slip top/bottom, free-slip sides, density and viscosity ratio 10,
+split_icpcg pressure (rho_ref = min density), WENO5 phase advection, seeded interface modes 2-8 -- run in the
+reference's R0-unit parameterisation (testcase 26: lx=4, ly=8, R=1, Re=12.374, Ca=0.0202, Cn=0.04, Pe=150,
+g=1, dt=5e-5).  The unit-square mapping of this bubble (lx=1, ly=2, R=0.25) diverges on the reference itself
+after ~30 steps, so a bounded trajectory on the same grid is timed.  Inputs are synthetic (seeded numpy),
+FP64 ("plain" form).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One JSON line on stdout (rank 0).  For N > 1 the driver launches one process per GPU (torchrun); every rank
-advances its own replica (the 2D step does not shard without changing the preconditioner), value is the
-aggregate over ranks, timed as the max over ranks.
+One JSON line on stdout (rank 0).  Under torchrun (N > 1) every rank advances its own replica (the 2D step
+does not shard without changing the preconditioner); value is the aggregate over ranks, timed as the max
+over ranks.
 """
 import argparse
 import json
@@ -68,6 +68,21 @@ def initial_state(cfg: dict, seed: int = 2) -> dict:
     for n in ("c", "c_prev", "c_prev2"):
         state[n] = cell.copy()
     return state
+
+
+PCG_PROFILE = os.path.join(ROOT, "profiles", "k_pcg_5_3_pressure_192x384.txt")
+
+
+def pcg_traffic_per_launch():
+    """DRAM bytes (read + write) of one pressure-PCG launch from the committed ncu summary, per iteration,
+    or None when no summary is present."""
+    try:
+        for line in open(PCG_PROFILE):
+            if line.startswith("dram_bytes_per_iteration:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def hbm_peak():
@@ -249,11 +264,20 @@ def run_ours(args):
     peak, peak_kind = hbm_peak()
     bytes_per_launch = PCG_BYTES_PER_CELL_IT * n_cells * statistics.mean(pcg_its)
     achieved = bytes_per_launch / (statistics.mean(pcg_ms) * 1e-3) / 1e9
+    per_it = pcg_traffic_per_launch()
     roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
-                "kernel": "k_pcg<5,0> (pressure ICC-PCG, persistent, one launch per solve)",
+                "frac": round(achieved / peak, 5),
+                "traffic": None if per_it is None else round(per_it * statistics.mean(pcg_its)),
+                "peak_source": peak_kind,
+                "kernel": "k_pcg<5,3> (pressure ICC-PCG, persistent, staged wavefront, one launch per solve)",
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "kernel_ms_mean": statistics.mean(pcg_ms)}
+    # The sweeps are a dependency chain of nx + ny - 1 steps each way per iteration: time per dependent step
+    # against the shuffle + FMA chain latency (61 cycles, about 31 ns at 1965 MHz, measured on B200).
+    dep_steps = 2 * (cfg["nx"] + cfg["ny"] - 1) * statistics.mean(pcg_its)
+    sweep_ms = statistics.mean(p[10] for p in phases)
+    critical_path = {"dependent_sweep_steps_per_launch": round(dep_steps), "sweep_ms_per_launch": round(sweep_ms, 3),
+                     "ns_per_dependent_step": round(sweep_ms * 1e6 / dep_steps, 1), "chain_floor_ns": 31.0}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -282,6 +306,7 @@ def run_ours(args):
                 ("ch", "momentum", "pressure", "correction", "pressure_pcg_kernel", "ch_pcg_kernel",
                  "bicgstab_kernel"))},
             "roofline": roofline,
+            "critical_path": critical_path,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": h2d},

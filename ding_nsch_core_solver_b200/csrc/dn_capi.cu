@@ -1148,7 +1148,12 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     h->sw5 = sw;
     if (sw > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
-      cudaFuncSetAttribute(k_pcg<5, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+      // The limit is a property of the kernel on this device, shared by every handle: set it to the device
+      // maximum, so that a later handle with a smaller grid never lowers it below an earlier handle's need.
+      cudaFuncAttributes fa{};
+      cudaFuncGetAttributes(&fa, k_pcg<5, 3>);
+      cudaFuncSetAttribute(k_pcg<5, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           std::max((int)dyn, optin - (int)fa.sharedSizeBytes));
       int occ5 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k_pcg<5, 3>, kBlock, dyn);
       h->sw5_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * h->num_sms);

@@ -118,6 +118,22 @@ def test_step_parity(dn, name):
         assert math.isclose(rep["pressure_residual"], ro["pressure_residual"], rel_tol=1e-3, abs_tol=1e-14)
 
 
+def test_handles_keep_independent_launch_limits(dn):
+    """A handle created after a larger one, whose wavefront needs less shared memory, leaves the larger one
+    runnable: the kernel's dynamic shared-memory limit is one per-device setting that all handles share."""
+    big = unit(nx=96, ny=200, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
+               body_force_y=-0.98, dt=1e-4)
+    orc, gpu = seeded_pair(dn, big, seed=21)
+    small = dn.Solver(CASES["walls_split_icpcg_wide"])
+    try:
+        orc.step(0)
+        rep = gpu.step(0)
+        assert_fields_close(orc, gpu, COMPARE, "larger handle after a smaller one")
+        assert rep["pressure_iterations"] == orc.report()["pressure_iterations"]
+    finally:
+        small.close()
+
+
 def test_phase_by_phase_parity(dn):
     """Every phase entry point on its own (the per-backend boundary)."""
     cfg = CASES["walls_split_ildlt"]
