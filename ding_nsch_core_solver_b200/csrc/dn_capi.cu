@@ -334,7 +334,8 @@ struct dn_handle {
   double *prof = nullptr;       // device profiling counters of the last pressure solve (64 doubles)
   double *host_scal = nullptr;  // pinned
   int max_coop_blocks = 0;
-  int nsweep = 0;
+  int nsweep = 0;   // 32-line sweep warps of the global-memory wavefront (periodic x)
+  int nsweep5 = 0;  // 31-line sweep warps of the staged wavefront
   // staged wavefront (non-periodic x): hand-over lines and launch shape
   double *bnd_f = nullptr, *bnd_b = nullptr, *wline0 = nullptr, *zlast = nullptr;
   int sw5 = 0;                 // sweep warps per CTA, 0 = staged path unavailable
@@ -555,14 +556,14 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
     W.zlast = h->zlast;
     W.prog_f = h->prog;
     W.prog_b = h->prog + kMaxBlocks * 8;
-    W.nsweep = h->nsweep;
+    W.nsweep = h->nsweep5;
     W.sw = h->sw5;
     W.status = h->status;
     P.warp_smem = (int)h->sw5_warp_smem[var ? 1 : 0];
     W.warp_smem = P.warp_smem;
     W.prof = h->prof;
     dyn_smem = 64 + (size_t)h->sw5 * P.warp_smem;
-    const int sweep_ctas = (h->nsweep + h->sw5 - 1) / h->sw5;
+    const int sweep_ctas = (h->nsweep5 + h->sw5 - 1) / h->sw5;
     blocks = std::max(blocks, sweep_ctas);
     blocks = std::min(blocks, h->sw5_blocks_max);
     if (blocks < sweep_ctas) return fail(h, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
@@ -1128,8 +1129,9 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   if (s == DN_OK && cudaMallocHost(&h->host_scal, kHostScal * sizeof(double)) != cudaSuccess) s = DN_ERR_CUDA;
   if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
   h->nsweep = (nx + 31) / 32;
-  A(dalloc(h, &h->bnd_f, (size_t)h->nsweep * ny));
-  A(dalloc(h, &h->bnd_b, (size_t)h->nsweep * ny));
+  h->nsweep5 = staged_sweep_warps(nx);
+  A(dalloc(h, &h->bnd_f, 2 * (size_t)std::max(h->nsweep, h->nsweep5) * ny));
+  A(dalloc(h, &h->bnd_b, 2 * (size_t)std::max(h->nsweep, h->nsweep5) * ny));
   A(dalloc(h, &h->wline0, ny));
   A(dalloc(h, &h->zlast, ny));
   if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
@@ -1143,7 +1145,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     const size_t per = h->sw5_warp_smem[use_split(c) ? 0 : 1];
     const size_t budget = (size_t)optin > 64 + 2304 ? (size_t)optin - 64 - 2304 : 0;  // minus static smem
     int sw = (int)std::min<size_t>(8, budget / per);
-    sw = std::min(sw, h->nsweep);
+    sw = std::min(sw, h->nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
     h->sw5 = sw;
     if (sw > 0) {
@@ -1557,7 +1559,8 @@ StaticLayout static_layout(int nx, int ny, int g) {
     off += (bytes + 255) & ~(size_t)255;
     return at;
   };
-  const size_t n = (size_t)nx * ny, nsweep = (size_t)(nx + 31) / 32;
+  const size_t n = (size_t)nx * ny;
+  const size_t nsweep = std::max((size_t)(nx + 31) / 32, (size_t)staged_sweep_warps(nx));
   L.bar_count = take(sizeof(unsigned int));
   L.bar_gen = take(sizeof(unsigned int));
   L.status = take(sizeof(int));
@@ -1571,8 +1574,8 @@ StaticLayout static_layout(int nx, int ny, int g) {
   L.d5 = take(n * sizeof(double));
   L.dinv5 = take(n * sizeof(double));
   L.pe = take((size_t)(nx + 2 * g) * (ny + 2 * g) * sizeof(double));
-  L.bnd_f = take(nsweep * ny * sizeof(double));
-  L.bnd_b = take(nsweep * ny * sizeof(double));
+  L.bnd_f = take(2 * nsweep * ny * sizeof(double));
+  L.bnd_b = take(2 * nsweep * ny * sizeof(double));
   L.wline0 = take((size_t)ny * sizeof(double));
   L.zlast = take((size_t)ny * sizeof(double));
   L.total = off;
@@ -1708,6 +1711,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   const int nx = c.nx, ny = c.ny, g = c.ghost;
   const long long n = (long long)nx * ny;
   const int nsweep = (nx + 31) / 32;
+  const int nsweep5 = staged_sweep_warps(nx);
 
   // caller's fields (read only, except p_corr) and the scratch sub-buffers
   Fv f_us{const_cast<double *>(u_star), nx + 1, ny, g};
@@ -1799,7 +1803,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
     const size_t per = (sweep_warp_smem(split ? 2 : 4, ny) + 15) & ~(size_t)15;
     const size_t budget = (size_t)D.smem_optin > 64 + 2304 ? (size_t)D.smem_optin - 64 - 2304 : 0;
     sw = (int)std::min<size_t>(8, budget / per);
-    sw = std::min(sw, nsweep);
+    sw = std::min(sw, nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
     if (sw > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
@@ -1844,13 +1848,13 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
     W.zlast = dptr(L.zlast);
     W.prog_f = P.prog_f;
     W.prog_b = P.prog_b;
-    W.nsweep = nsweep;
+    W.nsweep = nsweep5;
     W.sw = sw;
     W.status = status;
     P.warp_smem = (int)warp_smem;
     W.warp_smem = P.warp_smem;
     W.prof = dptr(L.prof);
-    const int sweep_ctas = (nsweep + sw - 1) / sw;
+    const int sweep_ctas = (nsweep5 + sw - 1) / sw;
     blocks = std::max(blocks, sweep_ctas);
     blocks = std::min(blocks, sw_blocks_max);
     if (blocks < sweep_ctas)

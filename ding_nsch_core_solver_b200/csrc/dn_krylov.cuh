@@ -488,6 +488,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   unsigned int *cnt_cta = (unsigned int *)dsm;
   if (SWEEP == 3) {
     if (threadIdx.x < 16) cnt_cta[threadIdx.x] = 0u;
+    // cross-CTA hand-over lines start empty; the first grid reduction orders this before any sweep
+    const size_t nb = 2 * (size_t)P.s5.nsweep * P.s5.ny;
+    const double empty = __longlong_as_double((long long)kHandEmpty);
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
+      P.s5.bnd_f[t] = empty;
+      P.s5.bnd_b[t] = empty;
+    }
     __syncthreads();
   }
 
@@ -531,7 +538,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
         bwd5(P, k, epoch, m_r_now, acc);
     } else if (SWEEP == 3) {
       const int k = blockIdx.x * P.s5.sw + warp;
-      if (warp < P.s5.sw && k < P.nsweep) {
+      if (warp < P.s5.sw && k < P.s5.nsweep) {
         char *mine = dsm + 64 + (size_t)warp * P.warp_smem;
         if (P.prec == kPrecICC) {
           if (P.s5.varcoef) {

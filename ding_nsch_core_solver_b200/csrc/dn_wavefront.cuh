@@ -8,23 +8,29 @@
 // w_c = Dinv_c y_c, z_r = Dinv_r (y_r - sum a_rc z_c).  The subtraction order per row follows the reference's
 // CSR column order (wrap, W, wrap, S forward; N, wrap, E, wrap backward).
 //
-// Mapping.  Sweep warp k owns x-lines i = 32k + t (t = lane) for both sweeps and marches along j; lane t runs
-// t steps behind lane t-1 (forward) or one step behind lane t+1 (backward), so the neighbour line's value of
-// the previous step arrives by one warp shuffle.  Inputs are staged into shared memory by cp.async in
-// 32-column chunks, two chunks ahead, into a 128-column ring (lane t reads column j at ring slot j & 127:
-// row pitch 128 doubles keeps the skewed reads conflict-free).  Neighbouring warps hand over their edge
-// line through shared memory (same CTA) or through global memory with release/acquire progress flags
-// (different CTAs), published every 8 columns.  Every wait is bounded and reports kDevTimeout.
+// Mapping.  Sweep warp k owns the kLines = 31 x-lines i = 31k .. 31k+30 and marches along j.  The 32nd lane
+// is a ghost that replays the neighbouring warp's edge line (line 31k-1 in the forward sweep, 31k+31 in the
+// backward sweep) from a shared-memory hand-over line through the same arithmetic with zero coefficients
+// and unit dinv, so every lane receives its neighbour's value of the previous step by one plain warp
+// shuffle and a step has no lane-dependent selects.  Lanes that own no line read a zero row and carry 0.
+// Inputs are staged by cp.async in 8-column chunks, three chunks ahead, into per-lane ring rows of 64
+// columns plus an 8-column mirror (row pitch 72 doubles: skewed reads stay bank-conflict free), so that
+// the 8 steps of a group read at fixed offsets from one base pointer.  Neighbouring warps hand over their
+// edge line through shared memory (same CTA) or global memory (different CTAs) with release/acquire
+// progress counters, published every 8 columns.  Every wait is bounded and reports kDevTimeout.
 #pragma once
 
 #include "dn_common.cuh"
 
 namespace dn {
 
-constexpr int kRing = 64;   // ring columns per staged array
-constexpr int kChunk = 8;   // columns per cp.async chunk (= one hand-over group of steps)
-constexpr int kHand = 8;    // columns per boundary publication
-constexpr int kAhead = 3;   // chunks staged ahead of the one being consumed
+constexpr int kRing = 64;                // ring columns per staged array
+constexpr int kMirror = 8;               // mirrored columns so an 8-step group never wraps
+constexpr int kPitch = kRing + kMirror;  // doubles per ring row
+constexpr int kChunk = 8;                // columns per cp.async chunk (= one hand-over group of steps)
+constexpr int kHand = 8;                 // columns per boundary publication
+constexpr int kAhead = 3;                // chunks staged ahead of the one being consumed
+constexpr int kLines = 31;               // grid lines per sweep warp (lane 31 / lane 0 is the ghost)
 
 struct Sweep5 {
   int nx, ny, n, px, py;
@@ -35,18 +41,22 @@ struct Sweep5 {
   const double *dinv;
   const double *r;  // forward input (the pending mean m_r is subtracted on the fly)
   double *y, *z;
-  double *bnd_f, *bnd_b;      // [nsweep][ny] edge lines handed between CTAs
-  double *wline0, *zlast;     // periodic-x wrap lines: w of line 0 (forward), z of line nx-1 (backward)
-  unsigned int *prog_f, *prog_b;  // [nsweep] progress, monotonic across applications
-  int nsweep, sw;             // sweep warps in total / per CTA
+  double *bnd_f, *bnd_b;      // [2][nsweep][ny] edge lines handed between CTAs (by application parity)
+  double *wline0, *zlast;     // periodic-x wrap lines (unused by the staged path, which needs px = 0)
+  unsigned int *prog_f, *prog_b;  // unused by the staged path (kept for the launch arguments' layout)
+  int nsweep, sw;             // sweep warps in total (ceil(nx / kLines)) / per CTA
   int warp_smem;              // bytes between consecutive sweep warps' shared-memory regions
   int *status;
-  double *prof;               // per sweep warp, 4 counters (ns): forward total, hand-over waits, staging waits, backward total
+  double *prof;               // per sweep warp, 4 counters (ns): forward total, hand-over waits, 0, backward total
 };
 
-// per-warp shared-memory footprint (bytes) for `na` staged arrays and a ny-long hand-over line
+__host__ __device__ inline int staged_sweep_warps(int nx) { return (nx + kLines - 1) / kLines; }
+
+// per-warp shared-memory footprint (bytes) for `na` staged arrays, a ny-long hand-over line and the
+// zero / unit rows read by lanes that own no line
 __host__ __device__ inline size_t sweep_warp_smem(int na, int ny) {
-  return (size_t)na * 32 * kRing * sizeof(double) + (size_t)((ny + 1) & ~1) * sizeof(double) + 64;
+  return (size_t)na * 32 * kPitch * sizeof(double) + (size_t)((ny + 1) & ~1) * sizeof(double) +
+         2 * (size_t)kPitch * sizeof(double) + 64;
 }
 
 __device__ __forceinline__ unsigned int ld_acquire_cta(const unsigned int *p) {
@@ -74,13 +84,21 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_ahead() { asm volatile("cp.async.wait_group 3;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-__device__ __forceinline__ void st_global_if(double *p, double v, bool pred) {
-  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.global.f64 [%0], %1;\n\t}" ::"l"(p), "d"(v),
-               "r"((int)pred));
+// Cross-CTA hand-over.  The edge line goes through global memory without flags or fences: each launch
+// fills the line buffers with a NaN sentinel, the producer stores its values, and the consumer polls the
+// values themselves (relaxed GPU-scope loads) and writes the sentinel back after use.  Buffers alternate
+// by application parity, so a reset lands two applications (and several grid barriers) before reuse.
+constexpr unsigned long long kHandEmpty = 0x7ff4dead5eed0001ull;
+__device__ __forceinline__ double ld_relaxed_gpu(const double *p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool hand_empty(double v) {
+  return (unsigned long long)__double_as_longlong(v) == kHandEmpty;
 }
 
 // Bounded warp-uniform wait for a progress counter (shared or global) to reach `target`.
@@ -94,6 +112,9 @@ __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, u
     v = __shfl_sync(0xffffffffu, v, 0);
     if (v >= target) return v;
     ++spins;
+    // a warp that waits long (a backward sweep waiting for the whole chain above it) sleeps between
+    // polls, so that it takes no issue slots from a sweep warp sharing its scheduler
+    if (spins > 32) __nanosleep(64);
     if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
       if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
       return 0;
@@ -101,40 +122,90 @@ __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, u
   }
 }
 
-// Stage columns [c0, c0+kChunk) of 32 lines starting at line i0 of array `src` into ring slot columns.
-__device__ __forceinline__ void stage_chunk(double *ring, const double *src, int i0, int nlines, int ny, int c0,
-                                           bool vec16) {
+// Stage columns [c0, c1) of `nl` grid lines starting at line i0 into ring rows row0 .. row0+nl-1.  Column j
+// goes to row offset off + (j & 63); the mirrored columns are written twice (forward: slots 0..7 again at
+// 64..71, off = 0; backward: slots 56..63 again at 0..7, off = 8).  16-byte pieces when ny is even.
+template <bool FWD>
+__device__ __forceinline__ void stage_cols(double *ring, const double *src, int i0, int row0, int nl, int ny, int c0,
+                                           int c1, bool vec16) {
   const int lane = threadIdx.x & 31;
-  if (c0 >= ny || c0 < 0) return;
-  const int ncol = min(kChunk, ny - c0);
-  if (vec16) {
-    constexpr int per_line = kChunk / 2;  // 16-byte pieces per line
-    for (int p = lane; p < 32 * per_line; p += 32) {
-      const int line = p / per_line, pc = (p % per_line) * 2;
-      if (line < nlines && pc < ncol)
-        cp_async16(&ring[line * kRing + ((c0 + pc) & (kRing - 1))], &src[(size_t)(i0 + line) * ny + c0 + pc]);
+  c0 = max(c0, 0);
+  c1 = min(c1, ny);
+  if (c0 >= c1) return;
+  constexpr int off = FWD ? 0 : kMirror;
+  if (vec16) {  // ny even: c0 and c1 are even too
+    const int npair = (c1 - c0) >> 1;
+    for (int p = lane; p < nl * npair; p += 32) {
+      const int line = p / npair, j = c0 + 2 * (p - line * npair);
+      const double *g = &src[(size_t)(i0 + line) * ny + j];
+      double *row = ring + (size_t)(row0 + line) * kPitch;
+      const int slot = j & (kRing - 1);
+      cp_async16(&row[off + slot], g);
+      if (FWD ? (slot < kMirror) : (slot >= kRing - kMirror)) cp_async16(&row[FWD ? kRing + slot : slot - (kRing - kMirror)], g);
     }
   } else {
-    for (int p = lane; p < 32 * kChunk; p += 32) {
-      const int line = p / kChunk, pc = p % kChunk;
-      if (line < nlines && pc < ncol)
-        cp_async8(&ring[line * kRing + ((c0 + pc) & (kRing - 1))], &src[(size_t)(i0 + line) * ny + c0 + pc]);
+    const int ncol = c1 - c0;
+    for (int p = lane; p < nl * ncol; p += 32) {
+      const int line = p / ncol, j = c0 + (p - line * ncol);
+      const double *g = &src[(size_t)(i0 + line) * ny + j];
+      double *row = ring + (size_t)(row0 + line) * kPitch;
+      const int slot = j & (kRing - 1);
+      cp_async8(&row[off + slot], g);
+      if (FWD ? (slot < kMirror) : (slot >= kRing - kMirror)) cp_async8(&row[FWD ? kRing + slot : slot - (kRing - kMirror)], g);
     }
   }
 }
 
-// Forward sweep of sweep warp k (warp slot `ws` inside its CTA).  Accumulates rz (= y^T y for ICC,
-// y^T D^-1 y for ILDLT) and the sum of the projected residual into acc[1], acc[2].  Steps run in groups
-// of kHand: the hand-over check precedes a group, the publication follows it; within a group every
-// lane computes unconditionally (ring slots are always in range) and only stores / carries are
-// predicated, so the per-step dependency chain is one shuffle and one FMA.
+// Stage one whole 8-column chunk [c0, c0+8) (ny even; for the backward ring also ny % 8 == 0, so that
+// the chunk sits at an 8-aligned ring slot): lane t copies columns c0 + 2 (t & 3) + {0, 1} of lines
+// (t >> 2) + 8 it, it = 0..3, with one 16-byte cp.async per array -- no division, addresses from one
+// per-lane offset.  The chunk at the mirrored slot is copied a second time (forward: slot 0 again at 64,
+// backward: slot 56 again at 0).
+template <bool FWD, int NA>
+__device__ __forceinline__ void stage_full(double *r0, double *r1, double *r2, double *r3, const double *s0,
+                                           const double *s1, const double *s2, const double *s3, int i0, int row0,
+                                           int nl, int ny, int c0) {
+  const int lane = threadIdx.x & 31;
+  const int l0 = lane >> 2, cc = 2 * (lane & 3);
+  const int slot = c0 & (kRing - 1);
+  constexpr int off = FWD ? 0 : kMirror;
+  const bool mirror = FWD ? (slot == 0) : (slot == kRing - kChunk);
+  constexpr int mdelta = FWD ? kRing : -kRing;
+  const size_t gofs = (size_t)(i0 + l0) * ny + c0 + cc;
+  const int sofs = (row0 + l0) * kPitch + off + slot + cc;
+#pragma unroll
+  for (int it = 0; it < 4; ++it) {
+    if (l0 + 8 * it < nl) {
+      const size_t g = gofs + (size_t)(8 * it) * ny;
+      const int sd = sofs + 8 * it * kPitch;
+      cp_async16(r0 + sd, s0 + g);
+      cp_async16(r1 + sd, s1 + g);
+      if (NA == 4) {
+        cp_async16(r2 + sd, s2 + g);
+        cp_async16(r3 + sd, s3 + g);
+      }
+      if (mirror) {
+        cp_async16(r0 + sd + mdelta, s0 + g);
+        cp_async16(r1 + sd + mdelta, s1 + g);
+        if (NA == 4) {
+          cp_async16(r2 + sd + mdelta, s2 + g);
+          cp_async16(r3 + sd + mdelta, s3 + g);
+        }
+      }
+    }
+  }
+}
+
+// Forward sweep of sweep warp k (warp slot `ws` inside its CTA).  Lane 0 is the ghost of line 31k-1, lanes
+// 1..nl own lines 31k .. 31k+nl-1; lane t runs t steps behind the ghost.  Accumulates rz (= y^T y for
+// ICC, y^T D^-1 y for ILDLT) and the sum of the projected residual into acc[1], acc[2].  Steps run in
+// groups of kHand: the hand-over check precedes a group, the publication follows it.
 template <bool ICC, bool VAR>
 __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
                                             unsigned int epoch, double m_r, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
   const int nx = P.nx, ny = P.ny, nsweep = P.nsweep, sw = P.sw;
-  const int px = P.px, py = P.py;
-  constexpr bool varcoef = VAR, icc = ICC;
+  const int py = P.py;
   const double cx = P.cx, cy = P.cy;
   double *const yout = P.y;
   const double *const gr = P.r;
@@ -142,167 +213,216 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   const double *const gW = P.aW;
   const double *const gS = P.aS;
   const double *const gN = P.aN;
-  const double *const gE = P.aE;
   double *const bnd_f = P.bnd_f;
-  double *const wline0 = P.wline0;
-  unsigned int *const prog_f = P.prog_f;
   int *const status = P.status;
   double *const prof = P.prof;
-  const int i0 = 32 * k;
-  const int nlines = min(32, nx - i0);
-  const int i = i0 + lane;
-  const bool valid = lane < nlines;
-  const int na = varcoef ? 4 : 2;
+  const int i0 = kLines * k;
+  const int nl = min(kLines, nx - i0);
+  const bool real = lane >= 1 && lane <= nl;
+  const bool has_prod = k > 0;
+  const bool lin = (lane == 0) && has_prod;  // the ghost replays the hand-over line
+  const int i = i0 + lane - 1;
+  constexpr int na = VAR ? 4 : 2;
   double *ring_r = (double *)smem_warp;
-  double *ring_d = ring_r + 32 * kRing;
-  double *ring_w = ring_d + 32 * kRing;
-  double *ring_s = ring_w + 32 * kRing;
-  double *bline = ring_r + (size_t)na * 32 * kRing;
+  double *ring_d = ring_r + 32 * kPitch;
+  double *ring_w = ring_d + 32 * kPitch;
+  double *ring_s = ring_w + 32 * kPitch;
+  double *bline = ring_r + (size_t)na * 32 * kPitch;
+  double *zrow = bline + ((ny + 1) & ~1);
+  double *ones = zrow + kPitch;
   const bool vec16 = (ny % 2) == 0;
-  const bool prod_local = (k > 0) && (ws > 0);
-  const bool cons_local = (k + 1 < nsweep) && (ws + 1 < sw);
-  const bool last_warp = (k + 1 >= nsweep);
+  const bool prod_local = has_prod && (ws > 0);
+  const bool has_cons = (k + 1 < nsweep);
+  const bool cons_local = has_cons && (ws + 1 < sw);
   const unsigned int base = epoch * (unsigned int)(ny + 1);
-  const int total = ny + nlines - 1;
+  const int total = ny + nl;
   const int nchunk = (total + kChunk - 1) / kChunk;
-  double *next_bline = cons_local ? (double *)(smem_warp + P.warp_smem) + (size_t)na * 32 * kRing : nullptr;
   unsigned int *my_cnt = &cnt_cta[2 * ws];
   unsigned int *next_cnt = &cnt_cta[2 * (ws + 1)];
-  const double aw_const = (valid && i > 0) ? cx : 0.0;  // W coefficient of the constant operator
+  // per-lane rows: real lanes their ring rows, the ghost unit dinv, everything else zeros
+  const double *r_row = real ? ring_r + lane * kPitch : zrow;
+  const double *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
+  const double *w_row = real ? ring_w + lane * kPitch : zrow;
+  const double *s_row = real ? ring_s + lane * kPitch : zrow;
+  const double m_lane = real ? m_r : 0.0;
+  const double as_c = real ? cy : 0.0;
+  const double aw_c = (real && i > 0) ? cx : 0.0;
+  double *const ydst = yout + (size_t)(real ? i : 0) * ny;
+  const bool hand = has_cons && lane == 31;  // a warp with a consumer has nl = 31
+  double *const hdst = cons_local ? (double *)(smem_warp + P.warp_smem) + (size_t)na * 32 * kPitch
+                                  : bnd_f + ((size_t)(epoch & 1u) * nsweep + k) * ny;
   auto stage = [&](int c) {
     const int c0 = c * kChunk;
-    stage_chunk(ring_r, gr, i0, nlines, ny, c0, vec16);
-    stage_chunk(ring_d, gd, i0, nlines, ny, c0, vec16);
-    if (varcoef) {
-      stage_chunk(ring_w, gW, i0, nlines, ny, c0, vec16);
-      stage_chunk(ring_s, gS, i0, nlines, ny, c0, vec16);
+    if (c0 < ny) {
+      if (vec16 && c0 + kChunk <= ny) {
+        stage_full<true, na>(ring_r, ring_d, ring_w, ring_s, gr, gd, gW, gS, i0, 1, nl, ny, c0);
+      } else {
+        stage_cols<true>(ring_r, gr, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+        stage_cols<true>(ring_d, gd, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+        if (VAR) {
+          stage_cols<true>(ring_w, gW, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+          stage_cols<true>(ring_s, gS, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+        }
+      }
     }
     cp_async_commit();
   };
   const unsigned long long t_begin = global_ns();
   unsigned long long t_wait = 0;
-  for (int c = 0; c < kAhead; ++c) stage(c);
-  double w_prev = 0.0, w_first = 0.0, w_step = 0.0, bvals = 0.0;
-  double rz = 0.0, rsum = 0.0;
+  for (int t = lane; t < kPitch; t += 32) {
+    zrow[t] = 0.0;
+    ones[t] = 1.0;
+  }
+  // A producer in another CTA hands its line over through global memory: the values of group c are loaded
+  // kAhead groups early (issued at the start of a group, landed in the shared line at its end).
+  const bool remote = has_prod && !prod_local;
   unsigned int avail = 0;
-  const double *rowr = ring_r + lane * kRing;
-  const double *rowd = ring_d + lane * kRing;
-  const double *roww = ring_w + lane * kRing;
-  const double *rows = ring_s + lane * kRing;
-  double *ydst = yout + (size_t)i * ny;
+  double *const hin = has_prod ? bnd_f + ((size_t)(epoch & 1u) * nsweep + (k - 1)) * ny : nullptr;
+  auto hand_issue = [&](int c) -> double {
+    const int col = c * kChunk + lane;
+    return (lane < kHand && col < ny) ? ld_relaxed_gpu(hin + col) : 0.0;
+  };
+  auto hand_land = [&](int c, double v) -> bool {
+    const int col = c * kChunk + lane;
+    const bool mine = lane < kHand && col < ny;
+    bool miss = mine && hand_empty(v);
+    if (__any_sync(0xffffffffu, miss)) {
+      const unsigned long long tw0 = global_ns();
+      long long spins = 0;
+      while (__any_sync(0xffffffffu, miss)) {
+        ++spins;
+        if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+          if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
+          return false;
+        }
+        if (spins > 32) __nanosleep(64);
+        if (miss) {
+          v = ld_relaxed_gpu(hin + col);
+          miss = hand_empty(v);
+        }
+      }
+      t_wait += global_ns() - tw0;
+    }
+    if (mine) {
+      bline[col] = v;
+      hin[col] = __longlong_as_double((long long)kHandEmpty);
+    }
+    __syncwarp();
+    return true;
+  };
+  for (int c = 0; c < kAhead; ++c) {
+    if (remote && !hand_land(c, hand_issue(c))) {
+      cp_async_wait0();
+      return;
+    }
+    stage(c);
+  }
+  double w_prev = 0.0, w_first = 0.0, rz = 0.0, rsum = 0.0;
   for (int q = 0; q < nchunk; ++q) {
     stage(q + kAhead);
+    const double hv = remote ? hand_issue(q + kAhead) : 0.0;
     cp_async_wait_ahead();
     __syncwarp();
-    {
-      const int s0 = q * kChunk;
-      // hand-over values of line i0-1 for columns [s0, s0+kHand), held by lanes 0..kHand-1
-      if (k > 0 && s0 < ny) {
-        const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
-        if (avail + base < need) {
-          const unsigned long long tw0 = global_ns();
-          const unsigned int v = prod_local ? wait_progress<true>(my_cnt, need, status)
-                                            : wait_progress<false>(&prog_f[k - 1], need, status);
-          t_wait += global_ns() - tw0;
-          if (v == 0) return;
-          avail = v - base;
+    const int s0 = q * kChunk;
+    if (prod_local && s0 < ny) {  // hand-over values of line i0-1 for columns [s0, s0+kHand), same CTA
+      const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
+      if (avail + base < need) {
+        const unsigned long long tw0 = global_ns();
+        const unsigned int v = wait_progress<true>(my_cnt, need, status);
+        t_wait += global_ns() - tw0;
+        if (v == 0) {
+          cp_async_wait0();
+          return;
         }
-        const int col = s0 + lane;
-        if (lane < kHand && col < ny) bvals = prod_local ? bline[col] : __ldcg(&bnd_f[(size_t)(k - 1) * ny + col]);
+        avail = v - base;
       }
-      // steady state: every lane of the group is inside [0, ny) -- no range checks, no wraps
-      if (s0 >= 32 && s0 + kHand < ny && s0 + kHand <= total && !(px && i0 + 31 >= nx - 1 && i0 <= nx - 1)) {
-        const bool hand = (lane == 31) && !last_warp;
-#pragma unroll
-        for (int ss = 0; ss < kHand; ++ss) {
-          const int j = s0 + ss - lane;
-          const int slot = j & (kRing - 1);
-          const double rv = rowr[slot] - m_r;
-          const double dv = rowd[slot];
-          const double as = varcoef ? rows[slot] : cy;
-          const double aw = varcoef ? ((i > 0) ? roww[slot] : 0.0) : aw_const;
-          const double t1 = fma(-as, w_prev, rv);
-          double w_up = __shfl_up_sync(0xffffffffu, w_step, 1);
-          if (k > 0) {
-            const double b = __shfl_sync(0xffffffffu, bvals, ss);
-            if (lane == 0) w_up = b;
-          }
-          const double sum = fma(-aw, w_up, t1);
-          const double yv = icc ? sum * dv : sum;
-          const double wv = sum * (icc ? dv * dv : dv);
-          st_global_if(&ydst[j], yv, valid);
-          rz = fma(yv, icc ? yv : wv, rz);
-          rsum += rv;
-          if (cons_local) {
-            if (hand) next_bline[j] = wv;
-          } else {
-            st_global_if(&bnd_f[(size_t)k * ny + j], wv, hand);
-          }
-          w_prev = valid ? wv : 0.0;
-          w_step = valid ? wv : 0.0;
-        }
-        if (!valid) {
-          rz = 0.0;
-          rsum = 0.0;
-        }
-      } else {
+      __syncwarp();
+    }
+    if (s0 >= 32 && s0 + kHand < ny) {
+      // steady state: every lane's column lies in [1, ny-2]; fixed offsets from one base per array
+      const int j0 = s0 - lane;
+      const int slot = j0 & (kRing - 1);
+      const double *rb = lin ? bline + j0 : r_row + slot;
+      const double *db = d_row + slot;
+      const double *wb = w_row + slot;
+      const double *sb = s_row + slot;
+      double *yp = ydst + j0;
+      double *hp = hdst + j0;
+      double rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
-        const int s = s0 + ss;
-        const int j = s - lane;
-        const bool act = valid && j >= 0 && j < ny && s < total;
-        const int slot = j & (kRing - 1);
-        const double rv = rowr[slot] - m_r;
-        const double dv = rowd[slot];
-        const double as = (j > 0) ? (varcoef ? rows[slot] : cy) : 0.0;
-        const double aw = varcoef ? ((valid && i > 0) ? roww[slot] : 0.0) : aw_const;
-        // own-line terms first (periodic-x wrap, periodic-y wrap, S), so that only one FMA follows the
-        // shuffle that brings w of line i-1
-        double t1 = rv;
-        if (px && i == nx - 1 && act) t1 -= (varcoef ? gE[(size_t)i * ny + j] : cx) * __ldcg(&wline0[j]);
-        if (py && j == ny - 1 && valid) t1 = fma(-(varcoef ? gN[(size_t)i * ny + j] : cy), w_first, t1);
-        t1 = fma(-as, w_prev, t1);
-        double w_up = __shfl_up_sync(0xffffffffu, w_step, 1);
-        if (k > 0) {
-          const double b = __shfl_sync(0xffffffffu, bvals, ss);
-          if (lane == 0) w_up = b;
-        }
+        rvv[ss] = rb[ss];
+        dvv[ss] = db[ss];
+        asv[ss] = VAR ? sb[ss] : as_c;
+        awv[ss] = VAR ? wb[ss] : aw_c;
+      }
+#pragma unroll
+      for (int ss = 0; ss < kHand; ++ss) {
+        const double rv = rvv[ss] - m_lane;
+        const double dv = dvv[ss];
+        const double as = asv[ss];
+        const double aw = awv[ss];
+        const double t1 = fma(-as, w_prev, rv);
+        const double w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
         const double sum = fma(-aw, w_up, t1);
-        const double yv = icc ? sum * dv : sum;
-        const double wv = sum * (icc ? dv * dv : dv);
+        const double yv = ICC ? sum * dv : sum;
+        const double wv = sum * (ICC ? dv * dv : dv);
+        if (real) yp[ss] = yv;
+        rz = fma(yv, ICC ? yv : wv, rz);
+        rsum += rv;
+        if (hand) hp[ss] = wv;
+        w_prev = wv;
+      }
+    } else {
+#pragma unroll
+      for (int ss = 0; ss < kHand; ++ss) {
+        const int j = s0 + ss - lane;
+        const bool inr = j >= 0 && j < ny;
+        const bool act = inr && (real || lin);
+        const int slot = j & (kRing - 1);
+        const double rv = (lin ? (inr ? bline[j] : 0.0) : r_row[slot]) - m_lane;
+        const double dv = d_row[slot];
+        const double as = (j > 0) ? (VAR ? s_row[slot] : as_c) : 0.0;
+        const double aw = VAR ? w_row[slot] : aw_c;
+        // own-line terms first (periodic-y wrap, S), so that one FMA follows the shuffle from line i-1
+        double t1 = rv;
+        if (py && j == ny - 1 && real) t1 = fma(-(VAR ? gN[(size_t)i * ny + j] : cy), w_first, t1);
+        t1 = fma(-as, w_prev, t1);
+        const double w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
+        const double sum = fma(-aw, w_up, t1);
+        const double yv = ICC ? sum * dv : sum;
+        const double wv = sum * (ICC ? dv * dv : dv);
         if (act) {
-          ydst[j] = yv;
-          rz = fma(yv, icc ? yv : wv, rz);
-          rsum += rv;
-          if (px && i == 0) wline0[j] = wv;
-          if (lane == 31 && !last_warp) {
-            if (cons_local)
-              next_bline[j] = wv;
-            else
-              bnd_f[(size_t)k * ny + j] = wv;
+          if (real) {
+            ydst[j] = yv;
+            rz = fma(yv, ICC ? yv : wv, rz);
+            rsum += rv;
           }
+          if (hand) hdst[j] = wv;
           if (j == 0) w_first = wv;
           w_prev = wv;
-          w_step = wv;
-        }
-      }
-      }
-      // publish columns finished by lane 31 (the hand-over line)
-      const int done = min(ny, s0 + kHand - 31);
-      if (!last_warp && done > 0) {
-        __syncwarp();
-        if (lane == 31) {
-          if (cons_local)
-            st_release_cta(next_cnt, base + (unsigned int)done);
-          else
-            st_release_gpu(&prog_f[k], base + (unsigned int)done);
         }
       }
     }
+    // publish the columns lane 31 (skew 31) has finished to a consumer in this CTA (a consumer in another
+    // CTA polls the values themselves)
+    const int done = min(ny, s0 + kHand - 31);
+    if (cons_local && done > 0) {
+      __syncwarp();
+      if (lane == 31) st_release_cta(next_cnt, base + (unsigned int)done);
+    }
     __syncwarp();
+    if (remote && !hand_land(q + kAhead, hv)) {
+      cp_async_wait0();
+      return;
+    }
   }
   cp_async_wait0();
   __syncwarp();
+  if (!real) {
+    rz = 0.0;
+    rsum = 0.0;
+  }
   acc[1] += rz;
   acc[2] += rsum;
   if (prof && lane == 0 && k < 16) {
@@ -312,15 +432,15 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   }
 }
 
-// Backward sweep of sweep warp k.  The lead lane is the last valid one (line i0+nlines-1); lane t runs
-// (nlines-1-t) steps behind it.  Accumulates the sum of z into acc[0].
+// Backward sweep of sweep warp k.  Lanes 0..nl-1 own lines 31k .. 31k+nl-1; lane 31 is the ghost of line
+// 31k+31 when a next warp exists.  The lead lane (the ghost, or the last real lane of the last warp) runs
+// first, lane t (lead-t) steps behind it.  Accumulates the sum of z into acc[0].
 template <bool ICC, bool VAR>
 __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
                                             unsigned int epoch, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
   const int nx = P.nx, ny = P.ny, nsweep = P.nsweep, sw = P.sw;
-  const int px = P.px, py = P.py;
-  constexpr bool varcoef = VAR, icc = ICC;
+  const int py = P.py;
   const double cx = P.cx, cy = P.cy;
   double *const zout = P.z;
   const double *const gy = P.y;
@@ -328,59 +448,55 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
   const double *const gN = P.aN;
   const double *const gE = P.aE;
   const double *const gS = P.aS;
-  const double *const gW = P.aW;
   double *const bnd_b = P.bnd_b;
-  double *const zlast = P.zlast;
-  unsigned int *const prog_b = P.prog_b;
   int *const status = P.status;
   double *const prof = P.prof;
-  const int i0 = 32 * k;
-  const int nlines = min(32, nx - i0);
+  const int i0 = kLines * k;
+  const int nl = min(kLines, nx - i0);
+  const bool has_prod = (k + 1 < nsweep);
+  const bool prod_local = has_prod && (ws + 1 < sw);
+  const bool has_cons = k > 0;
+  const bool cons_local = has_cons && (ws > 0);
+  const int lead = has_prod ? 31 : nl - 1;
+  const bool real = lane < nl;
+  const bool lin = (lane == 31) && has_prod;
+  const int skew = lead - lane;  // negative for the idle lanes above the lead of the last warp
   const int i = i0 + lane;
-  const bool valid = lane < nlines;
-  const int lead = nlines - 1;
-  const int na = varcoef ? 4 : 2;
+  constexpr int na = VAR ? 4 : 2;
   double *ring_y = (double *)smem_warp;
-  double *ring_d = ring_y + 32 * kRing;
-  double *ring_n = ring_d + 32 * kRing;
-  double *ring_e = ring_n + 32 * kRing;
-  double *bline = ring_y + (size_t)na * 32 * kRing;
+  double *ring_d = ring_y + 32 * kPitch;
+  double *ring_n = ring_d + 32 * kPitch;
+  double *ring_e = ring_n + 32 * kPitch;
+  double *bline = ring_y + (size_t)na * 32 * kPitch;
+  double *zrow = bline + ((ny + 1) & ~1);
+  double *ones = zrow + kPitch;
   const bool vec16 = (ny % 2) == 0;
-  const bool prod_local = (k + 1 < nsweep) && (ws + 1 < sw);
-  const bool cons_local = (k > 0) && (ws > 0);
   const unsigned int base = epoch * (unsigned int)(ny + 1);
-  const int total = ny + nlines - 1;
+  const int total = ny + lead;
   const int nchunk = (total + kChunk - 1) / kChunk;
-  double *prev_bline = cons_local ? (double *)(smem_warp - P.warp_smem) + (size_t)na * 32 * kRing : nullptr;
   unsigned int *my_cnt = &cnt_cta[2 * ws + 1];
   unsigned int *prev_cnt = &cnt_cta[2 * (ws - 1) + 1];
-  const double ae_const = (valid && i + 1 < nx) ? cx : 0.0;
+  const double *y_row = real ? ring_y + lane * kPitch : zrow;
+  const double *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
+  const double *n_row = real ? ring_n + lane * kPitch : zrow;
+  const double *e_row = real ? ring_e + lane * kPitch : zrow;
+  const double an_c = real ? cy : 0.0;
+  const double ae_c = (real && i + 1 < nx) ? cx : 0.0;
+  double *const zdst = zout + (size_t)(real ? i : 0) * ny;
+  const bool hand = has_cons && lane == 0;
+  double *const hdst = cons_local ? (double *)(smem_warp - P.warp_smem) + (size_t)na * 32 * kPitch
+                                  : bnd_b + ((size_t)(epoch & 1u) * nsweep + k) * ny;
   auto stage = [&](int c) {
-    const int c0 = ny - kChunk * (c + 1);
-    if (ny - kChunk * c <= 0) {
-      cp_async_commit();
-      return;
-    }
-    if (c0 >= 0) {
-      stage_chunk(ring_y, gy, i0, nlines, ny, c0, vec16);
-      stage_chunk(ring_d, gd, i0, nlines, ny, c0, vec16);
-      if (varcoef) {
-        stage_chunk(ring_n, gN, i0, nlines, ny, c0, vec16);
-        stage_chunk(ring_e, gE, i0, nlines, ny, c0, vec16);
-      }
-    } else {
-      const int hi = ny - kChunk * c;
-      for (int p = lane; p < 32 * kChunk; p += 32) {
-        const int line = p / kChunk, pc = p % kChunk;
-        if (line < nlines && pc < hi) {
-          const size_t gi = (size_t)(i0 + line) * ny + pc;
-          const int sidx = line * kRing + (pc & (kRing - 1));
-          cp_async8(&ring_y[sidx], &gy[gi]);
-          cp_async8(&ring_d[sidx], &gd[gi]);
-          if (varcoef) {
-            cp_async8(&ring_n[sidx], &gN[gi]);
-            cp_async8(&ring_e[sidx], &gE[gi]);
-          }
+    const int c1 = ny - kChunk * c;
+    if (c1 > 0) {
+      if (vec16 && (ny % kChunk) == 0) {
+        stage_full<false, na>(ring_y, ring_d, ring_n, ring_e, gy, gd, gN, gE, i0, 0, nl, ny, c1 - kChunk);
+      } else {
+        stage_cols<false>(ring_y, gy, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+        stage_cols<false>(ring_d, gd, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+        if (VAR) {
+          stage_cols<false>(ring_n, gN, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+          stage_cols<false>(ring_e, gE, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
         }
       }
     }
@@ -388,114 +504,144 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
   };
   __syncwarp();  // y of these lines was written by this warp's forward sweep
   const unsigned long long t_begin = global_ns();
-  for (int c = 0; c < kAhead; ++c) stage(c);
-  double z_prev = 0.0, z_first = 0.0, z_step = 0.0, bvals = 0.0, zsum = 0.0;
+  for (int t = lane; t < kPitch; t += 32) {
+    zrow[t] = 0.0;
+    ones[t] = 1.0;
+  }
+  // a producer in another CTA: values loaded kAhead groups early and polled, as in the forward sweep
+  const bool remote = has_prod && !prod_local;
+  double *const hin = has_prod ? bnd_b + ((size_t)(epoch & 1u) * nsweep + (k + 1)) * ny : nullptr;
+  auto hand_issue = [&](int c) -> double {
+    const int col = ny - 1 - (c * kChunk + lane);
+    return (lane < kHand && col >= 0) ? ld_relaxed_gpu(hin + col) : 0.0;
+  };
+  auto hand_land = [&](int c, double v) -> bool {
+    const int col = ny - 1 - (c * kChunk + lane);
+    const bool mine = lane < kHand && col >= 0;
+    bool miss = mine && hand_empty(v);
+    long long spins = 0;
+    while (__any_sync(0xffffffffu, miss)) {
+      ++spins;
+      if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+        if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
+        return false;
+      }
+      if (spins > 32) __nanosleep(64);
+      if (miss) {
+        v = ld_relaxed_gpu(hin + col);
+        miss = hand_empty(v);
+      }
+    }
+    if (mine) {
+      bline[col] = v;
+      hin[col] = __longlong_as_double((long long)kHandEmpty);
+    }
+    __syncwarp();
+    return true;
+  };
   unsigned int avail = 0;
-  const double *rowy = ring_y + lane * kRing;
-  const double *rowd = ring_d + lane * kRing;
-  const double *rown = ring_n + lane * kRing;
-  const double *rowe = ring_e + lane * kRing;
-  double *zdst = zout + (size_t)i * ny;
+  for (int c = 0; c < kAhead; ++c) {
+    if (remote && !hand_land(c, hand_issue(c))) {
+      cp_async_wait0();
+      return;
+    }
+    stage(c);
+  }
+  double z_prev = 0.0, z_first = 0.0, zsum = 0.0;
   for (int q = 0; q < nchunk; ++q) {
     stage(q + kAhead);
+    const double hv = remote ? hand_issue(q + kAhead) : 0.0;
     cp_async_wait_ahead();
     __syncwarp();
-    {
-      const int s0 = q * kChunk;
-      if (k + 1 < nsweep && s0 < ny) {
-        const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
-        if (avail + base < need) {
-          const unsigned int v = prod_local ? wait_progress<true>(my_cnt, need, status)
-                                            : wait_progress<false>(&prog_b[k + 1], need, status);
-          if (v == 0) return;
-          avail = v - base;
+    const int s0 = q * kChunk;
+    if (prod_local && s0 < ny) {  // hand-over values of line i0+31, columns ny-1-s0 .. ny-kHand-s0, same CTA
+      const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
+      if (avail + base < need) {
+        const unsigned int v = wait_progress<true>(my_cnt, need, status);
+        if (v == 0) {
+          cp_async_wait0();
+          return;
         }
-        const int col = ny - 1 - (s0 + lane);
-        if (lane < kHand && col >= 0)
-          bvals = prod_local ? bline[col] : __ldcg(&bnd_b[(size_t)(k + 1) * ny + col]);
+        avail = v - base;
       }
-      // steady state: every valid lane of the group is inside [0, ny) -- no range checks, no wraps
-      if (s0 >= 32 && s0 + kHand < ny && s0 + kHand <= total && !(px && i0 == 0)) {
-        const bool hand = (lane == 0) && (k > 0);
-#pragma unroll
-        for (int ss = 0; ss < kHand; ++ss) {
-          const int j = ny - 1 - (s0 + ss - (lead - lane));
-          const int slot = j & (kRing - 1);
-          const double yv = rowy[slot];
-          const double dv = rowd[slot];
-          const double an = varcoef ? rown[slot] : cy;
-          const double ae = varcoef ? ((i + 1 < nx) ? rowe[slot] : 0.0) : ae_const;
-          const double t = an * z_prev;
-          double z_dn = __shfl_down_sync(0xffffffffu, z_step, 1);
-          if (k + 1 < nsweep) {
-            const double b = __shfl_sync(0xffffffffu, bvals, ss);
-            if (lane == lead) z_dn = b;
-          }
-          const double zv = icc ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
-          st_global_if(&zdst[j], zv, valid);
-          zsum += valid ? zv : 0.0;
-          if (cons_local) {
-            if (hand) prev_bline[j] = zv;
-          } else {
-            st_global_if(&bnd_b[(size_t)k * ny + j], zv, hand);
-          }
-          z_prev = valid ? zv : 0.0;
-          z_step = valid ? zv : 0.0;
-        }
-      } else {
+      __syncwarp();
+    }
+    if (s0 >= 32 && s0 + kHand < ny) {
+      // steady state: every real lane's column lies in [1, ny-2]
+      const int jt = ny - 1 - (s0 - skew);
+      const int slot = jt & (kRing - 1);
+      const double *yb = lin ? bline + jt : y_row + kMirror + slot;
+      const double *db = d_row + kMirror + slot;
+      const double *nb = n_row + kMirror + slot;
+      const double *eb = e_row + kMirror + slot;
+      double *zp = zdst + jt;
+      double *hp = hdst + jt;
+      double yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
-        const int s = s0 + ss;
-        const int j = ny - 1 - (s - (lead - lane));
-        const bool act = valid && j >= 0 && j < ny && s < total;
+        yvv[ss] = yb[-ss];
+        dvv[ss] = db[-ss];
+        anv[ss] = VAR ? nb[-ss] : an_c;
+        aev[ss] = VAR ? eb[-ss] : ae_c;
+      }
+#pragma unroll
+      for (int ss = 0; ss < kHand; ++ss) {
+        const double yv = yvv[ss];
+        const double dv = dvv[ss];
+        const double an = anv[ss];
+        const double ae = aev[ss];
+        const double t = an * z_prev;
+        const double z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
+        const double zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
+        if (real) zp[-ss] = zv;
+        zsum += zv;
+        if (hand) hp[-ss] = zv;
+        z_prev = zv;
+      }
+    } else {
+#pragma unroll
+      for (int ss = 0; ss < kHand; ++ss) {
+        const int j = ny - 1 - (s0 + ss - skew);
+        const bool inr = j >= 0 && j < ny;
+        const bool act = inr && (real || lin);
         const int slot = j & (kRing - 1);
-        const double yv = rowy[slot];
-        const double dv = rowd[slot];
-        const double an = (j + 1 < ny) ? (varcoef ? rown[slot] : cy) : 0.0;
-        const double ae = varcoef ? ((valid && i + 1 < nx) ? rowe[slot] : 0.0) : ae_const;
-        // upper neighbours in ascending column order: (i,j+1), (i,ny-1) [j==0], (i+1,j), (nx-1,j) [i==0]
-        // own-line terms first; one FMA (plus the final scaling) follows the shuffle from line i+1
+        const double yv = lin ? (inr ? bline[j] : 0.0) : y_row[kMirror + slot];
+        const double dv = d_row[kMirror + slot];
+        const double an = (j + 1 < ny) ? (VAR ? n_row[kMirror + slot] : an_c) : 0.0;
+        const double ae = VAR ? e_row[kMirror + slot] : ae_c;
+        // upper neighbours in ascending column order: (i,j+1), (i,ny-1) [j==0], (i+1,j); own-line terms
+        // first, one FMA (plus the final scaling) follows the shuffle from line i+1
         double t = an * z_prev;
-        if (py && j == 0 && valid) t = fma(varcoef ? gS[(size_t)i * ny] : cy, z_first, t);
-        if (px && i == 0 && act) t = fma(varcoef ? gW[j] : cx, __ldcg(&zlast[j]), t);
-        double z_dn = __shfl_down_sync(0xffffffffu, z_step, 1);
-        if (k + 1 < nsweep) {
-          const double b = __shfl_sync(0xffffffffu, bvals, ss);
-          if (lane == lead) z_dn = b;
-        }
+        if (py && j == 0 && real) t = fma(VAR ? gS[(size_t)i * ny] : cy, z_first, t);
+        const double z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
         // ICC: z = (y - d t) d = y d - d^2 t ; ILDLT: z = D^-1 (y - t)
-        const double zv = icc ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
+        const double zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
         if (act) {
-          zdst[j] = zv;
-          zsum += zv;
-          if (px && i == nx - 1) zlast[j] = zv;
-          if (lane == 0 && k > 0) {
-            if (cons_local)
-              prev_bline[j] = zv;
-            else
-              bnd_b[(size_t)k * ny + j] = zv;
+          if (real) {
+            zdst[j] = zv;
+            zsum += zv;
           }
+          if (hand) hdst[j] = zv;
           if (j == ny - 1) z_first = zv;
           z_prev = zv;
-          z_step = zv;
-        }
-      }
-      }
-      const int done = min(ny, s0 + kHand - lead);
-      if (k > 0 && done > 0) {
-        __syncwarp();
-        if (lane == 0) {
-          if (cons_local)
-            st_release_cta(prev_cnt, base + (unsigned int)done);
-          else
-            st_release_gpu(&prog_b[k], base + (unsigned int)done);
         }
       }
     }
+    // publish the columns lane 0 (skew `lead`) has finished to a consumer in this CTA
+    const int done = min(ny, s0 + kHand - lead);
+    if (cons_local && done > 0) {
+      __syncwarp();
+      if (lane == 0) st_release_cta(prev_cnt, base + (unsigned int)done);
+    }
     __syncwarp();
+    if (remote && !hand_land(q + kAhead, hv)) {
+      cp_async_wait0();
+      return;
+    }
   }
   cp_async_wait0();
   __syncwarp();
+  if (!real) zsum = 0.0;
   acc[0] += zsum;
   if (prof && lane == 0 && k < 16) prof[4 * k + 3] = (double)(global_ns() - t_begin);
 }
