@@ -101,6 +101,19 @@ __device__ __forceinline__ bool hand_empty(double v) {
   return (unsigned long long)__double_as_longlong(v) == kHandEmpty;
 }
 
+// Stores under a per-lane predicate without a branch: the warp stays converged for the shuffle that
+// follows in the same step.
+__device__ __forceinline__ void st_global_if(double *p, double v, bool pred) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.global.f64 [%0], %1;\n\t}" ::"l"(p), "d"(v),
+               "r"((int)pred)
+               : "memory");
+}
+__device__ __forceinline__ void st_generic_if(double *p, double v, bool pred) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.f64 [%0], %1;\n\t}" ::"l"(p), "d"(v),
+               "r"((int)pred)
+               : "memory");
+}
+
 // Bounded warp-uniform wait for a progress counter (shared or global) to reach `target`.
 template <bool SHARED>
 __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, unsigned int target, int *status) {
@@ -367,41 +380,50 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
         const double sum = fma(-aw, w_up, t1);
         const double yv = ICC ? sum * dv : sum;
         const double wv = sum * (ICC ? dv * dv : dv);
-        if (real) yp[ss] = yv;
+        st_global_if(yp + ss, yv, real);
         rz = fma(yv, ICC ? yv : wv, rz);
         rsum += rv;
-        if (hand) hp[ss] = wv;
+        st_generic_if(hp + ss, wv, hand);
         w_prev = wv;
       }
     } else {
+      // ramp-up / ramp-down group (some lane's column outside [0, ny), or the periodic-y wrap column):
+      // the steady arithmetic, with the carried state, the stores and the sums gated by the column range
+      const int j0 = s0 - lane;
+      const int slot = j0 & (kRing - 1);
+      const double *rb = lin ? bline + j0 : r_row + slot;
+      const double *db = d_row + slot;
+      const double *wb = w_row + slot;
+      const double *sb = s_row + slot;
+      double rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
-        const int j = s0 + ss - lane;
-        const bool inr = j >= 0 && j < ny;
-        const bool act = inr && (real || lin);
-        const int slot = j & (kRing - 1);
-        const double rv = (lin ? (inr ? bline[j] : 0.0) : r_row[slot]) - m_lane;
-        const double dv = d_row[slot];
-        const double as = (j > 0) ? (VAR ? s_row[slot] : as_c) : 0.0;
-        const double aw = VAR ? w_row[slot] : aw_c;
-        // own-line terms first (periodic-y wrap, S), so that one FMA follows the shuffle from line i-1
+        rvv[ss] = rb[ss];
+        dvv[ss] = db[ss];
+        asv[ss] = VAR ? sb[ss] : as_c;
+        awv[ss] = VAR ? wb[ss] : aw_c;
+      }
+#pragma unroll
+      for (int ss = 0; ss < kHand; ++ss) {
+        const int j = j0 + ss;
+        const bool act = j >= 0 && j < ny;
+        const double rv = rvv[ss] - m_lane;
+        const double dv = dvv[ss];
+        // own-line terms first (periodic-y wrap, S), so that one FMA follows the shuffle from line i-1; a
+        // lane's first active step has w_prev = 0, so the S term vanishes at j = 0
         double t1 = rv;
         if (py && j == ny - 1 && real) t1 = fma(-(VAR ? gN[(size_t)i * ny + j] : cy), w_first, t1);
-        t1 = fma(-as, w_prev, t1);
+        t1 = fma(-asv[ss], w_prev, t1);
         const double w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
-        const double sum = fma(-aw, w_up, t1);
+        const double sum = fma(-awv[ss], w_up, t1);
         const double yv = ICC ? sum * dv : sum;
         const double wv = sum * (ICC ? dv * dv : dv);
-        if (act) {
-          if (real) {
-            ydst[j] = yv;
-            rz = fma(yv, ICC ? yv : wv, rz);
-            rsum += rv;
-          }
-          if (hand) hdst[j] = wv;
-          if (j == 0) w_first = wv;
-          w_prev = wv;
-        }
+        st_global_if(ydst + j, yv, act && real);
+        rz = (act && real) ? fma(yv, ICC ? yv : wv, rz) : rz;
+        rsum = (act && real) ? rsum + rv : rsum;
+        st_generic_if(hdst + j, wv, act && hand);
+        w_first = (py && j == 0) ? wv : w_first;
+        w_prev = act ? wv : w_prev;
       }
     }
     // publish the columns lane 31 (skew 31) has finished to a consumer in this CTA (a consumer in another
@@ -593,38 +615,47 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
         const double t = an * z_prev;
         const double z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
         const double zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
-        if (real) zp[-ss] = zv;
+        st_global_if(zp - ss, zv, real);
         zsum += zv;
-        if (hand) hp[-ss] = zv;
+        st_generic_if(hp - ss, zv, hand);
         z_prev = zv;
       }
     } else {
+      // ramp-up / ramp-down group: the steady arithmetic with the state, stores and sums gated by the
+      // column range; a lane's first active step has z_prev = 0, so the N term vanishes at j = ny-1
+      const int jt = ny - 1 - (s0 - skew);
+      const int slot = jt & (kRing - 1);
+      const double *yb = lin ? bline + jt : y_row + kMirror + slot;
+      const double *db = d_row + kMirror + slot;
+      const double *nb = n_row + kMirror + slot;
+      const double *eb = e_row + kMirror + slot;
+      double yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
-        const int j = ny - 1 - (s0 + ss - skew);
-        const bool inr = j >= 0 && j < ny;
-        const bool act = inr && (real || lin);
-        const int slot = j & (kRing - 1);
-        const double yv = lin ? (inr ? bline[j] : 0.0) : y_row[kMirror + slot];
-        const double dv = d_row[kMirror + slot];
-        const double an = (j + 1 < ny) ? (VAR ? n_row[kMirror + slot] : an_c) : 0.0;
-        const double ae = VAR ? e_row[kMirror + slot] : ae_c;
+        yvv[ss] = yb[-ss];
+        dvv[ss] = db[-ss];
+        anv[ss] = VAR ? nb[-ss] : an_c;
+        aev[ss] = VAR ? eb[-ss] : ae_c;
+      }
+#pragma unroll
+      for (int ss = 0; ss < kHand; ++ss) {
+        const int j = jt - ss;
+        const bool act = j >= 0 && j < ny;
+        const double yv = yvv[ss];
+        const double dv = dvv[ss];
+        const double ae = aev[ss];
         // upper neighbours in ascending column order: (i,j+1), (i,ny-1) [j==0], (i+1,j); own-line terms
         // first, one FMA (plus the final scaling) follows the shuffle from line i+1
-        double t = an * z_prev;
+        double t = anv[ss] * z_prev;
         if (py && j == 0 && real) t = fma(VAR ? gS[(size_t)i * ny] : cy, z_first, t);
         const double z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
         // ICC: z = (y - d t) d = y d - d^2 t ; ILDLT: z = D^-1 (y - t)
         const double zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
-        if (act) {
-          if (real) {
-            zdst[j] = zv;
-            zsum += zv;
-          }
-          if (hand) hdst[j] = zv;
-          if (j == ny - 1) z_first = zv;
-          z_prev = zv;
-        }
+        st_global_if(zdst + j, zv, act && real);
+        zsum = (act && real) ? zsum + zv : zsum;
+        st_generic_if(hdst + j, zv, act && hand);
+        z_first = (py && j == ny - 1) ? zv : z_first;
+        z_prev = act ? zv : z_prev;
       }
     }
     // publish the columns lane 0 (skew `lead`) has finished to a consumer in this CTA
