@@ -101,6 +101,63 @@ __global__ void k_p_assemble(Grid G, BCSet bc, Fv rm, Fv us, Fv vs, Fv pe, int s
 }
 
 // ---------------------------------------------------------------------------------------------------
+// Mixed-precision pressure solve: FP64 defect correction around FP32 inner PCG solves
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_to_float(const double *src, float *dst, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (float)src[t];
+}
+// r = b - A x in FP64, with per-CTA sums of r, r^2 and b^2 (the outer residual and its stopping norms)
+__global__ void k_outer_residual(SpOp A, const double *b, const double *x, double *r, double *partials) {
+  __shared__ double sh[3 * 32];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < A.n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / A.ny), j = (int)(t % A.ny);
+    const double rr = b[t] - spmv_row<5>(A, x, i, j);
+    r[t] = rr;
+    v[0] += rr;
+    v[1] += rr * rr;
+    v[2] += b[t] * b[t];
+  }
+  block_sum<3>(v, sh);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x + 0] = v[0];
+    partials[3 * blockIdx.x + 1] = v[1];
+    partials[3 * blockIdx.x + 2] = v[2];
+  }
+}
+// the three sums of k_outer_residual, added in a fixed order by one warp
+__global__ void k_finish3(const double *partials, int nparts, double *out) {
+  const int lane = threadIdx.x;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int p = lane; p < nparts; p += 32) {
+    s0 += partials[3 * p];
+    s1 += partials[3 * p + 1];
+    s2 += partials[3 * p + 2];
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  if (lane == 0) {
+    out[0] = s0;
+    out[1] = s1;
+    out[2] = s2;
+  }
+}
+// right-hand side of an inner solve: the projected FP64 residual rounded to FP32; the correction starts at 0
+__global__ void k_inner_rhs(const double *r, double mean, float *rf, float *ef, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) {
+    rf[t] = (float)(r[t] - mean);
+    ef[t] = 0.0f;
+  }
+}
+__global__ void k_add_correction(double *x, const float *e, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) x[t] += (double)e[t];
+}
+
+// ---------------------------------------------------------------------------------------------------
 // CH operator A = alpha0 I - beta1 L + beta2 L^2 (build_laplacian_matrix / multiply /
 // build_cahn_hilliard_operator, ch_sparse_krylov.hpp:135-233) with std::map accumulation semantics.
 // ---------------------------------------------------------------------------------------------------
@@ -350,6 +407,13 @@ struct dn_handle {
   cudaEvent_t kev[2] = {};
   double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ch, momentum, pressure, correction, pressure PCG kernel,
                                                  // CH PCG kernel, BiCGSTAB kernel, pressure PCG iterations
+  // mixed-precision form: FP32 operator, factor and inner Krylov vectors; FP32 staged launch shape
+  float *fa5 = nullptr, *fl5 = nullptr, *fdinv5 = nullptr;
+  float *fb = nullptr, *fx = nullptr, *fr = nullptr, *fz = nullptr, *fy = nullptr, *fp0 = nullptr, *fp1 = nullptr,
+        *fap = nullptr;
+  int sw5f = 0, sw5f_blocks_max = 0;
+  size_t sw5f_warp_smem[2] = {0, 0};
+  int refinement_cycles = 0;  // outer cycles of the last mixed-precision pressure solve
   int step = 0;  // step index of the step in progress (split extrapolation, operators.cpp:416)
   double pcg_split_ms[3] = {0, 0, 0};  // pressure PCG, in-kernel: [P1 SpMV+barrier, P2 update+barrier, sweeps]
 };
@@ -517,6 +581,7 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   P.project = project;
   P.max_it = max_it;
   P.tol = tol;
+  P.tol_abs = tol;  // the reference stops on rel < tol || abs < tol
   P.bar_count = h->bar_count;
   P.bar_gen = h->bar_gen;
   P.status = h->status;
@@ -591,6 +656,157 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
     h->pcg_split_ms[1] = tmp[5];
     h->pcg_split_ms[2] = tmp[6];
   }
+  return DN_OK;
+}
+
+// One FP32 inner PCG solve (the persistent kernel instantiated for float) on the handle's FP32 buffers.
+dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol, double out[4]) {
+  PcgArgsT<float> P{};
+  P.A = SpOpT<float>{h->fa5, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  P.l = h->fl5;
+  P.dinv = h->fdinv5;
+  P.prec = prec;
+  P.b = h->fb;
+  P.x = h->fx;
+  P.r = h->fr;
+  P.z = h->fz;
+  P.y = h->fy;
+  P.p0 = h->fp0;
+  P.p1 = h->fp1;
+  P.ap = h->fap;
+  P.project = project;
+  P.max_it = std::max(1, max_it);
+  P.tol = tol;
+  P.tol_abs = 0.0;  // an inner solve stops on its relative residual only
+  P.bar_count = h->bar_count;
+  P.bar_gen = h->bar_gen;
+  P.status = h->status;
+  P.prog_f = h->prog;
+  P.prog_b = h->prog + kMaxBlocks * 8;
+  P.partials = h->partials;
+  P.out = h->scal + 8;
+  P.nsweep = h->nsweep;
+  P.warp_smem = 0;
+  size_t dyn_smem = 0;
+  int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(h->nsweep, (h->n + 2047) / 2048));
+  blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
+  const bool staged = h->sw5f > 0 && !h->G.px;
+  if (staged) {
+    const bool var = !use_split(h->cfg);
+    Sweep5T<float> &W = P.s5;
+    W.nx = h->G.nx;
+    W.ny = h->G.ny;
+    W.n = (int)h->n;
+    W.px = h->G.px;
+    W.py = h->G.py;
+    W.prec = prec;
+    W.varcoef = var ? 1 : 0;
+    W.aW = h->fa5;
+    W.aS = h->fa5 + h->n;
+    W.aN = h->fa5 + 3 * h->n;
+    W.aE = h->fa5 + 4 * h->n;
+    W.cx = (float)(-(1.0 / (h->G.dx * h->G.dx)));
+    W.cy = (float)(-(1.0 / (h->G.dy * h->G.dy)));
+    W.dinv = h->fdinv5;
+    W.r = h->fr;
+    W.y = h->fy;
+    W.z = h->fz;
+    W.bnd_f = reinterpret_cast<float *>(h->bnd_f);  // the FP64 hand-over buffers, reused
+    W.bnd_b = reinterpret_cast<float *>(h->bnd_b);
+    W.wline0 = reinterpret_cast<float *>(h->wline0);
+    W.zlast = reinterpret_cast<float *>(h->zlast);
+    W.prog_f = h->prog;
+    W.prog_b = h->prog + kMaxBlocks * 8;
+    W.nsweep = h->nsweep5;
+    W.sw = h->sw5f;
+    W.status = h->status;
+    P.warp_smem = (int)h->sw5f_warp_smem[var ? 1 : 0];
+    W.warp_smem = P.warp_smem;
+    W.prof = h->prof;
+    dyn_smem = 64 + (size_t)h->sw5f * P.warp_smem;
+    const int sweep_ctas = (h->nsweep5 + h->sw5f - 1) / h->sw5f;
+    blocks = std::max(blocks, sweep_ctas);
+    blocks = std::min(blocks, h->sw5f_blocks_max);
+    if (blocks < sweep_ctas) return fail(h, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
+  } else if ((long long)blocks * (kBlock / 32) < h->nsweep) {
+    return fail(h, DN_ERR_UNSUPPORTED, "grid too wide for the co-resident wavefront warps");
+  }
+  DN_TRY(reset_sync(h));
+  void *args[] = {&P};
+  cudaEventRecord(h->kev[0], h->stream);
+  DN_CUDA(h, cudaLaunchCooperativeKernel(staged ? (const void *)k_pcg<5, 3, float> : (const void *)k_pcg<5, 0, float>,
+                                         dim3(blocks), dim3(kBlock), args, dyn_smem, h->stream));
+  cudaEventRecord(h->kev[1], h->stream);
+  h->launches++;
+  int st = 0;
+  DN_TRY(read_status(h, &st));
+  if (st != kDevOk) return dev_status_to_dn(h, st);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+  h->phase_ms[4] += ms;
+  double tmp[7];
+  DN_TRY(read_scalars(h, 7, tmp));
+  for (int k = 0; k < 4; ++k) out[k] = tmp[k];
+  h->pcg_split_ms[0] += tmp[4];
+  h->pcg_split_ms[1] += tmp[5];
+  h->pcg_split_ms[2] += tmp[6];
+  return DN_OK;
+}
+
+// Mixed-precision pressure solve: x = 0; repeat r = b - A x (FP64, projected when the system is singular),
+// stop on the reference's rule (rel < tol or abs < tol on the FP64 residual), else solve A e = r with the
+// FP32 PCG to the relative tolerance mixed_inner_tolerance and add e to x in FP64.  The operator and the
+// factor are the FP64 ones rounded to FP32.  out: [0] inner iterations in total, [1] abs and [2] rel FP64
+// residual, [3] 0.
+dn_status mixed_pressure(dn_handle *h, int kind, double out[4]) {
+  const dn_config &cfg = h->cfg;
+  const long long n = h->n;
+  const int project = h->has_dirichlet ? 0 : 1;
+  k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
+  DN_TRY(check_launch(h, "k_to_float"));
+  if (h->G.px) {  // the global-memory wavefront reads the L slots
+    k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->l5, h->fl5, 5 * n);
+    DN_TRY(check_launch(h, "k_to_float"));
+  }
+  k_to_float<<<blocks_for(n), 256, 0, h->stream>>>(h->dinv5, h->fdinv5, n);
+  DN_TRY(check_launch(h, "k_to_float"));
+  const SpOp A{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  h->phase_ms[4] = 0.0;
+  h->pcg_split_ms[0] = h->pcg_split_ms[1] = h->pcg_split_ms[2] = 0.0;
+  constexpr int kMaxCycles = 40;
+  int total = 0, cycles = 0;
+  double absr = 0.0, relr = 0.0, prev = INFINITY;
+  for (;;) {
+    const int nb = 128;
+    k_outer_residual<<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
+    DN_TRY(check_launch(h, "k_outer_residual"));
+    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
+    DN_TRY(check_launch(h, "k_finish3"));
+    double sums[3];
+    DN_TRY(read_scalars(h, 3, sums));
+    const double mean = project ? sums[0] / (double)n : 0.0;
+    const double rn2 = project ? std::max(sums[1] - sums[0] * sums[0] / (double)n, 0.0) : sums[1];
+    absr = std::sqrt(rn2);
+    relr = absr / std::max(std::sqrt(std::max(sums[2], 0.0)), 1.0e-30);
+    if (relr < cfg.pressure_tolerance || absr < cfg.pressure_tolerance) break;
+    // the iteration budget is shared by the inner solves; a cycle that no longer reduces the residual ends it
+    if (cycles >= kMaxCycles || total >= cfg.poisson_iterations || !(absr < prev)) break;
+    prev = absr;
+    k_inner_rhs<<<blocks_for(n), 256, 0, h->stream>>>(h->r, mean, h->fb, h->fx, n);
+    DN_TRY(check_launch(h, "k_inner_rhs"));
+    double o[4];
+    DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, o));
+    total += (int)o[0];
+    k_add_correction<<<blocks_for(n), 256, 0, h->stream>>>(h->x, h->fx, n);
+    DN_TRY(check_launch(h, "k_add_correction"));
+    ++cycles;
+    if ((int)o[0] == 0) break;
+  }
+  h->refinement_cycles = cycles;
+  out[0] = (double)total;
+  out[1] = absr;
+  out[2] = relr;
+  out[3] = 0.0;
   return DN_OK;
 }
 
@@ -940,7 +1156,11 @@ dn_status pressure(dn_handle *h, int step, dn_report *rep) {
   }
   DN_CUDA(h, cudaMemsetAsync(h->x, 0, h->n * sizeof(double), h->stream));
   double out[4];
-  if (h->sw5 > 0 && !h->G.px && h->nsweep >= 1) {
+  rep->refinement_cycles = 0;
+  if (cfg.precision == DN_PRECISION_MIXED) {
+    DN_TRY(mixed_pressure(h, kind, out));
+    rep->refinement_cycles = h->refinement_cycles;
+  } else if (h->sw5 > 0 && !h->G.px && h->nsweep >= 1) {
     DN_TRY((run_pcg<5, 3>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
                           cfg.pressure_tolerance, out)));
   } else {
@@ -1053,8 +1273,6 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     return bad(DN_ERR_CONFIG, "surface_tension_smoothing_passes must be non-negative");
   if (c.surface_tension_smoothing_weight < 0.0 || c.surface_tension_smoothing_weight > 0.25)
     return bad(DN_ERR_CONFIG, "surface_tension_smoothing_weight must lie in [0, 0.25]");
-  if (c.precision != DN_PRECISION_FP64)
-    return bad(DN_ERR_UNSUPPORTED, "precision mixed is not available in this build");
 
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bad(DN_ERR_CUDA, "no CUDA device available");
@@ -1162,6 +1380,34 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
       if (h->sw5_blocks_max == 0) h->sw5 = 0;
     }
   }
+  if (c.precision == DN_PRECISION_MIXED) {
+    A(dalloc(h, &h->fa5, 5 * h->n));
+    A(dalloc(h, &h->fl5, 5 * h->n));
+    for (float **p : {&h->fdinv5, &h->fb, &h->fx, &h->fr, &h->fz, &h->fy, &h->fp0, &h->fp1, &h->fap})
+      A(dalloc(h, p, h->n));
+    if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+    const int optin = h->smem_optin;
+    auto round16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    h->sw5f_warp_smem[0] = round16(sweep_warp_smem(2, ny, 4));
+    h->sw5f_warp_smem[1] = round16(sweep_warp_smem(4, ny, 4));
+    const size_t per = h->sw5f_warp_smem[use_split(c) ? 0 : 1];
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_pcg<5, 3, float>);
+    const size_t budget = (size_t)optin > 64 + fa.sharedSizeBytes ? (size_t)optin - 64 - fa.sharedSizeBytes : 0;
+    int sw = (int)std::min<size_t>(8, budget / per);
+    sw = std::min(sw, h->nsweep5);
+    if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
+    h->sw5f = sw;
+    if (sw > 0) {
+      const size_t dyn = 64 + (size_t)sw * per;
+      cudaFuncSetAttribute(k_pcg<5, 3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           std::max((int)dyn, optin - (int)fa.sharedSizeBytes));
+      int occf = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, k_pcg<5, 3, float>, kBlock, dyn);
+      h->sw5f_blocks_max = std::min(kMaxBlocks, std::max(0, occf) * h->num_sms);
+      if (h->sw5f_blocks_max == 0) h->sw5f = 0;
+    }
+  }
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg<5, 0>, kBlock, 0);
   int occ2 = 0;
@@ -1169,6 +1415,11 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   int occ3 = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_bicgstab, kBlock, 0);
   occ = std::min(occ, std::min(occ2, occ3));
+  if (c.precision == DN_PRECISION_MIXED) {
+    int occ4 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4, k_pcg<5, 0, float>, kBlock, 0);
+    occ = std::min(occ, occ4);
+  }
   h->max_coop_blocks = std::min(kMaxBlocks, std::max(1, occ) * h->num_sms);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bad(DN_ERR_CUDA, "initial synchronisation failed");
   *out = h;
@@ -1785,6 +2036,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   P.project = has_dirichlet ? 0 : 1;
   P.max_it = c.poisson_iterations;
   P.tol = c.pressure_tolerance;
+  P.tol_abs = c.pressure_tolerance;
   P.bar_count = uptr(L.bar_count);
   P.bar_gen = uptr(L.bar_gen);
   P.status = status;

@@ -58,19 +58,21 @@ __device__ __forceinline__ long long slot_col(int i, int j, int s, int nx, int n
   return (long long)ii * ny + jj;
 }
 
-struct SpOp {
-  const double *a;  // [S][n]
+template <typename T>
+struct SpOpT {
+  const T *a;  // [S][n]
   int n, nx, ny, px, py;
 };
+using SpOp = SpOpT<double>;
 
-template <int S>
-__device__ __forceinline__ double spmv_row(const SpOp &A, const double *x, int i, int j) {
+template <int S, typename T>
+__device__ __forceinline__ T spmv_row(const SpOpT<T> &A, const T *x, int i, int j) {
   const long long r = (long long)i * A.ny + j;
-  double sum = 0.0;
+  T sum = T(0);
 #pragma unroll
   for (int s = 0; s < S; ++s) {
-    const double a = A.a[(size_t)s * A.n + r];
-    if (a != 0.0) {
+    const T a = A.a[(size_t)s * A.n + r];
+    if (a != T(0)) {
       const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
       sum += a * x[c];
     }
@@ -245,16 +247,20 @@ __global__ void k_diag_inverse(SpOp A, double *dinv) {
 // ---------------------------------------------------------------------------------------------------
 // Persistent PCG (solve_preconditioned_cg, ch_sparse_krylov.hpp:515-660)
 // ---------------------------------------------------------------------------------------------------
-struct PcgArgs {
-  SpOp A;
-  const double *l;     // factor slots [S][n]
-  const double *dinv;  // [n]
-  int prec;            // PrecKind
-  const double *b;
-  double *x, *r, *z, *y, *p0, *p1, *ap;
+// T is the type of the operator, the factor and the Krylov vectors (double; float for the inner solves of
+// the mixed-precision form).  Dot products, norms and the projection means are accumulated in double.
+template <typename T>
+struct PcgArgsT {
+  SpOpT<T> A;
+  const T *l;     // factor slots [S][n]
+  const T *dinv;  // [n]
+  int prec;       // PrecKind
+  const T *b;
+  T *x, *r, *z, *y, *p0, *p1, *ap;
   int project;  // mean projection of x, r, z, p (pressure null space, pressure.cpp:225-239)
   int max_it;
-  double tol;
+  double tol;      // relative stopping tolerance
+  double tol_abs;  // absolute stopping tolerance (the reference uses tol for both; 0 disables it)
   // synchronisation
   unsigned int *bar_count;
   unsigned int *bar_gen;
@@ -262,10 +268,11 @@ struct PcgArgs {
   unsigned int *prog_f, *prog_b;  // per sweep warp progress, monotonic across applications
   double *partials;
   double *out;  // [0] iterations [1] abs residual [2] rel residual [3] iterate residual
-  int nsweep;   // sweep warps (ceil(nx/32)) for the 5-point wavefront
-  Sweep5 s5;    // staged wavefront (SWEEP 3)
-  int warp_smem;  // shared-memory bytes per sweep warp (SWEEP 3)
+  int nsweep;      // sweep warps (ceil(nx/32)) for the 5-point wavefront
+  Sweep5T<T> s5;   // staged wavefront (SWEEP 3)
+  int warp_smem;   // shared-memory bytes per sweep warp (SWEEP 3)
 };
+using PcgArgs = PcgArgsT<double>;
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
   unsigned int v;
@@ -297,18 +304,19 @@ constexpr int kPub = 16;  // columns between progress publications of a sweep wa
 
 // Forward sweep of the 5-point factor for sweep warp k.  Reads r (minus the pending mean m_r; when
 // projecting, writes the projected residual back), writes y.  ICC: y = (r - sum L y) / d.  LDLT: y = r - sum L y.
-__device__ void fwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r) {
+template <typename T>
+__device__ void fwd5(const PcgArgsT<T> &P, int k, unsigned int epoch, double m_r) {
   const int lane = threadIdx.x & 31;
   const int nx = P.A.nx, ny = P.A.ny, n = P.A.n;
   const int i = 32 * k + lane;
   const bool valid = i < nx;
   const unsigned int base = epoch * (unsigned int)(ny + 1);
-  const double *lW = P.l, *lS = P.l + n, *lN = P.l + 3 * (size_t)n, *lE = P.l + 4 * (size_t)n;
-  double y_prev = 0.0, y_first = 0.0, y_step = 0.0;
+  const T *lW = P.l, *lS = P.l + n, *lN = P.l + 3 * (size_t)n, *lE = P.l + 4 * (size_t)n;
+  T y_prev = T(0), y_first = T(0), y_step = T(0);
   unsigned int avail = 0;
   for (int s = 0; s < ny + 31; ++s) {
     const int j = s - lane;
-    double y_up = __shfl_up_sync(0xffffffffu, y_step, 1);
+    T y_up = __shfl_up_sync(0xffffffffu, y_step, 1);
     if (k > 0 && s < ny) {
       if ((unsigned int)s >= avail) {
         const unsigned int v = wait_flag(&P.prog_f[k - 1], base + (unsigned int)s + 1u, P.status);
@@ -319,13 +327,13 @@ __device__ void fwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r) {
     }
     if (valid && j >= 0 && j < ny) {
       const size_t idx = (size_t)i * ny + j;
-      const double rv = __ldcg(&P.r[idx]) - m_r;
-      double sum = rv;
+      const T rv = __ldcg(&P.r[idx]) - (T)m_r;
+      T sum = rv;
       if (P.A.px && i == nx - 1) sum -= __ldg(&lE[idx]) * __ldcg(&P.y[j]);
       if (i > 0) sum -= __ldg(&lW[idx]) * y_up;
       if (P.A.py && j == ny - 1) sum -= __ldg(&lN[idx]) * y_first;
       if (j > 0) sum -= __ldg(&lS[idx]) * y_prev;
-      const double yv = (P.prec == kPrecICC) ? sum * __ldg(&P.dinv[idx]) : sum;
+      const T yv = (P.prec == kPrecICC) ? sum * __ldg(&P.dinv[idx]) : sum;
       P.y[idx] = yv;
       y_prev = yv;
       if (j == 0) y_first = yv;
@@ -344,22 +352,23 @@ __device__ void fwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r) {
 
 // Backward sweep for sweep warp k (lines nx-1-32k-t, marching j downward).  Accumulates sum z,
 // sum r.z and sum r into acc[0..2].  ICC: z = (y - sum L^T z) / d.  LDLT: z = y / D - sum L^T z.
-__device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r, double (&acc)[3]) {
+template <typename T>
+__device__ void bwd5(const PcgArgsT<T> &P, int k, unsigned int epoch, double m_r, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
   const int nx = P.A.nx, ny = P.A.ny, n = P.A.n;
   const int i = nx - 1 - (32 * k + lane);
   const bool valid = i >= 0;
   const unsigned int base = epoch * (unsigned int)(ny + 1);
-  const double *lW = P.l, *lS = P.l + n, *lN = P.l + 3 * (size_t)n, *lE = P.l + 4 * (size_t)n;
+  const T *lW = P.l, *lS = P.l + n, *lN = P.l + 3 * (size_t)n, *lE = P.l + 4 * (size_t)n;
   // the whole forward sweep must be finished (its last warp publishes ny columns last)
   if (k == 0) {
     if (wait_flag(&P.prog_f[P.nsweep - 1], base + (unsigned int)ny, P.status) == 0) return;
   }
-  double z_prev = 0.0, z_first = 0.0, z_step = 0.0;
+  T z_prev = T(0), z_first = T(0), z_step = T(0);
   unsigned int avail = 0;
   for (int s = 0; s < ny + 31; ++s) {
     const int j = ny - 1 - (s - lane);
-    double z_dn = __shfl_up_sync(0xffffffffu, z_step, 1);
+    T z_dn = __shfl_up_sync(0xffffffffu, z_step, 1);
     if (k > 0 && s < ny) {
       if ((unsigned int)s >= avail) {
         const unsigned int v = wait_flag(&P.prog_b[k - 1], base + (unsigned int)s + 1u, P.status);
@@ -370,8 +379,8 @@ __device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r, do
     }
     if (valid && j >= 0 && j < ny) {
       const size_t idx = (size_t)i * ny + j;
-      const double yv = __ldcg(&P.y[idx]);
-      double sum = (P.prec == kPrecICC) ? yv : yv * __ldg(&P.dinv[idx]);
+      const T yv = __ldcg(&P.y[idx]);
+      T sum = (P.prec == kPrecICC) ? yv : yv * __ldg(&P.dinv[idx]);
       if (j + 1 < ny) sum -= __ldg(&lS[idx + 1]) * z_prev;
       if (P.A.py && j == 0) sum -= __ldg(&lN[(size_t)i * ny + ny - 1]) * z_first;
       if (i + 1 < nx) sum -= __ldg(&lW[idx + ny]) * z_dn;
@@ -379,14 +388,14 @@ __device__ void bwd5(const PcgArgs &P, int k, unsigned int epoch, double m_r, do
         const size_t e = (size_t)(nx - 1) * ny + j;
         sum -= __ldg(&lE[e]) * __ldcg(&P.z[e]);
       }
-      const double zv = (P.prec == kPrecICC) ? sum * __ldg(&P.dinv[idx]) : sum;
+      const T zv = (P.prec == kPrecICC) ? sum * __ldg(&P.dinv[idx]) : sum;
       P.z[idx] = zv;
       z_prev = zv;
       if (j == ny - 1) z_first = zv;
       z_step = zv;
-      const double rv = __ldcg(&P.r[idx]) - m_r;
+      const T rv = __ldcg(&P.r[idx]) - (T)m_r;
       acc[0] += zv;
-      acc[1] += rv * zv;
+      acc[1] += (double)rv * (double)zv;
       acc[2] += rv;
     }
     const int done = s - 30;
@@ -472,13 +481,13 @@ __device__ void apply_levels(const PcgArgs &P, double m_r, double (&acc)[3]) {
 // The residual r is kept unprojected in memory; the mean of the latest update (m_r) is subtracted on the
 // fly by the preconditioner and folded in by the next update, which equals projecting r after every
 // update (pressure.cpp:225-239 applied in ch_sparse_krylov.hpp:602-605).
-template <int S, int SWEEP>
-__global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
+template <int S, int SWEEP, typename T = double>
+__global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
   __shared__ double sh[8 * 32 + 8];
   extern __shared__ __align__(16) char dsm[];
   const GridBarrier bar{P.bar_count, P.bar_gen, P.status, gridDim.x};
   int parity = 0;
-  const SpOp &A = P.A;
+  const SpOpT<T> &A = P.A;
   const int n = A.n, ny = A.ny;
   const double dn_ = (double)n;
   const long long per = (n + gridDim.x - 1) / gridDim.x;
@@ -490,7 +499,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
     if (threadIdx.x < 16) cnt_cta[threadIdx.x] = 0u;
     // cross-CTA hand-over lines start empty; the first grid reduction orders this before any sweep
     const size_t nb = 2 * (size_t)P.s5.nsweep * P.s5.ny;
-    const double empty = __longlong_as_double((long long)kHandEmpty);
+    const T empty = hand_empty_value<T>();
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
       P.s5.bnd_f[t] = empty;
       P.s5.bnd_b[t] = empty;
@@ -502,11 +511,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   double v3[3] = {0.0, 0.0, 0.0};
   for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
     const int i = (int)(r / ny), j = (int)(r % ny);
-    const double rr = P.b[r] - spmv_row<S>(A, P.x, i, j);
+    const T rr = P.b[r] - spmv_row<S>(A, P.x, i, j);
     P.r[r] = rr;
-    v3[0] += rr;
-    v3[1] += rr * rr;
-    v3[2] += P.b[r] * P.b[r];
+    const double rd = rr, bd = P.b[r];
+    v3[0] += rd;
+    v3[1] += rd * rd;
+    v3[2] += bd * bd;
   }
   if (!grid_sum<3>(v3, P.partials, parity, sh, bar)) return;
   double m_r = P.project ? v3[0] / dn_ : 0.0;
@@ -516,7 +526,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   double relr = absr / fmax(rhs_norm, 1.0e-30);
   int iterations = 0;
   double iter_res = 0.0;
-  if (relr < P.tol || absr < P.tol) {  // x stays x0 (the reference projects r only)
+  if (relr < P.tol || absr < P.tol_abs) {  // x stays x0 (the reference projects r only)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       P.out[0] = 0;
       P.out[1] = absr;
@@ -559,14 +569,17 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
         }
       }
     } else if (SWEEP == 1) {
-      if (blockIdx.x == 0) apply_levels<S>(P, m_r_now, acc);
+      if constexpr (sizeof(T) == sizeof(double)) {
+        if (blockIdx.x == 0) apply_levels<S>(P, m_r_now, acc);
+      }
     } else {
+      const T m = (T)m_r_now;
       for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
-        const double rv = P.r[r] - m_r_now;
-        const double zv = P.dinv[r] * rv;
+        const T rv = P.r[r] - m;
+        const T zv = P.dinv[r] * rv;
         P.z[r] = zv;
         acc[0] += zv;
-        acc[1] += rv * zv;
+        acc[1] += (double)rv * (double)zv;
         acc[2] += rv;
       }
     }
@@ -585,31 +598,33 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
   }
   double beta = 0.0;
   double m_x = 0.0;
-  double *p_old = P.p0, *p_new = P.p1;
+  T *p_old = P.p0, *p_new = P.p1;
   bool first = true;
   const int limit = P.max_it > 1 ? P.max_it : 1;
   for (int it = 0; it < limit; ++it) {
     // ---- P1: p = z - m_z + beta p_old ; Ap = A p  (p at neighbours formed on the fly)
     t0 = global_ns();
+    const T m_z_t = (T)m_z, beta_t = (T)beta;
     double v[3] = {0.0, 0.0, 0.0};
     for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
       const int i = (int)(r / ny), j = (int)(r % ny);
-      double apv = 0.0;
+      T apv = T(0);
 #pragma unroll
       for (int s = 0; s < S; ++s) {
-        const double a = A.a[(size_t)s * n + r];
-        if (a != 0.0) {
+        const T a = A.a[(size_t)s * n + r];
+        if (a != T(0)) {
           const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
-          const double pc = first ? (P.z[c] - m_z) : (P.z[c] - m_z) + beta * p_old[c];
+          const T pc = first ? (P.z[c] - m_z_t) : (P.z[c] - m_z_t) + beta_t * p_old[c];
           apv += a * pc;
         }
       }
-      const double pr = first ? (P.z[r] - m_z) : (P.z[r] - m_z) + beta * p_old[r];
+      const T pr = first ? (P.z[r] - m_z_t) : (P.z[r] - m_z_t) + beta_t * p_old[r];
       p_new[r] = pr;
       P.ap[r] = apv;
-      v[0] += pr;
-      v[1] += pr * apv;
-      v[2] += apv;
+      const double prd = pr, apd = apv;
+      v[0] += prd;
+      v[1] += prd * apd;
+      v[2] += apd;
     }
     if (!grid_sum<3>(v, P.partials, parity, sh, bar)) return;
     const double m_p = P.project ? v[0] / dn_ : 0.0;
@@ -622,20 +637,22 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
     const unsigned long long t1 = global_ns();
     t_p1 += t1 - t0;
     // ---- P2: x += alpha p ; r -= alpha Ap ; norms (ch_sparse_krylov.hpp:592-610)
+    const T m_p_t = (T)m_p, alpha_t = (T)alpha, m_x_t = (T)m_x, m_r_t = (T)m_r;
     double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
-      const double pp = p_new[r] - m_p;
+      const T pp = p_new[r] - m_p_t;
       p_new[r] = pp;
-      const double delta = alpha * pp;
-      const double xv = (P.x[r] - m_x) + delta;
+      const T delta = alpha_t * pp;
+      const T xv = (P.x[r] - m_x_t) + delta;
       P.x[r] = xv;
-      const double rv = (P.r[r] - m_r) - alpha * P.ap[r];
+      const T rv = (P.r[r] - m_r_t) - alpha_t * P.ap[r];
       P.r[r] = rv;
-      w[0] += delta * delta;
-      w[1] += xv * xv;
-      w[2] += xv;
-      w[3] += rv;
-      w[4] += rv * rv;
+      const double dd = delta, xd = xv, rd = rv;
+      w[0] += dd * dd;
+      w[1] += xd * xd;
+      w[2] += xd;
+      w[3] += rd;
+      w[4] += rd * rd;
     }
     if (!grid_sum<5>(w, P.partials, parity, sh, bar)) return;
     const unsigned long long t2 = global_ns();
@@ -647,7 +664,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
     iter_res = sqrt(w[0] / fmax(w[1], 1.0e-30));
     absr = sqrt(fmax(rn2, 0.0));
     relr = absr / fmax(rhs_norm, 1.0e-30);
-    if (relr < P.tol || absr < P.tol) break;
+    if (relr < P.tol || absr < P.tol_abs) break;
     // ---- z = M^{-1} r, project z, r.z (ch_sparse_krylov.hpp:626-635)
     if (!precondition(m_r, acc)) return;
     t_pc += global_ns() - t2;
@@ -659,14 +676,15 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgs P) {
     }
     beta = rz_new / rz_old;
     rz_old = rz_new;
-    double *t = p_old;
+    T *t = p_old;
     p_old = p_new;
     p_new = t;
     first = false;
   }
   // pending projection of x
   if (P.project && m_x != 0.0) {
-    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) P.x[r] = P.x[r] - m_x;
+    const T m_x_t = (T)m_x;
+    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) P.x[r] = P.x[r] - m_x_t;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.out[0] = (double)iterations;

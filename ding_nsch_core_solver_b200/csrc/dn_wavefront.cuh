@@ -32,31 +32,34 @@ constexpr int kHand = 8;                 // columns per boundary publication
 constexpr int kAhead = 3;                // chunks staged ahead of the one being consumed
 constexpr int kLines = 31;               // grid lines per sweep warp (lane 31 / lane 0 is the ghost)
 
-struct Sweep5 {
+// T is the storage and arithmetic type of the sweep (double, or float for the inner solves of the
+// mixed-precision form); the sums handed back (r.z, sum z, sum r) are accumulated in double either way.
+template <typename T>
+struct Sweep5T {
   int nx, ny, n, px, py;
   int prec;     // kPrecICC (2) or kPrecLDLT (1)
   int varcoef;  // 0: constant off-diagonals cx/cy (split operator); 1: per-row slots aW, aS, aN, aE
-  const double *aW, *aS, *aN, *aE;
-  double cx, cy;  // -1/dx^2, -1/dy^2 for the constant operator
-  const double *dinv;
-  const double *r;  // forward input (the pending mean m_r is subtracted on the fly)
-  double *y, *z;
-  double *bnd_f, *bnd_b;      // [2][nsweep][ny] edge lines handed between CTAs (by application parity)
-  double *wline0, *zlast;     // periodic-x wrap lines (unused by the staged path, which needs px = 0)
+  const T *aW, *aS, *aN, *aE;
+  T cx, cy;  // -1/dx^2, -1/dy^2 for the constant operator
+  const T *dinv;
+  const T *r;  // forward input (the pending mean m_r is subtracted on the fly)
+  T *y, *z;
+  T *bnd_f, *bnd_b;           // [2][nsweep][ny] edge lines handed between CTAs (by application parity)
+  T *wline0, *zlast;          // periodic-x wrap lines (unused by the staged path, which needs px = 0)
   unsigned int *prog_f, *prog_b;  // unused by the staged path (kept for the launch arguments' layout)
   int nsweep, sw;             // sweep warps in total (ceil(nx / kLines)) / per CTA
   int warp_smem;              // bytes between consecutive sweep warps' shared-memory regions
   int *status;
   double *prof;               // per sweep warp, 4 counters (ns): forward total, hand-over waits, 0, backward total
 };
+using Sweep5 = Sweep5T<double>;
 
 __host__ __device__ inline int staged_sweep_warps(int nx) { return (nx + kLines - 1) / kLines; }
 
-// per-warp shared-memory footprint (bytes) for `na` staged arrays, a ny-long hand-over line and the
-// zero / unit rows read by lanes that own no line
-__host__ __device__ inline size_t sweep_warp_smem(int na, int ny) {
-  return (size_t)na * 32 * kPitch * sizeof(double) + (size_t)((ny + 1) & ~1) * sizeof(double) +
-         2 * (size_t)kPitch * sizeof(double) + 64;
+// per-warp shared-memory footprint (bytes) for `na` staged arrays of `esize`-byte elements, a ny-long
+// hand-over line and the zero / unit rows read by lanes that own no line
+__host__ __device__ inline size_t sweep_warp_smem(int na, int ny, int esize = 8) {
+  return (size_t)na * 32 * kPitch * esize + (size_t)((ny + 3) & ~3) * esize + 2 * (size_t)kPitch * esize + 64;
 }
 
 __device__ __forceinline__ unsigned int ld_acquire_cta(const unsigned int *p) {
@@ -75,6 +78,10 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
 __device__ __forceinline__ void st_release_gpu(unsigned int *p, unsigned int v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
                : "memory");
@@ -82,6 +89,13 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
                : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem) {
+  if (sizeof(T) == 8)
+    cp_async8(smem, gmem);
+  else
+    cp_async4(smem, gmem);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_ahead() { asm volatile("cp.async.wait_group 3;" ::: "memory"); }
@@ -92,13 +106,30 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 // values themselves (relaxed GPU-scope loads) and writes the sentinel back after use.  Buffers alternate
 // by application parity, so a reset lands two applications (and several grid barriers) before reuse.
 constexpr unsigned long long kHandEmpty = 0x7ff4dead5eed0001ull;
+constexpr unsigned int kHandEmpty32 = 0x7fa5eed1u;
 __device__ __forceinline__ double ld_relaxed_gpu(const double *p) {
   double v;
   asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ float ld_relaxed_gpu(const float *p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ bool hand_empty(double v) {
   return (unsigned long long)__double_as_longlong(v) == kHandEmpty;
+}
+__device__ __forceinline__ bool hand_empty(float v) { return (unsigned int)__float_as_uint(v) == kHandEmpty32; }
+template <typename T>
+__device__ __forceinline__ T hand_empty_value();
+template <>
+__device__ __forceinline__ double hand_empty_value<double>() {
+  return __longlong_as_double((long long)kHandEmpty);
+}
+template <>
+__device__ __forceinline__ float hand_empty_value<float>() {
+  return __uint_as_float(kHandEmpty32);
 }
 
 // Stores under a per-lane predicate without a branch: the warp stays converged for the shuffle that
@@ -110,6 +141,16 @@ __device__ __forceinline__ void st_global_if(double *p, double v, bool pred) {
 }
 __device__ __forceinline__ void st_generic_if(double *p, double v, bool pred) {
   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.f64 [%0], %1;\n\t}" ::"l"(p), "d"(v),
+               "r"((int)pred)
+               : "memory");
+}
+__device__ __forceinline__ void st_global_if(float *p, float v, bool pred) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.global.f32 [%0], %1;\n\t}" ::"l"(p), "f"(v),
+               "r"((int)pred)
+               : "memory");
+}
+__device__ __forceinline__ void st_generic_if(float *p, float v, bool pred) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.f32 [%0], %1;\n\t}" ::"l"(p), "f"(v),
                "r"((int)pred)
                : "memory");
 }
@@ -137,21 +178,22 @@ __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, u
 
 // Stage columns [c0, c1) of `nl` grid lines starting at line i0 into ring rows row0 .. row0+nl-1.  Column j
 // goes to row offset off + (j & 63); the mirrored columns are written twice (forward: slots 0..7 again at
-// 64..71, off = 0; backward: slots 56..63 again at 0..7, off = 8).  16-byte pieces when ny is even.
-template <bool FWD>
-__device__ __forceinline__ void stage_cols(double *ring, const double *src, int i0, int row0, int nl, int ny, int c0,
+// 64..71, off = 0; backward: slots 56..63 again at 0..7, off = 8).  16-byte pieces when ny allows them.
+template <bool FWD, typename T>
+__device__ __forceinline__ void stage_cols(T *ring, const T *src, int i0, int row0, int nl, int ny, int c0,
                                            int c1, bool vec16) {
   const int lane = threadIdx.x & 31;
   c0 = max(c0, 0);
   c1 = min(c1, ny);
   if (c0 >= c1) return;
   constexpr int off = FWD ? 0 : kMirror;
-  if (vec16) {  // ny even: c0 and c1 are even too
-    const int npair = (c1 - c0) >> 1;
+  constexpr int E = 16 / (int)sizeof(T);  // elements per 16-byte piece
+  if (vec16) {  // ny a multiple of E: c0 and c1 are too
+    const int npair = (c1 - c0) / E;
     for (int p = lane; p < nl * npair; p += 32) {
-      const int line = p / npair, j = c0 + 2 * (p - line * npair);
-      const double *g = &src[(size_t)(i0 + line) * ny + j];
-      double *row = ring + (size_t)(row0 + line) * kPitch;
+      const int line = p / npair, j = c0 + E * (p - line * npair);
+      const T *g = &src[(size_t)(i0 + line) * ny + j];
+      T *row = ring + (size_t)(row0 + line) * kPitch;
       const int slot = j & (kRing - 1);
       cp_async16(&row[off + slot], g);
       if (FWD ? (slot < kMirror) : (slot >= kRing - kMirror)) cp_async16(&row[FWD ? kRing + slot : slot - (kRing - kMirror)], g);
@@ -160,26 +202,30 @@ __device__ __forceinline__ void stage_cols(double *ring, const double *src, int 
     const int ncol = c1 - c0;
     for (int p = lane; p < nl * ncol; p += 32) {
       const int line = p / ncol, j = c0 + (p - line * ncol);
-      const double *g = &src[(size_t)(i0 + line) * ny + j];
-      double *row = ring + (size_t)(row0 + line) * kPitch;
+      const T *g = &src[(size_t)(i0 + line) * ny + j];
+      T *row = ring + (size_t)(row0 + line) * kPitch;
       const int slot = j & (kRing - 1);
-      cp_async8(&row[off + slot], g);
-      if (FWD ? (slot < kMirror) : (slot >= kRing - kMirror)) cp_async8(&row[FWD ? kRing + slot : slot - (kRing - kMirror)], g);
+      cp_async_elem<T>(&row[off + slot], g);
+      if (FWD ? (slot < kMirror) : (slot >= kRing - kMirror))
+        cp_async_elem<T>(&row[FWD ? kRing + slot : slot - (kRing - kMirror)], g);
     }
   }
 }
 
-// Stage one whole 8-column chunk [c0, c0+8) (ny even; for the backward ring also ny % 8 == 0, so that
-// the chunk sits at an 8-aligned ring slot): lane t copies columns c0 + 2 (t & 3) + {0, 1} of lines
-// (t >> 2) + 8 it, it = 0..3, with one 16-byte cp.async per array -- no division, addresses from one
-// per-lane offset.  The chunk at the mirrored slot is copied a second time (forward: slot 0 again at 64,
+// Stage one whole 8-column chunk [c0, c0+8) (ny a multiple of the 16-byte piece; for the backward ring
+// also ny % 8 == 0, so that the chunk sits at an 8-aligned ring slot): in doubles, lane t copies columns
+// c0 + 2 (t & 3) + {0, 1} of lines (t >> 2) + 8 it, it = 0..3 (in floats, four columns of lines
+// (t >> 1) + 16 it), one 16-byte cp.async per array -- no division, addresses from one per-lane offset.  The chunk at the mirrored slot is copied a second time (forward: slot 0 again at 64,
 // backward: slot 56 again at 0).
-template <bool FWD, int NA>
-__device__ __forceinline__ void stage_full(double *r0, double *r1, double *r2, double *r3, const double *s0,
-                                           const double *s1, const double *s2, const double *s3, int i0, int row0,
-                                           int nl, int ny, int c0) {
+template <bool FWD, int NA, typename T>
+__device__ __forceinline__ void stage_full(T *r0, T *r1, T *r2, T *r3, const T *s0, const T *s1, const T *s2,
+                                           const T *s3, int i0, int row0, int nl, int ny, int c0) {
+  constexpr int E = 16 / (int)sizeof(T);  // elements per 16-byte piece
+  constexpr int PL = kChunk / E;          // pieces per line of the chunk
+  constexpr int LI = 32 / PL;             // lines per pass of the warp
+  constexpr int IT = (kLines + LI - 1) / LI;
   const int lane = threadIdx.x & 31;
-  const int l0 = lane >> 2, cc = 2 * (lane & 3);
+  const int l0 = lane / PL, cc = E * (lane % PL);
   const int slot = c0 & (kRing - 1);
   constexpr int off = FWD ? 0 : kMirror;
   const bool mirror = FWD ? (slot == 0) : (slot == kRing - kChunk);
@@ -187,10 +233,10 @@ __device__ __forceinline__ void stage_full(double *r0, double *r1, double *r2, d
   const size_t gofs = (size_t)(i0 + l0) * ny + c0 + cc;
   const int sofs = (row0 + l0) * kPitch + off + slot + cc;
 #pragma unroll
-  for (int it = 0; it < 4; ++it) {
-    if (l0 + 8 * it < nl) {
-      const size_t g = gofs + (size_t)(8 * it) * ny;
-      const int sd = sofs + 8 * it * kPitch;
+  for (int it = 0; it < IT; ++it) {
+    if (l0 + LI * it < nl) {
+      const size_t g = gofs + (size_t)(LI * it) * ny;
+      const int sd = sofs + LI * it * kPitch;
       cp_async16(r0 + sd, s0 + g);
       cp_async16(r1 + sd, s1 + g);
       if (NA == 4) {
@@ -213,20 +259,20 @@ __device__ __forceinline__ void stage_full(double *r0, double *r1, double *r2, d
 // 1..nl own lines 31k .. 31k+nl-1; lane t runs t steps behind the ghost.  Accumulates rz (= y^T y for
 // ICC, y^T D^-1 y for ILDLT) and the sum of the projected residual into acc[1], acc[2].  Steps run in
 // groups of kHand: the hand-over check precedes a group, the publication follows it.
-template <bool ICC, bool VAR>
-__device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
+template <bool ICC, bool VAR, typename T = double>
+__device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
                                             unsigned int epoch, double m_r, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
   const int nx = P.nx, ny = P.ny, nsweep = P.nsweep, sw = P.sw;
   const int py = P.py;
-  const double cx = P.cx, cy = P.cy;
-  double *const yout = P.y;
-  const double *const gr = P.r;
-  const double *const gd = P.dinv;
-  const double *const gW = P.aW;
-  const double *const gS = P.aS;
-  const double *const gN = P.aN;
-  double *const bnd_f = P.bnd_f;
+  const T cx = P.cx, cy = P.cy;
+  T *const yout = P.y;
+  const T *const gr = P.r;
+  const T *const gd = P.dinv;
+  const T *const gW = P.aW;
+  const T *const gS = P.aS;
+  const T *const gN = P.aN;
+  T *const bnd_f = P.bnd_f;
   int *const status = P.status;
   double *const prof = P.prof;
   const int i0 = kLines * k;
@@ -236,14 +282,14 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   const bool lin = (lane == 0) && has_prod;  // the ghost replays the hand-over line
   const int i = i0 + lane - 1;
   constexpr int na = VAR ? 4 : 2;
-  double *ring_r = (double *)smem_warp;
-  double *ring_d = ring_r + 32 * kPitch;
-  double *ring_w = ring_d + 32 * kPitch;
-  double *ring_s = ring_w + 32 * kPitch;
-  double *bline = ring_r + (size_t)na * 32 * kPitch;
-  double *zrow = bline + ((ny + 1) & ~1);
-  double *ones = zrow + kPitch;
-  const bool vec16 = (ny % 2) == 0;
+  T *ring_r = (T *)smem_warp;
+  T *ring_d = ring_r + 32 * kPitch;
+  T *ring_w = ring_d + 32 * kPitch;
+  T *ring_s = ring_w + 32 * kPitch;
+  T *bline = ring_r + (size_t)na * 32 * kPitch;
+  T *zrow = bline + ((ny + 3) & ~3);
+  T *ones = zrow + kPitch;
+  const bool vec16 = (ny % (16 / (int)sizeof(T))) == 0;  // 16-byte pieces
   const bool prod_local = has_prod && (ws > 0);
   const bool has_cons = (k + 1 < nsweep);
   const bool cons_local = has_cons && (ws + 1 < sw);
@@ -253,28 +299,28 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   unsigned int *my_cnt = &cnt_cta[2 * ws];
   unsigned int *next_cnt = &cnt_cta[2 * (ws + 1)];
   // per-lane rows: real lanes their ring rows, the ghost unit dinv, everything else zeros
-  const double *r_row = real ? ring_r + lane * kPitch : zrow;
-  const double *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
-  const double *w_row = real ? ring_w + lane * kPitch : zrow;
-  const double *s_row = real ? ring_s + lane * kPitch : zrow;
-  const double m_lane = real ? m_r : 0.0;
-  const double as_c = real ? cy : 0.0;
-  const double aw_c = (real && i > 0) ? cx : 0.0;
-  double *const ydst = yout + (size_t)(real ? i : 0) * ny;
+  const T *r_row = real ? ring_r + lane * kPitch : zrow;
+  const T *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
+  const T *w_row = real ? ring_w + lane * kPitch : zrow;
+  const T *s_row = real ? ring_s + lane * kPitch : zrow;
+  const T m_lane = real ? (T)m_r : T(0);
+  const T as_c = real ? cy : T(0);
+  const T aw_c = (real && i > 0) ? cx : T(0);
+  T *const ydst = yout + (size_t)(real ? i : 0) * ny;
   const bool hand = has_cons && lane == 31;  // a warp with a consumer has nl = 31
-  double *const hdst = cons_local ? (double *)(smem_warp + P.warp_smem) + (size_t)na * 32 * kPitch
+  T *const hdst = cons_local ? (T *)(smem_warp + P.warp_smem) + (size_t)na * 32 * kPitch
                                   : bnd_f + ((size_t)(epoch & 1u) * nsweep + k) * ny;
   auto stage = [&](int c) {
     const int c0 = c * kChunk;
     if (c0 < ny) {
       if (vec16 && c0 + kChunk <= ny) {
-        stage_full<true, na>(ring_r, ring_d, ring_w, ring_s, gr, gd, gW, gS, i0, 1, nl, ny, c0);
+        stage_full<true, na, T>(ring_r, ring_d, ring_w, ring_s, gr, gd, gW, gS, i0, 1, nl, ny, c0);
       } else {
-        stage_cols<true>(ring_r, gr, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
-        stage_cols<true>(ring_d, gd, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+        stage_cols<true, T>(ring_r, gr, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+        stage_cols<true, T>(ring_d, gd, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
         if (VAR) {
-          stage_cols<true>(ring_w, gW, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
-          stage_cols<true>(ring_s, gS, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+          stage_cols<true, T>(ring_w, gW, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
+          stage_cols<true, T>(ring_s, gS, i0, 1, nl, ny, c0, c0 + kChunk, vec16);
         }
       }
     }
@@ -283,19 +329,19 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
   const unsigned long long t_begin = global_ns();
   unsigned long long t_wait = 0;
   for (int t = lane; t < kPitch; t += 32) {
-    zrow[t] = 0.0;
-    ones[t] = 1.0;
+    zrow[t] = T(0);
+    ones[t] = T(1);
   }
   // A producer in another CTA hands its line over through global memory: the values of group c are loaded
   // kAhead groups early (issued at the start of a group, landed in the shared line at its end).
   const bool remote = has_prod && !prod_local;
   unsigned int avail = 0;
-  double *const hin = has_prod ? bnd_f + ((size_t)(epoch & 1u) * nsweep + (k - 1)) * ny : nullptr;
-  auto hand_issue = [&](int c) -> double {
+  T *const hin = has_prod ? bnd_f + ((size_t)(epoch & 1u) * nsweep + (k - 1)) * ny : nullptr;
+  auto hand_issue = [&](int c) -> T {
     const int col = c * kChunk + lane;
-    return (lane < kHand && col < ny) ? ld_relaxed_gpu(hin + col) : 0.0;
+    return (lane < kHand && col < ny) ? ld_relaxed_gpu(hin + col) : T(0);
   };
-  auto hand_land = [&](int c, double v) -> bool {
+  auto hand_land = [&](int c, T v) -> bool {
     const int col = c * kChunk + lane;
     const bool mine = lane < kHand && col < ny;
     bool miss = mine && hand_empty(v);
@@ -318,7 +364,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
     }
     if (mine) {
       bline[col] = v;
-      hin[col] = __longlong_as_double((long long)kHandEmpty);
+      hin[col] = hand_empty_value<T>();
     }
     __syncwarp();
     return true;
@@ -330,10 +376,11 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
     }
     stage(c);
   }
-  double w_prev = 0.0, w_first = 0.0, rz = 0.0, rsum = 0.0;
+  T w_prev = T(0), w_first = T(0);
+  double rz = 0.0, rsum = 0.0;  // r.z and sum r accumulate in double
   for (int q = 0; q < nchunk; ++q) {
     stage(q + kAhead);
-    const double hv = remote ? hand_issue(q + kAhead) : 0.0;
+    const T hv = remote ? hand_issue(q + kAhead) : T(0);
     cp_async_wait_ahead();
     __syncwarp();
     const int s0 = q * kChunk;
@@ -355,13 +402,13 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
       // steady state: every lane's column lies in [1, ny-2]; fixed offsets from one base per array
       const int j0 = s0 - lane;
       const int slot = j0 & (kRing - 1);
-      const double *rb = lin ? bline + j0 : r_row + slot;
-      const double *db = d_row + slot;
-      const double *wb = w_row + slot;
-      const double *sb = s_row + slot;
-      double *yp = ydst + j0;
-      double *hp = hdst + j0;
-      double rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
+      const T *rb = lin ? bline + j0 : r_row + slot;
+      const T *db = d_row + slot;
+      const T *wb = w_row + slot;
+      const T *sb = s_row + slot;
+      T *yp = ydst + j0;
+      T *hp = hdst + j0;
+      T rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         rvv[ss] = rb[ss];
@@ -371,17 +418,17 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
       }
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
-        const double rv = rvv[ss] - m_lane;
-        const double dv = dvv[ss];
-        const double as = asv[ss];
-        const double aw = awv[ss];
-        const double t1 = fma(-as, w_prev, rv);
-        const double w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
-        const double sum = fma(-aw, w_up, t1);
-        const double yv = ICC ? sum * dv : sum;
-        const double wv = sum * (ICC ? dv * dv : dv);
+        const T rv = rvv[ss] - m_lane;
+        const T dv = dvv[ss];
+        const T as = asv[ss];
+        const T aw = awv[ss];
+        const T t1 = fma(-as, w_prev, rv);
+        const T w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
+        const T sum = fma(-aw, w_up, t1);
+        const T yv = ICC ? sum * dv : sum;
+        const T wv = sum * (ICC ? dv * dv : dv);
         st_global_if(yp + ss, yv, real);
-        rz = fma(yv, ICC ? yv : wv, rz);
+        rz = fma((double)yv, (double)(ICC ? yv : wv), rz);
         rsum += rv;
         st_generic_if(hp + ss, wv, hand);
         w_prev = wv;
@@ -391,11 +438,11 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
       // the steady arithmetic, with the carried state, the stores and the sums gated by the column range
       const int j0 = s0 - lane;
       const int slot = j0 & (kRing - 1);
-      const double *rb = lin ? bline + j0 : r_row + slot;
-      const double *db = d_row + slot;
-      const double *wb = w_row + slot;
-      const double *sb = s_row + slot;
-      double rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
+      const T *rb = lin ? bline + j0 : r_row + slot;
+      const T *db = d_row + slot;
+      const T *wb = w_row + slot;
+      const T *sb = s_row + slot;
+      T rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         rvv[ss] = rb[ss];
@@ -407,19 +454,19 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
       for (int ss = 0; ss < kHand; ++ss) {
         const int j = j0 + ss;
         const bool act = j >= 0 && j < ny;
-        const double rv = rvv[ss] - m_lane;
-        const double dv = dvv[ss];
+        const T rv = rvv[ss] - m_lane;
+        const T dv = dvv[ss];
         // own-line terms first (periodic-y wrap, S), so that one FMA follows the shuffle from line i-1; a
         // lane's first active step has w_prev = 0, so the S term vanishes at j = 0
-        double t1 = rv;
+        T t1 = rv;
         if (py && j == ny - 1 && real) t1 = fma(-(VAR ? gN[(size_t)i * ny + j] : cy), w_first, t1);
         t1 = fma(-asv[ss], w_prev, t1);
-        const double w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
-        const double sum = fma(-awv[ss], w_up, t1);
-        const double yv = ICC ? sum * dv : sum;
-        const double wv = sum * (ICC ? dv * dv : dv);
+        const T w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
+        const T sum = fma(-awv[ss], w_up, t1);
+        const T yv = ICC ? sum * dv : sum;
+        const T wv = sum * (ICC ? dv * dv : dv);
         st_global_if(ydst + j, yv, act && real);
-        rz = (act && real) ? fma(yv, ICC ? yv : wv, rz) : rz;
+        rz = (act && real) ? fma((double)yv, (double)(ICC ? yv : wv), rz) : rz;
         rsum = (act && real) ? rsum + rv : rsum;
         st_generic_if(hdst + j, wv, act && hand);
         w_first = (py && j == 0) ? wv : w_first;
@@ -457,20 +504,20 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5 &P, char *smem_warp, un
 // Backward sweep of sweep warp k.  Lanes 0..nl-1 own lines 31k .. 31k+nl-1; lane 31 is the ghost of line
 // 31k+31 when a next warp exists.  The lead lane (the ghost, or the last real lane of the last warp) runs
 // first, lane t (lead-t) steps behind it.  Accumulates the sum of z into acc[0].
-template <bool ICC, bool VAR>
-__device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
+template <bool ICC, bool VAR, typename T = double>
+__device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
                                             unsigned int epoch, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
   const int nx = P.nx, ny = P.ny, nsweep = P.nsweep, sw = P.sw;
   const int py = P.py;
-  const double cx = P.cx, cy = P.cy;
-  double *const zout = P.z;
-  const double *const gy = P.y;
-  const double *const gd = P.dinv;
-  const double *const gN = P.aN;
-  const double *const gE = P.aE;
-  const double *const gS = P.aS;
-  double *const bnd_b = P.bnd_b;
+  const T cx = P.cx, cy = P.cy;
+  T *const zout = P.z;
+  const T *const gy = P.y;
+  const T *const gd = P.dinv;
+  const T *const gN = P.aN;
+  const T *const gE = P.aE;
+  const T *const gS = P.aS;
+  T *const bnd_b = P.bnd_b;
   int *const status = P.status;
   double *const prof = P.prof;
   const int i0 = kLines * k;
@@ -485,40 +532,40 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
   const int skew = lead - lane;  // negative for the idle lanes above the lead of the last warp
   const int i = i0 + lane;
   constexpr int na = VAR ? 4 : 2;
-  double *ring_y = (double *)smem_warp;
-  double *ring_d = ring_y + 32 * kPitch;
-  double *ring_n = ring_d + 32 * kPitch;
-  double *ring_e = ring_n + 32 * kPitch;
-  double *bline = ring_y + (size_t)na * 32 * kPitch;
-  double *zrow = bline + ((ny + 1) & ~1);
-  double *ones = zrow + kPitch;
-  const bool vec16 = (ny % 2) == 0;
+  T *ring_y = (T *)smem_warp;
+  T *ring_d = ring_y + 32 * kPitch;
+  T *ring_n = ring_d + 32 * kPitch;
+  T *ring_e = ring_n + 32 * kPitch;
+  T *bline = ring_y + (size_t)na * 32 * kPitch;
+  T *zrow = bline + ((ny + 3) & ~3);
+  T *ones = zrow + kPitch;
+  const bool vec16 = (ny % (16 / (int)sizeof(T))) == 0;  // 16-byte pieces
   const unsigned int base = epoch * (unsigned int)(ny + 1);
   const int total = ny + lead;
   const int nchunk = (total + kChunk - 1) / kChunk;
   unsigned int *my_cnt = &cnt_cta[2 * ws + 1];
   unsigned int *prev_cnt = &cnt_cta[2 * (ws - 1) + 1];
-  const double *y_row = real ? ring_y + lane * kPitch : zrow;
-  const double *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
-  const double *n_row = real ? ring_n + lane * kPitch : zrow;
-  const double *e_row = real ? ring_e + lane * kPitch : zrow;
-  const double an_c = real ? cy : 0.0;
-  const double ae_c = (real && i + 1 < nx) ? cx : 0.0;
-  double *const zdst = zout + (size_t)(real ? i : 0) * ny;
+  const T *y_row = real ? ring_y + lane * kPitch : zrow;
+  const T *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
+  const T *n_row = real ? ring_n + lane * kPitch : zrow;
+  const T *e_row = real ? ring_e + lane * kPitch : zrow;
+  const T an_c = real ? cy : T(0);
+  const T ae_c = (real && i + 1 < nx) ? cx : T(0);
+  T *const zdst = zout + (size_t)(real ? i : 0) * ny;
   const bool hand = has_cons && lane == 0;
-  double *const hdst = cons_local ? (double *)(smem_warp - P.warp_smem) + (size_t)na * 32 * kPitch
+  T *const hdst = cons_local ? (T *)(smem_warp - P.warp_smem) + (size_t)na * 32 * kPitch
                                   : bnd_b + ((size_t)(epoch & 1u) * nsweep + k) * ny;
   auto stage = [&](int c) {
     const int c1 = ny - kChunk * c;
     if (c1 > 0) {
       if (vec16 && (ny % kChunk) == 0) {
-        stage_full<false, na>(ring_y, ring_d, ring_n, ring_e, gy, gd, gN, gE, i0, 0, nl, ny, c1 - kChunk);
+        stage_full<false, na, T>(ring_y, ring_d, ring_n, ring_e, gy, gd, gN, gE, i0, 0, nl, ny, c1 - kChunk);
       } else {
-        stage_cols<false>(ring_y, gy, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
-        stage_cols<false>(ring_d, gd, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+        stage_cols<false, T>(ring_y, gy, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+        stage_cols<false, T>(ring_d, gd, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
         if (VAR) {
-          stage_cols<false>(ring_n, gN, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
-          stage_cols<false>(ring_e, gE, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+          stage_cols<false, T>(ring_n, gN, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
+          stage_cols<false, T>(ring_e, gE, i0, 0, nl, ny, c1 - kChunk, c1, vec16);
         }
       }
     }
@@ -527,17 +574,17 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
   __syncwarp();  // y of these lines was written by this warp's forward sweep
   const unsigned long long t_begin = global_ns();
   for (int t = lane; t < kPitch; t += 32) {
-    zrow[t] = 0.0;
-    ones[t] = 1.0;
+    zrow[t] = T(0);
+    ones[t] = T(1);
   }
   // a producer in another CTA: values loaded kAhead groups early and polled, as in the forward sweep
   const bool remote = has_prod && !prod_local;
-  double *const hin = has_prod ? bnd_b + ((size_t)(epoch & 1u) * nsweep + (k + 1)) * ny : nullptr;
-  auto hand_issue = [&](int c) -> double {
+  T *const hin = has_prod ? bnd_b + ((size_t)(epoch & 1u) * nsweep + (k + 1)) * ny : nullptr;
+  auto hand_issue = [&](int c) -> T {
     const int col = ny - 1 - (c * kChunk + lane);
-    return (lane < kHand && col >= 0) ? ld_relaxed_gpu(hin + col) : 0.0;
+    return (lane < kHand && col >= 0) ? ld_relaxed_gpu(hin + col) : T(0);
   };
-  auto hand_land = [&](int c, double v) -> bool {
+  auto hand_land = [&](int c, T v) -> bool {
     const int col = ny - 1 - (c * kChunk + lane);
     const bool mine = lane < kHand && col >= 0;
     bool miss = mine && hand_empty(v);
@@ -556,7 +603,7 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
     }
     if (mine) {
       bline[col] = v;
-      hin[col] = __longlong_as_double((long long)kHandEmpty);
+      hin[col] = hand_empty_value<T>();
     }
     __syncwarp();
     return true;
@@ -569,10 +616,11 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
     }
     stage(c);
   }
-  double z_prev = 0.0, z_first = 0.0, zsum = 0.0;
+  T z_prev = T(0), z_first = T(0);
+  double zsum = 0.0;
   for (int q = 0; q < nchunk; ++q) {
     stage(q + kAhead);
-    const double hv = remote ? hand_issue(q + kAhead) : 0.0;
+    const T hv = remote ? hand_issue(q + kAhead) : T(0);
     cp_async_wait_ahead();
     __syncwarp();
     const int s0 = q * kChunk;
@@ -592,13 +640,13 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
       // steady state: every real lane's column lies in [1, ny-2]
       const int jt = ny - 1 - (s0 - skew);
       const int slot = jt & (kRing - 1);
-      const double *yb = lin ? bline + jt : y_row + kMirror + slot;
-      const double *db = d_row + kMirror + slot;
-      const double *nb = n_row + kMirror + slot;
-      const double *eb = e_row + kMirror + slot;
-      double *zp = zdst + jt;
-      double *hp = hdst + jt;
-      double yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
+      const T *yb = lin ? bline + jt : y_row + kMirror + slot;
+      const T *db = d_row + kMirror + slot;
+      const T *nb = n_row + kMirror + slot;
+      const T *eb = e_row + kMirror + slot;
+      T *zp = zdst + jt;
+      T *hp = hdst + jt;
+      T yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         yvv[ss] = yb[-ss];
@@ -608,13 +656,13 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
       }
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
-        const double yv = yvv[ss];
-        const double dv = dvv[ss];
-        const double an = anv[ss];
-        const double ae = aev[ss];
-        const double t = an * z_prev;
-        const double z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
-        const double zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
+        const T yv = yvv[ss];
+        const T dv = dvv[ss];
+        const T an = anv[ss];
+        const T ae = aev[ss];
+        const T t = an * z_prev;
+        const T z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
+        const T zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
         st_global_if(zp - ss, zv, real);
         zsum += zv;
         st_generic_if(hp - ss, zv, hand);
@@ -625,11 +673,11 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
       // column range; a lane's first active step has z_prev = 0, so the N term vanishes at j = ny-1
       const int jt = ny - 1 - (s0 - skew);
       const int slot = jt & (kRing - 1);
-      const double *yb = lin ? bline + jt : y_row + kMirror + slot;
-      const double *db = d_row + kMirror + slot;
-      const double *nb = n_row + kMirror + slot;
-      const double *eb = e_row + kMirror + slot;
-      double yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
+      const T *yb = lin ? bline + jt : y_row + kMirror + slot;
+      const T *db = d_row + kMirror + slot;
+      const T *nb = n_row + kMirror + slot;
+      const T *eb = e_row + kMirror + slot;
+      T yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         yvv[ss] = yb[-ss];
@@ -641,16 +689,16 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5 &P, char *smem_warp, un
       for (int ss = 0; ss < kHand; ++ss) {
         const int j = jt - ss;
         const bool act = j >= 0 && j < ny;
-        const double yv = yvv[ss];
-        const double dv = dvv[ss];
-        const double ae = aev[ss];
+        const T yv = yvv[ss];
+        const T dv = dvv[ss];
+        const T ae = aev[ss];
         // upper neighbours in ascending column order: (i,j+1), (i,ny-1) [j==0], (i+1,j); own-line terms
         // first, one FMA (plus the final scaling) follows the shuffle from line i+1
-        double t = anv[ss] * z_prev;
+        T t = anv[ss] * z_prev;
         if (py && j == 0 && real) t = fma(VAR ? gS[(size_t)i * ny] : cy, z_first, t);
-        const double z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
+        const T z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
         // ICC: z = (y - d t) d = y d - d^2 t ; ILDLT: z = D^-1 (y - t)
-        const double zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
+        const T zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
         st_global_if(zdst + j, zv, act && real);
         zsum = (act && real) ? zsum + zv : zsum;
         st_generic_if(hdst + j, zv, act && hand);
