@@ -373,6 +373,8 @@ struct dn_handle {
   int p_factor_kind = 0;
   // CH operator + factor
   double *a13 = nullptr, *l13 = nullptr, *d13 = nullptr, *dinv13 = nullptr;
+  Rows13 rows13{};       // ordered factor rows for the ring-based level sweeps (y not periodic)
+  bool rows13_ok = false;
   double ch_alpha0 = -1.0;
   int ch_prec = kPrecLDLT;  // kPrecLDLT or kPrecDiag
   // momentum
@@ -591,7 +593,12 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   P.out = h->scal + 8;
   P.nsweep = h->nsweep;
   P.warp_smem = 0;
+  P.rows13 = Rows13{};
   size_t dyn_smem = 0;
+  if (S == 13 && SWEEP == 1 && h->rows13.lval != nullptr) {  // ring of kLvlRing levels x nx doubles
+    P.rows13 = h->rows13;
+    dyn_smem = (size_t)kLvlRing * h->G.nx * sizeof(double);
+  }
   int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(h->nsweep, (h->n + 2047) / 2048));
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
   if (SWEEP == 3) {
@@ -988,6 +995,11 @@ dn_status ensure_ch_system(dn_handle *h, double alpha0) {
     DN_TRY(check_launch(h, "k_diag_inverse"));
   } else {
     h->ch_prec = kPrecLDLT;
+    if (h->rows13.lval != nullptr) {
+      k_rows13<<<blocks_for(h->n), 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, F,
+                                                       h->rows13);
+      DN_TRY(check_launch(h, "k_rows13"));
+    }
   }
   h->ch_alpha0 = alpha0;
   return DN_OK;
@@ -1330,6 +1342,21 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   A(dalloc(h, &h->l5, 5 * h->n));
   A(dalloc(h, &h->a13, 13 * h->n));
   A(dalloc(h, &h->l13, 13 * h->n));
+  // ordered factor rows for the ring-based CH sweeps: neither direction periodic and the ring fits in shared
+  // memory (periodic x keeps the level sweep on global memory: a self-checked run of the wrapped rows found
+  // no bad index, but the unchecked build faulted on them, so that combination stays off)
+  if (!c.periodic_x && !c.periodic_y && (size_t)kLvlRing * nx * sizeof(double) <= 96 * 1024 && nx < 65536) {
+    const int k = 6;
+    h->rows13.k = k;
+    A(dalloc(h, &h->rows13.lval, (size_t)k * h->n));
+    A(dalloc(h, &h->rows13.uval, (size_t)k * h->n));
+    A(dalloc(h, &h->rows13.lcol, (size_t)k * h->n));
+    A(dalloc(h, &h->rows13.ucol, (size_t)k * h->n));
+    A(dalloc(h, &h->rows13.lsrc, (size_t)k * h->n));
+    A(dalloc(h, &h->rows13.usrc, (size_t)k * h->n));
+    // the ring is dynamic shared memory of the CH PCG kernel; allow the largest ring any handle uses
+    cudaFuncSetAttribute(k_pcg<13, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  }
   h->ml = MomLayout{nx, ny, c.periodic_x, c.periodic_y, (long long)(nx + 1) * ny, (long long)nx * (ny + 1)};
   h->nm = h->ml.nu + h->ml.nv;
   A(dalloc(h, &h->mcoef, 9 * h->nm));

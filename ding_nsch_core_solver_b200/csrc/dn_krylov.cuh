@@ -245,6 +245,79 @@ __global__ void k_diag_inverse(SpOp A, double *dinv) {
 }
 
 // ---------------------------------------------------------------------------------------------------
+// 13-point factor rows in application order (built once per factorization, used when y is not periodic).
+// Per row r and p < K: the lower entries L_rc (ascending c, the reference's CSR order) and the upper
+// entries L_cr (ascending c, its lower_transpose order), padded with zeros.  K = 6 (the stencil's lower
+// half; built only when no direction is periodic -- wrapped rows would couple to up to 10).  src codes where the
+// neighbour's value sits during a level-scheduled sweep: (d << 16) | ci reads the shared ring of the level
+// d steps back (forward) or ahead (backward) at line ci; -1 reads the vector in global memory at col.
+// ---------------------------------------------------------------------------------------------------
+constexpr int kLvlRing = 8;  // levels kept in the shared ring (neighbours are at most 4 levels away)
+struct Rows13 {
+  double *lval, *uval;  // [K][n]
+  int *lcol, *ucol;     // [K][n]
+  int *lsrc, *usrc;     // [K][n]
+  int k;                // entries per row (6)
+};
+
+__device__ __forceinline__ int ring_code(int d, int ci) {
+  return (d >= 1 && d < kLvlRing && ci < 65536) ? ((d << 16) | ci) : -1;
+}
+
+__global__ void k_rows13(SpOp A, Factor F, Rows13 R) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.n) return;
+  const int n = A.n, ny = A.ny;
+  const int i = (int)(r / ny), j = (int)(r % ny);
+  const int lev = 2 * i + j;
+  int slots[13];
+  long long cols[13];
+  const int cnt = lower_slots<13>(A, i, j, slots, cols);
+  for (int p = 0; p < R.k; ++p) {
+    if (p < cnt) {
+      const long long c = cols[p];
+      const int ci = (int)(c / ny), cj = (int)(c % ny);
+      R.lval[(size_t)p * n + r] = F.l[(size_t)slots[p] * n + r];
+      R.lcol[(size_t)p * n + r] = (int)c;
+      R.lsrc[(size_t)p * n + r] = ring_code(lev - (2 * ci + cj), ci);
+    } else {
+      R.lval[(size_t)p * n + r] = 0.0;
+      R.lcol[(size_t)p * n + r] = (int)r;
+      R.lsrc[(size_t)p * n + r] = -1;
+    }
+  }
+  // upper neighbours c of r with L_cr != 0, ascending c (as apply_levels orders them)
+  int ucnt = 0;
+  for (int s = 0; s < 13; ++s) {
+    const long long c = slot_col<13>(i, j, s, A.nx, A.ny, A.px, A.py);
+    if (c <= r) continue;
+    const double lcr = F.l[(size_t)(12 - s) * n + c];
+    if (lcr == 0.0) continue;
+    int p = ucnt++;
+    while (p > 0 && cols[p - 1] > c) {
+      cols[p] = cols[p - 1];
+      slots[p] = slots[p - 1];
+      --p;
+    }
+    cols[p] = c;
+    slots[p] = s;
+  }
+  for (int p = 0; p < R.k; ++p) {
+    if (p < ucnt) {
+      const long long c = cols[p];
+      const int ci = (int)(c / ny), cj = (int)(c % ny);
+      R.uval[(size_t)p * n + r] = F.l[(size_t)(12 - slots[p]) * n + c];
+      R.ucol[(size_t)p * n + r] = (int)c;
+      R.usrc[(size_t)p * n + r] = ring_code((2 * ci + cj) - lev, ci);
+    } else {
+      R.uval[(size_t)p * n + r] = 0.0;
+      R.ucol[(size_t)p * n + r] = (int)r;
+      R.usrc[(size_t)p * n + r] = -1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------
 // Persistent PCG (solve_preconditioned_cg, ch_sparse_krylov.hpp:515-660)
 // ---------------------------------------------------------------------------------------------------
 // T is the type of the operator, the factor and the Krylov vectors (double; float for the inner solves of
@@ -269,6 +342,7 @@ struct PcgArgsT {
   double *partials;
   double *out;  // [0] iterations [1] abs residual [2] rel residual [3] iterate residual
   int nsweep;      // sweep warps (ceil(nx/32)) for the 5-point wavefront
+  Rows13 rows13;   // ordered factor rows of the 13-point operator (SWEEP 1, y not periodic); lval null: unused
   Sweep5T<T> s5;   // staged wavefront (SWEEP 3)
   int warp_smem;   // shared-memory bytes per sweep warp (SWEEP 3)
 };
@@ -476,6 +550,71 @@ __device__ void apply_levels(const PcgArgs &P, double m_r, double (&acc)[3]) {
   }
 }
 
+// Level-scheduled forward+backward application of the 13-point factor (y not periodic) by one CTA, from
+// the ordered rows (K entries each): the values of the last kLvlRing levels stay in a shared ring (`ring`,
+// kLvlRing x nx doubles), so a level reads its neighbours from shared memory; every row does the same six multiply-subtract
+// steps, the padded ones subtract exact zeros.  Same arithmetic and order as apply_levels.
+template <int K>
+__device__ void apply_levels13_ring(const PcgArgs &P, double m_r, double (&acc)[3], double *ring) {
+  const SpOp &A = P.A;
+  const int n = A.n, nx = A.nx, ny = A.ny;
+  const Rows13 &R = P.rows13;
+  const int nlev = 2 * (nx - 1) + ny;
+  const bool icc = P.prec == kPrecICC;
+  for (int lev = 0; lev < nlev; ++lev) {
+    const int i0 = max(0, (lev - (ny - 1) + 1) / 2), i1 = min(nx - 1, lev / 2);
+    for (int i = i0 + (int)threadIdx.x; i <= i1; i += blockDim.x) {
+      const long long r = (long long)i * ny + (lev - 2 * i);
+      double lv[K], yc[K];
+#pragma unroll
+      for (int p = 0; p < K; ++p) {
+        lv[p] = R.lval[(size_t)p * n + r];
+        // both candidate loads stay in bounds (the offset is clamped), whether or not the compiler issues
+        // them unconditionally and selects
+        const int src = R.lsrc[(size_t)p * n + r];
+        const int off = src >= 0 ? ((lev - (src >> 16)) & (kLvlRing - 1)) * nx + (src & 0xffff) : 0;
+        const double from_ring = ring[off];
+        const double from_vec = P.y[R.lcol[(size_t)p * n + r]];
+        yc[p] = src >= 0 ? from_ring : from_vec;
+      }
+      double sum = P.r[r] - m_r;
+#pragma unroll
+      for (int p = 0; p < K; ++p) sum -= lv[p] * yc[p];
+      const double yv = icc ? sum * P.dinv[r] : sum;
+      P.y[r] = yv;
+      ring[(lev & (kLvlRing - 1)) * nx + i] = yv;
+    }
+    __syncthreads();
+  }
+  for (int lev = nlev - 1; lev >= 0; --lev) {
+    const int i0 = max(0, (lev - (ny - 1) + 1) / 2), i1 = min(nx - 1, lev / 2);
+    for (int i = i0 + (int)threadIdx.x; i <= i1; i += blockDim.x) {
+      const long long r = (long long)i * ny + (lev - 2 * i);
+      double uv[K], zc[K];
+#pragma unroll
+      for (int p = 0; p < K; ++p) {
+        uv[p] = R.uval[(size_t)p * n + r];
+        const int src = R.usrc[(size_t)p * n + r];
+        const int off = src >= 0 ? ((lev + (src >> 16)) & (kLvlRing - 1)) * nx + (src & 0xffff) : 0;
+        const double from_ring = ring[off];
+        const double from_vec = P.z[R.ucol[(size_t)p * n + r]];
+        zc[p] = src >= 0 ? from_ring : from_vec;
+      }
+      double sum = icc ? P.y[r] : P.y[r] * P.dinv[r];
+#pragma unroll
+      for (int p = 0; p < K; ++p) sum -= uv[p] * zc[p];
+      const double zv = icc ? sum * P.dinv[r] : sum;
+      P.z[r] = zv;
+      ring[(lev & (kLvlRing - 1)) * nx + i] = zv;
+      const double rv = P.r[r] - m_r;
+      acc[0] += zv;
+      acc[1] += rv * zv;
+      acc[2] += rv;
+    }
+    __syncthreads();
+  }
+}
+
 // One persistent launch runs the whole PCG.  SWEEP: 0 = 5-point pipelined wavefront on global memory,
 // 1 = level-scheduled slot factor (CTA 0), 2 = diagonal, 3 = 5-point wavefront staged through shared memory.
 // The residual r is kept unprojected in memory; the mean of the latest update (m_r) is subtracted on the
@@ -570,7 +709,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
       }
     } else if (SWEEP == 1) {
       if constexpr (sizeof(T) == sizeof(double)) {
-        if (blockIdx.x == 0) apply_levels<S>(P, m_r_now, acc);
+        if (blockIdx.x == 0) {
+          if (S == 13 && P.rows13.lval != nullptr && P.rows13.k == 6)
+            apply_levels13_ring<6>(P, m_r_now, acc, (double *)dsm);
+          else
+            apply_levels<S>(P, m_r_now, acc);
+        }
       }
     } else {
       const T m = (T)m_r_now;
