@@ -599,7 +599,10 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
     P.rows13 = h->rows13;
     dyn_smem = (size_t)kLvlRing * h->G.nx * sizeof(double);
   }
-  int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(h->nsweep, (h->n + 2047) / 2048));
+  // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
+  const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
+  int blocks = (int)std::min<long long>(h->num_sms,
+                                        std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
   if (SWEEP == 3) {
     const dn_config &c = h->cfg;
@@ -695,7 +698,10 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
   P.nsweep = h->nsweep;
   P.warp_smem = 0;
   size_t dyn_smem = 0;
-  int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(h->nsweep, (h->n + 2047) / 2048));
+  // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
+  const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
+  int blocks = (int)std::min<long long>(h->num_sms,
+                                        std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
   const bool staged = h->sw5f > 0 && !h->G.px;
   if (staged) {
@@ -2073,7 +2079,8 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   P.out = scal + 8;
   P.nsweep = nsweep;
   P.warp_smem = 0;
-  int blocks = (int)std::min<long long>(D.num_sms, std::max<long long>(nsweep, (n + 2047) / 2048));
+  const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
+  int blocks = (int)std::min<long long>(D.num_sms, std::max<long long>(nsweep, (n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(1, std::min(blocks, D.max_coop_blocks));
   // staged wavefront: sweep warps per CTA from the shared-memory budget, as dn_create chooses them
   int sw = 0, sw_blocks_max = 0;
