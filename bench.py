@@ -32,6 +32,7 @@ FALLBACK_HBM_GBS = 6650.0
 # Algorithmic bytes per cell per pressure-PCG iteration of the split scheme, FP64 (SpMV 16, x/r update 48,
 # forward sweep 24, backward sweep 24, p update 24): every distinct array read once and written once.
 PCG_BYTES_PER_CELL_IT = 136.0
+METRIC = "Mcell-steps/s (plain FP64 step; the mixed-precision form in `mixed`)"
 RESTART_FIELDS = ("c", "c_prev", "c_prev2", "p", "p_prev", "u", "v", "u_prev", "v_prev", "e_prev", "hu_prev",
                   "hv_prev")
 
@@ -236,6 +237,7 @@ def run_ours(args):
             reports.append(rep)
             step += 1
     launches = solver.kernel_launches() - launches0
+    plain_fields = {n: solver.get_field(n) for n in ("p", "u", "v")}
     total_ms = sum(times)
     total_ms = reduce_max(dist, total_ms)
     value = n_cells * args.steps * world / (total_ms * 1e-3) / 1e6
@@ -259,6 +261,48 @@ def run_ours(args):
         step += 1
     e2e_ms = reduce_max(dist, e2e_ms)
     e2e_value = n_cells * args.steps * world / (e2e_ms * 1e-3) / 1e6
+
+    # ---- the mixed-precision form: same state, same steps, timed the same way; fields compared with the
+    # plain FP64 run after the same number of steps
+    mixed = None
+    if not args.no_mixed:
+        msolver = dn.Solver(dict(cfg, precision="mixed"), device=device)
+        for n, a in state.items():
+            msolver.set_field(n, a)
+        msolver.refresh_derived()
+        msolver.set_initial_mass(msolver.compute_mass("c"))
+        mstream = torch.cuda.ExternalStream(msolver.stream(), device=device)
+        mstep = 0
+        for _ in range(args.warmup):
+            msolver.step(mstep)
+            mstep += 1
+        mtimes, mreps = [], []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(mstream)
+            mreps.append(msolver.step(mstep))
+            e1.record(mstream)
+            e1.synchronize()
+            mtimes.append(e0.elapsed_time(e1))
+            mstep += 1
+        g = cfg["ghost"]
+        errs = {}
+        for n, ref in plain_fields.items():
+            got = msolver.get_field(n)[g:-g, g:-g]
+            ref = ref[g:-g, g:-g]
+            errs[n] = float(np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-300))
+        mtotal = reduce_max(dist, sum(mtimes))
+        mvalue = n_cells * args.steps * world / (mtotal * 1e-3) / 1e6
+        mixed = {"value": round(mvalue, 4), "unit": "Mcell-steps/s", "ms_per_step": round(mtotal / args.steps, 4),
+                 "vs_plain": round(mvalue / value, 4),
+                 "pressure_iterations_mean": statistics.mean(r["pressure_iterations"] for r in mreps),
+                 "refinement_cycles_mean": statistics.mean(r["refinement_cycles"] for r in mreps),
+                 "inner_tolerance": 1e-5,
+                 "rel_l2_vs_plain_fp64": {k: float(f"{v:.3e}") for k, v in errs.items()},
+                 "compared_after_steps": args.warmup + args.steps}
+        msolver.close()
 
     # ---- roofline of the dominant kernel (the pressure PCG), bytes per launch / launch time
     peak, peak_kind = hbm_peak()
@@ -293,7 +337,7 @@ def run_ours(args):
         mean_rep = {k: statistics.mean(r[k] for r in reports) for k in ("pressure_iterations", "ch_iterations",
                                                                        "momentum_iterations")}
         line = {
-            "metric": "Mcell-steps/s (plain FP64 step; mixed form not built yet)",
+            "metric": METRIC,
             "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -308,6 +352,7 @@ def run_ours(args):
             "roofline": roofline,
             "critical_path": critical_path,
             "cpu_baseline": cpu,
+            "mixed": mixed,
             "e2e": {"value": round(e2e_value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": h2d},
             "gpu_launches": launches,
@@ -340,7 +385,7 @@ def run_reference(args):
            "sample": f"{args.steps} steps of the 192x384 workload; the reference step is single-threaded, so one "
                      f"host thread is all it can use"}
     print(json.dumps({
-        "impl": "reference", "metric": "Mcell-steps/s (plain FP64 step; mixed form not built yet)",
+        "impl": "reference", "metric": METRIC,
         "value": round(value, 6), "unit": "Mcell-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3 / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -359,6 +404,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
