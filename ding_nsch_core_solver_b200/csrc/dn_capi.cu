@@ -28,6 +28,10 @@ namespace {
 
 constexpr double kSqrt2 = 1.4142135623730950488;
 constexpr int kHostScal = 8192;  // pinned host scratch (doubles): scalars and reduction partials
+// Sweep warps per CTA: one per SM sub-partition (scheduler).  A fifth warp shares a scheduler with the
+// first and slows both; fewer warps per CTA put more hand-overs across CTAs (measured 81.9 ms per pressure
+// solve with 4, 87.8 with 5, 92.6 with 1 on the 192 x 384 bench workload).
+constexpr int kSweepWarpsPerCta = 4;
 
 // ---------------------------------------------------------------------------------------------------
 // Pressure system (build_pressure_linear_system, pressure.cpp:123-196) into 5 slots W,S,C,N,E + rhs
@@ -1395,7 +1399,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     h->sw5_warp_smem[1] = round16(sweep_warp_smem(4, ny));
     const size_t per = h->sw5_warp_smem[use_split(c) ? 0 : 1];
     const size_t budget = (size_t)optin > 64 + 2304 ? (size_t)optin - 64 - 2304 : 0;  // minus static smem
-    int sw = (int)std::min<size_t>(8, budget / per);
+    int sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
     sw = std::min(sw, h->nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
     h->sw5 = sw;
@@ -1427,7 +1431,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     cudaFuncAttributes fa{};
     cudaFuncGetAttributes(&fa, k_pcg<5, 3, float>);
     const size_t budget = (size_t)optin > 64 + fa.sharedSizeBytes ? (size_t)optin - 64 - fa.sharedSizeBytes : 0;
-    int sw = (int)std::min<size_t>(8, budget / per);
+    int sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
     sw = std::min(sw, h->nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
     h->sw5f = sw;
@@ -2088,7 +2092,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   if (!G.px) {
     const size_t per = (sweep_warp_smem(split ? 2 : 4, ny) + 15) & ~(size_t)15;
     const size_t budget = (size_t)D.smem_optin > 64 + 2304 ? (size_t)D.smem_optin - 64 - 2304 : 0;
-    sw = (int)std::min<size_t>(8, budget / per);
+    sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
     sw = std::min(sw, nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
     if (sw > 0) {

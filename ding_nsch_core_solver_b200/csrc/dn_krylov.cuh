@@ -643,6 +643,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
       P.s5.bnd_f[t] = empty;
       P.s5.bnd_b[t] = empty;
     }
+    // so do the same-CTA hand-over lines (forward and backward) of this CTA's sweep warps
+    const int na = P.s5.varcoef ? 4 : 2;
+    const size_t lines = 2 * (size_t)((P.s5.ny + 3) & ~3);
+    for (int w = 0; w < P.s5.sw; ++w) {
+      T *line = (T *)(dsm + 64 + (size_t)w * P.warp_smem) + sweep_hand_line(na);
+      for (size_t t = threadIdx.x; t < lines; t += blockDim.x) line[t] = empty;
+    }
     __syncthreads();
   }
 

@@ -16,8 +16,9 @@
 // Inputs are staged by cp.async in 8-column chunks, three chunks ahead, into per-lane ring rows of 64
 // columns plus an 8-column mirror (row pitch 72 doubles: skewed reads stay bank-conflict free), so that
 // the 8 steps of a group read at fixed offsets from one base pointer.  Neighbouring warps hand over their
-// edge line through shared memory (same CTA) or global memory (different CTAs) with release/acquire
-// progress counters, published every 8 columns.  Every wait is bounded and reports kDevTimeout.
+// edge line through a shared-memory line (same CTA) or a global line (different CTAs) without flags: the
+// lines hold a NaN sentinel until the producer stores a value, and the consumer waits on the values
+// themselves and writes the sentinel back after use.  Every wait is bounded and reports kDevTimeout.
 #pragma once
 
 #include "dn_common.cuh"
@@ -56,11 +57,13 @@ using Sweep5 = Sweep5T<double>;
 
 __host__ __device__ inline int staged_sweep_warps(int nx) { return (nx + kLines - 1) / kLines; }
 
-// per-warp shared-memory footprint (bytes) for `na` staged arrays of `esize`-byte elements, a ny-long
-// hand-over line and the zero / unit rows read by lanes that own no line
+// per-warp shared-memory footprint (bytes) for `na` staged arrays of `esize`-byte elements, two ny-long
+// hand-over lines (forward, backward) and the zero / unit rows read by lanes that own no line
 __host__ __device__ inline size_t sweep_warp_smem(int na, int ny, int esize = 8) {
-  return (size_t)na * 32 * kPitch * esize + (size_t)((ny + 3) & ~3) * esize + 2 * (size_t)kPitch * esize + 64;
+  return (size_t)na * 32 * kPitch * esize + 2 * (size_t)((ny + 3) & ~3) * esize + 2 * (size_t)kPitch * esize + 64;
 }
+// Offset (elements) of a sweep warp's forward hand-over line in its region; the backward line follows it.
+__host__ __device__ inline size_t sweep_hand_line(int na) { return (size_t)na * 32 * kPitch; }
 
 __device__ __forceinline__ unsigned int ld_acquire_cta(const unsigned int *p) {
   unsigned int v;
@@ -153,6 +156,30 @@ __device__ __forceinline__ void st_generic_if(float *p, float v, bool pred) {
   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.f32 [%0], %1;\n\t}" ::"l"(p), "f"(v),
                "r"((int)pred)
                : "memory");
+}
+
+// Same-CTA hand-over without flags: the consumer's line starts as the sentinel, the producer stores its
+// values into it, the consumer waits (bounded) until the group's columns are no longer the sentinel and
+// writes the sentinel back after use.  `cols` gives lane t's column of the group (negative: none).
+template <typename T>
+__device__ __forceinline__ bool wait_local_line(T *line, int col, int *status, unsigned long long &t_wait) {
+  bool miss = col >= 0 && hand_empty(*(volatile T *)&line[col]);
+  if (__any_sync(0xffffffffu, miss)) {
+    const unsigned long long tw0 = global_ns();
+    long long spins = 0;
+    while (__any_sync(0xffffffffu, miss)) {
+      ++spins;
+      if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+        if ((threadIdx.x & 31) == 0) atomicCAS(status, kDevOk, kDevTimeout);
+        return false;
+      }
+      if (spins > 32) __nanosleep(64);
+      if (miss) miss = hand_empty(*(volatile T *)&line[col]);
+    }
+    t_wait += global_ns() - tw0;
+  }
+  __syncwarp();
+  return true;
 }
 
 // Bounded warp-uniform wait for a progress counter (shared or global) to reach `target`.
@@ -286,18 +313,16 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
   T *ring_d = ring_r + 32 * kPitch;
   T *ring_w = ring_d + 32 * kPitch;
   T *ring_s = ring_w + 32 * kPitch;
-  T *bline = ring_r + (size_t)na * 32 * kPitch;
-  T *zrow = bline + ((ny + 3) & ~3);
+  T *bline = ring_r + sweep_hand_line(na);  // forward hand-over line (line i0-1), written by the producer
+  T *zrow = bline + 2 * ((ny + 3) & ~3);
   T *ones = zrow + kPitch;
   const bool vec16 = (ny % (16 / (int)sizeof(T))) == 0;  // 16-byte pieces
   const bool prod_local = has_prod && (ws > 0);
   const bool has_cons = (k + 1 < nsweep);
   const bool cons_local = has_cons && (ws + 1 < sw);
-  const unsigned int base = epoch * (unsigned int)(ny + 1);
   const int total = ny + nl;
   const int nchunk = (total + kChunk - 1) / kChunk;
-  unsigned int *my_cnt = &cnt_cta[2 * ws];
-  unsigned int *next_cnt = &cnt_cta[2 * (ws + 1)];
+  const T empty = hand_empty_value<T>();
   // per-lane rows: real lanes their ring rows, the ghost unit dinv, everything else zeros
   const T *r_row = real ? ring_r + lane * kPitch : zrow;
   const T *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
@@ -308,7 +333,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
   const T aw_c = (real && i > 0) ? cx : T(0);
   T *const ydst = yout + (size_t)(real ? i : 0) * ny;
   const bool hand = has_cons && lane == 31;  // a warp with a consumer has nl = 31
-  T *const hdst = cons_local ? (T *)(smem_warp + P.warp_smem) + (size_t)na * 32 * kPitch
+  T *const hdst = cons_local ? (T *)(smem_warp + P.warp_smem) + sweep_hand_line(na)
                                   : bnd_f + ((size_t)(epoch & 1u) * nsweep + k) * ny;
   auto stage = [&](int c) {
     const int c0 = c * kChunk;
@@ -335,7 +360,6 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
   // A producer in another CTA hands its line over through global memory: the values of group c are loaded
   // kAhead groups early (issued at the start of a group, landed in the shared line at its end).
   const bool remote = has_prod && !prod_local;
-  unsigned int avail = 0;
   T *const hin = has_prod ? bnd_f + ((size_t)(epoch & 1u) * nsweep + (k - 1)) * ny : nullptr;
   auto hand_issue = [&](int c) -> T {
     const int col = c * kChunk + lane;
@@ -384,19 +408,10 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
     cp_async_wait_ahead();
     __syncwarp();
     const int s0 = q * kChunk;
-    if (prod_local && s0 < ny) {  // hand-over values of line i0-1 for columns [s0, s0+kHand), same CTA
-      const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
-      if (avail + base < need) {
-        const unsigned long long tw0 = global_ns();
-        const unsigned int v = wait_progress<true>(my_cnt, need, status);
-        t_wait += global_ns() - tw0;
-        if (v == 0) {
-          cp_async_wait0();
-          return;
-        }
-        avail = v - base;
-      }
-      __syncwarp();
+    const int hcol = (lane < kHand && s0 + lane < ny) ? s0 + lane : -1;  // this group's hand-over columns
+    if (prod_local && s0 < ny && !wait_local_line(bline, hcol, status, t_wait)) {
+      cp_async_wait0();
+      return;
     }
     if (s0 >= 32 && s0 + kHand < ny) {
       // steady state: every lane's column lies in [1, ny-2]; fixed offsets from one base per array
@@ -473,14 +488,8 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
         w_prev = act ? wv : w_prev;
       }
     }
-    // publish the columns lane 31 (skew 31) has finished to a consumer in this CTA (a consumer in another
-    // CTA polls the values themselves)
-    const int done = min(ny, s0 + kHand - 31);
-    if (cons_local && done > 0) {
-      __syncwarp();
-      if (lane == 31) st_release_cta(next_cnt, base + (unsigned int)done);
-    }
     __syncwarp();
+    if (prod_local && hcol >= 0) bline[hcol] = empty;  // consumed: back to the sentinel for the next application
     if (remote && !hand_land(q + kAhead, hv)) {
       cp_async_wait0();
       return;
@@ -536,15 +545,13 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
   T *ring_d = ring_y + 32 * kPitch;
   T *ring_n = ring_d + 32 * kPitch;
   T *ring_e = ring_n + 32 * kPitch;
-  T *bline = ring_y + (size_t)na * 32 * kPitch;
-  T *zrow = bline + ((ny + 3) & ~3);
+  T *bline = ring_y + sweep_hand_line(na) + ((ny + 3) & ~3);  // backward hand-over line (line i0+31)
+  T *zrow = ring_y + sweep_hand_line(na) + 2 * ((ny + 3) & ~3);
   T *ones = zrow + kPitch;
   const bool vec16 = (ny % (16 / (int)sizeof(T))) == 0;  // 16-byte pieces
-  const unsigned int base = epoch * (unsigned int)(ny + 1);
   const int total = ny + lead;
   const int nchunk = (total + kChunk - 1) / kChunk;
-  unsigned int *my_cnt = &cnt_cta[2 * ws + 1];
-  unsigned int *prev_cnt = &cnt_cta[2 * (ws - 1) + 1];
+  const T empty = hand_empty_value<T>();
   const T *y_row = real ? ring_y + lane * kPitch : zrow;
   const T *d_row = real ? ring_d + lane * kPitch : (lin ? ones : zrow);
   const T *n_row = real ? ring_n + lane * kPitch : zrow;
@@ -553,7 +560,7 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
   const T ae_c = (real && i + 1 < nx) ? cx : T(0);
   T *const zdst = zout + (size_t)(real ? i : 0) * ny;
   const bool hand = has_cons && lane == 0;
-  T *const hdst = cons_local ? (T *)(smem_warp - P.warp_smem) + (size_t)na * 32 * kPitch
+  T *const hdst = cons_local ? (T *)(smem_warp - P.warp_smem) + sweep_hand_line(na) + ((ny + 3) & ~3)
                                   : bnd_b + ((size_t)(epoch & 1u) * nsweep + k) * ny;
   auto stage = [&](int c) {
     const int c1 = ny - kChunk * c;
@@ -608,7 +615,6 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
     __syncwarp();
     return true;
   };
-  unsigned int avail = 0;
   for (int c = 0; c < kAhead; ++c) {
     if (remote && !hand_land(c, hand_issue(c))) {
       cp_async_wait0();
@@ -624,17 +630,12 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
     cp_async_wait_ahead();
     __syncwarp();
     const int s0 = q * kChunk;
-    if (prod_local && s0 < ny) {  // hand-over values of line i0+31, columns ny-1-s0 .. ny-kHand-s0, same CTA
-      const unsigned int need = base + (unsigned int)min(ny, s0 + kHand);
-      if (avail + base < need) {
-        const unsigned int v = wait_progress<true>(my_cnt, need, status);
-        if (v == 0) {
-          cp_async_wait0();
-          return;
-        }
-        avail = v - base;
-      }
-      __syncwarp();
+    // this group's hand-over columns (line i0+31, columns ny-1-s0 down to ny-kHand-s0)
+    const int hcol = (lane < kHand && ny - 1 - (s0 + lane) >= 0) ? ny - 1 - (s0 + lane) : -1;
+    unsigned long long t_unused = 0;
+    if (prod_local && s0 < ny && !wait_local_line(bline, hcol, status, t_unused)) {
+      cp_async_wait0();
+      return;
     }
     if (s0 >= 32 && s0 + kHand < ny) {
       // steady state: every real lane's column lies in [1, ny-2]
@@ -706,13 +707,8 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
         z_prev = act ? zv : z_prev;
       }
     }
-    // publish the columns lane 0 (skew `lead`) has finished to a consumer in this CTA
-    const int done = min(ny, s0 + kHand - lead);
-    if (cons_local && done > 0) {
-      __syncwarp();
-      if (lane == 0) st_release_cta(prev_cnt, base + (unsigned int)done);
-    }
     __syncwarp();
+    if (prod_local && hcol >= 0) bline[hcol] = empty;  // consumed: back to the sentinel
     if (remote && !hand_land(q + kAhead, hv)) {
       cp_async_wait0();
       return;
