@@ -13,9 +13,9 @@
 // backward sweep) from a shared-memory hand-over line through the same arithmetic with zero coefficients
 // and unit dinv, so every lane receives its neighbour's value of the previous step by one plain warp
 // shuffle and a step has no lane-dependent selects.  Lanes that own no line read a zero row and carry 0.
-// Inputs are staged by cp.async in 8-column chunks, three chunks ahead, into per-lane ring rows of 64
-// columns plus an 8-column mirror (row pitch 72 doubles: skewed reads stay bank-conflict free), so that
-// the 8 steps of a group read at fixed offsets from one base pointer.  Neighbouring warps hand over their
+// Inputs are staged by cp.async in 16-column chunks, one chunk ahead, into per-lane ring rows of 64
+// columns plus a 16-column mirror (row pitch 80 elements: skewed reads stay bank-conflict free), so that
+// the 16 steps of a group read at fixed offsets from one base pointer.  Neighbouring warps hand over their
 // edge line through a shared-memory line (same CTA) or a global line (different CTAs) without flags: the
 // lines hold a NaN sentinel until the producer stores a value, and the consumer waits on the values
 // themselves and writes the sentinel back after use.  Every wait is bounded and reports kDevTimeout.
@@ -26,11 +26,11 @@
 namespace dn {
 
 constexpr int kRing = 64;                // ring columns per staged array
-constexpr int kMirror = 8;               // mirrored columns so an 8-step group never wraps
+constexpr int kMirror = 16;              // mirrored columns so a group of kHand steps never wraps
 constexpr int kPitch = kRing + kMirror;  // doubles per ring row
-constexpr int kChunk = 8;                // columns per cp.async chunk (= one hand-over group of steps)
-constexpr int kHand = 8;                 // columns per boundary publication
-constexpr int kAhead = 3;                // chunks staged ahead of the one being consumed
+constexpr int kChunk = 16;               // columns per cp.async chunk (= one group of steps)
+constexpr int kHand = 16;                // steps per group (hand-over columns checked together)
+constexpr int kAhead = 1;                // chunks staged ahead of the one being consumed
 constexpr int kLines = 31;               // grid lines per sweep warp (lane 31 / lane 0 is the ghost)
 
 // T is the storage and arithmetic type of the sweep (double, or float for the inner solves of the
@@ -101,7 +101,9 @@ __device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem) {
     cp_async4(smem, gmem);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_ahead() { asm volatile("cp.async.wait_group 3;" ::: "memory"); }
+static_assert(kAhead == 1, "cp_async_wait_ahead waits for all but the newest kAhead groups");
+static_assert(kLines + kChunk * (kAhead + 1) <= kRing, "the ring holds the skew window plus the staged chunks");
+__device__ __forceinline__ void cp_async_wait_ahead() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Cross-CTA hand-over.  The edge line goes through global memory without flags or fences: each launch
@@ -204,8 +206,8 @@ __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, u
 }
 
 // Stage columns [c0, c1) of `nl` grid lines starting at line i0 into ring rows row0 .. row0+nl-1.  Column j
-// goes to row offset off + (j & 63); the mirrored columns are written twice (forward: slots 0..7 again at
-// 64..71, off = 0; backward: slots 56..63 again at 0..7, off = 8).  16-byte pieces when ny allows them.
+// goes to row offset off + (j & 63); the mirrored columns are written twice (forward: slots 0..15 again at
+// 64..79, off = 0; backward: slots 48..63 again at 0..15, off = 16).  16-byte pieces when ny allows them.
 template <bool FWD, typename T>
 __device__ __forceinline__ void stage_cols(T *ring, const T *src, int i0, int row0, int nl, int ny, int c0,
                                            int c1, bool vec16) {
@@ -239,11 +241,11 @@ __device__ __forceinline__ void stage_cols(T *ring, const T *src, int i0, int ro
   }
 }
 
-// Stage one whole 8-column chunk [c0, c0+8) (ny a multiple of the 16-byte piece; for the backward ring
-// also ny % 8 == 0, so that the chunk sits at an 8-aligned ring slot): in doubles, lane t copies columns
-// c0 + 2 (t & 3) + {0, 1} of lines (t >> 2) + 8 it, it = 0..3 (in floats, four columns of lines
-// (t >> 1) + 16 it), one 16-byte cp.async per array -- no division, addresses from one per-lane offset.  The chunk at the mirrored slot is copied a second time (forward: slot 0 again at 64,
-// backward: slot 56 again at 0).
+// Stage one whole chunk [c0, c0+kChunk) (ny a multiple of the 16-byte piece; for the backward ring also
+// ny % kChunk == 0, so that the chunk sits at a chunk-aligned ring slot): lane t copies one 16-byte piece
+// (2 doubles or 4 floats) per array of line t / PL + LI it, PL pieces per line, with no division and
+// addresses from one per-lane offset.  The chunk at the mirrored slot is copied a second time (forward:
+// slot 0 again at kRing, backward: slot kRing - kChunk again at 0).
 template <bool FWD, int NA, typename T>
 __device__ __forceinline__ void stage_full(T *r0, T *r1, T *r2, T *r3, const T *s0, const T *s1, const T *s2,
                                            const T *s3, int i0, int row0, int nl, int ny, int c0) {
