@@ -191,6 +191,7 @@ def run_ours(args):
     import torch
 
     import ding_nsch_core_solver_b200 as dn
+    from ding_nsch_core_solver_b200 import capi
 
     dist, rank, world, local = dist_setup(args.gpus)
     device = local if dist is not None else 0
@@ -304,6 +305,47 @@ def run_ours(args):
                  "compared_after_steps": args.warmup + args.steps}
         msolver.close()
 
+    # ---- batched ensemble: B instances of the workload (different seeded interfaces) advanced together by
+    # dn_step_batch, each on its own stream and on 1/B of the SMs (device_share = B); one batch step = one
+    # step of every instance.  Timed with events
+    # on the default stream around the whole call (device idle before; the call returns when every instance
+    # has finished), so host launch latency counts against it.
+    batched = None
+    if args.batch > 0:
+        members = []
+        for k in range(args.batch):
+            s = dn.Solver(dict(cfg, device_share=args.batch), device=device)
+            for n, a in initial_state(cfg, seed=40 + k).items():
+                s.set_field(n, a)
+            s.refresh_derived()
+            s.set_initial_mass(s.compute_mass("c"))
+            members.append(s)
+        bstep = 0
+        for _ in range(args.warmup):
+            capi.step_batch(members, [bstep] * len(members))
+            bstep += 1
+        blaunch0 = sum(s.kernel_launches() for s in members)
+        btimes = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            capi.step_batch(members, [bstep] * len(members))
+            e1.record()
+            e1.synchronize()
+            btimes.append(e0.elapsed_time(e1))
+            bstep += 1
+        blaunches = sum(s.kernel_launches() for s in members) - blaunch0
+        btotal = reduce_max(dist, sum(btimes))
+        bvalue = n_cells * len(members) * args.steps * world / (btotal * 1e-3) / 1e6
+        batched = {"instances": len(members), "value": round(bvalue, 4), "unit": "Mcell-steps/s",
+                   "ms_per_batch_step": round(btotal / args.steps, 4), "vs_single": round(bvalue / value, 4),
+                   "gpu_launches": blaunches,
+                   "entry_point": "dn_step_batch (one stream and host worker per instance)"}
+        for s in members:
+            s.close()
+
     # ---- roofline of the dominant kernel (the pressure PCG), bytes per launch / launch time
     peak, peak_kind = hbm_peak()
     bytes_per_launch = PCG_BYTES_PER_CELL_IT * n_cells * statistics.mean(pcg_its)
@@ -353,6 +395,7 @@ def run_ours(args):
             "critical_path": critical_path,
             "cpu_baseline": cpu,
             "mixed": mixed,
+            "batched": batched,
             "e2e": {"value": round(e2e_value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": h2d},
             "gpu_launches": launches,
@@ -405,6 +448,7 @@ def main():
     ap.add_argument("--cpu-sample-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
+    ap.add_argument("--batch", type=int, default=8, help="instances of the batched-ensemble arm (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -48,7 +48,7 @@ class Config(C.Structure):
         "zalesak_slot_depth", "advect_u", "advect_v", "rotation_center_x", "rotation_center_y",
         "angular_velocity", "top_wall_velocity_x", "bottom_wall_velocity_x")] + [
         ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4), ("precision", C.c_int),
-        ("mixed_inner_tolerance", C.c_double)]
+        ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int)]
 
 
 class Report(C.Structure):
@@ -104,6 +104,7 @@ def load():
         "dn_set_initial_mass": (None, [H, D]),
         "dn_refresh_derived": (I, [H]),
         "dn_step": (I, [H, I, C.POINTER(Report)]),
+        "dn_step_batch": (I, [C.POINTER(H), I, C.POINTER(C.c_int), C.POINTER(Report)]),
         "dn_begin_step": (I, [H, I]),
         "dn_phase": (I, [H, I, C.POINTER(Report)]),
         "dn_momentum": (I, [H, I, C.POINTER(Report)]),
@@ -298,3 +299,18 @@ class Solver:
 
     def kernel_launches(self) -> int:
         return int(self._lib.dn_kernel_launches(self._h))
+
+
+def step_batch(solvers, steps) -> list:
+    """One step of each solver, the solvers advanced concurrently on the device (dn_step_batch).  Returns one
+    report dict per solver; each solver's result equals its own step()."""
+    lib = load()
+    n = len(solvers)
+    hs = (C.c_void_p * n)(*[s._h.value for s in solvers])
+    st = (C.c_int * n)(*[int(k) for k in steps])
+    reps = (Report * n)()
+    code = lib.dn_step_batch(hs, n, st, reps)
+    if code != 0:
+        msgs = [lib.dn_last_error(s._h).decode() for s in solvers]
+        raise DnError(code, "; ".join(m for m in msgs if m))
+    return [{f: getattr(r, f) for f, _ in Report._fields_} for r in reps]

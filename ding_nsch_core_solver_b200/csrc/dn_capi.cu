@@ -14,7 +14,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dn_common.cuh"
@@ -360,6 +362,7 @@ struct dn_handle {
   dn_config cfg;
   int device = 0;
   int num_sms = 148;
+  int cta_cap = 148;  // CTAs one persistent launch may take: num_sms / device_share
   cudaStream_t stream = nullptr;
   Grid G;
   BCSet bc;
@@ -605,8 +608,9 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   }
   // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
   const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
-  int blocks = (int)std::min<long long>(h->num_sms,
+  int blocks = (int)std::min<long long>(h->cta_cap,
                                         std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
+  blocks = std::max(blocks, (h->nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
   if (SWEEP == 3) {
     const dn_config &c = h->cfg;
@@ -704,8 +708,9 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
   size_t dyn_smem = 0;
   // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
   const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
-  int blocks = (int)std::min<long long>(h->num_sms,
+  int blocks = (int)std::min<long long>(h->cta_cap,
                                         std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
+  blocks = std::max(blocks, (h->nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
   const bool staged = h->sw5f > 0 && !h->G.px;
   if (staged) {
@@ -857,7 +862,7 @@ dn_status run_bicgstab(dn_handle *h, double out[4]) {
   k_mom_dinv<<<blocks_for(h->nm), 256, 0, h->stream>>>(P);
   DN_TRY(check_launch(h, "k_mom_dinv"));
   DN_TRY(reset_sync(h));
-  int blocks = (int)std::min<long long>(h->num_sms, std::max<long long>(1, (h->nm + 2047) / 2048));
+  int blocks = (int)std::min<long long>(h->cta_cap, std::max<long long>(1, (h->nm + 2047) / 2048));
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
   void *args[] = {&P};
   cudaEventRecord(h->kev[0], h->stream);
@@ -1304,6 +1309,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, device);
   h->num_sms = prop.multiProcessorCount;
+  h->cta_cap = std::max(1, h->num_sms / std::max(1, cfg->device_share));
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
   for (auto &e : h->ev) cudaEventCreate(&e);
   for (auto &e : h->kev) cudaEventCreate(&e);
@@ -1634,6 +1640,40 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
     cudaEventElapsedTime(&ms, h->ev[k], h->ev[k + 1]);
     h->phase_ms[k] = ms;
   }
+  return DN_OK;
+}
+
+// Batched ensemble: one step of each handle, the handles advanced concurrently.  Each handle's kernels run
+// on its own stream from a host worker of its own, so the GPU overlaps the instances: a single instance's
+// wavefront keeps only a few warps busy, many instances fill the device.  Every handle computes exactly
+// what dn_step computes for it alone.
+dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, dn_report *reports) {
+  if (!handles || count < 0) return DN_ERR_INVALID_ARGUMENT;
+  for (int a = 0; a < count; ++a) {
+    if (!handles[a]) return DN_ERR_INVALID_ARGUMENT;
+    for (int b2 = 0; b2 < a; ++b2)
+      if (handles[b2] == handles[a]) return DN_ERR_INVALID_ARGUMENT;  // one handle twice would race with itself
+  }
+  std::vector<dn_status> st((size_t)count, DN_OK);
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    for (int a = next.fetch_add(1); a < count; a = next.fetch_add(1)) {
+      dn_handle *h = handles[a];
+      if (cudaSetDevice(h->device) != cudaSuccess) {
+        st[(size_t)a] = fail(h, DN_ERR_CUDA, "cudaSetDevice failed");
+        continue;
+      }
+      st[(size_t)a] = dn_step(h, steps ? steps[a] : 0, reports ? &reports[a] : nullptr);
+    }
+  };
+  const int nworkers = std::min(count, 64);
+  std::vector<std::thread> pool;
+  pool.reserve((size_t)std::max(0, nworkers - 1));
+  for (int w = 1; w < nworkers; ++w) pool.emplace_back(worker);
+  if (nworkers > 0) worker();
+  for (auto &t : pool) t.join();
+  for (int a = 0; a < count; ++a)
+    if (st[(size_t)a] != DN_OK) return st[(size_t)a];
   return DN_OK;
 }
 

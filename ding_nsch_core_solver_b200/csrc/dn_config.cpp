@@ -99,6 +99,7 @@ extern "C" void dn_config_default(dn_config *c) {
   c->periodic_y = 1;
   c->precision = DN_PRECISION_FP64;
   c->mixed_inner_tolerance = 1.0e-5;
+  c->device_share = 1;
 }
 
 extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err, size_t err_len) {
@@ -202,6 +203,8 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
     getd("top_wall_velocity_x", cfg->top_wall_velocity_x);
     getd("bottom_wall_velocity_x", cfg->bottom_wall_velocity_x);
     getd("mixed_inner_tolerance", cfg->mixed_inner_tolerance);
+    geti("device_share", cfg->device_share);
+    if (cfg->device_share < 1) throw std::runtime_error("device_share must be at least 1");
     static const char *sides[4] = {"left", "right", "bottom", "top"};
     for (int s = 0; s < 4; ++s) {
       char tk[64], vk[64];

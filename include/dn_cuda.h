@@ -78,6 +78,9 @@ typedef struct {
   dn_bc p_bc[4], u_bc[4], v_bc[4]; /* indexed by dn_side */
   int precision;                   /* dn_precision */
   double mixed_inner_tolerance;    /* relative tolerance of each FP32 inner solve (mixed form) */
+  int device_share;                /* handles meant to run concurrently on one device (dn_step_batch): each
+                                      persistent launch takes at most 1/device_share of the SMs, never fewer
+                                      CTAs than its wavefront needs; 1 = the whole device */
 } dn_config;
 
 /* Fields (Solver members, src/core/coupled/solver.hpp:64-91). */
@@ -137,6 +140,12 @@ dn_status dn_refresh_derived(dn_handle *h);
 /* ---- the time step and its phases (each replaces the cited reference member) ------------------------ */
 /* Solver::advance_one_timestep (solver.cpp:224-283). */
 dn_status dn_step(dn_handle *h, int step, dn_report *rep);
+/* Batched ensemble (the reference runs one Solver per process; here many handles share the device): one
+ * dn_step of each of `count` distinct handles, run concurrently -- each on its own stream from a host worker
+ * thread -- so that many small instances fill the GPU.  steps[a] is handle a's step index (NULL: 0);
+ * reports (NULL allowed) receives one dn_report per handle.  Each handle's result equals its dn_step alone.
+ * Returns the first failing handle's status (its message via dn_last_error). */
+dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, dn_report *reports);
 /* history copies at the start of advance_one_timestep (solver.cpp:225-231) */
 dn_status dn_begin_step(dn_handle *h, int step);
 /* Solver::advance_phase_state (phase_field.cpp:258-281): CH solve, materials, surface force */

@@ -77,6 +77,10 @@ def test_config_errors(lib):
         capi.parse_config("u_bc_left_type = robin\n")
     c = capi.parse_config("pressure_scheme = cuda_split_icpcg\nprecision = mixed\n")
     assert c.pressure_scheme == 3 and c.precision == 1
+    assert capi.parse_config("nx = 32\n").device_share == 1
+    assert capi.parse_config("device_share = 8\n").device_share == 8
+    with pytest.raises(capi.DnError):
+        capi.parse_config("device_share = 0\n")
 
 
 def test_create_without_device_fails_loudly(lib):
