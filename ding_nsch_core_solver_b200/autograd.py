@@ -1,0 +1,81 @@
+"""torch.autograd.Function over the projection entry points of the C-ABI.
+
+`projection(solver, step, u_star, v_star, p, p_prev)` runs the pressure projection of one step --
+pressure solve plus velocity correction (dn_projection) -- on interior-shaped float64 CUDA tensors and
+returns (u, v, p_new, p_prev_new).  Its backward is the hand-written discrete adjoint dn_projection_adjoint,
+whose transposed pressure solve is the same PCG.  rho_mid is a constant of the map: the solver's rho_mid at
+the forward call is kept and put back before the backward runs.  The reference has no adjoint.
+
+Shapes (interior values only): u, u_star (nx+1, ny); v, v_star (nx, ny+1); p, p_prev, p_new (nx, ny).
+"""
+import ctypes as C
+
+import torch
+
+from . import capi
+
+
+def _full(solver, t, kind):
+    """Zero-ghosted Field2D buffer holding interior values t."""
+    g = solver.ghost
+    nx, ny = solver.nx, solver.ny
+    shp = {"u": (nx + 1, ny), "v": (nx, ny + 1), "c": (nx, ny)}[kind]
+    if tuple(t.shape) != shp:
+        raise ValueError(f"expected interior shape {shp}, got {tuple(t.shape)}")
+    buf = torch.zeros((shp[0] + 2 * g, shp[1] + 2 * g), dtype=torch.float64, device=t.device)
+    buf[g:g + shp[0], g:g + shp[1]] = t
+    return buf
+
+
+def _interior(solver, buf):
+    g = solver.ghost
+    return buf[g:buf.shape[0] - g, g:buf.shape[1] - g].clone()
+
+
+def _call(solver, fn, step, ins, outs):
+    torch.cuda.current_stream().synchronize()  # the C-ABI runs on the solver's own stream
+    its, rel = C.c_int(), C.c_double()
+    solver._check(fn(solver._h, int(step), *[t.data_ptr() for t in ins], *[t.data_ptr() for t in outs],
+                     C.byref(its), C.byref(rel)))
+    return its.value, rel.value
+
+
+class Projection(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, solver, step, u_star, v_star, p, p_prev):
+        ins = [_full(solver, u_star, "u"), _full(solver, v_star, "v"), _full(solver, p, "c"),
+               _full(solver, p_prev, "c")]
+        outs = [torch.empty_like(b) for b in ins]
+        its, rel = _call(solver, solver._lib.dn_projection, step, ins, outs)
+        ctx.solver, ctx.step = solver, int(step)
+        ctx.rho_mid = solver.get_field("rho_mid")
+        ctx.forward_report = (its, rel)
+        return tuple(_interior(solver, b) for b in outs)
+
+    @staticmethod
+    def backward(ctx, gu, gv, gp, gpp):
+        solver = ctx.solver
+        solver.set_field("rho_mid", ctx.rho_mid)
+        zeros = {"u": (solver.nx + 1, solver.ny), "v": (solver.nx, solver.ny + 1), "c": (solver.nx, solver.ny)}
+        cot = []
+        for g_, kind in zip((gu, gv, gp, gpp), ("u", "v", "c", "c")):
+            if g_ is None:
+                g_ = torch.zeros(zeros[kind], dtype=torch.float64, device="cuda")
+            cot.append(_full(solver, g_.to(torch.float64).contiguous(), kind))
+        outs = [torch.empty_like(b) for b in cot]
+        _call(solver, solver._lib.dn_projection_adjoint, ctx.step, cot, outs)
+        return (None, None) + tuple(_interior(solver, b) for b in outs)
+
+
+def projection(solver, step, u_star, v_star, p, p_prev):
+    """(u, v, p_new, p_prev_new) of one projection; differentiable in u_star, v_star, p and p_prev."""
+    return Projection.apply(solver, step, u_star, v_star, p, p_prev)
+
+
+def projection_adjoint(solver, step, gu, gv, gp, gpp):
+    """The vector-Jacobian product alone: cotangents of (u, v, p_new, p_prev_new) in, of (u_star, v_star, p,
+    p_prev) out, with the solver's current rho_mid.  Returns the four arrays and (iterations, residual)."""
+    cot = [_full(solver, gu, "u"), _full(solver, gv, "v"), _full(solver, gp, "c"), _full(solver, gpp, "c")]
+    outs = [torch.empty_like(b) for b in cot]
+    rep = _call(solver, solver._lib.dn_projection_adjoint, step, cot, outs)
+    return tuple(_interior(solver, b) for b in outs), rep

@@ -112,6 +112,8 @@ def load():
         "dn_correct": (I, [H, C.POINTER(Report)]),
         "dn_ch_linear_solve": (I, [H, DP, D, DP, DP, DP, C.POINTER(C.c_int)]),
         "dn_pressure_solve": (I, [H, I, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int), DP]),
+        "dn_projection": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
+        "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_diagnostics": (I, [H, C.POINTER(Diag)]),
         "dn_compute_mass": (I, [H, I, DP]),
         "dn_synchronize": (I, [H]),

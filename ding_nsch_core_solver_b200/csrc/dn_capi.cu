@@ -8,17 +8,18 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
-#include <atomic>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include "dn_adjoint.cuh"
 #include "dn_common.cuh"
 #include "dn_fields.cuh"
 #include "dn_krylov.cuh"
@@ -1140,6 +1141,19 @@ dn_status split_extrapolation(dn_handle *h, int step) {
 }
 
 // solve_pressure_correction_{icpcg,ildlt_pcg,liu_split_icpcg,liu_split_ildlt_pcg}, pressure.cpp:302-365, 470-491
+dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *rep);
+
+// x -= mean(x) for a compact vector of the n cells
+dn_status compact_subtract_mean(dn_handle *h, double *x) {
+  const int nb = 128;
+  k_vec_sum<<<nb, 256, 0, h->stream>>>(x, h->n, h->partials);
+  DN_TRY(check_launch(h, "k_vec_sum"));
+  k_finish_mean<<<1, 32, 0, h->stream>>>(h->partials, nb, (double)h->n, h->scal);
+  DN_TRY(check_launch(h, "k_finish_mean"));
+  k_vec_sub_scalar<<<blocks_for(h->n), 256, 0, h->stream>>>(x, h->n, h->scal);
+  return check_launch(h, "k_vec_sub_scalar");
+}
+
 dn_status pressure(dn_handle *h, int step, dn_report *rep) {
   Fv *f = h->f;
   const dn_config &cfg = h->cfg;
@@ -1154,16 +1168,18 @@ dn_status pressure(dn_handle *h, int step, dn_report *rep) {
   k_p_assemble<<<blocks_for(h->n), 256, 0, h->stream>>>(h->G, h->bc, f[DN_F_RHO_MID], f[DN_F_U_STAR], f[DN_F_V_STAR],
                                                        h->pe, split ? 1 : 0, rho_ref, cfg.dt, h->a5, h->b);
   DN_TRY(check_launch(h, "k_p_assemble"));
-  if (!h->has_dirichlet) {  // regularize_pressure_linear_system, pressure.cpp:198-212
-    const int nb = 128;
-    k_vec_sum<<<nb, 256, 0, h->stream>>>(h->b, h->n, h->partials);
-    DN_TRY(check_launch(h, "k_vec_sum"));
-    k_finish_mean<<<1, 32, 0, h->stream>>>(h->partials, nb, (double)h->n, h->scal);
-    DN_TRY(check_launch(h, "k_finish_mean"));
-    k_vec_sub_scalar<<<blocks_for(h->n), 256, 0, h->stream>>>(h->b, h->n, h->scal);
-    DN_TRY(check_launch(h, "k_vec_sub_scalar"));
-  }
-  // The split operator is constant, so its factor is built once; the variable one every step.
+  if (!h->has_dirichlet) DN_TRY(compact_subtract_mean(h, h->b));  // pressure.cpp:198-212
+  DN_TRY(pressure_factor_solve(h, split, icc, rep));
+  LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], h->x, f[DN_F_P_CORR]);
+  if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
+  return bc(h, f[DN_F_P_CORR], kBCPressure);
+}
+
+// x = A^-1 b for the assembled pressure operator a5 and right-hand side b, from x = 0: the factor (built
+// once for the constant split operator, every call for the variable one), then the PCG of the configured
+// precision and sweep form.
+dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *rep) {
+  const dn_config &cfg = h->cfg;
   const int kind = icc ? kPrecICC : kPrecLDLT;
   if (!(split && h->p_factor_valid && h->p_factor_kind == kind)) {
     DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
@@ -1197,9 +1213,7 @@ dn_status pressure(dn_handle *h, int step, dn_report *rep) {
   rep->pressure_iterations = (int)out[0];
   rep->pressure_residual = out[2];
   h->phase_ms[7] = out[0];
-  LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], h->x, f[DN_F_P_CORR]);
-  if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
-  return bc(h, f[DN_F_P_CORR], kBCPressure);
+  return DN_OK;
 }
 
 // apply_pressure_velocity_correction, operators.cpp:480-534
@@ -1717,6 +1731,84 @@ dn_status dn_pressure_solve(dn_handle *h, int step, const double *u_star, const 
   DN_TRY(pressure(h, step, &rep));
   DN_CUDA(h, cudaMemcpyAsync(p_corr, f[DN_F_P_CORR].d, f[DN_F_P_CORR].size() * sizeof(double), cudaMemcpyDeviceToHost,
                              h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (iterations) *iterations = rep.pressure_iterations;
+  if (relative_residual) *relative_residual = rep.pressure_residual;
+  return DN_OK;
+}
+
+// The projection on caller device buffers: u*, v*, p, p_prev in, u, v, p_new, p_prev_new out (Field2D
+// layouts of the handle's u, v and cell fields).  It runs the step's own pressure solve and correction on
+// the handle's fields, with the handle's rho_mid.
+dn_status dn_projection(dn_handle *h, int step, const double *u_star, const double *v_star, const double *p,
+                        const double *p_prev, double *u, double *v, double *p_new, double *p_prev_new, int *iterations,
+                        double *relative_residual) {
+  if (!h || !u_star || !v_star || !p || !p_prev || !u || !v || !p_new || !p_prev_new) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  auto d2d = [&](double *dst, const double *src, int id) -> dn_status {
+    DN_CUDA(h, cudaMemcpyAsync(dst, src, f[id].size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    return DN_OK;
+  };
+  DN_TRY(d2d(f[DN_F_U_STAR].d, u_star, DN_F_U_STAR));
+  DN_TRY(d2d(f[DN_F_V_STAR].d, v_star, DN_F_V_STAR));
+  DN_TRY(d2d(f[DN_F_P].d, p, DN_F_P));
+  DN_TRY(d2d(f[DN_F_P_PREV].d, p_prev, DN_F_P_PREV));
+  dn_report rep{};
+  DN_TRY(pressure(h, step, &rep));
+  DN_TRY(correct(h, step, &rep));
+  DN_TRY(d2d(u, f[DN_F_U].d, DN_F_U));
+  DN_TRY(d2d(v, f[DN_F_V].d, DN_F_V));
+  DN_TRY(d2d(p_new, f[DN_F_P].d, DN_F_P));
+  DN_TRY(d2d(p_prev_new, f[DN_F_P_PREV].d, DN_F_P_PREV));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (iterations) *iterations = rep.pressure_iterations;
+  if (relative_residual) *relative_residual = rep.pressure_residual;
+  return DN_OK;
+}
+
+// Transpose of dn_projection's linear part (rho_mid fixed): cotangents of the interior values of u, v,
+// p_new, p_prev_new in; cotangents of the interior values of u*, v*, p, p_prev out (ghosts zero).
+dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
+                                const double *gpp, double *au, double *av, double *ap, double *app, int *iterations,
+                                double *relative_residual) {
+  if (!h || !gu || !gv || !gp || !gpp || !au || !av || !ap || !app) return DN_ERR_INVALID_ARGUMENT;
+  const dn_config &cfg = h->cfg;
+  if (cfg.pressure_scheme == DN_P_JACOBI)
+    return fail(h, DN_ERR_UNSUPPORTED, "pressure_scheme jacobi is not implemented by the CUDA backend");
+  Fv *f = h->f;
+  const Fv &U = f[DN_F_U], &V = f[DN_F_V], &P = f[DN_F_P];
+  const Fv GU{const_cast<double *>(gu), U.nx, U.ny, U.g}, GV{const_cast<double *>(gv), V.nx, V.ny, V.g};
+  const Fv GP{const_cast<double *>(gp), P.nx, P.ny, P.g}, GPP{const_cast<double *>(gpp), P.nx, P.ny, P.g};
+  const Fv AU{au, U.nx, U.ny, U.g}, AV{av, V.nx, V.ny, V.g}, AP{ap, P.nx, P.ny, P.g}, APP{app, P.nx, P.ny, P.g};
+  DN_CUDA(h, cudaMemsetAsync(au, 0, U.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(av, 0, V.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(ap, 0, P.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(app, 0, P.size() * sizeof(double), h->stream));
+  const bool split = use_split(cfg);
+  const bool icc = cfg.pressure_scheme == DN_P_ICPCG || cfg.pressure_scheme == DN_P_SPLIT_ICPCG;
+  const double rho_ref = split ? rho_ref_of(cfg) : 1.0;
+  // face cotangents through the BCs; u* and v* take them unchanged (u = u* - ...)
+  LAUNCH_INTERIOR(k_adj_fold_u, AU, GU, AU, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adj_fold_v, AV, GV, AV, h->G, h->bc);
+  // the operator of the current rho_mid, assembled as the forward assembles it (its right-hand side is
+  // replaced below)
+  k_p_assemble<<<blocks_for(h->n), 256, 0, h->stream>>>(h->G, h->bc, f[DN_F_RHO_MID], f[DN_F_U_STAR], f[DN_F_V_STAR],
+                                                       h->pe, split ? 1 : 0, rho_ref, cfg.dt, h->a5, h->b);
+  DN_TRY(check_launch(h, "k_p_assemble"));
+  k_adj_cells_pre<<<blocks_for(h->n), 256, 0, h->stream>>>(AU, AV, GP, f[DN_F_RHO_MID], h->G, split ? 1 : 0, rho_ref,
+                                                           cfg.dt, h->b, APP);
+  DN_TRY(check_launch(h, "k_adj_cells_pre"));
+  // p_corr and the right-hand side are both mean-free without a Dirichlet side: project before and after
+  if (!h->has_dirichlet) DN_TRY(compact_subtract_mean(h, h->b));
+  dn_report rep{};
+  DN_TRY(pressure_factor_solve(h, split, icc, &rep));
+  if (!h->has_dirichlet) DN_TRY(compact_subtract_mean(h, h->x));
+  const double kappa = (split ? rho_ref : 1.0) / cfg.dt;
+  LAUNCH_INTERIOR(k_adj_div_u, AU, AU, h->x, h->G, kappa);
+  LAUNCH_INTERIOR(k_adj_div_v, AV, AV, h->x, h->G, kappa);
+  k_adj_cells_post<<<blocks_for(h->n), 256, 0, h->stream>>>(h->x, GPP, f[DN_F_RHO_MID], h->G, split ? 1 : 0, rho_ref,
+                                                            step, AP, APP);
+  DN_TRY(check_launch(h, "k_adj_cells_post"));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
   if (iterations) *iterations = rep.pressure_iterations;
   if (relative_residual) *relative_residual = rep.pressure_residual;

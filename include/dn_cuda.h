@@ -187,6 +187,24 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
                                    void *stream, int *iterations, double *relative_residual, char *err,
                                    size_t err_len);
 
+/* ---- differentiation of the projection ---------------------------------------------------------------- */
+/* The pressure projection of one step on caller DEVICE buffers (Field2D layouts of the handle's u, v and
+ * cell fields): u_star, v_star, p, p_prev in; u, v, p_new and p_prev_new (= p) out, as
+ * solve_pressure_correction + apply_pressure_velocity_correction (pressure.cpp:1031-1089,
+ * operators.cpp:480-534) compute them, with the handle's rho_mid.  Uses the handle's fields as work space.
+ * Only interior values of the inputs are read. */
+dn_status dn_projection(dn_handle *h, int step, const double *u_star, const double *v_star, const double *p,
+                        const double *p_prev, double *u, double *v, double *p_new, double *p_prev_new,
+                        int *iterations, double *relative_residual);
+/* No counterpart in the reference (it has no adjoint).  Vector-Jacobian product of dn_projection with
+ * rho_mid held fixed: cotangents gu, gv, gp, gpp of the interior values of u, v, p_new, p_prev_new in;
+ * cotangents au, av, ap, app of the interior values of u_star, v_star, p, p_prev out (ghosts set to 0).  The
+ * transposed pressure solve is the same PCG (the operator is symmetric), so it reports its iterations and
+ * relative residual; the handle's rho_mid must be the one of the forward call.  DEVICE buffers. */
+dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
+                                const double *gpp, double *au, double *av, double *ap, double *app,
+                                int *iterations, double *relative_residual);
+
 /* ---- diagnostics ------------------------------------------------------------------------------------ */
 /* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
 dn_status dn_diagnostics(dn_handle *h, dn_diag *out);
