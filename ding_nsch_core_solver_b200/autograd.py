@@ -1,4 +1,5 @@
-"""torch.autograd.Function over the projection entry points of the C-ABI.
+"""torch.autograd.Functions over the differentiable pieces of the C-ABI: the pressure projection and the
+CH advective term.
 
 `projection(solver, step, u_star, v_star, p, p_prev)` runs the pressure projection of one step --
 pressure solve plus velocity correction (dn_projection) -- on interior-shaped float64 CUDA tensors and
@@ -6,7 +7,12 @@ returns (u, v, p_new, p_prev_new).  Its backward is the hand-written discrete ad
 whose transposed pressure solve is the same PCG.  rho_mid is a constant of the map: the solver's rho_mid at
 the forward call is kept and put back before the backward runs.  The reference has no adjoint.
 
-Shapes (interior values only): u, u_star (nx+1, ny); v, v_star (nx, ny+1); p, p_prev, p_new (nx, ny).
+`advection(solver, c, u, v)` returns the CH advective term -div(u c) with WENO5 face values (dn_advection);
+its backward (dn_advection_adjoint) differentiates the WENO5 nonlinear weights.  The upwind side follows the
+sign of each face velocity, so the term is not differentiable where a face velocity is exactly 0.
+
+Shapes (interior values only): u, u_star (nx+1, ny); v, v_star (nx, ny+1); c, p, p_prev, p_new, the
+advective term (nx, ny).
 """
 import ctypes as C
 
@@ -79,3 +85,32 @@ def projection_adjoint(solver, step, gu, gv, gp, gpp):
     outs = [torch.empty_like(b) for b in cot]
     rep = _call(solver, solver._lib.dn_projection_adjoint, step, cot, outs)
     return tuple(_interior(solver, b) for b in outs), rep
+
+
+class Advection(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, solver, c, u, v):
+        ins = [_full(solver, c, "c"), _full(solver, u, "u"), _full(solver, v, "v")]
+        out = torch.empty_like(ins[0])
+        torch.cuda.current_stream().synchronize()
+        solver._check(solver._lib.dn_advection(solver._h, *[t.data_ptr() for t in ins], out.data_ptr()))
+        ctx.solver = solver
+        ctx.save_for_backward(*ins)
+        return _interior(solver, out)
+
+    @staticmethod
+    def backward(ctx, g):
+        solver = ctx.solver
+        cf, uf, vf = ctx.saved_tensors
+        gf = _full(solver, g.to(torch.float64).contiguous(), "c")
+        outs = [torch.empty_like(cf), torch.empty_like(uf), torch.empty_like(vf)]
+        torch.cuda.current_stream().synchronize()
+        solver._check(solver._lib.dn_advection_adjoint(solver._h, cf.data_ptr(), uf.data_ptr(), vf.data_ptr(),
+                                                       gf.data_ptr(), *[t.data_ptr() for t in outs]))
+        return (None,) + tuple(_interior(solver, b) for b in outs)
+
+
+def advection(solver, c, u, v):
+    """-div(u c) with WENO5 face values; differentiable in c, u and v."""
+    return Advection.apply(solver, c, u, v)
+

@@ -114,6 +114,8 @@ def load():
         "dn_pressure_solve": (I, [H, I, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int), DP]),
         "dn_projection": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
+        "dn_advection": (I, [H, VP, VP, VP, VP]),
+        "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_diagnostics": (I, [H, C.POINTER(Diag)]),
         "dn_compute_mass": (I, [H, I, DP]),
         "dn_synchronize": (I, [H]),

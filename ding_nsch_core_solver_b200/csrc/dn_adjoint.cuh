@@ -152,4 +152,165 @@ __global__ void k_adj_cells_post(const double *rbar, Fv gpp, Fv rm, Grid G, int 
   app.at(i, j) = (split && step != 0) ? -pe : 0.0;
 }
 
+// ------------------------------------------------------------------------------------------------------
+// Adjoint of the CH advective term rhs = -div(F), F_x(f) = u(f) W(c stencil of f), with W the WENO5 face
+// value (weno5_left, phase_field.cpp:144-157, upwinded by the sign of the face velocity) of c extended by
+// its scalar BC ghosts (apply_scalar_bc, operators.cpp:130-141), and the face BCs of the velocity applied to
+// F (build_phase_advection_fluxes, phase_field.cpp:283-311).  Differentiated with the nonlinear weights
+// included; the upwind switch is piecewise (the derivative in u is taken on the side of the sign of u).
+// ------------------------------------------------------------------------------------------------------
+
+// W and dW/dv_m for W = weno5_left(v1..v5): W = sum a_k q_k / S, a_k = d_k / (eps + b_k)^2, S = sum a_k, so
+// dW = sum_k a_k dq_k / S + sum_k (q_k - W) da_k / S with da_k = -2 d_k / (eps + b_k)^3 db_k.
+__device__ __forceinline__ double weno5_left_grad(const double (&v)[5], double (&dw)[5]) {
+  const double eps = 1.0e-6;
+  const double q[3] = {(2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2]) / 6.0, (-v[1] + 5.0 * v[2] + 2.0 * v[3]) / 6.0,
+                       (2.0 * v[2] + 5.0 * v[3] - v[4]) / 6.0};
+  const double dq[3][5] = {{2.0 / 6.0, -7.0 / 6.0, 11.0 / 6.0, 0.0, 0.0},
+                           {0.0, -1.0 / 6.0, 5.0 / 6.0, 2.0 / 6.0, 0.0},
+                           {0.0, 0.0, 2.0 / 6.0, 5.0 / 6.0, -1.0 / 6.0}};
+  // b_k = 13/12 s_k^2 + 1/4 t_k^2 with s_k, t_k linear in v
+  const double ds[3][5] = {{1, -2, 1, 0, 0}, {0, 1, -2, 1, 0}, {0, 0, 1, -2, 1}};
+  const double dt[3][5] = {{1, -4, 3, 0, 0}, {0, 1, 0, -1, 0}, {0, 0, 3, -4, 1}};
+  const double dk[3] = {0.1, 0.6, 0.3};
+  double a[3], da[3][5], S = 0.0, num = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double sk = 0.0, tk = 0.0;
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      sk += ds[k][m] * v[m];
+      tk += dt[k][m] * v[m];
+    }
+    const double b = 13.0 / 12.0 * sk * sk + 0.25 * tk * tk;
+    const double e = eps + b;
+    a[k] = dk[k] / (e * e);
+    const double c = -2.0 * dk[k] / (e * e * e);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) da[k][m] = c * (13.0 / 6.0 * sk * ds[k][m] + 0.5 * tk * dt[k][m]);
+    S += a[k];
+    num += a[k] * q[k];
+  }
+  const double W = num / S;
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    double g = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) g += a[k] * dq[k][m] + (q[k] - W) * da[k][m];
+    dw[m] = g / S;
+  }
+  return W;
+}
+
+// Extended cell index (-3 .. n+2) -> interior cell holding its value under the scalar BCs.
+__device__ __forceinline__ int scalar_bc_source(int e, int n, int periodic) {
+  if (e >= 0 && e < n) return e;
+  if (periodic) return e < 0 ? e + n : e - n;
+  return e < 0 ? 0 : n - 1;
+}
+
+// Cotangent of the flux at x-face f, after the velocity face BC written onto the fluxes (the same fold as
+// k_adj_fold_u) and before it: F(f) enters rhs(f-1) as -F/dx and rhs(f) as +F/dx.
+__device__ __forceinline__ double adv_flux_bar_x(const Fv &rb, const Grid &G, const BCSet &bc, int f, int j) {
+  auto raw = [&](int q) {
+    const double e = q < G.nx ? rb.at(q, j) : 0.0;
+    const double w = q > 0 ? rb.at(q - 1, j) : 0.0;
+    return (e - w) / G.dx;
+  };
+  const int last = G.nx;
+  if (G.px) return f == last ? 0.0 : (f == 0 ? raw(0) + raw(last) : raw(f));
+  if (f == 0 || f == last) return 0.0;
+  double v = raw(f);
+  if (f == 1 && bc.u[DN_LEFT].type != DN_BC_DIRICHLET) v += raw(0);
+  if (f == last - 1 && bc.u[DN_RIGHT].type != DN_BC_DIRICHLET) v += raw(last);
+  return v;
+}
+__device__ __forceinline__ double adv_flux_bar_y(const Fv &rb, const Grid &G, const BCSet &bc, int i, int f) {
+  auto raw = [&](int q) {
+    const double nn = q < G.ny ? rb.at(i, q) : 0.0;
+    const double s = q > 0 ? rb.at(i, q - 1) : 0.0;
+    return (nn - s) / G.dy;
+  };
+  const int last = G.ny;
+  if (G.py) return f == last ? 0.0 : (f == 0 ? raw(0) + raw(last) : raw(f));
+  if (f == 0 || f == last) return 0.0;
+  double v = raw(f);
+  if (f == 1 && bc.v[DN_BOTTOM].type != DN_BC_DIRICHLET) v += raw(0);
+  if (f == last - 1 && bc.v[DN_TOP].type != DN_BC_DIRICHLET) v += raw(last);
+  return v;
+}
+
+// Stencil of face f along one direction: the five values in weno5_left order and, per slot, the extended
+// cell index it reads (u >= 0: cells f-3 .. f+1; u < 0: f+2 .. f-2).
+__device__ __forceinline__ int adv_slot_cell(int f, int m, bool up) { return up ? f - 3 + m : f + 2 - m; }
+
+// u_bar(f) = F_bar(f) W(f)
+__global__ void k_adv_adj_u(Fv ce, Fv u, Fv rb, Fv ubar, Grid G, BCSet bc) {
+  DN_FOR_INTERIOR(ubar);
+  const bool up = u.at(i, j) >= 0.0;
+  double v[5], dw[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) v[m] = ce.at(adv_slot_cell(i, m, up), j);
+  ubar.at(i, j) = adv_flux_bar_x(rb, G, bc, i, j) * weno5_left_grad(v, dw);
+}
+__global__ void k_adv_adj_v(Fv ce, Fv vv, Fv rb, Fv vbar, Grid G, BCSet bc) {
+  DN_FOR_INTERIOR(vbar);
+  const bool up = vv.at(i, j) >= 0.0;
+  double v[5], dw[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) v[m] = ce.at(i, adv_slot_cell(j, m, up));
+  vbar.at(i, j) = adv_flux_bar_y(rb, G, bc, i, j) * weno5_left_grad(v, dw);
+}
+
+// Extended indices (-3 .. n+2) whose BC ghost value is interior cell i: i itself, the three ghosts beyond
+// a non-periodic edge cell, or the periodic image.  Returns how many (at most 4).
+__device__ __forceinline__ int scalar_bc_images(int i, int n, int periodic, int (&e)[4]) {
+  int k = 0;
+  e[k++] = i;
+  if (periodic) {
+    if (i >= n - 3) e[k++] = i - n;
+    if (i <= 2) e[k++] = i + n;
+  } else {
+    if (i == 0)
+      for (int g = 1; g <= 3; ++g) e[k++] = -g;
+    else if (i == n - 1)
+      for (int g = 0; g < 3; ++g) e[k++] = n + g;
+  }
+  return k;
+}
+
+// Sum over the faces along one direction whose stencil reads extended index e, of F_bar(f) u(f) dW/dv_m.
+// X selects x (faces f along i at row j) or y (faces f along j at column i).
+template <bool X>
+__device__ __forceinline__ double adv_adj_gather(const Fv &ce, const Fv &vel, const Fv &rb, const Grid &G,
+                                                 const BCSet &bc, int i, int j, int e) {
+  const int nf = X ? G.nx : G.ny;
+  double acc = 0.0;
+  for (int f = max(e - 2, 0); f <= min(e + 3, nf); ++f) {
+    const double w = X ? vel.at(f, j) : vel.at(i, f);
+    const bool up = w >= 0.0;
+    const int m = up ? e - f + 3 : f + 2 - e;
+    if (m < 0 || m > 4) continue;
+    const double fb = X ? adv_flux_bar_x(rb, G, bc, f, j) : adv_flux_bar_y(rb, G, bc, i, f);
+    double v[5], dw[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = X ? ce.at(adv_slot_cell(f, k, up), j) : ce.at(i, adv_slot_cell(f, k, up));
+    weno5_left_grad(v, dw);
+    acc += fb * w * dw[m];
+  }
+  return acc;
+}
+
+// c_bar(i, j): every face whose stencil reads cell (i, j), directly or through a BC ghost, in a fixed order.
+__global__ void k_adv_adj_c(Fv ce, Fv u, Fv vv, Fv rb, Fv cbar, Grid G, BCSet bc) {
+  DN_FOR_INTERIOR(cbar);
+  double acc = 0.0;
+  int e[4];
+  const int kx = scalar_bc_images(i, G.nx, G.px, e);
+  for (int k = 0; k < kx; ++k) acc += adv_adj_gather<true>(ce, u, rb, G, bc, i, j, e[k]);
+  const int ky = scalar_bc_images(j, G.ny, G.py, e);
+  for (int k = 0; k < ky; ++k) acc += adv_adj_gather<false>(ce, vv, rb, G, bc, i, j, e[k]);
+  cbar.at(i, j) = acc;
+}
+
 }  // namespace dn

@@ -1815,6 +1815,48 @@ dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const 
   return DN_OK;
 }
 
+// The CH advective term on caller device buffers: c (cell), u, v (faces) in, rhs = -div(u c) (cell) out,
+// computed as the phase step computes it (WENO5 faces, velocity face BCs on the fluxes).
+dn_status dn_advection(dn_handle *h, const double *c, const double *u, const double *v, double *rhs) {
+  if (!h || !c || !u || !v || !rhs) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  const Fv &CF = f[DN_F_C], &UF = f[DN_F_U], &VF = f[DN_F_V];
+  const Fv U{const_cast<double *>(u), UF.nx, UF.ny, UF.g}, V{const_cast<double *>(v), VF.nx, VF.ny, VF.g};
+  const Fv R{rhs, CF.nx, CF.ny, CF.g};
+  DN_CUDA(h, cudaMemcpyAsync(h->cmid.d, c, CF.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  LAUNCH_INTERIOR(k_adv_flux_x, h->afx, h->cmid, U, h->afx);
+  LAUNCH_INTERIOR(k_adv_flux_y, h->afy, h->cmid, V, h->afy);
+  DN_TRY(bc(h, h->afx, kBCU));
+  DN_TRY(bc(h, h->afy, kBCV));
+  LAUNCH_INTERIOR(k_flux_div, R, h->afx, h->afy, R, h->G, 1);
+  DN_TRY(bc(h, R, kBCScalar));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+// Vector-Jacobian product of dn_advection at (c, u, v): cotangent g_rhs of the interior of rhs in;
+// cotangents of the interior values of c, u, v out (ghosts set to 0).
+dn_status dn_advection_adjoint(dn_handle *h, const double *c, const double *u, const double *v, const double *g_rhs,
+                               double *c_bar, double *u_bar, double *v_bar) {
+  if (!h || !c || !u || !v || !g_rhs || !c_bar || !u_bar || !v_bar) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  const Fv &CF = f[DN_F_C], &UF = f[DN_F_U], &VF = f[DN_F_V];
+  const Fv U{const_cast<double *>(u), UF.nx, UF.ny, UF.g}, V{const_cast<double *>(v), VF.nx, VF.ny, VF.g};
+  const Fv RB{const_cast<double *>(g_rhs), CF.nx, CF.ny, CF.g};
+  const Fv CB{c_bar, CF.nx, CF.ny, CF.g}, UB{u_bar, UF.nx, UF.ny, UF.g}, VB{v_bar, VF.nx, VF.ny, VF.g};
+  DN_CUDA(h, cudaMemsetAsync(c_bar, 0, CF.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(u_bar, 0, UF.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(v_bar, 0, VF.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(h->cmid.d, c, CF.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  LAUNCH_INTERIOR(k_adv_adj_u, UB, h->cmid, U, RB, UB, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adv_adj_v, VB, h->cmid, V, RB, VB, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adv_adj_c, CB, h->cmid, U, V, RB, CB, h->G, h->bc);
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
 dn_status dn_compute_mass(dn_handle *h, int field, double *mass) {
   if (!h || !mass || field < 0 || field >= DN_F_COUNT) return DN_ERR_INVALID_ARGUMENT;
   const int nb = 128;

@@ -205,6 +205,17 @@ dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const 
                                 const double *gpp, double *au, double *av, double *ap, double *app,
                                 int *iterations, double *relative_residual);
 
+/* The CH advective term -div(u c) with WENO5 face values, as build_phase_advection_fluxes
+ * (phase_field.cpp:283-311) computes it, on caller DEVICE buffers: c (cell field), u, v (face fields) in,
+ * rhs (cell field, ghosts filled) out.  Uses the handle's work fields. */
+dn_status dn_advection(dn_handle *h, const double *c, const double *u, const double *v, double *rhs);
+/* No counterpart in the reference.  Vector-Jacobian product of dn_advection at (c, u, v), the WENO5
+ * nonlinear weights differentiated: cotangent g_rhs of the interior of rhs in; cotangents c_bar, u_bar,
+ * v_bar of the interior values of c, u, v out (ghosts 0).  The upwind choice follows the sign of each face
+ * velocity, so the map is not differentiable where a face velocity is exactly 0.  DEVICE buffers. */
+dn_status dn_advection_adjoint(dn_handle *h, const double *c, const double *u, const double *v, const double *g_rhs,
+                               double *c_bar, double *u_bar, double *v_bar);
+
 /* ---- diagnostics ------------------------------------------------------------------------------------ */
 /* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
 dn_status dn_diagnostics(dn_handle *h, dn_diag *out);

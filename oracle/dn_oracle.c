@@ -2020,6 +2020,19 @@ int orc_correct(orc_solver *s) {
   GUARD_END
 }
 
+int orc_advection(orc_solver *s, const double *c, const double *u, const double *v, double *rhs) {
+  GUARD_BEGIN
+  const int nx = s->cfg.nx, ny = s->cfg.ny, g = s->cfg.ghost;
+  const fld cf = {nx, ny, g, (double *)c}, uf = {nx + 1, ny, g, (double *)u}, vf = {nx, ny + 1, g, (double *)v};
+  fld out = {nx, ny, g, rhs}, fx, fy;
+  fld_init(&fx, nx + 1, ny, g, 0.0);
+  fld_init(&fy, nx, ny + 1, g, 0.0);
+  adv_fluxes(s, &cf, &uf, &vf, &fx, &fy, &out);
+  fld_free(&fx);
+  fld_free(&fy);
+  GUARD_END
+}
+
 int orc_finish_step(orc_solver *s) {
   GUARD_BEGIN
   refresh_mu(s);

@@ -102,6 +102,9 @@ int orc_finish_step(orc_solver *s);                /* refresh mu, solver.cpp:274
 int orc_refresh_derived(orc_solver *s);            /* restart-load rebuild of derived fields, io.cpp:412-436 */
 int orc_ch_linear_solve(orc_solver *s, const double *rhs_field, double alpha0, double *c_state,
                         double *iterate_residual, double *equation_residual); /* phase_field.cpp:437-503 */
+/* The CH advective term -div(u c) with WENO5 face values (build_phase_advection_fluxes,
+ * phase_field.cpp:283-311) of Field2D arrays c (cell), u, v (faces) into rhs (cell, interior + ghosts). */
+int orc_advection(orc_solver *s, const double *c, const double *u, const double *v, double *rhs);
 void orc_get_report(const orc_solver *s, orc_report *r);
 void orc_diagnostics(orc_solver *s, orc_diag *d); /* diagnostics.cpp:114-167 */
 double orc_compute_mass(orc_solver *s, int field_id);

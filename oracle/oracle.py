@@ -207,6 +207,8 @@ def _load(impl: str):
     }
     if impl == "reference":
         sig["time_steps"] = (C.c_double, [vp, C.c_int, C.c_int])
+    else:
+        sig["advection"] = (C.c_int, [vp, dp, dp, dp, dp])
     fns = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, pre + name)
@@ -301,6 +303,14 @@ class OracleSolver:
         self._check(self._f["ch_linear_solve"](self._h, rhs.ctypes.data_as(dp), float(alpha0), cs.ctypes.data_as(dp),
                                                C.byref(it), C.byref(eq)))
         return cs, it.value, eq.value
+
+    def advection(self, c: np.ndarray, u: np.ndarray, v: np.ndarray) -> np.ndarray:
+        """-div(u c) with WENO5 face values (port only); Field2D arrays in, the cell array out."""
+        dp = C.POINTER(C.c_double)
+        c, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (c, u, v))
+        out = np.zeros_like(self.field("c"))
+        self._check(self._f["advection"](self._h, *(a.ctypes.data_as(dp) for a in (c, u, v, out))))
+        return out
 
     def report(self) -> dict:
         r = Report()
