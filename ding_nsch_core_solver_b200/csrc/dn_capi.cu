@@ -403,10 +403,10 @@ struct dn_handle {
   int max_coop_blocks = 0;
   int nsweep = 0;   // 32-line sweep warps of the global-memory wavefront (periodic x)
   int nsweep5 = 0;  // 31-line sweep warps of the staged wavefront
-  // staged wavefront (non-periodic x): hand-over lines and launch shape
+  // staged wavefront: hand-over lines, periodic-x wrap lines and launch shape
   double *bnd_f = nullptr, *bnd_b = nullptr, *wline0 = nullptr, *zlast = nullptr;
   int sw5 = 0;                 // sweep warps per CTA, 0 = staged path unavailable
-  int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3>
+  int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3> (k_pcg<5,4> with periodic x)
   size_t sw5_warp_smem[2] = {0, 0};  // per sweep warp, [constant operator, variable operator]
   int smem_optin = 0;
   double initial_mass = 0.0;
@@ -613,7 +613,7 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
                                         std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(blocks, (h->nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
-  if (SWEEP == 3) {
+  if (SWEEP == 3 || SWEEP == 4) {
     const dn_config &c = h->cfg;
     const bool var = !use_split(c);
     Sweep5 &W = P.s5;
@@ -713,7 +713,7 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
                                         std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(blocks, (h->nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
   blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
-  const bool staged = h->sw5f > 0 && !h->G.px;
+  const bool staged = h->sw5f > 0;
   if (staged) {
     const bool var = !use_split(h->cfg);
     Sweep5T<float> &W = P.s5;
@@ -757,7 +757,9 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
   DN_TRY(reset_sync(h));
   void *args[] = {&P};
   cudaEventRecord(h->kev[0], h->stream);
-  DN_CUDA(h, cudaLaunchCooperativeKernel(staged ? (const void *)k_pcg<5, 3, float> : (const void *)k_pcg<5, 0, float>,
+  DN_CUDA(h, cudaLaunchCooperativeKernel(!staged ? (const void *)k_pcg<5, 0, float>
+                                         : h->G.px ? (const void *)k_pcg<5, 4, float>
+                                                   : (const void *)k_pcg<5, 3, float>,
                                          dim3(blocks), dim3(kBlock), args, dyn_smem, h->stream));
   cudaEventRecord(h->kev[1], h->stream);
   h->launches++;
@@ -1203,7 +1205,10 @@ dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *r
   if (cfg.precision == DN_PRECISION_MIXED) {
     DN_TRY(mixed_pressure(h, kind, out));
     rep->refinement_cycles = h->refinement_cycles;
-  } else if (h->sw5 > 0 && !h->G.px && h->nsweep >= 1) {
+  } else if (h->sw5 > 0 && h->G.px) {
+    DN_TRY((run_pcg<5, 4>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
+                          cfg.pressure_tolerance, out)));
+  } else if (h->sw5 > 0) {
     DN_TRY((run_pcg<5, 3>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
                           cfg.pressure_tolerance, out)));
   } else {
@@ -1407,32 +1412,36 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   h->nsweep5 = staged_sweep_warps(nx);
   A(dalloc(h, &h->bnd_f, 2 * (size_t)std::max(h->nsweep, h->nsweep5) * ny));
   A(dalloc(h, &h->bnd_b, 2 * (size_t)std::max(h->nsweep, h->nsweep5) * ny));
-  A(dalloc(h, &h->wline0, ny));
-  A(dalloc(h, &h->zlast, ny));
+  A(dalloc(h, &h->wline0, 2 * (size_t)ny));
+  A(dalloc(h, &h->zlast, 2 * (size_t)ny));
   if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
   {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     h->smem_optin = optin;
     auto round16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
-    h->sw5_warp_smem[0] = round16(sweep_warp_smem(2, ny));
-    h->sw5_warp_smem[1] = round16(sweep_warp_smem(4, ny));
+    // periodic x takes the staged path with its wrap terms when line nx-1 lies in another warp than line 0
+    const bool px = c.periodic_x != 0;
+    const bool stageable = !px || h->nsweep5 >= 2;
+    const void *k53 = px ? (const void *)k_pcg<5, 4> : (const void *)k_pcg<5, 3>;
+    h->sw5_warp_smem[0] = round16(sweep_warp_smem(2, ny, 8, px));
+    h->sw5_warp_smem[1] = round16(sweep_warp_smem(4, ny, 8, px));
     const size_t per = h->sw5_warp_smem[use_split(c) ? 0 : 1];
     const size_t budget = (size_t)optin > 64 + 2304 ? (size_t)optin - 64 - 2304 : 0;  // minus static smem
-    int sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
+    int sw = stageable ? (int)std::min<size_t>(kSweepWarpsPerCta, budget / per) : 0;
     sw = std::min(sw, h->nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
-    h->sw5 = sw;
-    if (sw > 0) {
+    h->sw5 = stageable ? sw : 0;
+    if (h->sw5 > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
       // The limit is a property of the kernel on this device, shared by every handle: set it to the device
       // maximum, so that a later handle with a smaller grid never lowers it below an earlier handle's need.
       cudaFuncAttributes fa{};
-      cudaFuncGetAttributes(&fa, k_pcg<5, 3>);
-      cudaFuncSetAttribute(k_pcg<5, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncGetAttributes(&fa, k53);
+      cudaFuncSetAttribute(k53, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            std::max((int)dyn, optin - (int)fa.sharedSizeBytes));
       int occ5 = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k_pcg<5, 3>, kBlock, dyn);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k53, kBlock, dyn);
       h->sw5_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * h->num_sms);
       if (h->sw5_blocks_max == 0) h->sw5 = 0;
     }
@@ -1445,22 +1454,25 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
     const int optin = h->smem_optin;
     auto round16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
-    h->sw5f_warp_smem[0] = round16(sweep_warp_smem(2, ny, 4));
-    h->sw5f_warp_smem[1] = round16(sweep_warp_smem(4, ny, 4));
+    const bool px = c.periodic_x != 0;
+    const bool stageable = !px || h->nsweep5 >= 2;
+    const void *k53f = px ? (const void *)k_pcg<5, 4, float> : (const void *)k_pcg<5, 3, float>;
+    h->sw5f_warp_smem[0] = round16(sweep_warp_smem(2, ny, 4, px));
+    h->sw5f_warp_smem[1] = round16(sweep_warp_smem(4, ny, 4, px));
     const size_t per = h->sw5f_warp_smem[use_split(c) ? 0 : 1];
     cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, k_pcg<5, 3, float>);
+    cudaFuncGetAttributes(&fa, k53f);
     const size_t budget = (size_t)optin > 64 + fa.sharedSizeBytes ? (size_t)optin - 64 - fa.sharedSizeBytes : 0;
-    int sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
+    int sw = stageable ? (int)std::min<size_t>(kSweepWarpsPerCta, budget / per) : 0;
     sw = std::min(sw, h->nsweep5);
     if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
-    h->sw5f = sw;
-    if (sw > 0) {
+    h->sw5f = stageable ? sw : 0;
+    if (h->sw5f > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
-      cudaFuncSetAttribute(k_pcg<5, 3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k53f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            std::max((int)dyn, optin - (int)fa.sharedSizeBytes));
       int occf = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, k_pcg<5, 3, float>, kBlock, dyn);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, k53f, kBlock, dyn);
       h->sw5f_blocks_max = std::min(kMaxBlocks, std::max(0, occf) * h->num_sms);
       if (h->sw5f_blocks_max == 0) h->sw5f = 0;
     }
@@ -1979,7 +1991,7 @@ struct StaticDevice {
   int num_sms;
   int smem_optin;
   int max_coop_blocks;
-  int pcg3_static_smem;
+  int pcg3_static_smem;  // static shared memory of k_pcg<5,3> / k_pcg<5,4> (the larger)
 };
 std::mutex g_static_mu;
 StaticDevice g_static_dev[kStaticMaxDevices];
@@ -2038,8 +2050,8 @@ StaticLayout static_layout(int nx, int ny, int g) {
   L.pe = take((size_t)(nx + 2 * g) * (ny + 2 * g) * sizeof(double));
   L.bnd_f = take(2 * nsweep * ny * sizeof(double));
   L.bnd_b = take(2 * nsweep * ny * sizeof(double));
-  L.wline0 = take((size_t)ny * sizeof(double));
-  L.zlast = take((size_t)ny * sizeof(double));
+  L.wline0 = take(2 * (size_t)ny * sizeof(double));
+  L.zlast = take(2 * (size_t)ny * sizeof(double));
   L.total = off;
   return L;
 }
@@ -2062,6 +2074,8 @@ dn_status static_setup(int device, StaticDevice *out, char *err, size_t err_len)
     cudaFuncAttributes fa{};
     DN_SCUDA(cudaFuncGetAttributes(&fa, k_pcg<5, 3>));
     t.pcg3_static_smem = (int)fa.sharedSizeBytes;
+    DN_SCUDA(cudaFuncGetAttributes(&fa, k_pcg<5, 4>));
+    t.pcg3_static_smem = std::max(t.pcg3_static_smem, (int)fa.sharedSizeBytes);
     // the same co-residency bound as a handle's (all persistent kernels of the library)
     int occ = 0, occ2 = 0, occ3 = 0;
     DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg<5, 0>, kBlock, 0));
@@ -2263,8 +2277,9 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   // staged wavefront: sweep warps per CTA from the shared-memory budget, as dn_create chooses them
   int sw = 0, sw_blocks_max = 0;
   size_t warp_smem = 0;
-  if (!G.px) {
-    const size_t per = (sweep_warp_smem(split ? 2 : 4, ny) + 15) & ~(size_t)15;
+  const void *k53 = G.px ? (const void *)k_pcg<5, 4> : (const void *)k_pcg<5, 3>;
+  if (!G.px || nsweep5 >= 2) {
+    const size_t per = (sweep_warp_smem(split ? 2 : 4, ny, 8, G.px != 0) + 15) & ~(size_t)15;
     const size_t budget = (size_t)D.smem_optin > 64 + 2304 ? (size_t)D.smem_optin - 64 - 2304 : 0;
     sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
     sw = std::min(sw, nsweep5);
@@ -2276,10 +2291,10 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
       } else {
         // raise the kernel's dynamic shared-memory limit to the device maximum: never below what any
         // handle on this device launches it with
-        DN_SCUDA(cudaFuncSetAttribute(k_pcg<5, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        DN_SCUDA(cudaFuncSetAttribute(k53, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       D.smem_optin - D.pcg3_static_smem));
         int occ5 = 0;
-        DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k_pcg<5, 3>, kBlock, dyn));
+        DN_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k53, kBlock, dyn));
         sw_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * D.num_sms);
         if (sw_blocks_max == 0) sw = 0;
         warp_smem = per;
@@ -2323,8 +2338,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
     blocks = std::min(blocks, sw_blocks_max);
     if (blocks < sweep_ctas)
       return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
-    DN_SCUDA(cudaLaunchCooperativeKernel((const void *)k_pcg<5, 3>, dim3(blocks), dim3(kBlock), args,
-                                         64 + (size_t)sw * warp_smem, st));
+    DN_SCUDA(cudaLaunchCooperativeKernel(k53, dim3(blocks), dim3(kBlock), args, 64 + (size_t)sw * warp_smem, st));
   } else {
     if ((long long)blocks * (kBlock / 32) < nsweep)
       return static_fail(err, err_len, DN_ERR_UNSUPPORTED, "grid too wide for the co-resident wavefront warps");

@@ -616,7 +616,8 @@ __device__ void apply_levels13_ring(const PcgArgs &P, double m_r, double (&acc)[
 }
 
 // One persistent launch runs the whole PCG.  SWEEP: 0 = 5-point pipelined wavefront on global memory,
-// 1 = level-scheduled slot factor (CTA 0), 2 = diagonal, 3 = 5-point wavefront staged through shared memory.
+// 1 = level-scheduled slot factor (CTA 0), 2 = diagonal, 3 = 5-point wavefront staged through shared memory,
+// 4 = the staged wavefront with the periodic-x wrap terms (nx >= 32).
 // The residual r is kept unprojected in memory; the mean of the latest update (m_r) is subtracted on the
 // fly by the preconditioner and folded in by the next update, which equals projecting r after every
 // update (pressure.cpp:225-239 applied in ch_sparse_krylov.hpp:602-605).
@@ -634,7 +635,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
   const int warp = threadIdx.x >> 5;
   const int nwarps_cta = blockDim.x >> 5;
   unsigned int *cnt_cta = (unsigned int *)dsm;
-  if (SWEEP == 3) {
+  if (SWEEP == 3 || SWEEP == 4) {
     if (threadIdx.x < 16) cnt_cta[threadIdx.x] = 0u;
     // cross-CTA hand-over lines start empty; the first grid reduction orders this before any sweep
     const size_t nb = 2 * (size_t)P.s5.nsweep * P.s5.ny;
@@ -643,6 +644,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
       P.s5.bnd_f[t] = empty;
       P.s5.bnd_b[t] = empty;
     }
+    if (SWEEP == 4)  // the periodic-x wrap lines, [2][ny] each
+      for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * (size_t)P.s5.ny;
+           t += (size_t)gridDim.x * blockDim.x) {
+        P.s5.wline0[t] = empty;
+        P.s5.zlast[t] = empty;
+      }
     // so do the same-CTA hand-over lines (forward and backward) of this CTA's sweep warps
     const int na = P.s5.varcoef ? 4 : 2;
     const size_t lines = 2 * (size_t)((P.s5.ny + 3) & ~3);
@@ -692,25 +699,26 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
         fwd5(P, k, epoch, m_r_now);
       for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta)
         bwd5(P, k, epoch, m_r_now, acc);
-    } else if (SWEEP == 3) {
+    } else if (SWEEP == 3 || SWEEP == 4) {
+      constexpr bool PX = SWEEP == 4;
       const int k = blockIdx.x * P.s5.sw + warp;
       if (warp < P.s5.sw && k < P.s5.nsweep) {
         char *mine = dsm + 64 + (size_t)warp * P.warp_smem;
         if (P.prec == kPrecICC) {
           if (P.s5.varcoef) {
-            fwd5_staged<true, true>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
-            bwd5_staged<true, true>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+            fwd5_staged<true, true, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<true, true, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
           } else {
-            fwd5_staged<true, false>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
-            bwd5_staged<true, false>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+            fwd5_staged<true, false, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<true, false, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
           }
         } else {
           if (P.s5.varcoef) {
-            fwd5_staged<false, true>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
-            bwd5_staged<false, true>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+            fwd5_staged<false, true, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<false, true, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
           } else {
-            fwd5_staged<false, false>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
-            bwd5_staged<false, false>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+            fwd5_staged<false, false, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, m_r_now, acc);
+            bwd5_staged<false, false, T, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
           }
         }
       }

@@ -32,6 +32,7 @@ constexpr int kChunk = 16;               // columns per cp.async chunk (= one gr
 constexpr int kHand = 16;                // steps per group (hand-over columns checked together)
 constexpr int kAhead = 1;                // chunks staged ahead of the one being consumed
 constexpr int kLines = 31;               // grid lines per sweep warp (lane 31 / lane 0 is the ghost)
+constexpr int kWrapPad = 32;             // elements of padding on each side of a periodic-x wrap line
 
 // T is the storage and arithmetic type of the sweep (double, or float for the inner solves of the
 // mixed-precision form); the sums handed back (r.z, sum z, sum r) are accumulated in double either way.
@@ -46,7 +47,8 @@ struct Sweep5T {
   const T *r;  // forward input (the pending mean m_r is subtracted on the fly)
   T *y, *z;
   T *bnd_f, *bnd_b;           // [2][nsweep][ny] edge lines handed between CTAs (by application parity)
-  T *wline0, *zlast;          // periodic-x wrap lines (unused by the staged path, which needs px = 0)
+  T *wline0, *zlast;          // [2][ny] periodic-x wrap lines (by application parity): w of line 0 for
+                              // line nx-1 (forward), z of line nx-1 for line 0 (backward)
   unsigned int *prog_f, *prog_b;  // unused by the staged path (kept for the launch arguments' layout)
   int nsweep, sw;             // sweep warps in total (ceil(nx / kLines)) / per CTA
   int warp_smem;              // bytes between consecutive sweep warps' shared-memory regions
@@ -57,10 +59,14 @@ using Sweep5 = Sweep5T<double>;
 
 __host__ __device__ inline int staged_sweep_warps(int nx) { return (nx + kLines - 1) / kLines; }
 
+// Elements of one periodic-x wrap line in shared memory (values or coefficients), padding included.
+__host__ __device__ inline size_t wrap_line_stride(int ny) { return (size_t)((ny + 3) & ~3) + 2 * kWrapPad; }
 // per-warp shared-memory footprint (bytes) for `na` staged arrays of `esize`-byte elements, two ny-long
-// hand-over lines (forward, backward) and the zero / unit rows read by lanes that own no line
-__host__ __device__ inline size_t sweep_warp_smem(int na, int ny, int esize = 8) {
-  return (size_t)na * 32 * kPitch * esize + 2 * (size_t)((ny + 3) & ~3) * esize + 2 * (size_t)kPitch * esize + 64;
+// hand-over lines (forward, backward), the zero / unit rows read by lanes that own no line, and with
+// periodic x the wrap values and coefficients
+__host__ __device__ inline size_t sweep_warp_smem(int na, int ny, int esize = 8, bool px = false) {
+  return (size_t)na * 32 * kPitch * esize + 2 * (size_t)((ny + 3) & ~3) * esize + 2 * (size_t)kPitch * esize + 64 +
+         (px ? 2 * wrap_line_stride(ny) * esize : 0);
 }
 // Offset (elements) of a sweep warp's forward hand-over line in its region; the backward line follows it.
 __host__ __device__ inline size_t sweep_hand_line(int na) { return (size_t)na * 32 * kPitch; }
@@ -284,11 +290,36 @@ __device__ __forceinline__ void stage_full(T *r0, T *r1, T *r2, T *r3, const T *
   }
 }
 
+// Wait (bounded) until this lane's value v of src[col] is no longer the sentinel; `mine` lanes only.
+// Returns false, with status set to kDevTimeout, when the wait gives up.
+template <typename T>
+__device__ __forceinline__ bool poll_line(const T *src, int col, bool mine, T &v, int *status,
+                                          unsigned long long &t_wait) {
+  bool miss = mine && hand_empty(v);
+  if (!__any_sync(0xffffffffu, miss)) return true;
+  const unsigned long long tw0 = global_ns();
+  long long spins = 0;
+  while (__any_sync(0xffffffffu, miss)) {
+    ++spins;
+    if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+      if ((threadIdx.x & 31) == 0) atomicCAS(status, kDevOk, kDevTimeout);
+      return false;
+    }
+    if (spins > 32) __nanosleep(64);
+    if (miss) {
+      v = ld_relaxed_gpu(src + col);
+      miss = hand_empty(v);
+    }
+  }
+  t_wait += global_ns() - tw0;
+  return true;
+}
+
 // Forward sweep of sweep warp k (warp slot `ws` inside its CTA).  Lane 0 is the ghost of line 31k-1, lanes
 // 1..nl own lines 31k .. 31k+nl-1; lane t runs t steps behind the ghost.  Accumulates rz (= y^T y for
 // ICC, y^T D^-1 y for ILDLT) and the sum of the projected residual into acc[1], acc[2].  Steps run in
 // groups of kHand: the hand-over check precedes a group, the publication follows it.
-template <bool ICC, bool VAR, typename T = double>
+template <bool ICC, bool VAR, typename T = double, bool PX = false>
 __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
                                             unsigned int epoch, double m_r, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
@@ -318,6 +349,16 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
   T *bline = ring_r + sweep_hand_line(na);  // forward hand-over line (line i0-1), written by the producer
   T *zrow = bline + 2 * ((ny + 3) & ~3);
   T *ones = zrow + kPitch;
+  // Periodic x (nsweep >= 2): row (nx-1, j) also subtracts aE(nx-1, j) w(0, j).  Line 0 (lane 1 of warp 0)
+  // stores w into the global wrap line; the last warp's lanes 16..31 land it, one group ahead, into a
+  // shared line (with the coefficients beside it), from which the lane of line nx-1 reads at fixed offsets.
+  T *const xline = ones + kPitch + kWrapPad;
+  T *const xcoef = xline + wrap_line_stride(ny);
+  const bool wprod = PX && k == 0 && lane == 1;
+  const bool wcons = PX && k == nsweep - 1;
+  const int wl = nx - i0;  // lane of line nx-1 in the last warp
+  const bool wlane = wcons && lane == wl;
+  T *const wbuf = PX ? P.wline0 + (size_t)(epoch & 1u) * ny : nullptr;
   const bool vec16 = (ny % (16 / (int)sizeof(T))) == 0;  // 16-byte pieces
   const bool prod_local = has_prod && (ws > 0);
   const bool has_cons = (k + 1 < nsweep);
@@ -395,10 +436,37 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
     __syncwarp();
     return true;
   };
+  auto wrap_col = [&](int c) { return c * kChunk - wl + (lane - 16); };
+  auto wrap_issue = [&](int c, T &cf) -> T {
+    const int col = wrap_col(c);
+    const bool mine = lane >= 16 && col >= 0 && col < ny;
+    cf = (VAR && mine) ? P.aE[(size_t)(nx - 1) * ny + col] : T(0);
+    return mine ? ld_relaxed_gpu(wbuf + col) : T(0);
+  };
+  auto wrap_land = [&](int c, T v, T cf) -> bool {
+    const int col = wrap_col(c);
+    const bool mine = lane >= 16 && col >= 0 && col < ny;
+    if (!poll_line(wbuf, col, mine, v, status, t_wait)) return false;
+    if (mine) {
+      xline[col] = v;
+      if (VAR) xcoef[col] = cf;
+      wbuf[col] = hand_empty_value<T>();
+    }
+    __syncwarp();
+    return true;
+  };
   for (int c = 0; c < kAhead; ++c) {
     if (remote && !hand_land(c, hand_issue(c))) {
       cp_async_wait0();
       return;
+    }
+    if (wcons) {
+      T cf;
+      const T v = wrap_issue(c, cf);
+      if (!wrap_land(c, v, cf)) {
+        cp_async_wait0();
+        return;
+      }
     }
     stage(c);
   }
@@ -407,6 +475,8 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
   for (int q = 0; q < nchunk; ++q) {
     stage(q + kAhead);
     const T hv = remote ? hand_issue(q + kAhead) : T(0);
+    T xcf = T(0);
+    const T xv = wcons ? wrap_issue(q + kAhead, xcf) : T(0);
     cp_async_wait_ahead();
     __syncwarp();
     const int s0 = q * kChunk;
@@ -425,7 +495,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
       const T *sb = s_row + slot;
       T *yp = ydst + j0;
       T *hp = hdst + j0;
-      T rvv[kHand], dvv[kHand], asv[kHand], awv[kHand];
+      T rvv[kHand], dvv[kHand], asv[kHand], awv[kHand], xvv[PX ? kHand : 1], xcv[PX ? kHand : 1];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         rvv[ss] = rb[ss];
@@ -433,13 +503,25 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
         asv[ss] = VAR ? sb[ss] : as_c;
         awv[ss] = VAR ? wb[ss] : aw_c;
       }
+      if constexpr (PX) {
+        const T *xb = wlane ? xline + j0 : zrow + slot;
+        const T *xc = wlane ? xcoef + j0 : zrow + slot;
+        const T ae_w = wlane ? cx : T(0);
+#pragma unroll
+        for (int ss = 0; ss < kHand; ++ss) {
+          xvv[ss] = xb[ss];
+          xcv[ss] = VAR ? xc[ss] : ae_w;
+        }
+      }
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         const T rv = rvv[ss] - m_lane;
         const T dv = dvv[ss];
         const T as = asv[ss];
         const T aw = awv[ss];
-        const T t1 = fma(-as, w_prev, rv);
+        T t0 = rv;
+        if constexpr (PX) t0 = fma(-xcv[ss], xvv[ss], t0);  // wrap (0, j): the smallest column of row (nx-1, j)
+        const T t1 = fma(-as, w_prev, t0);
         const T w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
         const T sum = fma(-aw, w_up, t1);
         const T yv = ICC ? sum * dv : sum;
@@ -448,6 +530,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
         rz = fma((double)yv, (double)(ICC ? yv : wv), rz);
         rsum += rv;
         st_generic_if(hp + ss, wv, hand);
+        if constexpr (PX) st_global_if(wbuf + j0 + ss, wv, wprod);
         w_prev = wv;
       }
     } else {
@@ -476,6 +559,9 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
         // own-line terms first (periodic-y wrap, S), so that one FMA follows the shuffle from line i-1; a
         // lane's first active step has w_prev = 0, so the S term vanishes at j = 0
         T t1 = rv;
+        if constexpr (PX) {
+          if (wlane && act) t1 = fma(-(VAR ? xcoef[j] : cx), xline[j], t1);
+        }
         if (py && j == ny - 1 && real) t1 = fma(-(VAR ? gN[(size_t)i * ny + j] : cy), w_first, t1);
         t1 = fma(-asv[ss], w_prev, t1);
         const T w_up = __shfl_up_sync(0xffffffffu, w_prev, 1);
@@ -486,6 +572,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
         rz = (act && real) ? fma((double)yv, (double)(ICC ? yv : wv), rz) : rz;
         rsum = (act && real) ? rsum + rv : rsum;
         st_generic_if(hdst + j, wv, act && hand);
+        if constexpr (PX) st_global_if(wbuf + j, wv, act && wprod);
         w_first = (py && j == 0) ? wv : w_first;
         w_prev = act ? wv : w_prev;
       }
@@ -493,6 +580,10 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
     __syncwarp();
     if (prod_local && hcol >= 0) bline[hcol] = empty;  // consumed: back to the sentinel for the next application
     if (remote && !hand_land(q + kAhead, hv)) {
+      cp_async_wait0();
+      return;
+    }
+    if (wcons && !wrap_land(q + kAhead, xv, xcf)) {
       cp_async_wait0();
       return;
     }
@@ -515,7 +606,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
 // Backward sweep of sweep warp k.  Lanes 0..nl-1 own lines 31k .. 31k+nl-1; lane 31 is the ghost of line
 // 31k+31 when a next warp exists.  The lead lane (the ghost, or the last real lane of the last warp) runs
 // first, lane t (lead-t) steps behind it.  Accumulates the sum of z into acc[0].
-template <bool ICC, bool VAR, typename T = double>
+template <bool ICC, bool VAR, typename T = double, bool PX = false>
 __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp, unsigned int *cnt_cta, int k, int ws,
                                             unsigned int epoch, double (&acc)[3]) {
   const int lane = threadIdx.x & 31;
@@ -550,6 +641,16 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
   T *bline = ring_y + sweep_hand_line(na) + ((ny + 3) & ~3);  // backward hand-over line (line i0+31)
   T *zrow = ring_y + sweep_hand_line(na) + 2 * ((ny + 3) & ~3);
   T *ones = zrow + kPitch;
+  // Periodic x (nsweep >= 2): row (0, j) also adds aW(0, j) z(nx-1, j) to its upper sum.  Line nx-1 (the
+  // lead lane of the last warp) stores z into the global wrap line; warp 0's lanes 16..31 land it into the
+  // shared wrap line (free again: warp 0 is not the forward's wrap consumer), read by lane 0 (line 0).
+  T *const xline = ones + kPitch + kWrapPad;
+  T *const xcoef = xline + wrap_line_stride(ny);
+  const bool zprod = PX && k == nsweep - 1 && lane == nl - 1;
+  const bool zcons = PX && k == 0;
+  const bool zlane = zcons && lane == 0;
+  T *const zbuf = PX ? P.zlast + (size_t)(epoch & 1u) * ny : nullptr;
+  unsigned long long t_wrap = 0;
   const bool vec16 = (ny % (16 / (int)sizeof(T))) == 0;  // 16-byte pieces
   const int total = ny + lead;
   const int nchunk = (total + kChunk - 1) / kChunk;
@@ -617,10 +718,38 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
     __syncwarp();
     return true;
   };
+  // lane 0 (skew `lead`) reads columns ny-1-(c*kChunk-lead)-ss in group c
+  auto wrap_col = [&](int c) { return ny - 1 - (c * kChunk - lead) - (lane - 16); };
+  auto wrap_issue = [&](int c, T &cf) -> T {
+    const int col = wrap_col(c);
+    const bool mine = lane >= 16 && col >= 0 && col < ny;
+    cf = (VAR && mine) ? P.aW[col] : T(0);
+    return mine ? ld_relaxed_gpu(zbuf + col) : T(0);
+  };
+  auto wrap_land = [&](int c, T v, T cf) -> bool {
+    const int col = wrap_col(c);
+    const bool mine = lane >= 16 && col >= 0 && col < ny;
+    if (!poll_line(zbuf, col, mine, v, status, t_wrap)) return false;
+    if (mine) {
+      xline[col] = v;
+      if (VAR) xcoef[col] = cf;
+      zbuf[col] = hand_empty_value<T>();
+    }
+    __syncwarp();
+    return true;
+  };
   for (int c = 0; c < kAhead; ++c) {
     if (remote && !hand_land(c, hand_issue(c))) {
       cp_async_wait0();
       return;
+    }
+    if (zcons) {
+      T cf;
+      const T v = wrap_issue(c, cf);
+      if (!wrap_land(c, v, cf)) {
+        cp_async_wait0();
+        return;
+      }
     }
     stage(c);
   }
@@ -629,6 +758,8 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
   for (int q = 0; q < nchunk; ++q) {
     stage(q + kAhead);
     const T hv = remote ? hand_issue(q + kAhead) : T(0);
+    T xcf = T(0);
+    const T xv = zcons ? wrap_issue(q + kAhead, xcf) : T(0);
     cp_async_wait_ahead();
     __syncwarp();
     const int s0 = q * kChunk;
@@ -649,7 +780,7 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
       const T *eb = e_row + kMirror + slot;
       T *zp = zdst + jt;
       T *hp = hdst + jt;
-      T yvv[kHand], dvv[kHand], anv[kHand], aev[kHand];
+      T yvv[kHand], dvv[kHand], anv[kHand], aev[kHand], xvv[PX ? kHand : 1], xcv[PX ? kHand : 1];
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         yvv[ss] = yb[-ss];
@@ -657,18 +788,30 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
         anv[ss] = VAR ? nb[-ss] : an_c;
         aev[ss] = VAR ? eb[-ss] : ae_c;
       }
+      if constexpr (PX) {
+        const T *xb = zlane ? xline + jt : zrow + kMirror + slot;
+        const T *xc = zlane ? xcoef + jt : zrow + kMirror + slot;
+        const T aw_w = zlane ? cx : T(0);
+#pragma unroll
+        for (int ss = 0; ss < kHand; ++ss) {
+          xvv[ss] = xb[-ss];
+          xcv[ss] = VAR ? xc[-ss] : aw_w;
+        }
+      }
 #pragma unroll
       for (int ss = 0; ss < kHand; ++ss) {
         const T yv = yvv[ss];
         const T dv = dvv[ss];
         const T an = anv[ss];
         const T ae = aev[ss];
-        const T t = an * z_prev;
+        T t = an * z_prev;
+        if constexpr (PX) t = fma(xcv[ss], xvv[ss], t);  // wrap (nx-1, j) of row (0, j)
         const T z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
         const T zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
         st_global_if(zp - ss, zv, real);
         zsum += zv;
         st_generic_if(hp - ss, zv, hand);
+        if constexpr (PX) st_global_if(zbuf + jt - ss, zv, zprod);
         z_prev = zv;
       }
     } else {
@@ -699,12 +842,16 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
         // first, one FMA (plus the final scaling) follows the shuffle from line i+1
         T t = anv[ss] * z_prev;
         if (py && j == 0 && real) t = fma(VAR ? gS[(size_t)i * ny] : cy, z_first, t);
+        if constexpr (PX) {
+          if (zlane && act) t = fma(VAR ? xcoef[j] : cx, xline[j], t);
+        }
         const T z_dn = __shfl_down_sync(0xffffffffu, z_prev, 1);
         // ICC: z = (y - d t) d = y d - d^2 t ; ILDLT: z = D^-1 (y - t)
         const T zv = ICC ? fma(-(dv * dv), fma(ae, z_dn, t), yv * dv) : dv * (yv - fma(ae, z_dn, t));
         st_global_if(zdst + j, zv, act && real);
         zsum = (act && real) ? zsum + zv : zsum;
         st_generic_if(hdst + j, zv, act && hand);
+        if constexpr (PX) st_global_if(zbuf + j, zv, act && zprod);
         z_first = (py && j == ny - 1) ? zv : z_first;
         z_prev = act ? zv : z_prev;
       }
@@ -712,6 +859,10 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
     __syncwarp();
     if (prod_local && hcol >= 0) bline[hcol] = empty;  // consumed: back to the sentinel
     if (remote && !hand_land(q + kAhead, hv)) {
+      cp_async_wait0();
+      return;
+    }
+    if (zcons && !wrap_land(q + kAhead, xv, xcf)) {
       cp_async_wait0();
       return;
     }
