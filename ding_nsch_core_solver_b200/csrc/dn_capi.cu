@@ -35,6 +35,8 @@ constexpr int kHostScal = 8192;  // pinned host scratch (doubles): scalars and r
 // first and slows both; fewer warps per CTA put more hand-overs across CTAs (measured 81.9 ms per pressure
 // solve with 4, 87.8 with 5, 92.6 with 1 on the 192 x 384 bench workload).
 constexpr int kSweepWarpsPerCta = 4;
+// dynamic shared memory the CH PCG kernel may use (the ring of the level sweep, the periodic-y line buffers)
+constexpr size_t kSeqSmemMax = 96 * 1024;
 
 // ---------------------------------------------------------------------------------------------------
 // Pressure system (build_pressure_linear_system, pressure.cpp:123-196) into 5 slots W,S,C,N,E + rhs
@@ -603,9 +605,13 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   P.warp_smem = 0;
   P.rows13 = Rows13{};
   size_t dyn_smem = 0;
+  P.seq_lines = 0;
   if (S == 13 && SWEEP == 1 && h->rows13.lval != nullptr) {  // ring of kLvlRing levels x nx doubles
     P.rows13 = h->rows13;
     dyn_smem = (size_t)kLvlRing * h->G.nx * sizeof(double);
+  } else if (S == 13 && SWEEP == 1 && h->G.py && 9 * (size_t)h->G.ny * sizeof(double) <= kSeqSmemMax) {
+    P.seq_lines = 1;  // periodic y: line-staged sequential sweeps
+    dyn_smem = 9 * (size_t)h->G.ny * sizeof(double);
   }
   // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
   const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
@@ -1389,9 +1395,11 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     A(dalloc(h, &h->rows13.ucol, (size_t)k * h->n));
     A(dalloc(h, &h->rows13.lsrc, (size_t)k * h->n));
     A(dalloc(h, &h->rows13.usrc, (size_t)k * h->n));
-    // the ring is dynamic shared memory of the CH PCG kernel; allow the largest ring any handle uses
-    cudaFuncSetAttribute(k_pcg<13, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   }
+  // the CH PCG kernel's dynamic shared memory (the ring, or the periodic-y line buffers): allow the largest
+  // amount any handle uses
+  if ((h->rows13.lval != nullptr || c.periodic_y) && s == DN_OK)
+    cudaFuncSetAttribute(k_pcg<13, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSeqSmemMax);
   h->ml = MomLayout{nx, ny, c.periodic_x, c.periodic_y, (long long)(nx + 1) * ny, (long long)nx * (ny + 1)};
   h->nm = h->ml.nu + h->ml.nv;
   A(dalloc(h, &h->mcoef, 9 * h->nm));

@@ -345,6 +345,7 @@ struct PcgArgsT {
   Rows13 rows13;   // ordered factor rows of the 13-point operator (SWEEP 1, y not periodic); lval null: unused
   Sweep5T<T> s5;   // staged wavefront (SWEEP 3)
   int warp_smem;   // shared-memory bytes per sweep warp (SWEEP 3)
+  int seq_lines;   // 13-point with periodic y: 1 = line-staged sequential sweeps (9 ny doubles of dynamic smem)
 };
 using PcgArgs = PcgArgsT<double>;
 
@@ -615,6 +616,179 @@ __device__ void apply_levels13_ring(const PcgArgs &P, double m_r, double (&acc)[
   }
 }
 
+// 13-point ILDLT/ICC sweeps with periodic y, where the dependency graph is one chain over all rows in
+// natural order.  The chain is only carried along a line: a row's lower neighbours in earlier lines were
+// finished with those lines, and in the reference's ascending column order they come before its same-line
+// neighbours (its upper neighbours in later lines come after them).  So, per line, all threads of CTA 0
+// first form each row's earlier-line sum (forward) or its later-line products (backward) in shared memory,
+// and thread 0 then runs the line's recurrence with the previous values in registers.  Every row performs
+// the same operations in the same order as apply_levels, so the results are identical.  Interior rows
+// (2 <= j < ny-2) use the fixed same-line pattern (j-1, j-2 / j+1, j+2); the four wrap rows of a line take
+// the general slot loop.
+__device__ void apply_seq13(const PcgArgs &P, double m_r, double (&acc)[3], double *sm) {
+  constexpr int S = 13;
+  const SpOp &A = P.A;
+  const int n = A.n, nx = A.nx, ny = A.ny;
+  const bool icc = P.prec == kPrecICC;
+  double *part = sm, *c1 = sm + ny, *c2 = sm + 2 * ny, *dv = sm + 3 * ny;
+  double *q = sm + 4 * ny;    // backward: four later-line products per row, [4][ny]
+  double *fit = sm + 8 * ny;  // backward: 1 when the row takes the fixed pattern
+  auto interior = [&](int j) { return j >= 2 && j < ny - 2; };
+  // ---- forward: y_r = (r_r - m - sum_{lower, ascending} L y) (* dinv for ICC)
+  for (int i = 0; i < nx; ++i) {
+    const long long base = (long long)i * ny;
+    for (int j = threadIdx.x; j < ny; j += blockDim.x) {
+      const long long r = base + j;
+      int slots[S];
+      long long cols[S];
+      const int cnt = lower_slots<S>(A, i, j, slots, cols);
+      double sum = P.r[r] - m_r;
+      int p = 0;
+      for (; p < cnt && cols[p] < base; ++p) sum -= P.l[(size_t)slots[p] * n + r] * P.y[cols[p]];
+      part[j] = sum;
+      double l1 = 0.0, l2 = 0.0;
+      for (; p < cnt; ++p) {
+        if (cols[p] == r - 1) l1 = P.l[(size_t)slots[p] * n + r];
+        if (cols[p] == r - 2) l2 = P.l[(size_t)slots[p] * n + r];
+      }
+      c1[j] = l1;
+      c2[j] = l2;
+      dv[j] = P.dinv[r];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      auto general = [&](int j) -> double {
+        const long long r = base + j;
+        int slots[S];
+        long long cols[S];
+        const int cnt = lower_slots<S>(A, i, j, slots, cols);
+        double sum = part[j];
+        for (int p = 0; p < cnt; ++p)
+          if (cols[p] >= base) sum -= P.l[(size_t)slots[p] * n + r] * P.y[cols[p]];
+        const double yv = icc ? sum * dv[j] : sum;
+        P.y[r] = yv;
+        return yv;
+      };
+      double ym2 = general(0);  // y(i, j-2)
+      double ym1 = general(1);  // y(i, j-1)
+#pragma unroll 4
+      for (int j = 2; j < ny - 2; ++j) {
+        double sum = part[j];
+        sum -= c2[j] * ym2;
+        sum -= c1[j] * ym1;
+        const double yv = icc ? sum * dv[j] : sum;
+        P.y[base + j] = yv;
+        ym2 = ym1;
+        ym1 = yv;
+      }
+      general(ny - 2);
+      general(ny - 1);
+    }
+    __syncthreads();
+  }
+  // ---- backward: z_r = y_r (/D) - sum_{c > r ascending} L_cr z_c (* dinv for ICC); rows in descending order
+  for (int i = nx - 1; i >= 0; --i) {
+    const long long base = (long long)i * ny;
+    for (int j = threadIdx.x; j < ny; j += blockDim.x) {
+      const long long r = base + j;
+      double e1 = 0.0, e2 = 0.0, qv[4] = {0.0, 0.0, 0.0, 0.0};
+      int nq = 0;
+      bool fits = interior(j);
+      if (fits) {
+        int slots[S];
+        long long cols[S];
+        int cnt = 0;
+        for (int s = 0; s < S; ++s) {
+          const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+          if (c <= r) continue;
+          const double lcr = P.l[(size_t)(S - 1 - s) * n + c];
+          if (lcr == 0.0) continue;
+          int p = cnt++;
+          while (p > 0 && cols[p - 1] > c) {
+            cols[p] = cols[p - 1];
+            slots[p] = slots[p - 1];
+            --p;
+          }
+          cols[p] = c;
+          slots[p] = s;
+        }
+        // same-line entries (r+1, r+2) first in ascending order, then the later-line products
+        int p = 0;
+        for (; p < cnt && cols[p] < base + ny; ++p) {
+          const double lcr = P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]];
+          if (cols[p] == r + 1) e1 = lcr;
+          else if (cols[p] == r + 2) e2 = lcr;
+          else fits = false;
+        }
+        for (; p < cnt; ++p) {
+          if (nq == 4) {
+            fits = false;
+            break;
+          }
+          qv[nq++] = P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
+        }
+      }
+      part[j] = icc ? P.y[r] : P.y[r] * P.dinv[r];
+      c1[j] = e1;
+      c2[j] = e2;
+      dv[j] = P.dinv[r];
+      fit[j] = fits ? 1.0 : 0.0;
+      for (int k = 0; k < 4; ++k) q[(size_t)k * ny + j] = qv[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      auto general = [&](int j) -> double {
+        const long long r = base + j;
+        int slots[S];
+        long long cols[S];
+        int cnt = 0;
+        for (int s = 0; s < S; ++s) {
+          const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+          if (c <= r) continue;
+          const double lcr = P.l[(size_t)(S - 1 - s) * n + c];
+          if (lcr == 0.0) continue;
+          int p = cnt++;
+          while (p > 0 && cols[p - 1] > c) {
+            cols[p] = cols[p - 1];
+            slots[p] = slots[p - 1];
+            --p;
+          }
+          cols[p] = c;
+          slots[p] = s;
+        }
+        double sum = part[j];
+        for (int p = 0; p < cnt; ++p) sum -= P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
+        return icc ? sum * P.dinv[r] : sum;
+      };
+      double zp1 = 0.0, zp2 = 0.0;  // z(i, j+1), z(i, j+2)
+      for (int j = ny - 1; j >= 0; --j) {
+        double zv;
+        if (fit[j] != 0.0) {
+          double sum = part[j];
+          sum -= c1[j] * zp1;
+          sum -= c2[j] * zp2;
+          sum -= q[j];
+          sum -= q[(size_t)ny + j];
+          sum -= q[2 * (size_t)ny + j];
+          sum -= q[3 * (size_t)ny + j];
+          zv = icc ? sum * dv[j] : sum;
+        } else {
+          zv = general(j);
+        }
+        const long long r = base + j;
+        P.z[r] = zv;
+        const double rv = P.r[r] - m_r;
+        acc[0] += zv;
+        acc[1] += rv * zv;
+        acc[2] += rv;
+        zp2 = zp1;
+        zp1 = zv;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // One persistent launch runs the whole PCG.  SWEEP: 0 = 5-point pipelined wavefront on global memory,
 // 1 = level-scheduled slot factor (CTA 0), 2 = diagonal, 3 = 5-point wavefront staged through shared memory,
 // 4 = the staged wavefront with the periodic-x wrap terms (nx >= 32).
@@ -727,6 +901,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
         if (blockIdx.x == 0) {
           if (S == 13 && P.rows13.lval != nullptr && P.rows13.k == 6)
             apply_levels13_ring<6>(P, m_r_now, acc, (double *)dsm);
+          else if (S == 13 && P.seq_lines)
+            apply_seq13(P, m_r_now, acc, (double *)dsm);
           else
             apply_levels<S>(P, m_r_now, acc);
         }
