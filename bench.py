@@ -26,6 +26,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The ensemble arm runs one stream per instance; the CUDA runtime maps streams onto this many hardware work
+# queues (8 by default), and streams sharing a queue serialise.  Read when the process creates its context.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -72,6 +75,29 @@ def initial_state(cfg: dict, seed: int = 2) -> dict:
 
 
 PCG_PROFILE = os.path.join(ROOT, "profiles", "k_pcg_5_3_pressure_192x384.txt")
+
+
+def ensemble_cfgs(count: int, seed: int = 4) -> list:
+    """Droplet instances of uneven grids: nx, ny each from {64, 96, 128, 192, 256}; unit square, periodic
+    both ways; radius U(0.15, 0.3) at a centre kept 0.05 inside the box; density and viscosity ratios
+    log-uniform in [1, 100]; surface tension multiplier U(0.5, 2) with re = ca = 1; cn = 1.5 min(dx, dy);
+    uniform background velocity U(-0.1, 0.1)^2; split_icpcg in the mixed-precision form."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx, ny = (int(v) for v in rng.choice([64, 96, 128, 192, 256], size=2))
+        radius = rng.uniform(0.15, 0.3)
+        cx, cy = rng.uniform(radius + 0.05, 1.0 - radius - 0.05, size=2)
+        au, av = rng.uniform(-0.1, 0.1, size=2)
+        out.append(dict(
+            name=f"droplet_{nx}x{ny}", mode="coupled", nx=nx, ny=ny, ghost=3, lx=1.0, ly=1.0, periodic_x=True,
+            periodic_y=True, interface_center_x=float(cx), interface_center_y=float(cy), interface_radius=float(radius),
+            density_ratio=float(10 ** rng.uniform(0, 2)), viscosity_ratio=float(10 ** rng.uniform(0, 2)),
+            surface_tension_multiplier=float(rng.uniform(0.5, 2.0)), re=1.0, ca=1.0, cn=1.5 / max(nx, ny),
+            advect_u=float(au), advect_v=float(av), dt=1e-5, pressure_scheme="split_icpcg", precision="mixed",
+            poisson_iterations=2000, pressure_tolerance=1e-10, ch_inner_iterations=500, ch_tolerance=1e-10,
+            momentum_iterations=200, momentum_tolerance=1e-10))
+    return out
 
 
 def pcg_traffic_per_launch():
@@ -346,6 +372,52 @@ def run_ours(args):
         for s in members:
             s.close()
 
+    # ---- ensemble of uneven droplet instances (periodic both ways, mixed precision), all through one
+    # dn_step_batch call per batch step; each handle's persistent grids take 1/count of the SMs
+    ensemble = None
+    if args.ensemble > 0:
+        cfgs = ensemble_cfgs(args.ensemble)
+        members = []
+        try:
+            for ec in cfgs:
+                m = dn.Solver(dict(ec, device_share=len(cfgs)), device=device)
+                m.initialize()
+                m.set_initial_mass(m.compute_mass("c"))
+                members.append(m)
+            estep = 0
+            for _ in range(args.warmup):
+                capi.step_batch(members, [estep] * len(members))
+                estep += 1
+            etimes, ereps = [], []
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                ereps.append(capi.step_batch(members, [estep] * len(members)))
+                e1.record()
+                e1.synchronize()
+                etimes.append(e0.elapsed_time(e1))
+                estep += 1
+            cells = sum(c["nx"] * c["ny"] for c in cfgs)
+            etotal = reduce_max(dist, sum(etimes))
+            diag = [m.diagnostics() for m in members]
+            ensemble = {"instances": len(cfgs), "cells": cells,
+                        "value": round(cells * args.steps * world / (etotal * 1e-3) / 1e6, 4), "unit": "Mcell-steps/s",
+                        "ms_per_batch_step": round(etotal / args.steps, 3),
+                        "pressure_iterations_mean": round(statistics.mean(
+                            r["pressure_iterations"] for rs in ereps for r in rs), 1),
+                        "ch_iterations_mean": round(statistics.mean(r["ch_iterations"] for rs in ereps for r in rs), 1),
+                        "max_velocity_max": max(d["max_velocity"] for d in diag),
+                        "mass_drift_max": max(d["mass_drift"] for d in diag),
+                        "workload": "uneven droplets: grids {64..256}^2, periodic both ways, split_icpcg, mixed, "
+                                    "dt 1e-5, seed 4; all instances stepped together by dn_step_batch",
+                        "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS")}
+        except capi.DnError as e:
+            ensemble = {"instances": len(cfgs), "error": str(e)}
+        for m in members:
+            m.close()
+
     # ---- roofline of the dominant kernel (the pressure PCG), bytes per launch / launch time
     peak, peak_kind = hbm_peak()
     bytes_per_launch = PCG_BYTES_PER_CELL_IT * n_cells * statistics.mean(pcg_its)
@@ -396,6 +468,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "mixed": mixed,
             "batched": batched,
+            "ensemble": ensemble,
             "e2e": {"value": round(e2e_value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": h2d},
             "gpu_launches": launches,
@@ -449,6 +522,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--batch", type=int, default=8, help="instances of the batched-ensemble arm (0 skips it)")
+    ap.add_argument("--ensemble", type=int, default=64, help="uneven droplet instances of the ensemble arm (0 skips)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -144,7 +144,9 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep);
  * dn_step of each of `count` distinct handles, run concurrently -- each on its own stream from a host worker
  * thread -- so that many small instances fill the GPU.  steps[a] is handle a's step index (NULL: 0);
  * reports (NULL allowed) receives one dn_report per handle.  Each handle's result equals its dn_step alone.
- * Returns the first failing handle's status (its message via dn_last_error). */
+ * Returns the first failing handle's status (its message via dn_last_error).  The CUDA runtime maps streams
+ * onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 unless the environment sets it before the process
+ * creates its CUDA context; up to 32), and streams that share a queue serialise. */
 dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, dn_report *reports);
 /* history copies at the start of advance_one_timestep (solver.cpp:225-231) */
 dn_status dn_begin_step(dn_handle *h, int step);
