@@ -609,9 +609,10 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
   if (S == 13 && SWEEP == 1 && h->rows13.lval != nullptr) {  // ring of kLvlRing levels x nx doubles
     P.rows13 = h->rows13;
     dyn_smem = (size_t)kLvlRing * h->G.nx * sizeof(double);
-  } else if (S == 13 && SWEEP == 1 && h->G.py && 9 * (size_t)h->G.ny * sizeof(double) <= kSeqSmemMax) {
+  } else if (S == 13 && SWEEP == 1 && h->G.py &&
+             (size_t)seq13_smem_doubles_per_row() * h->G.ny * sizeof(double) <= kSeqSmemMax) {
     P.seq_lines = 1;  // periodic y: line-staged sequential sweeps
-    dyn_smem = 9 * (size_t)h->G.ny * sizeof(double);
+    dyn_smem = (size_t)seq13_smem_doubles_per_row() * h->G.ny * sizeof(double);
   }
   // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
   const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;

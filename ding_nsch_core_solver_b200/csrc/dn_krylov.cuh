@@ -345,7 +345,7 @@ struct PcgArgsT {
   Rows13 rows13;   // ordered factor rows of the 13-point operator (SWEEP 1, y not periodic); lval null: unused
   Sweep5T<T> s5;   // staged wavefront (SWEEP 3)
   int warp_smem;   // shared-memory bytes per sweep warp (SWEEP 3)
-  int seq_lines;   // 13-point with periodic y: 1 = line-staged sequential sweeps (9 ny doubles of dynamic smem)
+  int seq_lines;   // 13-point with periodic y: 1 = line-staged sequential sweeps (seq13 dynamic smem)
 };
 using PcgArgs = PcgArgsT<double>;
 
@@ -620,20 +620,28 @@ __device__ void apply_levels13_ring(const PcgArgs &P, double m_r, double (&acc)[
 // natural order.  The chain is only carried along a line: a row's lower neighbours in earlier lines were
 // finished with those lines, and in the reference's ascending column order they come before its same-line
 // neighbours (its upper neighbours in later lines come after them).  So, per line, all threads of CTA 0
-// first form each row's earlier-line sum (forward) or its later-line products (backward) in shared memory,
-// and thread 0 then runs the line's recurrence with the previous values in registers.  Every row performs
-// the same operations in the same order as apply_levels, so the results are identical.  Interior rows
-// (2 <= j < ny-2) use the fixed same-line pattern (j-1, j-2 / j+1, j+2); the four wrap rows of a line take
-// the general slot loop.
+// first gather everything a row needs into shared memory -- its earlier-line sum (forward) or later-line
+// products (backward), and the coefficients and offsets of its same-line neighbours -- and thread 0 then
+// runs the line's recurrence from shared memory alone, interior rows (2 <= j < ny-2, same-line neighbours
+// j-1, j-2 / j+1, j+2) with the previous values in registers.  Every row performs the same operations in the
+// same order as apply_levels, so the results are identical.
+constexpr int kSeqSame = 4;   // same-line neighbours of a row, at most (wrap rows)
+constexpr int kSeqLater = 8;  // later-line upper neighbours of a row, at most (periodic x)
+__host__ __device__ constexpr int seq13_smem_doubles_per_row() { return 5 + 2 * kSeqSame + kSeqLater; }
+
 __device__ void apply_seq13(const PcgArgs &P, double m_r, double (&acc)[3], double *sm) {
   constexpr int S = 13;
   const SpOp &A = P.A;
   const int n = A.n, nx = A.nx, ny = A.ny;
   const bool icc = P.prec == kPrecICC;
-  double *part = sm, *c1 = sm + ny, *c2 = sm + 2 * ny, *dv = sm + 3 * ny;
-  double *q = sm + 4 * ny;    // backward: four later-line products per row, [4][ny]
-  double *fit = sm + 8 * ny;  // backward: 1 when the row takes the fixed pattern
-  auto interior = [&](int j) { return j >= 2 && j < ny - 2; };
+  double *part = sm;                  // earlier-line sum (forward) / y or y D^-1 (backward)
+  double *dv = sm + ny;               // dinv
+  double *ln = sm + 2 * ny;           // the current line's y (forward) or z (backward)
+  double *ns = sm + 3 * ny;           // number of same-line neighbours (then of later-line products)
+  double *sc = sm + 4 * ny;           // [kSeqSame][ny] same-line coefficients, ascending column
+  int *so = (int *)(sm + (4 + kSeqSame) * ny);  // [kSeqSame][ny] their columns j'
+  double *q = sm + (4 + 2 * kSeqSame) * ny;     // [kSeqLater][ny] backward: later-line products, ascending column
+  double *rr = sm + (4 + 2 * kSeqSame + kSeqLater) * ny;  // backward: r of the line
   // ---- forward: y_r = (r_r - m - sum_{lower, ascending} L y) (* dinv for ICC)
   for (int i = 0; i < nx; ++i) {
     const long long base = (long long)i * ny;
@@ -646,37 +654,39 @@ __device__ void apply_seq13(const PcgArgs &P, double m_r, double (&acc)[3], doub
       int p = 0;
       for (; p < cnt && cols[p] < base; ++p) sum -= P.l[(size_t)slots[p] * n + r] * P.y[cols[p]];
       part[j] = sum;
-      double l1 = 0.0, l2 = 0.0;
-      for (; p < cnt; ++p) {
-        if (cols[p] == r - 1) l1 = P.l[(size_t)slots[p] * n + r];
-        if (cols[p] == r - 2) l2 = P.l[(size_t)slots[p] * n + r];
+      int k = 0;
+      for (; p < cnt && k < kSeqSame; ++p, ++k) {
+        sc[(size_t)k * ny + j] = P.l[(size_t)slots[p] * n + r];
+        so[(size_t)k * ny + j] = (int)(cols[p] - base);
       }
-      c1[j] = l1;
-      c2[j] = l2;
+      ns[j] = (double)k;
       dv[j] = P.dinv[r];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       auto general = [&](int j) -> double {
-        const long long r = base + j;
-        int slots[S];
-        long long cols[S];
-        const int cnt = lower_slots<S>(A, i, j, slots, cols);
         double sum = part[j];
-        for (int p = 0; p < cnt; ++p)
-          if (cols[p] >= base) sum -= P.l[(size_t)slots[p] * n + r] * P.y[cols[p]];
+        const int k = (int)ns[j];
+        for (int t = 0; t < k; ++t) sum -= sc[(size_t)t * ny + j] * ln[so[(size_t)t * ny + j]];
         const double yv = icc ? sum * dv[j] : sum;
-        P.y[r] = yv;
+        ln[j] = yv;
+        P.y[base + j] = yv;
         return yv;
       };
       double ym2 = general(0);  // y(i, j-2)
       double ym1 = general(1);  // y(i, j-1)
 #pragma unroll 4
       for (int j = 2; j < ny - 2; ++j) {
+        // same-line neighbours (i, j-2), (i, j-1) in that order; an absent one has coefficient 0 here and
+        // is skipped by apply_levels: subtracting 0 * y leaves the sum unchanged
+        const int kk = (int)ns[j];
+        const double l2 = kk == 2 ? sc[j] : ((kk == 1 && so[j] == j - 2) ? sc[j] : 0.0);
+        const double l1 = kk == 2 ? sc[(size_t)ny + j] : ((kk == 1 && so[j] == j - 1) ? sc[j] : 0.0);
         double sum = part[j];
-        sum -= c2[j] * ym2;
-        sum -= c1[j] * ym1;
+        sum -= l2 * ym2;
+        sum -= l1 * ym1;
         const double yv = icc ? sum * dv[j] : sum;
+        ln[j] = yv;
         P.y[base + j] = yv;
         ym2 = ym1;
         ym1 = yv;
@@ -691,93 +701,57 @@ __device__ void apply_seq13(const PcgArgs &P, double m_r, double (&acc)[3], doub
     const long long base = (long long)i * ny;
     for (int j = threadIdx.x; j < ny; j += blockDim.x) {
       const long long r = base + j;
-      double e1 = 0.0, e2 = 0.0, qv[4] = {0.0, 0.0, 0.0, 0.0};
-      int nq = 0;
-      bool fits = interior(j);
-      if (fits) {
-        int slots[S];
-        long long cols[S];
-        int cnt = 0;
-        for (int s = 0; s < S; ++s) {
-          const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
-          if (c <= r) continue;
-          const double lcr = P.l[(size_t)(S - 1 - s) * n + c];
-          if (lcr == 0.0) continue;
-          int p = cnt++;
-          while (p > 0 && cols[p - 1] > c) {
-            cols[p] = cols[p - 1];
-            slots[p] = slots[p - 1];
-            --p;
-          }
-          cols[p] = c;
-          slots[p] = s;
+      int slots[S];
+      long long cols[S];
+      int cnt = 0;
+      for (int s = 0; s < S; ++s) {
+        const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+        if (c <= r) continue;
+        if (P.l[(size_t)(S - 1 - s) * n + c] == 0.0) continue;
+        int p = cnt++;
+        while (p > 0 && cols[p - 1] > c) {
+          cols[p] = cols[p - 1];
+          slots[p] = slots[p - 1];
+          --p;
         }
-        // same-line entries (r+1, r+2) first in ascending order, then the later-line products
-        int p = 0;
-        for (; p < cnt && cols[p] < base + ny; ++p) {
-          const double lcr = P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]];
-          if (cols[p] == r + 1) e1 = lcr;
-          else if (cols[p] == r + 2) e2 = lcr;
-          else fits = false;
-        }
-        for (; p < cnt; ++p) {
-          if (nq == 4) {
-            fits = false;
-            break;
-          }
-          qv[nq++] = P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
-        }
+        cols[p] = c;
+        slots[p] = s;
       }
+      int p = 0, k = 0;
+      for (; p < cnt && cols[p] < base + ny && k < kSeqSame; ++p, ++k) {
+        sc[(size_t)k * ny + j] = P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]];
+        so[(size_t)k * ny + j] = (int)(cols[p] - base);
+      }
+      int t = 0;
+      for (; p < cnt && t < kSeqLater; ++p, ++t)
+        q[(size_t)t * ny + j] = P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
+      ns[j] = (double)(k + 16 * t);  // same-line count + 16 x later-line count
       part[j] = icc ? P.y[r] : P.y[r] * P.dinv[r];
-      c1[j] = e1;
-      c2[j] = e2;
       dv[j] = P.dinv[r];
-      fit[j] = fits ? 1.0 : 0.0;
-      for (int k = 0; k < 4; ++k) q[(size_t)k * ny + j] = qv[k];
+      rr[j] = P.r[r];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      auto general = [&](int j) -> double {
-        const long long r = base + j;
-        int slots[S];
-        long long cols[S];
-        int cnt = 0;
-        for (int s = 0; s < S; ++s) {
-          const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
-          if (c <= r) continue;
-          const double lcr = P.l[(size_t)(S - 1 - s) * n + c];
-          if (lcr == 0.0) continue;
-          int p = cnt++;
-          while (p > 0 && cols[p - 1] > c) {
-            cols[p] = cols[p - 1];
-            slots[p] = slots[p - 1];
-            --p;
-          }
-          cols[p] = c;
-          slots[p] = s;
-        }
-        double sum = part[j];
-        for (int p = 0; p < cnt; ++p) sum -= P.l[(size_t)(S - 1 - slots[p]) * n + cols[p]] * P.z[cols[p]];
-        return icc ? sum * P.dinv[r] : sum;
-      };
       double zp1 = 0.0, zp2 = 0.0;  // z(i, j+1), z(i, j+2)
       for (int j = ny - 1; j >= 0; --j) {
-        double zv;
-        if (fit[j] != 0.0) {
-          double sum = part[j];
-          sum -= c1[j] * zp1;
-          sum -= c2[j] * zp2;
-          sum -= q[j];
-          sum -= q[(size_t)ny + j];
-          sum -= q[2 * (size_t)ny + j];
-          sum -= q[3 * (size_t)ny + j];
-          zv = icc ? sum * dv[j] : sum;
+        const int code = (int)ns[j];
+        const int k = code & 15, t = code >> 4;
+        double sum = part[j];
+        if (j >= 2 && j < ny - 2) {
+          // same-line neighbours (i, j+1), (i, j+2) in that order (coefficient 0 when absent)
+          const double e1 = (k >= 1 && so[j] == j + 1) ? sc[j] : 0.0;
+          const double e2 = (k == 2) ? sc[(size_t)ny + j] : ((k == 1 && so[j] == j + 2) ? sc[j] : 0.0);
+          sum -= e1 * zp1;
+          sum -= e2 * zp2;
         } else {
-          zv = general(j);
+          for (int u = 0; u < k; ++u) sum -= sc[(size_t)u * ny + j] * ln[so[(size_t)u * ny + j]];
         }
+        for (int u = 0; u < t; ++u) sum -= q[(size_t)u * ny + j];
+        const double zv = icc ? sum * dv[j] : sum;
+        ln[j] = zv;
         const long long r = base + j;
         P.z[r] = zv;
-        const double rv = P.r[r] - m_r;
+        const double rv = rr[j] - m_r;
         acc[0] += zv;
         acc[1] += rv * zv;
         acc[2] += rv;
