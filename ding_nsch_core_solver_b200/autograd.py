@@ -1,5 +1,5 @@
-"""torch.autograd.Functions over the differentiable pieces of the C-ABI: the pressure projection and the
-CH advective term.
+"""torch.autograd.Functions over the differentiable pieces of the C-ABI: the pressure projection, the CH
+advective term and the CH implicit solve.
 
 `projection(solver, step, u_star, v_star, p, p_prev)` runs the pressure projection of one step --
 pressure solve plus velocity correction (dn_projection) -- on interior-shaped float64 CUDA tensors and
@@ -10,6 +10,10 @@ the forward call is kept and put back before the backward runs.  The reference h
 `advection(solver, c, u, v)` returns the CH advective term -div(u c) with WENO5 face values (dn_advection);
 its backward (dn_advection_adjoint) differentiates the WENO5 nonlinear weights.  The upwind side follows the
 sign of each face velocity, so the term is not differentiable where a face velocity is exactly 0.
+
+`ch_solve(solver, alpha0, rhs)` is the CH implicit solve (dn_ch_linear_solve); its operator is symmetric, so
+its backward is the same solve.  `explicit_operator(solver, c, u, v)` is the CH explicit operator, and
+`ch_phase` composes the two into the CH phase of a step.
 
 Shapes (interior values only): u, u_star (nx+1, ny); v, v_star (nx, ny+1); c, p, p_prev, p_new, the
 advective term (nx, ny).
@@ -114,3 +118,78 @@ def advection(solver, c, u, v):
     """-div(u c) with WENO5 face values; differentiable in c, u and v."""
     return Advection.apply(solver, c, u, v)
 
+
+
+class CHSolve(torch.autograd.Function):
+    """c = A^-1 rhs for the CH implicit operator A = alpha0 I - beta1 L + beta2 L^2 (dn_ch_linear_solve, the
+    ch_solver backend: ILDLT-preconditioned CG from a zero start).  A is symmetric, so the backward is the same
+    solve applied to the cotangent."""
+
+    @staticmethod
+    def forward(ctx, solver, alpha0, rhs):
+        ctx.solver, ctx.alpha0 = solver, float(alpha0)
+        return _ch_solve(solver, float(alpha0), rhs)
+
+    @staticmethod
+    def backward(ctx, g):
+        return None, None, _ch_solve(ctx.solver, ctx.alpha0, g)
+
+
+def _ch_solve(solver, alpha0, t):
+    import numpy as np
+
+    g = solver.ghost
+    full = np.zeros((solver.nx + 2 * g, solver.ny + 2 * g))
+    full[g:g + solver.nx, g:g + solver.ny] = t.detach().to(torch.float64).cpu().numpy()
+    cs = solver.ch_linear_solve(full, alpha0, np.zeros_like(full))[0]
+    return torch.from_numpy(np.ascontiguousarray(cs[g:g + solver.nx, g:g + solver.ny])).to(t.device)
+
+
+def ch_solve(solver, alpha0, rhs):
+    """The CH implicit solve on an interior-shaped (nx, ny) right-hand side; differentiable in rhs."""
+    return CHSolve.apply(solver, alpha0, rhs)
+
+
+class ExplicitOperator(torch.autograd.Function):
+    """E(c, u, v), the CH explicit operator of the phase step (dn_explicit_operator); backward
+    dn_explicit_operator_adjoint."""
+
+    @staticmethod
+    def forward(ctx, solver, c, u, v):
+        ins = [_full(solver, c, "c"), _full(solver, u, "u"), _full(solver, v, "v")]
+        out = torch.empty_like(ins[0])
+        torch.cuda.current_stream().synchronize()
+        solver._check(solver._lib.dn_explicit_operator(solver._h, *[t.data_ptr() for t in ins], out.data_ptr()))
+        ctx.solver = solver
+        ctx.save_for_backward(*ins)
+        return _interior(solver, out)
+
+    @staticmethod
+    def backward(ctx, g):
+        solver = ctx.solver
+        cf, uf, vf = ctx.saved_tensors
+        gf = _full(solver, g.to(torch.float64).contiguous(), "c")
+        outs = [torch.empty_like(cf), torch.empty_like(uf), torch.empty_like(vf)]
+        torch.cuda.current_stream().synchronize()
+        solver._check(solver._lib.dn_explicit_operator_adjoint(solver._h, cf.data_ptr(), uf.data_ptr(),
+                                                               vf.data_ptr(), gf.data_ptr(),
+                                                               *[t.data_ptr() for t in outs]))
+        return (None,) + tuple(_interior(solver, b) for b in outs)
+
+
+def explicit_operator(solver, c, u, v):
+    """The CH explicit operator E(c, u, v); differentiable in c, u and v."""
+    return ExplicitOperator.apply(solver, c, u, v)
+
+
+def ch_phase(solver, step, c, u, v, c_prev2=None, e_prev=None):
+    """c at the end of the CH phase of step `step` (advance_phase_state, phase_field.cpp:258-281, with
+    c_prev = c as the step's history copy leaves it): A^-1 (c / dt + E) on step 0 and
+    A^-1 ((4 c - c_prev2) / (2 dt) + 2 E - E_prev) after, A = alpha0 I - beta1 L + beta2 L^2 with alpha0 = 1/dt
+    or 3/(2 dt).  Composed from explicit_operator and ch_solve, so its gradient in c, u, v, c_prev2 and
+    E_prev is the discrete adjoint of the phase."""
+    dt = solver.config.dt
+    e = explicit_operator(solver, c, u, v)
+    if step == 0:
+        return ch_solve(solver, 1.0 / dt, c / dt + e)
+    return ch_solve(solver, 3.0 / (2.0 * dt), (4.0 * c - c_prev2) / (2.0 * dt) + 2.0 * e - e_prev)

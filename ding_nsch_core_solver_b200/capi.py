@@ -116,6 +116,8 @@ def load():
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_advection": (I, [H, VP, VP, VP, VP]),
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
+        "dn_explicit_operator": (I, [H, VP, VP, VP, VP]),
+        "dn_explicit_operator_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_diagnostics": (I, [H, C.POINTER(Diag)]),
         "dn_compute_mass": (I, [H, I, DP]),
         "dn_synchronize": (I, [H]),

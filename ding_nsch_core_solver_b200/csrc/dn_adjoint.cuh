@@ -310,7 +310,91 @@ __global__ void k_adv_adj_c(Fv ce, Fv u, Fv vv, Fv rb, Fv cbar, Grid G, BCSet bc
   for (int k = 0; k < kx; ++k) acc += adv_adj_gather<true>(ce, u, rb, G, bc, i, j, e[k]);
   const int ky = scalar_bc_images(j, G.ny, G.py, e);
   for (int k = 0; k < ky; ++k) acc += adv_adj_gather<false>(ce, vv, rb, G, bc, i, j, e[k]);
-  cbar.at(i, j) = acc;
+  cbar.at(i, j) += acc;  // accumulates: the caller clears cbar first
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Adjoint of the CH explicit operator (build_phase_explicit_operator, phase_field.cpp:354-396)
+//   E = div(M grad mu) / pe - (a1 L c - a2 L L c) / pe + adv(c, u, v),
+//   M = max(0, c (1 - c)) on faces by xface, mu = 6 sqrt2 (W'(c) / cn - cn L c), W' = c (1 - c) (1 - 2c) / 2,
+// with L the scalar-BC Laplacian (symmetric, so it is its own transpose) and the velocity face BCs written
+// onto the diffusive fluxes.  The advective part is k_adv_adj_*.
+// ------------------------------------------------------------------------------------------------------
+
+// Cotangent of the diffusive flux at x-face f before its face BC: the flux enters ddiv(f-1) as +F/dx and
+// ddiv(f) as -F/dx, scaled by 1/pe; the fold is that of the velocity face BC (k_adj_fold_u).
+__device__ __forceinline__ double diff_flux_bar_x(const Fv &g, const Grid &G, const BCSet &bc, int f, int j,
+                                                  double inv_pe) {
+  auto raw = [&](int q) {
+    const double w = q > 0 ? g.at(q - 1, j) : 0.0;
+    const double e = q < G.nx ? g.at(q, j) : 0.0;
+    return (w - e) * inv_pe / G.dx;
+  };
+  const int last = G.nx;
+  if (G.px) return f == last ? 0.0 : (f == 0 ? raw(0) + raw(last) : raw(f));
+  if (f == 0 || f == last) return 0.0;
+  double v = raw(f);
+  if (f == 1 && bc.u[DN_LEFT].type != DN_BC_DIRICHLET) v += raw(0);
+  if (f == last - 1 && bc.u[DN_RIGHT].type != DN_BC_DIRICHLET) v += raw(last);
+  return v;
+}
+__device__ __forceinline__ double diff_flux_bar_y(const Fv &g, const Grid &G, const BCSet &bc, int i, int f,
+                                                  double inv_pe) {
+  auto raw = [&](int q) {
+    const double s = q > 0 ? g.at(i, q - 1) : 0.0;
+    const double nn = q < G.ny ? g.at(i, q) : 0.0;
+    return (s - nn) * inv_pe / G.dy;
+  };
+  const int last = G.ny;
+  if (G.py) return f == last ? 0.0 : (f == 0 ? raw(0) + raw(last) : raw(f));
+  if (f == 0 || f == last) return 0.0;
+  double v = raw(f);
+  if (f == 1 && bc.v[DN_BOTTOM].type != DN_BC_DIRICHLET) v += raw(0);
+  if (f == last - 1 && bc.v[DN_TOP].type != DN_BC_DIRICHLET) v += raw(last);
+  return v;
+}
+
+// Per x-face: with F = M_face * dmu/dx, the cotangents M_bar = F_bar dmu/dx (into mb) and
+// G_bar = F_bar M_face (into gb).
+__global__ void k_eadj_face_x(Fv g, Fv mob, Fv mu, Fv mb, Fv gb, Grid G, BCSet bc, double inv_pe) {
+  DN_FOR_INTERIOR(mb);
+  const double p = diff_flux_bar_x(g, G, bc, i, j, inv_pe);
+  mb.at(i, j) = p * gfx(mu, G, i, j);
+  gb.at(i, j) = p * xface(mob, G, i, j);
+}
+__global__ void k_eadj_face_y(Fv g, Fv mob, Fv mu, Fv mb, Fv gb, Grid G, BCSet bc, double inv_pe) {
+  DN_FOR_INTERIOR(mb);
+  const double p = diff_flux_bar_y(g, G, bc, i, j, inv_pe);
+  mb.at(i, j) = p * gfy(mu, G, i, j);
+  gb.at(i, j) = p * yface(mob, G, i, j);
+}
+
+// Per cell: the mobility cotangent (each face average puts half on either cell; the periodic face 0 pairs
+// cells nx-1 and 0) and the chemical-potential cotangent mu_bar (into mub); c_bar (into cbar) gets the local
+// parts mob_bar M'(c) + 6 sqrt2 W''(c) / cn mu_bar.
+__global__ void k_eadj_cells(Fv c, Fv mbx, Fv gbx, Fv mby, Fv gby, Fv mub, Fv cbar, Grid G, double cn) {
+  DN_FOR_INTERIOR(cbar);
+  const int fe = (G.px && i == G.nx - 1) ? 0 : i + 1;
+  const int fn = (G.py && j == G.ny - 1) ? 0 : j + 1;
+  const double mobb = 0.5 * (mbx.at(i, j) + mbx.at(fe, j)) + 0.5 * (mby.at(i, j) + mby.at(i, fn));
+  const double mu_b = (gbx.at(i, j) - gbx.at(fe, j)) / G.dx + (gby.at(i, j) - gby.at(i, fn)) / G.dy;
+  const double cc = c.at(i, j);
+  const double dmob = cc * (1.0 - cc) > 0.0 ? 1.0 - 2.0 * cc : 0.0;
+  const double alpha = 6.0 * 1.4142135623730950488;
+  const double ddw = 0.5 * (1.0 - 6.0 * cc + 6.0 * cc * cc);
+  mub.at(i, j) = mu_b;
+  cbar.at(i, j) = mobb * dmob + alpha * ddw / cn * mu_b;
+}
+
+// out += s * L in  (in carries its scalar-BC ghosts)
+__global__ void k_add_scaled_lap(Fv in, Fv out, Grid G, double s) {
+  DN_FOR_INTERIOR(out);
+  out.at(i, j) += s * lapc(in, G, i, j);
+}
+// out = s0 in + s1 L in
+__global__ void k_lin_lap(Fv in, Fv out, Grid G, double s0, double s1) {
+  DN_FOR_INTERIOR(out);
+  out.at(i, j) = s0 * in.at(i, j) + s1 * lapc(in, G, i, j);
 }
 
 }  // namespace dn

@@ -1878,6 +1878,66 @@ dn_status dn_advection_adjoint(dn_handle *h, const double *c, const double *u, c
   return DN_OK;
 }
 
+// The CH explicit operator E(c, u, v) on caller device buffers (cell c, faces u, v in; cell E out, ghosts
+// filled), computed as the phase step computes it.
+dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, const double *v, double *E) {
+  if (!h || !c || !u || !v || !E) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  const Fv &CF = f[DN_F_C], &UF = f[DN_F_U], &VF = f[DN_F_V];
+  const Fv U{const_cast<double *>(u), UF.nx, UF.ny, UF.g}, V{const_cast<double *>(v), VF.nx, VF.ny, VF.g};
+  DN_CUDA(h, cudaMemcpyAsync(h->cmid.d, c, CF.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  DN_TRY(phase_explicit(h, h->cmid, U, V));
+  DN_CUDA(h, cudaMemcpyAsync(E, h->E_new.d, CF.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+// Vector-Jacobian product of dn_explicit_operator at (c, u, v): cotangent gE of the interior of E in;
+// cotangents of the interior values of c, u, v out (ghosts 0).
+dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
+                                       const double *gE, double *c_bar, double *u_bar, double *v_bar) {
+  if (!h || !c || !u || !v || !gE || !c_bar || !u_bar || !v_bar) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  const dn_config &cfg = h->cfg;
+  const Fv &CF = f[DN_F_C], &UF = f[DN_F_U], &VF = f[DN_F_V];
+  const Fv U{const_cast<double *>(u), UF.nx, UF.ny, UF.g}, V{const_cast<double *>(v), VF.nx, VF.ny, VF.g};
+  const Fv RB{const_cast<double *>(gE), CF.nx, CF.ny, CF.g};
+  const Fv CB{c_bar, CF.nx, CF.ny, CF.g}, UB{u_bar, UF.nx, UF.ny, UF.g}, VB{v_bar, VF.nx, VF.ny, VF.g};
+  DN_CUDA(h, cudaMemsetAsync(c_bar, 0, CF.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(u_bar, 0, UF.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(v_bar, 0, VF.size() * sizeof(double), h->stream));
+  // forward intermediates: c with its ghosts, mobility, chemical potential
+  DN_CUDA(h, cudaMemcpyAsync(h->cmid.d, c, CF.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  LAUNCH_INTERIOR(k_mob_lap, h->mob, h->cmid, h->mob, h->lap, h->G);
+  DN_TRY(bc(h, h->mob, kBCScalar));
+  DN_TRY(chem(h, h->cmid, h->mu_t));
+  // the cotangent with its scalar-BC ghosts (for the transposed Laplacians)
+  DN_CUDA(h, cudaMemcpyAsync(h->E_new.d, gE, CF.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->E_new, kBCScalar));
+  const double inv_pe = 1.0 / cfg.pe;
+  // diffusive part: face cotangents, then mobility and chemical potential per cell
+  LAUNCH_INTERIOR(k_eadj_face_x, h->afx, h->E_new, h->mob, h->mu_t, h->afx, h->dfx, h->G, h->bc, inv_pe);
+  LAUNCH_INTERIOR(k_eadj_face_y, h->afy, h->E_new, h->mob, h->mu_t, h->afy, h->dfy, h->G, h->bc, inv_pe);
+  LAUNCH_INTERIOR(k_eadj_cells, CB, h->cmid, h->afx, h->dfx, h->afy, h->dfy, h->ddiv, CB, h->G, cfg.cn);
+  DN_TRY(bc(h, h->ddiv, kBCScalar));
+  const double alpha = 6.0 * kSqrt2;
+  LAUNCH_INTERIOR(k_add_scaled_lap, CB, h->ddiv, CB, h->G, -alpha * cfg.cn);
+  // -(a1 L c - a2 L L c) / pe: L^T (-(a1/pe) g + (a2/pe) L^T g)
+  const double a1 = cfg.cn > 0.0 ? (3.0 * kSqrt2 / (16.0 * cfg.cn)) : 0.0;
+  const double a2 = cfg.cn > 0.0 ? (3.0 * kSqrt2 * cfg.cn / 4.0) : 0.0;
+  LAUNCH_INTERIOR(k_lin_lap, h->arhs, h->E_new, h->arhs, h->G, -a1 * inv_pe, a2 * inv_pe);
+  DN_TRY(bc(h, h->arhs, kBCScalar));
+  LAUNCH_INTERIOR(k_add_scaled_lap, CB, h->arhs, CB, h->G, 1.0);
+  // advective part
+  LAUNCH_INTERIOR(k_adv_adj_u, UB, h->cmid, U, RB, UB, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adv_adj_v, VB, h->cmid, V, RB, VB, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adv_adj_c, CB, h->cmid, U, V, RB, CB, h->G, h->bc);
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
 dn_status dn_compute_mass(dn_handle *h, int field, double *mass) {
   if (!h || !mass || field < 0 || field >= DN_F_COUNT) return DN_ERR_INVALID_ARGUMENT;
   const int nb = 128;

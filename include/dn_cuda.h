@@ -218,6 +218,18 @@ dn_status dn_advection(dn_handle *h, const double *c, const double *u, const dou
 dn_status dn_advection_adjoint(dn_handle *h, const double *c, const double *u, const double *v, const double *g_rhs,
                                double *c_bar, double *u_bar, double *v_bar);
 
+/* The CH explicit operator E(c, u, v) of the phase step (build_phase_explicit_operator,
+ * phase_field.cpp:354-396: diffusion of the chemical potential with the c(1-c) mobility, the linear
+ * Laplacian terms and the WENO5 advective term) on caller DEVICE buffers: c (cell field), u, v (face fields)
+ * in, E (cell field, ghosts filled) out.  Uses the handle's work fields. */
+dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, const double *v, double *E);
+/* No counterpart in the reference.  Vector-Jacobian product of dn_explicit_operator at (c, u, v): cotangent
+ * gE of the interior of E in; cotangents c_bar, u_bar, v_bar of the interior values of c, u, v out (ghosts
+ * 0).  The mobility max(0, c(1-c)) and the upwind choice of the advective term are piecewise smooth; the
+ * derivative is taken on the side the forward evaluation lies on.  DEVICE buffers. */
+dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
+                                       const double *gE, double *c_bar, double *u_bar, double *v_bar);
+
 /* ---- diagnostics ------------------------------------------------------------------------------------ */
 /* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
 dn_status dn_diagnostics(dn_handle *h, dn_diag *out);

@@ -2033,6 +2033,19 @@ int orc_advection(orc_solver *s, const double *c, const double *u, const double 
   GUARD_END
 }
 
+int orc_explicit_operator(orc_solver *s, const double *c, const double *u, const double *v, double *E) {
+  GUARD_BEGIN
+  const int nx = s->cfg.nx, ny = s->cfg.ny, g = s->cfg.ghost;
+  const fld uf = {nx + 1, ny, g, (double *)u}, vf = {nx, ny + 1, g, (double *)v};
+  fld cw, out = {nx, ny, g, E};
+  fld_init(&cw, nx, ny, g, 0.0);
+  memcpy(cw.d, c, fld_size(&cw) * sizeof(double));
+  bc_scalar(s, &cw);
+  phase_explicit(s, &cw, &uf, &vf, &out);
+  fld_free(&cw);
+  GUARD_END
+}
+
 int orc_finish_step(orc_solver *s) {
   GUARD_BEGIN
   refresh_mu(s);

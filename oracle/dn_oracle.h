@@ -105,6 +105,9 @@ int orc_ch_linear_solve(orc_solver *s, const double *rhs_field, double alpha0, d
 /* The CH advective term -div(u c) with WENO5 face values (build_phase_advection_fluxes,
  * phase_field.cpp:283-311) of Field2D arrays c (cell), u, v (faces) into rhs (cell, interior + ghosts). */
 int orc_advection(orc_solver *s, const double *c, const double *u, const double *v, double *rhs);
+/* The CH explicit operator E (build_phase_explicit_operator, phase_field.cpp:354-396) of Field2D arrays c
+ * (cell; its ghosts are refilled by the scalar BC), u, v (faces) into E (cell, interior + ghosts). */
+int orc_explicit_operator(orc_solver *s, const double *c, const double *u, const double *v, double *E);
 void orc_get_report(const orc_solver *s, orc_report *r);
 void orc_diagnostics(orc_solver *s, orc_diag *d); /* diagnostics.cpp:114-167 */
 double orc_compute_mass(orc_solver *s, int field_id);

@@ -209,6 +209,7 @@ def _load(impl: str):
         sig["time_steps"] = (C.c_double, [vp, C.c_int, C.c_int])
     else:
         sig["advection"] = (C.c_int, [vp, dp, dp, dp, dp])
+        sig["explicit_operator"] = (C.c_int, [vp, dp, dp, dp, dp])
     fns = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, pre + name)
@@ -310,6 +311,14 @@ class OracleSolver:
         c, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (c, u, v))
         out = np.zeros_like(self.field("c"))
         self._check(self._f["advection"](self._h, *(a.ctypes.data_as(dp) for a in (c, u, v, out))))
+        return out
+
+    def explicit_operator(self, c: np.ndarray, u: np.ndarray, v: np.ndarray) -> np.ndarray:
+        """The CH explicit operator E(c, u, v) (port only); Field2D arrays in, the cell array out."""
+        dp = C.POINTER(C.c_double)
+        c, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (c, u, v))
+        out = np.zeros_like(self.field("c"))
+        self._check(self._f["explicit_operator"](self._h, *(a.ctypes.data_as(dp) for a in (c, u, v, out))))
         return out
 
     def report(self) -> dict:

@@ -185,3 +185,93 @@ def test_autograd_gradcheck_smallest_grid():
         assert torch.autograd.gradcheck(lambda *a: projection(s, 1, *a), x, eps=1e-6, atol=1e-6, rtol=1e-5)
     finally:
         s.close()
+
+
+# ------------------------------------------------------------------------------------- CH implicit solve
+CH_CASES = {
+    "ch_periodic": _cfg(nx=10, ny=12, ch_tolerance=1e-13, ch_inner_iterations=500),
+    "ch_walls": _cfg(nx=12, ny=10, periodic_x=False, periodic_y=False, ch_tolerance=1e-13, ch_inner_iterations=500),
+    "ch_channel_x": _cfg(nx=12, ny=10, periodic_x=True, periodic_y=False, ch_tolerance=1e-13,
+                         ch_inner_iterations=500),
+}
+
+
+def _oracle_ch_jacobian(cfg, alpha0):
+    """Columns A^-1 e_k from the oracle's CH solve (zero start, tolerance 1e-13)."""
+    from oracle.oracle import OracleSolver
+
+    o = OracleSolver(cfg, "port")
+    o.initialize()
+    g = cfg["ghost"]
+    nx, ny = cfg["nx"], cfg["ny"]
+    cols = []
+    try:
+        for k in range(nx * ny):
+            full = np.zeros((nx + 2 * g, ny + 2 * g))
+            full[g + k // ny, g + k % ny] = 1.0
+            c = o.ch_linear_solve(full, alpha0, np.zeros_like(full))[0]
+            cols.append(c[g:g + nx, g:g + ny].ravel())
+    finally:
+        o.close()
+    return np.stack(cols, axis=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CH_CASES))
+def test_ch_solve_adjoint_matches_reference_transpose(name):
+    """The backward of the CH implicit solve (the same solve on the cotangent) against J^T from the oracle."""
+    import torch
+
+    from ding_nsch_core_solver_b200 import capi
+    from ding_nsch_core_solver_b200.autograd import ch_solve
+
+    cfg = CH_CASES[name]
+    alpha0 = 1.5 / cfg["dt"]
+    J = _oracle_ch_jacobian(cfg, alpha0)
+    s = capi.Solver(cfg)
+    try:
+        rng = np.random.default_rng(43)
+        rhs = torch.from_numpy(rng.standard_normal((cfg["nx"], cfg["ny"]))).cuda().requires_grad_()
+        w = rng.standard_normal((cfg["nx"], cfg["ny"]))
+        out = ch_solve(s, alpha0, rhs)
+        assert _rel(out.detach().cpu().numpy().ravel(), J @ rhs.detach().cpu().numpy().ravel()) < TOL_REF
+        out.backward(torch.from_numpy(w).cuda())
+        assert _rel(rhs.grad.cpu().numpy().ravel(), J.T @ w.ravel()) < TOL_REF, name
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_ch_solve_gradient_central_fd():
+    import torch
+
+    from ding_nsch_core_solver_b200 import capi
+    from ding_nsch_core_solver_b200.autograd import ch_solve
+
+    cfg = CH_CASES["ch_walls"]
+    alpha0 = 1.0 / cfg["dt"]
+    s = capi.Solver(cfg)
+    try:
+        rng = np.random.default_rng(47)
+        x = torch.from_numpy(rng.standard_normal((cfg["nx"], cfg["ny"]))).cuda().requires_grad_()
+        w = torch.from_numpy(rng.standard_normal((cfg["nx"], cfg["ny"]))).cuda()
+        (ch_solve(s, alpha0, x) * w).sum().backward()
+        eps = 1e-6
+        for k in range(16):
+            d = torch.from_numpy(np.random.default_rng(300 + k).standard_normal((cfg["nx"], cfg["ny"]))).cuda()
+            with torch.no_grad():
+                lp = (ch_solve(s, alpha0, x + eps * d) * w).sum().item()
+                lm = (ch_solve(s, alpha0, x - eps * d) * w).sum().item()
+            fd = (lp - lm) / (2 * eps)
+            an = (x.grad * d).sum().item()
+            assert abs(fd - an) <= TOL_FD * abs(an), (k, fd, an)
+    finally:
+        s.close()
+
+
+def test_ch_operator_inverse_is_symmetric():
+    """The premise of using the CH solve as its own adjoint: the oracle's A^-1 (assembled column by column)
+    is symmetric to round-off for periodic, wall and channel boundaries."""
+    for name, cfg in CH_CASES.items():
+        J = _oracle_ch_jacobian(cfg, 1.5 / cfg["dt"])
+        assert np.linalg.norm(J - J.T) <= 1e-12 * np.linalg.norm(J), name

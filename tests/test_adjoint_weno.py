@@ -1,5 +1,6 @@
-"""Adjoint of the CH advective term with WENO5 face values (dn_advection_adjoint, the backward of
-ding_nsch_core_solver_b200.autograd.Advection), nonlinear weights included.
+"""Adjoints of the CH phase: the advective term with WENO5 face values (dn_advection_adjoint), nonlinear
+weights included; the whole explicit operator E (dn_explicit_operator_adjoint); and the phase composed from E
+and the implicit solve (autograd.ch_phase).
 
 - dn_advection against the oracle's build_phase_advection_fluxes restatement on the same inputs;
 - the adjoint against the reference FP64 adjoint J^T, J assembled by central differences of the oracle's
@@ -197,3 +198,123 @@ def test_oracle_advection_properties():
         assert _rel(r, -0.7 * div) <= 1e-13
     finally:
         orc.close()
+
+
+# ------------------------------------------------------------------ explicit operator E and the CH phase
+def _ch_cfg(cfg):
+    return dict(cfg, ch_tolerance=1e-13, ch_inner_iterations=500)
+
+
+def _point_e(cfg, seed):
+    """c around 0.5 (mostly inside the mobility's (0, 1) branch), face velocities away from 0."""
+    x = _point(cfg, seed)
+    x[0] = 0.5 + 0.3 * x[0]
+    return x
+
+
+def _oracle_e(orc, cfg, c, u, v):
+    g = cfg["ghost"]
+    out = orc.explicit_operator(_full(cfg, c), _full(cfg, u), _full(cfg, v))
+    return out[g:out.shape[0] - g, g:out.shape[1] - g]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_explicit_operator_forward_and_adjoint(name):
+    from ding_nsch_core_solver_b200 import capi
+    from ding_nsch_core_solver_b200.autograd import explicit_operator
+
+    cfg = CASES[name]
+    x = _point_e(cfg, 7)
+    orc, s = _oracle(cfg), capi.Solver(cfg)
+    try:
+        xt = [t.requires_grad_() for t in _cuda(x)]
+        out = explicit_operator(s, *xt)
+        assert _rel(out.detach().cpu().numpy(), _oracle_e(orc, cfg, *x)) <= TOL_FWD, name
+        h = 1e-6
+        cols = []
+        for k in range(3):
+            for idx in range(x[k].size):
+                xp = [a.copy() for a in x]
+                xm = [a.copy() for a in x]
+                xp[k].flat[idx] += h
+                xm[k].flat[idx] -= h
+                cols.append(((_oracle_e(orc, cfg, *xp) - _oracle_e(orc, cfg, *xm)) / (2 * h)).ravel())
+        J = np.stack(cols, axis=1)
+        w = np.random.default_rng(11).standard_normal(_shapes(cfg)[0])
+        out.backward(_cuda([w])[0])
+        got = np.concatenate([t.grad.cpu().numpy().ravel() for t in xt])
+        ref = J.T @ w.ravel()
+        n0 = x[0].size
+        assert _rel(got[:n0], ref[:n0]) <= TOL_REF and _rel(got[n0:], ref[n0:]) <= TOL_REF, (name, _rel(got, ref))
+    finally:
+        s.close()
+        orc.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("step", [0, 1])
+@pytest.mark.parametrize("name", ["walls", "channel_x", "periodic"])
+def test_ch_phase_forward_matches_oracle(name, step):
+    """The composed phase reproduces the oracle's CH phase of the same state."""
+    from ding_nsch_core_solver_b200 import capi
+    from ding_nsch_core_solver_b200.autograd import ch_phase
+
+    cfg = _ch_cfg(CASES[name])
+    g = cfg["ghost"]
+    c, u, v = _point_e(cfg, 13)
+    rng = np.random.default_rng(17)
+    c_prev2 = c + 0.01 * rng.standard_normal(c.shape)
+    e_prev = rng.standard_normal(c.shape)
+    orc, s = _oracle(cfg), capi.Solver(cfg)
+    try:
+        orc.set_field("c", _full(cfg, c))
+        orc.set_field("c_prev", _full(cfg, c_prev2))  # the step's history copy moves it to c_prev2
+        orc.set_field("u", _full(cfg, u))
+        orc.set_field("v", _full(cfg, v))
+        orc.set_field("e_prev", _full(cfg, e_prev))
+        orc.refresh_derived()  # BC ghosts of the injected state, as a step leaves them
+        orc.begin_step(step)
+        orc.phase(step)
+        ref = orc.field("c")[g:g + cfg["nx"], g:g + cfg["ny"]]
+        got = ch_phase(s, step, *_cuda([c, u, v]), *_cuda([c_prev2, e_prev])).cpu().numpy()
+        assert _rel(got, ref) <= 1e-9, (name, step, _rel(got, ref))
+    finally:
+        s.close()
+        orc.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["walls", "channel_x"])
+def test_ch_phase_gradient_central_fd(name):
+    import torch
+
+    from ding_nsch_core_solver_b200 import capi
+    from ding_nsch_core_solver_b200.autograd import ch_phase
+
+    cfg = _ch_cfg(CASES[name])
+    s = capi.Solver(cfg)
+    try:
+        c, u, v = _point_e(cfg, 19)
+        rng = np.random.default_rng(23)
+        extra = [c + 0.01 * rng.standard_normal(c.shape), rng.standard_normal(c.shape)]
+        x = [t.requires_grad_() for t in _cuda([c, u, v] + extra)]
+        w = _cuda([rng.standard_normal(c.shape)])[0]
+
+        def loss(a):
+            return (ch_phase(s, 1, *a) * w).sum()
+
+        loss(x).backward()
+        grads = [t.grad.detach() for t in x]
+        shapes = _shapes(cfg) + [c.shape, c.shape]
+        eps = 1e-6
+        for k in range(16):
+            d = _cuda([np.random.default_rng(400 + k).standard_normal(sh) for sh in shapes])
+            with torch.no_grad():
+                lp = loss([a + eps * b for a, b in zip(x, d)]).item()
+                lm = loss([a - eps * b for a, b in zip(x, d)]).item()
+            fd = (lp - lm) / (2 * eps)
+            an = sum((g_ * b).sum().item() for g_, b in zip(grads, d))
+            assert abs(fd - an) <= TOL_FD * abs(an), (name, k, fd, an)
+    finally:
+        s.close()
