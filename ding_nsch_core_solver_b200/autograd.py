@@ -13,7 +13,8 @@ sign of each face velocity, so the term is not differentiable where a face veloc
 
 `ch_solve(solver, alpha0, rhs)` is the CH implicit solve (dn_ch_linear_solve); its operator is symmetric, so
 its backward is the same solve.  `explicit_operator(solver, c, u, v)` is the CH explicit operator, and
-`ch_phase` composes the two into the CH phase of a step.
+`ch_phase` composes the two into the CH phase of a step, and `ch_rollout` chains phases over a horizon with
+optional checkpointing every K steps.
 
 Shapes (interior values only): u, u_star (nx+1, ny); v, v_star (nx, ny+1); c, p, p_prev, p_new, the
 advective term (nx, ny).
@@ -193,3 +194,36 @@ def ch_phase(solver, step, c, u, v, c_prev2=None, e_prev=None):
     if step == 0:
         return ch_solve(solver, 1.0 / dt, c / dt + e)
     return ch_solve(solver, 3.0 / (2.0 * dt), (4.0 * c - c_prev2) / (2.0 * dt) + 2.0 * e - e_prev)
+
+
+def _ch_segment(solver, first_step, count, u, v, c, c_old, e_prev):
+    """`count` CH phases from step `first_step` at fixed velocity; returns the state (c, c_old, e_prev)."""
+    dt = solver.config.dt
+    for k in range(first_step, first_step + count):
+        e = explicit_operator(solver, c, u, v)
+        if k == 0:
+            c_new = ch_solve(solver, 1.0 / dt, c / dt + e)
+        else:
+            c_new = ch_solve(solver, 3.0 / (2.0 * dt), (4.0 * c - c_old) / (2.0 * dt) + 2.0 * e - e_prev)
+        c, c_old, e_prev = c_new, c, e
+    return c, c_old, e_prev
+
+
+def ch_rollout(solver, c0, u, v, steps, checkpoint_every=0):
+    """c after `steps` CH phases from c0 (step 0 onwards) with the velocity held at (u, v): the CH part of
+    the time step (BDF1 then BDF2 with the AB2 explicit operator) rolled out over a horizon.  With
+    checkpoint_every = K > 0 the backward keeps only every K-th state and recomputes each segment of K steps
+    from it (torch.utils.checkpoint), so memory grows with steps / K + K rather than with steps."""
+    from torch.utils.checkpoint import checkpoint
+
+    state = (c0, torch.zeros_like(c0), torch.zeros_like(c0))
+    k = 0
+    while k < steps:
+        n = min(checkpoint_every, steps - k) if checkpoint_every > 0 else steps - k
+        if checkpoint_every > 0:
+            state = checkpoint(lambda a, b, c_, d, e, k0=k, m=n: _ch_segment(solver, k0, m, a, b, c_, d, e),
+                               u, v, *state, use_reentrant=False)
+        else:
+            state = _ch_segment(solver, k, n, u, v, *state)
+        k += n
+    return state[0]

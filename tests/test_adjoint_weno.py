@@ -318,3 +318,40 @@ def test_ch_phase_gradient_central_fd(name):
             assert abs(fd - an) <= TOL_FD * abs(an), (name, k, fd, an)
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_ch_rollout_checkpointed_gradient():
+    """Six CH phases at fixed velocity: the gradient of <w, c^6> in (c^0, u, v) with checkpoints every 2 steps
+    equals the gradient that keeps every step, and matches central FD on 16 directions."""
+    import torch
+
+    from ding_nsch_core_solver_b200 import capi
+    from ding_nsch_core_solver_b200.autograd import ch_rollout
+
+    cfg = _ch_cfg(CASES["channel_x"])
+    s = capi.Solver(cfg)
+    try:
+        c, u, v = _point_e(cfg, 29)
+        w = _cuda([np.random.default_rng(31).standard_normal(c.shape)])[0]
+        grads = []
+        for every in (0, 2):
+            x = [t.requires_grad_() for t in _cuda([c, u, v])]
+            (ch_rollout(s, x[0], x[1], x[2], 6, checkpoint_every=every) * w).sum().backward()
+            grads.append([t.grad.detach().clone() for t in x])
+        for a, b in zip(*grads):
+            assert torch.equal(a, b)
+        base = [t.detach() for t in _cuda([c, u, v])]
+
+        def loss(a):
+            return (ch_rollout(s, a[0], a[1], a[2], 6) * w).sum().item()
+
+        eps = 1e-6
+        for k in range(16):
+            d = _cuda([np.random.default_rng(500 + k).standard_normal(sh) for sh in _shapes(cfg)])
+            with torch.no_grad():
+                fd = (loss([a + eps * b for a, b in zip(base, d)]) - loss([a - eps * b for a, b in zip(base, d)])) / (2 * eps)
+            an = sum((g_ * b).sum().item() for g_, b in zip(grads[1], d))
+            assert abs(fd - an) <= TOL_FD * abs(an), (k, fd, an)
+    finally:
+        s.close()
