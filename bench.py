@@ -40,8 +40,9 @@ RESTART_FIELDS = ("c", "c_prev", "c_prev2", "p", "p_prev", "u", "v", "u_prev", "
                   "hv_prev")
 
 
-def workload_cfg() -> dict:
-    return dict(
+def workload_cfg(grid=None) -> dict:
+    """The rising bubble in R0 units (box 4 x 8); `grid` = (nx, ny) refines it (192 x 384 by default)."""
+    cfg = dict(
         name="rising_bubble_192x384_split_icpcg", mode="coupled", nx=192, ny=384, ghost=3, lx=4.0, ly=8.0,
         periodic_x=False, periodic_y=False, v_bc_left_type="neumann", v_bc_left_value=0.0,
         v_bc_right_type="neumann", v_bc_right_value=0.0, interface_center_x=2.0, interface_center_y=2.0,
@@ -49,6 +50,11 @@ def workload_cfg() -> dict:
         density_ratio=10.0, viscosity_ratio=10.0, body_force_y=-1.0, dt=5e-5, pressure_scheme="split_icpcg",
         poisson_iterations=2000, pressure_tolerance=1e-10, ch_inner_iterations=500, ch_tolerance=1e-10,
         momentum_iterations=200, momentum_tolerance=1e-10, surface_tension_multiplier=1.0)
+    if grid is not None:
+        # finer grids need more CG iterations to reach the same tolerance: no cap in the way
+        cfg.update(nx=int(grid[0]), ny=int(grid[1]), name=f"rising_bubble_{grid[0]}x{grid[1]}_split_icpcg",
+                   poisson_iterations=50000, ch_inner_iterations=5000)
+    return cfg
 
 
 def initial_state(cfg: dict, seed: int = 2) -> dict:
@@ -222,9 +228,10 @@ def run_ours(args):
     dist, rank, world, local = dist_setup(args.gpus)
     device = local if dist is not None else 0
     torch.cuda.set_device(device)
-    cfg = workload_cfg()
+    cfg = workload_cfg(args.grid)
     state = initial_state(cfg)
     n_cells = cfg["nx"] * cfg["ny"]
+    nxy = f"{cfg['nx']}x{cfg['ny']}"
 
     solver = dn.Solver(cfg, device=device)
 
@@ -443,7 +450,7 @@ def run_ours(args):
         sec, impl = cpu_reference_run(cfg, state, 0, sample)
         cpu = {"value": round(n_cells * sample / sec / 1e6, 6), "unit": "Mcell-steps/s", "cores": 1,
                "kind": "reference" if impl == "reference" else "port",
-               "sample": f"{sample} steps (steps 0-{sample - 1}) of the same 192x384 workload from the same "
+               "sample": f"{sample} steps (steps 0-{sample - 1}) of the same {nxy} workload from the same "
                          f"seeded state; the reference step is single-threaded",
                "seconds": round(sec, 3)}
 
@@ -455,8 +462,8 @@ def run_ours(args):
             "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "rising bubble 192x384 split_icpcg, R0-unit parameters of testcase 26, seeded "
-                                   "interface modes 2-8", "grid": [192, 384], "pressure_scheme": "split_icpcg",
+            "config": {"workload": f"rising bubble {nxy} split_icpcg, R0-unit parameters of testcase 26, seeded "
+                                   "interface modes 2-8", "grid": [cfg["nx"], cfg["ny"]], "pressure_scheme": "split_icpcg",
                        "pressure_tolerance": 1e-10, "ch_tolerance": 1e-10, "precision": "fp64",
                        "l2": "flushed (512 MB write) between timed steps", "parallelism": f"replicas x{world}"},
             "iterations_mean": mean_rep,
@@ -523,6 +530,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--batch", type=int, default=8, help="instances of the batched-ensemble arm (0 skips it)")
     ap.add_argument("--ensemble", type=int, default=64, help="uneven droplet instances of the ensemble arm (0 skips)")
+    ap.add_argument("--grid", type=lambda t: tuple(int(v) for v in t.lower().split("x")), default=None,
+                    help="NXxNY: the rising bubble on another grid (default 192x384)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -769,6 +769,92 @@ __device__ void apply_seq13(const PcgArgs &P, double m_r, double (&acc)[3], doub
 // The residual r is kept unprojected in memory; the mean of the latest update (m_r) is subtracted on the
 // fly by the preconditioner and folded in by the next update, which equals projecting r after every
 // update (pressure.cpp:225-239 applied in ch_sparse_krylov.hpp:602-605).
+constexpr int kRowsInFlight = 2;  // rows per thread whose loads the SpMV and update phases issue together
+
+// P1 rows of one thread: p = z - m_z + beta p_old, Ap, and the sums (sum p, p.Ap, sum Ap).  kRowsInFlight rows
+// at a time: their loads are issued before any of their stores, so the memory system has that many rows in
+// flight per thread (the kernel runs one 256-thread CTA per SM); the sums still run over the thread's rows
+// in increasing order.
+template <int S, typename T>
+__device__ __forceinline__ void pcg_spmv_rows(const PcgArgsT<T> &P, long long lo, long long hi, bool first, T m_z_t,
+                                           T beta_t, const T *p_old, T *p_new, double (&v)[3]) {
+  const SpOpT<T> &A = P.A;
+  const int n = A.n, ny = A.ny;
+  for (long long r0 = lo + threadIdx.x; r0 < hi; r0 += (long long)kRowsInFlight * blockDim.x) {
+    T prv[kRowsInFlight], apvv[kRowsInFlight];
+#pragma unroll
+    for (int q = 0; q < kRowsInFlight; ++q) {
+      const long long r = r0 + (long long)q * blockDim.x;
+      prv[q] = T(0);
+      apvv[q] = T(0);
+      if (r < hi) {
+        const int ri = (int)r, i = ri / ny, j = ri - i * ny;
+        T apv = T(0);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const T a = A.a[(size_t)s * n + r];
+          if (a != T(0)) {
+            const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
+            const T pc = first ? (P.z[c] - m_z_t) : (P.z[c] - m_z_t) + beta_t * p_old[c];
+            apv += a * pc;
+          }
+        }
+        prv[q] = first ? (P.z[r] - m_z_t) : (P.z[r] - m_z_t) + beta_t * p_old[r];
+        apvv[q] = apv;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsInFlight; ++q) {
+      const long long r = r0 + (long long)q * blockDim.x;
+      if (r < hi) {
+        p_new[r] = prv[q];
+        P.ap[r] = apvv[q];
+        const double prd = prv[q], apd = apvv[q];
+        v[0] += prd;
+        v[1] += prd * apd;
+        v[2] += apd;
+      }
+    }
+  }
+}
+
+// P2 rows of one thread: p -= m_p, x += alpha p, r -= alpha Ap, and the sums for the norms; rows in flight
+// as in pcg_spmv_rows.
+template <typename T>
+__device__ __forceinline__ void pcg_update_rows(const PcgArgsT<T> &P, long long lo, long long hi, T m_p_t, T alpha_t,
+                                             T m_x_t, T m_r_t, T *p_new, double (&w)[5]) {
+  for (long long r0 = lo + threadIdx.x; r0 < hi; r0 += (long long)kRowsInFlight * blockDim.x) {
+    T ppv[kRowsInFlight], xvv[kRowsInFlight], rvv[kRowsInFlight], dv[kRowsInFlight];
+#pragma unroll
+    for (int q = 0; q < kRowsInFlight; ++q) {
+      const long long r = r0 + (long long)q * blockDim.x;
+      if (r < hi) {
+        const T pp = p_new[r] - m_p_t;
+        const T delta = alpha_t * pp;
+        ppv[q] = pp;
+        dv[q] = delta;
+        xvv[q] = (P.x[r] - m_x_t) + delta;
+        rvv[q] = (P.r[r] - m_r_t) - alpha_t * P.ap[r];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsInFlight; ++q) {
+      const long long r = r0 + (long long)q * blockDim.x;
+      if (r < hi) {
+        p_new[r] = ppv[q];
+        P.x[r] = xvv[q];
+        P.r[r] = rvv[q];
+        const double dd = dv[q], xd = xvv[q], rd = rvv[q];
+        w[0] += dd * dd;
+        w[1] += xd * xd;
+        w[2] += xd;
+        w[3] += rd;
+        w[4] += rd * rd;
+      }
+    }
+  }
+}
+
 template <int S, int SWEEP, typename T = double>
 __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
   __shared__ double sh[8 * 32 + 8];
@@ -915,26 +1001,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
     t0 = global_ns();
     const T m_z_t = (T)m_z, beta_t = (T)beta;
     double v[3] = {0.0, 0.0, 0.0};
-    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
-      const int i = (int)(r / ny), j = (int)(r % ny);
-      T apv = T(0);
-#pragma unroll
-      for (int s = 0; s < S; ++s) {
-        const T a = A.a[(size_t)s * n + r];
-        if (a != T(0)) {
-          const long long c = slot_col<S>(i, j, s, A.nx, A.ny, A.px, A.py);
-          const T pc = first ? (P.z[c] - m_z_t) : (P.z[c] - m_z_t) + beta_t * p_old[c];
-          apv += a * pc;
-        }
-      }
-      const T pr = first ? (P.z[r] - m_z_t) : (P.z[r] - m_z_t) + beta_t * p_old[r];
-      p_new[r] = pr;
-      P.ap[r] = apv;
-      const double prd = pr, apd = apv;
-      v[0] += prd;
-      v[1] += prd * apd;
-      v[2] += apd;
-    }
+    pcg_spmv_rows<S, T>(P, lo, hi, first, m_z_t, beta_t, p_old, p_new, v);
     if (!grid_sum<3>(v, P.partials, parity, sh, bar)) return;
     const double m_p = P.project ? v[0] / dn_ : 0.0;
     const double pap = P.project ? v[1] - m_p * v[2] : v[1];
@@ -948,21 +1015,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
     // ---- P2: x += alpha p ; r -= alpha Ap ; norms (ch_sparse_krylov.hpp:592-610)
     const T m_p_t = (T)m_p, alpha_t = (T)alpha, m_x_t = (T)m_x, m_r_t = (T)m_r;
     double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (long long r = lo + threadIdx.x; r < hi; r += blockDim.x) {
-      const T pp = p_new[r] - m_p_t;
-      p_new[r] = pp;
-      const T delta = alpha_t * pp;
-      const T xv = (P.x[r] - m_x_t) + delta;
-      P.x[r] = xv;
-      const T rv = (P.r[r] - m_r_t) - alpha_t * P.ap[r];
-      P.r[r] = rv;
-      const double dd = delta, xd = xv, rd = rv;
-      w[0] += dd * dd;
-      w[1] += xd * xd;
-      w[2] += xd;
-      w[3] += rd;
-      w[4] += rd * rd;
-    }
+    pcg_update_rows<T>(P, lo, hi, m_p_t, alpha_t, m_x_t, m_r_t, p_new, w);
     if (!grid_sum<5>(w, P.partials, parity, sh, bar)) return;
     const unsigned long long t2 = global_ns();
     t_p2 += t2 - t1;
