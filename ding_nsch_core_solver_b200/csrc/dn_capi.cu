@@ -1689,7 +1689,12 @@ dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, 
     for (int b2 = 0; b2 < a; ++b2)
       if (handles[b2] == handles[a]) return DN_ERR_INVALID_ARGUMENT;  // one handle twice would race with itself
   }
-  std::vector<dn_status> st((size_t)count, DN_OK);
+  std::vector<dn_status> st;
+  try {
+    st.assign((size_t)count, DN_OK);
+  } catch (...) {
+    return DN_ERR_INVALID_ARGUMENT;
+  }
   std::atomic<int> next{0};
   auto worker = [&]() {
     for (int a = next.fetch_add(1); a < count; a = next.fetch_add(1)) {
@@ -1703,8 +1708,12 @@ dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, 
   };
   const int nworkers = std::min(count, 64);
   std::vector<std::thread> pool;
-  pool.reserve((size_t)std::max(0, nworkers - 1));
-  for (int w = 1; w < nworkers; ++w) pool.emplace_back(worker);
+  try {
+    pool.reserve((size_t)std::max(0, nworkers - 1));
+    for (int w = 1; w < nworkers; ++w) pool.emplace_back(worker);
+  } catch (...) {
+    // no more threads: the ones started and this thread share the remaining handles
+  }
   if (nworkers > 0) worker();
   for (auto &t : pool) t.join();
   for (int a = 0; a < count; ++a)
