@@ -384,10 +384,16 @@ def run_ours(args):
     ensemble = None
     if args.ensemble > 0:
         cfgs = ensemble_cfgs(args.ensemble)
+        total_cells = sum(c["nx"] * c["ny"] for c in cfgs)
+
+        def share(c):
+            # each instance's persistent grids take its share of the cells' worth of SMs
+            return len(cfgs) if args.ensemble_equal else max(1, round(total_cells / (c["nx"] * c["ny"])))
+
         members = []
         try:
             for ec in cfgs:
-                m = dn.Solver(dict(ec, device_share=len(cfgs)), device=device)
+                m = dn.Solver(dict(ec, device_share=share(ec)), device=device)
                 m.initialize()
                 m.set_initial_mass(m.compute_mass("c"))
                 members.append(m)
@@ -419,7 +425,8 @@ def run_ours(args):
                         "mass_drift_max": max(d["mass_drift"] for d in diag),
                         "workload": "uneven droplets: grids {64..256}^2, periodic both ways, split_icpcg, mixed, "
                                     "dt 1e-5, seed 4; all instances stepped together by dn_step_batch",
-                        "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS")}
+                        "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
+                        "sm_share": "equal (1/instances)" if args.ensemble_equal else "in proportion to cells"}
         except capi.DnError as e:
             ensemble = {"instances": len(cfgs), "error": str(e)}
         for m in members:
@@ -530,6 +537,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--batch", type=int, default=8, help="instances of the batched-ensemble arm (0 skips it)")
     ap.add_argument("--ensemble", type=int, default=64, help="uneven droplet instances of the ensemble arm (0 skips)")
+    ap.add_argument("--ensemble-equal", action="store_true",
+                    help="give every ensemble instance the same share of the SMs (default: in proportion to its cells)")
     ap.add_argument("--grid", type=lambda t: tuple(int(v) for v in t.lower().split("x")), default=None,
                     help="NXxNY: the rising bubble on another grid (default 192x384)")
     args = ap.parse_args()
