@@ -569,6 +569,7 @@ dn_status dev_status_to_dn(dn_handle *h, int st) {
   case kDevBicgRhatV: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid r_hat^T A M^{-1} p");
   case kDevBicgTT: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid t^T t");
   case kDevBicgOmega: return fail(h, DN_ERR_BICGSTAB_BREAKDOWN, "bicgstab breakdown: invalid omega");
+  case kDevJacobiDiverged: return fail(h, DN_ERR_NONFINITE, "Jacobi pressure solve diverged");
   default: return fail(h, DN_ERR_CUDA, "unknown device status");
   }
 }
@@ -1163,11 +1164,121 @@ dn_status compact_subtract_mean(dn_handle *h, double *x) {
   return check_launch(h, "k_vec_sub_scalar");
 }
 
+// solve_pressure_correction_jacobi, pressure.cpp:250-300: the variable-coefficient system (as icpcg builds it,
+// regularised) solved by Jacobi sweeps from x = 0 until max |b - A x| < tol or the iteration limit.  The
+// sweeps and the residual checks are launched in batches; a device flag stops the batch at convergence, and
+// the host reads the flag, the count and the residual after each batch.
+dn_status pressure_jacobi(dn_handle *h, dn_report *rep) {
+  Fv *f = h->f;
+  const dn_config &cfg = h->cfg;
+  DN_TRY(fill_field(h, f[DN_F_P_CORR], 0.0));
+  DN_TRY(bc(h, f[DN_F_P_CORR], kBCPressure));
+  k_p_assemble<<<blocks_for(h->n), 256, 0, h->stream>>>(h->G, h->bc, f[DN_F_RHO_MID], f[DN_F_U_STAR], f[DN_F_V_STAR],
+                                                       h->pe, 0, 1.0, cfg.dt, h->a5, h->b);
+  DN_TRY(check_launch(h, "k_p_assemble"));
+  if (!h->has_dirichlet) DN_TRY(compact_subtract_mean(h, h->b));
+  double *xb[2] = {h->x, h->y};
+  DN_CUDA(h, cudaMemsetAsync(h->x, 0, h->n * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(h->y, 0, h->n * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+  unsigned int *done = h->prog, *iters = h->prog + 1;
+  DN_CUDA(h, cudaMemsetAsync(h->prog, 0, 2 * sizeof(unsigned int), h->stream));
+  double *resid = h->scal + 24;
+  const int nb = (int)((h->n + 255) / 256);
+  const int limit = std::max(0, cfg.poisson_iterations);
+  int launched = 0;
+  unsigned int host_flags[2] = {0u, 0u};
+  while (launched < limit) {
+    const int batch = std::min(256, limit - launched);
+    for (int k = 0; k < batch; ++k) {
+      const int it = launched + k;
+      k_jacobi_sweep<<<nb, 256, 0, h->stream>>>(h->a5, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py, h->b,
+                                                 xb[it & 1], xb[(it + 1) & 1], h->partials, done, h->status);
+      k_jacobi_check<<<1, 32, 0, h->stream>>>(h->partials, nb, cfg.pressure_tolerance, done, iters, resid);
+    }
+    DN_TRY(check_launch(h, "k_jacobi_sweep"));
+    launched += batch;
+    DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 40, h->prog, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                               h->stream));
+    DN_CUDA(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(host_flags, h->host_scal + 40, sizeof(host_flags));
+    int st = 0;
+    DN_TRY(read_status(h, &st));
+    if (st != kDevOk) return dev_status_to_dn(h, st);
+    if (host_flags[0]) break;
+  }
+  const int its = (int)host_flags[1];
+  double res = 0.0;
+  if (its > 0) {
+    DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 44, resid, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    DN_CUDA(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(&res, h->host_scal + 44, sizeof(double));
+  }
+  h->launches += 2LL * its + 1;
+  rep->pressure_iterations = its;
+  rep->pressure_residual = res;
+  rep->refinement_cycles = 0;
+  h->phase_ms[7] = its;
+  LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], xb[its & 1], f[DN_F_P_CORR]);
+  if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
+  return bc(h, f[DN_F_P_CORR], kBCPressure);
+}
+
+// The CH advective term rhs = -div(u c) of `c` (its scalar BC ghosts refilled first) into h->arhs.
+dn_status advective_rhs(dn_handle *h, const Fv &c) {
+  Fv *f = h->f;
+  DN_TRY(bc(h, c, kBCScalar));
+  LAUNCH_INTERIOR(k_adv_flux_x, h->afx, c, f[DN_F_U], h->afx);
+  LAUNCH_INTERIOR(k_adv_flux_y, h->afy, c, f[DN_F_V], h->afy);
+  DN_TRY(bc(h, h->afx, kBCU));
+  DN_TRY(bc(h, h->afy, kBCV));
+  LAUNCH_INTERIOR(k_flux_div, h->arhs, h->afx, h->afy, h->arhs, h->G, 1);
+  return DN_OK;
+}
+
+// mode = advection_only (solver.cpp:232-245 with solve_phase_advection_only, phase_field.cpp:398-435): c
+// advanced by SSPRK3 with WENO5 fluxes in the current velocity, materials from the new c, mu = 0.
+dn_status advection_step(dn_handle *h, dn_report *rep) {
+  Fv *f = h->f;
+  const double dt = h->cfg.dt;
+  const Fv &c0 = h->cmid, &c1 = h->mm, &c2 = h->sm_c;
+  DN_TRY(copy_field(h, c0, f[DN_F_C]));
+  DN_TRY(advective_rhs(h, c0));
+  LAUNCH_INTERIOR(k_ssprk3_stage, c1, c0, c0, h->arhs, c1, dt, 1);
+  DN_TRY(advective_rhs(h, c1));
+  LAUNCH_INTERIOR(k_ssprk3_stage, c2, c0, c1, h->arhs, c2, dt, 2);
+  DN_TRY(advective_rhs(h, c2));
+  LAUNCH_INTERIOR(k_ssprk3_stage, f[DN_F_C], c0, c2, h->arhs, f[DN_F_C], dt, 3);
+  DN_TRY(bc(h, f[DN_F_C], kBCScalar));
+  // ch_residual: ||c - c0|| / ||c|| over the interior (field_diff_l2)
+  const int nb = 128;
+  k_diff_l2_partials<<<nb, 256, 0, h->stream>>>(f[DN_F_C], c0, h->partials);
+  DN_TRY(check_launch(h, "k_diff_l2_partials"));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->partials, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_TRY(materials(h, f[DN_F_C], f[DN_F_RHO], f[DN_F_ETA]));
+  DN_TRY(fill_field(h, f[DN_F_MU], 0.0));
+  DN_TRY(bc(h, f[DN_F_MU], kBCScalar));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  double d2 = 0.0, n2 = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    d2 += h->host_scal[b];
+    n2 += h->host_scal[nb + b];
+  }
+  rep->ch_residual = std::sqrt(d2 / std::max(n2, 1.0e-30));
+  rep->ch_iterations = 3;
+  rep->momentum_iterations = 0;
+  rep->pressure_iterations = 0;
+  rep->coupling_iterations = 0;
+  rep->boundary_speed_pre = 0.0;
+  rep->boundary_speed_post = 0.0;
+  rep->ch_equation_residual = 0.0;
+  return DN_OK;
+}
+
 dn_status pressure(dn_handle *h, int step, dn_report *rep) {
   Fv *f = h->f;
   const dn_config &cfg = h->cfg;
-  if (cfg.pressure_scheme == DN_P_JACOBI)
-    return fail(h, DN_ERR_UNSUPPORTED, "pressure_scheme jacobi is not implemented by the CUDA backend");
+  if (cfg.pressure_scheme == DN_P_JACOBI) return pressure_jacobi(h, rep);
   const bool split = use_split(cfg);
   const bool icc = cfg.pressure_scheme == DN_P_ICPCG || cfg.pressure_scheme == DN_P_SPLIT_ICPCG;
   DN_TRY(fill_field(h, f[DN_F_P_CORR], 0.0));
@@ -1308,8 +1419,6 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   if (c.nx < 8 || c.ny < 8) return bad(DN_ERR_UNSUPPORTED, "the CUDA backend needs nx, ny >= 8");
   if (c.ghost < 3) return bad(DN_ERR_UNSUPPORTED, "ghost must be >= 3 (WENO5 stencil)");
   if ((long long)c.nx * c.ny > (1LL << 30)) return bad(DN_ERR_UNSUPPORTED, "grid too large");
-  if (c.mode == DN_MODE_ADVECTION_ONLY)
-    return bad(DN_ERR_UNSUPPORTED, "mode advection_only is not implemented by the CUDA backend");
   // validate_boundary_configuration, operators.cpp:11-34
   static const char *names[4] = {"left", "right", "bottom", "top"};
   for (int s = 0; s < 4; ++s) {
@@ -1661,6 +1770,11 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
   for (int k = 4; k < 8; ++k) h->phase_ms[k] = 0.0;
   cudaEventRecord(h->ev[0], h->stream);
   DN_TRY(begin_step(h));
+  if (h->cfg.mode == DN_MODE_ADVECTION_ONLY) {
+    DN_TRY(advection_step(h, rep));
+    for (int k = 0; k < 4; ++k) h->phase_ms[k] = 0.0;
+    return DN_OK;
+  }
   DN_TRY(phase(h, step, rep));
   cudaEventRecord(h->ev[1], h->stream);
   DN_TRY(momentum(h, step, rep));

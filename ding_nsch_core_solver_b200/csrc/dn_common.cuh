@@ -29,6 +29,7 @@ enum DevStatus : int {
   kDevBicgTT = 7,            // "bicgstab breakdown: invalid t^T t"
   kDevBicgOmega = 8,         // "bicgstab breakdown: invalid omega"
   kDevFactorFailed = 9,      // incomplete factorization hit the pivot floor
+  kDevJacobiDiverged = 10,   // "Jacobi pressure solve diverged"
 };
 
 enum PrecKind { kPrecDiag = 0, kPrecLDLT = 1, kPrecICC = 2 };

@@ -410,6 +410,99 @@ __global__ void k_field_sum(Fv f, double scale, double *partials) {
   block_sum<1>(v, sh);
   if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
 }
+// Jacobi pressure iteration (solve_pressure_correction_jacobi, pressure.cpp:250-300): one sweep
+// xn = x + (b - A x) / |diag| over the 5-point system, each row's A x summed in ascending column order (the
+// CSR order), and the block maxima of |b - A x|.  Skips when `done` is set, so batches of launches past
+// convergence do nothing.
+__global__ void k_jacobi_sweep(const double *a, int n, int nx, int ny, int px, int py, const double *rhs,
+                               const double *x, double *xn, double *bmax, const unsigned int *done, int *status) {
+  __shared__ double sh[32];
+  if (*(volatile const unsigned int *)done) return;
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double res = 0.0;
+  if (r < n) {
+    const int i = (int)(r / ny), j = (int)(r % ny);
+    // neighbours W, S, C, N, E with periodic wraps, sorted by column
+    long long col[5];
+    double val[5];
+    int cnt = 0;
+    const int di[5] = {-1, 0, 0, 0, 1}, dj[5] = {0, -1, 0, 1, 0};
+    for (int s = 0; s < 5; ++s) {
+      const double v = a[(size_t)s * n + r];
+      if (v == 0.0) continue;
+      int ii = i + di[s], jj = j + dj[s];
+      if (ii < 0 || ii >= nx) ii = (ii + nx) % nx;  // a nonzero entry across the boundary is periodic
+      if (jj < 0 || jj >= ny) jj = (jj + ny) % ny;
+      const long long c = (long long)ii * ny + jj;
+      int p = cnt++;
+      while (p > 0 && col[p - 1] > c) {
+        col[p] = col[p - 1];
+        val[p] = val[p - 1];
+        --p;
+      }
+      col[p] = c;
+      val[p] = v;
+    }
+    double diag = 0.0, ax = 0.0;
+    for (int p = 0; p < cnt; ++p) {
+      ax += val[p] * x[col[p]];
+      if (col[p] == r) diag = val[p];
+    }
+    const double rr = rhs[r] - ax;
+    if (!isfinite(rr) || !isfinite(diag) || fabs(diag) < 1.0e-30) atomicCAS(status, kDevOk, kDevJacobiDiverged);
+    xn[r] = x[r] + 1.0 * rr / fmax(fabs(diag), 1.0e-30);
+    res = fabs(rr);
+  }
+  res = warp_max(res);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = res;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    v = warp_max(v);
+    if (threadIdx.x == 0) bmax[blockIdx.x] = v;
+  }
+}
+// After a sweep: the residual max |b - A x| (one warp), the iteration count, and done when it is below tol.
+__global__ void k_jacobi_check(const double *bmax, int nb, double tol, unsigned int *done, unsigned int *iters,
+                               double *residual) {
+  if (*(volatile unsigned int *)done) return;
+  double m = 0.0;
+  for (int b = threadIdx.x; b < nb; b += 32) m = fmax(m, bmax[b]);
+  m = warp_max(m);
+  if (threadIdx.x == 0) {
+    *residual = m;
+    *iters += 1u;
+    if (m < tol) *done = 1u;
+  }
+}
+// SSPRK3 stage (solve_phase_advection_only, phase_field.cpp:398-435): stage 1 out = c0 + dt rs; stage 2
+// out = 3/4 c0 + 1/4 (cs + dt rs); stage 3 out = 1/3 c0 + 2/3 (cs + dt rs).
+__global__ void k_ssprk3_stage(Fv c0, Fv cs, Fv rs, Fv out, double dt, int stage) {
+  DN_FOR_INTERIOR(out);
+  if (stage == 1) {
+    out.at(i, j) = c0.at(i, j) + dt * rs.at(i, j);
+  } else {
+    const double pred = cs.at(i, j) + dt * rs.at(i, j);
+    out.at(i, j) = stage == 2 ? 0.75 * c0.at(i, j) + 0.25 * pred : (1.0 / 3.0) * c0.at(i, j) + (2.0 / 3.0) * pred;
+  }
+}
+// Per-block partial sums of (a - b)^2 and a^2 over the interior (field_diff_l2 of the reference), [2][nb].
+__global__ void k_diff_l2_partials(Fv a, Fv b, double *partials) {
+  __shared__ double sh[8 * 32 * 2];
+  const long long n = (long long)a.nx * a.ny;
+  double v[2] = {0.0, 0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / a.ny), j = (int)(t % a.ny);
+    const double d = a.at(i, j) - b.at(i, j);
+    v[0] += d * d;
+    v[1] += a.at(i, j) * a.at(i, j);
+  }
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+  }
+}
 __global__ void k_vec_sum(const double *x, long long n, double *partials) {
   __shared__ double sh[8 * 32];
   double v[1] = {0.0};

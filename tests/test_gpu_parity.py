@@ -67,6 +67,14 @@ CASES = {
     "single_phase": unit(mode="single_phase", pressure_scheme="icpcg", density_ratio=3.0),
     "many_lines_split": unit(nx=130, ny=24, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
                              dt=1e-4, body_force_y=-1.0),
+    # Jacobi pressure (pressure.cpp:250-300), run to its iteration limit as the reference does here
+    "jacobi_walls": unit(nx=12, ny=12, periodic_x=False, periodic_y=False, pressure_scheme="jacobi",
+                         poisson_iterations=300, dt=1e-4),
+    "jacobi_periodic": unit(pressure_scheme="jacobi", poisson_iterations=300, dt=1e-4),
+    # advection only: SSPRK3 + WENO5 of the Zalesak disk in solid-body rotation (phase_field.cpp:398-435)
+    "advection_only_zalesak": unit(mode="advection_only", velocity_profile="solid_body_rotation",
+                                   angular_velocity=2 * math.pi, phase_initializer="zalesak_disk",
+                                   interface_radius=0.3),
 }
 
 
