@@ -116,6 +116,8 @@ def load():
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_advection": (I, [H, VP, VP, VP, VP]),
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
+        "dn_write_restart": (I, [H, I, C.c_char_p]),
+        "dn_load_restart": (I, [H, C.c_char_p, C.POINTER(C.c_int)]),
         "dn_explicit_operator": (I, [H, VP, VP, VP, VP]),
         "dn_explicit_operator_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_diagnostics": (I, [H, C.POINTER(Diag)]),
@@ -275,6 +277,16 @@ class Solver:
         return out, its.value, rel.value
 
     # ---- diagnostics / timing
+    def write_restart(self, path: str, step: int) -> None:
+        """Solver::write_restart_snapshot: the reference's v2 snapshot of this solver's state."""
+        self._check(self._lib.dn_write_restart(self._h, int(step), str(path).encode()))
+
+    def load_restart(self, path: str) -> int:
+        """Solver::load_restart_snapshot: state from a v1/v2 snapshot; returns its step."""
+        st = C.c_int()
+        self._check(self._lib.dn_load_restart(self._h, str(path).encode(), C.byref(st)))
+        return st.value
+
     def diagnostics(self) -> dict:
         d = Diag()
         self._check(self._lib.dn_diagnostics(self._h, C.byref(d)))

@@ -1734,6 +1734,188 @@ dn_status dn_refresh_derived(dn_handle *h) {
   return DN_OK;
 }
 
+// ---- restart snapshot v2 (Solver::write_restart_snapshot / load_restart_snapshot, io.cpp:271-437) ----
+// Native-endian binary: the magic string, version 2, step, initial mass, mode string, grid and physics
+// scalars, periodicity, the 12 configured boundary specs, then 12 Field2D arrays with their extents.
+namespace {
+constexpr char kRestartMagic[] = "ding_nsch_restart_v1";
+const int kRestartFields[12] = {DN_F_C,      DN_F_C_PREV, DN_F_C_PREV2, DN_F_P,      DN_F_P_PREV,  DN_F_U,
+                                DN_F_V,      DN_F_U_PREV, DN_F_V_PREV,  DN_F_E_PREV, DN_F_HU_PREV, DN_F_HV_PREV};
+
+const char *mode_name(int m) {
+  return m == DN_MODE_SINGLE_PHASE ? "single_phase" : (m == DN_MODE_ADVECTION_ONLY ? "advection_only" : "coupled");
+}
+bool restart_nearly_equal(double a, double b) {  // io.cpp:86-89
+  const double scale = std::max({1.0, std::fabs(a), std::fabs(b)});
+  return std::fabs(a - b) <= 1.0e-12 * scale;
+}
+const double *restart_scalars(const dn_config &c, double (&v)[13]) {
+  const double t[13] = {c.dt, c.lx, c.ly, c.re, c.ca, c.pe, c.cn, c.density_ratio, c.viscosity_ratio,
+                        c.body_force_x, c.body_force_y, c.top_wall_velocity_x, c.bottom_wall_velocity_x};
+  std::copy(t, t + 13, v);
+  return v;
+}
+const char *const kRestartScalarNames[13] = {"dt", "lx", "ly", "re", "ca", "pe", "cn", "density_ratio",
+                                             "viscosity_ratio", "body_force_x", "body_force_y",
+                                             "top_wall_velocity_x", "bottom_wall_velocity_x"};
+}  // namespace
+
+dn_status dn_write_restart(dn_handle *h, int step, const char *path) {
+  if (!h || !path) return DN_ERR_INVALID_ARGUMENT;
+  const dn_config &c = h->cfg;
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));  // the state of every launched step
+  const std::string tmp = std::string(path) + ".tmp";
+  std::FILE *fp = std::fopen(tmp.c_str(), "wb");
+  if (!fp) return fail(h, DN_ERR_INVALID_ARGUMENT, "cannot open restart snapshot for writing");
+  bool ok = true;
+  auto wr = [&](const void *p, size_t n) { ok = ok && std::fwrite(p, 1, n, fp) == n; };
+  auto ws = [&](const std::string &v) {
+    const std::uint64_t n = v.size();
+    wr(&n, sizeof n);
+    wr(v.data(), v.size());
+  };
+  ws(kRestartMagic);
+  const std::uint32_t version = 2;
+  wr(&version, sizeof version);
+  wr(&step, sizeof step);
+  wr(&h->initial_mass, sizeof(double));
+  ws(mode_name(c.mode));
+  wr(&c.nx, sizeof(int));
+  wr(&c.ny, sizeof(int));
+  wr(&c.ghost, sizeof(int));
+  double sc[13];
+  wr(restart_scalars(c, sc), sizeof sc);
+  const int px = c.periodic_x != 0, py = c.periodic_y != 0;
+  wr(&px, sizeof px);
+  wr(&py, sizeof py);
+  for (const dn_bc *set : {c.p_bc, c.u_bc, c.v_bc})
+    for (int sd = 0; sd < 4; ++sd) {
+      wr(&set[sd].type, sizeof(int));
+      wr(&set[sd].value, sizeof(double));
+    }
+  std::vector<double> buf;
+  for (int id : kRestartFields) {
+    const Fv &f = h->f[id];
+    const std::uint64_t size = f.size();
+    wr(&f.nx, sizeof(int));
+    wr(&f.ny, sizeof(int));
+    wr(&f.g, sizeof(int));
+    wr(&size, sizeof size);
+    buf.resize(size);
+    if (cudaMemcpyAsync(buf.data(), f.d, size * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+      ok = false;
+    wr(buf.data(), size * sizeof(double));
+  }
+  ok = (std::fflush(fp) == 0) && ok;
+  ok = (std::fclose(fp) == 0) && ok;
+  if (!ok) {
+    std::remove(tmp.c_str());
+    return fail(h, DN_ERR_INVALID_ARGUMENT, "failed to write restart snapshot");
+  }
+  if (std::rename(tmp.c_str(), path) != 0) return fail(h, DN_ERR_INVALID_ARGUMENT, "failed to rename restart snapshot");
+  return DN_OK;
+}
+
+dn_status dn_load_restart(dn_handle *h, const char *path, int *step) {
+  if (!h || !path) return DN_ERR_INVALID_ARGUMENT;
+  const dn_config &c = h->cfg;
+  std::FILE *fp = std::fopen(path, "rb");
+  if (!fp) return fail(h, DN_ERR_INVALID_ARGUMENT, std::string("cannot open restart snapshot: ") + path);
+  std::vector<double> buf;
+  auto body = [&]() -> dn_status {
+    bool ok = true;
+    auto rd = [&](void *p, size_t n) { ok = ok && std::fread(p, 1, n, fp) == n; };
+    auto rs = [&](std::string &v) {
+      std::uint64_t n = 0;
+      rd(&n, sizeof n);
+      if (!ok || n > 4096) {
+        ok = false;
+        return;
+      }
+      v.assign((size_t)n, '\0');
+      rd(&v[0], (size_t)n);
+    };
+    auto incompatible = [&](const std::string &what) {
+      return fail(h, DN_ERR_CONFIG, "restart snapshot incompatible with config: " + what);
+    };
+    std::string magic, mode;
+    rs(magic);
+    if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot string");
+    if (magic != kRestartMagic) return incompatible("unrecognized restart file");
+    std::uint32_t version = 0;
+    int rstep = 0;
+    double mass = 0.0;
+    rd(&version, sizeof version);
+    if (!ok || (version != 1u && version != 2u)) return incompatible("unsupported restart file version");
+    rd(&rstep, sizeof rstep);
+    rd(&mass, sizeof mass);
+    rs(mode);
+    if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot");
+    if (mode != mode_name(c.mode)) return incompatible("mode");
+    int iv[3];
+    rd(iv, sizeof iv);
+    if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot");
+    if (iv[0] != c.nx) return incompatible("nx");
+    if (iv[1] != c.ny) return incompatible("ny");
+    if (iv[2] != c.ghost) return incompatible("ghost");
+    double sc[13], mine[13];
+    rd(sc, sizeof sc);
+    if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot");
+    restart_scalars(c, mine);
+    for (int k = 0; k < 13; ++k)
+      if (!restart_nearly_equal(sc[k], mine[k])) return incompatible(kRestartScalarNames[k]);
+    int per[2];
+    rd(per, sizeof per);
+    if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot");
+    if (per[0] != (c.periodic_x != 0)) return incompatible("periodic_x");
+    if (per[1] != (c.periodic_y != 0)) return incompatible("periodic_y");
+    if (version >= 2u) {
+      static const char *sides[4] = {"left", "right", "bottom", "top"};
+      const char *kinds[3] = {"pressure", "u", "v"};
+      const dn_bc *sets[3] = {c.p_bc, c.u_bc, c.v_bc};
+      for (int k = 0; k < 3; ++k)
+        for (int sd = 0; sd < 4; ++sd) {
+          int type = 0;
+          double value = 0.0;
+          rd(&type, sizeof type);
+          rd(&value, sizeof value);
+          if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot");
+          const std::string name = std::string(kinds[k]) + "_bc_" + sides[sd];
+          if (type != sets[k][sd].type) return incompatible(name + "_type");
+          if (!restart_nearly_equal(value, sets[k][sd].value)) return incompatible(name + "_value");
+        }
+    }
+    for (int id : kRestartFields) {
+      const Fv &f = h->f[id];
+      int ext[3];
+      std::uint64_t size = 0;
+      rd(ext, sizeof ext);
+      rd(&size, sizeof size);
+      if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot field");
+      if (ext[0] != f.nx || ext[1] != f.ny || ext[2] != f.g || size != f.size())
+        return fail(h, DN_ERR_CONFIG, "restart snapshot field size mismatch");
+      buf.resize(size);
+      rd(buf.data(), size * sizeof(double));
+      if (!ok) return fail(h, DN_ERR_CONFIG, "failed to read restart snapshot field");
+      DN_CUDA(h, cudaMemcpyAsync(f.d, buf.data(), size * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      DN_CUDA(h, cudaStreamSynchronize(h->stream));  // buf is reused by the next field
+    }
+    h->initial_mass = mass;
+    if (step) *step = rstep;
+    return DN_OK;
+  };
+  const dn_status st = body();
+  std::fclose(fp);
+  if (st != DN_OK) return st;
+  // the restart's rebuild (io.cpp:412-436): BC ghosts, materials n and n-1, midpoint, mu; cleared work fields
+  DN_TRY(dn_refresh_derived(h));
+  for (int id : {DN_F_P_CORR, DN_F_U_STAR, DN_F_V_STAR, DN_F_SFX_CELL, DN_F_SFY_CELL, DN_F_SFX_U, DN_F_SFY_V})
+    DN_TRY(fill_field(h, h->f[id], 0.0));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
 dn_status dn_begin_step(dn_handle *h, int step) {
   if (!h) return DN_ERR_INVALID_ARGUMENT;
   h->step = step;

@@ -230,6 +230,18 @@ dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, c
 dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
                                        const double *gE, double *c_bar, double *u_bar, double *v_bar);
 
+/* ---- restart snapshots --------------------------------------------------------------------------------- */
+/* Solver::write_restart_snapshot (io.cpp:271-343): the reference's v2 snapshot of the handle's state (the
+ * restart fields, initial mass, grid, physics scalars and boundary specs) at `path`, written to path.tmp and
+ * renamed.  `step` is the step index stored for the resumed run.  Mode is written as "coupled",
+ * "single_phase" or "advection_only". */
+dn_status dn_write_restart(dn_handle *h, int step, const char *path);
+/* Solver::load_restart_snapshot (io.cpp:345-437): reads a v1 or v2 snapshot (the reference's or
+ * dn_write_restart's), checks it against the handle's config with the reference's rules and messages
+ * ("restart snapshot incompatible with config: ..." -> DN_ERR_CONFIG), uploads the fields and rebuilds the
+ * derived ones as the reference does.  *step (may be NULL) receives the stored step. */
+dn_status dn_load_restart(dn_handle *h, const char *path, int *step);
+
 /* ---- diagnostics ------------------------------------------------------------------------------------ */
 /* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
 dn_status dn_diagnostics(dn_handle *h, dn_diag *out);
