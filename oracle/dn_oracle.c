@@ -1554,7 +1554,8 @@ static double momentum_predictor(orc_solver *s, const fld *uadv, const fld *vadv
 /* Pressure correction (pressure.cpp, operators.cpp:400-534)                                    */
 /* ------------------------------------------------------------------------------------------ */
 static int use_split(const orc_solver *s) {
-  return s->cfg.pressure_scheme == ORC_P_SPLIT_ICPCG || s->cfg.pressure_scheme == ORC_P_SPLIT_ILDLT_PCG;
+  return s->cfg.pressure_scheme == ORC_P_SPLIT_ICPCG || s->cfg.pressure_scheme == ORC_P_SPLIT_ILDLT_PCG ||
+         s->cfg.pressure_scheme == ORC_P_SPLIT_DCDM_ICPCG;
 }
 static double split_rho_ref(const orc_solver *s) { return dmin(1.0, s->cfg.density_ratio); }
 
@@ -1688,6 +1689,149 @@ static double pressure_pcg(orc_solver *s, int split, int icc) {
   return rep.relative_residual;
 }
 
+/* solve_dcdm_conjugate_directions, ch_sparse_krylov.hpp:662-837: conjugate directions from the ICC-applied
+ * (or identity) normalised residual, A-orthogonalised against the last history_size stored directions (all
+ * stored ones when history_size is 0), at most max(max_stored, history_size, 1) kept, cleared every
+ * restart_interval iterations; the residual is recomputed as b - A x after every update. */
+static solve_rep dcdm(orc_solver *s, const csr *m, const precond *pc, const double *rhs, int max_it, double tol,
+                      double *x, int project) {
+  const int n = m->n;
+  const double floor_ = 1.0e-30;
+  double *ax = s->w[0], *r = s->w[1], *rh = s->w[2], *z = s->w[3], *d = s->w[4], *ad = s->w[5], *y = s->w[6];
+  solve_rep rep = {0, 0.0, 0.0, 0.0};
+  if (n <= 0) fail(s, "cannot solve an empty linear system");
+  spmv(m, x, ax);
+  for (int k = 0; k < n; ++k) r[k] = rhs[k] - ax[k];
+  if (project) {
+    project_mean(r, n);
+    project_mean(x, n);
+  }
+  const double rhs_norm = sqrt(dmax(dot(rhs, rhs, n), 0.0));
+  rep.absolute_residual = sqrt(dmax(dot(r, r, n), 0.0));
+  rep.relative_residual = rep.absolute_residual / dmax(rhs_norm, 1.0e-30);
+  if (rep.relative_residual < tol || rep.absolute_residual < tol) return rep;
+  const int hist = s->cfg.dcdm_history_size;
+  const int keep_max = (int)dmax((double)s->cfg.dcdm_max_stored_directions, dmax((double)hist, 1.0));
+  double **dirs = (double **)calloc((size_t)keep_max + 1, sizeof(double *));
+  double **adirs = (double **)calloc((size_t)keep_max + 1, sizeof(double *));
+  for (int k = 0; k <= keep_max; ++k) {
+    dirs[k] = (double *)malloc((size_t)n * sizeof(double));
+    adirs[k] = (double *)malloc((size_t)n * sizeof(double));
+  }
+  int stored = 0;
+  const char *err = NULL;
+  const int limit = max_it > 1 ? max_it : 1;
+  for (int it = 0; it < limit; ++it) {
+    if (s->cfg.dcdm_restart_interval > 0 && it > 0 && (it % s->cfg.dcdm_restart_interval) == 0) stored = 0;
+    const double rnorm = sqrt(dmax(dot(r, r, n), 0.0));
+    if (rnorm < tol) break;
+    for (int k = 0; k < n; ++k) rh[k] = r[k] / dmax(rnorm, floor_);
+    if (s->cfg.dcdm_direction_mode == 1)
+      memcpy(z, rh, (size_t)n * sizeof(double));
+    else
+      apply_pc(m, pc, rh, z, y);
+    int finite = 1;
+    for (int k = 0; k < n && finite; ++k) finite = isfinite(z[k]);
+    if (!finite || sqrt(dmax(dot(z, z, n), 0.0)) < floor_) memcpy(z, r, (size_t)n * sizeof(double));
+    if (project) project_mean(z, n);
+    finite = 1;
+    for (int k = 0; k < n && finite; ++k) finite = isfinite(z[k]);
+    if (!finite || sqrt(dmax(dot(z, z, n), 0.0)) < floor_) {
+      memcpy(z, r, (size_t)n * sizeof(double));
+      if (project) project_mean(z, n);
+    }
+    memcpy(d, z, (size_t)n * sizeof(double));
+    const int begin = (hist > 0 && stored > hist) ? stored - hist : 0;
+    for (int h = begin; h < stored; ++h) {
+      const double den = dot(dirs[h], adirs[h], n);
+      if (!isfinite(den) || fabs(den) < floor_) continue;
+      const double coeff = dot(d, adirs[h], n) / den;
+      for (int k = 0; k < n; ++k) d[k] -= coeff * dirs[h][k];
+    }
+    if (project) project_mean(d, n);
+    spmv(m, d, ad);
+    double rd = dot(r, d, n), dad = dot(d, ad, n);
+    finite = 1;
+    for (int k = 0; k < n && finite; ++k) finite = isfinite(d[k]) && isfinite(ad[k]);
+    if (!finite || sqrt(dmax(dot(d, d, n), 0.0)) < floor_ || !isfinite(rd) || rd <= 0.0 || !isfinite(dad) ||
+        fabs(dad) < floor_) {
+      memcpy(d, r, (size_t)n * sizeof(double));
+      if (project) project_mean(d, n);
+      spmv(m, d, ad);
+      rd = dot(r, d, n);
+      dad = dot(d, ad, n);
+      if (!isfinite(rd) || rd <= 0.0 || !isfinite(dad) || fabs(dad) < floor_) {
+        err = "dcdm breakdown: invalid fallback direction";
+        break;
+      }
+    }
+    const double alpha = rd / dad;
+    double update_sq = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const double delta = alpha * d[k];
+      x[k] += delta;
+      update_sq += delta * delta;
+    }
+    if (project) project_mean(x, n);
+    spmv(m, x, ax);
+    for (int k = 0; k < n; ++k) r[k] = rhs[k] - ax[k];
+    if (project) project_mean(r, n);
+    const double x_norm_sq = dot(x, x, n);
+    rep.iterations = it + 1;
+    rep.iterate_residual = sqrt(update_sq / dmax(x_norm_sq, 1.0e-30));
+    rep.absolute_residual = sqrt(dmax(dot(r, r, n), 0.0));
+    rep.relative_residual = rep.absolute_residual / dmax(rhs_norm, 1.0e-30);
+    /* push_back, then drop the oldest beyond keep_max */
+    memcpy(dirs[stored], d, (size_t)n * sizeof(double));
+    memcpy(adirs[stored], ad, (size_t)n * sizeof(double));
+    ++stored;
+    if (stored > keep_max) {
+      double *t0 = dirs[0], *t1 = adirs[0];
+      for (int h = 0; h < stored - 1; ++h) {
+        dirs[h] = dirs[h + 1];
+        adirs[h] = adirs[h + 1];
+      }
+      dirs[stored - 1] = t0;
+      adirs[stored - 1] = t1;
+      --stored;
+    }
+    if (rep.relative_residual < tol || rep.absolute_residual < tol) break;
+  }
+  for (int k = 0; k <= keep_max; ++k) {
+    free(dirs[k]);
+    free(adirs[k]);
+  }
+  free(dirs);
+  free(adirs);
+  if (err) fail(s, err);
+  return rep;
+}
+
+/* solve_pressure_correction_liu_split_dcdm_icpcg, pressure.cpp:367-468 (icc_preconditioned and identity
+ * directions; the neural direction needs an external worker) */
+static double pressure_dcdm(orc_solver *s) {
+  fld *pc = &s->f[ORC_F_P_CORR];
+  fld_fill(pc, 0.0);
+  bc_pressure(s, pc);
+  s->rep.pressure_iterations = 0;
+  const int n = s->cfg.nx * s->cfg.ny;
+  double *rhs = s->w[11], *x = s->w[12];
+  fld pe;
+  fld_init(&pe, s->cfg.nx, s->cfg.ny, s->cfg.ghost, 0.0);
+  split_extrapolation(s, &pe);
+  pressure_system(s, 1, split_rho_ref(s), &pe, rhs);
+  fld_free(&pe);
+  for (int k = 0; k < n; ++k) x[k] = 0.0;
+  if (!try_icc(&s->pm, &s->ppc)) fail(s, "ICC preconditioner construction failed");
+  const solve_rep rep = dcdm(s, &s->pm, &s->ppc, rhs, s->cfg.poisson_iterations, s->cfg.pressure_tolerance, x,
+                             !pressure_has_dirichlet(s));
+  s->rep.pressure_iterations = rep.iterations;
+  scatter_pressure(s, x);
+  if (!pressure_has_dirichlet(s)) subtract_mean(s, pc);
+  bc_pressure(s, pc);
+  return rep.relative_residual;
+}
+
 /* solve_pressure_correction_jacobi, pressure.cpp:250-300 */
 static double pressure_jacobi(orc_solver *s) {
   fld *pc = &s->f[ORC_F_P_CORR];
@@ -1736,6 +1880,7 @@ static double pressure_solve(orc_solver *s) {
   case ORC_P_ILDLT_PCG: return pressure_pcg(s, 0, 0);
   case ORC_P_SPLIT_ICPCG: return pressure_pcg(s, 1, 1);
   case ORC_P_SPLIT_ILDLT_PCG: return pressure_pcg(s, 1, 0);
+  case ORC_P_SPLIT_DCDM_ICPCG: return pressure_dcdm(s);
   case ORC_P_JACOBI: return pressure_jacobi(s);
   default: fail(s, "unsupported pressure scheme"); return 0.0;
   }

@@ -27,7 +27,8 @@ enum {
   ORC_P_ICPCG = 1,
   ORC_P_ILDLT_PCG = 2,
   ORC_P_SPLIT_ICPCG = 3,
-  ORC_P_SPLIT_ILDLT_PCG = 4
+  ORC_P_SPLIT_ILDLT_PCG = 4,
+  ORC_P_SPLIT_DCDM_ICPCG = 5
 };
 
 typedef struct {
@@ -56,6 +57,8 @@ typedef struct {
   double advect_u, advect_v, rotation_center_x, rotation_center_y, angular_velocity;
   double top_wall_velocity_x, bottom_wall_velocity_x;
   orc_bc p_bc[4], u_bc[4], v_bc[4]; /* indexed by ORC_LEFT..ORC_TOP */
+  int dcdm_direction_mode;           /* 0 icc_preconditioned, 1 identity (config.hpp:51) */
+  int dcdm_history_size, dcdm_max_stored_directions, dcdm_restart_interval; /* config.hpp:72-74 */
 } orc_config;
 
 /* Field identifiers (Solver members, solver.hpp:64-91). */

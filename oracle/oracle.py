@@ -34,7 +34,9 @@ PRESSURE = {
     "ildlt_pcg": 2,
     "split_icpcg": 3, "liu_split_icpcg": 3, "paper_split_icpcg": 3,
     "split_ildlt_pcg": 4, "liu_split_ildlt_pcg": 4, "paper_split_ildlt_pcg": 4,
+    "split_dcdm_icpcg": 5, "liu_split_dcdm_icpcg": 5, "paper_split_dcdm_icpcg": 5,
 }
+DCDM_DIRECTION = {"icc_preconditioned": 0, "icc": 0, "pcg_preconditioned": 0, "identity": 1}
 
 # struct Config defaults, config.hpp:35-136 (keys read by the time step).
 DEFAULTS = {
@@ -54,6 +56,8 @@ DEFAULTS = {
     "advect_u": 0.0, "advect_v": 0.0, "rotation_center_x": 0.5, "rotation_center_y": 0.5,
     "angular_velocity": 0.0, "top_wall_velocity_x": 0.0, "bottom_wall_velocity_x": 0.0,
     "periodic_x": True, "periodic_y": True, "invert_phase": False, "freeze_ch": False,
+    "dcdm_direction_mode": "icc_preconditioned", "dcdm_history_size": 2, "dcdm_max_stored_directions": 8,
+    "dcdm_restart_interval": 0,
 }
 for _f in ("pressure", "u", "v"):
     for _s in SIDES:
@@ -61,10 +65,11 @@ for _f in ("pressure", "u", "v"):
         DEFAULTS[f"{_f}_bc_{_s}_value"] = 0.0
 
 _INT_KEYS = {"nx", "ny", "ghost", "steps", "ch_inner_iterations", "momentum_iterations", "poisson_iterations",
-             "surface_tension_smoothing_passes"}
+             "surface_tension_smoothing_passes", "dcdm_history_size", "dcdm_max_stored_directions",
+             "dcdm_restart_interval"}
 _BOOL_KEYS = {"periodic_x", "periodic_y", "invert_phase", "freeze_ch"}
 _STR_KEYS = {"name", "mode", "ch_solver", "pressure_scheme", "phase_initializer", "velocity_profile",
-             "momentum_advection_scheme"}
+             "momentum_advection_scheme", "dcdm_direction_mode"}
 
 
 def _parse_bool(v: str) -> bool:
@@ -118,7 +123,8 @@ class Config(C.Structure):
         "interface_radius", "interface_amplitude", "interface_wavenumber", "zalesak_slot_width",
         "zalesak_slot_depth", "advect_u", "advect_v", "rotation_center_x", "rotation_center_y",
         "angular_velocity", "top_wall_velocity_x", "bottom_wall_velocity_x")] + [
-        ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4)]
+        ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4)] + [(n, C.c_int) for n in (
+        "dcdm_direction_mode", "dcdm_history_size", "dcdm_max_stored_directions", "dcdm_restart_interval")]
 
 
 class Report(C.Structure):
@@ -162,6 +168,11 @@ def to_struct(cfg: dict) -> Config:
             c.phase_initializer = 1 if cfg["phase_initializer"] == "zalesak_disk" else 0
         elif n == "velocity_profile":
             c.velocity_profile = 1 if cfg["velocity_profile"] == "solid_body_rotation" else 0
+        elif n == "dcdm_direction_mode":
+            mode = str(cfg["dcdm_direction_mode"]).lower()
+            if mode not in DCDM_DIRECTION:
+                raise ValueError(f"unsupported dcdm_direction_mode: {cfg['dcdm_direction_mode']}")
+            c.dcdm_direction_mode = DCDM_DIRECTION[mode]
         else:
             setattr(c, n, t(cfg[n]).value if t is C.c_double else int(cfg[n]))
     for f, attr in (("pressure", "p_bc"), ("u", "u_bc"), ("v", "v_bc")):

@@ -45,6 +45,7 @@ ding::Config to_config(const orc_config &c) {
   case ORC_P_ILDLT_PCG: cfg.pressure_scheme = "ildlt_pcg"; break;
   case ORC_P_SPLIT_ICPCG: cfg.pressure_scheme = "split_icpcg"; break;
   case ORC_P_SPLIT_ILDLT_PCG: cfg.pressure_scheme = "split_ildlt_pcg"; break;
+  case ORC_P_SPLIT_DCDM_ICPCG: cfg.pressure_scheme = "split_dcdm_icpcg"; break;
   default: cfg.pressure_scheme = "jacobi"; break;
   }
   cfg.phase_initializer = c.phase_initializer == 1 ? "zalesak_disk" : "default";
@@ -98,6 +99,11 @@ ding::Config to_config(const orc_config &c) {
   cfg.v_bc_right = to_spec(c.v_bc[ORC_RIGHT]);
   cfg.v_bc_bottom = to_spec(c.v_bc[ORC_BOTTOM]);
   cfg.v_bc_top = to_spec(c.v_bc[ORC_TOP]);
+  cfg.dcdm_direction_mode = c.dcdm_direction_mode == 1 ? "identity" : "icc_preconditioned";
+  cfg.dcdm_history_size = c.dcdm_history_size;
+  cfg.dcdm_max_stored_directions = c.dcdm_max_stored_directions;
+  cfg.dcdm_restart_interval = c.dcdm_restart_interval;
+  cfg.output_dir = "oracle/_ref/out";  // the dcdm backend creates its solver directory under the case output
   cfg.verbose = false;
   cfg.print_step_log = false;
   cfg.write_vtk = false;

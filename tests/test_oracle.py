@@ -100,6 +100,13 @@ CASES = {
     "freeze_ch": unit_config(freeze_ch=True, pressure_scheme="icpcg", surface_tension_multiplier=0.0),
     "single_phase": unit_config(mode="single_phase", pressure_scheme="icpcg", density_ratio=3.0),
     "jacobi": unit_config(nx=12, ny=12, pressure_scheme="jacobi", poisson_iterations=300, dt=1e-4),
+    "dcdm_walls": unit_config(nx=20, ny=28, periodic_x=False, periodic_y=False, pressure_scheme="split_dcdm_icpcg",
+                              body_force_y=-0.98, dt=1e-4),
+    "dcdm_periodic": unit_config(pressure_scheme="split_dcdm_icpcg"),
+    "dcdm_identity_dirichlet": unit_config(nx=18, ny=22, periodic_x=False, periodic_y=False,
+                                           pressure_scheme="split_dcdm_icpcg", dcdm_direction_mode="identity",
+                                           dcdm_history_size=0, dcdm_max_stored_directions=4,
+                                           pressure_bc_top_type="dirichlet", pressure_bc_top_value=0.3, dt=1e-4),
     "advection_only": unit_config(mode="advection_only", velocity_profile="solid_body_rotation",
                                   angular_velocity=2 * math.pi, phase_initializer="zalesak_disk",
                                   interface_radius=0.3),
