@@ -48,7 +48,8 @@ class Config(C.Structure):
         "zalesak_slot_depth", "advect_u", "advect_v", "rotation_center_x", "rotation_center_y",
         "angular_velocity", "top_wall_velocity_x", "bottom_wall_velocity_x")] + [
         ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4), ("precision", C.c_int),
-        ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int)]
+        ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int), ("dcdm_direction_mode", C.c_int),
+        ("dcdm_history_size", C.c_int), ("dcdm_max_stored_directions", C.c_int), ("dcdm_restart_interval", C.c_int)]
 
 
 class Report(C.Structure):

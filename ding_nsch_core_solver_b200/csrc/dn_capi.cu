@@ -407,6 +407,8 @@ struct dn_handle {
   int nsweep5 = 0;  // 31-line sweep warps of the staged wavefront
   // staged wavefront: hand-over lines, periodic-x wrap lines and launch shape
   double *bnd_f = nullptr, *bnd_b = nullptr, *wline0 = nullptr, *zlast = nullptr;
+  double *dcdm_dirs = nullptr, *dcdm_adirs = nullptr;  // split_dcdm_icpcg direction history, [keep][n] each
+  int dcdm_keep = 0;
   int sw5 = 0;                 // sweep warps per CTA, 0 = staged path unavailable
   int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3> (k_pcg<5,4> with periodic x)
   size_t sw5_warp_smem[2] = {0, 0};  // per sweep warp, [constant operator, variable operator]
@@ -437,7 +439,8 @@ bool solve_ch(const dn_config &c) {
 }
 bool compute_mu(const dn_config &c) { return c.mode != DN_MODE_ADVECTION_ONLY && c.mode != DN_MODE_SINGLE_PHASE; }
 bool use_split(const dn_config &c) {
-  return c.pressure_scheme == DN_P_SPLIT_ICPCG || c.pressure_scheme == DN_P_SPLIT_ILDLT_PCG;
+  return c.pressure_scheme == DN_P_SPLIT_ICPCG || c.pressure_scheme == DN_P_SPLIT_ILDLT_PCG ||
+         c.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG;
 }
 double rho_ref_of(const dn_config &c) { return std::min(1.0, c.density_ratio); }
 
@@ -575,10 +578,11 @@ dn_status dev_status_to_dn(dn_handle *h, int st) {
 }
 
 // ---- persistent PCG launch
+// The arguments and launch shape of the persistent PCG kernel k_pcg<S, SWEEP> (and of k_prec_apply, which
+// runs its sweeps alone).
 template <int S, int SWEEP>
-dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *dinv, int prec, int project, int max_it,
-                  double tol, double out[4]) {
-  PcgArgs P;
+dn_status pcg_launch_args(dn_handle *h, const double *a, const double *l, const double *dinv, int prec, int project,
+                          int max_it, double tol, PcgArgs &P, size_t &dyn_smem_out, int &blocks_out) {
   P.A = SpOp{a, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py};
   P.l = l;
   P.dinv = dinv;
@@ -660,9 +664,21 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
     blocks = std::min(blocks, h->sw5_blocks_max);
     if (blocks < sweep_ctas) return fail(h, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
   }
-  DN_TRY(reset_sync(h));
   if (SWEEP == 0 && (long long)blocks * (kBlock / 32) < h->nsweep)
     return fail(h, DN_ERR_UNSUPPORTED, "grid too wide for the co-resident wavefront warps");
+  dyn_smem_out = dyn_smem;
+  blocks_out = blocks;
+  return DN_OK;
+}
+
+template <int S, int SWEEP>
+dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *dinv, int prec, int project, int max_it,
+                  double tol, double out[4]) {
+  PcgArgs P;
+  size_t dyn_smem = 0;
+  int blocks = 1;
+  DN_TRY((pcg_launch_args<S, SWEEP>(h, a, l, dinv, prec, project, max_it, tol, P, dyn_smem, blocks)));
+  DN_TRY(reset_sync(h));
   void *args[] = {&P};
   cudaEventRecord(h->kev[0], h->stream);
   DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_pcg<S, SWEEP>, dim3(blocks), dim3(kBlock), args, dyn_smem,
@@ -1152,6 +1168,8 @@ dn_status split_extrapolation(dn_handle *h, int step) {
 
 // solve_pressure_correction_{icpcg,ildlt_pcg,liu_split_icpcg,liu_split_ildlt_pcg}, pressure.cpp:302-365, 470-491
 dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *rep);
+dn_status pressure_factor(dn_handle *h, bool split, bool icc);
+dn_status dcdm_solve(dn_handle *h, dn_report *rep);
 
 // x -= mean(x) for a compact vector of the n cells
 dn_status compact_subtract_mean(dn_handle *h, double *x) {
@@ -1162,6 +1180,17 @@ dn_status compact_subtract_mean(dn_handle *h, double *x) {
   DN_TRY(check_launch(h, "k_finish_mean"));
   k_vec_sub_scalar<<<blocks_for(h->n), 256, 0, h->stream>>>(x, h->n, h->scal);
   return check_launch(h, "k_vec_sub_scalar");
+}
+
+__global__ void k_spmv5(SpOp A, const double *x, double *y) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.n) return;
+  y[r] = spmv_row<5>(A, x, (int)(r / A.ny), (int)(r % A.ny));
+}
+__global__ void k_residual5(SpOp A, const double *b, const double *x, double *r) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.n) return;
+  r[t] = b[t] - spmv_row<5>(A, x, (int)(t / A.ny), (int)(t % A.ny));
 }
 
 // solve_pressure_correction_jacobi, pressure.cpp:250-300: the variable-coefficient system (as icpcg builds it,
@@ -1222,6 +1251,174 @@ dn_status pressure_jacobi(dn_handle *h, dn_report *rep) {
   LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], xb[its & 1], f[DN_F_P_CORR]);
   if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
   return bc(h, f[DN_F_P_CORR], kBCPressure);
+}
+
+// z = M^-1 in with the ICC factor of the pressure system (k_prec_apply); z lands in h->z.
+dn_status prec_apply(dn_handle *h, const double *in) {
+  PcgArgs P;
+  size_t dyn_smem = 0;
+  int blocks = 1;
+  const bool staged = h->sw5 > 0;
+  const void *kern;
+  if (staged && h->G.px) {
+    DN_TRY((pcg_launch_args<5, 4>(h, h->a5, h->l5, h->dinv5, kPrecICC, 0, 1, 0.0, P, dyn_smem, blocks)));
+    kern = (const void *)k_prec_apply<4>;
+  } else if (staged) {
+    DN_TRY((pcg_launch_args<5, 3>(h, h->a5, h->l5, h->dinv5, kPrecICC, 0, 1, 0.0, P, dyn_smem, blocks)));
+    kern = (const void *)k_prec_apply<3>;
+  } else {
+    DN_TRY((pcg_launch_args<5, 0>(h, h->a5, h->l5, h->dinv5, kPrecICC, 0, 1, 0.0, P, dyn_smem, blocks)));
+    kern = (const void *)k_prec_apply<0>;
+  }
+  P.r = const_cast<double *>(in);
+  P.s5.r = in;
+  DN_TRY(reset_sync(h));
+  void *args[] = {&P};
+  DN_CUDA(h, cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kBlock), args, dyn_smem, h->stream));
+  h->launches++;
+  int st = 0;
+  DN_TRY(read_status(h, &st));
+  return st == kDevOk ? DN_OK : dev_status_to_dn(h, st);
+}
+
+// Host sums of k_dots4's partials in block order: out[0..3] the four products, out[4] the non-finite count.
+dn_status dots4(dn_handle *h, const double *a0, const double *b0, const double *a1, const double *b1,
+                const double *a2, const double *b2, const double *a3, const double *b3, const double *f0,
+                const double *f1, double out[5]) {
+  const int nb = 128;
+  k_dots4<<<nb, 256, 0, h->stream>>>(a0, b0, a1, b1, a2, b2, a3, b3, f0, f1, h->n, h->partials);
+  DN_TRY(check_launch(h, "k_dots4"));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->partials, 5 * nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < 5; ++k) {
+    double v = 0.0;
+    for (int b = 0; b < nb; ++b) v += h->host_scal[k * nb + b];
+    out[k] = v;
+  }
+  return DN_OK;
+}
+
+// solve_dcdm_conjugate_directions (ch_sparse_krylov.hpp:662-837) on the assembled split system b, from
+// x = 0, directions from the ICC factor (or the identity), history in h->dcdm_dirs / dcdm_adirs.  Every
+// vector operation and its order follow the reference; the scalars come back to the host, which decides the
+// fallbacks as the reference does.
+dn_status dcdm_solve(dn_handle *h, dn_report *rep) {
+  const dn_config &cfg = h->cfg;
+  const long long n = h->n;
+  const int nb = blocks_for(n);
+  const double floor_ = 1.0e-30, tol = cfg.pressure_tolerance;
+  const bool project = !h->has_dirichlet;
+  const SpOp A{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  double *x = h->x, *r = h->r, *rh = h->p0, *z = h->z, *d = h->p1, *ad = h->ap, *delta = h->y;
+  auto proj = [&](double *v) -> dn_status { return project ? compact_subtract_mean(h, v) : DN_OK; };
+  auto copy = [&](double *dst, const double *src) -> dn_status {
+    DN_CUDA(h, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    return DN_OK;
+  };
+  DN_CUDA(h, cudaMemsetAsync(x, 0, n * sizeof(double), h->stream));
+  k_residual5<<<nb, 256, 0, h->stream>>>(A, h->b, x, r);
+  DN_TRY(check_launch(h, "k_residual5"));
+  DN_TRY(proj(r));
+  DN_TRY(proj(x));
+  double q[5];
+  DN_TRY(dots4(h, h->b, h->b, r, r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+  const double rhs_norm = std::sqrt(std::max(q[0], 0.0));
+  double absr = std::sqrt(std::max(q[1], 0.0));
+  double relr = absr / std::max(rhs_norm, 1.0e-30);
+  int its = 0;
+  rep->pressure_residual = relr;
+  if (relr < tol || absr < tol) {
+    rep->pressure_iterations = 0;
+    return DN_OK;
+  }
+  const int hist = cfg.dcdm_history_size, keep = h->dcdm_keep;
+  std::vector<int> slot;      // slot[k]: storage row of the k-th oldest stored direction
+  std::vector<double> den;    // d.Ad of each stored direction (the reference recomputes the same value)
+  const int limit = std::max(1, cfg.poisson_iterations);
+  for (int it = 0; it < limit; ++it) {
+    if (cfg.dcdm_restart_interval > 0 && it > 0 && it % cfg.dcdm_restart_interval == 0) {
+      slot.clear();
+      den.clear();
+    }
+    DN_TRY(dots4(h, r, r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+    const double rnorm = std::sqrt(std::max(q[0], 0.0));
+    if (rnorm < tol) break;
+    k_div_scalar<<<nb, 256, 0, h->stream>>>(r, rh, n, std::max(rnorm, floor_));
+    DN_TRY(check_launch(h, "k_div_scalar"));
+    if (cfg.dcdm_direction_mode == 1) {
+      DN_TRY(copy(z, rh));
+    } else {
+      DN_TRY(prec_apply(h, rh));
+    }
+    DN_TRY(dots4(h, z, z, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, z, nullptr, q));
+    if (q[4] != 0.0 || std::sqrt(std::max(q[0], 0.0)) < floor_) DN_TRY(copy(z, r));
+    DN_TRY(proj(z));
+    DN_TRY(dots4(h, z, z, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, z, nullptr, q));
+    if (q[4] != 0.0 || std::sqrt(std::max(q[0], 0.0)) < floor_) {
+      DN_TRY(copy(z, r));
+      DN_TRY(proj(z));
+    }
+    DN_TRY(copy(d, z));
+    const int stored = (int)slot.size();
+    const int begin = (hist > 0 && stored > hist) ? stored - hist : 0;
+    for (int k = begin; k < stored; ++k) {
+      if (!std::isfinite(den[(size_t)k]) || std::fabs(den[(size_t)k]) < floor_) continue;
+      const double *dir = h->dcdm_dirs + (size_t)slot[(size_t)k] * n;
+      const double *adir = h->dcdm_adirs + (size_t)slot[(size_t)k] * n;
+      DN_TRY(dots4(h, d, adir, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+      k_sub_scaled<<<nb, 256, 0, h->stream>>>(d, dir, n, q[0] / den[(size_t)k]);
+      DN_TRY(check_launch(h, "k_sub_scaled"));
+    }
+    DN_TRY(proj(d));
+    k_spmv5<<<nb, 256, 0, h->stream>>>(A, d, ad);
+    DN_TRY(check_launch(h, "k_spmv5"));
+    DN_TRY(dots4(h, r, d, d, ad, d, d, nullptr, nullptr, d, ad, q));
+    double rd = q[0], dad = q[1];
+    if (q[4] != 0.0 || std::sqrt(std::max(q[2], 0.0)) < floor_ || !std::isfinite(rd) || rd <= 0.0 ||
+        !std::isfinite(dad) || std::fabs(dad) < floor_) {
+      DN_TRY(copy(d, r));
+      DN_TRY(proj(d));
+      k_spmv5<<<nb, 256, 0, h->stream>>>(A, d, ad);
+      DN_TRY(check_launch(h, "k_spmv5"));
+      DN_TRY(dots4(h, r, d, d, ad, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+      rd = q[0];
+      dad = q[1];
+      if (!std::isfinite(rd) || rd <= 0.0 || !std::isfinite(dad) || std::fabs(dad) < floor_)
+        return fail(h, DN_ERR_PCG_BREAKDOWN, "dcdm breakdown: invalid fallback direction");
+    }
+    const double alpha = rd / dad;
+    k_x_step<<<nb, 256, 0, h->stream>>>(x, d, delta, n, alpha);
+    DN_TRY(check_launch(h, "k_x_step"));
+    DN_TRY(dots4(h, delta, delta, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+    const double update_sq = q[0];
+    DN_TRY(proj(x));
+    k_residual5<<<nb, 256, 0, h->stream>>>(A, h->b, x, r);
+    DN_TRY(check_launch(h, "k_residual5"));
+    DN_TRY(proj(r));
+    DN_TRY(dots4(h, x, x, r, r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+    its = it + 1;
+    absr = std::sqrt(std::max(q[1], 0.0));
+    relr = absr / std::max(rhs_norm, 1.0e-30);
+    (void)update_sq;
+    // push_back, dropping the oldest beyond `keep`
+    int row;
+    if ((int)slot.size() < keep) {
+      row = (int)slot.size();
+    } else {
+      row = slot.front();
+      slot.erase(slot.begin());
+      den.erase(den.begin());
+    }
+    DN_TRY(copy(h->dcdm_dirs + (size_t)row * n, d));
+    DN_TRY(copy(h->dcdm_adirs + (size_t)row * n, ad));
+    slot.push_back(row);
+    den.push_back(dad);
+    if (relr < tol || absr < tol) break;
+  }
+  rep->pressure_iterations = its;
+  rep->pressure_residual = relr;
+  h->phase_ms[7] = its;
+  return DN_OK;
 }
 
 // The CH advective term rhs = -div(u c) of `c` (its scalar BC ghosts refilled first) into h->arhs.
@@ -1289,7 +1486,12 @@ dn_status pressure(dn_handle *h, int step, dn_report *rep) {
                                                        h->pe, split ? 1 : 0, rho_ref, cfg.dt, h->a5, h->b);
   DN_TRY(check_launch(h, "k_p_assemble"));
   if (!h->has_dirichlet) DN_TRY(compact_subtract_mean(h, h->b));  // pressure.cpp:198-212
-  DN_TRY(pressure_factor_solve(h, split, icc, rep));
+  if (cfg.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG) {
+    DN_TRY(pressure_factor(h, true, true));  // build_icc_preconditioner_strict
+    DN_TRY(dcdm_solve(h, rep));
+  } else {
+    DN_TRY(pressure_factor_solve(h, split, icc, rep));
+  }
   LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], h->x, f[DN_F_P_CORR]);
   if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
   return bc(h, f[DN_F_P_CORR], kBCPressure);
@@ -1298,8 +1500,7 @@ dn_status pressure(dn_handle *h, int step, dn_report *rep) {
 // x = A^-1 b for the assembled pressure operator a5 and right-hand side b, from x = 0: the factor (built
 // once for the constant split operator, every call for the variable one), then the PCG of the configured
 // precision and sweep form.
-dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *rep) {
-  const dn_config &cfg = h->cfg;
+dn_status pressure_factor(dn_handle *h, bool split, bool icc) {
   const int kind = icc ? kPrecICC : kPrecLDLT;
   if (!(split && h->p_factor_valid && h->p_factor_kind == kind)) {
     DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
@@ -1317,6 +1518,13 @@ dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *r
     h->p_factor_valid = split;
     h->p_factor_kind = kind;
   }
+  return DN_OK;
+}
+
+dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *rep) {
+  const dn_config &cfg = h->cfg;
+  const int kind = icc ? kPrecICC : kPrecLDLT;
+  DN_TRY(pressure_factor(h, split, icc));
   DN_CUDA(h, cudaMemsetAsync(h->x, 0, h->n * sizeof(double), h->stream));
   double out[4];
   rep->refinement_cycles = 0;
@@ -1562,6 +1770,19 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k53, kBlock, dyn);
       h->sw5_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * h->num_sms);
       if (h->sw5_blocks_max == 0) h->sw5 = 0;
+    }
+  }
+  if (c.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG) {
+    // the direction history, and the preconditioner-only kernel's shared-memory limit (as k_pcg's)
+    h->dcdm_keep = std::max(c.dcdm_max_stored_directions, std::max(c.dcdm_history_size, 1));
+    A(dalloc(h, &h->dcdm_dirs, (size_t)h->dcdm_keep * h->n));
+    A(dalloc(h, &h->dcdm_adirs, (size_t)h->dcdm_keep * h->n));
+    if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+    const int optin = h->smem_optin;
+    for (const void *k : {(const void *)k_prec_apply<3>, (const void *)k_prec_apply<4>}) {
+      cudaFuncAttributes fa{};
+      cudaFuncGetAttributes(&fa, k);
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
     }
   }
   if (c.precision == DN_PRECISION_MIXED) {
@@ -2111,7 +2332,8 @@ dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const 
   DN_CUDA(h, cudaMemsetAsync(ap, 0, P.size() * sizeof(double), h->stream));
   DN_CUDA(h, cudaMemsetAsync(app, 0, P.size() * sizeof(double), h->stream));
   const bool split = use_split(cfg);
-  const bool icc = cfg.pressure_scheme == DN_P_ICPCG || cfg.pressure_scheme == DN_P_SPLIT_ICPCG;
+  const bool icc = cfg.pressure_scheme == DN_P_ICPCG || cfg.pressure_scheme == DN_P_SPLIT_ICPCG ||
+                   cfg.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG;
   const double rho_ref = split ? rho_ref_of(cfg) : 1.0;
   // face cotangents through the BCs; u* and v* take them unchanged (u = u* - ...)
   LAUNCH_INTERIOR(k_adj_fold_u, AU, GU, AU, h->G, h->bc);
@@ -2511,6 +2733,9 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   if (c.pressure_scheme == DN_P_JACOBI)
     return static_fail(err, err_len, DN_ERR_UNSUPPORTED,
                        "pressure_scheme jacobi is not implemented by the CUDA backend");
+  if (c.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG)
+    return static_fail(err, err_len, DN_ERR_UNSUPPORTED,
+                       "pressure_scheme split_dcdm_icpcg keeps a direction history and needs a handle");
   if (c.pressure_scheme < DN_P_ICPCG || c.pressure_scheme > DN_P_SPLIT_ILDLT_PCG)
     return static_fail(err, err_len, DN_ERR_CONFIG, "unknown pressure_scheme %d", c.pressure_scheme);
   if (c.precision != DN_PRECISION_FP64)

@@ -56,6 +56,10 @@ int parse_pressure_scheme(const std::string &v) {
       {"liu_split_ildlt_pcg", DN_P_SPLIT_ILDLT_PCG},
       {"paper_split_ildlt_pcg", DN_P_SPLIT_ILDLT_PCG},
       {"cuda_split_ildlt_pcg", DN_P_SPLIT_ILDLT_PCG},
+      {"split_dcdm_icpcg", DN_P_SPLIT_DCDM_ICPCG},
+      {"liu_split_dcdm_icpcg", DN_P_SPLIT_DCDM_ICPCG},
+      {"paper_split_dcdm_icpcg", DN_P_SPLIT_DCDM_ICPCG},
+      {"cuda_split_dcdm_icpcg", DN_P_SPLIT_DCDM_ICPCG},
   };
   auto it = m.find(v);
   if (it == m.end()) throw std::runtime_error("unsupported pressure scheme: " + v);
@@ -100,6 +104,10 @@ extern "C" void dn_config_default(dn_config *c) {
   c->precision = DN_PRECISION_FP64;
   c->mixed_inner_tolerance = 1.0e-5;
   c->device_share = 1;
+  c->dcdm_direction_mode = 0;  // icc_preconditioned
+  c->dcdm_history_size = 2;
+  c->dcdm_max_stored_directions = 8;
+  c->dcdm_restart_interval = 0;
 }
 
 extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err, size_t err_len) {
@@ -204,6 +212,20 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
     getd("bottom_wall_velocity_x", cfg->bottom_wall_velocity_x);
     getd("mixed_inner_tolerance", cfg->mixed_inner_tolerance);
     geti("device_share", cfg->device_share);
+    geti("dcdm_history_size", cfg->dcdm_history_size);
+    geti("dcdm_max_stored_directions", cfg->dcdm_max_stored_directions);
+    geti("dcdm_restart_interval", cfg->dcdm_restart_interval);
+    if (kv.count("dcdm_direction_mode")) {  // pressure.cpp:383-395
+      const std::string m = lower(kv["dcdm_direction_mode"]);
+      if (m == "identity")
+        cfg->dcdm_direction_mode = 1;
+      else if (m == "icc" || m == "icc_preconditioned" || m == "pcg_preconditioned")
+        cfg->dcdm_direction_mode = 0;
+      else if (m == "neural" || m == "hydea_neural" || m == "ml")
+        throw std::runtime_error("dcdm neural directions need the HyDEA worker, which the CUDA backend does not run");
+      else
+        throw std::runtime_error("unsupported dcdm_direction_mode: " + kv["dcdm_direction_mode"]);
+    }
     if (cfg->device_share < 1) throw std::runtime_error("device_share must be at least 1");
     static const char *sides[4] = {"left", "right", "bottom", "top"};
     for (int s = 0; s < 4; ++s) {

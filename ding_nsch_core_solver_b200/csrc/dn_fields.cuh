@@ -503,6 +503,41 @@ __global__ void k_diff_l2_partials(Fv a, Fv b, double *partials) {
     partials[gridDim.x + blockIdx.x] = v[1];
   }
 }
+// Per-block partial sums of up to four products sum a_k b_k (a null a_k contributes 0) and the number of
+// non-finite values in f0 and f1 (null: none), [5][gridDim.x]; the caller adds the blocks in order.
+__global__ void k_dots4(const double *a0, const double *b0, const double *a1, const double *b1, const double *a2,
+                        const double *b2, const double *a3, const double *b3, const double *f0, const double *f1,
+                        long long n, double *partials) {
+  __shared__ double sh[8 * 32 * 5];
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    if (a0) v[0] += a0[t] * b0[t];
+    if (a1) v[1] += a1[t] * b1[t];
+    if (a2) v[2] += a2[t] * b2[t];
+    if (a3) v[3] += a3[t] * b3[t];
+    if (f0 && !isfinite(f0[t])) v[4] += 1.0;
+    if (f1 && !isfinite(f1[t])) v[4] += 1.0;
+  }
+  block_sum<5>(v, sh);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 5; ++k) partials[(size_t)k * gridDim.x + blockIdx.x] = v[k];
+}
+__global__ void k_div_scalar(const double *in, double *out, long long n, double d) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = in[t] / d;
+}
+__global__ void k_sub_scaled(double *y, const double *x, long long n, double a) {  // y -= a x
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) y[t] -= a * x[t];
+}
+__global__ void k_x_step(double *x, const double *d, double *delta, long long n, double alpha) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) {
+    const double dl = alpha * d[t];
+    x[t] += dl;
+    delta[t] = dl;
+  }
+}
 __global__ void k_vec_sum(const double *x, long long n, double *partials) {
   __shared__ double sh[8 * 32];
   double v[1] = {0.0};

@@ -1077,4 +1077,81 @@ __global__ void k_residual_partials(SpOp A, const double *b, const double *x, do
   }
 }
 
+// One application z = M^-1 r of the 5-point ICC/ILDLT preconditioner (apply_preconditioner,
+// ch_sparse_krylov.hpp:444-513) on its own, for solvers that need the direction but not the CG recurrence
+// (the conjugate-directions backend): the same sweeps as k_pcg<5, SWEEP> (the staged wavefront, with the
+// periodic-x wrap for SWEEP 4, or the global-memory wavefront for SWEEP 0) on P.r / P.s5.r, m_r = 0.
+// P.out[0..2] receive sum z, r.z and sum r.
+template <int SWEEP>
+__global__ void __launch_bounds__(kBlock) k_prec_apply(PcgArgs P) {
+  __shared__ double sh[8 * 32 + 8];
+  extern __shared__ __align__(16) char dsm[];
+  const GridBarrier bar{P.bar_count, P.bar_gen, P.status, gridDim.x};
+  int parity = 0;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps_cta = blockDim.x >> 5;
+  unsigned int *cnt_cta = (unsigned int *)dsm;
+  if (SWEEP == 3 || SWEEP == 4) {
+    if (threadIdx.x < 16) cnt_cta[threadIdx.x] = 0u;
+    const size_t nb = 2 * (size_t)P.s5.nsweep * P.s5.ny;
+    const double empty = hand_empty_value<double>();
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
+      P.s5.bnd_f[t] = empty;
+      P.s5.bnd_b[t] = empty;
+    }
+    if (SWEEP == 4)
+      for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * (size_t)P.s5.ny;
+           t += (size_t)gridDim.x * blockDim.x) {
+        P.s5.wline0[t] = empty;
+        P.s5.zlast[t] = empty;
+      }
+    const int na = P.s5.varcoef ? 4 : 2;
+    const size_t lines = 2 * (size_t)((P.s5.ny + 3) & ~3);
+    for (int w = 0; w < P.s5.sw; ++w) {
+      double *line = (double *)(dsm + 64 + (size_t)w * P.warp_smem) + sweep_hand_line(na);
+      for (size_t t = threadIdx.x; t < lines; t += blockDim.x) line[t] = empty;
+    }
+    __syncthreads();
+  }
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (!grid_sum<3>(acc, P.partials, parity, sh, bar)) return;  // orders the set-up before any sweep
+  acc[0] = acc[1] = acc[2] = 0.0;
+  const unsigned int epoch = 1;
+  if (SWEEP == 0) {
+    for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta)
+      fwd5(P, k, epoch, 0.0);
+    for (int k = blockIdx.x + (int)gridDim.x * warp; k < P.nsweep; k += (int)gridDim.x * nwarps_cta)
+      bwd5(P, k, epoch, 0.0, acc);
+  } else {
+    constexpr bool PX = SWEEP == 4;
+    const int k = blockIdx.x * P.s5.sw + warp;
+    if (warp < P.s5.sw && k < P.s5.nsweep) {
+      char *mine = dsm + 64 + (size_t)warp * P.warp_smem;
+      if (P.prec == kPrecICC) {
+        if (P.s5.varcoef) {
+          fwd5_staged<true, true, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, 0.0, acc);
+          bwd5_staged<true, true, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+        } else {
+          fwd5_staged<true, false, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, 0.0, acc);
+          bwd5_staged<true, false, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+        }
+      } else {
+        if (P.s5.varcoef) {
+          fwd5_staged<false, true, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, 0.0, acc);
+          bwd5_staged<false, true, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+        } else {
+          fwd5_staged<false, false, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, 0.0, acc);
+          bwd5_staged<false, false, double, PX>(P.s5, mine, cnt_cta, k, warp, epoch, acc);
+        }
+      }
+    }
+  }
+  if (!grid_sum<3>(acc, P.partials, parity, sh, bar)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.out[0] = acc[0];
+    P.out[1] = acc[1];
+    P.out[2] = acc[2];
+  }
+}
+
 }  // namespace dn

@@ -45,7 +45,8 @@ typedef enum {
   DN_P_ICPCG = 1,
   DN_P_ILDLT_PCG = 2,
   DN_P_SPLIT_ICPCG = 3,
-  DN_P_SPLIT_ILDLT_PCG = 4
+  DN_P_SPLIT_ILDLT_PCG = 4,
+  DN_P_SPLIT_DCDM_ICPCG = 5 /* conjugate directions (pressure.cpp:367-468) */
 } dn_pressure_scheme;
 /* arithmetic of the Krylov inner loops: plain FP64, or FP32 inner solves wrapped in FP64 defect correction */
 typedef enum { DN_PRECISION_FP64 = 0, DN_PRECISION_MIXED = 1 } dn_precision;
@@ -81,6 +82,8 @@ typedef struct {
   int device_share;                /* handles meant to run concurrently on one device (dn_step_batch): each
                                       persistent launch takes at most 1/device_share of the SMs, never fewer
                                       CTAs than its wavefront needs; 1 = the whole device */
+  int dcdm_direction_mode;         /* split_dcdm_icpcg directions: 0 icc_preconditioned, 1 identity (config.hpp:51) */
+  int dcdm_history_size, dcdm_max_stored_directions, dcdm_restart_interval; /* config.hpp:72-74 */
 } dn_config;
 
 /* Fields (Solver members, src/core/coupled/solver.hpp:64-91). */

@@ -71,6 +71,13 @@ CASES = {
     "jacobi_walls": unit(nx=12, ny=12, periodic_x=False, periodic_y=False, pressure_scheme="jacobi",
                          poisson_iterations=300, dt=1e-4),
     "jacobi_periodic": unit(pressure_scheme="jacobi", poisson_iterations=300, dt=1e-4),
+    # conjugate directions with a direction history (pressure.cpp:367-468, ch_sparse_krylov.hpp:662-837)
+    "dcdm_walls": unit(nx=40, ny=56, periodic_x=False, periodic_y=False, pressure_scheme="split_dcdm_icpcg",
+                       body_force_y=-0.98, dt=1e-4),
+    "dcdm_periodic": unit(pressure_scheme="split_dcdm_icpcg"),
+    "dcdm_channel_x_identity": unit(nx=48, ny=32, periodic_x=True, periodic_y=False, pressure_scheme="split_dcdm_icpcg",
+                                    dcdm_direction_mode="identity", dcdm_history_size=0, dcdm_max_stored_directions=4,
+                                    top_wall_velocity_x=0.5, bottom_wall_velocity_x=-0.5, dt=1e-4),
     # advection only: SSPRK3 + WENO5 of the Zalesak disk in solid-body rotation (phase_field.cpp:398-435)
     "advection_only_zalesak": unit(mode="advection_only", velocity_profile="solid_body_rotation",
                                    angular_velocity=2 * math.pi, phase_initializer="zalesak_disk",
