@@ -117,6 +117,8 @@ def load():
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_advection": (I, [H, VP, VP, VP, VP]),
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
+        "dn_history_csv_header": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+        "dn_history_csv_row": (I, [H, I, D, C.POINTER(Report), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "dn_write_restart": (I, [H, I, C.c_char_p]),
         "dn_load_restart": (I, [H, C.c_char_p, C.POINTER(C.c_int)]),
         "dn_explicit_operator": (I, [H, VP, VP, VP, VP]),
@@ -278,6 +280,13 @@ class Solver:
         return out, its.value, rel.value
 
     # ---- diagnostics / timing
+    def history_csv_row(self, step: int, time: float, report: dict) -> str:
+        """Solver::append_history_csv_entry: the history.csv row of the step whose report is `report`."""
+        r = Report(**{n: report[n] for n, _ in Report._fields_})
+        buf = C.create_string_buffer(2048)
+        self._check(self._lib.dn_history_csv_row(self._h, int(step), float(time), C.byref(r), buf, len(buf), None))
+        return buf.value.decode()
+
     def write_restart(self, path: str, step: int) -> None:
         """Solver::write_restart_snapshot: the reference's v2 snapshot of this solver's state."""
         self._check(self._lib.dn_write_restart(self._h, int(step), str(path).encode()))
@@ -333,3 +342,12 @@ def step_batch(solvers, steps) -> list:
         msgs = [lib.dn_last_error(s._h).decode() for s in solvers]
         raise DnError(code, "; ".join(m for m in msgs if m))
     return [{f: getattr(r, f) for f, _ in Report._fields_} for r in reps]
+
+
+def history_csv_header() -> str:
+    """Solver::write_history_csv_header: the history.csv header line."""
+    lib = load()
+    buf = C.create_string_buffer(1024)
+    lib.dn_history_csv_header(buf, len(buf))
+    return buf.value.decode()
+

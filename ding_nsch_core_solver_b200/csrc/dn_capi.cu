@@ -2137,6 +2137,85 @@ dn_status dn_load_restart(dn_handle *h, const char *path, int *step) {
   return DN_OK;
 }
 
+// ---- history.csv (Solver::write_history_csv_header / append_history_csv_entry, io.cpp:179-206) ----
+namespace {
+const char kHistoryHeader[] =
+    "step,time,mass,mass_drift,divergence_l2,max_divergence,max_abs_mu,max_velocity,kinetic_energy,"
+    "total_free_energy,ch_inner_residual,ch_equation_residual,coupling_residual,pressure_correction_residual,"
+    "momentum_residual,boundary_speed_pre_correction,boundary_speed_post_correction,rho_min,rho_max,eta_min,"
+    "eta_max,dt_limit_advective,dt_limit_capillary,dt_limit_ch_explicit,dt_limit_active,dt_limit_ratio,"
+    "ch_iterations,coupling_iterations,pressure_iterations,momentum_iterations,"
+    "ch_solver_name,momentum_solver_name,pressure_solver_name,dt_limit_source\n";
+
+const char *pressure_solver_label(int scheme) {  // pressure.cpp:1031-1071
+  switch (scheme) {
+  case DN_P_SPLIT_ICPCG: return "SplitICCPCG";
+  case DN_P_SPLIT_DCDM_ICPCG: return "SplitDCDMICC";
+  case DN_P_SPLIT_ILDLT_PCG: return "SplitILDLTPCG";
+  case DN_P_ICPCG: return "ICCPCG";
+  case DN_P_ILDLT_PCG: return "ILDLTPCG";
+  default: return "Jacobi";
+  }
+}
+const char *ch_solver_label(const dn_config &c, int prec) {  // phase_field.cpp:20-28, 277, 464-470; solver.cpp:244
+  if (c.mode == DN_MODE_ADVECTION_ONLY) return "PureAdvectionSSPRK3[WENO5]";
+  switch (prec) {
+  case 1: return "SparsePCG[ILDLT]";
+  case 0: return "SparsePCG[Diagonal]";
+  case 2: return "SparsePCG[DiagonalFallback]";
+  default: return "NotUsed";
+  }
+}
+}  // namespace
+
+size_t dn_history_csv_header(char *buf, size_t len) {
+  const size_t n = sizeof(kHistoryHeader) - 1;
+  if (buf && len > 0) {
+    const size_t m = std::min(n, len - 1);
+    std::memcpy(buf, kHistoryHeader, m);
+    buf[m] = '\0';
+  }
+  return n;
+}
+
+dn_status dn_history_csv_row(dn_handle *h, int step, double time, const dn_report *rep, char *buf, size_t len,
+                             size_t *written) {
+  if (!h || !rep || !buf || len == 0) return DN_ERR_INVALID_ARGUMENT;
+  dn_diag d{};
+  DN_TRY(dn_diagnostics(h, &d));
+  const dn_config &c = h->cfg;
+  const bool adv = c.mode == DN_MODE_ADVECTION_ONLY;
+  // populate_timestep_limits, diagnostics.cpp:96-110
+  const char *source = "advective";
+  double active = d.dt_limit_advective;
+  if (d.dt_limit_capillary < active) {
+    active = d.dt_limit_capillary;
+    source = "capillary";
+  }
+  if (d.dt_limit_ch_explicit < active) {
+    active = d.dt_limit_ch_explicit;
+    source = "ch_explicit";
+  }
+  if (!std::isfinite(active) || active <= 1.0e-30) source = "unbounded";
+  const int n = std::snprintf(
+      buf, len,
+      "%d,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,"
+      "%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%d,%d,%d,%d,%s,%s,%s,%s\n",
+      step, time, d.mass, d.mass_drift, d.divergence_l2, d.max_divergence, d.max_abs_mu, d.max_velocity,
+      d.kinetic_energy, d.total_free_energy, rep->ch_residual, adv ? 0.0 : rep->ch_equation_residual, 0.0,
+      adv ? 0.0 : rep->pressure_residual, adv ? 0.0 : rep->momentum_residual, rep->boundary_speed_pre,
+      rep->boundary_speed_post, d.rho_min, d.rho_max, d.eta_min, d.eta_max, d.dt_limit_advective,
+      d.dt_limit_capillary, d.dt_limit_ch_explicit, d.dt_limit_active, d.dt_limit_ratio, rep->ch_iterations,
+      rep->coupling_iterations, rep->pressure_iterations, rep->momentum_iterations,
+      ch_solver_label(c, rep->ch_preconditioner),
+      adv ? "NotUsed" : "ExplicitConvection+MonolithicImplicitViscosityBiCGSTAB[Diagonal]",
+      adv ? "NotUsed" : pressure_solver_label(c.pressure_scheme), source);
+  if (n < 0) return fail(h, DN_ERR_INVALID_ARGUMENT, "history row formatting failed");
+  if (written) *written = (size_t)n;
+  if ((size_t)n >= len) return fail(h, DN_ERR_INVALID_ARGUMENT, "history row buffer too small");
+  return DN_OK;
+}
+
 dn_status dn_begin_step(dn_handle *h, int step) {
   if (!h) return DN_ERR_INVALID_ARGUMENT;
   h->step = step;

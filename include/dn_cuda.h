@@ -233,6 +233,15 @@ dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, c
 dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
                                        const double *gE, double *c_bar, double *u_bar, double *v_bar);
 
+/* ---- history.csv --------------------------------------------------------------------------------------- */
+/* Solver::write_history_csv_header (io.cpp:179-185): the header line; returns its length (buf may be NULL). */
+size_t dn_history_csv_header(char *buf, size_t len);
+/* Solver::append_history_csv_entry (io.cpp:187-202): the history row of the step just taken (its report
+ * `rep`, the device diagnostics, the solver names and the dt-limit source), doubles at 17 significant
+ * digits, newline-terminated, into buf (len bytes); *written (may be NULL) receives its length. */
+dn_status dn_history_csv_row(dn_handle *h, int step, double time, const dn_report *rep, char *buf, size_t len,
+                             size_t *written);
+
 /* ---- restart snapshots --------------------------------------------------------------------------------- */
 /* Solver::write_restart_snapshot (io.cpp:271-343): the reference's v2 snapshot of the handle's state (the
  * restart fields, initial mass, grid, physics scalars and boundary specs) at `path`, written to path.tmp and
