@@ -117,6 +117,8 @@ def load():
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_advection": (I, [H, VP, VP, VP, VP]),
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
+        "dn_set_pressure_monitor": (I, [H, I]),
+        "dn_pressure_monitor": (I, [H, DP, I, C.POINTER(C.c_int)]),
         "dn_history_csv_header": (C.c_size_t, [C.c_char_p, C.c_size_t]),
         "dn_history_csv_row": (I, [H, I, D, C.POINTER(Report), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "dn_write_restart": (I, [H, I, C.c_char_p]),
@@ -280,6 +282,17 @@ class Solver:
         return out, its.value, rel.value
 
     # ---- diagnostics / timing
+    def set_pressure_monitor(self, capacity: int) -> None:
+        """Record up to `capacity` iterations of every later FP64 pressure solve (the CG monitor)."""
+        self._check(self._lib.dn_set_pressure_monitor(self._h, int(capacity)))
+
+    def pressure_monitor(self, capacity: int = 100000) -> np.ndarray:
+        """The last pressure solve's record, one row per iteration: abs, rel, iterate residual, alpha."""
+        out = np.zeros((capacity, 4))
+        cnt = C.c_int()
+        self._check(self._lib.dn_pressure_monitor(self._h, _dp(out), capacity, C.byref(cnt)))
+        return out[:min(cnt.value, capacity)].copy()
+
     def history_csv_row(self, step: int, time: float, report: dict) -> str:
         """Solver::append_history_csv_entry: the history.csv row of the step whose report is `report`."""
         r = Report(**{n: report[n] for n, _ in Report._fields_})

@@ -408,6 +408,9 @@ struct dn_handle {
   // staged wavefront: hand-over lines, periodic-x wrap lines and launch shape
   double *bnd_f = nullptr, *bnd_b = nullptr, *wline0 = nullptr, *zlast = nullptr;
   double *dcdm_dirs = nullptr, *dcdm_adirs = nullptr;  // split_dcdm_icpcg direction history, [keep][n] each
+  double *mon = nullptr;  // pressure-solve monitor record [mon_cap][4] (dn_set_pressure_monitor), device
+  int mon_cap = 0, mon_count = 0;
+  std::vector<double> mon_host;  // the same record for the host-driven solvers
   int dcdm_keep = 0;
   int sw5 = 0;                 // sweep warps per CTA, 0 = staged path unavailable
   int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3> (k_pcg<5,4> with periodic x)
@@ -611,6 +614,8 @@ dn_status pcg_launch_args(dn_handle *h, const double *a, const double *l, const 
   P.rows13 = Rows13{};
   size_t dyn_smem = 0;
   P.seq_lines = 0;
+  P.mon = S == 5 ? h->mon : nullptr;
+  P.mon_cap = S == 5 ? h->mon_cap : 0;
   if (S == 13 && SWEEP == 1 && h->rows13.lval != nullptr) {  // ring of kLvlRing levels x nx doubles
     P.rows13 = h->rows13;
     dyn_smem = (size_t)kLvlRing * h->G.nx * sizeof(double);
@@ -674,7 +679,7 @@ dn_status pcg_launch_args(dn_handle *h, const double *a, const double *l, const 
 template <int S, int SWEEP>
 dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *dinv, int prec, int project, int max_it,
                   double tol, double out[4]) {
-  PcgArgs P;
+  PcgArgs P{};
   size_t dyn_smem = 0;
   int blocks = 1;
   DN_TRY((pcg_launch_args<S, SWEEP>(h, a, l, dinv, prec, project, max_it, tol, P, dyn_smem, blocks)));
@@ -705,6 +710,8 @@ dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *
 // One FP32 inner PCG solve (the persistent kernel instantiated for float) on the handle's FP32 buffers.
 dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol, double out[4]) {
   PcgArgsT<float> P{};
+  P.mon = nullptr;
+  P.mon_cap = 0;
   P.A = SpOpT<float>{h->fa5, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py};
   P.l = h->fl5;
   P.dinv = h->fdinv5;
@@ -1255,7 +1262,7 @@ dn_status pressure_jacobi(dn_handle *h, dn_report *rep) {
 
 // z = M^-1 in with the ICC factor of the pressure system (k_prec_apply); z lands in h->z.
 dn_status prec_apply(dn_handle *h, const double *in) {
-  PcgArgs P;
+  PcgArgs P{};
   size_t dyn_smem = 0;
   int blocks = 1;
   const bool staged = h->sw5 > 0;
@@ -1332,6 +1339,7 @@ dn_status dcdm_solve(dn_handle *h, dn_report *rep) {
     return DN_OK;
   }
   const int hist = cfg.dcdm_history_size, keep = h->dcdm_keep;
+  h->mon_host.clear();
   std::vector<int> slot;      // slot[k]: storage row of the k-th oldest stored direction
   std::vector<double> den;    // d.Ad of each stored direction (the reference recomputes the same value)
   const int limit = std::max(1, cfg.poisson_iterations);
@@ -1399,7 +1407,10 @@ dn_status dcdm_solve(dn_handle *h, dn_report *rep) {
     its = it + 1;
     absr = std::sqrt(std::max(q[1], 0.0));
     relr = absr / std::max(rhs_norm, 1.0e-30);
-    (void)update_sq;
+    if (it < h->mon_cap) {
+      const double rec[4] = {absr, relr, std::sqrt(update_sq / std::max(q[0], 1.0e-30)), alpha};
+      h->mon_host.insert(h->mon_host.end(), rec, rec + 4);
+    }
     // push_back, dropping the oldest beyond `keep`
     int row;
     if ((int)slot.size() < keep) {
@@ -1418,6 +1429,7 @@ dn_status dcdm_solve(dn_handle *h, dn_report *rep) {
   rep->pressure_iterations = its;
   rep->pressure_residual = relr;
   h->phase_ms[7] = its;
+  h->mon_count = std::min(its, h->mon_cap);
   return DN_OK;
 }
 
@@ -1544,6 +1556,7 @@ dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *r
   rep->pressure_iterations = (int)out[0];
   rep->pressure_residual = out[2];
   h->phase_ms[7] = out[0];
+  h->mon_count = cfg.precision == DN_PRECISION_MIXED ? 0 : std::min((int)out[0], h->mon_cap);
   return DN_OK;
 }
 
@@ -1838,6 +1851,7 @@ dn_status dn_destroy(dn_handle *h) {
   if (!h) return DN_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void *p : h->allocations) cudaFree(p);
+  if (h->mon) cudaFree(h->mon);
   if (h->host_scal) cudaFreeHost(h->host_scal);
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -2134,6 +2148,38 @@ dn_status dn_load_restart(dn_handle *h, const char *path, int *step) {
   for (int id : {DN_F_P_CORR, DN_F_U_STAR, DN_F_V_STAR, DN_F_SFX_CELL, DN_F_SFY_CELL, DN_F_SFX_U, DN_F_SFY_V})
     DN_TRY(fill_field(h, h->f[id], 0.0));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+// ---- CG monitor (the per-iteration record of the reference's CGMonitor, ch_sparse_krylov.hpp:515-660, as the
+// pressure analysis hook reads it, pressure_analysis.cpp:156-328) ----
+dn_status dn_set_pressure_monitor(dn_handle *h, int capacity) {
+  if (!h || capacity < 0) return DN_ERR_INVALID_ARGUMENT;
+  if (h->mon) {
+    cudaFree(h->mon);
+    h->mon = nullptr;
+  }
+  h->mon_cap = 0;
+  h->mon_count = 0;
+  if (capacity > 0) {
+    DN_CUDA(h, cudaMalloc(&h->mon, (size_t)capacity * 4 * sizeof(double)));
+    h->mon_cap = capacity;
+  }
+  return DN_OK;
+}
+
+dn_status dn_pressure_monitor(dn_handle *h, double *out, int capacity, int *count) {
+  if (!h || (capacity > 0 && !out)) return DN_ERR_INVALID_ARGUMENT;
+  const int m = std::min(capacity, h->mon_count);
+  if (m > 0) {
+    if (h->cfg.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG) {
+      std::memcpy(out, h->mon_host.data(), (size_t)m * 4 * sizeof(double));
+    } else {
+      DN_CUDA(h, cudaMemcpyAsync(out, h->mon, (size_t)m * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      DN_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+  }
+  if (count) *count = h->mon_count;
   return DN_OK;
 }
 
@@ -2923,7 +2969,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   if (dev_st != kDevOk) return static_device_status(dev_st, err, err_len);
 
   // the persistent PCG kernel, launched with the shape a handle would use for this grid
-  PcgArgs P;
+  PcgArgs P{};
   P.A = A;
   P.l = dptr(L.l5);
   P.dinv = dptr(L.dinv5);

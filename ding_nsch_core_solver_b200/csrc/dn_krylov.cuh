@@ -346,6 +346,8 @@ struct PcgArgsT {
   Sweep5T<T> s5;   // staged wavefront (SWEEP 3)
   int warp_smem;   // shared-memory bytes per sweep warp (SWEEP 3)
   int seq_lines;   // 13-point with periodic y: 1 = line-staged sequential sweeps (seq13 dynamic smem)
+  double *mon;     // per-iteration record [iteration][4]: abs residual, rel residual, iterate residual, alpha
+  int mon_cap;     // iterations the record holds (0: no record)
 };
 using PcgArgs = PcgArgsT<double>;
 
@@ -1026,6 +1028,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
     iter_res = sqrt(w[0] / fmax(w[1], 1.0e-30));
     absr = sqrt(fmax(rn2, 0.0));
     relr = absr / fmax(rhs_norm, 1.0e-30);
+    if (P.mon && it < P.mon_cap && blockIdx.x == 0 && threadIdx.x == 0) {  // the CG monitor's record
+      P.mon[4 * it + 0] = absr;
+      P.mon[4 * it + 1] = relr;
+      P.mon[4 * it + 2] = iter_res;
+      P.mon[4 * it + 3] = alpha;
+    }
     if (relr < P.tol || absr < P.tol_abs) break;
     // ---- z = M^{-1} r, project z, r.z (ch_sparse_krylov.hpp:626-635)
     if (!precondition(m_r, acc)) return;

@@ -233,6 +233,16 @@ dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, c
 dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
                                        const double *gE, double *c_bar, double *u_bar, double *v_bar);
 
+/* ---- CG monitor ---------------------------------------------------------------------------------------- */
+/* The per-iteration record of the pressure solve that the reference's CG monitor receives
+ * (ch_sparse_krylov.hpp:515-660; read by the pressure analysis, pressure.cpp / pressure_analysis.cpp:156-328).
+ * dn_set_pressure_monitor keeps up to `capacity` iterations of every later FP64 pressure solve (0 turns it
+ * off; allocates a device record).  dn_pressure_monitor copies the last solve's record into out,
+ * [iteration][4] = absolute residual, relative residual, iterate residual, alpha, for up to `capacity`
+ * iterations; *count receives how many the solve recorded.  The mixed form records nothing. */
+dn_status dn_set_pressure_monitor(dn_handle *h, int capacity);
+dn_status dn_pressure_monitor(dn_handle *h, double *out, int capacity, int *count);
+
 /* ---- history.csv --------------------------------------------------------------------------------------- */
 /* Solver::write_history_csv_header (io.cpp:179-185): the header line; returns its length (buf may be NULL). */
 size_t dn_history_csv_header(char *buf, size_t len);

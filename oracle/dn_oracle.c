@@ -158,6 +158,8 @@ struct orc_solver {
   int nrows_cap;
   char err[256];
   jmp_buf *jb;
+  double *mon;      /* CG monitor record of the last pressure solve, [iteration][4] */
+  int mon_cap, mon_count, mon_active;
 };
 
 static void fail(orc_solver *s, const char *fmt, ...) {
@@ -641,6 +643,16 @@ typedef struct {
   double absolute_residual, relative_residual, iterate_residual;
 } solve_rep;
 
+/* CGMonitor data of one iteration (ch_sparse_krylov.hpp:515-660), kept while a pressure solve runs */
+static void monitor_record(orc_solver *s, int it, const solve_rep *rep, double alpha) {
+  if (!s->mon_active || it >= s->mon_cap) return;
+  s->mon[4 * it + 0] = rep->absolute_residual;
+  s->mon[4 * it + 1] = rep->relative_residual;
+  s->mon[4 * it + 2] = rep->iterate_residual;
+  s->mon[4 * it + 3] = alpha;
+  s->mon_count = it + 1;
+}
+
 /* mean projection, pressure.cpp:225-239 (std::accumulate order) */
 static void project_mean(double *v, int n) {
   if (n <= 0) return;
@@ -691,6 +703,7 @@ static solve_rep pcg(orc_solver *s, const csr *m, const precond *pc, const doubl
     rep.iterate_residual = sqrt(update_sq / dmax(x_norm_sq, 1.0e-30));
     rep.absolute_residual = sqrt(dmax(dot(r, r, n), 0.0));
     rep.relative_residual = rep.absolute_residual / dmax(rhs_norm, 1.0e-30);
+    monitor_record(s, it, &rep, alpha);
     if (rep.relative_residual < tol || rep.absolute_residual < tol) break;
     apply_pc(m, pc, r, z, y);
     if (project) project_mean(z, n);
@@ -1680,8 +1693,11 @@ static double pressure_pcg(orc_solver *s, int split, int icc) {
     if (!try_ildlt(&s->pm, &s->ppc)) fail(s, "ILDLT preconditioner construction failed");
   }
   for (int k = 0; k < n; ++k) x[k] = 0.0;
+  s->mon_active = 1;
+  s->mon_count = 0;
   const solve_rep rep = pcg(s, &s->pm, &s->ppc, rhs, s->cfg.poisson_iterations, s->cfg.pressure_tolerance, x,
                             !pressure_has_dirichlet(s));
+  s->mon_active = 0;
   s->rep.pressure_iterations = rep.iterations;
   scatter_pressure(s, x);
   if (!pressure_has_dirichlet(s)) subtract_mean(s, pc);
@@ -1781,6 +1797,7 @@ static solve_rep dcdm(orc_solver *s, const csr *m, const precond *pc, const doub
     rep.iterate_residual = sqrt(update_sq / dmax(x_norm_sq, 1.0e-30));
     rep.absolute_residual = sqrt(dmax(dot(r, r, n), 0.0));
     rep.relative_residual = rep.absolute_residual / dmax(rhs_norm, 1.0e-30);
+    monitor_record(s, it, &rep, alpha);
     /* push_back, then drop the oldest beyond keep_max */
     memcpy(dirs[stored], d, (size_t)n * sizeof(double));
     memcpy(adirs[stored], ad, (size_t)n * sizeof(double));
@@ -1823,8 +1840,11 @@ static double pressure_dcdm(orc_solver *s) {
   fld_free(&pe);
   for (int k = 0; k < n; ++k) x[k] = 0.0;
   if (!try_icc(&s->pm, &s->ppc)) fail(s, "ICC preconditioner construction failed");
+  s->mon_active = 1;
+  s->mon_count = 0;
   const solve_rep rep = dcdm(s, &s->pm, &s->ppc, rhs, s->cfg.poisson_iterations, s->cfg.pressure_tolerance, x,
                              !pressure_has_dirichlet(s));
+  s->mon_active = 0;
   s->rep.pressure_iterations = rep.iterations;
   scatter_pressure(s, x);
   if (!pressure_has_dirichlet(s)) subtract_mean(s, pc);
@@ -2033,8 +2053,22 @@ orc_solver *orc_create(const orc_config *cfg) {
   return s;
 }
 
+void orc_set_pressure_monitor(orc_solver *s, int capacity) {
+  free(s->mon);
+  s->mon = capacity > 0 ? (double *)calloc((size_t)capacity * 4, sizeof(double)) : NULL;
+  s->mon_cap = capacity > 0 ? capacity : 0;
+  s->mon_count = 0;
+}
+
+int orc_pressure_monitor(const orc_solver *s, double *out, int capacity) {
+  const int m = s->mon_count < capacity ? s->mon_count : capacity;
+  if (m > 0) memcpy(out, s->mon, (size_t)m * 4 * sizeof(double));
+  return s->mon_count;
+}
+
 void orc_destroy(orc_solver *s) {
   if (!s) return;
+  free(s->mon);
   for (int k = 0; k < ORC_F_COUNT; ++k) fld_free(&s->f[k]);
   for (int k = 0; k < 16; ++k) free(s->w[k]);
   csr_free(&s->ch_lap);

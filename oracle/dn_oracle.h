@@ -111,6 +111,9 @@ int orc_advection(orc_solver *s, const double *c, const double *u, const double 
 /* The CH explicit operator E (build_phase_explicit_operator, phase_field.cpp:354-396) of Field2D arrays c
  * (cell; its ghosts are refilled by the scalar BC), u, v (faces) into E (cell, interior + ghosts). */
 int orc_explicit_operator(orc_solver *s, const double *c, const double *u, const double *v, double *E);
+/* The CG monitor's per-iteration record of the pressure solve (abs, rel, iterate residual, alpha). */
+void orc_set_pressure_monitor(orc_solver *s, int capacity);
+int orc_pressure_monitor(const orc_solver *s, double *out, int capacity);
 void orc_get_report(const orc_solver *s, orc_report *r);
 void orc_diagnostics(orc_solver *s, orc_diag *d); /* diagnostics.cpp:114-167 */
 double orc_compute_mass(orc_solver *s, int field_id);

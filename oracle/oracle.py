@@ -221,6 +221,8 @@ def _load(impl: str):
     else:
         sig["advection"] = (C.c_int, [vp, dp, dp, dp, dp])
         sig["explicit_operator"] = (C.c_int, [vp, dp, dp, dp, dp])
+        sig["set_pressure_monitor"] = (None, [vp, C.c_int])
+        sig["pressure_monitor"] = (C.c_int, [vp, dp, C.c_int])
     fns = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, pre + name)
@@ -331,6 +333,15 @@ class OracleSolver:
         out = np.zeros_like(self.field("c"))
         self._check(self._f["explicit_operator"](self._h, *(a.ctypes.data_as(dp) for a in (c, u, v, out))))
         return out
+
+    def set_pressure_monitor(self, capacity: int) -> None:
+        self._f["set_pressure_monitor"](self._h, int(capacity))
+
+    def pressure_monitor(self, capacity: int = 100000) -> np.ndarray:
+        """The last pressure solve's CG-monitor record (port only): abs, rel, iterate residual, alpha."""
+        out = np.zeros((capacity, 4))
+        cnt = self._f["pressure_monitor"](self._h, out.ctypes.data_as(C.POINTER(C.c_double)), capacity)
+        return out[:min(cnt, capacity)].copy()
 
     def report(self) -> dict:
         r = Report()

@@ -57,3 +57,29 @@ def test_rows_carry_the_step(name, pname):
             assert vals["dt_limit_source"] == src
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["walls_split_icpcg_wide", "channel_x_icpcg", "dcdm_walls"])
+def test_pressure_monitor_matches_oracle(name):
+    """The CG monitor's per-iteration record of the pressure solve (abs, rel, iterate residual, alpha) against
+    the oracle's, on the same seeded step."""
+    import ding_nsch_core_solver_b200 as dn
+    from test_gpu_parity import CASES, seeded_pair
+
+    orc, gpu = seeded_pair(dn, CASES[name], seed=9)
+    try:
+        orc.set_pressure_monitor(5000)
+        gpu.set_pressure_monitor(5000)
+        orc.step(0)
+        rep = gpu.step(0)
+        a, b = gpu.pressure_monitor(), orc.pressure_monitor()
+        assert len(a) == rep["pressure_iterations"] == len(b) > 0
+        # residuals differ only by the reduction order: compare where they are well above round-off
+        keep = b[:, 1] > 1e-8
+        np.testing.assert_allclose(a[keep, 1], b[keep, 1], rtol=1e-6)
+        np.testing.assert_allclose(a[keep, 3], b[keep, 3], rtol=1e-6)
+        np.testing.assert_allclose(a[keep, 0], b[keep, 0], rtol=1e-6)
+    finally:
+        gpu.close()
+        orc.close()
