@@ -49,7 +49,8 @@ class Config(C.Structure):
         "angular_velocity", "top_wall_velocity_x", "bottom_wall_velocity_x")] + [
         ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4), ("precision", C.c_int),
         ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int), ("dcdm_direction_mode", C.c_int),
-        ("dcdm_history_size", C.c_int), ("dcdm_max_stored_directions", C.c_int), ("dcdm_restart_interval", C.c_int)]
+        ("dcdm_history_size", C.c_int), ("dcdm_max_stored_directions", C.c_int), ("dcdm_restart_interval", C.c_int),
+        ("pcg_rows_per_cta", C.c_int), ("sweep_warps_per_cta", C.c_int)]
 
 
 class Report(C.Structure):
@@ -119,6 +120,7 @@ def load():
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_set_pressure_monitor": (I, [H, I]),
         "dn_pressure_monitor": (I, [H, DP, I, C.POINTER(C.c_int)]),
+        "dn_autotune_pressure": (I, [H, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         "dn_history_csv_header": (C.c_size_t, [C.c_char_p, C.c_size_t]),
         "dn_history_csv_row": (I, [H, I, D, C.POINTER(Report), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "dn_write_restart": (I, [H, I, C.c_char_p]),
@@ -292,6 +294,13 @@ class Solver:
         cnt = C.c_int()
         self._check(self._lib.dn_pressure_monitor(self._h, _dp(out), capacity, C.byref(cnt)))
         return out[:min(cnt.value, capacity)].copy()
+
+    def autotune_pressure(self) -> dict:
+        """Time the pressure solve of the current state over the launch shapes (rows per CTA x sweep warps
+        per CTA) and keep the fastest; the solve's P_CORR is rewritten, nothing else of the state."""
+        rows, sw, ms = C.c_int(), C.c_int(), C.c_double()
+        self._check(self._lib.dn_autotune_pressure(self._h, C.byref(rows), C.byref(sw), C.byref(ms)))
+        return {"pcg_rows_per_cta": rows.value, "sweep_warps_per_cta": sw.value, "pressure_ms": ms.value}
 
     def history_csv_row(self, step: int, time: float, report: dict) -> str:
         """Solver::append_history_csv_entry: the history.csv row of the step whose report is `report`."""

@@ -37,6 +37,8 @@ constexpr int kHostScal = 8192;  // pinned host scratch (doubles): scalars and r
 constexpr int kSweepWarpsPerCta = 4;
 // dynamic shared memory the CH PCG kernel may use (the ring of the level sweep, the periodic-y line buffers)
 constexpr size_t kSeqSmemMax = 96 * 1024;
+// rows per CTA of the persistent PCG's SpMV / update phases: they are latency-bound, so more CTAs shorten them
+constexpr long long kPcgRowsPerCta = 512;
 
 // ---------------------------------------------------------------------------------------------------
 // Pressure system (build_pressure_linear_system, pressure.cpp:123-196) into 5 slots W,S,C,N,E + rhs
@@ -413,7 +415,10 @@ struct dn_handle {
   std::vector<double> mon_host;  // the same record for the host-driven solvers
   int dcdm_keep = 0;
   int sw5 = 0;                 // sweep warps per CTA, 0 = staged path unavailable
-  int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3> (k_pcg<5,4> with periodic x)
+  int sw5_budget = 0;          // the most sweep warps per CTA the shared memory allows
+  long long rows_per_cta = 512;  // rows per CTA of the PCG kernels' SpMV / update phases
+  int sw5_blocks_max = 0;      // co-resident CTAs of k_pcg<5,3> (k_pcg<5,4> with periodic x) at sw5 warps
+  int sw5_blocks_by_sw[kSweepWarpsPerCta + 1] = {};  // the same for each sweep-warp count up to sw5_budget
   size_t sw5_warp_smem[2] = {0, 0};  // per sweep warp, [constant operator, variable operator]
   int smem_optin = 0;
   double initial_mass = 0.0;
@@ -625,7 +630,7 @@ dn_status pcg_launch_args(dn_handle *h, const double *a, const double *l, const 
     dyn_smem = (size_t)seq13_smem_doubles_per_row() * h->G.ny * sizeof(double);
   }
   // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
-  const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
+  const long long rows_per_cta = h->rows_per_cta;
   int blocks = (int)std::min<long long>(h->cta_cap,
                                         std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(blocks, (h->nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
@@ -666,7 +671,7 @@ dn_status pcg_launch_args(dn_handle *h, const double *a, const double *l, const 
     dyn_smem = 64 + (size_t)h->sw5 * P.warp_smem;
     const int sweep_ctas = (h->nsweep5 + h->sw5 - 1) / h->sw5;
     blocks = std::max(blocks, sweep_ctas);
-    blocks = std::min(blocks, h->sw5_blocks_max);
+    blocks = std::min(blocks, h->sw5_blocks_by_sw[h->sw5]);
     if (blocks < sweep_ctas) return fail(h, DN_ERR_UNSUPPORTED, "not enough co-resident CTAs for the wavefront");
   }
   if (SWEEP == 0 && (long long)blocks * (kBlock / 32) < h->nsweep)
@@ -739,7 +744,7 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
   P.warp_smem = 0;
   size_t dyn_smem = 0;
   // about 512 rows per CTA: the SpMV / update phases are latency-bound, so more CTAs shorten them
-  const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
+  const long long rows_per_cta = h->rows_per_cta;
   int blocks = (int)std::min<long long>(h->cta_cap,
                                         std::max<long long>(h->nsweep, (h->n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(blocks, (h->nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
@@ -1666,6 +1671,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   cudaGetDeviceProperties(&prop, device);
   h->num_sms = prop.multiProcessorCount;
   h->cta_cap = std::max(1, h->num_sms / std::max(1, cfg->device_share));
+  h->rows_per_cta = cfg->pcg_rows_per_cta > 0 ? cfg->pcg_rows_per_cta : kPcgRowsPerCta;
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
   for (auto &e : h->ev) cudaEventCreate(&e);
   for (auto &e : h->kev) cudaEventCreate(&e);
@@ -1769,7 +1775,8 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     const size_t budget = (size_t)optin > 64 + 2304 ? (size_t)optin - 64 - 2304 : 0;  // minus static smem
     int sw = stageable ? (int)std::min<size_t>(kSweepWarpsPerCta, budget / per) : 0;
     sw = std::min(sw, h->nsweep5);
-    if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
+    h->sw5_budget = stageable ? sw : 0;
+    if (sw > 0 && c.sweep_warps_per_cta > 0) sw = std::min(sw, c.sweep_warps_per_cta);
     h->sw5 = stageable ? sw : 0;
     if (h->sw5 > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
@@ -1779,9 +1786,12 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
       cudaFuncGetAttributes(&fa, k53);
       cudaFuncSetAttribute(k53, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            std::max((int)dyn, optin - (int)fa.sharedSizeBytes));
-      int occ5 = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k53, kBlock, dyn);
-      h->sw5_blocks_max = std::min(kMaxBlocks, std::max(0, occ5) * h->num_sms);
+      for (int w = 1; w <= h->sw5_budget; ++w) {
+        int occ5 = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, k53, kBlock, 64 + (size_t)w * per);
+        h->sw5_blocks_by_sw[w] = std::min(kMaxBlocks, std::max(0, occ5) * h->num_sms);
+      }
+      h->sw5_blocks_max = h->sw5_blocks_by_sw[sw];
       if (h->sw5_blocks_max == 0) h->sw5 = 0;
     }
   }
@@ -1817,7 +1827,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     const size_t budget = (size_t)optin > 64 + fa.sharedSizeBytes ? (size_t)optin - 64 - fa.sharedSizeBytes : 0;
     int sw = stageable ? (int)std::min<size_t>(kSweepWarpsPerCta, budget / per) : 0;
     sw = std::min(sw, h->nsweep5);
-    if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
+    if (sw > 0 && c.sweep_warps_per_cta > 0) sw = std::min(sw, c.sweep_warps_per_cta);
     h->sw5f = stageable ? sw : 0;
     if (h->sw5f > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
@@ -2148,6 +2158,62 @@ dn_status dn_load_restart(dn_handle *h, const char *path, int *step) {
   for (int id : {DN_F_P_CORR, DN_F_U_STAR, DN_F_V_STAR, DN_F_SFX_CELL, DN_F_SFY_CELL, DN_F_SFX_U, DN_F_SFY_V})
     DN_TRY(fill_field(h, h->f[id], 0.0));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+// Launch-shape autotuner of the pressure PCG: times one pressure solve of the handle's current state (its
+// u*, v*, rho_mid, p, p_prev, as a step leaves them) for each candidate (rows per CTA of the SpMV / update
+// phases x sweep warps per CTA of the staged wavefront) and keeps the fastest on the handle.
+dn_status dn_autotune_pressure(dn_handle *h, int *rows_per_cta, int *sweep_warps_per_cta, double *best_ms) {
+  if (!h) return DN_ERR_INVALID_ARGUMENT;
+  if (h->cfg.pressure_scheme == DN_P_JACOBI || h->cfg.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG)
+    return fail(h, DN_ERR_UNSUPPORTED, "the launch-shape autotuner covers the PCG pressure schemes");
+  const long long rows_c[] = {256, 512, 1024, 2048, 4096};
+  // sweep-warp counts whose wavefront CTAs are co-resident; the FP64 staged path only (the mixed form's
+  // FP32 wavefront keeps its own)
+  std::vector<int> sws;
+  if (h->sw5 > 0 && h->cfg.precision != DN_PRECISION_MIXED) {
+    for (int w = 1; w <= h->sw5_budget; ++w)
+      if ((h->nsweep5 + w - 1) / w <= h->sw5_blocks_by_sw[w]) sws.push_back(w);
+  } else {
+    sws.push_back(h->sw5);
+  }
+  const long long rows0 = h->rows_per_cta;
+  const int sw0 = h->sw5;
+  long long best_rows = rows0;
+  int best_sw = sw0;
+  double best = INFINITY;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  dn_status st = DN_OK;
+  for (int pass = 0; pass < 2 && st == DN_OK; ++pass)  // the first pass also warms up each shape
+    for (long long rows : rows_c)
+      for (int sw : sws) {
+        h->rows_per_cta = rows;
+        h->sw5 = sw;
+        dn_report rep{};
+        cudaEventRecord(e0, h->stream);
+        st = pressure(h, h->step, &rep);
+        cudaEventRecord(e1, h->stream);
+        if (st != DN_OK) break;
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (pass == 1 && ms < best) {
+          best = ms;
+          best_rows = rows;
+          best_sw = sw;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->rows_per_cta = st == DN_OK ? best_rows : rows0;
+  h->sw5 = st == DN_OK ? best_sw : sw0;
+  if (st != DN_OK) return st;
+  if (rows_per_cta) *rows_per_cta = (int)best_rows;
+  if (sweep_warps_per_cta) *sweep_warps_per_cta = best_sw;
+  if (best_ms) *best_ms = best;
   return DN_OK;
 }
 
@@ -2995,7 +3061,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   P.out = scal + 8;
   P.nsweep = nsweep;
   P.warp_smem = 0;
-  const long long rows_per_cta = std::getenv("DN_PCG_ROWS_PER_CTA") ? std::atoll(std::getenv("DN_PCG_ROWS_PER_CTA")) : 512;
+  const long long rows_per_cta = c.pcg_rows_per_cta > 0 ? c.pcg_rows_per_cta : kPcgRowsPerCta;
   int blocks = (int)std::min<long long>(D.num_sms, std::max<long long>(nsweep, (n + rows_per_cta - 1) / rows_per_cta));
   blocks = std::max(1, std::min(blocks, D.max_coop_blocks));
   // staged wavefront: sweep warps per CTA from the shared-memory budget, as dn_create chooses them
@@ -3007,7 +3073,7 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
     const size_t budget = (size_t)D.smem_optin > 64 + 2304 ? (size_t)D.smem_optin - 64 - 2304 : 0;
     sw = (int)std::min<size_t>(kSweepWarpsPerCta, budget / per);
     sw = std::min(sw, nsweep5);
-    if (const char *e = std::getenv("DN_SWEEP_WARPS_PER_CTA")) sw = std::max(1, std::min(sw, std::atoi(e)));
+    if (sw > 0 && c.sweep_warps_per_cta > 0) sw = std::min(sw, c.sweep_warps_per_cta);
     if (sw > 0) {
       const size_t dyn = 64 + (size_t)sw * per;
       if (dyn + (size_t)D.pcg3_static_smem > (size_t)D.smem_optin) {

@@ -108,6 +108,8 @@ extern "C" void dn_config_default(dn_config *c) {
   c->dcdm_history_size = 2;
   c->dcdm_max_stored_directions = 8;
   c->dcdm_restart_interval = 0;
+  c->pcg_rows_per_cta = 0;     // 512
+  c->sweep_warps_per_cta = 0;  // as many as the shared memory holds, up to 4
 }
 
 extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err, size_t err_len) {
@@ -215,6 +217,8 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
     geti("dcdm_history_size", cfg->dcdm_history_size);
     geti("dcdm_max_stored_directions", cfg->dcdm_max_stored_directions);
     geti("dcdm_restart_interval", cfg->dcdm_restart_interval);
+    geti("pcg_rows_per_cta", cfg->pcg_rows_per_cta);
+    geti("sweep_warps_per_cta", cfg->sweep_warps_per_cta);
     if (kv.count("dcdm_direction_mode")) {  // pressure.cpp:383-395
       const std::string m = lower(kv["dcdm_direction_mode"]);
       if (m == "identity")
@@ -227,6 +231,8 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
         throw std::runtime_error("unsupported dcdm_direction_mode: " + kv["dcdm_direction_mode"]);
     }
     if (cfg->device_share < 1) throw std::runtime_error("device_share must be at least 1");
+    if (cfg->pcg_rows_per_cta < 0 || cfg->sweep_warps_per_cta < 0)
+      throw std::runtime_error("pcg_rows_per_cta and sweep_warps_per_cta must be non-negative (0: the default)");
     static const char *sides[4] = {"left", "right", "bottom", "top"};
     for (int s = 0; s < 4; ++s) {
       char tk[64], vk[64];

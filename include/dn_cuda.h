@@ -84,6 +84,9 @@ typedef struct {
                                       CTAs than its wavefront needs; 1 = the whole device */
   int dcdm_direction_mode;         /* split_dcdm_icpcg directions: 0 icc_preconditioned, 1 identity (config.hpp:51) */
   int dcdm_history_size, dcdm_max_stored_directions, dcdm_restart_interval; /* config.hpp:72-74 */
+  int pcg_rows_per_cta;            /* launch shape of the pressure PCG: rows per CTA of its SpMV / update
+                                      phases (0: 512) -- see dn_autotune_pressure */
+  int sweep_warps_per_cta;         /* sweep warps per CTA of the staged wavefront (0: as many as fit, up to 4) */
 } dn_config;
 
 /* Fields (Solver members, src/core/coupled/solver.hpp:64-91). */
@@ -232,6 +235,13 @@ dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, c
  * derivative is taken on the side the forward evaluation lies on.  DEVICE buffers. */
 dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
                                        const double *gE, double *c_bar, double *u_bar, double *v_bar);
+
+/* ---- launch-shape autotuning ----------------------------------------------------------------------------- */
+/* No counterpart in the reference.  Times one pressure solve of the handle's current state (u*, v*, rho_mid,
+ * p, p_prev as a step leaves them) for each launch shape -- rows per CTA of the PCG's SpMV / update phases
+ * in {256 .. 4096} x sweep warps per CTA of the staged wavefront -- twice, and keeps the fastest of the
+ * second pass on the handle.  Outputs (each may be NULL): the chosen shape and its pressure-solve time. */
+dn_status dn_autotune_pressure(dn_handle *h, int *rows_per_cta, int *sweep_warps_per_cta, double *best_ms);
 
 /* ---- CG monitor ---------------------------------------------------------------------------------------- */
 /* The per-iteration record of the pressure solve that the reference's CG monitor receives
