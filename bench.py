@@ -83,29 +83,6 @@ def initial_state(cfg: dict, seed: int = 2) -> dict:
 PCG_PROFILE = os.path.join(ROOT, "profiles", "k_pcg_5_3_pressure_192x384.txt")
 
 
-def ensemble_cfgs(count: int, seed: int = 4) -> list:
-    """Droplet instances of uneven grids: nx, ny each from {64, 96, 128, 192, 256}; unit square, periodic
-    both ways; radius U(0.15, 0.3) at a centre kept 0.05 inside the box; density and viscosity ratios
-    log-uniform in [1, 100]; surface tension multiplier U(0.5, 2) with re = ca = 1; cn = 1.5 min(dx, dy);
-    uniform background velocity U(-0.1, 0.1)^2; split_icpcg in the mixed-precision form."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(count):
-        nx, ny = (int(v) for v in rng.choice([64, 96, 128, 192, 256], size=2))
-        radius = rng.uniform(0.15, 0.3)
-        cx, cy = rng.uniform(radius + 0.05, 1.0 - radius - 0.05, size=2)
-        au, av = rng.uniform(-0.1, 0.1, size=2)
-        out.append(dict(
-            name=f"droplet_{nx}x{ny}", mode="coupled", nx=nx, ny=ny, ghost=3, lx=1.0, ly=1.0, periodic_x=True,
-            periodic_y=True, interface_center_x=float(cx), interface_center_y=float(cy), interface_radius=float(radius),
-            density_ratio=float(10 ** rng.uniform(0, 2)), viscosity_ratio=float(10 ** rng.uniform(0, 2)),
-            surface_tension_multiplier=float(rng.uniform(0.5, 2.0)), re=1.0, ca=1.0, cn=1.5 / max(nx, ny),
-            advect_u=float(au), advect_v=float(av), dt=1e-5, pressure_scheme="split_icpcg", precision="mixed",
-            poisson_iterations=2000, pressure_tolerance=1e-10, ch_inner_iterations=500, ch_tolerance=1e-10,
-            momentum_iterations=200, momentum_tolerance=1e-10))
-    return out
-
-
 def pcg_traffic_per_launch():
     """DRAM bytes (read + write) of one pressure-PCG launch from the committed ncu summary, per iteration,
     or None when no summary is present."""
@@ -384,58 +361,67 @@ def run_ours(args):
         for s in members:
             s.close()
 
-    # ---- ensemble of uneven droplet instances (periodic both ways, mixed precision), all through one
-    # dn_step_batch call per batch step; each handle's persistent grids take 1/count of the SMs
+    # ---- ensemble of uneven droplet instances (periodic both ways, mixed precision): whole instances
+    # sharded over the ranks by LPT on estimated cost, each rank's share stepped together by one
+    # dn_step_batch call per batch step; one gather of per-instance records at the end
     ensemble = None
     if args.ensemble > 0:
-        cfgs = ensemble_cfgs(args.ensemble)
-        total_cells = sum(c["nx"] * c["ny"] for c in cfgs)
+        from ding_nsch_core_solver_b200.ensemble import ShardedEnsemble, droplet_cfgs, gather_records
 
-        def share(c):
-            # each instance's persistent grids take its share of the cells' worth of SMs
-            return len(cfgs) if args.ensemble_equal else max(1, round(total_cells / (c["nx"] * c["ny"])))
-
-        members = []
+        cfgs = droplet_cfgs(args.ensemble)
+        cells = sum(c["nx"] * c["ny"] for c in cfgs)
+        shard, err, etimes, ereps = None, "", [], []
         try:
-            for ec in cfgs:
-                m = dn.Solver(dict(ec, device_share=share(ec)), device=device)
-                m.initialize()
-                m.set_initial_mass(m.compute_mass("c"))
-                members.append(m)
+            shard = ShardedEnsemble(cfgs, rank, world, device, proportional=not args.ensemble_equal)
+            shard.initialize()
             estep = 0
             for _ in range(args.warmup):
-                capi.step_batch(members, [estep] * len(members))
+                shard.step(estep)
                 estep += 1
-            etimes, ereps = [], []
             for _ in range(args.steps):
                 flush.zero_()
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
-                ereps.append(capi.step_batch(members, [estep] * len(members)))
+                ereps.append(shard.step(estep))
                 e1.record()
                 e1.synchronize()
                 etimes.append(e0.elapsed_time(e1))
                 estep += 1
-            cells = sum(c["nx"] * c["ny"] for c in cfgs)
-            etotal = reduce_max(dist, sum(etimes))
-            diag = [m.diagnostics() for m in members]
+        except capi.DnError as e:
+            err = str(e)
+        # every rank reaches the same two collectives, an error on one rank included
+        etotal = reduce_max(dist, sum(etimes) if not err else float("inf"))
+        mine = shard.mine if shard is not None else []
+        recs = []
+        for k, i in enumerate(mine):
+            d = shard.members[k].diagnostics() if not err else {}
+            recs.append({"err": err, "pressure_iterations": [rs[k]["pressure_iterations"] for rs in ereps],
+                         "ch_iterations": [rs[k]["ch_iterations"] for rs in ereps],
+                         "max_velocity": d.get("max_velocity"), "mass_drift": d.get("mass_drift")})
+        if err and not mine:
+            recs, mine = [{"err": err}], [-1 - rank]
+        allrec = gather_records(dist, mine, recs)
+        errors = sorted({r["err"] for r in allrec if r.get("err")})
+        if errors:
+            ensemble = {"instances": len(cfgs), "error": "; ".join(errors)}
+        else:
             ensemble = {"instances": len(cfgs), "cells": cells,
-                        "value": round(cells * args.steps * world / (etotal * 1e-3) / 1e6, 4), "unit": "Mcell-steps/s",
-                        "ms_per_batch_step": round(etotal / args.steps, 3),
+                        "value": round(cells * args.steps / (etotal * 1e-3) / 1e6, 4), "unit": "Mcell-steps/s",
+                        "ms_per_batch_step": round(etotal / args.steps, 3), "scaling": "strong",
+                        "instances_per_rank": [len(p) for p in shard.parts],
                         "pressure_iterations_mean": round(statistics.mean(
-                            r["pressure_iterations"] for rs in ereps for r in rs), 1),
-                        "ch_iterations_mean": round(statistics.mean(r["ch_iterations"] for rs in ereps for r in rs), 1),
-                        "max_velocity_max": max(d["max_velocity"] for d in diag),
-                        "mass_drift_max": max(d["mass_drift"] for d in diag),
+                            x for r in allrec for x in r["pressure_iterations"]), 1),
+                        "ch_iterations_mean": round(statistics.mean(x for r in allrec for x in r["ch_iterations"]), 1),
+                        "max_velocity_max": max(r["max_velocity"] for r in allrec),
+                        "mass_drift_max": max(r["mass_drift"] for r in allrec),
                         "workload": "uneven droplets: grids {64..256}^2, periodic both ways, split_icpcg, mixed, "
-                                    "dt 1e-5, seed 4; all instances stepped together by dn_step_batch",
+                                    "dt 1e-5, seed 4; whole instances sharded over the ranks by LPT on cells x "
+                                    "max(nx, ny), each rank's share stepped together by dn_step_batch",
                         "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                         "sm_share": "equal (1/instances)" if args.ensemble_equal else "in proportion to cells"}
-        except capi.DnError as e:
-            ensemble = {"instances": len(cfgs), "error": str(e)}
-        for m in members:
-            m.close()
+        if shard is not None:
+            shard.close()
 
     # ---- roofline of the dominant kernel (the pressure PCG), bytes per launch / launch time
     peak, peak_kind = hbm_peak()
