@@ -50,7 +50,11 @@ class Config(C.Structure):
         ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4), ("precision", C.c_int),
         ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int), ("dcdm_direction_mode", C.c_int),
         ("dcdm_history_size", C.c_int), ("dcdm_max_stored_directions", C.c_int), ("dcdm_restart_interval", C.c_int),
-        ("pcg_rows_per_cta", C.c_int), ("sweep_warps_per_cta", C.c_int)]
+        ("pcg_rows_per_cta", C.c_int), ("sweep_warps_per_cta", C.c_int),
+        ("analysis_enabled", C.c_int), ("analysis_mode", C.c_int), ("analysis_trigger_step", C.c_int),
+        ("analysis_interface_band_multiplier", C.c_double), ("name", C.c_char * 128), ("output_dir", C.c_char * 512),
+        ("analysis_case_group", C.c_char * 128), ("analysis_initial_guess", C.c_char * 64),
+        ("analysis_nullspace_treatment", C.c_char * 64), ("analysis_spectrum_iterations", C.c_char * 256)]
 
 
 class Report(C.Structure):
@@ -121,6 +125,7 @@ def load():
         "dn_set_pressure_monitor": (I, [H, I]),
         "dn_pressure_monitor": (I, [H, DP, I, C.POINTER(C.c_int)]),
         "dn_autotune_pressure": (I, [H, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+        "dn_pressure_analysis": (I, [H, I, C.c_char_p]),
         "dn_history_csv_header": (C.c_size_t, [C.c_char_p, C.c_size_t]),
         "dn_history_csv_row": (I, [H, I, D, C.POINTER(Report), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "dn_write_restart": (I, [H, I, C.c_char_p]),
@@ -294,6 +299,11 @@ class Solver:
         cnt = C.c_int()
         self._check(self._lib.dn_pressure_monitor(self._h, _dp(out), capacity, C.byref(cnt)))
         return out[:min(cnt.value, capacity)].copy()
+
+    def pressure_analysis(self, step: int, source_mode: str = "frozen") -> None:
+        """Solver::run_pressure_analysis_from_snapshot on the current state (step index `step`): the analysis
+        files under output_dir/name/pressure_analysis/."""
+        self._check(self._lib.dn_pressure_analysis(self._h, int(step), source_mode.encode()))
 
     def autotune_pressure(self) -> dict:
         """Time the pressure solve of the current state over the launch shapes (rows per CTA x sweep warps

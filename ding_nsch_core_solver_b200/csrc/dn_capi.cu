@@ -10,11 +10,14 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cctype>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1265,21 +1268,21 @@ dn_status pressure_jacobi(dn_handle *h, dn_report *rep) {
   return bc(h, f[DN_F_P_CORR], kBCPressure);
 }
 
-// z = M^-1 in with the ICC factor of the pressure system (k_prec_apply); z lands in h->z.
-dn_status prec_apply(dn_handle *h, const double *in) {
+// z = M^-1 in with the ICC (or LDLT) factor of the pressure system (k_prec_apply); z lands in h->z.
+dn_status prec_apply(dn_handle *h, const double *in, int kind = kPrecICC) {
   PcgArgs P{};
   size_t dyn_smem = 0;
   int blocks = 1;
   const bool staged = h->sw5 > 0;
   const void *kern;
   if (staged && h->G.px) {
-    DN_TRY((pcg_launch_args<5, 4>(h, h->a5, h->l5, h->dinv5, kPrecICC, 0, 1, 0.0, P, dyn_smem, blocks)));
+    DN_TRY((pcg_launch_args<5, 4>(h, h->a5, h->l5, h->dinv5, kind, 0, 1, 0.0, P, dyn_smem, blocks)));
     kern = (const void *)k_prec_apply<4>;
   } else if (staged) {
-    DN_TRY((pcg_launch_args<5, 3>(h, h->a5, h->l5, h->dinv5, kPrecICC, 0, 1, 0.0, P, dyn_smem, blocks)));
+    DN_TRY((pcg_launch_args<5, 3>(h, h->a5, h->l5, h->dinv5, kind, 0, 1, 0.0, P, dyn_smem, blocks)));
     kern = (const void *)k_prec_apply<3>;
   } else {
-    DN_TRY((pcg_launch_args<5, 0>(h, h->a5, h->l5, h->dinv5, kPrecICC, 0, 1, 0.0, P, dyn_smem, blocks)));
+    DN_TRY((pcg_launch_args<5, 0>(h, h->a5, h->l5, h->dinv5, kind, 0, 1, 0.0, P, dyn_smem, blocks)));
     kern = (const void *)k_prec_apply<0>;
   }
   P.r = const_cast<double *>(in);
@@ -1435,6 +1438,338 @@ dn_status dcdm_solve(dn_handle *h, dn_report *rep) {
   rep->pressure_residual = relr;
   h->phase_ms[7] = its;
   h->mon_count = std::min(its, h->mon_cap);
+  return DN_OK;
+}
+
+// ---- pressure analysis (Solver::run_pressure_analysis_from_snapshot, pressure_analysis.cpp:156-328) ----
+// 1 where |2c - 1| < cutoff (the interface band), else 0, per compact row i*ny + j
+__global__ void k_interface_mask(Fv c, double cutoff, double *mask) {
+  const long long n = (long long)c.nx * c.ny;
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const double phi = 2.0 * c.at((int)(r / c.ny), (int)(r % c.ny)) - 1.0;
+  mask[r] = fabs(phi) < cutoff ? 1.0 : 0.0;
+}
+// per block: max |r|, the sum of r^2 over the band, the sum of r^2 outside it
+__global__ void k_resid_stats(const double *r, const double *mask, long long n, double *partials) {
+  __shared__ double sm[3][256];
+  double mx = 0.0, in = 0.0, out = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double v = r[t];
+    mx = fmax(mx, fabs(v));
+    if (mask[t] > 0.5)
+      in += v * v;
+    else
+      out += v * v;
+  }
+  sm[0][threadIdx.x] = mx;
+  sm[1][threadIdx.x] = in;
+  sm[2][threadIdx.x] = out;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      sm[0][threadIdx.x] = fmax(sm[0][threadIdx.x], sm[0][threadIdx.x + o]);
+      sm[1][threadIdx.x] += sm[1][threadIdx.x + o];
+      sm[2][threadIdx.x] += sm[2][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partials[(size_t)k * gridDim.x + blockIdx.x] = sm[k][0];
+}
+// z = in / max(|diag|, 1e-30): build_diagonal_preconditioner / apply_preconditioner (ch_sparse_krylov.hpp:421-432)
+__global__ void k_diag_apply(const double *diag, const double *in, double *z, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) z[t] = (1.0 / fmax(fabs(diag[t]), 1.0e-30)) * in[t];
+}
+__global__ void k_p_update(double *p, const double *z, long long n, double beta) {  // p = z + beta p
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) p[t] = z[t] + beta * p[t];
+}
+
+// %.17g, as an ostream with setprecision(17) prints a double
+std::string g17(double v) {
+  char b[40];
+  std::snprintf(b, sizeof b, "%.17g", v);
+  return b;
+}
+// write_matrix_csv (pressure_analysis.cpp:46-61) of a compact vector (row i*ny + j): ny lines of nx values
+bool write_field_csv(const std::filesystem::path &path, const std::vector<double> &v, int nx, int ny) {
+  FILE *fp = std::fopen(path.string().c_str(), "w");
+  if (!fp) return false;
+  for (int j = 0; j < ny; ++j) {
+    for (int i = 0; i < nx; ++i) std::fprintf(fp, i > 0 ? ",%.17g" : "%.17g", v[(size_t)i * ny + j]);
+    std::fputc('\n', fp);
+  }
+  return std::fclose(fp) == 0;
+}
+
+// Sums (max for k == 0 when `max0`) of per-block partials written by a 128-block kernel, in block order.
+dn_status host_partials(dn_handle *h, int k_count, int nb, bool max0, double *out) {
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->partials, (size_t)k_count * nb * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < k_count; ++k) {
+    double v = 0.0;
+    for (int b = 0; b < nb; ++b) v = (max0 && k == 0) ? std::max(v, h->host_scal[k * nb + b]) : v + h->host_scal[k * nb + b];
+    out[k] = v;
+  }
+  return DN_OK;
+}
+
+dn_status download(dn_handle *h, const double *dev, std::vector<double> &host, size_t count) {
+  host.resize(count);
+  DN_CUDA(h, cudaMemcpyAsync(host.data(), dev, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+dn_status pressure_analysis(dn_handle *h, int step, const std::string &source) {
+  namespace fs = std::filesystem;
+  Fv *f = h->f;
+  const dn_config &cfg = h->cfg;
+  const long long n = h->n;
+  const int nb = blocks_for(n), nx = h->G.nx, ny = h->G.ny;
+  const bool split = use_split(cfg);
+  const bool ildlt = cfg.pressure_scheme == DN_P_ILDLT_PCG || cfg.pressure_scheme == DN_P_SPLIT_ILDLT_PCG;
+  const bool project = !h->has_dirichlet;
+  const double tol = cfg.pressure_tolerance;
+  // the key iterations (analysis_key_iterations, pressure_analysis.cpp:108-124)
+  std::set<int> keys;
+  {
+    const std::string list = cfg.analysis_spectrum_iterations;
+    size_t at = 0;
+    while (at <= list.size()) {
+      const size_t comma = std::min(list.find(',', at), list.size());
+      std::string tok;
+      for (size_t q = at; q < comma; ++q)
+        if (!std::isspace((unsigned char)list[q])) tok += list[q];
+      at = comma + 1;
+      std::string low = tok;
+      for (char &ch : low) ch = (char)std::tolower((unsigned char)ch);
+      if (tok.empty() || low == "final") continue;
+      try {
+        keys.insert(std::stoi(tok));
+      } catch (const std::exception &) {
+        return fail(h, DN_ERR_CONFIG, "invalid analysis_spectrum_iterations entry: " + tok);
+      }
+    }
+  }
+  // the system as the scheme assembles it, and its preconditioner (ICC / ILDLT, the diagonal when it fails)
+  if (split) DN_TRY(split_extrapolation(h, step));
+  k_p_assemble<<<blocks_for(n), 256, 0, h->stream>>>(h->G, h->bc, f[DN_F_RHO_MID], f[DN_F_U_STAR], f[DN_F_V_STAR],
+                                                    h->pe, split ? 1 : 0, split ? rho_ref_of(cfg) : 1.0, cfg.dt,
+                                                    h->a5, h->b);
+  DN_TRY(check_launch(h, "k_p_assemble"));
+  if (project) DN_TRY(compact_subtract_mean(h, h->b));
+  const int kind = ildlt ? kPrecLDLT : kPrecICC;
+  bool diag = false;
+  {
+    const dn_status fs_ = pressure_factor(h, split, !ildlt);
+    if (fs_ == DN_ERR_ICC_FAILED || fs_ == DN_ERR_ILDLT_FAILED) {
+      diag = true;
+      h->err.clear();
+    } else if (fs_ != DN_OK) {
+      return fs_;
+    }
+  }
+  const std::string solver_name = ildlt ? (split ? "SplitILDLTPCG" : "ILDLTPCG")
+                                  : cfg.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG ? "SplitDCDMICC"
+                                  : split                                        ? "SplitICCPCG"
+                                                                                 : "ICCPCG";
+  const std::string prec_name = diag ? "Diagonal" : ildlt ? "ILDLT" : "ICC";
+  const SpOp A{h->a5, (int)n, nx, ny, h->G.px, h->G.py};
+  double *x = h->x, *r = h->r, *z = h->z, *p = h->p0, *ap = h->ap, *delta = h->y, *mask = h->p1;
+  auto proj = [&](double *v) -> dn_status { return project ? compact_subtract_mean(h, v) : DN_OK; };
+  auto precondition = [&]() -> dn_status {  // z = M^-1 r, projected
+    if (diag) {
+      k_diag_apply<<<nb, 256, 0, h->stream>>>(h->a5 + 2 * (size_t)n, r, z, n);
+      DN_TRY(check_launch(h, "k_diag_apply"));
+    } else {
+      DN_TRY(prec_apply(h, r, kind));
+    }
+    return proj(z);
+  };
+  k_interface_mask<<<nb, 256, 0, h->stream>>>(f[DN_F_C], std::tanh(cfg.analysis_interface_band_multiplier /
+                                                                    (2.0 * std::sqrt(2.0))), mask);
+  DN_TRY(check_launch(h, "k_interface_mask"));
+
+  // output paths (pressure_analysis.cpp:187-198)
+  const int snap_step = step + 1;
+  const double time = (double)snap_step * cfg.dt;
+  char stem_c[256];
+  std::snprintf(stem_c, sizeof stem_c, "%s_%s_step_%06d", cfg.name, source.c_str(), snap_step);
+  const fs::path dir = fs::path(cfg.output_dir) / cfg.name / "pressure_analysis";
+  const fs::path field_dir = dir / (std::string(stem_c) + "_fields");
+  const fs::path iter_path = dir / (std::string(stem_c) + "_pcg.csv");
+  try {
+    fs::create_directories(field_dir);
+  } catch (const std::exception &e) {
+    return fail(h, DN_ERR_INVALID_ARGUMENT, std::string("cannot create pressure analysis directory: ") + e.what());
+  }
+  FILE *it_out = std::fopen(iter_path.string().c_str(), "w");
+  if (!it_out) return fail(h, DN_ERR_INVALID_ARGUMENT, "cannot open pressure analysis iteration file: " + iter_path.string());
+  std::fputs("case_name,case_group,source_mode,step,time,grid_size,density_ratio,sigma,viscosity_ratio,solver_name,"
+             "preconditioner_name,max_iter,tolerance,initial_guess_type,iter,true_res_l2,rel_true_res_l2,"
+             "true_res_linf,precond_res,alpha_k,beta_k,q_k,interface_res_l2,bulk_res_l2,interface_res_fraction,"
+             "bulk_res_fraction\n", it_out);
+  const double sigma = cfg.surface_tension_multiplier == 0.0
+                           ? 0.0
+                           : cfg.surface_tension_multiplier / std::max(cfg.re * cfg.ca, 1.0e-30);
+  char grid_c[32];
+  std::snprintf(grid_c, sizeof grid_c, "%dx%d", nx, ny);
+  // the columns before `iter`, shared by every row and by the summary row
+  const std::string lead = std::string(cfg.name) + "," + cfg.analysis_case_group + "," + source + "," +
+                           std::to_string(snap_step) + "," + g17(time) + "," + grid_c + "," + g17(cfg.density_ratio) +
+                           "," + g17(sigma) + "," + g17(cfg.viscosity_ratio) + "," + solver_name + "," + prec_name +
+                           "," + std::to_string(cfg.poisson_iterations) + "," + g17(tol) + "," +
+                           cfg.analysis_initial_guess;
+  std::vector<double> hostv;
+  double prev_abs = 0.0, final_abs = 0.0, final_rel = 0.0;
+  int final_it = 0;
+  dn_status st = DN_OK;
+  // one CGMonitor call: the row of the iteration file and, at a key iteration, the residual field
+  auto monitor = [&](int it, double alpha, double beta, double absr, double relr, double precr) -> dn_status {
+    k_resid_stats<<<128, 256, 0, h->stream>>>(r, mask, n, h->partials);
+    DN_TRY(check_launch(h, "k_resid_stats"));
+    double q[3];
+    DN_TRY(host_partials(h, 3, 128, true, q));
+    const double il2 = std::sqrt(q[1]), bl2 = std::sqrt(q[2]);
+    const double qk = (it == 0 || prev_abs <= 0.0) ? 1.0 : absr / prev_abs;
+    std::fprintf(it_out, "%s,%d,%s,%s,%s,%s,%s,%s,%s,%s,%s,%s,%s\n", lead.c_str(), it, g17(absr).c_str(),
+                 g17(relr).c_str(), g17(q[0]).c_str(), g17(precr).c_str(), g17(alpha).c_str(), g17(beta).c_str(),
+                 g17(qk).c_str(), g17(il2).c_str(), g17(bl2).c_str(), g17(absr > 0.0 ? il2 / absr : 0.0).c_str(),
+                 g17(absr > 0.0 ? bl2 / absr : 0.0).c_str());
+    prev_abs = absr;
+    final_it = it;
+    final_abs = absr;
+    final_rel = relr;
+    if (keys.count(it)) {
+      DN_TRY(download(h, r, hostv, (size_t)n));
+      char name[64];
+      std::snprintf(name, sizeof name, "residual_iter_%06d.csv", it);
+      if (!write_field_csv(field_dir / name, hostv, nx, ny))
+        return fail(h, DN_ERR_INVALID_ARGUMENT, "cannot open pressure analysis field file: " + (field_dir / name).string());
+    }
+    return DN_OK;
+  };
+  // solve_preconditioned_cg (ch_sparse_krylov.hpp:515-660) from x = 0 with the monitor above
+  auto solve = [&]() -> dn_status {
+    double q[5];
+    DN_CUDA(h, cudaMemsetAsync(x, 0, n * sizeof(double), h->stream));
+    k_residual5<<<nb, 256, 0, h->stream>>>(A, h->b, x, r);
+    DN_TRY(check_launch(h, "k_residual5"));
+    DN_TRY(proj(r));
+    DN_TRY(dots4(h, h->b, h->b, r, r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+    const double rhs_norm = std::sqrt(std::max(q[0], 0.0));
+    double absr = std::sqrt(std::max(q[1], 0.0));
+    double relr = absr / std::max(rhs_norm, 1.0e-30);
+    if (relr < tol || absr < tol) return monitor(0, 0.0, 0.0, absr, relr, 0.0);
+    DN_TRY(precondition());
+    DN_TRY(dots4(h, r, z, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+    double rz_old = q[0];
+    if (!std::isfinite(rz_old) || rz_old <= 0.0)
+      return fail(h, DN_ERR_PCG_BREAKDOWN, "pcg preconditioner breakdown: non-positive r^T M^{-1} r");
+    DN_TRY(monitor(0, 0.0, 0.0, absr, relr, std::sqrt(std::max(rz_old, 0.0))));
+    DN_CUDA(h, cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    const int limit = std::max(1, cfg.poisson_iterations);
+    for (int it = 0; it < limit; ++it) {
+      k_spmv5<<<nb, 256, 0, h->stream>>>(A, p, ap);
+      DN_TRY(check_launch(h, "k_spmv5"));
+      DN_TRY(dots4(h, p, ap, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+      const double pap = q[0];
+      if (!std::isfinite(pap) || std::fabs(pap) < 1.0e-30)
+        return fail(h, DN_ERR_PCG_BREAKDOWN, "pcg breakdown: p^T A p is invalid");
+      const double alpha = rz_old / pap;
+      k_x_step<<<nb, 256, 0, h->stream>>>(x, p, delta, n, alpha);
+      DN_TRY(check_launch(h, "k_x_step"));
+      k_sub_scaled<<<nb, 256, 0, h->stream>>>(r, ap, n, alpha);
+      DN_TRY(check_launch(h, "k_sub_scaled"));
+      DN_TRY(proj(x));
+      DN_TRY(proj(r));
+      DN_TRY(dots4(h, r, r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+      absr = std::sqrt(std::max(q[0], 0.0));
+      relr = absr / std::max(rhs_norm, 1.0e-30);
+      if (relr < tol || absr < tol) return monitor(it + 1, alpha, 0.0, absr, relr, 0.0);
+      DN_TRY(precondition());
+      DN_TRY(dots4(h, r, z, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, q));
+      const double rz_new = q[0];
+      if (!std::isfinite(rz_new) || rz_new <= 0.0)
+        return fail(h, DN_ERR_PCG_BREAKDOWN, "pcg preconditioner breakdown: non-positive new r^T M^{-1} r");
+      const double beta = rz_new / rz_old;
+      DN_TRY(monitor(it + 1, alpha, beta, absr, relr, std::sqrt(std::max(rz_new, 0.0))));
+      k_p_update<<<nb, 256, 0, h->stream>>>(p, z, n, beta);
+      DN_TRY(check_launch(h, "k_p_update"));
+      DN_TRY(proj(p));
+      rz_old = rz_new;
+    }
+    return DN_OK;
+  };
+  // the fields written before the solve: rhs, interface mask, rho_mid, phi (pressure_analysis.cpp:213-227)
+  std::vector<double> cells((size_t)n), full;
+  auto write = [&](const char *name, const std::vector<double> &v) -> dn_status {
+    if (!write_field_csv(field_dir / name, v, nx, ny))
+      return fail(h, DN_ERR_INVALID_ARGUMENT, "cannot open pressure analysis field file: " + (field_dir / name).string());
+    return DN_OK;
+  };
+  if (st == DN_OK) st = download(h, h->b, hostv, (size_t)n);
+  if (st == DN_OK) st = write("rhs.csv", hostv);
+  if (st == DN_OK) st = download(h, mask, hostv, (size_t)n);
+  if (st == DN_OK) st = write("interface_mask.csv", hostv);
+  if (st == DN_OK) st = download(h, f[DN_F_RHO_MID].d, full, f[DN_F_RHO_MID].size());
+  if (st == DN_OK) {
+    const Fv &rm = f[DN_F_RHO_MID];
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) cells[(size_t)i * ny + j] = full[(size_t)(i + rm.g) * rm.pitch() + (j + rm.g)];
+    st = write("rho_mid.csv", cells);
+  }
+  if (st == DN_OK) st = download(h, f[DN_F_C].d, full, f[DN_F_C].size());
+  if (st == DN_OK) {
+    const Fv &cf = f[DN_F_C];
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j)
+        cells[(size_t)i * ny + j] = 2.0 * full[(size_t)(i + cf.g) * cf.pitch() + (j + cf.g)] - 1.0;
+    st = write("phi.csv", cells);
+  }
+  if (st == DN_OK) st = solve();
+  std::fclose(it_out);
+  if (st != DN_OK) return st;
+  // the final residual b - A x of the last monitored iterate, the pressure means and the summary row
+  k_residual5<<<nb, 256, 0, h->stream>>>(A, h->b, x, r);
+  DN_TRY(check_launch(h, "k_residual5"));
+  DN_TRY(proj(r));
+  DN_TRY(download(h, r, hostv, (size_t)n));
+  DN_TRY(write("residual_final.csv", hostv));
+  double sums[1];
+  k_vec_sum<<<128, 256, 0, h->stream>>>(h->b, n, h->partials);
+  DN_TRY(check_launch(h, "k_vec_sum"));
+  DN_TRY(host_partials(h, 1, 128, false, sums));
+  const double rhs_sum = sums[0];
+  k_vec_sum<<<128, 256, 0, h->stream>>>(x, n, h->partials);
+  DN_TRY(check_launch(h, "k_vec_sum"));
+  DN_TRY(host_partials(h, 1, 128, false, sums));
+  const double mean_before = sums[0] / (double)n;
+  double mean_after = mean_before;
+  if (project) {
+    DN_TRY(proj(x));
+    k_vec_sum<<<128, 256, 0, h->stream>>>(x, n, h->partials);
+    DN_TRY(check_launch(h, "k_vec_sum"));
+    DN_TRY(host_partials(h, 1, 128, false, sums));
+    mean_after = sums[0] / (double)n;
+  }
+  const fs::path summary = dir / "summary.csv";
+  const bool exists = fs::exists(summary);
+  FILE *sp = std::fopen(summary.string().c_str(), "a");
+  if (!sp) return fail(h, DN_ERR_INVALID_ARGUMENT, "cannot open pressure analysis summary file: " + summary.string());
+  if (!exists)
+    std::fputs("case_name,case_group,source_mode,step,time,grid_size,density_ratio,sigma,viscosity_ratio,solver_name,"
+               "preconditioner_name,max_iter,tolerance,initial_guess_type,rhs_volume_mean,rhs_sum,"
+               "pressure_mean_before_fix,pressure_mean_after_fix,nullspace_treatment,final_iter,final_true_res_l2,"
+               "final_rel_true_res_l2\n", sp);
+  std::fprintf(sp, "%s,%s,%s,%s,%s,%s,%d,%s,%s\n", lead.c_str(), g17(rhs_sum / (double)n).c_str(), g17(rhs_sum).c_str(),
+               g17(mean_before).c_str(), g17(mean_after).c_str(), cfg.analysis_nullspace_treatment, final_it,
+               g17(final_abs).c_str(), g17(final_rel).c_str());
+  std::fclose(sp);
   return DN_OK;
 }
 
@@ -1795,18 +2130,17 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
       if (h->sw5_blocks_max == 0) h->sw5 = 0;
     }
   }
-  if (c.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG) {
-    // the direction history, and the preconditioner-only kernel's shared-memory limit (as k_pcg's)
+  if (c.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG) {  // the direction history
     h->dcdm_keep = std::max(c.dcdm_max_stored_directions, std::max(c.dcdm_history_size, 1));
     A(dalloc(h, &h->dcdm_dirs, (size_t)h->dcdm_keep * h->n));
     A(dalloc(h, &h->dcdm_adirs, (size_t)h->dcdm_keep * h->n));
     if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
-    const int optin = h->smem_optin;
-    for (const void *k : {(const void *)k_prec_apply<3>, (const void *)k_prec_apply<4>}) {
-      cudaFuncAttributes fa{};
-      cudaFuncGetAttributes(&fa, k);
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
-    }
+  }
+  // the preconditioner-only kernel (DCDM directions, the pressure analysis) may use shared memory as k_pcg does
+  for (const void *k : {(const void *)k_prec_apply<3>, (const void *)k_prec_apply<4>}) {
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin - (int)fa.sharedSizeBytes);
   }
   if (c.precision == DN_PRECISION_MIXED) {
     A(dalloc(h, &h->fa5, 5 * h->n));
@@ -2161,6 +2495,11 @@ dn_status dn_load_restart(dn_handle *h, const char *path, int *step) {
   return DN_OK;
 }
 
+dn_status dn_pressure_analysis(dn_handle *h, int step, const char *source_mode) {
+  if (!h || !source_mode || step < 0) return DN_ERR_INVALID_ARGUMENT;
+  return pressure_analysis(h, step, source_mode);
+}
+
 // Launch-shape autotuner of the pressure PCG: times one pressure solve of the handle's current state (its
 // u*, v*, rho_mid, p, p_prev, as a step leaves them) for each candidate (rows per CTA of the SpMV / update
 // phases x sweep warps per CTA of the staged wavefront) and keeps the fastest on the handle.
@@ -2373,7 +2712,16 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
   cudaEventRecord(h->ev[1], h->stream);
   DN_TRY(momentum(h, step, rep));
   cudaEventRecord(h->ev[2], h->stream);
+  // the pressure analysis at its trigger step: frozen before the solve (solver.cpp:270), online after it
+  // for the PCG schemes (pressure.cpp:1078-1087)
+  const dn_config &c = h->cfg;
+  const bool analyse = c.analysis_enabled && step + 1 == c.analysis_trigger_step;
+  if (analyse && (c.analysis_mode == DN_ANALYSIS_FROZEN || c.analysis_mode == DN_ANALYSIS_BOTH))
+    DN_TRY(pressure_analysis(h, step, "frozen"));
   DN_TRY(pressure(h, step, rep));
+  if (analyse && (c.analysis_mode == DN_ANALYSIS_ONLINE || c.analysis_mode == DN_ANALYSIS_BOTH) &&
+      c.pressure_scheme != DN_P_JACOBI)
+    DN_TRY(pressure_analysis(h, step, "online"));
   cudaEventRecord(h->ev[3], h->stream);
   DN_TRY(correct(h, step, rep));
   cudaEventRecord(h->ev[4], h->stream);

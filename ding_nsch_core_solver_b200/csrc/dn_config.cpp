@@ -110,6 +110,16 @@ extern "C" void dn_config_default(dn_config *c) {
   c->dcdm_restart_interval = 0;
   c->pcg_rows_per_cta = 0;     // 512
   c->sweep_warps_per_cta = 0;  // as many as the shared memory holds, up to 4
+  c->analysis_enabled = 0;     // config.hpp:53-133
+  c->analysis_mode = DN_ANALYSIS_OFF;
+  c->analysis_trigger_step = 1;
+  c->analysis_interface_band_multiplier = 2.0;
+  std::snprintf(c->name, sizeof c->name, "%s", "unnamed");
+  std::snprintf(c->output_dir, sizeof c->output_dir, "%s", "output");
+  c->analysis_case_group[0] = '\0';
+  std::snprintf(c->analysis_initial_guess, sizeof c->analysis_initial_guess, "%s", "zero");
+  std::snprintf(c->analysis_nullspace_treatment, sizeof c->analysis_nullspace_treatment, "%s", "zero_mean_projection");
+  std::snprintf(c->analysis_spectrum_iterations, sizeof c->analysis_spectrum_iterations, "%s", "0,1,2,5,10,20,final");
 }
 
 extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err, size_t err_len) {
@@ -217,6 +227,25 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
     geti("dcdm_history_size", cfg->dcdm_history_size);
     geti("dcdm_max_stored_directions", cfg->dcdm_max_stored_directions);
     geti("dcdm_restart_interval", cfg->dcdm_restart_interval);
+    auto gets = [&](const char *k, char *dst, size_t cap) {
+      if (!kv.count(k)) return;
+      if (kv[k].size() >= cap) throw std::runtime_error(std::string(k) + " is too long");
+      std::snprintf(dst, cap, "%s", kv[k].c_str());
+    };
+    gets("name", cfg->name, sizeof cfg->name);
+    gets("output_dir", cfg->output_dir, sizeof cfg->output_dir);
+    gets("analysis_case_group", cfg->analysis_case_group, sizeof cfg->analysis_case_group);
+    gets("analysis_initial_guess", cfg->analysis_initial_guess, sizeof cfg->analysis_initial_guess);
+    gets("analysis_nullspace_treatment", cfg->analysis_nullspace_treatment, sizeof cfg->analysis_nullspace_treatment);
+    gets("analysis_spectrum_iterations", cfg->analysis_spectrum_iterations, sizeof cfg->analysis_spectrum_iterations);
+    getb("analysis_enabled", cfg->analysis_enabled);
+    geti("analysis_trigger_step", cfg->analysis_trigger_step);
+    getd("analysis_interface_band_multiplier", cfg->analysis_interface_band_multiplier);
+    if (kv.count("analysis_mode")) {  // analysis_mode_enabled, pressure_analysis.cpp:126-137
+      const std::string m = lower(kv["analysis_mode"]);
+      cfg->analysis_mode = m == "both" ? DN_ANALYSIS_BOTH : m == "online" ? DN_ANALYSIS_ONLINE
+                           : m == "frozen" ? DN_ANALYSIS_FROZEN : DN_ANALYSIS_OFF;
+    }
     geti("pcg_rows_per_cta", cfg->pcg_rows_per_cta);
     geti("sweep_warps_per_cta", cfg->sweep_warps_per_cta);
     if (kv.count("dcdm_direction_mode")) {  // pressure.cpp:383-395

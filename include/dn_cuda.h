@@ -87,7 +87,21 @@ typedef struct {
   int pcg_rows_per_cta;            /* launch shape of the pressure PCG: rows per CTA of its SpMV / update
                                       phases (0: 512) -- see dn_autotune_pressure */
   int sweep_warps_per_cta;         /* sweep warps per CTA of the staged wavefront (0: as many as fit, up to 4) */
+  /* pressure analysis (config.hpp:36-133; run_pressure_analysis_from_snapshot, pressure_analysis.cpp:156-328) */
+  int analysis_enabled;            /* analysis_enabled */
+  int analysis_mode;               /* dn_analysis_mode, from the analysis_mode string */
+  int analysis_trigger_step;       /* the step (1-based, current_step_index + 1) that is analysed */
+  double analysis_interface_band_multiplier;
+  char name[128];                  /* case name: output_dir/name/pressure_analysis/name_<mode>_step_NNNNNN_* */
+  char output_dir[512];
+  char analysis_case_group[128];
+  char analysis_initial_guess[64];
+  char analysis_nullspace_treatment[64];
+  char analysis_spectrum_iterations[256]; /* iterations whose residual field is written ("final" ignored) */
 } dn_config;
+
+/* analysis_mode: "online" after the step's pressure solve, "frozen" before it, "both"; anything else off */
+typedef enum { DN_ANALYSIS_OFF = 0, DN_ANALYSIS_ONLINE = 1, DN_ANALYSIS_FROZEN = 2, DN_ANALYSIS_BOTH = 3 } dn_analysis_mode;
 
 /* Fields (Solver members, src/core/coupled/solver.hpp:64-91). */
 typedef enum {
@@ -235,6 +249,17 @@ dn_status dn_explicit_operator(dn_handle *h, const double *c, const double *u, c
  * derivative is taken on the side the forward evaluation lies on.  DEVICE buffers. */
 dn_status dn_explicit_operator_adjoint(dn_handle *h, const double *c, const double *u, const double *v,
                                        const double *gE, double *c_bar, double *u_bar, double *v_bar);
+
+/* ---- pressure analysis ------------------------------------------------------------------------------------ */
+/* Solver::run_pressure_analysis_from_snapshot (pressure_analysis.cpp:156-328) on the handle's current state,
+ * whose step index is `step` (the files carry step + 1, as the reference's snapshot does): the pressure system
+ * as the configured scheme assembles it, a PCG from x = 0 with ICC (ILDLT for the ILDLT schemes; the diagonal
+ * when the factor fails), and under output_dir/name/pressure_analysis/ the per-iteration file
+ * <name>_<source_mode>_step_NNNNNN_pcg.csv, the fields rhs, interface_mask, rho_mid, phi, residual_iter_NNNNNN
+ * and residual_final in <stem>_fields/, and one appended row of summary.csv.  dn_step runs it itself at
+ * analysis_trigger_step when analysis_enabled: "frozen" before the pressure solve, "online" after it (PCG
+ * schemes only), as the reference's step does (solver.cpp:270, pressure.cpp:1078-1087). */
+dn_status dn_pressure_analysis(dn_handle *h, int step, const char *source_mode);
 
 /* ---- launch-shape autotuning ----------------------------------------------------------------------------- */
 /* No counterpart in the reference.  Times one pressure solve of the handle's current state (u*, v*, rho_mid,

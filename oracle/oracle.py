@@ -218,6 +218,8 @@ def _load(impl: str):
     }
     if impl == "reference":
         sig["time_steps"] = (C.c_double, [vp, C.c_int, C.c_int])
+        sig["pressure_analysis"] = (C.c_int, [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                              C.c_char_p, C.c_double])
     else:
         sig["advection"] = (C.c_int, [vp, dp, dp, dp, dp])
         sig["explicit_operator"] = (C.c_int, [vp, dp, dp, dp, dp])
@@ -308,6 +310,13 @@ class OracleSolver:
     def refresh_derived(self):
         """Rebuild BC ghosts, materials and mu from the state fields, as a restart load does (io.cpp:412-436)."""
         self._check(self._f["refresh_derived"](self._h))
+
+    def pressure_analysis(self, step: int, source_mode: str, output_dir: str, name: str, case_group: str = "",
+                          spectrum_iterations: str = "0,1,2,5,10,20,final", band: float = 2.0):
+        """The reference's pressure analysis files of the current state (reference build only)."""
+        self._check(self._f["pressure_analysis"](self._h, int(step), source_mode.encode(), output_dir.encode(),
+                                                 name.encode(), case_group.encode(), spectrum_iterations.encode(),
+                                                 float(band)))
 
     def ch_linear_solve(self, rhs: np.ndarray, alpha0: float, c_state: np.ndarray):
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)

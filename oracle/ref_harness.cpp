@@ -9,6 +9,22 @@
 #include <cstring>
 #include <exception>
 #include <string>
+// The standard headers the reference's headers pull in come first, so that the `private` redefinition below
+// reaches only the reference's own classes: standard classes compiled with it would lay out differently
+// from the same classes in the reference's translation units.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <map>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <vector>
 
 #define private public
 #include "core/coupled/solver.hpp"
@@ -273,6 +289,23 @@ int ref_ch_linear_solve(void *hp, const double *rhs_field, double alpha0, double
     std::memcpy(cs.data.data(), c_state, cs.data.size() * sizeof(double));
     s.solve_phase_linear_system_eq25(rhs, alpha0, 0.0, cs, *iterate_residual, *equation_residual);
     std::memcpy(c_state, cs.data.data(), cs.data.size() * sizeof(double));
+  });
+}
+
+// Solver::run_pressure_analysis_from_snapshot (pressure_analysis.cpp:156-328) on the current state, step index
+// `step`, with the analysis settings that the config struct does not carry set here.
+int ref_pressure_analysis(void *hp, int step, const char *source_mode, const char *output_dir, const char *name,
+                          const char *case_group, const char *spectrum_iterations, double band) {
+  auto *h = static_cast<RefHandle *>(hp);
+  return guarded(h, [&] {
+    ding::Solver &s = *h->solver;
+    s.cfg_.output_dir = output_dir;
+    s.cfg_.name = name;
+    s.cfg_.analysis_case_group = case_group;
+    s.cfg_.analysis_spectrum_iterations = spectrum_iterations;
+    s.cfg_.analysis_interface_band_multiplier = band;
+    s.current_step_index_ = step;
+    s.run_pressure_analysis_from_snapshot(s.make_pressure_analysis_snapshot(source_mode));
   });
 }
 
