@@ -1085,8 +1085,8 @@ dn_status ch_linear_solve(dn_handle *h, double alpha0, dn_report *rep, double *i
   DN_TRY(s);
   rep->ch_iterations = (int)out[0];
   *iter_res = out[3];
-  // equation residual ||b - A x|| / ||b||
-  const int nb = 128;
+  // equation residual ||b - A x|| / ||b||: enough CTAs to keep every SM's loads in flight
+  const int nb = 1024;
   k_residual_partials<13><<<nb, 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, h->b,
                                                       h->x, h->partials);
   DN_TRY(check_launch(h, "k_residual_partials"));

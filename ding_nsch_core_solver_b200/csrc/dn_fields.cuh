@@ -9,11 +9,13 @@
 
 namespace dn {
 
+// One thread per interior cell, j fastest.  Grids are capped at 2^30 cells (dn_create), so the index math
+// stays in 32-bit unsigned arithmetic: a 64-bit division is a long software sequence on the GPU.
 #define DN_FOR_INTERIOR(F)                                                          \
-  const long long _n = (long long)(F).nx * (F).ny;                                  \
-  const long long _t = (long long)blockIdx.x * blockDim.x + threadIdx.x;            \
+  const unsigned _n = (unsigned)(F).nx * (unsigned)(F).ny;                          \
+  const unsigned _t = blockIdx.x * blockDim.x + threadIdx.x;                        \
   if (_t >= _n) return;                                                             \
-  const int i = (int)(_t / (F).ny), j = (int)(_t % (F).ny);
+  const int i = (int)(_t / (unsigned)(F).ny), j = (int)(_t - (unsigned)i * (unsigned)(F).ny);
 
 // ------------------------------------------------------------------------------------------------------
 // Boundary conditions (operators.cpp:130-289).  The reference fills x-ghost layers for interior j and then

@@ -1073,7 +1073,7 @@ __global__ void k_residual_partials(SpOp A, const double *b, const double *x, do
   __shared__ double sh[8 * 32];
   double v[2] = {0.0, 0.0};
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(r / A.ny), j = (int)(r % A.ny);
+    const int i = (int)((unsigned)r / (unsigned)A.ny), j = (int)((unsigned)r - (unsigned)i * (unsigned)A.ny);
     const double d = b[r] - spmv_row<S>(A, x, i, j);
     v[0] += d * d;
     v[1] += b[r] * b[r];
