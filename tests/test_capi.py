@@ -98,3 +98,11 @@ def test_create_rejects_periodic_bc(lib):
     with pytest.raises(capi.DnError) as ei:
         capi.Solver("nx = 32\nny = 32\nperiodic_x = true\nu_bc_left_type = dirichlet\n")
     assert "cannot be set when the direction is periodic" in str(ei.value)
+
+
+def test_create_rejects_grids_below_eight_cells(lib):
+    """The staged sweeps and the 13-point CH operator need at least 8 cells each way; smaller grids are
+    refused before any device work (dn_create), with an UNSUPPORTED status, never run on the CPU."""
+    with pytest.raises(capi.DnError) as ei:
+        capi.Solver("nx = 6\nny = 6\nperiodic_x = false\nperiodic_y = false\n")
+    assert ei.value.status == 10 and "nx, ny >= 8" in str(ei.value)

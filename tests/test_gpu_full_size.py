@@ -1,0 +1,58 @@
+"""The 1024x2048 rising bubble at full size, where the oracle would take hours: checked through properties
+that do not depend on size.
+
+- every solve reaches its tolerance inside its iteration cap;
+- the CH update conserves the mass of c (flux form, no-flux walls) to the solver tolerance;
+- two handles stepped from the same state end bitwise equal (fixed reduction orders, fixed hand-over);
+- the mixed-precision form stays within 1e-8 (rel-L2) of the plain FP64 form on p, u, v.
+"""
+import numpy as np
+import pytest
+
+from bench import initial_state, workload_cfg
+from ding_nsch_core_solver_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+GRID = (1024, 2048)
+STEPS = 2
+
+
+def _solver(cfg):
+    s = capi.Solver(cfg)
+    for n, a in initial_state(cfg).items():
+        s.set_field(n, a)
+    s.refresh_derived()
+    s.set_initial_mass(s.compute_mass("c"))
+    return s
+
+
+def _rel(a, b, g):
+    a, b = a[g:-g, g:-g], b[g:-g, g:-g]
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_full_size_properties():
+    cfg = workload_cfg(GRID)
+    a, b = _solver(cfg), _solver(cfg)
+    m = _solver(dict(cfg, precision="mixed"))
+    try:
+        mass0 = a.compute_mass("c")
+        for k in range(STEPS):
+            ra, rb, rm = a.step(k), b.step(k), m.step(k)
+            assert ra == rb, (k, ra, rb)
+            assert ra["pressure_iterations"] < cfg["poisson_iterations"]
+            assert ra["pressure_residual"] < cfg["pressure_tolerance"]
+            assert ra["ch_iterations"] < cfg["ch_inner_iterations"]
+            assert rm["pressure_iterations"] > 0
+            drift = abs(a.compute_mass("c") - mass0) / abs(mass0)
+            assert drift < 1e-9, (k, drift)
+        for n in capi.FIELDS:
+            assert np.array_equal(a.get_field(n), b.get_field(n), equal_nan=True), n
+        g = cfg["ghost"]
+        for n in ("p", "u", "v"):
+            err = _rel(m.get_field(n), a.get_field(n), g)
+            assert err <= 1e-8, (n, err)
+    finally:
+        for s in (a, b, m):
+            s.close()

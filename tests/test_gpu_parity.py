@@ -82,6 +82,16 @@ CASES = {
     "advection_only_zalesak": unit(mode="advection_only", velocity_profile="solid_body_rotation",
                                    angular_velocity=2 * math.pi, phase_initializer="zalesak_disk",
                                    interface_radius=0.3),
+    # edge shapes: odd sizes (ragged column groups in both directions), a periodic-x channel narrower than two
+    # sweep groups (the global-memory wavefront with the wrap), a wide short box, the smallest box (8x8)
+    "odd_walls_split_icpcg": unit(nx=37, ny=29, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
+                                  body_force_y=-0.98, dt=1e-4),
+    "thin_channel_x_icpcg": unit(nx=8, ny=64, periodic_x=True, periodic_y=False, pressure_scheme="icpcg",
+                                 top_wall_velocity_x=0.5, bottom_wall_velocity_x=-0.5, dt=1e-4),
+    "wide_short_walls_ildlt": unit(nx=100, ny=10, periodic_x=False, periodic_y=False, pressure_scheme="ildlt_pcg",
+                                   dt=1e-4),
+    "tiny_walls_split_ildlt": unit(nx=8, ny=8, periodic_x=False, periodic_y=False, pressure_scheme="split_ildlt_pcg",
+                                   dt=1e-4),
 }
 
 
