@@ -555,64 +555,120 @@ __device__ void apply_levels(const PcgArgs &P, double m_r, double (&acc)[3]) {
 
 // Level-scheduled forward+backward application of the 13-point factor (y not periodic) by one CTA, from
 // the ordered rows (K entries each): the values of the last kLvlRing levels stay in a shared ring (`ring`,
-// kLvlRing x nx doubles), so a level reads its neighbours from shared memory; every row does the same six multiply-subtract
-// steps, the padded ones subtract exact zeros.  Same arithmetic and order as apply_levels.
+// kLvlRing x nx doubles), so a level reads its neighbours from shared memory; every row does the same six
+// multiply-subtract steps, the padded ones subtract exact zeros.  Same arithmetic and order as apply_levels.
+//
+// Every stored neighbour of this path is at most 4 levels away at a line below 65536 (the ring is built
+// only then), so it sits in the ring; the entries with src < 0 are the zero padding, whose column is the
+// row itself, and they read the row's own vector entry as it stands before the row is written.
+//
+// The per-level chain is a memory round trip for the row's coefficients, then the ring reads, the six
+// steps and a barrier.  Each thread therefore issues the loads of its first row of level l + 1 (which no
+// thread writes before that level) before it computes level l, so the round trip overlaps level l's
+// compute and barrier; further rows of a wide level are loaded as they come.
+template <int K>
+struct LevelRow {
+  long long r;   // row index, or -1: the thread has no row at that level
+  double v[K];   // lval / uval
+  int src[K];    // lsrc / usrc
+  double self;   // y[r] (forward) / z[r] (backward): the padding's value
+  double a, b;   // forward: r[r], dinv[r];  backward: y[r], dinv[r]
+};
+
+template <int K, bool FWD>
+__device__ __forceinline__ void load_level_row(const PcgArgs &P, int lev, int i, LevelRow<K> &q) {
+  const int n = P.A.n, ny = P.A.ny;
+  const Rows13 &R = P.rows13;
+  const long long r = (long long)i * ny + (lev - 2 * i);
+  q.r = r;
+#pragma unroll
+  for (int p = 0; p < K; ++p) {
+    q.v[p] = FWD ? R.lval[(size_t)p * n + r] : R.uval[(size_t)p * n + r];
+    q.src[p] = FWD ? R.lsrc[(size_t)p * n + r] : R.usrc[(size_t)p * n + r];
+  }
+  q.self = FWD ? P.y[r] : P.z[r];
+  q.a = FWD ? P.r[r] : P.y[r];
+  q.b = P.dinv[r];
+}
+
+template <int K, bool FWD>
+__device__ __forceinline__ void level_row_of(const PcgArgs &P, int lev, int first, LevelRow<K> &q) {
+  const int nx = P.A.nx, ny = P.A.ny;
+  const int i0 = max(0, (lev - (ny - 1) + 1) / 2), i1 = min(nx - 1, lev / 2);
+  const int i = i0 + first;
+  if (i <= i1)
+    load_level_row<K, FWD>(P, lev, i, q);
+  else
+    q.r = -1;
+}
+
 template <int K>
 __device__ void apply_levels13_ring(const PcgArgs &P, double m_r, double (&acc)[3], double *ring) {
-  const SpOp &A = P.A;
-  const int n = A.n, nx = A.nx, ny = A.ny;
-  const Rows13 &R = P.rows13;
+  const int nx = P.A.nx, ny = P.A.ny;
   const int nlev = 2 * (nx - 1) + ny;
   const bool icc = P.prec == kPrecICC;
+  // forward: y = L^-1 (r - m_r), scaled by dinv for ICC
+  auto fwd_row = [&](int lev, int i, const LevelRow<K> &q) {
+    double yc[K];
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+      const int src = q.src[p];
+      const int off = src >= 0 ? ((lev - (src >> 16)) & (kLvlRing - 1)) * nx + (src & 0xffff) : 0;
+      const double from_ring = ring[off];
+      yc[p] = src >= 0 ? from_ring : q.self;
+    }
+    double sum = q.a - m_r;
+#pragma unroll
+    for (int p = 0; p < K; ++p) sum -= q.v[p] * yc[p];
+    const double yv = icc ? sum * q.b : sum;
+    P.y[q.r] = yv;
+    ring[(lev & (kLvlRing - 1)) * nx + i] = yv;
+  };
+  LevelRow<K> nxt;
+  level_row_of<K, true>(P, 0, threadIdx.x, nxt);
   for (int lev = 0; lev < nlev; ++lev) {
     const int i0 = max(0, (lev - (ny - 1) + 1) / 2), i1 = min(nx - 1, lev / 2);
-    for (int i = i0 + (int)threadIdx.x; i <= i1; i += blockDim.x) {
-      const long long r = (long long)i * ny + (lev - 2 * i);
-      double lv[K], yc[K];
-#pragma unroll
-      for (int p = 0; p < K; ++p) {
-        lv[p] = R.lval[(size_t)p * n + r];
-        // both candidate loads stay in bounds (the offset is clamped), whether or not the compiler issues
-        // them unconditionally and selects
-        const int src = R.lsrc[(size_t)p * n + r];
-        const int off = src >= 0 ? ((lev - (src >> 16)) & (kLvlRing - 1)) * nx + (src & 0xffff) : 0;
-        const double from_ring = ring[off];
-        const double from_vec = P.y[R.lcol[(size_t)p * n + r]];
-        yc[p] = src >= 0 ? from_ring : from_vec;
-      }
-      double sum = P.r[r] - m_r;
-#pragma unroll
-      for (int p = 0; p < K; ++p) sum -= lv[p] * yc[p];
-      const double yv = icc ? sum * P.dinv[r] : sum;
-      P.y[r] = yv;
-      ring[(lev & (kLvlRing - 1)) * nx + i] = yv;
+    const LevelRow<K> cur = nxt;
+    if (lev + 1 < nlev) level_row_of<K, true>(P, lev + 1, threadIdx.x, nxt);
+    if (cur.r >= 0) fwd_row(lev, i0 + (int)threadIdx.x, cur);
+    for (int i = i0 + (int)threadIdx.x + (int)blockDim.x; i <= i1; i += blockDim.x) {
+      LevelRow<K> q;
+      load_level_row<K, true>(P, lev, i, q);
+      fwd_row(lev, i, q);
     }
     __syncthreads();
   }
+  // backward: z = L^-T y (ICC: D^-1 scaling of the result; LDLT: of the input)
+  auto bwd_row = [&](int lev, int i, const LevelRow<K> &q) {
+    double zc[K];
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+      const int src = q.src[p];
+      const int off = src >= 0 ? ((lev + (src >> 16)) & (kLvlRing - 1)) * nx + (src & 0xffff) : 0;
+      const double from_ring = ring[off];
+      zc[p] = src >= 0 ? from_ring : q.self;
+    }
+    double sum = icc ? q.a : q.a * q.b;
+#pragma unroll
+    for (int p = 0; p < K; ++p) sum -= q.v[p] * zc[p];
+    const double zv = icc ? sum * q.b : sum;
+    P.z[q.r] = zv;
+    ring[(lev & (kLvlRing - 1)) * nx + i] = zv;
+    const double rv = P.r[q.r] - m_r;
+    acc[0] += zv;
+    acc[1] += rv * zv;
+    acc[2] += rv;
+  };
+  level_row_of<K, false>(P, nlev - 1, threadIdx.x, nxt);
   for (int lev = nlev - 1; lev >= 0; --lev) {
     const int i0 = max(0, (lev - (ny - 1) + 1) / 2), i1 = min(nx - 1, lev / 2);
-    for (int i = i0 + (int)threadIdx.x; i <= i1; i += blockDim.x) {
-      const long long r = (long long)i * ny + (lev - 2 * i);
-      double uv[K], zc[K];
-#pragma unroll
-      for (int p = 0; p < K; ++p) {
-        uv[p] = R.uval[(size_t)p * n + r];
-        const int src = R.usrc[(size_t)p * n + r];
-        const int off = src >= 0 ? ((lev + (src >> 16)) & (kLvlRing - 1)) * nx + (src & 0xffff) : 0;
-        const double from_ring = ring[off];
-        const double from_vec = P.z[R.ucol[(size_t)p * n + r]];
-        zc[p] = src >= 0 ? from_ring : from_vec;
-      }
-      double sum = icc ? P.y[r] : P.y[r] * P.dinv[r];
-#pragma unroll
-      for (int p = 0; p < K; ++p) sum -= uv[p] * zc[p];
-      const double zv = icc ? sum * P.dinv[r] : sum;
-      P.z[r] = zv;
-      ring[(lev & (kLvlRing - 1)) * nx + i] = zv;
-      const double rv = P.r[r] - m_r;
-      acc[0] += zv;
-      acc[1] += rv * zv;
-      acc[2] += rv;
+    const LevelRow<K> cur = nxt;
+    if (lev > 0) level_row_of<K, false>(P, lev - 1, threadIdx.x, nxt);
+    if (cur.r >= 0) bwd_row(lev, i0 + (int)threadIdx.x, cur);
+    for (int i = i0 + (int)threadIdx.x + (int)blockDim.x; i <= i1; i += blockDim.x) {
+      LevelRow<K> q;
+      load_level_row<K, false>(P, lev, i, q);
+      bwd_row(lev, i, q);
     }
     __syncthreads();
   }
