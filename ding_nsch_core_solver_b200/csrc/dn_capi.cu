@@ -3118,8 +3118,10 @@ namespace {
 
 constexpr int kStaticMaxDevices = 64;
 
-// Per device: the device address of g_pressure_scratch (the name is only a host-side stand-in) and the
-// launch limits of the PCG kernels, resolved once with that device current.
+// Per device: the launch limits of the PCG kernels, resolved once with that device current.  The device
+// address of g_pressure_scratch (the name is only a host-side stand-in) is not cached here: it is resolved
+// by cudaGetSymbolAddress on every call, so that a context that was destroyed and re-created (for instance
+// after cudaDeviceReset, which loads the module again) never sees a stale address.
 struct StaticDevice {
   bool ready;
   char *base;
@@ -3191,19 +3193,18 @@ StaticLayout static_layout(int nx, int ny, int g) {
   return L;
 }
 
-// Set-up of the current device (first call on it): resolve the array's device address and the launch
-// limits.  Occupancy queries and attribute calls allocate nothing.
+// Set-up of the current device: the array's device address (every call) and the launch limits (first
+// call on the device).  Symbol lookups, occupancy queries and attribute calls allocate nothing.
 dn_status static_setup(int device, StaticDevice *out, char *err, size_t err_len) {
   std::lock_guard<std::mutex> lock(g_static_mu);
   StaticDevice &d = g_static_dev[device];
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_pressure_scratch);
+  if (e != cudaSuccess)
+    return static_fail(err, err_len, DN_ERR_CUDA, "cudaGetSymbolAddress(g_pressure_scratch): %s",
+                       cudaGetErrorString(e));
   if (!d.ready) {
-    void *ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_pressure_scratch);
-    if (e != cudaSuccess)
-      return static_fail(err, err_len, DN_ERR_CUDA, "cudaGetSymbolAddress(g_pressure_scratch): %s",
-                         cudaGetErrorString(e));
     StaticDevice t{};
-    t.base = static_cast<char *>(ptr);
     DN_SCUDA(cudaDeviceGetAttribute(&t.num_sms, cudaDevAttrMultiProcessorCount, device));
     DN_SCUDA(cudaDeviceGetAttribute(&t.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa{};
@@ -3222,6 +3223,7 @@ dn_status static_setup(int device, StaticDevice *out, char *err, size_t err_len)
     d = t;
   }
   *out = d;
+  out->base = static_cast<char *>(ptr);
   return DN_OK;
 }
 
@@ -3303,6 +3305,13 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
     if (s != DN_OK) return s;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (st != nullptr) {  // the scratch address and the launch limits belong to the current device
+    int stream_device = -1;
+    DN_SCUDA(cudaStreamGetDevice(st, &stream_device));
+    if (stream_device != device)
+      return static_fail(err, err_len, DN_ERR_INVALID_ARGUMENT,
+                         "stream belongs to device %d, but device %d is current", stream_device, device);
+  }
 
   // grid and effective pressure BCs (operators.cpp:36-112), as a handle derives them
   Grid G;
@@ -3382,7 +3391,9 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
                        icc ? "ICC preconditioner construction failed" : "ILDLT preconditioner construction failed");
   if (dev_st != kDevOk) return static_device_status(dev_st, err, err_len);
 
-  // the persistent PCG kernel, launched with the shape a handle would use for this grid
+  // the persistent PCG kernel, launched with the default shape a handle would use for this grid and
+  // configuration (device_share included); shapes a handle picked with dn_autotune_pressure are not known
+  // here and are not reproduced (pass them as pcg_rows_per_cta / sweep_warps_per_cta)
   PcgArgs P{};
   P.A = A;
   P.l = dptr(L.l5);
@@ -3410,7 +3421,9 @@ dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double 
   P.nsweep = nsweep;
   P.warp_smem = 0;
   const long long rows_per_cta = c.pcg_rows_per_cta > 0 ? c.pcg_rows_per_cta : kPcgRowsPerCta;
-  int blocks = (int)std::min<long long>(D.num_sms, std::max<long long>(nsweep, (n + rows_per_cta - 1) / rows_per_cta));
+  const int cta_cap = std::max(1, D.num_sms / std::max(1, c.device_share));
+  int blocks = (int)std::min<long long>(cta_cap, std::max<long long>(nsweep, (n + rows_per_cta - 1) / rows_per_cta));
+  blocks = std::max(blocks, (nsweep + kBlock / 32 - 1) / (kBlock / 32));  // the wavefront warps' CTAs
   blocks = std::max(1, std::min(blocks, D.max_coop_blocks));
   // staged wavefront: sweep warps per CTA from the shared-memory budget, as dn_create chooses them
   int sw = 0, sw_blocks_max = 0;

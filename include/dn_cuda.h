@@ -199,11 +199,15 @@ dn_status dn_pressure_solve(dn_handle *h, int step, const double *u_star, const 
  * a loop that must not stall on cudaMalloc, code holding only raw device pointers and no handle).  No
  * handle and no allocation: inputs u_star, v_star, rho_mid, p, p_prev and the output p_corr are the
  * caller's DEVICE buffers in Field2D layout for `cfg`'s grid; the work runs on `stream` (a cudaStream_t,
- * NULL for the default stream), which is synchronised before return.  Scratch lives in one static device
- * array of DN_STATIC_SCRATCH_BYTES that every GPU loading the library holds until exit; grids that need
- * more return DN_ERR_UNSUPPORTED.  The first call on a device (with that device current) resolves the
- * array's address; make it before any stream capture.  All calls share the array, so calls overlapping
- * in time on one device race.  On error a message goes to `err` (`err_len` bytes, may be NULL). */
+ * NULL for the default stream), which must belong to the current device (else DN_ERR_INVALID_ARGUMENT).
+ * The call reads status words back and synchronises the stream in the middle of the solve and before it
+ * returns, so it cannot be used inside stream capture at all.  Scratch lives in one static device array
+ * of DN_STATIC_SCRATCH_BYTES that every GPU loading the library holds until exit; grids that need more
+ * return DN_ERR_UNSUPPORTED.  Each call looks the array's device address up with the current device's
+ * context (so a re-created context is safe).  All calls share the array, so calls overlapping in time on
+ * one device race.  The launch shape is the default a handle would use for `cfg` (device_share
+ * included); shapes picked by dn_autotune_pressure are not reproduced.  On error a message goes to `err`
+ * (`err_len` bytes, may be NULL). */
 dn_status dn_pressure_solve_static(const dn_config *cfg, int step, const double *u_star, const double *v_star,
                                    const double *rho_mid, const double *p, const double *p_prev, double *p_corr,
                                    void *stream, int *iterations, double *relative_residual, char *err,

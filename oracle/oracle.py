@@ -186,9 +186,10 @@ def to_struct(cfg: dict) -> Config:
 def build(force: bool = False) -> None:
     """Compile the checkers with oracle/Makefile (the reference harness only where the reference exists)."""
     targets = ["oracle"]
-    if os.path.isdir(os.environ.get("DN_REFERENCE", "/root/reference")):
+    ref = os.environ.get("DN_REFERENCE", "")
+    if ref and os.path.isdir(ref):
         targets.append("ref")
-    cmd = ["make", "-s", "-C", HERE] + (["-B"] if force else []) + targets
+    cmd = ["make", "-s", "-C", HERE] + (["-B"] if force else []) + targets + ([f"REFERENCE={ref}"] if ref else [])
     subprocess.run(cmd, check=True)
 
 

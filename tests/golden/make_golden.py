@@ -23,7 +23,9 @@ import tarfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DN_REFERENCE", "")
+if not REF or not os.path.isdir(REF):
+    sys.exit("give the reference tree as the argument or in DN_REFERENCE")
 RUN = os.path.join(REF, "176Result", "static_droplet_surface_tension_validation_128")
 TARBALL = os.path.join(REF, "ding_nsch_buildable_source_90c0805_2026-04-12.tar.gz")
 CFG_MEMBER = "testcases/92_static_droplet_surface_tension_validation_128.cfg"
@@ -73,6 +75,19 @@ def main():
         payload[f"{c}_maxabs"] = float(np.abs(a).max())
     np.savez_compressed(os.path.join(HERE, "case92_final.npz"), **payload)
     print("wrote", len(keep), "history rows and", len(FIELD_COLUMNS), "final fields")
+
+    # the reference's case files that the config-parser test reads (smoke, static droplets, shear droplets,
+    # rising bubbles), copied as they are
+    import glob
+    import shutil
+
+    dst = os.path.join(HERE, "testcases")
+    os.makedirs(dst, exist_ok=True)
+    names = sorted(glob.glob(os.path.join(REF, "testcases", "0[4-9]*.cfg")) +
+                   glob.glob(os.path.join(REF, "testcases", "2[4-6]*.cfg")))
+    for path in names:
+        shutil.copyfile(path, os.path.join(dst, os.path.basename(path)))
+    print("copied", len(names), "case files")
 
 
 if __name__ == "__main__":

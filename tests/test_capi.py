@@ -48,7 +48,7 @@ def _struct_as_dict(c):
 
 
 @pytest.mark.parametrize("path", [os.path.join(GOLDEN, "case92.cfg")] + sorted(
-    glob.glob("/root/reference/testcases/0[4-9]*.cfg") + glob.glob("/root/reference/testcases/2[4-6]*.cfg")))
+    glob.glob(os.path.join(GOLDEN, "testcases", "*.cfg"))))
 def test_config_parse_matches_reference_parser(lib, path):
     text = open(path).read()
     ref = parse_cfg(text)  # restatement of config.cpp:49-208

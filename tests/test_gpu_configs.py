@@ -1,0 +1,269 @@
+"""Parity of the CUDA step with the oracle on the configurations the throughput figures are quoted on.
+
+* the bench workload: the 192x384 rising bubble (R0-unit parameters of the reference's testcase 26,
+  split_icpcg), from the bench's seeded state, under the launch shapes the autotuner can pick;
+* the 64x64 static droplet between walls (icpcg, dt 1e-4, Pe = 1/Cn) for all 200 steps: the two
+  trajectories side by side, and every 50th step re-solved from the oracle's own state;
+* the Rayleigh-Taylor physics of the 1024x2048 configuration on a 128x256 grid (periodic x, free-slip walls,
+  density ratio 1/3, Re 3000, Cn 0.005, Pe 2/Cn, icpcg, no surface tension, seeded interface modes 2-16),
+  in the plain and the mixed-precision form;
+* the 128x128 shear droplet between walls moving at +-0.5 (Re 0.1, Ca 0.45, Cn 0.03, icpcg, dt 1e-6);
+* the 1024x2048 rising bubble, one step against a fixture of sampled cells that the reference build wrote
+  (tests/golden/make_fullsize.py), plain and mixed.
+
+Bars: rel-L2 <= 1e-10 on c, mu, u, v, p and equal CH / pressure iteration counts for the plain form; 1e-8
+for the mixed form (p within the reference's own solver error where that is larger, as in
+test_gpu_mixed.py).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import FIELDS, OracleSolver, with_defaults
+from test_gpu_parity import assert_fields_close, interior, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+TOL = 1.0e-10
+TOL_MIXED = 1.0e-8
+COMPARE = ("c", "mu", "u", "v", "p")
+
+
+@pytest.fixture(scope="module")
+def dn():
+    import ding_nsch_core_solver_b200 as m
+
+    m.load()
+    return m
+
+
+def droplet64():
+    """64x64 static droplet between no-slip walls, icpcg (the CPU-runnable case)."""
+    return with_defaults(dict(
+        nx=64, ny=64, lx=1.0, ly=1.0, periodic_x=False, periodic_y=False, interface_radius=0.25,
+        interface_center_x=0.5, interface_center_y=0.5, cn=0.02, density_ratio=1.0, viscosity_ratio=1.0,
+        re=100.0, ca=0.01, pe=50.0, dt=1e-4, pressure_scheme="icpcg", pressure_tolerance=1e-10,
+        ch_tolerance=1e-10, poisson_iterations=5000, ch_inner_iterations=500, momentum_iterations=500,
+        momentum_tolerance=1e-12))
+
+
+def rayleigh_taylor(nx=128, ny=256, **kw):
+    """Rayleigh-Taylor: heavy fluid (c = 1) above y = 2 + 0.05 cos(2 pi x), periodic x, free-slip walls."""
+    cn = 0.005
+    cfg = dict(
+        nx=nx, ny=ny, lx=1.0, ly=4.0, periodic_x=True, periodic_y=False, interface_radius=0.0,
+        interface_center_y=2.0, interface_amplitude=0.05, interface_wavenumber=1.0, invert_phase=True,
+        density_ratio=1.0 / 3.0, viscosity_ratio=1.0, re=3000.0, ca=1.0, cn=cn, pe=2.0 / cn,
+        surface_tension_multiplier=0.0, body_force_y=-1.0, dt=5e-5, u_bc_bottom_type="neumann",
+        u_bc_top_type="neumann", v_bc_bottom_type="dirichlet", v_bc_top_type="dirichlet",
+        pressure_scheme="icpcg", pressure_tolerance=1e-10, ch_tolerance=1e-10, poisson_iterations=20000,
+        ch_inner_iterations=5000, momentum_iterations=500, momentum_tolerance=1e-12, mixed_inner_tolerance=1e-5)
+    cfg.update(kw)
+    return with_defaults(cfg)
+
+
+def rt_interface(cfg, seed=3):
+    """c of the seeded RT interface: y0(x) = 2 + 0.05 cos(2 pi x) + sum_{k=2..16} a_k cos(2 pi k x + phi_k),
+    a_k = 1e-3 U(-1, 1); c = 1/2 + 1/2 tanh((y - y0) / (2 sqrt 2 Cn)) (heavy fluid above)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, g = cfg["nx"], cfg["ny"], cfg["ghost"]
+    x = (np.arange(nx) + 0.5) * cfg["lx"] / nx
+    y = (np.arange(ny) + 0.5) * cfg["ly"] / ny
+    y0 = 2.0 + 0.05 * np.cos(2 * np.pi * x)
+    for k in range(2, 17):
+        y0 = y0 + 1e-3 * rng.uniform(-1, 1) * np.cos(2 * np.pi * k * x + rng.uniform(0, 2 * np.pi))
+    c = 0.5 + 0.5 * np.tanh((y[None, :] - y0[:, None]) / (2.0 * math.sqrt(2.0) * cfg["cn"]))
+    out = np.zeros((nx + 2 * g, ny + 2 * g))
+    out[g:-g, g:-g] = c
+    return out
+
+
+def shear_droplet():
+    """128x128 droplet between walls moving at +-0.5 (shear rate 1), periodic x, icpcg."""
+    return with_defaults(dict(
+        nx=128, ny=128, lx=1.0, ly=1.0, periodic_x=True, periodic_y=False, top_wall_velocity_x=0.5,
+        bottom_wall_velocity_x=-0.5, re=0.1, ca=0.45, cn=0.03, pe=150.0, density_ratio=1.0, viscosity_ratio=1.0,
+        interface_radius=0.25, interface_center_x=0.5, interface_center_y=0.5, dt=1e-6, pressure_scheme="icpcg",
+        pressure_tolerance=1e-10, ch_tolerance=1e-10, poisson_iterations=5000, ch_inner_iterations=500,
+        momentum_iterations=500, momentum_tolerance=1e-12))
+
+
+def start_pair(dn, cfg, phase=None, gpu_cfg=None):
+    """Oracle and GPU solver from the reference's own initial state (c replaced by `phase` when given)."""
+    orc = OracleSolver(cfg, "port")
+    orc.initialize()
+    if phase is not None:
+        for n in ("c", "c_prev", "c_prev2"):
+            orc.set_field(n, phase)
+        orc.refresh_derived()
+    gpu = dn.Solver(gpu_cfg or cfg)
+    inject(orc, gpu)
+    return orc, gpu
+
+
+def inject(orc, gpu):
+    for name in FIELDS:
+        gpu.set_field(name, orc.field(name))
+    gpu.set_initial_mass(0.0)
+    orc.set_initial_mass(0.0)
+
+
+def step_both(orc, gpu, k, where, tol=TOL, names=COMPARE):
+    orc.step(k)
+    rep = gpu.step(k)
+    ro = orc.report()
+    assert_fields_close(orc, gpu, names, f"{where} step {k}", tol=tol)
+    return rep, ro
+
+
+# ---- the bench workload -------------------------------------------------------------------------------
+@pytest.mark.parametrize("shape", [None, (1024, 2), (512, 4), (2048, 1)])
+def test_bench_workload_parity(dn, shape):
+    import bench
+
+    cfg = with_defaults(bench.workload_cfg())
+    gcfg = dict(cfg)
+    if shape is not None:
+        gcfg.update(pcg_rows_per_cta=shape[0], sweep_warps_per_cta=shape[1])
+    orc = OracleSolver(cfg, "port")
+    orc.initialize()
+    for n, a in bench.initial_state(cfg).items():
+        orc.set_field(n, a)
+    orc.refresh_derived()
+    gpu = dn.Solver(gcfg)
+    inject(orc, gpu)
+    for k in range(4):
+        rep, ro = step_both(orc, gpu, k, f"bench workload {shape}")
+        assert rep["pressure_iterations"] == ro["pressure_iterations"], (k, rep, ro)
+        assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
+        assert rep["momentum_iterations"] == ro["momentum_iterations"], (k, rep, ro)
+    gpu.close()
+
+
+# ---- the 64x64 static droplet, 200 steps --------------------------------------------------------------
+def test_droplet64_trajectory_200_steps(dn):
+    """Both trajectories over all 200 steps: iteration counts equal at every step; the fields stay within
+    TOL_TRAJ of the oracle's.  The flow is spiky (|u| reaches 15, |mu| 5e3 on the reference itself), so
+    round-off differences grow along the trajectory; the per-step bar is held by the re-solved steps of
+    test_droplet64_per_step_from_oracle_state."""
+    cfg = droplet64()
+    orc, gpu = start_pair(dn, cfg)
+    worst = 0.0
+    g = cfg["ghost"]
+    for k in range(200):
+        orc.step(k)
+        rep = gpu.step(k)
+        ro = orc.report()
+        assert rep["pressure_iterations"] == ro["pressure_iterations"], (k, rep, ro)
+        assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
+        assert rep["momentum_iterations"] == ro["momentum_iterations"], (k, rep, ro)
+        for name in COMPARE:
+            worst = max(worst, rel_l2(interior(gpu.get_field(name), g), interior(orc.field(name), g)))
+    print(f"droplet64: worst rel-L2 over 200 steps {worst:.3e}")
+    assert worst <= TOL_TRAJ, worst
+
+
+TOL_TRAJ = 1.0e-8
+
+
+def test_droplet64_per_step_from_oracle_state(dn):
+    """Every 50th step of the oracle's trajectory (and the last) re-solved on the GPU from the oracle's state."""
+    cfg = droplet64()
+    orc, gpu = start_pair(dn, cfg)
+    for k in range(200):
+        if k % 50 == 0 or k == 199:
+            inject(orc, gpu)
+            rep, ro = step_both(orc, gpu, k, "droplet64")
+            assert rep["pressure_iterations"] == ro["pressure_iterations"], (k, rep, ro)
+            assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
+        else:
+            orc.step(k)
+
+
+# ---- Rayleigh-Taylor physics, reduced grid ----------------------------------------------------------
+def test_rayleigh_taylor_reduced_plain(dn):
+    cfg = rayleigh_taylor()
+    orc, gpu = start_pair(dn, cfg, phase=rt_interface(cfg))
+    for k in range(3):
+        rep, ro = step_both(orc, gpu, k, "RT 128x256")
+        assert rep["pressure_iterations"] == ro["pressure_iterations"], (k, rep, ro)
+        assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
+
+
+def _tight_p(orc, cfg, step):
+    """p after `step` from orc's current state, solved at pressure tolerance 1e-13 (the oracle)."""
+    tight = OracleSolver(dict(cfg, pressure_tolerance=1e-13, poisson_iterations=100000), "port")
+    tight.initialize()
+    for name in FIELDS:
+        tight.set_field(name, orc.field(name))
+    tight.set_initial_mass(0.0)
+    tight.step(step)
+    return tight.field("p")
+
+
+def test_rayleigh_taylor_reduced_mixed(dn):
+    cfg = rayleigh_taylor()
+    orc, gpu = start_pair(dn, cfg, phase=rt_interface(cfg), gpu_cfg=dict(cfg, precision="mixed"))
+    g = cfg["ghost"]
+    for k in range(3):
+        p_tight = _tight_p(orc, cfg, k)
+        orc.step(k)
+        rep = gpu.step(k)
+        assert_fields_close(orc, gpu, ("c", "mu", "u", "v"), f"RT mixed step {k}", tol=TOL_MIXED)
+        ref_err = rel_l2(interior(orc.field("p"), g), interior(p_tight, g))
+        err = rel_l2(interior(gpu.get_field("p"), g), interior(orc.field("p"), g))
+        assert err <= max(TOL_MIXED, 3.0 * ref_err), (k, err, ref_err)
+        assert rep["pressure_residual"] < cfg["pressure_tolerance"]
+
+
+# ---- the shear droplet -----------------------------------------------------------------------------
+def test_shear_droplet_parity(dn):
+    cfg = shear_droplet()
+    orc, gpu = start_pair(dn, cfg)
+    for k in range(4):
+        rep, ro = step_both(orc, gpu, k, "shear droplet")
+        assert rep["pressure_iterations"] == ro["pressure_iterations"], (k, rep, ro)
+        assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
+        assert rep["momentum_iterations"] == ro["momentum_iterations"], (k, rep, ro)
+
+
+# ---- the 1024x2048 bubble against the reference's sampled step ---------------------------------------
+def _fullsize_fixture():
+    path = os.path.join(GOLDEN, "bubble_1024x2048_step0.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"missing fixture {path}: run tests/golden/make_fullsize.py")
+    return np.load(path)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bubble_1024x2048_one_step_vs_reference(dn, precision):
+    import bench
+
+    fx = _fullsize_fixture()
+    cfg = bench.workload_cfg((1024, 2048))
+    gpu = dn.Solver(dict(cfg, precision=precision))
+    for n, a in bench.initial_state(cfg).items():
+        gpu.set_field(n, a)
+    gpu.refresh_derived()
+    gpu.set_initial_mass(0.0)
+    rep = gpu.step(0)
+    g = cfg["ghost"]
+    tol = TOL if precision == "fp64" else TOL_MIXED
+    errs = {}
+    for name in COMPARE:
+        a = gpu.get_field(name)
+        got = a[fx[name + "_i"], fx[name + "_j"]]
+        errs[name] = rel_l2(got, fx[name + "_val"])
+        norm = np.linalg.norm(a[g:a.shape[0] - g, g:a.shape[1] - g])
+        assert abs(norm - float(fx[name + "_norm"])) <= tol * float(fx[name + "_norm"]), (name, norm)
+    print(precision, {k: f"{v:.2e}" for k, v in errs.items()}, rep)
+    assert all(v <= tol for v in errs.values()), errs
+    assert rep["ch_iterations"] == int(fx["ch_iterations"])
+    if precision == "fp64":
+        assert rep["pressure_iterations"] == int(fx["pressure_iterations"])
+        assert rep["momentum_iterations"] == int(fx["momentum_iterations"])
+    gpu.close()

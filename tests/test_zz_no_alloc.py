@@ -24,6 +24,8 @@ CASES = {
                                 pressure_bc_top_type="dirichlet", pressure_bc_top_value=0.25),
     # periodic x: the global-memory wavefront kernel
     "icpcg_periodic_x": dict(BASE, pressure_scheme="icpcg", periodic_x=True),
+    # a handle sharing the device (device_share = 2) launches on half the SMs; so does the static call
+    "split_icpcg_shared_device": dict(BASE, pressure_scheme="split_icpcg", device_share=2),
 }
 
 
