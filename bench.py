@@ -183,8 +183,9 @@ def barrier(dist):
         dist.barrier()
 
 
-def cpu_reference_run(cfg, state, first_step, count):
-    """Steps of the reference build (oracle/_ref, the reference's own C++ sources) on the host: seconds."""
+def cpu_reference_run(cfg, state, first_step, count, untimed=0):
+    """Steps of the reference build (oracle/_ref, the reference's own C++ sources) on the host: seconds for
+    `count` steps from step first_step + untimed, after `untimed` steps from `state` that are not timed."""
     from oracle.oracle import OracleSolver, available, with_defaults
 
     impl = "reference" if available("reference") else "port"
@@ -193,7 +194,27 @@ def cpu_reference_run(cfg, state, first_step, count):
     for n, a in state.items():
         s.set_field(n, a)
     s.refresh_derived()
-    return s.time_steps(first_step, count), impl
+    for k in range(untimed):
+        s.step(first_step + k)
+    return s.time_steps(first_step + untimed, count), impl
+
+
+def host_cpu():
+    """The host's CPU model and hardware threads (the CPU baseline's machine)."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_threads": os.cpu_count()}
+
+
+def first_timed_step(args) -> int:
+    """Index of the first timed step: the warm-up steps, then one more after the untimed autotuning."""
+    return args.warmup + (1 if args.autotune else 0)
 
 
 def run_ours(args):
@@ -231,6 +252,8 @@ def run_ours(args):
         launch_shape = solver.autotune_pressure()
         solver.step(step)
         step += 1
+    assert step == first_timed_step(args)
+    timed_state = {n: solver.get_field(n) for n in RESTART_FIELDS}  # the CPU baseline starts from here
     barrier(dist)
 
     # ---- device-resident timed region: K steps, L2 flushed between steps (outside the timed windows)
@@ -398,7 +421,8 @@ def run_ours(args):
             d = shard.members[k].diagnostics() if not err else {}
             recs.append({"err": err, "pressure_iterations": [rs[k]["pressure_iterations"] for rs in ereps],
                          "ch_iterations": [rs[k]["ch_iterations"] for rs in ereps],
-                         "max_velocity": d.get("max_velocity"), "mass_drift": d.get("mass_drift")})
+                         "max_velocity": d.get("max_velocity"), "mass_drift": d.get("mass_drift"),
+                         "dt_limit_ratio": d.get("dt_limit_ratio")})
         if err and not mine:
             recs, mine = [{"err": err}], [-1 - rank]
         allrec = gather_records(dist, mine, recs)
@@ -414,9 +438,11 @@ def run_ours(args):
                             x for r in allrec for x in r["pressure_iterations"]), 1),
                         "ch_iterations_mean": round(statistics.mean(x for r in allrec for x in r["ch_iterations"]), 1),
                         "max_velocity_max": max(r["max_velocity"] for r in allrec),
+                        "dt_limit_ratio_max": max(r["dt_limit_ratio"] for r in allrec),
                         "mass_drift_max": max(r["mass_drift"] for r in allrec),
                         "workload": "uneven droplets: grids {64..256}^2, periodic both ways, split_icpcg, mixed, "
-                                    "dt 1e-5, seed 4; whole instances sharded over the ranks by LPT on cells x "
+                                    "Pe = 1/Cn, each instance at half its tightest step limit (capillary, explicit "
+                                    "CH, advective), seed 4; whole instances sharded over the ranks by LPT on cells x "
                                     "max(nx, ny), each rank's share stepped together by dn_step_batch",
                         "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                         "sm_share": "equal (1/instances)" if args.ensemble_equal else "in proportion to cells"}
@@ -445,12 +471,14 @@ def run_ours(args):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         sample = max(1, args.cpu_sample_steps)
-        sec, impl = cpu_reference_run(cfg, state, 0, sample)
+        first = first_timed_step(args)
+        sec, impl = cpu_reference_run(cfg, timed_state, first, sample)
         cpu = {"value": round(n_cells * sample / sec / 1e6, 6), "unit": "Mcell-steps/s", "cores": 1,
                "kind": "reference" if impl == "reference" else "port",
-               "sample": f"{sample} steps (steps 0-{sample - 1}) of the same {nxy} workload from the same "
-                         f"seeded state; the reference step is single-threaded",
-               "seconds": round(sec, 3)}
+               "sample": f"{sample} steps (steps {first}-{first + sample - 1}, the first timed steps of the GPU "
+                         f"run, from the GPU's state before them) of the same {nxy} workload; the reference "
+                         f"step is single-threaded",
+               "seconds": round(sec, 3), **host_cpu()}
 
     if rank == 0:
         mean_rep = {k: statistics.mean(r[k] for r in reports) for k in ("pressure_iterations", "ch_iterations",
@@ -499,13 +527,14 @@ def run_reference(args):
     if not (available("reference") or available("port")):
         print(json.dumps({"impl": "reference", "unavailable": "CPU reference build missing (make -C oracle)"}))
         return
-    if args.warmup > 0:
-        cpu_reference_run(cfg, state, 0, 1)  # one warm-up step (page-in, allocator)
-    sec, impl = cpu_reference_run(cfg, state, 0, args.steps)
+    # the same steps the GPU arm times: its warm-up (and autotuning) steps run first, untimed
+    first = first_timed_step(args)
+    sec, impl = cpu_reference_run(cfg, state, 0, args.steps, untimed=first)
     value = n_cells * args.steps / sec / 1e6
     cpu = {"value": round(value, 6), "unit": "Mcell-steps/s", "cores": 1, "kind": impl,
-           "sample": f"{args.steps} steps of the 192x384 workload; the reference step is single-threaded, so one "
-                     f"host thread is all it can use"}
+           "sample": f"steps {first}-{first + args.steps - 1} of the 192x384 workload (the steps the GPU arm "
+                     f"times; steps 0-{first - 1} run untimed first); the reference step is single-threaded, so "
+                     f"one host thread is all it can use", **host_cpu()}
     print(json.dumps({
         "impl": "reference", "metric": METRIC,
         "value": round(value, 6), "unit": "Mcell-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
@@ -537,7 +566,7 @@ def main():
     ap.add_argument("--grid", type=lambda t: tuple(int(v) for v in t.lower().split("x")), default=None,
                     help="NXxNY: the rising bubble on another grid (default 192x384)")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    if args.warmup < 3:  # both arms: the reference arm times the same steps as this one
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)

@@ -133,6 +133,7 @@ def load():
         "dn_explicit_operator": (I, [H, VP, VP, VP, VP]),
         "dn_explicit_operator_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_diagnostics": (I, [H, C.POINTER(Diag)]),
+        "dn_last_diagnostics": (I, [H, C.POINTER(Diag)]),
         "dn_compute_mass": (I, [H, I, DP]),
         "dn_synchronize": (I, [H]),
         "dn_stream": (VP, [H]),
@@ -332,6 +333,12 @@ class Solver:
     def diagnostics(self) -> dict:
         d = Diag()
         self._check(self._lib.dn_diagnostics(self._h, C.byref(d)))
+        return {n: getattr(d, n) for n, _ in Diag._fields_}
+
+    def last_diagnostics(self) -> dict:
+        """The diagnostics computed at the end of the last step (no device work)."""
+        d = Diag()
+        self._check(self._lib.dn_last_diagnostics(self._h, C.byref(d)))
         return {n: getattr(d, n) for n, _ in Diag._fields_}
 
     def compute_mass(self, field: str = "c") -> float:

@@ -439,6 +439,7 @@ struct dn_handle {
   int sw5f = 0, sw5f_blocks_max = 0;
   size_t sw5f_warp_smem[2] = {0, 0};
   int refinement_cycles = 0;  // outer cycles of the last mixed-precision pressure solve
+  dn_diag last_diag{};        // diagnostics at the end of the last dn_step (compute_diagnostics, solver.cpp:276)
   int step = 0;  // step index of the step in progress (split extrapolation, operators.cpp:416)
   double pcg_split_ms[3] = {0, 0, 0};  // pressure PCG, in-kernel: [P1 SpMV+barrier, P2 update+barrier, sweeps]
 };
@@ -2706,7 +2707,7 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
   if (h->cfg.mode == DN_MODE_ADVECTION_ONLY) {
     DN_TRY(advection_step(h, rep));
     for (int k = 0; k < 4; ++k) h->phase_ms[k] = 0.0;
-    return DN_OK;
+    return dn_diagnostics(h, &h->last_diag);  // solver.cpp:252 and the run loop's abort (solver.cpp:355-364)
   }
   DN_TRY(phase(h, step, rep));
   cudaEventRecord(h->ev[1], h->stream);
@@ -2731,6 +2732,14 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
     cudaEventElapsedTime(&ms, h->ev[k], h->ev[k + 1]);
     h->phase_ms[k] = ms;
   }
+  // the step ends with compute_diagnostics (solver.cpp:276); the reference's run loop aborts on a
+  // non-finite one (solver.cpp:355-364), which here is the step's status DN_ERR_NONFINITE
+  return dn_diagnostics(h, &h->last_diag);
+}
+
+dn_status dn_last_diagnostics(dn_handle *h, dn_diag *d) {
+  if (!h || !d) return DN_ERR_INVALID_ARGUMENT;
+  *d = h->last_diag;
   return DN_OK;
 }
 

@@ -18,11 +18,28 @@ from . import capi
 GRID_SIZES = (64, 96, 128, 192, 256)
 
 
+def stable_dt(nx: int, ny: int, re: float, ca: float, pe: float, cn: float, density_ratio: float,
+              speed: float, safety: float = 0.5) -> float:
+    """`safety` x the tightest of the reference's step limits (populate_timestep_limits,
+    diagnostics.cpp:48-112) for a droplet state: advective 0.5 / (|u|/dx + |v|/dy) at background speed
+    `speed` in each direction, capillary 0.5 sqrt(Re Ca h^3 / rho_max), and the explicit CH limit
+    0.25 h^2 / (6 sqrt 2 M W'' / (Pe Cn)) at its bounds M = 1/4, |W''| = 1/2 (h = min(dx, dy))."""
+    dx, dy = 1.0 / nx, 1.0 / ny
+    h = min(dx, dy)
+    adv = 0.5 / max(speed / dx + speed / dy, 1e-30)
+    cap = 0.5 * np.sqrt(re * ca * h ** 3 / max(1.0, density_ratio))
+    chx = 0.25 * h * h / (6.0 * np.sqrt(2.0) * 0.25 * 0.5 / (pe * cn))
+    return float(safety * min(adv, cap, chx))
+
+
 def droplet_cfgs(count: int, seed: int = 4) -> list:
     """Droplet instances of uneven grids: nx, ny each from {64, 96, 128, 192, 256}; unit square, periodic
     both ways; radius U(0.15, 0.3) at a centre kept 0.05 inside the box; density and viscosity ratios
-    log-uniform in [1, 100]; surface tension multiplier U(0.5, 2) with re = ca = 1; cn = 1.5 min(dx, dy);
-    uniform background velocity U(-0.1, 0.1)^2; split_icpcg in the mixed-precision form."""
+    log-uniform in [1, 100]; surface tension multiplier U(0.5, 2) with re = ca = 1; cn = 1.5 min(dx, dy),
+    Pe = 1/Cn; uniform background velocity U(-0.1, 0.1)^2; split_icpcg in the mixed-precision form.  Each
+    instance steps at half its tightest step limit (stable_dt), so every trajectory stays bounded: a common
+    dt of 1e-5 lies above the explicit CH limit of the finer grids, whose chemical potential and then
+    velocity blow up within 20 steps on the reference itself."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
@@ -30,12 +47,16 @@ def droplet_cfgs(count: int, seed: int = 4) -> list:
         radius = rng.uniform(0.15, 0.3)
         cx, cy = rng.uniform(radius + 0.05, 1.0 - radius - 0.05, size=2)
         au, av = rng.uniform(-0.1, 0.1, size=2)
+        dr, vr = float(10 ** rng.uniform(0, 2)), float(10 ** rng.uniform(0, 2))
+        cn = 1.5 / max(nx, ny)
         out.append(dict(
             name=f"droplet_{nx}x{ny}", mode="coupled", nx=nx, ny=ny, ghost=3, lx=1.0, ly=1.0, periodic_x=True,
             periodic_y=True, interface_center_x=float(cx), interface_center_y=float(cy), interface_radius=float(radius),
-            density_ratio=float(10 ** rng.uniform(0, 2)), viscosity_ratio=float(10 ** rng.uniform(0, 2)),
-            surface_tension_multiplier=float(rng.uniform(0.5, 2.0)), re=1.0, ca=1.0, cn=1.5 / max(nx, ny),
-            advect_u=float(au), advect_v=float(av), dt=1e-5, pressure_scheme="split_icpcg", precision="mixed",
+            density_ratio=dr, viscosity_ratio=vr,
+            surface_tension_multiplier=float(rng.uniform(0.5, 2.0)), re=1.0, ca=1.0, cn=cn, pe=1.0 / cn,
+            advect_u=float(au), advect_v=float(av),
+            dt=stable_dt(nx, ny, 1.0, 1.0, 1.0 / cn, cn, dr, max(abs(au), abs(av))),
+            pressure_scheme="split_icpcg", precision="mixed",
             poisson_iterations=2000, pressure_tolerance=1e-10, ch_inner_iterations=500, ch_tolerance=1e-10,
             momentum_iterations=200, momentum_tolerance=1e-10))
     return out

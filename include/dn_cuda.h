@@ -304,8 +304,13 @@ dn_status dn_write_restart(dn_handle *h, int step, const char *path);
 dn_status dn_load_restart(dn_handle *h, const char *path, int *step);
 
 /* ---- diagnostics ------------------------------------------------------------------------------------ */
-/* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device. */
+/* Solver::compute_diagnostics (diagnostics.cpp:114-167) on the device.  Returns DN_ERR_NONFINITE, with
+ * `out` filled, when mass drift, divergence, max velocity or max |mu| is not finite (solver.cpp:355-364). */
 dn_status dn_diagnostics(dn_handle *h, dn_diag *out);
+/* The diagnostics dn_step computed at the end of the last step (advance_one_timestep ends with
+ * compute_diagnostics, solver.cpp:276; dn_step returns DN_ERR_NONFINITE where the reference's run loop
+ * aborts). */
+dn_status dn_last_diagnostics(dn_handle *h, dn_diag *out);
 /* Solver::compute_mass (diagnostics.cpp:24-32), FP64 on the device. */
 dn_status dn_compute_mass(dn_handle *h, int field, double *mass);
 

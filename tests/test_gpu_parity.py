@@ -92,6 +92,12 @@ CASES = {
                                    dt=1e-4),
     "tiny_walls_split_ildlt": unit(nx=8, ny=8, periodic_x=False, periodic_y=False, pressure_scheme="split_ildlt_pcg",
                                    dt=1e-4),
+    # tall grids (long sweep lines; a ragged last column group; periodic y with the wrap at the line ends)
+    "tall_walls_split_icpcg": unit(nx=48, ny=200, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
+                                   body_force_y=-0.98, dt=1e-4),
+    "tall_periodic_icpcg": unit(nx=40, ny=170, pressure_scheme="icpcg", dt=1e-4),
+    "tall_channel_y_ildlt": unit(nx=36, ny=260, periodic_x=False, periodic_y=True, pressure_scheme="ildlt_pcg",
+                                 dt=1e-4),
 }
 
 
