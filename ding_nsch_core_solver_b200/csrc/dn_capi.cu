@@ -1481,7 +1481,7 @@ __global__ void k_resid_stats(const double *r, const double *mask, long long n, 
 // z = in / max(|diag|, 1e-30): build_diagonal_preconditioner / apply_preconditioner (ch_sparse_krylov.hpp:421-432)
 __global__ void k_diag_apply(const double *diag, const double *in, double *z, long long n) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) z[t] = (1.0 / fmax(fabs(diag[t]), 1.0e-30)) * in[t];
+  if (t < n) z[t] = (1.0 / max_ref(fabs(diag[t]), 1.0e-30)) * in[t];
 }
 __global__ void k_p_update(double *p, const double *z, long long n, double beta) {  // p = z + beta p
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2082,13 +2082,19 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     A(dalloc(h, p, h->nm));
   A(dalloc(h, &h->bar_count, 1));
   A(dalloc(h, &h->bar_gen, 1));
-  A(dalloc(h, &h->status, 1));
+  A(dalloc(h, &h->status, 4));  // [status, pad, poll limit of the device waits (long long)]
   A(dalloc(h, &h->prog, 2 * (size_t)kMaxBlocks * 8));
   A(dalloc(h, &h->partials, 2 * (size_t)kMaxBlocks * 8));
   A(dalloc(h, &h->scal, 64));
   A(dalloc(h, &h->prof, 64));
   if (s == DN_OK && cudaMallocHost(&h->host_scal, kHostScal * sizeof(double)) != cudaSuccess) s = DN_ERR_CUDA;
   if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+  {
+    const long long limit = c.device_wait_limit;  // 0: the device code's default
+    if (cudaMemcpyAsync(h->status + 2, &limit, sizeof limit, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+      return bad(DN_ERR_CUDA, "setting the device wait limit failed");
+  }
   h->nsweep = (nx + 31) / 32;
   h->nsweep5 = staged_sweep_warps(nx);
   A(dalloc(h, &h->bnd_f, 2 * (size_t)std::max(h->nsweep, h->nsweep5) * ny));
@@ -3183,7 +3189,7 @@ StaticLayout static_layout(int nx, int ny, int g) {
   const size_t nsweep = std::max((size_t)(nx + 31) / 32, (size_t)staged_sweep_warps(nx));
   L.bar_count = take(sizeof(unsigned int));
   L.bar_gen = take(sizeof(unsigned int));
-  L.status = take(sizeof(int));
+  L.status = take(4 * sizeof(int));  // [status, pad, poll limit]: the limit stays 0 (the default)
   L.prog = take(2 * (size_t)kMaxBlocks * 8 * sizeof(unsigned int));
   L.partials = take(2 * (size_t)kMaxBlocks * 8 * sizeof(double));
   L.scal = take(64 * sizeof(double));

@@ -43,6 +43,13 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Bounded spin: ~2^22 polls with a short sleep, i.e. well under a few seconds, then give up.
 constexpr long long kSpinLimit = 1ll << 22;
 
+// The status buffer of a handle (or of a static solve) is [status, pad, poll limit (long long)]: every
+// bounded wait gives up after that many polls (kSpinLimit when the limit is 0 or negative).
+__device__ __forceinline__ long long spin_limit(const volatile int *status) {
+  const long long v = *(const volatile long long *)(status + 2);
+  return v > 0 ? v : kSpinLimit;
+}
+
 struct Grid {
   int nx, ny, g;
   int px, py;  // periodic flags
@@ -68,6 +75,12 @@ struct Fv {
   }
   __host__ __device__ __forceinline__ size_t size() const { return (size_t)(nx + 2 * g) * (size_t)(ny + 2 * g); }
 };
+
+// std::max / std::min as the reference calls them (a NaN in the first argument passes through), where the
+// reference clamps values that can be NaN -- norms, pivots, denominators -- so that a non-finite state fails
+// the same checks on the device as in the reference.  CUDA's fmax/fmin return the other argument instead.
+__host__ __device__ __forceinline__ double max_ref(double a, double b) { return (a < b) ? b : a; }
+__host__ __device__ __forceinline__ double min_ref(double a, double b) { return (b < a) ? b : a; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -129,7 +142,7 @@ struct GridBarrier {
         long long spins = 0;
         while (*gen == my_gen) {
           ++spins;
-          if ((spins & 1023) == 0 && (spins > kSpinLimit || *status != kDevOk)) {
+          if (spins > spin_limit(status) || ((spins & 1023) == 0 && *status != kDevOk)) {
             atomicCAS((int *)status, kDevOk, kDevTimeout);
             break;
           }

@@ -208,7 +208,7 @@ __global__ void k_factor(SpOp A, Factor F, int kind, int *status) {
               sum -= F.l[(size_t)slots[q] * A.n + r] * F.d[k] * l_ck;
           }
         }
-        const double denom = fmax(F.d[c], floor);
+        const double denom = max_ref(F.d[c], floor);
         F.l[(size_t)slots[p] * A.n + r] = sum / denom;
       }
       double d = A.a[(size_t)Stencil<S>::center * A.n + r];
@@ -230,7 +230,7 @@ __global__ void k_factor(SpOp A, Factor F, int kind, int *status) {
         d = floor * 2.0;
       }
       F.d[r] = d;
-      F.dinv[r] = 1.0 / fmax(d, floor);
+      F.dinv[r] = 1.0 / max_ref(d, floor);
     }
     __syncthreads();
   }
@@ -241,7 +241,7 @@ template <int S>
 __global__ void k_diag_inverse(SpOp A, double *dinv) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= A.n) return;
-  dinv[r] = 1.0 / fmax(fabs(A.a[(size_t)Stencil<S>::center * A.n + r]), 1.0e-30);
+  dinv[r] = 1.0 / max_ref(fabs(A.a[(size_t)Stencil<S>::center * A.n + r]), 1.0e-30);
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -370,7 +370,7 @@ __device__ __forceinline__ unsigned int wait_flag(const unsigned int *flag, unsi
     v = __shfl_sync(0xffffffffu, v, 0);
     if (v >= target) return v;
     ++spins;
-    if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+    if (spins > spin_limit(status) || ((spins & 1023) == 0 && *(volatile int *)status != kDevOk)) {
       if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
       return 0;
     }
@@ -965,10 +965,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
   }
   if (!grid_sum<3>(v3, P.partials, parity, sh, bar)) return;
   double m_r = P.project ? v3[0] / dn_ : 0.0;
-  double rn2 = P.project ? fmax(v3[1] - v3[0] * v3[0] / dn_, 0.0) : v3[1];
-  const double rhs_norm = sqrt(fmax(v3[2], 0.0));
-  double absr = sqrt(fmax(rn2, 0.0));
-  double relr = absr / fmax(rhs_norm, 1.0e-30);
+  double rn2 = P.project ? max_ref(v3[1] - v3[0] * v3[0] / dn_, 0.0) : v3[1];
+  const double rhs_norm = sqrt(max_ref(v3[2], 0.0));
+  double absr = sqrt(max_ref(rn2, 0.0));
+  double relr = absr / max_ref(rhs_norm, 1.0e-30);
   int iterations = 0;
   double iter_res = 0.0;
   if (relr < P.tol || absr < P.tol_abs) {  // x stays x0 (the reference projects r only)
@@ -1079,11 +1079,11 @@ __global__ void __launch_bounds__(kBlock) k_pcg(PcgArgsT<T> P) {
     t_p2 += t2 - t1;
     m_x = P.project ? w[2] / dn_ : 0.0;
     m_r = P.project ? w[3] / dn_ : 0.0;
-    rn2 = P.project ? fmax(w[4] - w[3] * w[3] / dn_, 0.0) : w[4];
+    rn2 = P.project ? max_ref(w[4] - w[3] * w[3] / dn_, 0.0) : w[4];
     iterations = it + 1;
-    iter_res = sqrt(w[0] / fmax(w[1], 1.0e-30));
-    absr = sqrt(fmax(rn2, 0.0));
-    relr = absr / fmax(rhs_norm, 1.0e-30);
+    iter_res = sqrt(w[0] / max_ref(w[1], 1.0e-30));
+    absr = sqrt(max_ref(rn2, 0.0));
+    relr = absr / max_ref(rhs_norm, 1.0e-30);
     if (P.mon && it < P.mon_cap && blockIdx.x == 0 && threadIdx.x == 0) {  // the CG monitor's record
       P.mon[4 * it + 0] = absr;
       P.mon[4 * it + 1] = relr;

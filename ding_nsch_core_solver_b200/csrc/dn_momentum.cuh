@@ -276,7 +276,7 @@ __global__ void k_mom_dinv(BicgArgs P) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= P.n) return;
   const long long c0 = P.tgt[r];
-  P.dinv[r] = (c0 >= 0) ? 1.0 / fmax(fabs(P.coef[r]), 1.0e-30) : 0.0;
+  P.dinv[r] = (c0 >= 0) ? 1.0 / max_ref(fabs(P.coef[r]), 1.0e-30) : 0.0;
 }
 
 __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
@@ -307,9 +307,9 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
     v2[1] += rr * rr;
   }
   if (!grid_sum<2>(v2, P.partials, parity, sh, bar)) return;
-  const double rhs_norm = sqrt(fmax(v2[0], 0.0));
-  double absr = sqrt(fmax(v2[1], 0.0));
-  double relr = absr / fmax(rhs_norm, 1.0e-30);
+  const double rhs_norm = sqrt(max_ref(v2[0], 0.0));
+  double absr = sqrt(max_ref(v2[1], 0.0));
+  double relr = absr / max_ref(rhs_norm, 1.0e-30);
   if ((P.use_rel && relr < P.tol) || absr < P.tol) {
     finish(0, absr, relr, 0.0);
     return;
@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
       a2[0] += sv * sv;
     }
     if (!grid_sum<1>(a2, P.partials, parity, sh, bar)) return;
-    const double s_norm = sqrt(fmax(a2[0], 0.0));
-    if ((P.use_rel && s_norm / fmax(rhs_norm, 1.0e-30) < P.tol) || s_norm < P.tol) {
+    const double s_norm = sqrt(max_ref(a2[0], 0.0));
+    if ((P.use_rel && s_norm / max_ref(rhs_norm, 1.0e-30) < P.tol) || s_norm < P.tol) {
       double a3[2] = {0.0, 0.0};
       for (long long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
         const double xv = P.x[q] + P.upd[q];
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
         a3[1] += xv * xv;
       }
       if (!grid_sum<2>(a3, P.partials, parity, sh, bar)) return;
-      finish(it + 1, s_norm, s_norm / fmax(rhs_norm, 1.0e-30), sqrt(a3[0] / fmax(a3[1], 1.0e-30)));
+      finish(it + 1, s_norm, s_norm / max_ref(rhs_norm, 1.0e-30), sqrt(a3[0] / max_ref(a3[1], 1.0e-30)));
       return;
     }
     // shat = D^-1 s; t = A shat
@@ -409,9 +409,9 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
       a5[3] += P.rhat[q] * rv;
     }
     if (!grid_sum<4>(a5, P.partials, parity, sh, bar)) return;
-    absr = sqrt(fmax(a5[2], 0.0));
-    relr = absr / fmax(rhs_norm, 1.0e-30);
-    const double itres = sqrt(a5[0] / fmax(a5[1], 1.0e-30));
+    absr = sqrt(max_ref(a5[2], 0.0));
+    relr = absr / max_ref(rhs_norm, 1.0e-30);
+    const double itres = sqrt(a5[0] / max_ref(a5[1], 1.0e-30));
     if ((P.use_rel && relr < P.tol) || absr < P.tol) {
       finish(it + 1, absr, relr, itres);
       return;

@@ -177,7 +177,7 @@ __device__ __forceinline__ bool wait_local_line(T *line, int col, int *status, u
     long long spins = 0;
     while (__any_sync(0xffffffffu, miss)) {
       ++spins;
-      if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+      if (spins > spin_limit(status) || ((spins & 1023) == 0 && *(volatile int *)status != kDevOk)) {
         if ((threadIdx.x & 31) == 0) atomicCAS(status, kDevOk, kDevTimeout);
         return false;
       }
@@ -204,7 +204,7 @@ __device__ __forceinline__ unsigned int wait_progress(const unsigned int *cnt, u
     // a warp that waits long (a backward sweep waiting for the whole chain above it) sleeps between
     // polls, so that it takes no issue slots from a sweep warp sharing its scheduler
     if (spins > 32) __nanosleep(64);
-    if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+    if (spins > spin_limit(status) || ((spins & 1023) == 0 && *(volatile int *)status != kDevOk)) {
       if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
       return 0;
     }
@@ -301,7 +301,7 @@ __device__ __forceinline__ bool poll_line(const T *src, int col, bool mine, T &v
   long long spins = 0;
   while (__any_sync(0xffffffffu, miss)) {
     ++spins;
-    if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+    if (spins > spin_limit(status) || ((spins & 1023) == 0 && *(volatile int *)status != kDevOk)) {
       if ((threadIdx.x & 31) == 0) atomicCAS(status, kDevOk, kDevTimeout);
       return false;
     }
@@ -417,7 +417,7 @@ __device__ __forceinline__ void fwd5_staged(const Sweep5T<T> &P, char *smem_warp
       long long spins = 0;
       while (__any_sync(0xffffffffu, miss)) {
         ++spins;
-        if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+        if (spins > spin_limit(status) || ((spins & 1023) == 0 && *(volatile int *)status != kDevOk)) {
           if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
           return false;
         }
@@ -701,7 +701,7 @@ __device__ __forceinline__ void bwd5_staged(const Sweep5T<T> &P, char *smem_warp
     long long spins = 0;
     while (__any_sync(0xffffffffu, miss)) {
       ++spins;
-      if ((spins & 1023) == 0 && (spins > kSpinLimit || *(volatile int *)status != kDevOk)) {
+      if (spins > spin_limit(status) || ((spins & 1023) == 0 && *(volatile int *)status != kDevOk)) {
         if (lane == 0) atomicCAS(status, kDevOk, kDevTimeout);
         return false;
       }

@@ -87,6 +87,9 @@ typedef struct {
   int pcg_rows_per_cta;            /* launch shape of the pressure PCG: rows per CTA of its SpMV / update
                                       phases (0: 512) -- see dn_autotune_pressure */
   int sweep_warps_per_cta;         /* sweep warps per CTA of the staged wavefront (0: as many as fit, up to 4) */
+  int device_wait_limit;           /* polls after which a device-side wait (grid barrier, wavefront hand-over)
+                                      gives up and the call returns DN_ERR_TIMEOUT (0: the default, 2^22, well
+                                      under a few seconds) */
   /* pressure analysis (config.hpp:36-133; run_pressure_analysis_from_snapshot, pressure_analysis.cpp:156-328) */
   int analysis_enabled;            /* analysis_enabled */
   int analysis_mode;               /* dn_analysis_mode, from the analysis_mode string */

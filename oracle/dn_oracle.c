@@ -171,8 +171,9 @@ static void fail(orc_solver *s, const char *fmt, ...) {
 }
 
 static double sq(double v) { return v * v; }
-static double dmax(double a, double b) { return a > b ? a : b; }
-static double dmin(double a, double b) { return a < b ? a : b; }
+/* std::max / std::min (a NaN first argument passes through), as the reference calls them */
+static double dmax(double a, double b) { return (a < b) ? b : a; }
+static double dmin(double a, double b) { return (b < a) ? b : a; }
 
 static rowacc *rows_get(orc_solver *s, int n) {
   if (s->nrows_cap < n) {

@@ -283,3 +283,49 @@ def test_projection_reduces_divergence():
     s.correct()
     after = div_l2(s.field("u"), s.field("v"))
     assert after < before / 100.0
+
+
+# ---- failure paths: the restatement fails where and how the reference fails --------------------------
+def _failure_cases():
+    cfg = unit_config(nx=40, ny=32, periodic_x=False, periodic_y=False, pressure_scheme="icpcg", dt=1e-4)
+    return cfg
+
+
+def _error_of(fn):
+    from oracle.oracle import OracleError
+    try:
+        fn()
+    except OracleError as e:
+        return str(e)
+    return None
+
+
+@pytest.mark.skipif(not available("reference"), reason="reference build (oracle/_ref) not built")
+def test_failure_paths_match_reference_build():
+    """A NaN in c (the CH PCG breaks down, its diagonal retry too: phase_field.cpp:468-473,
+    ch_sparse_krylov.hpp:566-568), a density field with negative values (the variable pressure operator is
+    indefinite, ICC fails: ch_sparse_krylov.hpp:400-402, pressure.cpp:36-38) and an exhausted pressure
+    iteration budget (no error, the unconverged residual is reported) give the same outcome on the port and
+    on the reference build."""
+    cfg = _failure_cases()
+    g = cfg["ghost"]
+    out = {}
+    for impl in ("port", "reference"):
+        nan = OracleSolver(cfg, impl)
+        nan.initialize()
+        nan.field("c")[g + 5, g + 5] = np.nan
+        bad = OracleSolver(cfg, impl)
+        bad.initialize()
+        bad.field("rho_mid")[g + 10:g + 20, g + 8:g + 16] = -2.0
+        bad.field("u_star")[g:-g, g:-g] = 0.01 * np.random.default_rng(0).standard_normal(
+            bad.field("u_star")[g:-g, g:-g].shape)
+        short = OracleSolver(dict(cfg, poisson_iterations=3), impl)
+        short.initialize()
+        short.step(0)
+        rep = short.report()
+        out[impl] = (_error_of(lambda: nan.step(0)), _error_of(bad.pressure), rep["pressure_iterations"],
+                     rep["pressure_residual"])
+    assert out["port"] == out["reference"], out
+    assert out["reference"][0] == "pcg preconditioner breakdown: non-positive r^T M^{-1} r"
+    assert out["reference"][1] == "ICC preconditioner construction failed"
+    assert out["reference"][2] == 3
