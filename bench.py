@@ -339,6 +339,8 @@ def run_ours(args):
                  "pressure_iterations_mean": statistics.mean(r["pressure_iterations"] for r in mreps),
                  "refinement_cycles_mean": statistics.mean(r["refinement_cycles"] for r in mreps),
                  "inner_tolerance": 1e-5,
+                 "inner_preconditioner": ("multigrid V-cycle" if all(r["mixed_inner_multigrid"] for r in mreps)
+                                          else "IC(0)/ILDLT(0) wavefront"),
                  "rel_l2_vs_plain_fp64": {k: float(f"{v:.3e}") for k, v in errs.items()},
                  "compared_after_steps": mstep}
         msolver.close()

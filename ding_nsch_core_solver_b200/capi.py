@@ -50,7 +50,7 @@ class Config(C.Structure):
         ("p_bc", BC * 4), ("u_bc", BC * 4), ("v_bc", BC * 4), ("precision", C.c_int),
         ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int), ("dcdm_direction_mode", C.c_int),
         ("dcdm_history_size", C.c_int), ("dcdm_max_stored_directions", C.c_int), ("dcdm_restart_interval", C.c_int),
-        ("pcg_rows_per_cta", C.c_int), ("sweep_warps_per_cta", C.c_int), ("device_wait_limit", C.c_int),
+        ("pcg_rows_per_cta", C.c_int), ("sweep_warps_per_cta", C.c_int), ("device_wait_limit", C.c_int), ("mixed_preconditioner", C.c_int),
         ("analysis_enabled", C.c_int), ("analysis_mode", C.c_int), ("analysis_trigger_step", C.c_int),
         ("analysis_interface_band_multiplier", C.c_double), ("name", C.c_char * 128), ("output_dir", C.c_char * 512),
         ("analysis_case_group", C.c_char * 128), ("analysis_initial_guess", C.c_char * 64),
@@ -62,7 +62,7 @@ class Report(C.Structure):
         "ch_iterations", "momentum_iterations", "pressure_iterations", "coupling_iterations",
         "ch_preconditioner")] + [(n, C.c_double) for n in (
         "ch_residual", "ch_equation_residual", "momentum_residual", "pressure_residual",
-        "boundary_speed_pre", "boundary_speed_post")] + [("refinement_cycles", C.c_int)]
+        "boundary_speed_pre", "boundary_speed_post")] + [("refinement_cycles", C.c_int), ("mixed_inner_multigrid", C.c_int)]
 
 
 class Diag(C.Structure):

@@ -27,6 +27,7 @@
 #include "dn_fields.cuh"
 #include "dn_krylov.cuh"
 #include "dn_momentum.cuh"
+#include "dn_multigrid.cuh"
 
 using namespace dn;
 
@@ -438,6 +439,21 @@ struct dn_handle {
         *fap = nullptr;
   int sw5f = 0, sw5f_blocks_max = 0;
   size_t sw5f_warp_smem[2] = {0, 0};
+  // mixed form, multigrid-preconditioned inner CG (dn_multigrid.cuh).  Level 0 is the FP32 operator fa5 with
+  // the inner CG's r as right-hand side, z as iterate and fy as residual; mg[l - 1] holds level l >= 1.
+  struct MgHost {
+    int nx = 0, ny = 0;
+    double *a64 = nullptr;
+    float *a = nullptr, *x = nullptr, *b = nullptr, *r = nullptr;
+  };
+  std::vector<MgHost> mg;
+  int mg_levels = 0;  // levels including level 0; 0 = no hierarchy for this grid (the IC inner solver runs)
+  float *mg_inv = nullptr;
+  double *mg_scal = nullptr, *mg_part = nullptr;
+  int *mg_flag = nullptr;
+  MgFold mg_fold{};
+  bool ic32_ready = false;  // FP32 copies of the IC/ILDLT factor made for this solve
+  bool mixed_used_mg = false;  // the last mixed pressure solve started with the multigrid inner solver
   int refinement_cycles = 0;  // outer cycles of the last mixed-precision pressure solve
   dn_diag last_diag{};        // diagnostics at the end of the last dn_step (compute_diagnostics, solver.cpp:276)
   int step = 0;  // step index of the step in progress (split extrapolation, operators.cpp:416)
@@ -818,23 +834,178 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
   return DN_OK;
 }
 
+// ---------------------------------------------------------------------------------------------------
+// Multigrid-preconditioned FP32 inner CG of the mixed form (kernels and design: dn_multigrid.cuh)
+// ---------------------------------------------------------------------------------------------------
+MgLevel mg_level(dn_handle *h, int l) {
+  if (l == 0) return MgLevel{h->fa5, h->fz, h->fr, h->fy, h->G.nx, h->G.ny};
+  const dn_handle::MgHost &m = h->mg[l - 1];
+  return MgLevel{m.a, m.x, m.b, m.r, m.nx, m.ny};
+}
+
+// Coarse operators of the current pressure matrix and the inverse of the coarsest one.  *usable = false when
+// the coarsest matrix has a non-positive pivot (the caller then runs the IC inner solver).
+dn_status mg_setup(dn_handle *h, bool *usable) {
+  *usable = false;
+  const double *af = h->a5;
+  int nxf = h->G.nx, nyf = h->G.ny;
+  for (int l = 1; l < h->mg_levels; ++l) {
+    dn_handle::MgHost &m = h->mg[l - 1];
+    k_mg_coarsen<<<blocks_for((long long)m.nx * m.ny), 256, 0, h->stream>>>(af, nxf, nyf, m.a64, m.a, m.nx, m.ny);
+    DN_TRY(check_launch(h, "k_mg_coarsen"));
+    af = m.a64;
+    nxf = m.nx;
+    nyf = m.ny;
+  }
+  const int nc = nxf * nyf;
+  k_mg_coarse_inverse<<<1, 256, sizeof(double) * nc * nc, h->stream>>>(af, nxf, nyf, h->G.px, h->G.py,
+                                                                         h->has_dirichlet ? 0 : 1, h->mg_inv,
+                                                                         h->mg_flag);
+  DN_TRY(check_launch(h, "k_mg_coarse_inverse"));
+  int flag = 0;
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 33, h->mg_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(&flag, h->host_scal + 33, sizeof(int));
+  *usable = flag == 0;
+  return DN_OK;
+}
+
+// z = B r: one V-cycle from level 0 (right-hand side h->fr, result h->fz)
+dn_status mg_vcycle(dn_handle *h) {
+  constexpr int kSweeps = 2;  // red-black sweeps before and after each coarse correction
+  const int L = h->mg_levels, px = h->G.px, py = h->G.py;
+  auto smooth = [&](const MgLevel &M, int color, int first) -> dn_status {
+    k_mg_smooth<<<blocks_for((long long)M.nx * (M.ny / 2)), 256, 0, h->stream>>>(M, color, first, px, py);
+    return check_launch(h, "k_mg_smooth");
+  };
+  for (int l = 0; l + 1 < L; ++l) {
+    const MgLevel F = mg_level(h, l), C = mg_level(h, l + 1);
+    for (int k = 0; k < kSweeps; ++k) {
+      DN_TRY(smooth(F, 0, k == 0));
+      DN_TRY(smooth(F, 1, 0));
+    }
+    k_mg_residual<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(F, px, py);
+    DN_TRY(check_launch(h, "k_mg_residual"));
+    k_mg_restrict<<<blocks_for((long long)C.nx * C.ny), 256, 0, h->stream>>>(F, C, h->mg_fold);
+    DN_TRY(check_launch(h, "k_mg_restrict"));
+  }
+  const MgLevel Lc = mg_level(h, L - 1);
+  k_mg_coarse_solve<<<1, kMgCoarseMax, 0, h->stream>>>(h->mg_inv, Lc);
+  DN_TRY(check_launch(h, "k_mg_coarse_solve"));
+  for (int l = L - 2; l >= 0; --l) {
+    const MgLevel F = mg_level(h, l), C = mg_level(h, l + 1);
+    k_mg_prolong<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(C, F, h->mg_fold);
+    DN_TRY(check_launch(h, "k_mg_prolong"));
+    for (int k = 0; k < kSweeps; ++k) {
+      DN_TRY(smooth(F, 1, 0));
+      DN_TRY(smooth(F, 0, 0));
+    }
+  }
+  return DN_OK;
+}
+
+// One FP32 inner solve A e = b (b = h->fb, e = h->fx, zero on entry) by CG with the V-cycle preconditioner,
+// to the relative residual tol of |b| = bnorm (the FP64 norm of the outer residual).  out: [0] iterations.
+dn_status run_mgpcg32(dn_handle *h, int project, int max_it, double tol, double bnorm, double out[4]) {
+  const long long n = h->n;
+  MgVec V;
+  V.A = SpOpT<float>{h->fa5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  V.x = h->fx;
+  V.r = h->fr;
+  V.z = h->fz;
+  V.p = h->fp0;
+  V.q = h->fap;
+  V.part = h->mg_part;
+  V.scal = h->mg_scal;
+  const int nb = (int)std::min<long long>({(long long)kMgParts, 4LL * h->num_sms, (long long)blocks_for(n)});
+  const double dn_ = (double)n;
+  auto finish = [&](int mode, int first) -> dn_status {
+    k_mgp_scalars<<<1, 32, 0, h->stream>>>(h->mg_part, nb, h->mg_scal, mode, first, project, dn_);
+    return check_launch(h, "k_mgp_scalars");
+  };
+  cudaEventRecord(h->kev[0], h->stream);
+  DN_CUDA(h, cudaMemsetAsync(h->mg_scal, 0, 16 * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(h->fr, h->fb, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(mg_vcycle(h));
+  k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
+  DN_TRY(check_launch(h, "k_mgp_rz"));
+  DN_TRY(finish(2, 1));
+  k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, 1);
+  DN_TRY(check_launch(h, "k_mgp_direction"));
+  int it = 0;
+  const int cap = std::max(1, max_it);
+  while (it < cap) {
+    k_mgp_apply<<<nb, 256, 0, h->stream>>>(V);
+    DN_TRY(check_launch(h, "k_mgp_apply"));
+    DN_TRY(finish(0, 0));
+    k_mgp_update<<<nb, 256, 0, h->stream>>>(V);
+    DN_TRY(check_launch(h, "k_mgp_update"));
+    DN_TRY(finish(1, 0));
+    ++it;
+    DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 40, h->mg_scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    DN_CUDA(h, cudaStreamSynchronize(h->stream));
+    double sc[8];
+    std::memcpy(sc, h->host_scal + 40, sizeof sc);
+    if (sc[kMgBad] != 0.0) break;  // breakdown: the outer FP64 loop judges the iterate
+    const double rel = std::sqrt(std::max(sc[kMgRr], 0.0)) / std::max(bnorm, 1.0e-300);
+    if (!(rel >= tol)) break;  // converged (or non-finite: the outer loop stops on its own residual)
+    DN_TRY(mg_vcycle(h));
+    k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
+    DN_TRY(check_launch(h, "k_mgp_rz"));
+    DN_TRY(finish(2, 0));
+    k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, 0);
+    DN_TRY(check_launch(h, "k_mgp_direction"));
+  }
+  cudaEventRecord(h->kev[1], h->stream);
+  DN_CUDA(h, cudaEventSynchronize(h->kev[1]));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+  h->phase_ms[4] += ms;
+  out[0] = (double)it;
+  out[1] = out[2] = out[3] = 0.0;
+  return DN_OK;
+}
+
 // Mixed-precision pressure solve: x = 0; repeat r = b - A x (FP64, projected when the system is singular),
 // stop on the reference's rule (rel < tol or abs < tol on the FP64 residual), else solve A e = r with the
 // FP32 PCG to the relative tolerance mixed_inner_tolerance and add e to x in FP64.  The operator and the
 // factor are the FP64 ones rounded to FP32.  out: [0] inner iterations in total, [1] abs and [2] rel FP64
 // residual, [3] 0.
-dn_status mixed_pressure(dn_handle *h, int kind, double out[4]) {
-  const dn_config &cfg = h->cfg;
+dn_status pressure_factor(dn_handle *h, bool split, bool icc);
+
+// FP32 copies of the FP64 IC/ILDLT factor for the IC inner solver (built on first use within a solve)
+dn_status ensure_ic32(dn_handle *h, bool split, int kind) {
+  if (h->ic32_ready) return DN_OK;
+  DN_TRY(pressure_factor(h, split, kind == kPrecICC));
   const long long n = h->n;
-  const int project = h->has_dirichlet ? 0 : 1;
-  k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
-  DN_TRY(check_launch(h, "k_to_float"));
   if (h->G.px) {  // the global-memory wavefront reads the L slots
     k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->l5, h->fl5, 5 * n);
     DN_TRY(check_launch(h, "k_to_float"));
   }
   k_to_float<<<blocks_for(n), 256, 0, h->stream>>>(h->dinv5, h->fdinv5, n);
   DN_TRY(check_launch(h, "k_to_float"));
+  h->ic32_ready = true;
+  return DN_OK;
+}
+
+// Mixed-precision pressure solve: x = 0; repeat r = b - A x (FP64, projected when the system is singular),
+// stop on the reference's rule (rel < tol or abs < tol on the FP64 residual), else solve A e = r in FP32 to
+// the relative tolerance mixed_inner_tolerance and add e to x in FP64.  The inner solver is CG with the
+// multigrid V-cycle (when the grid has a hierarchy and mixed_preconditioner allows it) or the persistent
+// PCG with the scheme's IC/ILDLT factor rounded to FP32.  An inner multigrid solve after which the FP64
+// residual does not decrease hands the rest of the solve to the IC inner solver.  The operator is the FP64
+// one rounded to FP32.  out: [0] inner iterations in total, [1] abs and [2] rel FP64 residual, [3] 0.
+dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
+  const dn_config &cfg = h->cfg;
+  const long long n = h->n;
+  const int project = h->has_dirichlet ? 0 : 1;
+  k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
+  DN_TRY(check_launch(h, "k_to_float"));
+  h->ic32_ready = false;
+  bool use_mg = false;
+  if (h->mg_levels > 0) DN_TRY(mg_setup(h, &use_mg));
+  h->mixed_used_mg = use_mg;
+  if (!use_mg) DN_TRY(ensure_ic32(h, split, kind));
   const SpOp A{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
   h->phase_ms[4] = 0.0;
   h->pcg_split_ms[0] = h->pcg_split_ms[1] = h->pcg_split_ms[2] = 0.0;
@@ -855,17 +1026,25 @@ dn_status mixed_pressure(dn_handle *h, int kind, double out[4]) {
     relr = absr / std::max(std::sqrt(std::max(sums[2], 0.0)), 1.0e-30);
     if (relr < cfg.pressure_tolerance || absr < cfg.pressure_tolerance) break;
     // the iteration budget is shared by the inner solves; a cycle that no longer reduces the residual ends it
-    if (cycles >= kMaxCycles || total >= cfg.poisson_iterations || !(absr < prev)) break;
+    if (cycles >= kMaxCycles || total >= cfg.poisson_iterations) break;
+    if (!(absr < prev)) {
+      if (!use_mg) break;
+      use_mg = false;  // the multigrid inner solve stalled: continue from this iterate with the IC inner solver
+      DN_TRY(ensure_ic32(h, split, kind));
+    }
     prev = absr;
     k_inner_rhs<<<blocks_for(n), 256, 0, h->stream>>>(h->r, mean, h->fb, h->fx, n);
     DN_TRY(check_launch(h, "k_inner_rhs"));
     double o[4];
-    DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, o));
+    if (use_mg)
+      DN_TRY(run_mgpcg32(h, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, absr, o));
+    else
+      DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, o));
     total += (int)o[0];
     k_add_correction<<<blocks_for(n), 256, 0, h->stream>>>(h->x, h->fx, n);
     DN_TRY(check_launch(h, "k_add_correction"));
     ++cycles;
-    if ((int)o[0] == 0) break;
+    if ((int)o[0] == 0 && !use_mg) break;
   }
   h->refinement_cycles = cycles;
   out[0] = (double)total;
@@ -1263,6 +1442,7 @@ dn_status pressure_jacobi(dn_handle *h, dn_report *rep) {
   rep->pressure_iterations = its;
   rep->pressure_residual = res;
   rep->refinement_cycles = 0;
+  rep->mixed_inner_multigrid = 0;
   h->phase_ms[7] = its;
   LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_P_CORR], xb[its & 1], f[DN_F_P_CORR]);
   if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P_CORR]));
@@ -1877,13 +2057,16 @@ dn_status pressure_factor(dn_handle *h, bool split, bool icc) {
 dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *rep) {
   const dn_config &cfg = h->cfg;
   const int kind = icc ? kPrecICC : kPrecLDLT;
-  DN_TRY(pressure_factor(h, split, icc));
+  // the mixed form builds the factor only when its inner solves use it
+  if (cfg.precision != DN_PRECISION_MIXED) DN_TRY(pressure_factor(h, split, icc));
   DN_CUDA(h, cudaMemsetAsync(h->x, 0, h->n * sizeof(double), h->stream));
   double out[4];
   rep->refinement_cycles = 0;
+  rep->mixed_inner_multigrid = 0;
   if (cfg.precision == DN_PRECISION_MIXED) {
-    DN_TRY(mixed_pressure(h, kind, out));
+    DN_TRY(mixed_pressure(h, split, kind, out));
     rep->refinement_cycles = h->refinement_cycles;
+    rep->mixed_inner_multigrid = h->mixed_used_mg ? 1 : 0;
   } else if (h->sw5 > 0 && h->G.px) {
     DN_TRY((run_pcg<5, 4>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
                           cfg.pressure_tolerance, out)));
@@ -2155,6 +2338,42 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     for (float **p : {&h->fdinv5, &h->fb, &h->fx, &h->fr, &h->fz, &h->fy, &h->fp0, &h->fp1, &h->fap})
       A(dalloc(h, p, h->n));
     if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+    if (c.mixed_preconditioner == DN_MIXED_PREC_MULTIGRID) {
+      // halve both extents while they are even and >= 4 and the level is larger than the direct coarse solve
+      std::vector<std::pair<int, int>> dims{{h->G.nx, h->G.ny}};
+      int lx = h->G.nx, ly = h->G.ny;
+      while ((long long)lx * ly > kMgCoarseMax && lx % 2 == 0 && ly % 2 == 0 && lx >= 4 && ly >= 4 &&
+             (int)dims.size() < kMgMaxLevels) {
+        lx /= 2;
+        ly /= 2;
+        dims.push_back({lx, ly});
+      }
+      if ((long long)lx * ly <= kMgCoarseMax) {
+        for (size_t l = 1; l < dims.size(); ++l) {
+          dn_handle::MgHost m;
+          m.nx = dims[l].first;
+          m.ny = dims[l].second;
+          const size_t nl = (size_t)m.nx * m.ny;
+          A(dalloc(h, &m.a64, 5 * nl));
+          A(dalloc(h, &m.a, 5 * nl));
+          A(dalloc(h, &m.x, nl));
+          A(dalloc(h, &m.b, nl));
+          A(dalloc(h, &m.r, nl));
+          h->mg.push_back(m);
+        }
+        A(dalloc(h, &h->mg_inv, (size_t)kMgCoarseMax * kMgCoarseMax));
+        A(dalloc(h, &h->mg_scal, 16));
+        A(dalloc(h, &h->mg_part, 3 * (size_t)kMgParts));
+        A(dalloc(h, &h->mg_flag, 1));
+        if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+        h->mg_levels = (int)dims.size();
+        for (int k = 0; k < 4; ++k) h->mg_fold.s[k] = h->bc.p[k].type == DN_BC_DIRICHLET ? -1.0f : 1.0f;
+        h->mg_fold.px = h->G.px;
+        h->mg_fold.py = h->G.py;
+        cudaFuncSetAttribute(k_mg_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * kMgCoarseMax * kMgCoarseMax));
+      }
+    }
     const int optin = h->smem_optin;
     auto round16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
     const bool px = c.periodic_x != 0;

@@ -111,6 +111,7 @@ extern "C" void dn_config_default(dn_config *c) {
   c->pcg_rows_per_cta = 0;     // 512
   c->sweep_warps_per_cta = 0;  // as many as the shared memory holds, up to 4
   c->device_wait_limit = 0;    // kSpinLimit polls
+  c->mixed_preconditioner = DN_MIXED_PREC_MULTIGRID;
   c->analysis_enabled = 0;     // config.hpp:53-133
   c->analysis_mode = DN_ANALYSIS_OFF;
   c->analysis_trigger_step = 1;
@@ -185,6 +186,15 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
         cfg->precision = DN_PRECISION_MIXED;
       else
         throw std::runtime_error("unsupported precision: " + kv["precision"]);
+    }
+    if (kv.count("mixed_preconditioner")) {
+      const std::string v = lower(kv["mixed_preconditioner"]);
+      if (v == "multigrid")
+        cfg->mixed_preconditioner = DN_MIXED_PREC_MULTIGRID;
+      else if (v == "ic" || v == "icc" || v == "ildlt")
+        cfg->mixed_preconditioner = DN_MIXED_PREC_IC;
+      else
+        throw std::runtime_error("unsupported mixed_preconditioner: " + kv["mixed_preconditioner"]);
     }
     geti("nx", cfg->nx);
     geti("ny", cfg->ny);

@@ -1,0 +1,373 @@
+// dn_multigrid.cuh -- the FP32 inner solver of the mixed-precision pressure correction: conjugate gradients
+// preconditioned by one geometric multigrid V-cycle.
+//
+// The mixed form wraps FP32 inner solves of A e = r in an FP64 defect-correction loop that stops on the
+// reference's own rule (relative or absolute FP64 residual below pressure_tolerance, the test of
+// solve_pressure_correction_*, pressure.cpp:302-365).  The inner preconditioner does not have to be the
+// reference's IC(0): the outer loop decides the answer.  ICC/ILDLT triangular solves are one long
+// dependency chain across the grid (nx + ny anti-diagonals per sweep), while a V-cycle is a handful of
+// fully parallel passes per level, and its iteration count does not grow with the grid.
+//
+// Hierarchy.  Level 0 is the assembled 5-point operator (k_p_assemble's W,S,C,N,E slots) rounded to FP32.
+// Level l+1 halves both extents while both are even, >= 4, and the level has more than kMgCoarseMax cells.
+// Its operator is the cell-centred rediscretisation: a coarse face weight is the mean of the two fine face
+// weights it covers; the diagonal is the sum of the coarse off-diagonal weights plus half the summed
+// boundary excess (diagonal minus off-diagonal sum, non-zero only on Dirichlet sides) of the four children.
+// On the coarsest level (<= kMgCoarseMax cells) the operator is inverted exactly in FP64 (Gauss-Jordan on
+// the SPD matrix; the pure-Neumann / periodic null space is removed by the rank-one shift A + mean(diag) /
+// n * 1 1^T, which leaves the solution of a mean-free right-hand side unchanged) and applied in FP32.
+//
+// Transfer operators: bilinear cell-centred prolongation P (weights 3/4, 1/4 per direction; across a wall
+// the ghost parent mirrors the boundary cell with sign +1 for a Neumann side and -1 for a Dirichlet side;
+// periodic directions wrap) and restriction R = P^T.  Smoother: red-black Gauss-Seidel, nu sweeps red-then-
+// black before the coarse correction and nu sweeps black-then-red after it, so that the V-cycle is a
+// symmetric positive definite operator and the outer iteration is plain CG.  Vectors, operators and the
+// SpMV accumulate in FP32; the CG dot products and norms accumulate in FP64.
+#pragma once
+
+#include "dn_common.cuh"
+#include "dn_krylov.cuh"
+
+namespace dn {
+
+constexpr int kMgCoarseMax = 128;  // cells of the directly inverted coarsest level (128^2 doubles of shared memory)
+constexpr int kMgMaxLevels = 24;
+constexpr int kMgParts = 1024;     // CTAs of the CG vector kernels at most (per-CTA partial sums)
+
+// one level of the hierarchy: operator slots [5][n] (W,S,C,N,E), iterate, right-hand side, residual
+struct MgLevel {
+  const float *a;
+  float *x, *b, *r;
+  int nx, ny;
+};
+// wall folding signs of the bilinear transfer (left, right, bottom, top) and the periodicity
+struct MgFold {
+  float s[4];
+  int px, py;
+};
+
+__device__ __forceinline__ float mg_row_sum(const MgLevel &L, const float *x, int i, int j, long long r, long long n,
+                                            int px, int py) {
+  // sum of the off-diagonal terms a_s * x_nb, FP32 accumulation in slot order
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    if (k == 2) continue;
+    const float a = L.a[(size_t)k * n + r];
+    if (a != 0.0f) {
+      const long long c = slot_col<5>(i, j, k, L.nx, L.ny, px, py);
+      if (c >= 0) s += a * x[c];
+    }
+  }
+  return s;
+}
+
+// Red-black Gauss-Seidel half sweep over the cells of one colour ((i + j) & 1 == color); ny is even on every
+// smoothed level, so each row holds ny/2 cells of each colour.  first: the iterate is zero on entry, so the
+// colour's cells take b / diag and the other colour's cells are set to zero.
+__global__ void k_mg_smooth(MgLevel L, int color, int first, int px, int py) {
+  const int half = L.ny >> 1;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (unsigned)L.nx * (unsigned)half) return;
+  const int i = (int)(t / (unsigned)half);
+  const int j = 2 * (int)(t - (unsigned)i * (unsigned)half) + ((i + color) & 1);
+  const long long n = (long long)L.nx * L.ny;
+  const long long r = (long long)i * L.ny + j;
+  float s = L.b[r];
+  if (!first) s -= mg_row_sum(L, L.x, i, j, r, n, px, py);
+  L.x[r] = s / L.a[2 * n + r];
+  if (first) L.x[(long long)i * L.ny + (j ^ 1)] = 0.0f;
+}
+
+// r = b - A x on one level
+__global__ void k_mg_residual(MgLevel L, int px, int py) {
+  const unsigned n = (unsigned)L.nx * (unsigned)L.ny;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = (int)(t / (unsigned)L.ny), j = (int)(t - (unsigned)i * (unsigned)L.ny);
+  L.r[t] = L.b[t] - (L.a[2 * (size_t)n + t] * L.x[t] + mg_row_sum(L, L.x, i, j, t, n, px, py));
+}
+
+// 1D bilinear weight of coarse index I in the interpolation of fine index i (fine extent 2 * nc)
+__device__ __forceinline__ float mg_w1(int i, int I, int nc, int per, float s_lo, float s_hi) {
+  const int par = i >> 1;
+  int nb = (i & 1) ? par + 1 : par - 1;
+  float w = (par == I) ? 0.75f : 0.0f;
+  if (nb >= 0 && nb < nc) {
+    if (nb == I) w += 0.25f;
+  } else if (per) {
+    nb = nb < 0 ? nb + nc : nb - nc;
+    if (nb == I) w += 0.25f;
+  } else if (par == I) {
+    w += 0.25f * (nb < 0 ? s_lo : s_hi);
+  }
+  return w;
+}
+
+// coarse b = P^T (fine r): each coarse cell gathers the 4 x 4 fine cells whose interpolation it enters
+__global__ void k_mg_restrict(MgLevel F, MgLevel C, MgFold fold) {
+  const unsigned nc = (unsigned)C.nx * (unsigned)C.ny;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc) return;
+  const int I = (int)(t / (unsigned)C.ny), J = (int)(t - (unsigned)I * (unsigned)C.ny);
+  float sum = 0.0f;
+#pragma unroll
+  for (int di = -1; di <= 2; ++di) {
+    int i = 2 * I + di;
+    if (i < 0 || i >= F.nx) {
+      if (!fold.px) continue;
+      i = i < 0 ? i + F.nx : i - F.nx;
+    }
+    const float wx = mg_w1(i, I, C.nx, fold.px, fold.s[0], fold.s[1]);
+    if (wx == 0.0f) continue;
+    float row = 0.0f;
+#pragma unroll
+    for (int dj = -1; dj <= 2; ++dj) {
+      int j = 2 * J + dj;
+      if (j < 0 || j >= F.ny) {
+        if (!fold.py) continue;
+        j = j < 0 ? j + F.ny : j - F.ny;
+      }
+      const float wy = mg_w1(j, J, C.ny, fold.py, fold.s[2], fold.s[3]);
+      if (wy != 0.0f) row += wy * F.r[(long long)i * F.ny + j];
+    }
+    sum += wx * row;
+  }
+  C.b[t] = sum;
+}
+
+// fine x += P (coarse x): each fine cell reads its parent and the parents' neighbours toward it
+__global__ void k_mg_prolong(MgLevel C, MgLevel F, MgFold fold) {
+  const unsigned nf = (unsigned)F.nx * (unsigned)F.ny;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  const int i = (int)(t / (unsigned)F.ny), j = (int)(t - (unsigned)i * (unsigned)F.ny);
+  int I[2], J[2];
+  float wx[2], wy[2];
+  I[0] = i >> 1;
+  I[1] = (i & 1) ? I[0] + 1 : I[0] - 1;
+  wx[0] = 0.75f;
+  wx[1] = 0.25f;
+  if (I[1] < 0 || I[1] >= C.nx) {
+    if (fold.px) {
+      I[1] = I[1] < 0 ? I[1] + C.nx : I[1] - C.nx;
+    } else {
+      wx[0] += 0.25f * (I[1] < 0 ? fold.s[0] : fold.s[1]);
+      wx[1] = 0.0f;
+      I[1] = I[0];
+    }
+  }
+  J[0] = j >> 1;
+  J[1] = (j & 1) ? J[0] + 1 : J[0] - 1;
+  wy[0] = 0.75f;
+  wy[1] = 0.25f;
+  if (J[1] < 0 || J[1] >= C.ny) {
+    if (fold.py) {
+      J[1] = J[1] < 0 ? J[1] + C.ny : J[1] - C.ny;
+    } else {
+      wy[0] += 0.25f * (J[1] < 0 ? fold.s[2] : fold.s[3]);
+      wy[1] = 0.0f;
+      J[1] = J[0];
+    }
+  }
+  float v = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) v += wx[a] * wy[b] * C.x[(long long)I[a] * C.ny + J[b]];
+  F.x[t] += v;
+}
+
+// Coarse operator of level l+1 from the FP64 slots of level l (see the file header), in FP64 with an FP32 copy.
+__global__ void k_mg_coarsen(const double *af, int nxf, int nyf, double *ac, float *acf, int nxc, int nyc) {
+  const unsigned nc = (unsigned)nxc * (unsigned)nyc;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc) return;
+  const int I = (int)(t / (unsigned)nyc), J = (int)(t - (unsigned)I * (unsigned)nyc);
+  const long long nf = (long long)nxf * nyf;
+  auto at = [&](int s, int i, int j) { return af[(size_t)s * nf + (long long)i * nyf + j]; };
+  double exc = 0.0;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      const int i = 2 * I + a, j = 2 * J + b;
+      const double d = at(2, i, j);
+      double e = d + at(0, i, j) + at(1, i, j) + at(3, i, j) + at(4, i, j);
+      if (fabs(e) <= 1.0e-12 * fabs(d)) e = 0.0;  // interior and Neumann rows: round-off of an exact zero
+      exc += e;
+    }
+  const double w = 0.5 * (at(0, 2 * I, 2 * J) + at(0, 2 * I, 2 * J + 1));
+  const double s = 0.5 * (at(1, 2 * I, 2 * J) + at(1, 2 * I + 1, 2 * J));
+  const double nn = 0.5 * (at(3, 2 * I, 2 * J + 1) + at(3, 2 * I + 1, 2 * J + 1));
+  const double e = 0.5 * (at(4, 2 * I + 1, 2 * J) + at(4, 2 * I + 1, 2 * J + 1));
+  const double c = -(w + s + nn + e) + 0.5 * exc;
+  const double v[5] = {w, s, c, nn, e};
+  for (int k = 0; k < 5; ++k) {
+    ac[(size_t)k * nc + t] = v[k];
+    acf[(size_t)k * nc + t] = (float)v[k];
+  }
+}
+
+// Inverse of the coarsest operator (n <= kMgCoarseMax cells), dense, by Gauss-Jordan elimination without
+// pivoting (the matrix is SPD, shifted by mean(diag) / n on every entry when singular), in FP64 shared
+// memory; the FP32 result is stored column-major (= row-major, it is symmetric).  *flag = 1 when a pivot is
+// not positive and finite, and the caller then does not use the hierarchy.
+__global__ void k_mg_coarse_inverse(const double *a, int nx, int ny, int px, int py, int singular, float *inv,
+                                    int *flag) {
+  extern __shared__ double M[];
+  __shared__ double f[kMgCoarseMax];
+  __shared__ double shift, piv;
+  const int n = nx * ny, tid = threadIdx.x, nt = blockDim.x;
+  for (int k = tid; k < n * n; k += nt) M[k] = 0.0;
+  __syncthreads();
+  if (tid == 0) {
+    double dsum = 0.0;
+    for (int r = 0; r < n; ++r) dsum += a[2 * (size_t)n + r];
+    shift = singular ? dsum / ((double)n * (double)n) : 0.0;
+    *flag = 0;
+  }
+  __syncthreads();
+  for (int r = tid; r < n; r += nt) {
+    const int i = r / ny, j = r % ny;
+    for (int s = 0; s < 5; ++s) {
+      const double v = a[(size_t)s * n + r];
+      if (v == 0.0) continue;
+      const long long c = slot_col<5>(i, j, s, nx, ny, px, py);
+      if (c >= 0) M[r * n + (int)c] += v;  // a row owns its entries: no other thread writes row r
+    }
+    for (int c = 0; c < n; ++c) M[r * n + c] += shift;
+  }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (tid == 0) {
+      piv = M[k * n + k];
+      if (!(piv > 0.0) || !isfinite(piv)) *flag = 1;
+    }
+    __syncthreads();
+    const double p = piv;
+    if (!(p > 0.0) || !isfinite(p)) return;  // uniform across the block
+    for (int j = tid; j < n; j += nt) M[k * n + j] = (j == k) ? 1.0 / p : M[k * n + j] / p;
+    for (int i = tid; i < n; i += nt) f[i] = (i == k) ? 0.0 : M[i * n + k];
+    __syncthreads();
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e - (e / n) * n;
+      if (i == k) continue;
+      M[e] = ((j == k) ? 0.0 : M[e]) - f[i] * M[k * n + j];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < n * n; e += nt) inv[e] = (float)M[e];
+}
+
+// coarsest solve x = inv b: one thread per row; inv is symmetric, so thread i reads column i (coalesced)
+__global__ void k_mg_coarse_solve(const float *inv, MgLevel L) {
+  const int n = L.nx * L.ny, i = threadIdx.x;
+  if (i >= n) return;
+  float s = 0.0f;
+  for (int k = 0; k < n; ++k) s += inv[(size_t)k * n + i] * L.b[k];
+  L.x[i] = s;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// CG on the FP32 operator of level 0.  Scalars live on the device (slots below); the host reads only the
+// residual norm of each iteration to decide when to stop.
+// ---------------------------------------------------------------------------------------------------
+enum MgScal { kMgRz = 0, kMgPq = 1, kMgRr = 2, kMgAlpha = 3, kMgBeta = 4, kMgMeanZ = 5, kMgBad = 6 };
+
+struct MgVec {
+  SpOpT<float> A;
+  float *x, *r, *z, *p, *q;
+  double *part;  // [gridDim.x][3] per-CTA partial sums
+  double *scal;
+};
+
+// q = A p, partial sums of p.q
+__global__ void k_mgp_apply(MgVec V) {
+  __shared__ double sh[32];
+  double v[1] = {0.0};
+  const unsigned n = (unsigned)V.A.n, ny = (unsigned)V.A.ny;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int i = (int)(t / ny), j = (int)(t - (unsigned)i * ny);
+    const float s = spmv_row<5>(V.A, V.p, i, j);
+    V.q[t] = s;
+    v[0] += (double)V.p[t] * (double)s;
+  }
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) V.part[3 * blockIdx.x] = v[0];
+}
+// x += alpha p, r -= alpha q, partial sums of r.r
+__global__ void k_mgp_update(MgVec V) {
+  __shared__ double sh[32];
+  double v[1] = {0.0};
+  const float alpha = (float)V.scal[kMgAlpha];
+  const unsigned n = (unsigned)V.A.n;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    V.x[t] += alpha * V.p[t];
+    const float r = V.r[t] - alpha * V.q[t];
+    V.r[t] = r;
+    v[0] += (double)r * (double)r;
+  }
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) V.part[3 * blockIdx.x] = v[0];
+}
+// partial sums of r.z, z and r (the projected r.z of a singular system needs the last two)
+__global__ void k_mgp_rz(MgVec V) {
+  __shared__ double sh[3 * 32];
+  double v[3] = {0.0, 0.0, 0.0};
+  const unsigned n = (unsigned)V.A.n;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const double z = V.z[t], r = V.r[t];
+    v[0] += r * z;
+    v[1] += z;
+    v[2] += r;
+  }
+  block_sum<3>(v, sh);
+  if (threadIdx.x == 0) {
+    V.part[3 * blockIdx.x] = v[0];
+    V.part[3 * blockIdx.x + 1] = v[1];
+    V.part[3 * blockIdx.x + 2] = v[2];
+  }
+}
+// p = (z - mean z) + beta p (first: p = z - mean z)
+__global__ void k_mgp_direction(MgVec V, int first) {
+  const float beta = (float)V.scal[kMgBeta], mz = (float)V.scal[kMgMeanZ];
+  const unsigned n = (unsigned)V.A.n;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    V.p[t] = first ? V.z[t] - mz : (V.z[t] - mz) + beta * V.p[t];
+}
+// The scalar step after each reduction, by one warp in a fixed order.
+//   mode 0 (after k_mgp_apply):  pq, alpha = rz / pq
+//   mode 1 (after k_mgp_update): rr
+//   mode 2 (after k_mgp_rz):     mean z, rz' (projected when singular), beta = rz' / rz (0 when first), rz = rz'
+// A non-positive or non-finite pq or rz' sets kMgBad (the host ends the inner solve).
+__global__ void k_mgp_scalars(const double *part, int nparts, double *scal, int mode, int first, int project,
+                              double n) {
+  const int lane = threadIdx.x;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int p = lane; p < nparts; p += 32) {
+    s0 += part[3 * p];
+    if (mode == 2) {
+      s1 += part[3 * p + 1];
+      s2 += part[3 * p + 2];
+    }
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  if (lane != 0) return;
+  if (mode == 0) {
+    scal[kMgPq] = s0;
+    if (!(s0 > 0.0) || !isfinite(s0)) scal[kMgBad] = 1.0;
+    scal[kMgAlpha] = scal[kMgRz] / s0;
+  } else if (mode == 1) {
+    scal[kMgRr] = s0;
+  } else {
+    const double mz = project ? s1 / n : 0.0;
+    const double rz = project ? s0 - mz * s2 : s0;
+    if (!(rz > 0.0) || !isfinite(rz)) scal[kMgBad] = 1.0;
+    scal[kMgMeanZ] = mz;
+    scal[kMgBeta] = first ? 0.0 : rz / scal[kMgRz];
+    scal[kMgRz] = rz;
+  }
+}
+
+}  // namespace dn

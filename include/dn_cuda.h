@@ -50,6 +50,7 @@ typedef enum {
 } dn_pressure_scheme;
 /* arithmetic of the Krylov inner loops: plain FP64, or FP32 inner solves wrapped in FP64 defect correction */
 typedef enum { DN_PRECISION_FP64 = 0, DN_PRECISION_MIXED = 1 } dn_precision;
+typedef enum { DN_MIXED_PREC_MULTIGRID = 0, DN_MIXED_PREC_IC = 1 } dn_mixed_preconditioner;
 
 typedef struct {
   int type; /* dn_bc_type */
@@ -90,6 +91,9 @@ typedef struct {
   int device_wait_limit;           /* polls after which a device-side wait (grid barrier, wavefront hand-over)
                                       gives up and the call returns DN_ERR_TIMEOUT (0: the default, 2^22, well
                                       under a few seconds) */
+  int mixed_preconditioner;        /* dn_mixed_preconditioner: preconditioner of the FP32 inner CG of the mixed
+                                      form (0: geometric multigrid V-cycle where the grid coarsens to <= 128
+                                      cells, else the scheme's own IC(0)/ILDLT(0); 1: always IC/ILDLT) */
   /* pressure analysis (config.hpp:36-133; run_pressure_analysis_from_snapshot, pressure_analysis.cpp:156-328) */
   int analysis_enabled;            /* analysis_enabled */
   int analysis_mode;               /* dn_analysis_mode, from the analysis_mode string */
@@ -121,6 +125,7 @@ typedef struct {
   double ch_residual, ch_equation_residual, momentum_residual, pressure_residual;
   double boundary_speed_pre, boundary_speed_post;
   int refinement_cycles; /* mixed form: outer FP64 defect-correction cycles of the pressure solve */
+  int mixed_inner_multigrid; /* mixed form: 1 when the inner solves started with the multigrid preconditioner */
 } dn_report;
 
 /* Diagnostics (src/core/base/diagnostics.hpp; computed as in diagnostics.cpp:114-167). */

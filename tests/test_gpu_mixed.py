@@ -1,8 +1,10 @@
 """Mixed-precision form of the pressure solve (precision = mixed) against the FP64 oracle.
 
-The pressure correction runs FP32 inner PCG solves (FP32 operator, factor, vectors and sweeps; FP64 dot
-products and norms) inside an FP64 defect-correction loop that stops on the reference's rule applied to the
-FP64 residual.  c, mu, u and v after each step must match the FP64 reference to rel-L2 <= 1e-8 (the tolerance
+The pressure correction runs FP32 inner solves inside an FP64 defect-correction loop that stops on the
+reference's rule applied to the FP64 residual.  Two inner solvers are covered: CG preconditioned by one
+geometric multigrid V-cycle (mixed_preconditioner = multigrid, the default where the grid coarsens to <= 128
+cells) and the persistent PCG with the scheme's IC/ILDLT factor rounded to FP32 (mixed_preconditioner = ic);
+both keep FP32 operators and vectors and FP64 dot products and norms.  c, mu, u and v after each step must match the FP64 reference to rel-L2 <= 1e-8 (the tolerance
 of the mixed form); the CH and momentum solves stay FP64.
 
 The pressure itself is held to the reference's own solver error.  Stopping at a relative residual of 1e-10
@@ -46,9 +48,10 @@ def _reference_p_error(orc, cfg, step):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["multigrid", "ic"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_mixed_step_matches_fp64_oracle(dn, name):
-    cfg = CASES[name]
+def test_mixed_step_matches_fp64_oracle(dn, name, prec):
+    cfg = dict(CASES[name], mixed_preconditioner=prec)
     orc, gpu = seeded_pair(dn, cfg, seed=13)
     g = cfg["ghost"]
     for k in range(3):
@@ -62,6 +65,7 @@ def test_mixed_step_matches_fp64_oracle(dn, name):
         # the outer loop stops on the reference's FP64 criterion, after at least one FP32 inner solve
         assert rep["pressure_residual"] < cfg["pressure_tolerance"] or rep["pressure_iterations"] == 0
         assert rep["refinement_cycles"] >= 1
+        assert rep["mixed_inner_multigrid"] == (1 if prec == "multigrid" else 0)
         assert rep["ch_iterations"] == orc.report()["ch_iterations"]
 
 
@@ -71,3 +75,33 @@ def dn():
 
     m.load()
     return m
+
+
+@pytest.mark.gpu
+def test_multigrid_inner_solve_on_a_grid_without_hierarchy(dn):
+    """130 x 24 halves once to 65 x 12 (780 cells, odd): no multigrid hierarchy, the IC inner solver runs."""
+    cfg = unit(nx=130, ny=24, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg", dt=1e-4,
+               precision="mixed")
+    orc, gpu = seeded_pair(dn, cfg, seed=5)
+    orc.step(0)
+    rep = gpu.step(0)
+    assert rep["mixed_inner_multigrid"] == 0
+    assert_fields_close(orc, gpu, ("c", "mu", "u", "v"), "130x24 mixed", tol=TOL_MIXED)
+
+
+@pytest.mark.gpu
+def test_multigrid_iterations_do_not_grow_with_the_grid(dn):
+    """The V-cycle preconditioner keeps the inner CG iteration count flat from 96 x 48 to 384 x 192, where
+    the IC inner solver's count grows with the grid."""
+    counts = {}
+    for nx, ny in ((96, 48), (192, 96), (384, 192)):
+        cfg = unit(nx=nx, ny=ny, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg",
+                   body_force_y=-0.98, dt=1e-4, precision="mixed")
+        orc, gpu = seeded_pair(dn, cfg, seed=13)
+        rep = gpu.step(0)
+        assert rep["mixed_inner_multigrid"] == 1
+        assert rep["pressure_residual"] < cfg["pressure_tolerance"]
+        counts[nx] = rep["pressure_iterations"] / max(rep["refinement_cycles"], 1)
+        gpu.close()
+    print("inner iterations per refinement cycle", counts)
+    assert max(counts.values()) <= 12, counts
