@@ -24,6 +24,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "libdnoracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libdnref.so")
+# the reference with its pressure and CH dispatchers patched to call libdn_cuda (patch_reference.py)
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libdnref_cuda.so")
 
 BC_UNSET, BC_DIRICHLET, BC_NEUMANN = 0, 1, 2
 SIDES = ("left", "right", "bottom", "top")
@@ -189,6 +191,8 @@ def build(force: bool = False) -> None:
     ref = os.environ.get("DN_REFERENCE", "")
     if ref and os.path.isdir(ref):
         targets.append("ref")
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "ding_nsch_core_solver_b200", "libdn_cuda.so")):
+            targets.append("refcuda")
     cmd = ["make", "-s", "-C", HERE] + (["-B"] if force else []) + targets + ([f"REFERENCE={ref}"] if ref else [])
     subprocess.run(cmd, check=True)
 
@@ -199,7 +203,7 @@ _LIBS: dict = {}
 def _load(impl: str):
     if impl in _LIBS:
         return _LIBS[impl]
-    path = PORT_LIB if impl == "port" else REF_LIB
+    path = {"port": PORT_LIB, "reference": REF_LIB, "reference_cuda": REF_CUDA_LIB}[impl]
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is missing; run `make -C oracle`")
     lib = C.CDLL(path)
@@ -217,7 +221,7 @@ def _load(impl: str):
         "get_report": (None, [vp, C.POINTER(Report)]), "diagnostics": (None, [vp, C.POINTER(Diag)]),
         "compute_mass": (C.c_double, [vp, C.c_int]),
     }
-    if impl == "reference":
+    if impl in ("reference", "reference_cuda"):
         sig["time_steps"] = (C.c_double, [vp, C.c_int, C.c_int])
         sig["pressure_analysis"] = (C.c_int, [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                               C.c_char_p, C.c_double])
@@ -378,4 +382,4 @@ class OracleSolver:
 
 
 def available(impl: str) -> bool:
-    return os.path.exists(PORT_LIB if impl == "port" else REF_LIB)
+    return os.path.exists({"port": PORT_LIB, "reference": REF_LIB, "reference_cuda": REF_CUDA_LIB}[impl])

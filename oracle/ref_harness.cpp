@@ -64,6 +64,11 @@ ding::Config to_config(const orc_config &c) {
   case ORC_P_SPLIT_DCDM_ICPCG: cfg.pressure_scheme = "split_dcdm_icpcg"; break;
   default: cfg.pressure_scheme = "jacobi"; break;
   }
+#ifdef DN_REF_CUDA_BACKEND
+  // the patched reference: the pressure and CH solves go to libdn_cuda through the reference-side binding
+  cfg.pressure_scheme = "cuda_" + cfg.pressure_scheme;
+  cfg.ch_solver = "cuda_sparse_pcg";
+#endif
   cfg.phase_initializer = c.phase_initializer == 1 ? "zalesak_disk" : "default";
   cfg.velocity_profile = c.velocity_profile == 1 ? "solid_body_rotation" : "default";
   cfg.invert_phase = c.invert_phase != 0;

@@ -329,3 +329,27 @@ def test_failure_paths_match_reference_build():
     assert out["reference"][0] == "pcg preconditioner breakdown: non-positive r^T M^{-1} r"
     assert out["reference"][1] == "ICC preconditioner construction failed"
     assert out["reference"][2] == 3
+
+
+def test_patched_reference_build_binds_the_c_abi():
+    """oracle/_ref/libdnref_cuda.so (the reference patched by oracle/patch_reference.py) loads, and every
+    library symbol it needs is declared in include/dn_cuda.h (the CPU half of
+    tests/test_gpu_reference_binding.py)."""
+    import ctypes
+    import re
+    import subprocess
+
+    from oracle.oracle import REF_CUDA_LIB, available
+
+    if not available("reference_cuda"):
+        pytest.skip("oracle/_ref/libdnref_cuda.so not built (make -C oracle refcuda with DN_REFERENCE set)")
+    lib = ctypes.CDLL(REF_CUDA_LIB)
+    assert hasattr(lib, "ref_create") and hasattr(lib, "ref_step")
+    out = subprocess.run(["nm", "-D", "--undefined-only", REF_CUDA_LIB], capture_output=True, text=True,
+                         check=True).stdout
+    needed = sorted(set(re.findall(r"\bU (dn_\w+)", out)))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "dn_cuda.h")).read()
+    assert {"dn_create", "dn_pressure_solve", "dn_ch_linear_solve"} <= set(needed), needed
+    for name in needed:
+        assert re.search(r"\b" + name + r"\s*\(", header), name
