@@ -1285,11 +1285,21 @@ dn_status ch_linear_solve(dn_handle *h, double alpha0, dn_report *rep, double *i
 // solve_cahn_hilliard_semi_implicit, phase_field.cpp:667-708
 dn_status ch_semi_implicit(dn_handle *h, int step, dn_report *rep) {
   Fv *f = h->f;
-  DN_TRY(phase_explicit(h, f[DN_F_C], f[DN_F_U], f[DN_F_V]));
-  const double dt = h->cfg.dt;
+  const dn_config &cfg = h->cfg;
+  const double dt = cfg.dt;
   const double alpha0 = (step == 0) ? (1.0 / dt) : (3.0 / (2.0 * dt));
-  LAUNCH_INTERIOR(k_ch_rhs, h->E_new, f[DN_F_C_PREV], f[DN_F_C_PREV2], h->E_new, f[DN_F_E_PREV], h->b, h->x, f[DN_F_C],
-                  step, dt);
+  // the explicit operator E(c, u, v) and the BDF right-hand side in one tiled pass (k_ch_explicit_rhs)
+  {
+    constexpr int TI = 16, TJ = 32;
+    const double a1 = cfg.cn > 0.0 ? (3.0 * kSqrt2 / (16.0 * cfg.cn)) : 0.0;
+    const double a2 = cfg.cn > 0.0 ? (3.0 * kSqrt2 * cfg.cn / 4.0) : 0.0;
+    const dim3 grid((unsigned)((h->G.ny + TJ - 1) / TJ), (unsigned)((h->G.nx + TI - 1) / TI));
+    k_ch_explicit_rhs<TI, TJ><<<grid, 256, 0, h->stream>>>(
+        f[DN_F_C], f[DN_F_U], f[DN_F_V], f[DN_F_C_PREV], f[DN_F_C_PREV2], f[DN_F_E_PREV], h->E_new, h->b, h->x, h->G,
+        h->bc.u[DN_LEFT], h->bc.u[DN_RIGHT], h->bc.v[DN_BOTTOM], h->bc.v[DN_TOP], cfg.cn, a1, a2, cfg.pe, step, dt);
+    DN_TRY(check_launch(h, "k_ch_explicit_rhs"));
+    DN_TRY(bc(h, h->E_new, kBCScalar));
+  }
   double iter_res = 0.0, eq_res = 0.0;
   DN_TRY(ch_linear_solve(h, alpha0, rep, &iter_res, &eq_res));
   LAUNCH_INTERIOR(k_scatter_compact, f[DN_F_C], h->x, f[DN_F_C]);

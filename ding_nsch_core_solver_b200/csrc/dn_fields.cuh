@@ -265,6 +265,151 @@ __global__ void k_ch_rhs(Fv cp, Fv cp2, Fv E, Fv Ep, double *rhs, double *x0, Fv
   rhs[r] = v;
   x0[r] = c.at(i, j);
 }
+// ------------------------------------------------------------------------------------------------------
+// Fused CH explicit operator + BDF right-hand side (build_phase_explicit_operator, phase_field.cpp:354-396,
+// with the rhs of solve_cahn_hilliard_semi_implicit, :679-690): one pass over a TI x TJ tile of cells.
+// The tile of c with a 3-cell halo is staged in shared memory; the Laplacian and the chemical potential
+// on the tile plus a 1-cell halo, then the advective (WENO5) and diffusive face fluxes of the tile, are
+// computed there, and each cell writes E, the Krylov right-hand side and the initial iterate.  The result
+// is bit-for-bit that of the separate kernels (k_mob_lap, k_lap, k_chem, k_adv_flux_*, k_diff_flux_*,
+// k_flux_div, k_explicit, k_ch_rhs) with their boundary passes in between:
+//  - a halo value of a scalar field (lap, mu) outside the domain is its ghost under the scalar BC: in a
+//    wall direction the boundary cell's value (the position is clamped), in a periodic direction the value
+//    at the ghost position computed from c's periodic ghosts, whose operands equal those at the wrapped
+//    interior position;
+//  - a boundary face flux on a wall side is replaced as the face BC of a u (v) array replaces it
+//    (k_bc_faces_u/v: the Dirichlet value, or the next interior face's flux plus value * dx); in a periodic
+//    direction face nx is computed and equals face 0, whose operands it repeats.
+// Algorithmic bytes per cell: reads c, u, v, c_prev, c_prev2, E_prev; writes E, rhs, x0 (72 B).
+// ------------------------------------------------------------------------------------------------------
+template <int TI, int TJ>
+__global__ void __launch_bounds__(256) k_ch_explicit_rhs(Fv c, Fv u, Fv v, Fv cp, Fv cp2, Fv Ep, Fv E,
+                                                         double *rhs, double *x0, Grid G, BCSide uL, BCSide uR,
+                                                         BCSide vB, BCSide vT, double cn, double a1, double a2,
+                                                         double pe, int step, double dt) {
+  constexpr int CI = TI + 6, CJ = TJ + 6;  // c with a 3-cell halo
+  constexpr int HI = TI + 2, HJ = TJ + 2;  // lap and mu with a 1-cell halo
+  __shared__ double cs[CI * CJ];
+  __shared__ double laps[HI * HJ], mus[HI * HJ];
+  __shared__ double fax[(TI + 1) * TJ], fdx[(TI + 1) * TJ];  // x faces i0 .. i0+TI
+  __shared__ double fay[TI * (TJ + 1)], fdy[TI * (TJ + 1)];  // y faces j0 .. j0+TJ
+  const int nx = G.nx, ny = G.ny;
+  const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  auto C = [&](int gi, int gj) -> double { return cs[(gi - i0 + 3) * CJ + (gj - j0 + 3)]; };
+  // 1. c over the tile and its 3-cell halo (the ghost layers hold the BC values)
+  for (int e = tid; e < CI * CJ; e += nt) {
+    const int li = e / CJ, lj = e - (e / CJ) * CJ;
+    const int gi = i0 - 3 + li, gj = j0 - 3 + lj;
+    cs[e] = (gi >= -3 && gi < nx + 3 && gj >= -3 && gj < ny + 3) ? c.at(gi, gj) : 0.0;
+  }
+  __syncthreads();
+  // 2. lap (lapc) and mu (k_chem) on the tile and its 1-cell halo, corners excluded
+  const double alpha = 6.0 * 1.4142135623730950488;
+  for (int e = tid; e < HI * HJ; e += nt) {
+    const int li = e / HJ, lj = e - (e / HJ) * HJ;
+    if ((li == 0 || li == HI - 1) && (lj == 0 || lj == HJ - 1)) continue;
+    int gi = i0 - 1 + li, gj = j0 - 1 + lj;
+    if (gi > nx || gj > ny) continue;  // beyond the last ghost row / column a tile covers
+    if (!G.px) gi = min(max(gi, 0), nx - 1);
+    if (!G.py) gj = min(max(gj, 0), ny - 1);
+    const double lap = (C(gi + 1, gj) - 2.0 * C(gi, gj) + C(gi - 1, gj)) / (G.dx * G.dx) +
+                       (C(gi, gj + 1) - 2.0 * C(gi, gj) + C(gi, gj - 1)) / (G.dy * G.dy);
+    const double cc = C(gi, gj);
+    const double dw = 0.5 * cc * (1.0 - cc) * (1.0 - 2.0 * cc);
+    laps[e] = lap;
+    mus[e] = alpha * (dw / cn - cn * lap);
+  }
+  __syncthreads();
+  auto LAP = [&](int gi, int gj) -> double { return laps[(gi - i0 + 1) * HJ + (gj - j0 + 1)]; };
+  auto MU = [&](int gi, int gj) -> double { return mus[(gi - i0 + 1) * HJ + (gj - j0 + 1)]; };
+  auto mob = [](double cc) { return fmax(0.0, cc * (1.0 - cc)); };
+  // 3. face fluxes (k_adv_flux_x/y, k_diff_flux_x/y)
+  for (int e = tid; e < (TI + 1) * TJ; e += nt) {
+    const int fi = e / TJ, fj = e - (e / TJ) * TJ;
+    const int gi = i0 + fi, gj = j0 + fj;
+    if (gi > nx || gj >= ny) continue;
+    const double uu = u.at(gi, gj);
+    const double face = (uu >= 0.0) ? weno5_left(C(gi - 3, gj), C(gi - 2, gj), C(gi - 1, gj), C(gi, gj), C(gi + 1, gj))
+                                    : weno5_left(C(gi + 2, gj), C(gi + 1, gj), C(gi, gj), C(gi - 1, gj), C(gi - 2, gj));
+    fax[e] = uu * face;
+    // xface(mob): interior faces and, periodic, faces 0 and nx average the two adjacent cells (the halo of c
+    // holds the periodic neighbour); wall boundary faces are replaced below
+    const double m = 0.5 * (mob(C(gi - 1, gj)) + mob(C(gi, gj)));
+    fdx[e] = m * ((MU(gi, gj) - MU(gi - 1, gj)) / G.dx);
+  }
+  for (int e = tid; e < TI * (TJ + 1); e += nt) {
+    const int fi = e / (TJ + 1), fj = e - (e / (TJ + 1)) * (TJ + 1);
+    const int gi = i0 + fi, gj = j0 + fj;
+    if (gi >= nx || gj > ny) continue;
+    const double vv = v.at(gi, gj);
+    const double face = (vv >= 0.0) ? weno5_left(C(gi, gj - 3), C(gi, gj - 2), C(gi, gj - 1), C(gi, gj), C(gi, gj + 1))
+                                    : weno5_left(C(gi, gj + 2), C(gi, gj + 1), C(gi, gj), C(gi, gj - 1), C(gi, gj - 2));
+    fay[e] = vv * face;
+    const double m = 0.5 * (mob(C(gi, gj - 1)) + mob(C(gi, gj)));
+    fdy[e] = m * ((MU(gi, gj) - MU(gi, gj - 1)) / G.dy);
+  }
+  __syncthreads();
+  // wall boundary faces (k_bc_faces_u / k_bc_faces_v on the flux arrays)
+  if (!G.px) {
+    for (int fj = tid; fj < TJ; fj += nt) {
+      const int gj = j0 + fj;
+      if (gj >= ny) continue;
+      if (i0 == 0) {
+        const int e = fj, e1 = TJ + fj;  // faces 0 and 1
+        fax[e] = (uL.type == DN_BC_DIRICHLET) ? uL.value : fax[e1] + uL.value * G.dx;
+        fdx[e] = (uL.type == DN_BC_DIRICHLET) ? uL.value : fdx[e1] + uL.value * G.dx;
+      }
+      if (nx >= i0 && nx <= i0 + TI) {
+        const int e = (nx - i0) * TJ + fj, e1 = (nx - 1 - i0) * TJ + fj;  // faces nx and nx-1
+        fax[e] = (uR.type == DN_BC_DIRICHLET) ? uR.value : fax[e1] + uR.value * G.dx;
+        fdx[e] = (uR.type == DN_BC_DIRICHLET) ? uR.value : fdx[e1] + uR.value * G.dx;
+      }
+    }
+  }
+  if (!G.py) {
+    for (int fi = tid; fi < TI; fi += nt) {
+      const int gi = i0 + fi;
+      if (gi >= nx) continue;
+      if (j0 == 0) {
+        const int e = fi * (TJ + 1), e1 = fi * (TJ + 1) + 1;  // faces 0 and 1
+        fay[e] = (vB.type == DN_BC_DIRICHLET) ? vB.value : fay[e1] + vB.value * G.dy;
+        fdy[e] = (vB.type == DN_BC_DIRICHLET) ? vB.value : fdy[e1] + vB.value * G.dy;
+      }
+      if (ny >= j0 && ny <= j0 + TJ) {
+        const int e = fi * (TJ + 1) + (ny - j0), e1 = fi * (TJ + 1) + (ny - 1 - j0);  // faces ny and ny-1
+        fay[e] = (vT.type == DN_BC_DIRICHLET) ? vT.value : fay[e1] + vT.value * G.dy;
+        fdy[e] = (vT.type == DN_BC_DIRICHLET) ? vT.value : fdy[e1] + vT.value * G.dy;
+      }
+    }
+  }
+  __syncthreads();
+  // 4. cells: divergences, the explicit operator and the BDF right-hand side
+  for (int e = tid; e < TI * TJ; e += nt) {
+    const int li = e / TJ, lj = e - (e / TJ) * TJ;
+    const int gi = i0 + li, gj = j0 + lj;
+    if (gi >= nx || gj >= ny) continue;
+    const double axp = fax[(li + 1) * TJ + lj], axm = fax[li * TJ + lj];
+    const double ayp = fay[li * (TJ + 1) + lj + 1], aym = fay[li * (TJ + 1) + lj];
+    const double dxp = fdx[(li + 1) * TJ + lj], dxm = fdx[li * TJ + lj];
+    const double dyp = fdy[li * (TJ + 1) + lj + 1], dym = fdy[li * (TJ + 1) + lj];
+    const double arhs = -(axp - axm) / G.dx - (ayp - aym) / G.dy;
+    const double ddiv = (dxp - dxm) / G.dx + (dyp - dym) / G.dy;
+    const double bih = (LAP(gi + 1, gj) - 2.0 * LAP(gi, gj) + LAP(gi - 1, gj)) / (G.dx * G.dx) +
+                       (LAP(gi, gj + 1) - 2.0 * LAP(gi, gj) + LAP(gi, gj - 1)) / (G.dy * G.dy);
+    const double en = ddiv / pe - (a1 * LAP(gi, gj) - a2 * bih) / pe + arhs;
+    E.at(gi, gj) = en;
+    double val;
+    if (step == 0)
+      val = cp.at(gi, gj) / dt + en;
+    else
+      val = (4.0 * cp.at(gi, gj) - cp2.at(gi, gj)) / (2.0 * dt) + 2.0 * en - Ep.at(gi, gj);
+    const long long r = (long long)gi * ny + gj;
+    rhs[r] = val;
+    x0[r] = C(gi, gj);
+  }
+}
+
 __global__ void k_scatter_compact(const double *x, Fv f) {
   DN_FOR_INTERIOR(f);
   f.at(i, j) = x[(long long)i * f.ny + j];

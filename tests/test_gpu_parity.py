@@ -191,10 +191,26 @@ def test_phase_by_phase_parity(dn):
         assert_fields_close(orc, gpu, ("u", "v", "p", "p_prev"), f"correct {k}")
 
 
-def test_stencil_kernels_bitwise(dn):
+BITWISE_CASES = {
+    "walls_wide": CASES["walls_split_icpcg_wide"],
+    # the fused explicit-operator kernel works on 16 x 32 tiles: partial tiles in both directions, periodic
+    # directions (face nx = face 0), and wall sides whose flux faces take Dirichlet / Neumann values
+    "periodic_ragged": unit(nx=37, ny=45, pressure_scheme="icpcg", dt=1e-4),
+    "channel_x_ragged": unit(nx=50, ny=29, periodic_x=True, periodic_y=False, pressure_scheme="icpcg",
+                             top_wall_velocity_x=0.5, bottom_wall_velocity_x=-0.5, dt=1e-4),
+    "bc_values": unit(nx=33, ny=70, periodic_x=False, periodic_y=False, pressure_scheme="split_icpcg", dt=1e-4,
+                      u_bc_left_type="dirichlet", u_bc_left_value=-0.5, u_bc_right_type="neumann",
+                      u_bc_right_value=0.25, v_bc_bottom_type="dirichlet", v_bc_bottom_value=-1.2,
+                      v_bc_top_type="neumann", v_bc_top_value=0.3),
+}
+
+
+@pytest.mark.parametrize("name", sorted(BITWISE_CASES))
+def test_stencil_kernels_bitwise(dn, name):
     """With --fmad=false the explicit stencil phase reproduces the reference's doubles exactly: compare the CH
-    explicit operator stored as E_prev after one phase, and the surface forces."""
-    cfg = CASES["walls_split_icpcg_wide"]
+    explicit operator stored as E_prev after one phase (the fused tiled kernel k_ch_explicit_rhs), and the
+    surface forces."""
+    cfg = BITWISE_CASES[name]
     orc, gpu = seeded_pair(dn, cfg, seed=3)
     orc.begin_step(1)
     gpu.begin_step(1)
