@@ -1160,17 +1160,16 @@ dn_status surface_force(dn_handle *h, const Fv &c_old, const Fv &c_new) {
   const dn_config &cfg = h->cfg;
   if (cfg.surface_tension_multiplier == 0.0 || !compute_mu(cfg)) return clear_surface_force(h);
   Fv *f = h->f;
-  DN_TRY(copy_field(h, h->cmid, c_new));
-  LAUNCH_INTERIOR(k_cmid, h->cmid, c_old, c_new, h->cmid);
-  DN_TRY(bc(h, h->cmid, kBCScalar));
-  DN_TRY(fill_field(h, h->mm, 0.0));
-  DN_TRY(chem(h, h->cmid, h->mm));
   const double scale = cfg.surface_tension_multiplier / (cfg.re * cfg.ca);
-  LAUNCH_INTERIOR(k_sf_cell, f[DN_F_SFX_CELL], h->mm, h->cmid, f[DN_F_SFX_CELL], f[DN_F_SFY_CELL], h->G, scale);
+  {  // c_mid, mu_mid and the four forces in one tiled pass (k_surface_force)
+    constexpr int TI = 16, TJ = 32;
+    const dim3 grid((unsigned)((h->G.ny + TJ - 1) / TJ), (unsigned)((h->G.nx + TI - 1) / TI));
+    k_surface_force<TI, TJ><<<grid, 256, 0, h->stream>>>(c_old, c_new, f[DN_F_SFX_CELL], f[DN_F_SFY_CELL],
+                                                         f[DN_F_SFX_U], f[DN_F_SFY_V], h->G, cfg.cn, scale);
+    DN_TRY(check_launch(h, "k_surface_force"));
+  }
   DN_TRY(bc(h, f[DN_F_SFX_CELL], kBCScalar));
   DN_TRY(bc(h, f[DN_F_SFY_CELL], kBCScalar));
-  LAUNCH_INTERIOR(k_sf_u, f[DN_F_SFX_U], h->mm, h->cmid, f[DN_F_SFX_U], h->G, scale);
-  LAUNCH_INTERIOR(k_sf_v, f[DN_F_SFY_V], h->mm, h->cmid, f[DN_F_SFY_V], h->G, scale);
   DN_TRY(bc(h, f[DN_F_SFX_U], kBCU));
   DN_TRY(bc(h, f[DN_F_SFY_V], kBCV));
   if (cfg.surface_tension_smoothing_passes <= 0 || cfg.surface_tension_smoothing_weight <= 0.0) return DN_OK;
@@ -1336,17 +1335,15 @@ dn_status phase(dn_handle *h, int step, dn_report *rep) {
 dn_status momentum(dn_handle *h, int step, dn_report *rep) {
   Fv *f = h->f;
   const dn_config &cfg = h->cfg;
-  DN_TRY(fill_field(h, h->hu, 0.0));
-  DN_TRY(fill_field(h, h->hv, 0.0));
-  LAUNCH_INTERIOR(k_mom_flux_u, h->hu, f[DN_F_U], f[DN_F_V], h->hu, h->G);
-  LAUNCH_INTERIOR(k_mom_flux_v, h->hv, f[DN_F_U], f[DN_F_V], h->hv, h->G);
-  DN_TRY(bc(h, h->hu, kBCU));
-  DN_TRY(bc(h, h->hv, kBCV));
   const double alpha = 0.5 * cfg.dt / cfg.re;
-  LAUNCH_INTERIOR(k_mom_rhs_u, h->urhs, f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hu, f[DN_F_HU_PREV],
-                  f[DN_F_SFX_U], h->urhs, h->G, step, cfg.dt, alpha, cfg.body_force_x);
-  LAUNCH_INTERIOR(k_mom_rhs_v, h->vrhs, f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hv, f[DN_F_HV_PREV],
-                  f[DN_F_SFY_V], h->vrhs, h->G, step, cfg.dt, alpha, cfg.body_force_y);
+  // H (centred convection, with the face BC of the flux arrays) and the predictor rhs in one pass
+  k_mom_conv_rhs<<<blocks_for(h->nm), 256, 0, h->stream>>>(
+      f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hu, h->hv, f[DN_F_HU_PREV], f[DN_F_HV_PREV],
+      f[DN_F_SFX_U], f[DN_F_SFY_V], h->urhs, h->vrhs, h->G, h->bc.u[DN_LEFT], h->bc.u[DN_RIGHT], h->bc.v[DN_BOTTOM],
+      h->bc.v[DN_TOP], step, cfg.dt, alpha, cfg.body_force_x, cfg.body_force_y);
+  DN_TRY(check_launch(h, "k_mom_conv_rhs"));
+  DN_TRY(bc(h, h->hu, kBCU));  // the ghosts of H (the faces it recomputes are the values already written)
+  DN_TRY(bc(h, h->hv, kBCV));
   k_mom_assemble<<<blocks_for(h->nm, 128), 128, 0, h->stream>>>(h->ml, h->G, h->bc, f[DN_F_U], f[DN_F_V], f[DN_F_RHO_MID],
                                                            f[DN_F_ETA], h->urhs, h->vrhs, alpha, h->mcoef, h->mtgt, h->mb,
                                                            h->mx);

@@ -445,6 +445,69 @@ __global__ void k_sf_cell(Fv mm, Fv cm, Fv fxc, Fv fyc, Grid G, double scale) {
   fxc.at(i, j) = scale * mm.at(i, j) * ((cm.at(i + 1, j) - cm.at(i - 1, j)) / (2.0 * G.dx));
   fyc.at(i, j) = scale * mm.at(i, j) * ((cm.at(i, j + 1) - cm.at(i, j - 1)) / (2.0 * G.dy));
 }
+// Fused surface force (update_surface_tension_force, phase_field.cpp:179-226): c_mid = (c_old + c_new) / 2
+// and its chemical potential mu_mid on a TI x TJ tile with halos in shared memory, then the cell forces
+// (k_sf_cell) and the face forces (k_sf_u / k_sf_v) of the tile.  Bit-for-bit the separate kernels with
+// their boundary passes: c_mid at a ghost position is the half sum of the two ghost values, which is the
+// scalar BC's ghost of c_mid (clamp or periodic copy); mu_mid at a halo position outside a wall side is the
+// boundary cell's value (clamped), in a periodic direction the value computed at the ghost position.  The
+// wall boundary faces written here are replaced by the caller's face BC pass, as before.
+// Algorithmic bytes per cell: reads c_old, c_new; writes the two cell forces and the two face forces (48 B).
+template <int TI, int TJ>
+__global__ void __launch_bounds__(256) k_surface_force(Fv co, Fv cn_, Fv fxc, Fv fyc, Fv fxu, Fv fyv, Grid G,
+                                                       double cn, double scale) {
+  constexpr int MI = TI + 4, MJ = TJ + 4;  // c_mid with a 2-cell halo
+  constexpr int HI = TI + 2, HJ = TJ + 2;  // mu_mid with a 1-cell halo
+  __shared__ double cms[MI * MJ], mms[HI * HJ];
+  const int nx = G.nx, ny = G.ny;
+  const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < MI * MJ; e += nt) {
+    const int li = e / MJ, lj = e - (e / MJ) * MJ;
+    const int gi = i0 - 2 + li, gj = j0 - 2 + lj;
+    cms[e] = (gi < nx + 3 && gj < ny + 3) ? 0.5 * (co.at(gi, gj) + cn_.at(gi, gj)) : 0.0;
+  }
+  __syncthreads();
+  auto CM = [&](int gi, int gj) -> double { return cms[(gi - i0 + 2) * MJ + (gj - j0 + 2)]; };
+  const double alpha = 6.0 * 1.4142135623730950488;
+  for (int e = tid; e < HI * HJ; e += nt) {
+    const int li = e / HJ, lj = e - (e / HJ) * HJ;
+    if ((li == 0 || li == HI - 1) && (lj == 0 || lj == HJ - 1)) continue;
+    int gi = i0 - 1 + li, gj = j0 - 1 + lj;
+    if (gi > nx || gj > ny) continue;
+    if (!G.px) gi = min(max(gi, 0), nx - 1);
+    if (!G.py) gj = min(max(gj, 0), ny - 1);
+    const double lap = (CM(gi + 1, gj) - 2.0 * CM(gi, gj) + CM(gi - 1, gj)) / (G.dx * G.dx) +
+                       (CM(gi, gj + 1) - 2.0 * CM(gi, gj) + CM(gi, gj - 1)) / (G.dy * G.dy);
+    const double cc = CM(gi, gj);
+    const double dw = 0.5 * cc * (1.0 - cc) * (1.0 - 2.0 * cc);
+    mms[e] = alpha * (dw / cn - cn * lap);
+  }
+  __syncthreads();
+  auto MM = [&](int gi, int gj) -> double { return mms[(gi - i0 + 1) * HJ + (gj - j0 + 1)]; };
+  for (int e = tid; e < TI * TJ; e += nt) {
+    const int li = e / TJ, lj = e - (e / TJ) * TJ;
+    const int gi = i0 + li, gj = j0 + lj;
+    if (gi >= nx || gj >= ny) continue;
+    fxc.at(gi, gj) = scale * MM(gi, gj) * ((CM(gi + 1, gj) - CM(gi - 1, gj)) / (2.0 * G.dx));
+    fyc.at(gi, gj) = scale * MM(gi, gj) * ((CM(gi, gj + 1) - CM(gi, gj - 1)) / (2.0 * G.dy));
+  }
+  // faces i0 .. i0+TI-1 of this tile, and face nx in the last tile
+  for (int e = tid; e < (TI + 1) * TJ; e += nt) {
+    const int fi = e / TJ, fj = e - (e / TJ) * TJ;
+    const int gi = i0 + fi, gj = j0 + fj;
+    if (gj >= ny || gi > nx || (fi == TI && gi != nx)) continue;
+    const double mf = 0.5 * (MM(gi - 1, gj) + MM(gi, gj));
+    fxu.at(gi, gj) = scale * mf * ((CM(gi, gj) - CM(gi - 1, gj)) / G.dx);
+  }
+  for (int e = tid; e < TI * (TJ + 1); e += nt) {
+    const int fi = e / (TJ + 1), fj = e - (e / (TJ + 1)) * (TJ + 1);
+    const int gi = i0 + fi, gj = j0 + fj;
+    if (gi >= nx || gj > ny || (fj == TJ && gj != ny)) continue;
+    const double mf = 0.5 * (MM(gi, gj - 1) + MM(gi, gj));
+    fyv.at(gi, gj) = scale * mf * ((CM(gi, gj) - CM(gi, gj - 1)) / G.dy);
+  }
+}
 // smoothing pass, phase_field.cpp:234-249
 __global__ void k_smooth(Fv f, Fv out, double cw, double nw) {
   DN_FOR_INTERIOR(out);

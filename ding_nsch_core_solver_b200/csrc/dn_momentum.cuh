@@ -231,6 +231,71 @@ __global__ void k_mom_rhs_v(Fv u, Fv v, Fv rm, Fv etap, Fv hv, Fv hvp, Fv fyv, F
   out.at(i, j) = rf * v.at(i, j) + dt * (-rf * conv + rf * bfy + fyv.at(i, j)) + alpha * vo;
 }
 
+// Fused momentum convection + right-hand side (compute_momentum_fluxes, momentum.cpp:55-85, with the rhs of
+// solve_momentum_predictor, :167-187): one thread per u face (t < nu) or v face, writing H (hu / hv) and the
+// rhs (urhs / vrhs) in one pass.  The face BC that the flux arrays get before the rhs reads them
+// (k_bc_faces_u / k_bc_faces_v) is applied in the thread: a wall boundary face takes the Dirichlet value or
+// the next interior face's H (recomputed here) plus value * spacing; on a periodic side face nx (ny) takes
+// face 0's H, computed from the same operands.  Bit-for-bit k_mom_flux_u/v + the face BC + k_mom_rhs_u/v;
+// the caller still runs the ghost pass of H.  Algorithmic bytes per face: reads u, v, rho_mid, eta_prev,
+// H_prev and the face force; writes H and the rhs (64 B).
+__device__ __forceinline__ double mom_flux_u_at(const Fv &u, const Fv &v, const Grid &G, int i, int j) {
+  const double uf = u.at(i, j);
+  const double dudx = (u.at(i + 1, j) - u.at(i - 1, j)) / (2.0 * G.dx);
+  const double dudy = (u.at(i, j + 1) - u.at(i, j - 1)) / (2.0 * G.dy);
+  const double vf = 0.25 * (v.at(i - 1, j) + v.at(i, j) + v.at(i - 1, j + 1) + v.at(i, j + 1));
+  return uf * dudx + vf * dudy;
+}
+__device__ __forceinline__ double mom_flux_v_at(const Fv &u, const Fv &v, const Grid &G, int i, int j) {
+  const double vf = v.at(i, j);
+  const double dvdx = (v.at(i + 1, j) - v.at(i - 1, j)) / (2.0 * G.dx);
+  const double dvdy = (v.at(i, j + 1) - v.at(i, j - 1)) / (2.0 * G.dy);
+  const double uf = 0.25 * (u.at(i, j - 1) + u.at(i, j) + u.at(i + 1, j - 1) + u.at(i + 1, j));
+  return uf * dvdx + vf * dvdy;
+}
+__global__ void k_mom_conv_rhs(Fv u, Fv v, Fv rm, Fv etap, Fv hu, Fv hv, Fv hup, Fv hvp, Fv fxu, Fv fyv, Fv urhs,
+                               Fv vrhs, Grid G, BCSide uL, BCSide uR, BCSide vB, BCSide vT, int step, double dt,
+                               double alpha, double bfx, double bfy) {
+  const long long nu = (long long)(G.nx + 1) * G.ny, nv = (long long)G.nx * (G.ny + 1);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nu) {
+    const int i = (int)(t / G.ny), j = (int)(t - (t / G.ny) * G.ny);
+    double h;
+    if (G.px) {
+      h = mom_flux_u_at(u, v, G, i == G.nx ? 0 : i, j);
+    } else if (i == 0) {
+      h = (uL.type == DN_BC_DIRICHLET) ? uL.value : mom_flux_u_at(u, v, G, 1, j) + uL.value * G.dx;
+    } else if (i == G.nx) {
+      h = (uR.type == DN_BC_DIRICHLET) ? uR.value : mom_flux_u_at(u, v, G, G.nx - 1, j) + uR.value * G.dx;
+    } else {
+      h = mom_flux_u_at(u, v, G, i, j);
+    }
+    hu.at(i, j) = h;
+    const double rf = xface(rm, G, i, j);
+    const double conv = (step == 0) ? h : 1.5 * h - 0.5 * hup.at(i, j);
+    const double vo = visc_u(u, v, etap, G, i, j);
+    urhs.at(i, j) = rf * u.at(i, j) + dt * (-rf * conv + rf * bfx + fxu.at(i, j)) + alpha * vo;
+  } else if (t < nu + nv) {
+    const long long q = t - nu;
+    const int i = (int)(q / (G.ny + 1)), j = (int)(q - (q / (G.ny + 1)) * (G.ny + 1));
+    double h;
+    if (G.py) {
+      h = mom_flux_v_at(u, v, G, i, j == G.ny ? 0 : j);
+    } else if (j == 0) {
+      h = (vB.type == DN_BC_DIRICHLET) ? vB.value : mom_flux_v_at(u, v, G, i, 1) + vB.value * G.dy;
+    } else if (j == G.ny) {
+      h = (vT.type == DN_BC_DIRICHLET) ? vT.value : mom_flux_v_at(u, v, G, i, G.ny - 1) + vT.value * G.dy;
+    } else {
+      h = mom_flux_v_at(u, v, G, i, j);
+    }
+    hv.at(i, j) = h;
+    const double rf = yface(rm, G, i, j);
+    const double conv = (step == 0) ? h : 1.5 * h - 0.5 * hvp.at(i, j);
+    const double vo = visc_v(u, v, etap, G, i, j);
+    vrhs.at(i, j) = rf * v.at(i, j) + dt * (-rf * conv + rf * bfy + fyv.at(i, j)) + alpha * vo;
+  }
+}
+
 // scatter of the solution into u*, v* (momentum.cpp:474-489); u*, v* were copied from u, v first
 __global__ void k_mom_scatter(MomLayout L, const double *x, Fv us, Fv vs) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
