@@ -276,7 +276,7 @@ def run_ours(args):
             reports.append(rep)
             step += 1
     launches = solver.kernel_launches() - launches0
-    plain_fields = {n: solver.get_field(n) for n in ("p", "u", "v")}
+    plain_fields = {n: solver.get_field(n) for n in ("c", "mu", "u", "v", "p")}
     total_ms = sum(times)
     total_ms = reduce_max(dist, total_ms)
     value = n_cells * args.steps * world / (total_ms * 1e-3) / 1e6
@@ -315,7 +315,7 @@ def run_ours(args):
         for _ in range(step - args.steps * 2):  # as many untimed steps as the plain run took
             msolver.step(mstep)
             mstep += 1
-        mtimes, mreps = [], []
+        mtimes, mreps, mphases = [], [], []
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -325,6 +325,7 @@ def run_ours(args):
             e1.record(mstream)
             e1.synchronize()
             mtimes.append(e0.elapsed_time(e1))
+            mphases.append(msolver.phase_times_ms())
             mstep += 1
         g = cfg["ghost"]
         errs = {}
@@ -341,7 +342,14 @@ def run_ours(args):
                  "inner_tolerance": 1e-5,
                  "inner_preconditioner": ("multigrid V-cycle" if all(r["mixed_inner_multigrid"] for r in mreps)
                                           else "IC(0)/ILDLT(0) wavefront"),
+                 # the plain FP64 step is the oracle's to rel-L2 <= 1e-10 (tests/test_gpu_configs.py)
                  "rel_l2_vs_plain_fp64": {k: float(f"{v:.3e}") for k, v in errs.items()},
+                 "ch_iterations_mean": statistics.mean(r["ch_iterations"] for r in mreps),
+                 "phase_ms_mean": {k: round(statistics.mean(p[i] for p in mphases), 4) for i, k in enumerate(
+                     ("ch", "momentum", "pressure", "correction", "pressure_inner_solves", "ch_inner_solves",
+                      "bicgstab_kernel"))},
+                 "ch_solver": ("FP32 CG, (K + s I)^-2 V-cycles, FP64 defect correction"
+                               if all(r["ch_preconditioner"] == 3 for r in mreps) else "FP64 ILDLT-PCG"),
                  "compared_after_steps": mstep}
         msolver.close()
 

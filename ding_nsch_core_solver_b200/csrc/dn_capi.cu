@@ -123,12 +123,13 @@ __global__ void k_to_float(const double *src, float *dst, long long n) {
   if (t < n) dst[t] = (float)src[t];
 }
 // r = b - A x in FP64, with per-CTA sums of r, r^2 and b^2 (the outer residual and its stopping norms)
+template <int S>
 __global__ void k_outer_residual(SpOp A, const double *b, const double *x, double *r, double *partials) {
   __shared__ double sh[3 * 32];
   double v[3] = {0.0, 0.0, 0.0};
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < A.n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / A.ny), j = (int)(t % A.ny);
-    const double rr = b[t] - spmv_row<5>(A, x, i, j);
+    const double rr = b[t] - spmv_row<S>(A, x, i, j);
     r[t] = rr;
     v[0] += rr;
     v[1] += rr * rr;
@@ -170,6 +171,23 @@ __global__ void k_inner_rhs(const double *r, double mean, float *rf, float *ef, 
 __global__ void k_add_correction(double *x, const float *e, long long n) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) x[t] += (double)e[t];
+}
+// x += e with per-CTA sums of e^2 and of the updated x^2 (the iterate residual |dx| / |x| of the CH report)
+__global__ void k_add_correction_norms(double *x, const float *e, long long n, double *partials) {
+  __shared__ double sh[3 * 32];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const double d = (double)e[t], xn = x[t] + d;
+    x[t] = xn;
+    v[0] += d * d;
+    v[1] += xn * xn;
+  }
+  block_sum<3>(v, sh);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x + 0] = v[0];
+    partials[3 * blockIdx.x + 1] = v[1];
+    partials[3 * blockIdx.x + 2] = 0.0;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -367,6 +385,25 @@ __global__ void k_init_v(Fv v, Grid G, InitParams P) {
 // ---------------------------------------------------------------------------------------------------
 // Handle
 // ---------------------------------------------------------------------------------------------------
+// A multigrid hierarchy on the device (dn_multigrid.cuh): lv[0] is the finest level, whose arrays may belong to
+// the caller; levels >= 1 own theirs.  Empty when the grid does not coarsen to <= kMgCoarseMax cells.
+struct MgHier {
+  struct Lv {
+    int nx = 0, ny = 0;
+    const double *a64 = nullptr;  // FP64 operator slots (the source of the coarse operators)
+    double *a64_own = nullptr;
+    const float *a = nullptr;
+    float *x = nullptr, *b = nullptr, *r = nullptr;
+  };
+  std::vector<Lv> lv;
+  float *inv = nullptr;  // the coarsest level's inverse
+  int *flag = nullptr;
+  MgFold fold{};
+  double mass = 0.0;  // uniform diagonal term of level 0 (CH: the shift s)
+  int singular = 0;   // pure-Neumann / periodic pressure: shift the coarsest matrix's null space away
+  int levels() const { return (int)lv.size(); }
+};
+
 struct dn_handle {
   dn_config cfg;
   int device = 0;
@@ -397,7 +434,7 @@ struct dn_handle {
   long long nm = 0;
   MomLayout ml;
   double *mcoef = nullptr;
-  long long *mtgt = nullptr;
+  int *mtgt = nullptr;
   double *mb = nullptr, *mx = nullptr, *mr = nullptr, *mrhat = nullptr, *mp0 = nullptr, *mp1 = nullptr, *mv0 = nullptr,
          *mv1 = nullptr, *mphat = nullptr, *ms = nullptr, *mshat = nullptr, *mt = nullptr, *mupd = nullptr,
          *mdinv = nullptr;
@@ -439,19 +476,25 @@ struct dn_handle {
         *fap = nullptr;
   int sw5f = 0, sw5f_blocks_max = 0;
   size_t sw5f_warp_smem[2] = {0, 0};
-  // mixed form, multigrid-preconditioned inner CG (dn_multigrid.cuh).  Level 0 is the FP32 operator fa5 with
-  // the inner CG's r as right-hand side, z as iterate and fy as residual; mg[l - 1] holds level l >= 1.
-  struct MgHost {
-    int nx = 0, ny = 0;
-    double *a64 = nullptr;
-    float *a = nullptr, *x = nullptr, *b = nullptr, *r = nullptr;
+  // mixed form, multigrid-preconditioned inner CG (dn_multigrid.cuh): the pressure hierarchy (level 0 = the
+  // FP32 pressure operator fa5, with the inner CG's r / z and fy as its right-hand side / iterate / residual)
+  // and the CH preconditioner's hierarchy (level 0 = the shifted Laplacian K + s I, own buffers).
+  MgHier mgp, mgc;
+  double *mg_scal = nullptr, *mg_part = nullptr;  // CG scalars and per-CTA partial sums (one solve at a time)
+  // one V-cycle of a hierarchy for one (right-hand side, result) pair, captured once as a CUDA graph
+  struct MgGraph {
+    const MgHier *H;
+    const float *b0;
+    const float *x0;
+    cudaGraphExec_t exec;
+    long long nodes;
   };
-  std::vector<MgHost> mg;
-  int mg_levels = 0;  // levels including level 0; 0 = no hierarchy for this grid (the IC inner solver runs)
-  float *mg_inv = nullptr;
-  double *mg_scal = nullptr, *mg_part = nullptr;
-  int *mg_flag = nullptr;
-  MgFold mg_fold{};
+  std::vector<MgGraph> mg_graphs;
+  // mixed CH solve: FP32 13-point operator and CG vectors; the alpha0 its operator and hierarchy were built for
+  float *fa13 = nullptr, *cx32 = nullptr, *cr32 = nullptr, *cz32 = nullptr, *cp32 = nullptr, *cq32 = nullptr,
+        *ct32 = nullptr, *cb32 = nullptr;
+  double ch_mg_alpha0 = -1.0;
+  bool ch_mg = false;  // the CH solve runs the mixed form (FP64 defect correction around the FP32 inner CG)
   bool ic32_ready = false;  // FP32 copies of the IC/ILDLT factor made for this solve
   bool mixed_used_mg = false;  // the last mixed pressure solve started with the multigrid inner solver
   int refinement_cycles = 0;  // outer cycles of the last mixed-precision pressure solve
@@ -837,64 +880,113 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
 // ---------------------------------------------------------------------------------------------------
 // Multigrid-preconditioned FP32 inner CG of the mixed form (kernels and design: dn_multigrid.cuh)
 // ---------------------------------------------------------------------------------------------------
-MgLevel mg_level(dn_handle *h, int l) {
-  if (l == 0) return MgLevel{h->fa5, h->fz, h->fr, h->fy, h->G.nx, h->G.ny};
-  const dn_handle::MgHost &m = h->mg[l - 1];
+MgLevel mg_level(const MgHier &H, int l) {
+  const MgHier::Lv &m = H.lv[l];
   return MgLevel{m.a, m.x, m.b, m.r, m.nx, m.ny};
 }
 
-// Coarse operators of the current pressure matrix and the inverse of the coarsest one.  *usable = false when
-// the coarsest matrix has a non-positive pivot (the caller then runs the IC inner solver).
-dn_status mg_setup(dn_handle *h, bool *usable) {
-  *usable = false;
-  const double *af = h->a5;
-  int nxf = h->G.nx, nyf = h->G.ny;
-  for (int l = 1; l < h->mg_levels; ++l) {
-    dn_handle::MgHost &m = h->mg[l - 1];
-    k_mg_coarsen<<<blocks_for((long long)m.nx * m.ny), 256, 0, h->stream>>>(af, nxf, nyf, m.a64, m.a, m.nx, m.ny);
-    DN_TRY(check_launch(h, "k_mg_coarsen"));
-    af = m.a64;
-    nxf = m.nx;
-    nyf = m.ny;
+// Levels 1.. of a hierarchy whose level 0 is an nx x ny grid: halve both extents while they are even and >= 4
+// and the level is larger than the direct coarse solve.  Leaves H empty when the grid never gets there.
+dn_status mg_alloc(dn_handle *h, MgHier &H, int nx, int ny, const BCSide *sides) {
+  std::vector<std::pair<int, int>> dims{{nx, ny}};
+  int lx = nx, ly = ny;
+  while ((long long)lx * ly > kMgCoarseMax && lx % 2 == 0 && ly % 2 == 0 && lx >= 4 && ly >= 4 &&
+         (int)dims.size() < kMgMaxLevels) {
+    lx /= 2;
+    ly /= 2;
+    dims.push_back({lx, ly});
   }
-  const int nc = nxf * nyf;
-  k_mg_coarse_inverse<<<1, 256, sizeof(double) * nc * nc, h->stream>>>(af, nxf, nyf, h->G.px, h->G.py,
-                                                                         h->has_dirichlet ? 0 : 1, h->mg_inv,
-                                                                         h->mg_flag);
+  H.lv.clear();
+  if ((long long)lx * ly > kMgCoarseMax) return DN_OK;
+  dn_status s = DN_OK;
+  auto A = [&](dn_status st) {
+    if (s == DN_OK) s = st;
+  };
+  H.lv.resize(dims.size());
+  H.lv[0].nx = nx;
+  H.lv[0].ny = ny;
+  for (size_t l = 1; l < dims.size(); ++l) {
+    MgHier::Lv &m = H.lv[l];
+    m.nx = dims[l].first;
+    m.ny = dims[l].second;
+    const size_t nl = (size_t)m.nx * m.ny;
+    double *a64 = nullptr;
+    float *a = nullptr;
+    A(dalloc(h, &a64, 5 * nl));
+    A(dalloc(h, &a, 5 * nl));
+    A(dalloc(h, &m.x, nl));
+    A(dalloc(h, &m.b, nl));
+    A(dalloc(h, &m.r, nl));
+    m.a64 = m.a64_own = a64;
+    m.a = a;
+  }
+  A(dalloc(h, &H.inv, (size_t)kMgCoarseMax * kMgCoarseMax));
+  A(dalloc(h, &H.flag, 1));
+  if (s != DN_OK) {
+    H.lv.clear();
+    return s;
+  }
+  for (int k = 0; k < 4; ++k) H.fold.s[k] = sides[k].type == DN_BC_DIRICHLET ? -1.0f : 1.0f;
+  H.fold.px = h->G.px;
+  H.fold.py = h->G.py;
+  cudaFuncSetAttribute(k_mg_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(double) * kMgCoarseMax * kMgCoarseMax));
+  return DN_OK;
+}
+
+// Coarse operators of H's current level-0 operator and the inverse of the coarsest one.  *usable = false when
+// the coarsest matrix has a non-positive pivot (the caller then does not use the hierarchy).
+dn_status mg_setup(dn_handle *h, MgHier &H, bool *usable) {
+  *usable = false;
+  double mass = H.mass;
+  for (int l = 1; l < H.levels(); ++l) {
+    const MgHier::Lv &f = H.lv[l - 1];
+    MgHier::Lv &m = H.lv[l];
+    k_mg_coarsen<<<blocks_for((long long)m.nx * m.ny), 256, 0, h->stream>>>(f.a64, f.nx, f.ny, mass, m.a64_own,
+                                                                            const_cast<float *>(m.a), m.nx, m.ny);
+    DN_TRY(check_launch(h, "k_mg_coarsen"));
+    mass *= 4.0;
+  }
+  const MgHier::Lv &c = H.lv.back();
+  const int nc = c.nx * c.ny;
+  k_mg_coarse_inverse<<<1, 256, sizeof(double) * nc * nc, h->stream>>>(c.a64, c.nx, c.ny, h->G.px, h->G.py,
+                                                                         H.singular, H.inv, H.flag);
   DN_TRY(check_launch(h, "k_mg_coarse_inverse"));
   int flag = 0;
-  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 33, h->mg_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 33, H.flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
   std::memcpy(&flag, h->host_scal + 33, sizeof(int));
   *usable = flag == 0;
   return DN_OK;
 }
 
-// z = B r: one V-cycle from level 0 (right-hand side h->fr, result h->fz)
-dn_status mg_vcycle(dn_handle *h) {
+// x0 = B b0: one V-cycle from level 0 with right-hand side b0 and result x0 (level 0's residual buffer is
+// H.lv[0].r)
+dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
   constexpr int kSweeps = 2;  // red-black sweeps before and after each coarse correction
-  const int L = h->mg_levels, px = h->G.px, py = h->G.py;
+  const int L = H.levels(), px = h->G.px, py = h->G.py;
+  H.lv[0].b = b0;
+  H.lv[0].x = x0;
   auto smooth = [&](const MgLevel &M, int color, int first) -> dn_status {
     k_mg_smooth<<<blocks_for((long long)M.nx * (M.ny / 2)), 256, 0, h->stream>>>(M, color, first, px, py);
     return check_launch(h, "k_mg_smooth");
   };
   for (int l = 0; l + 1 < L; ++l) {
-    const MgLevel F = mg_level(h, l), C = mg_level(h, l + 1);
+    const MgLevel F = mg_level(H, l), C = mg_level(H, l + 1);
     for (int k = 0; k < kSweeps; ++k) {
       DN_TRY(smooth(F, 0, k == 0));
       DN_TRY(smooth(F, 1, 0));
     }
     k_mg_residual<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(F, px, py);
     DN_TRY(check_launch(h, "k_mg_residual"));
-    k_mg_restrict<<<blocks_for((long long)C.nx * C.ny), 256, 0, h->stream>>>(F, C, h->mg_fold);
+    k_mg_restrict<<<blocks_for((long long)C.nx * C.ny), 256, 0, h->stream>>>(F, C, H.fold);
     DN_TRY(check_launch(h, "k_mg_restrict"));
   }
-  const MgLevel Lc = mg_level(h, L - 1);
-  k_mg_coarse_solve<<<1, kMgCoarseMax, 0, h->stream>>>(h->mg_inv, Lc);
+  k_mg_coarse_solve<<<1, kMgCoarseMax, 0, h->stream>>>(H.inv, mg_level(H, L - 1));
   DN_TRY(check_launch(h, "k_mg_coarse_solve"));
   for (int l = L - 2; l >= 0; --l) {
-    const MgLevel F = mg_level(h, l), C = mg_level(h, l + 1);
-    k_mg_prolong<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(C, F, h->mg_fold);
+    const MgLevel F = mg_level(H, l), C = mg_level(H, l + 1);
+    k_mg_prolong<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(C, F, H.fold);
     DN_TRY(check_launch(h, "k_mg_prolong"));
     for (int k = 0; k < kSweeps; ++k) {
       DN_TRY(smooth(F, 1, 0));
@@ -904,17 +996,45 @@ dn_status mg_vcycle(dn_handle *h) {
   return DN_OK;
 }
 
-// One FP32 inner solve A e = b (b = h->fb, e = h->fx, zero on entry) by CG with the V-cycle preconditioner,
-// to the relative residual tol of |b| = bnorm (the FP64 norm of the outer residual).  out: [0] iterations.
-dn_status run_mgpcg32(dn_handle *h, int project, int max_it, double tol, double bnorm, double out[4]) {
-  const long long n = h->n;
-  MgVec V;
-  V.A = SpOpT<float>{h->fa5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
-  V.x = h->fx;
-  V.r = h->fr;
-  V.z = h->fz;
-  V.p = h->fp0;
-  V.q = h->fap;
+// The V-cycle's ~11 launches per level are replayed from a CUDA graph captured on first use for this
+// (hierarchy, b0, x0): the kernels' arguments are the level buffers' pointers, which never change, and the
+// operators are rewritten in place by mg_setup.
+dn_status mg_vcycle(dn_handle *h, MgHier &H, float *b0, float *x0) {
+  for (const dn_handle::MgGraph &g : h->mg_graphs)
+    if (g.H == &H && g.b0 == b0 && g.x0 == x0) {
+      DN_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+      h->launches += g.nodes;
+      return DN_OK;
+    }
+  const long long before = h->launches;
+  DN_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  const dn_status st = mg_vcycle_launch(h, H, b0, x0);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+  const long long nodes = h->launches - before;
+  h->launches = before;
+  if (st != DN_OK || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return st != DN_OK ? st : fail(h, DN_ERR_CUDA, std::string("V-cycle capture: ") + cudaGetErrorString(ce));
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return fail(h, DN_ERR_CUDA, std::string("V-cycle graph: ") + cudaGetErrorString(ie));
+  h->mg_graphs.push_back(dn_handle::MgGraph{&H, b0, x0, exec, nodes});
+  DN_CUDA(h, cudaGraphLaunch(exec, h->stream));
+  h->launches += nodes;
+  return DN_OK;
+}
+
+// One FP32 inner solve A e = b by CG preconditioned with `vcycles` V-cycles of H applied in sequence (1 for
+// the pressure operator; 2 for the CH operator, preconditioned by (K + s I)^-2), to the relative residual tol
+// of |b| = bnorm.  V: the operator and the vectors (V.x is e, zero on entry; b is copied into V.r);
+// tmp: a level-0 buffer for the output of the first of two V-cycles.  out: [0] iterations.
+template <int S>
+dn_status run_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tmp, int vcycles, int project,
+                     int max_it, double tol, double bnorm, double out[4]) {
+  const long long n = V.A.n;
   V.part = h->mg_part;
   V.scal = h->mg_scal;
   const int nb = (int)std::min<long long>({(long long)kMgParts, 4LL * h->num_sms, (long long)blocks_for(n)});
@@ -923,10 +1043,16 @@ dn_status run_mgpcg32(dn_handle *h, int project, int max_it, double tol, double 
     k_mgp_scalars<<<1, 32, 0, h->stream>>>(h->mg_part, nb, h->mg_scal, mode, first, project, dn_);
     return check_launch(h, "k_mgp_scalars");
   };
-  cudaEventRecord(h->kev[0], h->stream);
+  auto precondition = [&]() -> dn_status {
+    if (vcycles == 2) {
+      DN_TRY(mg_vcycle(h, H, V.r, tmp));
+      return mg_vcycle(h, H, tmp, V.z);
+    }
+    return mg_vcycle(h, H, V.r, V.z);
+  };
   DN_CUDA(h, cudaMemsetAsync(h->mg_scal, 0, 16 * sizeof(double), h->stream));
-  DN_CUDA(h, cudaMemcpyAsync(h->fr, h->fb, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  DN_TRY(mg_vcycle(h));
+  DN_CUDA(h, cudaMemcpyAsync(V.r, b, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(precondition());
   k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
   DN_TRY(check_launch(h, "k_mgp_rz"));
   DN_TRY(finish(2, 1));
@@ -935,7 +1061,7 @@ dn_status run_mgpcg32(dn_handle *h, int project, int max_it, double tol, double 
   int it = 0;
   const int cap = std::max(1, max_it);
   while (it < cap) {
-    k_mgp_apply<<<nb, 256, 0, h->stream>>>(V);
+    k_mgp_apply<S><<<nb, 256, 0, h->stream>>>(V);
     DN_TRY(check_launch(h, "k_mgp_apply"));
     DN_TRY(finish(0, 0));
     k_mgp_update<<<nb, 256, 0, h->stream>>>(V);
@@ -949,28 +1075,18 @@ dn_status run_mgpcg32(dn_handle *h, int project, int max_it, double tol, double 
     if (sc[kMgBad] != 0.0) break;  // breakdown: the outer FP64 loop judges the iterate
     const double rel = std::sqrt(std::max(sc[kMgRr], 0.0)) / std::max(bnorm, 1.0e-300);
     if (!(rel >= tol)) break;  // converged (or non-finite: the outer loop stops on its own residual)
-    DN_TRY(mg_vcycle(h));
+    DN_TRY(precondition());
     k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
     DN_TRY(check_launch(h, "k_mgp_rz"));
     DN_TRY(finish(2, 0));
     k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, 0);
     DN_TRY(check_launch(h, "k_mgp_direction"));
   }
-  cudaEventRecord(h->kev[1], h->stream);
-  DN_CUDA(h, cudaEventSynchronize(h->kev[1]));
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
-  h->phase_ms[4] += ms;
   out[0] = (double)it;
   out[1] = out[2] = out[3] = 0.0;
   return DN_OK;
 }
 
-// Mixed-precision pressure solve: x = 0; repeat r = b - A x (FP64, projected when the system is singular),
-// stop on the reference's rule (rel < tol or abs < tol on the FP64 residual), else solve A e = r with the
-// FP32 PCG to the relative tolerance mixed_inner_tolerance and add e to x in FP64.  The operator and the
-// factor are the FP64 ones rounded to FP32.  out: [0] inner iterations in total, [1] abs and [2] rel FP64
-// residual, [3] 0.
 dn_status pressure_factor(dn_handle *h, bool split, bool icc);
 
 // FP32 copies of the FP64 IC/ILDLT factor for the IC inner solver (built on first use within a solve)
@@ -1003,7 +1119,12 @@ dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
   DN_TRY(check_launch(h, "k_to_float"));
   h->ic32_ready = false;
   bool use_mg = false;
-  if (h->mg_levels > 0) DN_TRY(mg_setup(h, &use_mg));
+  if (h->mgp.levels() > 0) {
+    h->mgp.lv[0].a64 = h->a5;
+    h->mgp.lv[0].a = h->fa5;
+    h->mgp.lv[0].r = h->fy;
+    DN_TRY(mg_setup(h, h->mgp, &use_mg));
+  }
   h->mixed_used_mg = use_mg;
   if (!use_mg) DN_TRY(ensure_ic32(h, split, kind));
   const SpOp A{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
@@ -1014,7 +1135,7 @@ dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
   double absr = 0.0, relr = 0.0, prev = INFINITY;
   for (;;) {
     const int nb = 128;
-    k_outer_residual<<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
+    k_outer_residual<5><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
     DN_TRY(check_launch(h, "k_outer_residual"));
     k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
     DN_TRY(check_launch(h, "k_finish3"));
@@ -1036,9 +1157,23 @@ dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
     k_inner_rhs<<<blocks_for(n), 256, 0, h->stream>>>(h->r, mean, h->fb, h->fx, n);
     DN_TRY(check_launch(h, "k_inner_rhs"));
     double o[4];
-    if (use_mg)
-      DN_TRY(run_mgpcg32(h, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, absr, o));
-    else
+    if (use_mg) {
+      MgVec V{};
+      V.A = SpOpT<float>{h->fa5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+      V.x = h->fx;
+      V.r = h->fr;
+      V.z = h->fz;
+      V.p = h->fp0;
+      V.q = h->fap;
+      cudaEventRecord(h->kev[0], h->stream);
+      DN_TRY(run_mgcg32<5>(h, h->mgp, V, h->fb, nullptr, 1, project, cfg.poisson_iterations - total,
+                           cfg.mixed_inner_tolerance, absr, o));
+      cudaEventRecord(h->kev[1], h->stream);
+      DN_CUDA(h, cudaEventSynchronize(h->kev[1]));
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+      h->phase_ms[4] += ms;
+    } else
       DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, o));
     total += (int)o[0];
     k_add_correction<<<blocks_for(n), 256, 0, h->stream>>>(h->x, h->fx, n);
@@ -1051,6 +1186,82 @@ dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
   out[1] = absr;
   out[2] = relr;
   out[3] = 0.0;
+  return DN_OK;
+}
+
+// Mixed-precision CH solve (precision = mixed, multigrid hierarchy present): the FP64 defect-correction loop
+// of mixed_pressure around FP32 inner CG solves of the 13-point operator A = alpha0 I + beta1 K + beta2 K^2
+// (K = -L, build_cahn_hilliard_operator, ch_sparse_krylov.hpp:205-233), preconditioned by two V-cycles of
+// K + s I with s = sqrt(alpha0 / beta2).  beta2 (K + s I)^2 has A's K^2 and constant terms, and on every
+// eigenvector of K (eigenvalue k >= 0) the ratio (alpha0 + beta1 k + beta2 k^2) / (beta2 (k + s)^2) lies
+// between 1/2 + beta1 / (4 beta2 s) (at k = s) and 1, so the preconditioned condition number stays below 2
+// on every grid.  Stops on the reference's rule (relative or absolute FP64 residual below ch_tolerance,
+// solve_preconditioned_cg, ch_sparse_krylov.hpp:545-560); x starts at the state (h->x).  *iter_res: the last
+// correction's size relative to the iterate, the analogue of the PCG's iterate residual.
+dn_status mixed_ch(dn_handle *h, double alpha0, dn_report *rep, double *iter_res, bool *used) {
+  const dn_config &cfg = h->cfg;
+  const long long n = h->n;
+  *used = false;
+  if (h->ch_mg_alpha0 != alpha0) {
+    const double a2 = cfg.cn > 0.0 ? (3.0 * kSqrt2 * cfg.cn / 4.0) : 0.0;
+    const double beta2 = a2 / cfg.pe;
+    if (!(beta2 > 0.0) || !(alpha0 > 0.0)) return DN_OK;
+    const double shift = std::sqrt(alpha0 / beta2);
+    k_to_float<<<blocks_for(13 * n), 256, 0, h->stream>>>(h->a13, h->fa13, 13 * n);
+    DN_TRY(check_launch(h, "k_to_float"));
+    MgHier::Lv &l0 = h->mgc.lv[0];
+    k_shifted_laplacian<<<blocks_for(n), 256, 0, h->stream>>>(h->G, shift, l0.a64_own, const_cast<float *>(l0.a));
+    DN_TRY(check_launch(h, "k_shifted_laplacian"));
+    h->mgc.mass = shift;
+    h->mgc.singular = 0;
+    bool ok = false;
+    DN_TRY(mg_setup(h, h->mgc, &ok));
+    if (!ok) return DN_OK;
+    h->ch_mg_alpha0 = alpha0;
+  }
+  *used = true;
+  const SpOp A{h->a13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  constexpr int kMaxCycles = 40;
+  int total = 0, cycles = 0;
+  double absr = 0.0, relr = 0.0, prev = INFINITY, ires = 0.0;
+  for (;;) {
+    const int nb = 128;
+    k_outer_residual<13><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
+    DN_TRY(check_launch(h, "k_outer_residual"));
+    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
+    DN_TRY(check_launch(h, "k_finish3"));
+    double sums[3];
+    DN_TRY(read_scalars(h, 3, sums));
+    absr = std::sqrt(std::max(sums[1], 0.0));
+    relr = absr / std::max(std::sqrt(std::max(sums[2], 0.0)), 1.0e-30);
+    if (relr < cfg.ch_tolerance || absr < cfg.ch_tolerance) break;
+    if (cycles >= kMaxCycles || total >= cfg.ch_inner_iterations || !(absr < prev)) break;
+    prev = absr;
+    k_inner_rhs<<<blocks_for(n), 256, 0, h->stream>>>(h->r, 0.0, h->cb32, h->cx32, n);
+    DN_TRY(check_launch(h, "k_inner_rhs"));
+    MgVec V{};
+    V.A = SpOpT<float>{h->fa13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+    V.x = h->cx32;
+    V.r = h->cr32;
+    V.z = h->cz32;
+    V.p = h->cp32;
+    V.q = h->cq32;
+    double o[4];
+    DN_TRY(run_mgcg32<13>(h, h->mgc, V, h->cb32, h->ct32, 2, 0, cfg.ch_inner_iterations - total,
+                          cfg.mixed_inner_tolerance, absr, o));
+    total += (int)o[0];
+    k_add_correction_norms<<<nb, 256, 0, h->stream>>>(h->x, h->cx32, n, h->partials);
+    DN_TRY(check_launch(h, "k_add_correction_norms"));
+    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
+    DN_TRY(check_launch(h, "k_finish3"));
+    double en[3];
+    DN_TRY(read_scalars(h, 3, en));
+    ires = std::sqrt(std::max(en[0], 0.0) / std::max(en[1], 1.0e-30));
+    ++cycles;
+  }
+  rep->ch_iterations = total;
+  rep->ch_preconditioner = 3;
+  *iter_res = ires;
   return DN_OK;
 }
 
@@ -1246,24 +1457,39 @@ dn_status ensure_ch_system(dn_handle *h, double alpha0) {
 dn_status ch_linear_solve(dn_handle *h, double alpha0, dn_report *rep, double *iter_res, double *eq_res) {
   DN_TRY(ensure_ch_system(h, alpha0));
   double out[4];
-  rep->ch_preconditioner = (h->ch_prec == kPrecLDLT) ? 1 : 0;
-  dn_status s;
-  if (h->ch_prec == kPrecLDLT)
-    s = run_pcg<13, 1>(h, h->a13, h->l13, h->dinv13, kPrecLDLT, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance, out);
-  else
-    s = run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance, out);
-  if (s == DN_ERR_PCG_BREAKDOWN) {
-    // phase_field.cpp:468-473: retry with the diagonal preconditioner from the current iterate
-    h->ch_prec = kPrecDiag;
-    k_diag_inverse<13><<<blocks_for(h->n), 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py},
-                                                              h->dinv13);
-    DN_TRY(check_launch(h, "k_diag_inverse"));
-    rep->ch_preconditioner = 2;
-    s = run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance, out);
+  bool mixed_done = false;
+  if (h->ch_mg && h->cfg.precision == DN_PRECISION_MIXED) {
+    cudaEventRecord(h->kev[0], h->stream);
+    DN_TRY(mixed_ch(h, alpha0, rep, iter_res, &mixed_done));
+    cudaEventRecord(h->kev[1], h->stream);
+    DN_CUDA(h, cudaEventSynchronize(h->kev[1]));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+    h->phase_ms[5] += ms;
   }
-  DN_TRY(s);
-  rep->ch_iterations = (int)out[0];
-  *iter_res = out[3];
+  rep->ch_preconditioner = mixed_done ? 3 : (h->ch_prec == kPrecLDLT) ? 1 : 0;
+  if (!mixed_done) {
+    dn_status s;
+    if (h->ch_prec == kPrecLDLT)
+      s = run_pcg<13, 1>(h, h->a13, h->l13, h->dinv13, kPrecLDLT, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance,
+                         out);
+    else
+      s = run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance,
+                         out);
+    if (s == DN_ERR_PCG_BREAKDOWN) {
+      // phase_field.cpp:468-473: retry with the diagonal preconditioner from the current iterate
+      h->ch_prec = kPrecDiag;
+      k_diag_inverse<13><<<blocks_for(h->n), 256, 0, h->stream>>>(
+          SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, h->dinv13);
+      DN_TRY(check_launch(h, "k_diag_inverse"));
+      rep->ch_preconditioner = 2;
+      s = run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations,
+                         h->cfg.ch_tolerance, out);
+    }
+    DN_TRY(s);
+    rep->ch_iterations = (int)out[0];
+    *iter_res = out[3];
+  }
   // equation residual ||b - A x|| / ||b||: enough CTAs to keep every SM's loads in flight
   const int nb = 1024;
   k_residual_partials<13><<<nb, 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, h->b,
@@ -2265,6 +2491,8 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     cudaFuncSetAttribute(k_pcg<13, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSeqSmemMax);
   h->ml = MomLayout{nx, ny, c.periodic_x, c.periodic_y, (long long)(nx + 1) * ny, (long long)nx * (ny + 1)};
   h->nm = h->ml.nu + h->ml.nv;
+  if (h->nm >= (1LL << 31))
+    return bad(DN_ERR_INVALID_ARGUMENT, "grid too large for the momentum system's 32-bit column indices");
   A(dalloc(h, &h->mcoef, 9 * h->nm));
   A(dalloc(h, &h->mtgt, 9 * h->nm));
   for (double **p : {&h->mb, &h->mx, &h->mr, &h->mrhat, &h->mp0, &h->mp1, &h->mv0, &h->mv1, &h->mphat, &h->ms, &h->mshat,
@@ -2346,40 +2574,31 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
       A(dalloc(h, p, h->n));
     if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
     if (c.mixed_preconditioner == DN_MIXED_PREC_MULTIGRID) {
-      // halve both extents while they are even and >= 4 and the level is larger than the direct coarse solve
-      std::vector<std::pair<int, int>> dims{{h->G.nx, h->G.ny}};
-      int lx = h->G.nx, ly = h->G.ny;
-      while ((long long)lx * ly > kMgCoarseMax && lx % 2 == 0 && ly % 2 == 0 && lx >= 4 && ly >= 4 &&
-             (int)dims.size() < kMgMaxLevels) {
-        lx /= 2;
-        ly /= 2;
-        dims.push_back({lx, ly});
-      }
-      if ((long long)lx * ly <= kMgCoarseMax) {
-        for (size_t l = 1; l < dims.size(); ++l) {
-          dn_handle::MgHost m;
-          m.nx = dims[l].first;
-          m.ny = dims[l].second;
-          const size_t nl = (size_t)m.nx * m.ny;
-          A(dalloc(h, &m.a64, 5 * nl));
-          A(dalloc(h, &m.a, 5 * nl));
-          A(dalloc(h, &m.x, nl));
-          A(dalloc(h, &m.b, nl));
-          A(dalloc(h, &m.r, nl));
-          h->mg.push_back(m);
+      A(mg_alloc(h, h->mgp, h->G.nx, h->G.ny, h->bc.p));
+      h->mgp.singular = h->has_dirichlet ? 0 : 1;
+      A(dalloc(h, &h->mg_scal, 16));
+      A(dalloc(h, &h->mg_part, 3 * (size_t)kMgParts));
+      // the CH solve: FP32 13-point operator, CG vectors and the (K + s I) hierarchy, when the operator has
+      // its biharmonic part (cn > 0) and the grid coarsens
+      const BCSide reflect[4] = {{DN_BC_NEUMANN, 0.0}, {DN_BC_NEUMANN, 0.0}, {DN_BC_NEUMANN, 0.0},
+                                 {DN_BC_NEUMANN, 0.0}};
+      if (c.cn > 0.0 && solve_ch(c)) {
+        A(mg_alloc(h, h->mgc, h->G.nx, h->G.ny, reflect));
+        if (h->mgc.levels() > 0) {
+          double *a64 = nullptr;
+          float *a32 = nullptr;
+          A(dalloc(h, &a64, 5 * h->n));
+          A(dalloc(h, &a32, 5 * h->n));
+          A(dalloc(h, &h->mgc.lv[0].r, h->n));
+          h->mgc.lv[0].a64 = h->mgc.lv[0].a64_own = a64;
+          h->mgc.lv[0].a = a32;
+          A(dalloc(h, &h->fa13, 13 * h->n));
+          for (float **q : {&h->cx32, &h->cr32, &h->cz32, &h->cp32, &h->cq32, &h->ct32, &h->cb32})
+            A(dalloc(h, q, h->n));
+          h->ch_mg = true;
         }
-        A(dalloc(h, &h->mg_inv, (size_t)kMgCoarseMax * kMgCoarseMax));
-        A(dalloc(h, &h->mg_scal, 16));
-        A(dalloc(h, &h->mg_part, 3 * (size_t)kMgParts));
-        A(dalloc(h, &h->mg_flag, 1));
-        if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
-        h->mg_levels = (int)dims.size();
-        for (int k = 0; k < 4; ++k) h->mg_fold.s[k] = h->bc.p[k].type == DN_BC_DIRICHLET ? -1.0f : 1.0f;
-        h->mg_fold.px = h->G.px;
-        h->mg_fold.py = h->G.py;
-        cudaFuncSetAttribute(k_mg_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(double) * kMgCoarseMax * kMgCoarseMax));
       }
+      if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
     }
     const int optin = h->smem_optin;
     auto round16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
@@ -2427,6 +2646,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
 dn_status dn_destroy(dn_handle *h) {
   if (!h) return DN_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  for (const dn_handle::MgGraph &g : h->mg_graphs) cudaGraphExecDestroy(g.exec);
   for (void *p : h->allocations) cudaFree(p);
   if (h->mon) cudaFree(h->mon);
   if (h->host_scal) cudaFreeHost(h->host_scal);

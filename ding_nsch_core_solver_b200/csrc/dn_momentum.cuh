@@ -47,7 +47,7 @@ struct MomRowBuilder {
 
 // Assembles coefficients, targets, rhs and x0 for every unknown (inactive unknowns: all zero, target -1).
 __global__ void k_mom_assemble(MomLayout L, Grid G, BCSet bc, Fv u, Fv v, Fv rm, Fv eta, Fv urhs, Fv vrhs,
-                               double alpha, double *coef, long long *tgt, double *rhs, double *x0) {
+                               double alpha, double *coef, int *tgt, double *rhs, double *x0) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long N = L.n();
   if (t >= N) return;
@@ -208,7 +208,7 @@ __global__ void k_mom_assemble(MomLayout L, Grid G, BCSet bc, Fv u, Fv v, Fv rm,
     // finalize_row_maps drops |a| < 1e-18 (ch_sparse_krylov.hpp:116)
     const bool keep = R.tgt[k] >= 0 && fabs(R.c[k]) >= 1.0e-18;
     coef[(size_t)k * N + t] = keep ? R.c[k] : 0.0;
-    tgt[(size_t)k * N + t] = keep ? R.tgt[k] : -1;
+    tgt[(size_t)k * N + t] = keep ? (int)R.tgt[k] : -1;  // nu + nv < 2^31 (checked at creation)
   }
   rhs[t] = R.rhs;
 }
@@ -315,7 +315,7 @@ __global__ void k_mom_scatter(MomLayout L, const double *x, Fv us, Fv vs) {
 struct BicgArgs {
   long long n;
   const double *coef;   // [9][n]
-  const long long *tgt; // [9][n]
+  const int *tgt;       // [9][n], -1 = no entry
   const double *b;
   double *x, *r, *rhat, *p0, *p1, *v0, *v1, *phat, *s, *shat, *t, *upd, *dinv;
   int max_it;
@@ -331,7 +331,7 @@ __device__ __forceinline__ double mom_row_apply(const BicgArgs &P, long long r, 
   double sum = 0.0;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    const long long c = P.tgt[(size_t)k * P.n + r];
+    const int c = P.tgt[(size_t)k * P.n + r];
     if (c >= 0) sum += P.coef[(size_t)k * P.n + r] * x[c];
   }
   return sum;
@@ -340,7 +340,7 @@ __device__ __forceinline__ double mom_row_apply(const BicgArgs &P, long long r, 
 __global__ void k_mom_dinv(BicgArgs P) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= P.n) return;
-  const long long c0 = P.tgt[r];
+  const int c0 = P.tgt[r];
   P.dinv[r] = (c0 >= 0) ? 1.0 / max_ref(fabs(P.coef[r]), 1.0e-30) : 0.0;
 }
 
@@ -389,21 +389,22 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
       return;
     }
     const double beta = (it == 0) ? 0.0 : (rho_new / rho_old) * (alpha / omega);
-    // p = r + beta (p - omega v); phat = D^-1 p; v = A phat (phat at neighbours formed on the fly)
+    // p = r + beta (p - omega v); phat = D^-1 p (stored, then gathered: one load per neighbour)
+    for (long long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+      const double pq = P.r[q] + beta * (p_old[q] - omega * v_old[q]);
+      p_new[q] = pq;
+      P.phat[q] = P.dinv[q] * pq;
+    }
+    if (!bar.sync()) return;
+    // v = A phat
     double a1[1] = {0.0};
     for (long long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
       double sum = 0.0;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const long long c = P.tgt[(size_t)k * n + q];
-        if (c >= 0) {
-          const double pc = P.r[c] + beta * (p_old[c] - omega * v_old[c]);
-          sum += P.coef[(size_t)k * n + q] * (P.dinv[c] * pc);
-        }
+        const int c = P.tgt[(size_t)k * n + q];
+        if (c >= 0) sum += P.coef[(size_t)k * n + q] * P.phat[c];
       }
-      const double pq = P.r[q] + beta * (p_old[q] - omega * v_old[q]);
-      p_new[q] = pq;
-      P.phat[q] = P.dinv[q] * pq;
       v_new[q] = sum;
       a1[0] += P.rhat[q] * sum;
     }
@@ -418,6 +419,7 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
     for (long long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
       const double sv = P.r[q] - alpha * v_new[q];
       P.s[q] = sv;
+      P.shat[q] = P.dinv[q] * sv;  // gathered by t = A shat after the barrier of the reduction below
       P.upd[q] = alpha * P.phat[q];
       a2[0] += sv * sv;
     }
@@ -441,10 +443,9 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab(BicgArgs P) {
       double sum = 0.0;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const long long c = P.tgt[(size_t)k * n + q];
-        if (c >= 0) sum += P.coef[(size_t)k * n + q] * (P.dinv[c] * P.s[c]);
+        const int c = P.tgt[(size_t)k * n + q];
+        if (c >= 0) sum += P.coef[(size_t)k * n + q] * P.shat[c];
       }
-      P.shat[q] = P.dinv[q] * P.s[q];
       P.t[q] = sum;
       a4[0] += sum * sum;
       a4[1] += sum * P.s[q];

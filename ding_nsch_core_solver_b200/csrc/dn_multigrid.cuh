@@ -179,7 +179,11 @@ __global__ void k_mg_prolong(MgLevel C, MgLevel F, MgFold fold) {
 }
 
 // Coarse operator of level l+1 from the FP64 slots of level l (see the file header), in FP64 with an FP32 copy.
-__global__ void k_mg_coarsen(const double *af, int nxf, int nyf, double *ac, float *acf, int nxc, int nyc) {
+// mass: a uniform diagonal term of level l's operator (the shift of a shifted Laplacian K + m I), kept apart
+// from the boundary excess: under R = P^T it aggregates over the four children (4 m on level l+1), while the
+// boundary excess, like the face weights, is rediscretised (half the children's sum).
+__global__ void k_mg_coarsen(const double *af, int nxf, int nyf, double mass, double *ac, float *acf, int nxc,
+                             int nyc) {
   const unsigned nc = (unsigned)nxc * (unsigned)nyc;
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nc) return;
@@ -191,7 +195,7 @@ __global__ void k_mg_coarsen(const double *af, int nxf, int nyf, double *ac, flo
     for (int b = 0; b < 2; ++b) {
       const int i = 2 * I + a, j = 2 * J + b;
       const double d = at(2, i, j);
-      double e = d + at(0, i, j) + at(1, i, j) + at(3, i, j) + at(4, i, j);
+      double e = d + at(0, i, j) + at(1, i, j) + at(3, i, j) + at(4, i, j) - mass;
       if (fabs(e) <= 1.0e-12 * fabs(d)) e = 0.0;  // interior and Neumann rows: round-off of an exact zero
       exc += e;
     }
@@ -199,11 +203,29 @@ __global__ void k_mg_coarsen(const double *af, int nxf, int nyf, double *ac, flo
   const double s = 0.5 * (at(1, 2 * I, 2 * J) + at(1, 2 * I + 1, 2 * J));
   const double nn = 0.5 * (at(3, 2 * I, 2 * J + 1) + at(3, 2 * I + 1, 2 * J + 1));
   const double e = 0.5 * (at(4, 2 * I + 1, 2 * J) + at(4, 2 * I + 1, 2 * J + 1));
-  const double c = -(w + s + nn + e) + 0.5 * exc;
+  const double c = -(w + s + nn + e) + 0.5 * exc + 4.0 * mass;
   const double v[5] = {w, s, c, nn, e};
   for (int k = 0; k < 5; ++k) {
     ac[(size_t)k * nc + t] = v[k];
     acf[(size_t)k * nc + t] = (float)v[k];
+  }
+}
+
+// Level 0 of the CH preconditioner's hierarchy: K + m I with K = -L, L the 5-point Laplacian with reflecting
+// rows at walls (build_laplacian_matrix, ch_sparse_krylov.hpp:135-177: a row counts only the neighbours that
+// exist), in the W,S,C,N,E slots.
+__global__ void k_shifted_laplacian(Grid G, double m, double *a, float *af) {
+  const long long n = (long long)G.nx * G.ny;
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int i = (int)(r / G.ny), j = (int)(r % G.ny);
+  const double cx = 1.0 / (G.dx * G.dx), cy = 1.0 / (G.dy * G.dy);
+  const double w = (G.px || i > 0) ? cx : 0.0, e = (G.px || i < G.nx - 1) ? cx : 0.0;
+  const double s = (G.py || j > 0) ? cy : 0.0, nn = (G.py || j < G.ny - 1) ? cy : 0.0;
+  const double v[5] = {-w, -s, w + e + s + nn + m, -nn, -e};
+  for (int k = 0; k < 5; ++k) {
+    a[(size_t)k * n + r] = v[k];
+    af[(size_t)k * n + r] = (float)v[k];
   }
 }
 
@@ -280,14 +302,15 @@ struct MgVec {
   double *scal;
 };
 
-// q = A p, partial sums of p.q
+// q = A p (the 5-point pressure or the 13-point CH operator), partial sums of p.q
+template <int S>
 __global__ void k_mgp_apply(MgVec V) {
   __shared__ double sh[32];
   double v[1] = {0.0};
   const unsigned n = (unsigned)V.A.n, ny = (unsigned)V.A.ny;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int i = (int)(t / ny), j = (int)(t - (unsigned)i * ny);
-    const float s = spmv_row<5>(V.A, V.p, i, j);
+    const float s = spmv_row<S>(V.A, V.p, i, j);
     V.q[t] = s;
     v[0] += (double)V.p[t] * (double)s;
   }

@@ -93,7 +93,10 @@ typedef struct {
                                       under a few seconds) */
   int mixed_preconditioner;        /* dn_mixed_preconditioner: preconditioner of the FP32 inner CG of the mixed
                                       form (0: geometric multigrid V-cycle where the grid coarsens to <= 128
-                                      cells, else the scheme's own IC(0)/ILDLT(0); 1: always IC/ILDLT) */
+                                      cells, else the scheme's own IC(0)/ILDLT(0); 1: always IC/ILDLT).  With 0
+                                      the CH solve also runs the mixed form (FP32 CG, two V-cycles of the
+                                      shifted Laplacian K + sqrt(alpha0/beta2) I as preconditioner); with 1 it
+                                      stays FP64 ILDLT-PCG */
   /* pressure analysis (config.hpp:36-133; run_pressure_analysis_from_snapshot, pressure_analysis.cpp:156-328) */
   int analysis_enabled;            /* analysis_enabled */
   int analysis_mode;               /* dn_analysis_mode, from the analysis_mode string */
@@ -121,7 +124,8 @@ typedef enum {
 /* What one step (or one backend call) reports: Solver::last_* members (solver.hpp:93-108). */
 typedef struct {
   int ch_iterations, momentum_iterations, pressure_iterations, coupling_iterations;
-  int ch_preconditioner; /* 0 diagonal, 1 ILDLT, 2 diagonal fallback after a breakdown, -1 not used */
+  int ch_preconditioner; /* 0 diagonal, 1 ILDLT, 2 diagonal fallback after a breakdown, -1 not used,
+                            3 mixed form: FP32 CG preconditioned by (K + s I)^-2 V-cycles */
   double ch_residual, ch_equation_residual, momentum_residual, pressure_residual;
   double boundary_speed_pre, boundary_speed_post;
   int refinement_cycles; /* mixed form: outer FP64 defect-correction cycles of the pressure solve */

@@ -8,7 +8,11 @@ field, the values at 8192 seeded cells together with the field's full L2 norm, p
 counts.  The GPU test regenerates the same initial state, takes the same step and compares the sampled
 cells (relative L2 over the sample) and the norms.
 
-    python tests/golden/make_fullsize.py [--impl reference|port] [--grid 1024x2048]
+With --tight the same step is taken at ch/pressure tolerance 1e-13 and momentum tolerance 1e-14 (iteration
+caps lifted) and written as bubble_<grid>_step0_tight.npz: the step solved well below the reference's own
+solver error, which the mixed-precision form is compared against beside the reference's answer.
+
+    python tests/golden/make_fullsize.py [--impl reference|port] [--grid 1024x2048] [--tight]
 """
 import argparse
 import os
@@ -39,11 +43,16 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--impl", default="reference" if available("reference") else "port")
     ap.add_argument("--grid", default="1024x2048")
+    ap.add_argument("--tight", action="store_true")
     args = ap.parse_args()
     grid = tuple(int(v) for v in args.grid.split("x"))
     cfg = bench.workload_cfg(grid)
     state = bench.initial_state(cfg)
-    orc = OracleSolver(with_defaults(cfg), args.impl)
+    run_cfg = dict(cfg)
+    if args.tight:
+        run_cfg.update(ch_tolerance=1e-13, pressure_tolerance=1e-13, momentum_tolerance=1e-14,
+                       ch_inner_iterations=100000, poisson_iterations=100000, momentum_iterations=10000)
+    orc = OracleSolver(with_defaults(run_cfg), args.impl)
     orc.initialize()
     for n, a in state.items():
         orc.set_field(n, a)
@@ -64,7 +73,7 @@ def main():
         out[name + "_j"] = jj.astype(np.int32)
         out[name + "_val"] = a[ii, jj].copy()
         out[name + "_norm"] = np.array(np.linalg.norm(a[g:a.shape[0] - g, g:a.shape[1] - g]))
-    path = os.path.join(HERE, f"bubble_{grid[0]}x{grid[1]}_step0.npz")
+    path = os.path.join(HERE, f"bubble_{grid[0]}x{grid[1]}_step0{'_tight' if args.tight else ''}.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {args.impl}, {sec:.1f} s, iterations ch {rep['ch_iterations']} "
           f"mom {rep['momentum_iterations']} p {rep['pressure_iterations']}")

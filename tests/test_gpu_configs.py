@@ -212,31 +212,18 @@ def test_rayleigh_taylor_reduced_plain(dn):
         assert rep["ch_iterations"] == ro["ch_iterations"], (k, rep, ro)
 
 
-def _tight_p(orc, cfg, step):
-    """p after `step` from orc's current state, solved at pressure tolerance 1e-13 (the oracle)."""
-    tight = OracleSolver(dict(cfg, pressure_tolerance=1e-13, poisson_iterations=100000), "port")
-    tight.initialize()
-    for name in FIELDS:
-        tight.set_field(name, orc.field(name))
-    tight.set_initial_mass(0.0)
-    tight.step(step)
-    return tight.field("p").copy()  # a copy: the view dies with `tight`
-
-
 def test_rayleigh_taylor_reduced_mixed(dn):
+    from test_gpu_mixed import assert_within_reference_error, tight_step
+
     cfg = rayleigh_taylor()
     orc, gpu = start_pair(dn, cfg, phase=rt_interface(cfg), gpu_cfg=dict(cfg, precision="mixed"))
-    g = cfg["ghost"]
     for k in range(3):
         for name in FIELDS:  # the same inputs for this step (see test_gpu_mixed.py)
             gpu.set_field(name, orc.field(name))
-        p_tight = _tight_p(orc, cfg, k)
+        tight = tight_step(orc, cfg, k)
         orc.step(k)
         rep = gpu.step(k)
-        assert_fields_close(orc, gpu, ("c", "mu", "u", "v"), f"RT mixed step {k}", tol=TOL_MIXED)
-        ref_err = rel_l2(interior(orc.field("p"), g), interior(p_tight, g))
-        err = rel_l2(interior(gpu.get_field("p"), g), interior(orc.field("p"), g))
-        assert err <= max(TOL_MIXED, 3.0 * ref_err), (k, err, ref_err)
+        assert_within_reference_error(orc, gpu, tight, f"RT mixed step {k}")
         assert rep["pressure_residual"] < cfg["pressure_tolerance"]
 
 
@@ -252,8 +239,8 @@ def test_shear_droplet_parity(dn):
 
 
 # ---- the 1024x2048 bubble against the reference's sampled step ---------------------------------------
-def _fullsize_fixture():
-    path = os.path.join(GOLDEN, "bubble_1024x2048_step0.npz")
+def _fullsize_fixture(suffix=""):
+    path = os.path.join(GOLDEN, f"bubble_1024x2048_step0{suffix}.npz")
     if not os.path.exists(path):
         pytest.fail(f"missing fixture {path}: run tests/golden/make_fullsize.py")
     return np.load(path)
@@ -273,17 +260,25 @@ def test_bubble_1024x2048_one_step_vs_reference(dn, precision):
     rep = gpu.step(0)
     g = cfg["ghost"]
     tol = TOL if precision == "fp64" else TOL_MIXED
-    errs = {}
+    # the mixed form is held, per field, to max(1e-8, 3 x the reference's own distance to the same step
+    # solved at tolerance 1e-13 (bubble_1024x2048_step0_tight.npz, same sampled cells)), as on small grids
+    tight = _fullsize_fixture("_tight") if precision == "mixed" else None
+    errs, bars = {}, {}
     for name in COMPARE:
         a = gpu.get_field(name)
         got = a[fx[name + "_i"], fx[name + "_j"]]
         errs[name] = rel_l2(got, fx[name + "_val"])
+        bars[name] = tol
+        if tight is not None:
+            bars[name] = max(tol, 3.0 * rel_l2(fx[name + "_val"], tight[name + "_val"]))
+            print(name, f"vs reference {errs[name]:.2e}, vs tight {rel_l2(got, tight[name + '_val']):.2e}, "
+                        f"reference vs tight {rel_l2(fx[name + '_val'], tight[name + '_val']):.2e}")
         norm = np.linalg.norm(a[g:a.shape[0] - g, g:a.shape[1] - g])
-        assert abs(norm - float(fx[name + "_norm"])) <= tol * float(fx[name + "_norm"]), (name, norm)
+        assert abs(norm - float(fx[name + "_norm"])) <= bars[name] * float(fx[name + "_norm"]), (name, norm)
     print(precision, {k: f"{v:.2e}" for k, v in errs.items()}, rep)
-    assert all(v <= tol for v in errs.values()), errs
-    assert rep["ch_iterations"] == int(fx["ch_iterations"])
+    assert all(errs[k] <= bars[k] for k in errs), (errs, bars)
     if precision == "fp64":
+        assert rep["ch_iterations"] == int(fx["ch_iterations"])
         # 2548 iterations stop where the relative residual crosses 1e-10: sums that round differently move
         # that crossing by a few iterations (the fields above still agree to 1e-10)
         assert abs(rep["pressure_iterations"] - int(fx["pressure_iterations"])) <= 3
