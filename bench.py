@@ -265,7 +265,9 @@ def run_ours(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
+            torch.cuda.nvtx.range_push("plain_step")  # ncu --nvtx-include plain_step/ selects a timed step
             rep = solver.step(step)
+            torch.cuda.nvtx.range_pop()
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
@@ -321,7 +323,9 @@ def run_ours(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(mstream)
+            torch.cuda.nvtx.range_push("mixed_step")
             mreps.append(msolver.step(mstep))
+            torch.cuda.nvtx.range_pop()
             e1.record(mstream)
             e1.synchronize()
             mtimes.append(e0.elapsed_time(e1))

@@ -409,6 +409,7 @@ struct dn_handle {
   int device = 0;
   int num_sms = 148;
   int cta_cap = 148;  // CTAs one persistent launch may take: num_sms / device_share
+  int bicg_occ = 1;   // co-resident CTAs per SM of k_bicgstab alone
   cudaStream_t stream = nullptr;
   Grid G;
   BCSet bc;
@@ -1295,8 +1296,9 @@ dn_status run_bicgstab(dn_handle *h, double out[4]) {
   k_mom_dinv<<<blocks_for(h->nm), 256, 0, h->stream>>>(P);
   DN_TRY(check_launch(h, "k_mom_dinv"));
   DN_TRY(reset_sync(h));
-  int blocks = (int)std::min<long long>(h->cta_cap, std::max<long long>(1, (h->nm + 2047) / 2048));
-  blocks = std::max(1, std::min(blocks, h->max_coop_blocks));
+  // every co-resident CTA of this kernel (its gathers are latency-bound), at least 1024 unknowns per CTA
+  int blocks = (int)std::min<long long>((long long)h->bicg_occ * h->cta_cap, std::max<long long>(1, h->nm / 1024));
+  blocks = std::max(1, std::min(blocks, kMaxBlocks));
   void *args[] = {&P};
   cudaEventRecord(h->kev[0], h->stream);
   DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(blocks), dim3(kBlock), args, 0, h->stream));
@@ -2631,6 +2633,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg<13, 1>, kBlock, 0);
   int occ3 = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_bicgstab, kBlock, 0);
+  h->bicg_occ = std::max(1, occ3);
   occ = std::min(occ, std::min(occ2, occ3));
   if (c.precision == DN_PRECISION_MIXED) {
     int occ4 = 0;
