@@ -33,6 +33,8 @@ namespace dn {
 constexpr int kMgCoarseMax = 128;  // cells of the directly inverted coarsest level (128^2 doubles of shared memory)
 constexpr int kMgMaxLevels = 24;
 constexpr int kMgParts = 1024;     // CTAs of the CG vector kernels at most (per-CTA partial sums)
+constexpr int kMgSweeps = 2;       // red-black sweeps before and after each coarse correction
+constexpr int kMgBottomCells = 8192;  // levels this small run inside the one-CTA bottom kernel
 
 // one level of the hierarchy: operator slots [5][n] (W,S,C,N,E), iterate, right-hand side, residual
 struct MgLevel {
@@ -62,13 +64,11 @@ __device__ __forceinline__ float mg_row_sum(const MgLevel &L, const float *x, in
   return s;
 }
 
-// Red-black Gauss-Seidel half sweep over the cells of one colour ((i + j) & 1 == color); ny is even on every
+// Red-black Gauss-Seidel half sweep at cell t of the colour's cells ((i + j) & 1 == color); ny is even on every
 // smoothed level, so each row holds ny/2 cells of each colour.  first: the iterate is zero on entry, so the
 // colour's cells take b / diag and the other colour's cells are set to zero.
-__global__ void k_mg_smooth(MgLevel L, int color, int first, int px, int py) {
+__device__ __forceinline__ void mg_smooth_at(const MgLevel &L, int color, int first, int px, int py, unsigned t) {
   const int half = L.ny >> 1;
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (unsigned)L.nx * (unsigned)half) return;
   const int i = (int)(t / (unsigned)half);
   const int j = 2 * (int)(t - (unsigned)i * (unsigned)half) + ((i + color) & 1);
   const long long n = (long long)L.nx * L.ny;
@@ -79,11 +79,9 @@ __global__ void k_mg_smooth(MgLevel L, int color, int first, int px, int py) {
   if (first) L.x[(long long)i * L.ny + (j ^ 1)] = 0.0f;
 }
 
-// r = b - A x on one level
-__global__ void k_mg_residual(MgLevel L, int px, int py) {
+// r = b - A x at cell t
+__device__ __forceinline__ void mg_residual_at(const MgLevel &L, int px, int py, unsigned t) {
   const unsigned n = (unsigned)L.nx * (unsigned)L.ny;
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
   const int i = (int)(t / (unsigned)L.ny), j = (int)(t - (unsigned)i * (unsigned)L.ny);
   L.r[t] = L.b[t] - (L.a[2 * (size_t)n + t] * L.x[t] + mg_row_sum(L, L.x, i, j, t, n, px, py));
 }
@@ -104,11 +102,8 @@ __device__ __forceinline__ float mg_w1(int i, int I, int nc, int per, float s_lo
   return w;
 }
 
-// coarse b = P^T (fine r): each coarse cell gathers the 4 x 4 fine cells whose interpolation it enters
-__global__ void k_mg_restrict(MgLevel F, MgLevel C, MgFold fold) {
-  const unsigned nc = (unsigned)C.nx * (unsigned)C.ny;
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nc) return;
+// coarse b = P^T (fine r) at coarse cell t: the 4 x 4 fine cells whose interpolation it enters
+__device__ __forceinline__ void mg_restrict_at(const MgLevel &F, const MgLevel &C, const MgFold &fold, unsigned t) {
   const int I = (int)(t / (unsigned)C.ny), J = (int)(t - (unsigned)I * (unsigned)C.ny);
   float sum = 0.0f;
 #pragma unroll
@@ -136,11 +131,8 @@ __global__ void k_mg_restrict(MgLevel F, MgLevel C, MgFold fold) {
   C.b[t] = sum;
 }
 
-// fine x += P (coarse x): each fine cell reads its parent and the parents' neighbours toward it
-__global__ void k_mg_prolong(MgLevel C, MgLevel F, MgFold fold) {
-  const unsigned nf = (unsigned)F.nx * (unsigned)F.ny;
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nf) return;
+// fine x += P (coarse x) at fine cell t: its parent and the parents' neighbours toward it
+__device__ __forceinline__ void mg_prolong_at(const MgLevel &C, const MgLevel &F, const MgFold &fold, unsigned t) {
   const int i = (int)(t / (unsigned)F.ny), j = (int)(t - (unsigned)i * (unsigned)F.ny);
   int I[2], J[2];
   float wx[2], wy[2];
@@ -176,6 +168,75 @@ __global__ void k_mg_prolong(MgLevel C, MgLevel F, MgFold fold) {
 #pragma unroll
     for (int b = 0; b < 2; ++b) v += wx[a] * wy[b] * C.x[(long long)I[a] * C.ny + J[b]];
   F.x[t] += v;
+}
+
+// one launch per phase on the levels above kMgBottomCells cells
+__global__ void k_mg_smooth(MgLevel L, int color, int first, int px, int py) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (unsigned)L.nx * (unsigned)(L.ny >> 1)) mg_smooth_at(L, color, first, px, py, t);
+}
+__global__ void k_mg_residual(MgLevel L, int px, int py) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (unsigned)L.nx * (unsigned)L.ny) mg_residual_at(L, px, py, t);
+}
+__global__ void k_mg_restrict(MgLevel F, MgLevel C, MgFold fold) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (unsigned)C.nx * (unsigned)C.ny) mg_restrict_at(F, C, fold, t);
+}
+__global__ void k_mg_prolong(MgLevel C, MgLevel F, MgFold fold) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (unsigned)F.nx * (unsigned)F.ny) mg_prolong_at(C, F, fold, t);
+}
+
+// The bottom of the V-cycle in one CTA: levels first .. last-1 (each at most kMgBottomCells cells) smoothed,
+// restricted, the coarsest (last) solved with its inverse, then prolonged and smoothed back up to `first`.
+// Phases are separated by __syncthreads instead of kernel boundaries; every cell sees the same operations
+// in the same order as with the per-phase kernels, so the result is the same.
+struct MgChain {
+  MgLevel lv[kMgMaxLevels];
+  int first, last;
+  MgFold fold;
+  const float *inv;
+};
+__global__ void __launch_bounds__(1024) k_mg_bottom(MgChain Ch) {
+  const unsigned tid = threadIdx.x, nt = blockDim.x;
+  const int px = Ch.fold.px, py = Ch.fold.py;
+  for (int l = Ch.first; l < Ch.last; ++l) {
+    const MgLevel &F = Ch.lv[l], &C = Ch.lv[l + 1];
+    const unsigned nf = (unsigned)F.nx * (unsigned)F.ny, nh = nf >> 1, nc = (unsigned)C.nx * (unsigned)C.ny;
+    for (int k = 0; k < kMgSweeps; ++k) {
+      for (unsigned t = tid; t < nh; t += nt) mg_smooth_at(F, 0, k == 0, px, py, t);
+      __syncthreads();
+      for (unsigned t = tid; t < nh; t += nt) mg_smooth_at(F, 1, 0, px, py, t);
+      __syncthreads();
+    }
+    for (unsigned t = tid; t < nf; t += nt) mg_residual_at(F, px, py, t);
+    __syncthreads();
+    for (unsigned t = tid; t < nc; t += nt) mg_restrict_at(F, C, Ch.fold, t);
+    __syncthreads();
+  }
+  {
+    const MgLevel &L = Ch.lv[Ch.last];
+    const int n = L.nx * L.ny;
+    for (int i = (int)tid; i < n; i += (int)nt) {  // inv is symmetric: thread i reads column i (coalesced)
+      float s = 0.0f;
+      for (int k = 0; k < n; ++k) s += Ch.inv[(size_t)k * n + i] * L.b[k];
+      L.x[i] = s;
+    }
+    __syncthreads();
+  }
+  for (int l = Ch.last - 1; l >= Ch.first; --l) {
+    const MgLevel &F = Ch.lv[l], &C = Ch.lv[l + 1];
+    const unsigned nf = (unsigned)F.nx * (unsigned)F.ny, nh = nf >> 1;
+    for (unsigned t = tid; t < nf; t += nt) mg_prolong_at(C, F, Ch.fold, t);
+    __syncthreads();
+    for (int k = 0; k < kMgSweeps; ++k) {
+      for (unsigned t = tid; t < nh; t += nt) mg_smooth_at(F, 1, 0, px, py, t);
+      __syncthreads();
+      for (unsigned t = tid; t < nh; t += nt) mg_smooth_at(F, 0, 0, px, py, t);
+      __syncthreads();
+    }
+  }
 }
 
 // Coarse operator of level l+1 from the FP64 slots of level l (see the file header), in FP64 with an FP32 copy.
@@ -278,15 +339,6 @@ __global__ void k_mg_coarse_inverse(const double *a, int nx, int ny, int px, int
     __syncthreads();
   }
   for (int e = tid; e < n * n; e += nt) inv[e] = (float)M[e];
-}
-
-// coarsest solve x = inv b: one thread per row; inv is symmetric, so thread i reads column i (coalesced)
-__global__ void k_mg_coarse_solve(const float *inv, MgLevel L) {
-  const int n = L.nx * L.ny, i = threadIdx.x;
-  if (i >= n) return;
-  float s = 0.0f;
-  for (int k = 0; k < n; ++k) s += inv[(size_t)k * n + i] * L.b[k];
-  L.x[i] = s;
 }
 
 // ---------------------------------------------------------------------------------------------------
