@@ -11,6 +11,11 @@ the forward call is kept and put back before the backward runs.  The reference h
 its backward (dn_advection_adjoint) differentiates the WENO5 nonlinear weights.  The upwind side follows the
 sign of each face velocity, so the term is not differentiable where a face velocity is exactly 0.
 
+`momentum_predictor(solver, step, u, v, hu_prev, hv_prev, fxu, fyv)` is the momentum predictor at fixed
+materials (dn_momentum_map); its backward (dn_momentum_adjoint) solves the transposed coupled viscous system
+with the same BiCGSTAB and transposes the centred convection (linearised at u, v) and the explicit viscous
+term.  `velocity_step` composes it with the projection.
+
 `ch_solve(solver, alpha0, rhs)` is the CH implicit solve (dn_ch_linear_solve); its operator is symmetric, so
 its backward is the same solve.  `explicit_operator(solver, c, u, v)` is the CH explicit operator, and
 `ch_phase` composes the two into the CH phase of a step, and `ch_rollout` chains phases over a horizon with
@@ -90,6 +95,56 @@ def projection_adjoint(solver, step, gu, gv, gp, gpp):
     outs = [torch.empty_like(b) for b in cot]
     rep = _call(solver, solver._lib.dn_projection_adjoint, step, cot, outs)
     return tuple(_interior(solver, b) for b in outs), rep
+
+
+class MomentumPredictor(torch.autograd.Function):
+    """(u, v, hu_prev, hv_prev, fxu, fyv) -> (u_star, v_star) through dn_momentum_map, with the solver's rho_mid,
+    eta and eta_prev held fixed (kept at the forward call, put back before the backward); backward is
+    dn_momentum_adjoint, whose transposed coupled solve is the same Jacobi-BiCGSTAB on M^T."""
+
+    @staticmethod
+    def forward(ctx, solver, step, u, v, hu_prev, hv_prev, fxu, fyv):
+        kinds = ("u", "v", "u", "v", "u", "v")
+        ins = [_full(solver, t.to(torch.float64).contiguous(), k)
+               for t, k in zip((u, v, hu_prev, hv_prev, fxu, fyv), kinds)]
+        outs = [torch.empty_like(ins[0]), torch.empty_like(ins[1])]
+        its, res = _call(solver, solver._lib.dn_momentum_map, step, ins, outs)
+        ctx.solver, ctx.step = solver, int(step)
+        ctx.materials = {n: solver.get_field(n) for n in ("rho_mid", "eta", "eta_prev")}
+        ctx.save_for_backward(ins[0], ins[1])
+        ctx.forward_report = (its, res)
+        return tuple(_interior(solver, b) for b in outs)
+
+    @staticmethod
+    def backward(ctx, gus, gvs):
+        solver = ctx.solver
+        for n, a in ctx.materials.items():
+            solver.set_field(n, a)
+        u_full, v_full = ctx.saved_tensors
+        shapes = {"u": (solver.nx + 1, solver.ny), "v": (solver.nx, solver.ny + 1)}
+        cot = []
+        for g_, kind in ((gus, "u"), (gvs, "v")):
+            if g_ is None:
+                g_ = torch.zeros(shapes[kind], dtype=torch.float64, device="cuda")
+            cot.append(_full(solver, g_.to(torch.float64).contiguous(), kind))
+        outs = [torch.empty_like(u_full), torch.empty_like(v_full), torch.empty_like(u_full),
+                torch.empty_like(v_full), torch.empty_like(u_full), torch.empty_like(v_full)]
+        _call(solver, solver._lib.dn_momentum_adjoint, ctx.step, [u_full, v_full] + cot, outs)
+        return (None, None) + tuple(_interior(solver, b) for b in outs)
+
+
+def momentum_predictor(solver, step, u, v, hu_prev, hv_prev, fxu, fyv):
+    """(u_star, v_star) of the momentum predictor; differentiable in u, v, H_prev and the face surface forces
+    (rho_mid, eta, eta_prev fixed).  Surface-tension parameters enter through fxu, fyv, which are linear in
+    the surface_tension_multiplier sigma: pass sigma * f_hat to get d/d sigma."""
+    return MomentumPredictor.apply(solver, step, u, v, hu_prev, hv_prev, fxu, fyv)
+
+
+def velocity_step(solver, step, u, v, hu_prev, hv_prev, fxu, fyv, p, p_prev):
+    """The velocity half of a step at fixed phase: the momentum predictor, then the projection.  Returns
+    (u, v, p_new, p_prev_new); differentiable in all inputs (rho_mid, eta, eta_prev fixed)."""
+    us, vs = momentum_predictor(solver, step, u, v, hu_prev, hv_prev, fxu, fyv)
+    return projection(solver, step, us, vs, p, p_prev)
 
 
 class Advection(torch.autograd.Function):

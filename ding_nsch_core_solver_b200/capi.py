@@ -120,6 +120,8 @@ def load():
         "dn_pressure_solve": (I, [H, I, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int), DP]),
         "dn_projection": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
+        "dn_momentum_map": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
+        "dn_momentum_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_advection": (I, [H, VP, VP, VP, VP]),
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_set_pressure_monitor": (I, [H, I]),

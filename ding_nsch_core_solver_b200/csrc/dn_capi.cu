@@ -27,6 +27,7 @@
 #include "dn_fields.cuh"
 #include "dn_krylov.cuh"
 #include "dn_momentum.cuh"
+#include "dn_momentum_adjoint.cuh"
 #include "dn_multigrid.cuh"
 
 using namespace dn;
@@ -436,6 +437,8 @@ struct dn_handle {
   MomLayout ml;
   double *mcoef = nullptr;
   int *mtgt = nullptr;
+  double *mtcoef = nullptr;  // M^T for the momentum adjoint (allocated on its first call)
+  int *mttgt = nullptr;
   double *mb = nullptr, *mx = nullptr, *mr = nullptr, *mrhat = nullptr, *mp0 = nullptr, *mp1 = nullptr, *mv0 = nullptr,
          *mv1 = nullptr, *mphat = nullptr, *ms = nullptr, *mshat = nullptr, *mt = nullptr, *mupd = nullptr,
          *mdinv = nullptr;
@@ -497,6 +500,7 @@ struct dn_handle {
   double ch_mg_alpha0 = -1.0;
   bool ch_mg = false;  // the CH solve runs the mixed form (FP64 defect correction around the FP32 inner CG)
   bool ic32_ready = false;  // FP32 copies of the IC/ILDLT factor made for this solve
+  bool mgp_split_ready = false, mgp_usable = false;  // the split operator's FP32 copy and hierarchy exist
   bool mixed_used_mg = false;  // the last mixed pressure solve started with the multigrid inner solver
   int refinement_cycles = 0;  // outer cycles of the last mixed-precision pressure solve
   dn_diag last_diag{};        // diagnostics at the end of the last dn_step (compute_diagnostics, solver.cpp:276)
@@ -964,17 +968,19 @@ dn_status mg_setup(dn_handle *h, MgHier &H, bool *usable) {
 // x0 = B b0: one V-cycle from level 0 with right-hand side b0 and result x0 (level 0's residual buffer is
 // H.lv[0].r)
 dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
-  constexpr int kSweeps = 2;  // red-black sweeps before and after each coarse correction
   const int L = H.levels(), px = h->G.px, py = h->G.py;
   H.lv[0].b = b0;
   H.lv[0].x = x0;
+  // levels from `bottom` down run inside one CTA (k_mg_bottom); the ones above get a launch per phase
+  int bottom = L - 1;
+  while (bottom > 0 && (long long)H.lv[bottom - 1].nx * H.lv[bottom - 1].ny <= kMgBottomCells) --bottom;
   auto smooth = [&](const MgLevel &M, int color, int first) -> dn_status {
     k_mg_smooth<<<blocks_for((long long)M.nx * (M.ny / 2)), 256, 0, h->stream>>>(M, color, first, px, py);
     return check_launch(h, "k_mg_smooth");
   };
-  for (int l = 0; l + 1 < L; ++l) {
+  for (int l = 0; l < bottom; ++l) {
     const MgLevel F = mg_level(H, l), C = mg_level(H, l + 1);
-    for (int k = 0; k < kSweeps; ++k) {
+    for (int k = 0; k < kMgSweeps; ++k) {
       DN_TRY(smooth(F, 0, k == 0));
       DN_TRY(smooth(F, 1, 0));
     }
@@ -983,13 +989,19 @@ dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
     k_mg_restrict<<<blocks_for((long long)C.nx * C.ny), 256, 0, h->stream>>>(F, C, H.fold);
     DN_TRY(check_launch(h, "k_mg_restrict"));
   }
-  k_mg_coarse_solve<<<1, kMgCoarseMax, 0, h->stream>>>(H.inv, mg_level(H, L - 1));
-  DN_TRY(check_launch(h, "k_mg_coarse_solve"));
-  for (int l = L - 2; l >= 0; --l) {
+  MgChain ch{};
+  for (int l = 0; l < L; ++l) ch.lv[l] = mg_level(H, l);
+  ch.first = bottom;
+  ch.last = L - 1;
+  ch.fold = H.fold;
+  ch.inv = H.inv;
+  k_mg_bottom<<<1, 1024, 0, h->stream>>>(ch);
+  DN_TRY(check_launch(h, "k_mg_bottom"));
+  for (int l = bottom - 1; l >= 0; --l) {
     const MgLevel F = mg_level(H, l), C = mg_level(H, l + 1);
     k_mg_prolong<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(C, F, H.fold);
     DN_TRY(check_launch(h, "k_mg_prolong"));
-    for (int k = 0; k < kSweeps; ++k) {
+    for (int k = 0; k < kMgSweeps; ++k) {
       DN_TRY(smooth(F, 1, 0));
       DN_TRY(smooth(F, 0, 0));
     }
@@ -1116,16 +1128,22 @@ dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
   const dn_config &cfg = h->cfg;
   const long long n = h->n;
   const int project = h->has_dirichlet ? 0 : 1;
-  k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
-  DN_TRY(check_launch(h, "k_to_float"));
   h->ic32_ready = false;
   bool use_mg = false;
-  if (h->mgp.levels() > 0) {
-    h->mgp.lv[0].a64 = h->a5;
-    h->mgp.lv[0].a = h->fa5;
-    h->mgp.lv[0].r = h->fy;
-    DN_TRY(mg_setup(h, h->mgp, &use_mg));
+  // the split operator is the same every step: its FP32 copy and hierarchy are built once
+  if (!(split && h->mgp_split_ready)) {
+    k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
+    DN_TRY(check_launch(h, "k_to_float"));
+    if (h->mgp.levels() > 0) {
+      h->mgp.lv[0].a64 = h->a5;
+      h->mgp.lv[0].a = h->fa5;
+      h->mgp.lv[0].r = h->fy;
+      DN_TRY(mg_setup(h, h->mgp, &use_mg));
+    }
+    h->mgp_split_ready = split;
+    h->mgp_usable = use_mg;
   }
+  use_mg = h->mgp_usable;
   h->mixed_used_mg = use_mg;
   if (!use_mg) DN_TRY(ensure_ic32(h, split, kind));
   const SpOp A{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
@@ -1266,11 +1284,14 @@ dn_status mixed_ch(dn_handle *h, double alpha0, dn_report *rep, double *iter_res
   return DN_OK;
 }
 
-dn_status run_bicgstab(dn_handle *h, double out[4]) {
+// Jacobi-BiCGSTAB on the momentum system (the handle's M, or another operator in the same row format --
+// the adjoint's M^T -- with its own stopping rule: relative when use_rel, else the reference's absolute one).
+dn_status run_bicgstab(dn_handle *h, double out[4], const double *coef = nullptr, const int *tgt = nullptr,
+                       int use_rel = 0, double tol = -1.0, int max_it = -1) {
   BicgArgs P;
   P.n = h->nm;
-  P.coef = h->mcoef;
-  P.tgt = h->mtgt;
+  P.coef = coef ? coef : h->mcoef;
+  P.tgt = tgt ? tgt : h->mtgt;
   P.b = h->mb;
   P.x = h->mx;
   P.r = h->mr;
@@ -1285,9 +1306,9 @@ dn_status run_bicgstab(dn_handle *h, double out[4]) {
   P.t = h->mt;
   P.upd = h->mupd;
   P.dinv = h->mdinv;
-  P.max_it = h->cfg.momentum_iterations;
-  P.tol = h->cfg.momentum_tolerance;
-  P.use_rel = 0;  // momentum.cpp:470-472: absolute tolerance
+  P.max_it = max_it > 0 ? max_it : h->cfg.momentum_iterations;
+  P.tol = tol > 0.0 ? tol : h->cfg.momentum_tolerance;
+  P.use_rel = use_rel;  // the forward solve: 0, momentum.cpp:470-472's absolute tolerance
   P.bar_count = h->bar_count;
   P.bar_gen = h->bar_gen;
   P.status = h->status;
@@ -3368,6 +3389,102 @@ dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const 
 
 // The CH advective term on caller device buffers: c (cell), u, v (faces) in, rhs = -div(u c) (cell) out,
 // computed as the phase step computes it (WENO5 faces, velocity face BCs on the fluxes).
+// The momentum predictor as a map (u, v, H_prev, f) -> (u*, v*) at the handle's rho_mid, eta, eta_prev
+// (compute_momentum_fluxes + solve_momentum_predictor, momentum.cpp:55-85, 157-502).  DEVICE Field2D buffers.
+dn_status dn_momentum_map(dn_handle *h, int step, const double *u, const double *v, const double *hu_prev,
+                          const double *hv_prev, const double *fxu, const double *fyv, double *u_star, double *v_star,
+                          int *iterations, double *residual) {
+  if (!h || !u || !v || !hu_prev || !hv_prev || !fxu || !fyv || !u_star || !v_star) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  auto d2d = [&](double *dst, const double *src, int id) -> dn_status {
+    DN_CUDA(h, cudaMemcpyAsync(dst, src, f[id].size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    return DN_OK;
+  };
+  DN_TRY(d2d(f[DN_F_U].d, u, DN_F_U));
+  DN_TRY(d2d(f[DN_F_V].d, v, DN_F_V));
+  DN_TRY(bc(h, f[DN_F_U], kBCU));
+  DN_TRY(bc(h, f[DN_F_V], kBCV));
+  DN_TRY(d2d(f[DN_F_HU_PREV].d, hu_prev, DN_F_HU_PREV));
+  DN_TRY(d2d(f[DN_F_HV_PREV].d, hv_prev, DN_F_HV_PREV));
+  DN_TRY(d2d(f[DN_F_SFX_U].d, fxu, DN_F_SFX_U));
+  DN_TRY(d2d(f[DN_F_SFY_V].d, fyv, DN_F_SFY_V));
+  dn_report rep{};
+  DN_TRY(momentum(h, step, &rep));
+  DN_TRY(d2d(u_star, f[DN_F_U_STAR].d, DN_F_U_STAR));
+  DN_TRY(d2d(v_star, f[DN_F_V_STAR].d, DN_F_V_STAR));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (iterations) *iterations = rep.momentum_iterations;
+  if (residual) *residual = rep.momentum_residual;
+  return DN_OK;
+}
+
+// Vector-Jacobian product of dn_momentum_map at the forward's (u, v) (dn_momentum_adjoint.cuh): cotangents
+// of u*, v* in; cotangents of u, v, H_prev (hu, hv) and f (fxu, fyv) out (ghosts zero).  The transposed
+// solve runs to a relative residual of 1e-14 (at most 20 x momentum_iterations iterations).
+dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const double *v, const double *gu_star,
+                              const double *gv_star, double *au, double *av, double *ahu, double *ahv, double *afu,
+                              double *afv, int *iterations, double *residual) {
+  if (!h || !u || !v || !gu_star || !gv_star || !au || !av || !ahu || !ahv || !afu || !afv)
+    return DN_ERR_INVALID_ARGUMENT;
+  const dn_config &cfg = h->cfg;
+  Fv *f = h->f;
+  const Fv &U = f[DN_F_U], &V = f[DN_F_V];
+  const Fv GU{const_cast<double *>(gu_star), U.nx, U.ny, U.g}, GV{const_cast<double *>(gv_star), V.nx, V.ny, V.g};
+  const Fv AU{au, U.nx, U.ny, U.g}, AV{av, V.nx, V.ny, V.g}, AHU{ahu, U.nx, U.ny, U.g}, AHV{ahv, V.nx, V.ny, V.g};
+  const Fv AFU{afu, U.nx, U.ny, U.g}, AFV{afv, V.nx, V.ny, V.g};
+  for (const Fv *o : {&AU, &AV, &AHU, &AHV, &AFU, &AFV})
+    DN_CUDA(h, cudaMemsetAsync(o->d, 0, o->size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(U.d, u, U.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(V.d, v, V.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, U, kBCU));
+  DN_TRY(bc(h, V, kBCV));
+  if (!h->mtcoef) {
+    dn_status s = dalloc(h, &h->mtcoef, 9 * h->nm);
+    if (s == DN_OK) s = dalloc(h, &h->mttgt, 9 * h->nm);
+    if (s != DN_OK) return fail(h, s, "device allocation failed: " + h->err);
+  }
+  const double alpha = 0.5 * cfg.dt / cfg.re;
+  // M at the handle's materials (its right-hand side is not used), then M^T
+  k_mom_assemble<<<blocks_for(h->nm, 128), 128, 0, h->stream>>>(h->ml, h->G, h->bc, U, V, f[DN_F_RHO_MID], f[DN_F_ETA],
+                                                           h->urhs, h->vrhs, alpha, h->mcoef, h->mtgt, h->mb, h->mx);
+  DN_TRY(check_launch(h, "k_mom_assemble"));
+  k_mom_transpose<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, h->mcoef, h->mtgt, h->mtcoef, h->mttgt);
+  DN_TRY(check_launch(h, "k_mom_transpose"));
+  // the cotangent of u*, v* through their face BCs, at the active faces
+  LAUNCH_INTERIOR(k_adj_fold_u, h->urhs, GU, h->urhs, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adj_fold_v, h->vrhs, GV, h->vrhs, h->G, h->bc);
+  k_mom_gather<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, h->urhs, h->vrhs, h->mb);
+  DN_TRY(check_launch(h, "k_mom_gather"));
+  DN_CUDA(h, cudaMemsetAsync(h->mx, 0, h->nm * sizeof(double), h->stream));
+  double out[4];
+  DN_TRY(run_bicgstab(h, out, h->mtcoef, h->mttgt, 1, 1.0e-14, 20 * std::max(1, cfg.momentum_iterations)));
+  // lambda on the faces, then the right-hand side's input cotangents
+  DN_TRY(fill_field(h, h->hu, 0.0));
+  DN_TRY(fill_field(h, h->hv, 0.0));
+  k_mom_scatter<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, h->mx, h->hu, h->hv);
+  DN_TRY(check_launch(h, "k_mom_scatter"));
+  k_mom_rhs_adj<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, U, V, f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hu, h->hv,
+                                                          AU, AV, AFU, AFV, AHU, AHV, h->G, step, cfg.dt, alpha);
+  DN_TRY(check_launch(h, "k_mom_rhs_adj"));
+  // the input BCs: ghosts onto the values they copy, then the boundary faces
+  auto ghosts = [&](const Fv &F, int kind, const BCSide *b) -> dn_status {
+    const long long ng = 2LL * F.g * F.ny + 2LL * F.g * (F.nx + 2 * F.g);
+    k_adj_ghosts<<<blocks_for(ng), 256, 0, h->stream>>>(F, h->G, kind, b[DN_LEFT], b[DN_RIGHT], b[DN_BOTTOM],
+                                                        b[DN_TOP]);
+    return check_launch(h, "k_adj_ghosts");
+  };
+  DN_TRY(ghosts(AU, kBCU, h->bc.u));
+  DN_TRY(ghosts(AV, kBCV, h->bc.v));
+  LAUNCH_INTERIOR(k_adj_fold_u, h->urhs, AU, h->urhs, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adj_fold_v, h->vrhs, AV, h->vrhs, h->G, h->bc);
+  LAUNCH_INTERIOR(k_copy_interior, AU, AU, h->urhs);
+  LAUNCH_INTERIOR(k_copy_interior, AV, AV, h->vrhs);
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (iterations) *iterations = (int)out[0];
+  if (residual) *residual = out[2];
+  return DN_OK;
+}
+
 dn_status dn_advection(dn_handle *h, const double *c, const double *u, const double *v, double *rhs) {
   if (!h || !c || !u || !v || !rhs) return DN_ERR_INVALID_ARGUMENT;
   Fv *f = h->f;

@@ -242,6 +242,21 @@ dn_status dn_projection(dn_handle *h, int step, const double *u_star, const doub
 dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
                                 const double *gpp, double *au, double *av, double *ap, double *app,
                                 int *iterations, double *relative_residual);
+/* The momentum predictor as a map (compute_momentum_fluxes + solve_momentum_predictor, momentum.cpp:55-85,
+ * 157-502): u, v (their BCs applied), H_prev (hu_prev, hv_prev) and the face surface forces (fxu, fyv) in;
+ * u_star, v_star out, with the handle's rho_mid, eta and eta_prev.  DEVICE Field2D buffers; uses the
+ * handle's fields as work space. */
+dn_status dn_momentum_map(dn_handle *h, int step, const double *u, const double *v, const double *hu_prev,
+                          const double *hv_prev, const double *fxu, const double *fyv, double *u_star, double *v_star,
+                          int *iterations, double *residual);
+/* No counterpart in the reference.  Vector-Jacobian product of dn_momentum_map at (u, v), rho_mid, eta and
+ * eta_prev held fixed: cotangents of the interior values of u_star, v_star in; cotangents of the interior
+ * values of u, v, hu_prev, hv_prev, fxu, fyv out (ghosts 0).  The transposed coupled system M^T is solved by
+ * the same Jacobi-BiCGSTAB to a relative residual of 1e-14; its iterations and relative residual are
+ * reported.  DEVICE buffers. */
+dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const double *v, const double *gu_star,
+                              const double *gv_star, double *au, double *av, double *ahu, double *ahv, double *afu,
+                              double *afv, int *iterations, double *residual);
 
 /* The CH advective term -div(u c) with WENO5 face values, as build_phase_advection_fluxes
  * (phase_field.cpp:283-311) computes it, on caller DEVICE buffers: c (cell field), u, v (face fields) in,
