@@ -120,8 +120,12 @@ def load():
         "dn_pressure_solve": (I, [H, I, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int), DP]),
         "dn_projection": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
         "dn_projection_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
-        "dn_momentum_map": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
-        "dn_momentum_adjoint": (I, [H, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, VP, C.POINTER(C.c_int), DP]),
+        "dn_momentum_map": (I, [H, I] + [VP] * 13 + [C.POINTER(C.c_int), DP]),
+        "dn_momentum_adjoint": (I, [H, I] + [VP] * 22 + [C.POINTER(C.c_int), DP]),
+        "dn_projection_rho": (I, [H, I] + [VP] * 9 + [C.POINTER(C.c_int), DP]),
+        "dn_projection_rho_adjoint": (I, [H, I] + [VP] * 13 + [C.POINTER(C.c_int), DP]),
+        "dn_surface_force_map": (I, [H, VP, VP, VP, VP]),
+        "dn_surface_force_adjoint": (I, [H, VP, VP, VP, VP, VP, VP]),
         "dn_advection": (I, [H, VP, VP, VP, VP]),
         "dn_advection_adjoint": (I, [H, VP, VP, VP, VP, VP, VP, VP]),
         "dn_set_pressure_monitor": (I, [H, I]),

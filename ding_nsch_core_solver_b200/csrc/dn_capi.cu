@@ -3339,10 +3339,12 @@ dn_status dn_projection(dn_handle *h, int step, const double *u_star, const doub
 
 // Transpose of dn_projection's linear part (rho_mid fixed): cotangents of the interior values of u, v,
 // p_new, p_prev_new in; cotangents of the interior values of u*, v*, p, p_prev out (ghosts zero).
-dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
-                                const double *gpp, double *au, double *av, double *ap, double *app, int *iterations,
-                                double *relative_residual) {
-  if (!h || !gu || !gv || !gp || !gpp || !au || !av || !ap || !app) return DN_ERR_INVALID_ARGUMENT;
+// With arho: also the cotangent of rho_mid (k_proj_rho_adj), for which the forward's p, p_prev and p_new are
+// needed (p_new is p_corr less its mean, which no rho_mid term sees).
+dn_status projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
+                             const double *gpp, double *au, double *av, double *ap, double *app, const double *p,
+                             const double *p_prev, const double *p_new, double *arho, int *iterations,
+                             double *relative_residual) {
   const dn_config &cfg = h->cfg;
   if (cfg.pressure_scheme == DN_P_JACOBI)
     return fail(h, DN_ERR_UNSUPPORTED, "pressure_scheme jacobi is not implemented by the CUDA backend");
@@ -3381,20 +3383,73 @@ dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const 
   k_adj_cells_post<<<blocks_for(h->n), 256, 0, h->stream>>>(h->x, GPP, f[DN_F_RHO_MID], h->G, split ? 1 : 0, rho_ref,
                                                             step, AP, APP);
   DN_TRY(check_launch(h, "k_adj_cells_post"));
+  if (arho) {
+    const Fv AR{arho, P.nx, P.ny, P.g};
+    DN_CUDA(h, cudaMemsetAsync(arho, 0, P.size() * sizeof(double), h->stream));
+    const size_t pb = P.size() * sizeof(double);
+    DN_CUDA(h, cudaMemcpyAsync(h->bih.d, p_new, pb, cudaMemcpyDeviceToDevice, h->stream));
+    DN_TRY(bc(h, h->bih, kBCPressure));
+    if (split) {
+      DN_CUDA(h, cudaMemcpyAsync(f[DN_F_P].d, p, pb, cudaMemcpyDeviceToDevice, h->stream));
+      DN_CUDA(h, cudaMemcpyAsync(f[DN_F_P_PREV].d, p_prev, pb, cudaMemcpyDeviceToDevice, h->stream));
+      DN_TRY(bc(h, f[DN_F_P], kBCPressure));
+      DN_TRY(bc(h, f[DN_F_P_PREV], kBCPressure));
+      DN_TRY(split_extrapolation(h, step));
+    }
+    LAUNCH_INTERIOR(k_adj_fold_u, h->urhs, GU, h->urhs, h->G, h->bc);
+    LAUNCH_INTERIOR(k_adj_fold_v, h->vrhs, GV, h->vrhs, h->G, h->bc);
+    const long long nf = (long long)(h->G.nx + 1) * h->G.ny + (long long)h->G.nx * (h->G.ny + 1);
+    k_proj_rho_adj<<<blocks_for(nf), 256, 0, h->stream>>>(h->urhs, h->vrhs, h->x, h->bih, h->pe, f[DN_F_RHO_MID], AR,
+                                                          h->G, h->bc, split ? 1 : 0, rho_ref, cfg.dt);
+    DN_TRY(check_launch(h, "k_proj_rho_adj"));
+  }
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
   if (iterations) *iterations = rep.pressure_iterations;
   if (relative_residual) *relative_residual = rep.pressure_residual;
   return DN_OK;
 }
 
-// The CH advective term on caller device buffers: c (cell), u, v (faces) in, rhs = -div(u c) (cell) out,
-// computed as the phase step computes it (WENO5 faces, velocity face BCs on the fluxes).
-// The momentum predictor as a map (u, v, H_prev, f) -> (u*, v*) at the handle's rho_mid, eta, eta_prev
+dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
+                                const double *gpp, double *au, double *av, double *ap, double *app, int *iterations,
+                                double *relative_residual) {
+  if (!h || !gu || !gv || !gp || !gpp || !au || !av || !ap || !app) return DN_ERR_INVALID_ARGUMENT;
+  return projection_adjoint(h, step, gu, gv, gp, gpp, au, av, ap, app, nullptr, nullptr, nullptr, nullptr,
+                            iterations, relative_residual);
+}
+
+// dn_projection with rho_mid as an input (scalar BC applied), and its vector-Jacobian product including the
+// cotangent of rho_mid.  DEVICE buffers.
+dn_status dn_projection_rho(dn_handle *h, int step, const double *u_star, const double *v_star, const double *p,
+                            const double *p_prev, const double *rho_mid, double *u, double *v, double *p_new,
+                            double *p_prev_new, int *iterations, double *relative_residual) {
+  if (!h || !rho_mid) return DN_ERR_INVALID_ARGUMENT;
+  const Fv &R = h->f[DN_F_RHO_MID];
+  DN_CUDA(h, cudaMemcpyAsync(R.d, rho_mid, R.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, R, kBCScalar));
+  return dn_projection(h, step, u_star, v_star, p, p_prev, u, v, p_new, p_prev_new, iterations, relative_residual);
+}
+dn_status dn_projection_rho_adjoint(dn_handle *h, int step, const double *rho_mid, const double *p,
+                                    const double *p_prev, const double *p_new, const double *gu, const double *gv,
+                                    const double *gp, const double *gpp, double *au, double *av, double *ap,
+                                    double *app, double *arho, int *iterations, double *relative_residual) {
+  if (!h || !rho_mid || !p || !p_prev || !p_new || !gu || !gv || !gp || !gpp || !au || !av || !ap || !app || !arho)
+    return DN_ERR_INVALID_ARGUMENT;
+  const Fv &R = h->f[DN_F_RHO_MID];
+  DN_CUDA(h, cudaMemcpyAsync(R.d, rho_mid, R.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, R, kBCScalar));
+  return projection_adjoint(h, step, gu, gv, gp, gpp, au, av, ap, app, p, p_prev, p_new, arho, iterations,
+                            relative_residual);
+}
+
+// The momentum predictor as a map (u, v, H_prev, f, rho_mid, eta, eta_prev) -> (u*, v*, H)
 // (compute_momentum_fluxes + solve_momentum_predictor, momentum.cpp:55-85, 157-502).  DEVICE Field2D buffers.
 dn_status dn_momentum_map(dn_handle *h, int step, const double *u, const double *v, const double *hu_prev,
-                          const double *hv_prev, const double *fxu, const double *fyv, double *u_star, double *v_star,
-                          int *iterations, double *residual) {
-  if (!h || !u || !v || !hu_prev || !hv_prev || !fxu || !fyv || !u_star || !v_star) return DN_ERR_INVALID_ARGUMENT;
+                          const double *hv_prev, const double *fxu, const double *fyv, const double *rho_mid,
+                          const double *eta, const double *eta_prev, double *u_star, double *v_star, double *hu,
+                          double *hv, int *iterations, double *residual) {
+  if (!h || !u || !v || !hu_prev || !hv_prev || !fxu || !fyv || !rho_mid || !eta || !eta_prev || !u_star ||
+      !v_star || !hu || !hv)
+    return DN_ERR_INVALID_ARGUMENT;
   Fv *f = h->f;
   auto d2d = [&](double *dst, const double *src, int id) -> dn_status {
     DN_CUDA(h, cudaMemcpyAsync(dst, src, f[id].size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -3408,43 +3463,66 @@ dn_status dn_momentum_map(dn_handle *h, int step, const double *u, const double 
   DN_TRY(d2d(f[DN_F_HV_PREV].d, hv_prev, DN_F_HV_PREV));
   DN_TRY(d2d(f[DN_F_SFX_U].d, fxu, DN_F_SFX_U));
   DN_TRY(d2d(f[DN_F_SFY_V].d, fyv, DN_F_SFY_V));
+  const int mats[3] = {DN_F_RHO_MID, DN_F_ETA, DN_F_ETA_PREV};
+  const double *msrc[3] = {rho_mid, eta, eta_prev};
+  for (int k = 0; k < 3; ++k) {
+    DN_TRY(d2d(f[mats[k]].d, msrc[k], mats[k]));
+    DN_TRY(bc(h, f[mats[k]], kBCScalar));
+  }
   dn_report rep{};
   DN_TRY(momentum(h, step, &rep));
   DN_TRY(d2d(u_star, f[DN_F_U_STAR].d, DN_F_U_STAR));
   DN_TRY(d2d(v_star, f[DN_F_V_STAR].d, DN_F_V_STAR));
+  DN_TRY(d2d(hu, f[DN_F_HU_PREV].d, DN_F_HU_PREV));  // momentum() leaves this step's H there
+  DN_TRY(d2d(hv, f[DN_F_HV_PREV].d, DN_F_HV_PREV));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
   if (iterations) *iterations = rep.momentum_iterations;
   if (residual) *residual = rep.momentum_residual;
   return DN_OK;
 }
 
-// Vector-Jacobian product of dn_momentum_map at the forward's (u, v) (dn_momentum_adjoint.cuh): cotangents
-// of u*, v* in; cotangents of u, v, H_prev (hu, hv) and f (fxu, fyv) out (ghosts zero).  The transposed
-// solve runs to a relative residual of 1e-14 (at most 20 x momentum_iterations iterations).
-dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const double *v, const double *gu_star,
-                              const double *gv_star, double *au, double *av, double *ahu, double *ahv, double *afu,
-                              double *afv, int *iterations, double *residual) {
-  if (!h || !u || !v || !gu_star || !gv_star || !au || !av || !ahu || !ahv || !afu || !afv)
+// Vector-Jacobian product of dn_momentum_map at its forward point (u, v, H_prev, materials, and the
+// solution u*, v*) (dn_momentum_adjoint.cuh): cotangents of u*, v*, H in; cotangents of u, v, H_prev
+// (ahu, ahv), f (afu, afv), rho_mid, eta and eta_prev out (ghosts zero).  The transposed solve runs to a
+// relative residual of 1e-14 (at most 20 x momentum_iterations iterations).
+dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const double *v, const double *hu_prev,
+                              const double *hv_prev, const double *rho_mid, const double *eta, const double *eta_prev,
+                              const double *u_star, const double *v_star, const double *gu_star,
+                              const double *gv_star, const double *ghu, const double *ghv, double *au, double *av,
+                              double *ahu, double *ahv, double *afu, double *afv, double *arho, double *aeta,
+                              double *aeta_prev, int *iterations, double *residual) {
+  if (!h || !u || !v || !hu_prev || !hv_prev || !rho_mid || !eta || !eta_prev || !u_star || !v_star || !gu_star ||
+      !gv_star || !ghu || !ghv || !au || !av || !ahu || !ahv || !afu || !afv || !arho || !aeta || !aeta_prev)
     return DN_ERR_INVALID_ARGUMENT;
   const dn_config &cfg = h->cfg;
   Fv *f = h->f;
-  const Fv &U = f[DN_F_U], &V = f[DN_F_V];
-  const Fv GU{const_cast<double *>(gu_star), U.nx, U.ny, U.g}, GV{const_cast<double *>(gv_star), V.nx, V.ny, V.g};
-  const Fv AU{au, U.nx, U.ny, U.g}, AV{av, V.nx, V.ny, V.g}, AHU{ahu, U.nx, U.ny, U.g}, AHV{ahv, V.nx, V.ny, V.g};
-  const Fv AFU{afu, U.nx, U.ny, U.g}, AFV{afv, V.nx, V.ny, V.g};
-  for (const Fv *o : {&AU, &AV, &AHU, &AHV, &AFU, &AFV})
+  const Fv &U = f[DN_F_U], &V = f[DN_F_V], &Cell = f[DN_F_RHO_MID];
+  auto view = [](const double *p, const Fv &like) { return Fv{const_cast<double *>(p), like.nx, like.ny, like.g}; };
+  const Fv GU = view(gu_star, U), GV = view(gv_star, V), GHU = view(ghu, U), GHV = view(ghv, V);
+  const Fv AU = view(au, U), AV = view(av, V), AHU = view(ahu, U), AHV = view(ahv, V), AFU = view(afu, U),
+           AFV = view(afv, V), AR = view(arho, Cell), AE = view(aeta, Cell), AEP = view(aeta_prev, Cell);
+  for (const Fv *o : {&AU, &AV, &AHU, &AHV, &AFU, &AFV, &AR, &AE, &AEP})
     DN_CUDA(h, cudaMemsetAsync(o->d, 0, o->size() * sizeof(double), h->stream));
-  DN_CUDA(h, cudaMemcpyAsync(U.d, u, U.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  DN_CUDA(h, cudaMemcpyAsync(V.d, v, V.size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  DN_TRY(bc(h, U, kBCU));
-  DN_TRY(bc(h, V, kBCV));
+  auto load = [&](int id, const double *src, int kind) -> dn_status {
+    DN_CUDA(h, cudaMemcpyAsync(f[id].d, src, f[id].size() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    return kind >= 0 ? bc(h, f[id], kind) : DN_OK;
+  };
+  DN_TRY(load(DN_F_U, u, kBCU));
+  DN_TRY(load(DN_F_V, v, kBCV));
+  DN_TRY(load(DN_F_U_STAR, u_star, kBCU));
+  DN_TRY(load(DN_F_V_STAR, v_star, kBCV));
+  DN_TRY(load(DN_F_HU_PREV, hu_prev, -1));
+  DN_TRY(load(DN_F_HV_PREV, hv_prev, -1));
+  DN_TRY(load(DN_F_RHO_MID, rho_mid, kBCScalar));
+  DN_TRY(load(DN_F_ETA, eta, kBCScalar));
+  DN_TRY(load(DN_F_ETA_PREV, eta_prev, kBCScalar));
   if (!h->mtcoef) {
     dn_status s = dalloc(h, &h->mtcoef, 9 * h->nm);
     if (s == DN_OK) s = dalloc(h, &h->mttgt, 9 * h->nm);
     if (s != DN_OK) return fail(h, s, "device allocation failed: " + h->err);
   }
   const double alpha = 0.5 * cfg.dt / cfg.re;
-  // M at the handle's materials (its right-hand side is not used), then M^T
+  // M at these materials (its right-hand side is not used), then M^T
   k_mom_assemble<<<blocks_for(h->nm, 128), 128, 0, h->stream>>>(h->ml, h->G, h->bc, U, V, f[DN_F_RHO_MID], f[DN_F_ETA],
                                                            h->urhs, h->vrhs, alpha, h->mcoef, h->mtgt, h->mb, h->mx);
   DN_TRY(check_launch(h, "k_mom_assemble"));
@@ -3458,14 +3536,22 @@ dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const dou
   DN_CUDA(h, cudaMemsetAsync(h->mx, 0, h->nm * sizeof(double), h->stream));
   double out[4];
   DN_TRY(run_bicgstab(h, out, h->mtcoef, h->mttgt, 1, 1.0e-14, 20 * std::max(1, cfg.momentum_iterations)));
-  // lambda on the faces, then the right-hand side's input cotangents
+  // lambda on the faces (h->hu, h->hv); H's cotangent through H's face BC (h->urhs, h->vrhs)
   DN_TRY(fill_field(h, h->hu, 0.0));
   DN_TRY(fill_field(h, h->hv, 0.0));
   k_mom_scatter<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, h->mx, h->hu, h->hv);
   DN_TRY(check_launch(h, "k_mom_scatter"));
+  LAUNCH_INTERIOR(k_adj_fold_u, h->urhs, GHU, h->urhs, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adj_fold_v, h->vrhs, GHV, h->vrhs, h->G, h->bc);
   k_mom_rhs_adj<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, U, V, f[DN_F_RHO_MID], f[DN_F_ETA_PREV], h->hu, h->hv,
-                                                          AU, AV, AFU, AFV, AHU, AHV, h->G, step, cfg.dt, alpha);
+                                                          h->urhs, h->vrhs, AU, AV, AFU, AFV, AHU, AHV, h->G, step,
+                                                          cfg.dt, alpha);
   DN_TRY(check_launch(h, "k_mom_rhs_adj"));
+  k_mom_material_adj<<<blocks_for(h->nm), 256, 0, h->stream>>>(h->ml, f[DN_F_U_STAR], f[DN_F_V_STAR], U, V,
+                                                               f[DN_F_HU_PREV], f[DN_F_HV_PREV], h->hu, h->hv, AR, AE,
+                                                               AEP, h->G, step, cfg.dt, alpha, cfg.body_force_x,
+                                                               cfg.body_force_y);
+  DN_TRY(check_launch(h, "k_mom_material_adj"));
   // the input BCs: ghosts onto the values they copy, then the boundary faces
   auto ghosts = [&](const Fv &F, int kind, const BCSide *b) -> dn_status {
     const long long ng = 2LL * F.g * F.ny + 2LL * F.g * (F.nx + 2 * F.g);
@@ -3475,6 +3561,7 @@ dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const dou
   };
   DN_TRY(ghosts(AU, kBCU, h->bc.u));
   DN_TRY(ghosts(AV, kBCV, h->bc.v));
+  for (const Fv *m : {&AR, &AE, &AEP}) DN_TRY(ghosts(*m, kBCScalar, h->bc.p));
   LAUNCH_INTERIOR(k_adj_fold_u, h->urhs, AU, h->urhs, h->G, h->bc);
   LAUNCH_INTERIOR(k_adj_fold_v, h->vrhs, AV, h->vrhs, h->G, h->bc);
   LAUNCH_INTERIOR(k_copy_interior, AU, AU, h->urhs);
@@ -3485,6 +3572,74 @@ dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const dou
   return DN_OK;
 }
 
+// The face surface forces as a map (c_old, c_new) -> (fxu, fyv) (update_surface_tension_force,
+// phase_field.cpp:179-256, with the step's smoothing passes).  DEVICE Field2D buffers.
+dn_status dn_surface_force_map(dn_handle *h, const double *c_old, const double *c_new, double *fxu, double *fyv) {
+  if (!h || !c_old || !c_new || !fxu || !fyv) return DN_ERR_INVALID_ARGUMENT;
+  Fv *f = h->f;
+  const size_t cb = h->mob.size() * sizeof(double);
+  DN_CUDA(h, cudaMemcpyAsync(h->mob.d, c_old, cb, cudaMemcpyDeviceToDevice, h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(h->lap.d, c_new, cb, cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->mob, kBCScalar));
+  DN_TRY(bc(h, h->lap, kBCScalar));
+  DN_TRY(surface_force(h, h->mob, h->lap));
+  DN_CUDA(h, cudaMemcpyAsync(fxu, f[DN_F_SFX_U].d, f[DN_F_SFX_U].size() * sizeof(double), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(fyv, f[DN_F_SFY_V].d, f[DN_F_SFY_V].size() * sizeof(double), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+// Vector-Jacobian product of dn_surface_force_map (dn_momentum_adjoint.cuh, k_sf_adj_faces, k_chem_adj):
+// cotangents of the interior face forces in, of the interior values of c_old and c_new out (equal: the
+// forces depend on c_mid = (c_old + c_new) / 2 only).  Not available with smoothing passes.
+dn_status dn_surface_force_adjoint(dn_handle *h, const double *c_old, const double *c_new, const double *gfxu,
+                                   const double *gfyv, double *ac_old, double *ac_new) {
+  if (!h || !c_old || !c_new || !gfxu || !gfyv || !ac_old || !ac_new) return DN_ERR_INVALID_ARGUMENT;
+  const dn_config &cfg = h->cfg;
+  Fv *f = h->f;
+  const Fv &Cc = f[DN_F_C];
+  const Fv ACO{ac_old, Cc.nx, Cc.ny, Cc.g}, ACN{ac_new, Cc.nx, Cc.ny, Cc.g};
+  DN_CUDA(h, cudaMemsetAsync(ac_old, 0, Cc.size() * sizeof(double), h->stream));
+  DN_CUDA(h, cudaMemsetAsync(ac_new, 0, Cc.size() * sizeof(double), h->stream));
+  if (cfg.surface_tension_multiplier == 0.0 || !compute_mu(cfg)) return DN_OK;
+  if (cfg.surface_tension_smoothing_passes > 0 && cfg.surface_tension_smoothing_weight > 0.0)
+    return fail(h, DN_ERR_UNSUPPORTED, "the surface-force adjoint does not cover smoothing passes");
+  const Fv &FU = f[DN_F_SFX_U], &FV = f[DN_F_SFY_V];
+  const Fv GFU{const_cast<double *>(gfxu), FU.nx, FU.ny, FU.g}, GFV{const_cast<double *>(gfyv), FV.nx, FV.ny, FV.g};
+  // c_mid (scalar BC ghosts) and mu_mid, as the forward builds them
+  const size_t cb = Cc.size() * sizeof(double);
+  DN_CUDA(h, cudaMemcpyAsync(h->mob.d, c_old, cb, cudaMemcpyDeviceToDevice, h->stream));
+  DN_CUDA(h, cudaMemcpyAsync(h->lap.d, c_new, cb, cudaMemcpyDeviceToDevice, h->stream));
+  DN_TRY(bc(h, h->mob, kBCScalar));
+  DN_TRY(bc(h, h->lap, kBCScalar));
+  LAUNCH_INTERIOR(k_cmid, h->cmid, h->mob, h->lap, h->cmid);
+  DN_TRY(bc(h, h->cmid, kBCScalar));
+  LAUNCH_INTERIOR(k_chem, h->mm, h->cmid, h->mm, h->G, cfg.cn);
+  // the forces' face BCs folded (into the face work arrays), then the transposed stencils
+  LAUNCH_INTERIOR(k_adj_fold_u, h->urhs, GFU, h->urhs, h->G, h->bc);
+  LAUNCH_INTERIOR(k_adj_fold_v, h->vrhs, GFV, h->vrhs, h->G, h->bc);
+  DN_TRY(fill_field(h, h->bih, 0.0));   // c_mid cotangent
+  DN_TRY(fill_field(h, h->ddiv, 0.0));  // mu_mid cotangent
+  const double scale = cfg.surface_tension_multiplier / (cfg.re * cfg.ca);
+  const long long nf = (long long)(h->G.nx + 1) * h->G.ny + (long long)h->G.nx * (h->G.ny + 1);
+  k_sf_adj_faces<<<blocks_for(nf), 256, 0, h->stream>>>(h->urhs, h->vrhs, h->cmid, h->mm, h->bih, h->ddiv, h->G, scale);
+  DN_TRY(check_launch(h, "k_sf_adj_faces"));
+  LAUNCH_INTERIOR(k_chem_adj, h->cmid, h->cmid, h->ddiv, h->bih, h->G, cfg.cn);
+  const Fv &B = h->bih;
+  const long long ng = 2LL * B.g * B.ny + 2LL * B.g * (B.nx + 2 * B.g);
+  k_adj_ghosts<<<blocks_for(ng), 256, 0, h->stream>>>(B, h->G, kBCScalar, h->bc.p[DN_LEFT], h->bc.p[DN_RIGHT],
+                                                      h->bc.p[DN_BOTTOM], h->bc.p[DN_TOP]);
+  DN_TRY(check_launch(h, "k_adj_ghosts"));
+  LAUNCH_INTERIOR(k_half_interior, ACO, B, ACO);
+  LAUNCH_INTERIOR(k_half_interior, ACN, B, ACN);
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return DN_OK;
+}
+
+// The CH advective term on caller device buffers: c (cell), u, v (faces) in, rhs = -div(u c) (cell) out,
+// computed as the phase step computes it (WENO5 faces, velocity face BCs on the fluxes).
 dn_status dn_advection(dn_handle *h, const double *c, const double *u, const double *v, double *rhs) {
   if (!h || !c || !u || !v || !rhs) return DN_ERR_INVALID_ARGUMENT;
   Fv *f = h->f;

@@ -1,16 +1,18 @@
 // dn_momentum_adjoint.cuh -- discrete adjoint of the momentum predictor (solve_momentum_predictor,
 // momentum.cpp:157-502) as a map of the velocity state, at fixed materials.
 //
-// The map: (u, v, H_prev, f) -> (u*, v*).  The inputs' BCs are applied (bc(u, kBCU), bc(v, kBCV)), the
+// The map: (u, v, H_prev, f, rho_mid, eta, eta_prev) -> (u*, v*, H).  The inputs' BCs are applied (bc(u, kBCU), bc(v, kBCV)), the
 // predictor right-hand side is formed (k_mom_conv_rhs: rho_face u + dt (-rho_face conv + rho_face g + f) +
 // alpha visc(u, v; eta_prev), conv = H(u, v) on step 0 and 1.5 H - 0.5 H_prev after), the coupled system
 // M(rho_mid, eta) x = rhs is solved, x is scattered to the active faces and the faces' BCs fill the rest.
-// rho_mid, eta and eta_prev are constants of the map.  Its adjoint, for a cotangent (gu*, gv*):
+// H = H(u, v) with its face BC is the next step's H_prev.  Its adjoint, for cotangents (gu*, gv*, gH):
 //   1. fold the cotangent through the output face BCs (k_adj_fold_u / _v) and gather it at the active faces;
 //   2. solve M^T lambda = g (M^T assembled from M's rows, solved by the same Jacobi-BiCGSTAB);
 //   3. lambda is the cotangent of the right-hand side: f_bar = dt lambda, H_prev_bar = 0.5 dt rho_face lambda
 //      (steps > 0), and (u, v)_bar collect rho_face lambda plus the transposed stencils of the centred
-//      convection (linearised at the forward's u, v) and of the viscous divergence (k_mom_rhs_adj);
+//      convection (linearised at the forward's u, v; with gH folded through H's face BC) and of the viscous
+//      divergence (k_mom_rhs_adj); the materials' cotangents follow from -lambda^T dF/dm
+//      (k_mom_material_adj);
 //   4. the input BCs are undone: each ghost's cotangent moves to the interior value its BC copies (sign -1
 //      through a Dirichlet reflection, k_adj_ghosts), then the face BCs are folded (k_adj_fold_u / _v).
 // Scatters use FP64 atomics (the summation order of a cotangent entry is not fixed, so gradients agree to
@@ -104,8 +106,10 @@ __global__ void k_mom_gather(MomLayout L, Fv gu, Fv gv, double *g) {
 // (H = uf du/dx + vf du/dy for u faces, uf dv/dx + vf dv/dy for v faces; momentum.cpp:55-85) scaled by
 // -dt rho_face (1 or 1.5), the transposed viscous divergence (visc_u / visc_v) scaled by alpha, and the
 // direct f and H_prev cotangents.  au, av are ghosted and zero on entry.
-__global__ void k_mom_rhs_adj(MomLayout L, Fv u, Fv v, Fv rm, Fv etap, Fv lu, Fv lv, Fv au, Fv av, Fv afu, Fv afv,
-                              Fv ahu, Fv ahv, Grid G, int step, double dt, double alpha) {
+// gh_u, gh_v: the (face-BC folded) cotangent of the map's H output, which enters the convection transposes
+// with lambda's -dt rho_face (1 or 1.5).
+__global__ void k_mom_rhs_adj(MomLayout L, Fv u, Fv v, Fv rm, Fv etap, Fv lu, Fv lv, Fv gh_u, Fv gh_v, Fv au, Fv av,
+                              Fv afu, Fv afv, Fv ahu, Fv ahv, Grid G, int step, double dt, double alpha) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= L.n()) return;
   const double dx = G.dx, dy = G.dy;
@@ -114,14 +118,14 @@ __global__ void k_mom_rhs_adj(MomLayout L, Fv u, Fv v, Fv rm, Fv etap, Fv lu, Fv
   auto addv = [&](int i, int j, double val) { atomicAdd(&av.at(i, j), val); };
   if (t < L.nu) {
     const int i = (int)(t / L.ny), j = (int)(t % L.ny);
-    const double w = lu.at(i, j);
-    if (w == 0.0) return;
+    const double w = lu.at(i, j), gh = gh_u.at(i, j);
+    if (w == 0.0 && gh == 0.0) return;
     const double rf = xface(rm, G, i, j);
     afu.at(i, j) = dt * w;
     if (step != 0) ahu.at(i, j) = 0.5 * dt * rf * w;
     addu(i, j, rf * w);
     // convection: H = uf * dudx + vf * dudy
-    const double c = -dt * rf * ch * w;
+    const double c = -dt * rf * ch * w + gh;
     const double uf = u.at(i, j);
     const double dudx = (u.at(i + 1, j) - u.at(i - 1, j)) / (2.0 * dx);
     const double dudy = (u.at(i, j + 1) - u.at(i, j - 1)) / (2.0 * dy);
@@ -155,14 +159,14 @@ __global__ void k_mom_rhs_adj(MomLayout L, Fv u, Fv v, Fv rm, Fv etap, Fv lu, Fv
   } else {
     const long long q = t - L.nu;
     const int i = (int)(q / (L.ny + 1)), j = (int)(q % (L.ny + 1));
-    const double w = lv.at(i, j);
-    if (w == 0.0) return;
+    const double w = lv.at(i, j), gh = gh_v.at(i, j);
+    if (w == 0.0 && gh == 0.0) return;
     const double rf = yface(rm, G, i, j);
     afv.at(i, j) = dt * w;
     if (step != 0) ahv.at(i, j) = 0.5 * dt * rf * w;
     addv(i, j, rf * w);
     // convection: H = uf * dvdx + vf * dvdy
-    const double c = -dt * rf * ch * w;
+    const double c = -dt * rf * ch * w + gh;
     const double vf = v.at(i, j);
     const double dvdx = (v.at(i + 1, j) - v.at(i - 1, j)) / (2.0 * dx);
     const double dvdy = (v.at(i, j + 1) - v.at(i, j - 1)) / (2.0 * dy);
@@ -193,6 +197,88 @@ __global__ void k_mom_rhs_adj(MomLayout L, Fv u, Fv v, Fv rm, Fv etap, Fv lu, Fv
     addu(i + 1, j - 1, -a * xe);
     addu(i, j, -a * xw);
     addu(i, j - 1, a * xw);
+  }
+}
+
+// Cotangents of the materials, one thread per face with lambda != 0.  With the solution x (u*, v*; its BC
+// ghosts filled), the row of the solved system is F = rf x - alpha visc(x; eta) - rhs(u, v; rf, eta_prev) = 0
+// (M's Dirichlet / Neumann folds are the BC ghosts of x, their constants the rhs's folds), so for every
+// material m:  dL/dm = -lambda^T dF/dm, that is
+//   rf:       -lambda (x - u + dt conv - dt g)      onto rho_mid through xface / yface;
+//   eta:      +alpha lambda dvisc(x; eta)/deta       onto the face / corner means of eta;
+//   eta_prev: +alpha lambda dvisc(u; eta_prev)/deta  the same with the forward's u, v.
+// The corner means read eta's ghosts; the caller moves those cotangents with k_adj_ghosts (scalar BC).
+__device__ __forceinline__ void add_face_mean(const Fv &a, const Grid &G, bool xdir, int i, int j, double val) {
+  // adjoint of xface(f, G, i, j) (xdir) / yface(f, G, i, j)
+  const int n = xdir ? G.nx : G.ny, k = xdir ? i : j;
+  const int per = xdir ? G.px : G.py;
+  auto at = [&](int kk) -> double & { return xdir ? a.at(kk, j) : a.at(i, kk); };
+  if (k <= 0 || k >= n) {
+    if (per) {
+      atomicAdd(&at(n - 1), 0.5 * val);
+      atomicAdd(&at(0), 0.5 * val);
+    } else {
+      atomicAdd(&at(k <= 0 ? 0 : n - 1), val);
+    }
+  } else {
+    atomicAdd(&at(k - 1), 0.5 * val);
+    atomicAdd(&at(k), 0.5 * val);
+  }
+}
+__device__ __forceinline__ void add_corner_mean(const Fv &a, int i, int j, double val) {
+  // adjoint of corner(f, i, j)
+  const double q = 0.25 * val;
+  atomicAdd(&a.at(i, j), q);
+  atomicAdd(&a.at(i - 1, j), q);
+  atomicAdd(&a.at(i, j - 1), q);
+  atomicAdd(&a.at(i - 1, j - 1), q);
+}
+// d visc_u(x) / d (eta_e, eta_w, eta_n, eta_s) scaled by s, onto eta (momentum.cpp:91-155 terms)
+__device__ __forceinline__ void visc_u_eta_adj(const Fv &x, const Fv &y, const Fv &a, const Grid &G, int i, int j,
+                                               double s) {
+  const double dudx_e = (x.at(i + 1, j) - x.at(i, j)) / G.dx, dudx_w = (x.at(i, j) - x.at(i - 1, j)) / G.dx;
+  const double dudy_n = (x.at(i, j + 1) - x.at(i, j)) / G.dy, dudy_s = (x.at(i, j) - x.at(i, j - 1)) / G.dy;
+  const double dvdx_n = (y.at(i, j + 1) - y.at(i - 1, j + 1)) / G.dx, dvdx_s = (y.at(i, j) - y.at(i - 1, j)) / G.dx;
+  add_face_mean(a, G, true, i + 1, j, s * 2.0 * dudx_e / G.dx);
+  add_face_mean(a, G, true, i, j, -s * 2.0 * dudx_w / G.dx);
+  add_corner_mean(a, i, j + 1, s * (dudy_n + dvdx_n) / G.dy);
+  add_corner_mean(a, i, j, -s * (dudy_s + dvdx_s) / G.dy);
+}
+__device__ __forceinline__ void visc_v_eta_adj(const Fv &x, const Fv &y, const Fv &a, const Grid &G, int i, int j,
+                                               double s) {
+  // x: u, y: v
+  const double dvdx_e = (y.at(i + 1, j) - y.at(i, j)) / G.dx, dvdx_w = (y.at(i, j) - y.at(i - 1, j)) / G.dx;
+  const double dvdy_n = (y.at(i, j + 1) - y.at(i, j)) / G.dy, dvdy_s = (y.at(i, j) - y.at(i, j - 1)) / G.dy;
+  const double dudy_e = (x.at(i + 1, j) - x.at(i + 1, j - 1)) / G.dy, dudy_w = (x.at(i, j) - x.at(i, j - 1)) / G.dy;
+  add_corner_mean(a, i + 1, j, s * (dvdx_e + dudy_e) / G.dx);
+  add_corner_mean(a, i, j, -s * (dvdx_w + dudy_w) / G.dx);
+  add_face_mean(a, G, false, i, j + 1, s * 2.0 * dvdy_n / G.dy);
+  add_face_mean(a, G, false, i, j, -s * 2.0 * dvdy_s / G.dy);
+}
+__global__ void k_mom_material_adj(MomLayout L, Fv us, Fv vs, Fv u, Fv v, Fv hup, Fv hvp, Fv lu, Fv lv, Fv arho,
+                                   Fv aeta, Fv aetap, Grid G, int step, double dt, double alpha, double bfx,
+                                   double bfy) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L.n()) return;
+  if (t < L.nu) {
+    const int i = (int)(t / L.ny), j = (int)(t % L.ny);
+    const double w = lu.at(i, j);
+    if (w == 0.0) return;
+    const double h = mom_flux_u_at(u, v, G, i, j);
+    const double conv = (step == 0) ? h : 1.5 * h - 0.5 * hup.at(i, j);
+    add_face_mean(arho, G, true, i, j, -w * (us.at(i, j) - u.at(i, j) + dt * conv - dt * bfx));
+    visc_u_eta_adj(us, vs, aeta, G, i, j, alpha * w);
+    visc_u_eta_adj(u, v, aetap, G, i, j, alpha * w);
+  } else {
+    const long long q = t - L.nu;
+    const int i = (int)(q / (L.ny + 1)), j = (int)(q % (L.ny + 1));
+    const double w = lv.at(i, j);
+    if (w == 0.0) return;
+    const double h = mom_flux_v_at(u, v, G, i, j);
+    const double conv = (step == 0) ? h : 1.5 * h - 0.5 * hvp.at(i, j);
+    add_face_mean(arho, G, false, i, j, -w * (vs.at(i, j) - v.at(i, j) + dt * conv - dt * bfy));
+    visc_v_eta_adj(us, vs, aeta, G, i, j, alpha * w);
+    visc_v_eta_adj(u, v, aetap, G, i, j, alpha * w);
   }
 }
 
@@ -259,6 +345,128 @@ __global__ void k_adj_ghosts(Fv f, Grid G, int kind, BCSide L, BCSide R, BCSide 
   const double gv = f.at(i, j);
   if (gv != 0.0) atomicAdd(&f.at(si, sj), coef * gv);
   f.at(i, j) = 0.0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Adjoint of the face surface forces (update_surface_tension_force, phase_field.cpp:179-226, no smoothing):
+// c_mid = (c_old + c_new) / 2 (scalar BC ghosts), mu_mid = chem(c_mid), f_u = scale mf (c_mid(i) - c_mid(i-1)) / dx
+// with mf the face mean of mu_mid (0.5 (mu(nx-1) + mu(0)) on faces 0 and nx), f_v likewise; the forces'
+// face BCs are folded by the caller.  Cotangents are accumulated with atomics into cmb (c_mid, ghosted) and
+// mmb (mu_mid, interior).
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_sf_adj_faces(Fv gfu, Fv gfv, Fv cm, Fv mm, Fv cmb, Fv mmb, Grid G, double scale) {
+  const long long nu = (long long)(G.nx + 1) * G.ny, nv = (long long)G.nx * (G.ny + 1);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nu) {
+    const int i = (int)(t / G.ny), j = (int)(t % G.ny);
+    const double g = gfu.at(i, j);
+    if (g == 0.0) return;
+    const bool edge = i <= 0 || i >= G.nx;
+    const int ia = edge ? G.nx - 1 : i - 1, ib = edge ? 0 : i;
+    const double mf = 0.5 * (mm.at(ia, j) + mm.at(ib, j));
+    const double gr = (cm.at(i, j) - cm.at(i - 1, j)) / G.dx;
+    atomicAdd(&mmb.at(ia, j), 0.5 * scale * gr * g);
+    atomicAdd(&mmb.at(ib, j), 0.5 * scale * gr * g);
+    atomicAdd(&cmb.at(i, j), scale * mf * g / G.dx);
+    atomicAdd(&cmb.at(i - 1, j), -scale * mf * g / G.dx);
+  } else if (t < nu + nv) {
+    const long long q = t - nu;
+    const int i = (int)(q / (G.ny + 1)), j = (int)(q % (G.ny + 1));
+    const double g = gfv.at(i, j);
+    if (g == 0.0) return;
+    const bool edge = j <= 0 || j >= G.ny;
+    const int ja = edge ? G.ny - 1 : j - 1, jb = edge ? 0 : j;
+    const double mf = 0.5 * (mm.at(i, ja) + mm.at(i, jb));
+    const double gr = (cm.at(i, j) - cm.at(i, j - 1)) / G.dy;
+    atomicAdd(&mmb.at(i, ja), 0.5 * scale * gr * g);
+    atomicAdd(&mmb.at(i, jb), 0.5 * scale * gr * g);
+    atomicAdd(&cmb.at(i, j), scale * mf * g / G.dy);
+    atomicAdd(&cmb.at(i, j - 1), -scale * mf * g / G.dy);
+  }
+}
+// chem (k_chem: mu = alpha (dw(c) / cn - cn lap c), dw = c (1 - c) (1 - 2 c) / 2) transposed at cell (i, j)
+__global__ void k_chem_adj(Fv cm, Fv mmb, Fv cmb, Grid G, double cn) {
+  DN_FOR_INTERIOR(cm);
+  const double g = mmb.at(i, j);
+  if (g == 0.0) return;
+  const double alpha = 6.0 * 1.4142135623730950488;
+  const double c = cm.at(i, j);
+  const double dwp = 0.5 * (1.0 - 6.0 * c + 6.0 * c * c);
+  const double a = alpha * g, l = -a * cn;
+  const double cx = 1.0 / (G.dx * G.dx), cy = 1.0 / (G.dy * G.dy);
+  atomicAdd(&cmb.at(i, j), a * dwp / cn - 2.0 * l * (cx + cy));
+  atomicAdd(&cmb.at(i + 1, j), l * cx);
+  atomicAdd(&cmb.at(i - 1, j), l * cx);
+  atomicAdd(&cmb.at(i, j + 1), l * cy);
+  atomicAdd(&cmb.at(i, j - 1), l * cy);
+}
+// ---------------------------------------------------------------------------------------------------
+// rho_mid cotangent of the projection (build_pressure_linear_system, pressure.cpp:123-196; the split
+// explicit divergence, operators.cpp:424-444; the correction, operators.cpp:490-516), one thread per face,
+// given the folded face cotangents (fu, fv) of the corrected velocities, rbar = A^-T (cotangent of p_corr)
+// (compact, projected), the forward's p_corr (pc) and extrapolated pressure (pe), both with pressure-BC
+// ghosts.  Per face with density rf = xface / yface(rho_mid):
+//   correction u -= dt (a dx(pc) + b dx(pe)), a = 1/rf (variable) or 1/rho_ref, b = 1/rf - 1/rho_ref (split)
+//       -> rf_bar += f_bar dt / rf^2 dx(pc or pe);
+//   split rhs  -= div(w dx(pe)), w = 1 - rho_ref / rf   -> rf_bar += F_bar dx(pe) rho_ref / rf^2;
+//   variable operator coefficient c = 1 / (rf h^2): open face  c_bar = -(rbar_a - rbar_b)(pc_a - pc_b);
+//       Dirichlet side c_bar = rbar_r (2 value - 2 pc_r); Neumann side c_bar = rbar_r value h
+//       -> rf_bar += c_bar (-1 / (rf^2 h^2)).
+// The face means are transposed onto rho_mid's cells (add_face_mean).  A periodic face shared by the last and
+// the first cell is counted once for the operator (face 0) and once per side for the split flux.
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_proj_rho_adj(Fv fu, Fv fv, const double *rbar, Fv pc, Fv pe, Fv rm, Fv arho, Grid G, BCSet bc,
+                               int split, double rho_ref, double dt) {
+  const long long nu = (long long)(G.nx + 1) * G.ny, nv = (long long)G.nx * (G.ny + 1);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nu + nv) return;
+  const bool xd = t < nu;
+  int i, j;
+  if (xd) {
+    i = (int)(t / G.ny);
+    j = (int)(t % G.ny);
+  } else {
+    const long long q = t - nu;
+    i = (int)(q / (G.ny + 1));
+    j = (int)(q % (G.ny + 1));
+  }
+  const int n = xd ? G.nx : G.ny, k = xd ? i : j, per = xd ? G.px : G.py;
+  const double h = xd ? G.dx : G.dy;
+  const double rf = xd ? xface(rm, G, i, j) : yface(rm, G, i, j);
+  const double dpc = xd ? gfx(pc, G, i, j) : gfy(pc, G, i, j);
+  const double dpe = split ? (xd ? gfx(pe, G, i, j) : gfy(pe, G, i, j)) : 0.0;
+  const double fb = xd ? fu.at(i, j) : fv.at(i, j);
+  double bar = fb * dt / (rf * rf) * (split ? dpe : dpc);
+  auto rb = [&](int kk) { return rbar[xd ? (long long)kk * G.ny + j : (long long)i * G.ny + kk]; };
+  const bool open = per || (k > 0 && k < n);
+  if (split) {
+    if (open) {
+      const double e = k < n ? rb(k) : 0.0, w = k > 0 ? rb(k - 1) : 0.0;
+      bar += (e - w) / h * dpe * rho_ref / (rf * rf);
+    }
+  } else {
+    double cbar = 0.0;
+    if (open) {
+      if (!(per && k == n)) {
+        const int a = k > 0 ? k - 1 : n - 1, b = k < n ? k : 0;
+        const double pa = xd ? pc.at(a, j) : pc.at(i, a), pb = xd ? pc.at(b, j) : pc.at(i, b);
+        cbar = -(rb(a) - rb(b)) * (pa - pb);
+      }
+    } else {
+      const int r = k <= 0 ? 0 : n - 1;
+      const BCSide &side = bc.p[xd ? (k <= 0 ? DN_LEFT : DN_RIGHT) : (k <= 0 ? DN_BOTTOM : DN_TOP)];
+      const double pr = xd ? pc.at(r, j) : pc.at(i, r);
+      cbar = (side.type == DN_BC_DIRICHLET) ? rb(r) * (2.0 * side.value - 2.0 * pr) : rb(r) * side.value * h;
+    }
+    bar += cbar * (-1.0 / (rf * rf * h * h));
+  }
+  if (bar != 0.0) add_face_mean(arho, G, xd, i, j, bar);
+}
+
+// out = in / 2 at the interior cells
+__global__ void k_half_interior(Fv in, Fv out) {
+  DN_FOR_INTERIOR(out);
+  out.at(i, j) = 0.5 * in.at(i, j);
 }
 
 }  // namespace dn

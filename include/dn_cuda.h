@@ -242,21 +242,44 @@ dn_status dn_projection(dn_handle *h, int step, const double *u_star, const doub
 dn_status dn_projection_adjoint(dn_handle *h, int step, const double *gu, const double *gv, const double *gp,
                                 const double *gpp, double *au, double *av, double *ap, double *app,
                                 int *iterations, double *relative_residual);
+/* dn_projection with rho_mid as an input (its scalar BC applied), and the vector-Jacobian product with the
+ * cotangent of rho_mid as well (the forward's p, p_prev and p_new in; arho out).  No counterpart in the
+ * reference.  DEVICE buffers. */
+dn_status dn_projection_rho(dn_handle *h, int step, const double *u_star, const double *v_star, const double *p,
+                            const double *p_prev, const double *rho_mid, double *u, double *v, double *p_new,
+                            double *p_prev_new, int *iterations, double *relative_residual);
+dn_status dn_projection_rho_adjoint(dn_handle *h, int step, const double *rho_mid, const double *p,
+                                    const double *p_prev, const double *p_new, const double *gu, const double *gv,
+                                    const double *gp, const double *gpp, double *au, double *av, double *ap,
+                                    double *app, double *arho, int *iterations, double *relative_residual);
 /* The momentum predictor as a map (compute_momentum_fluxes + solve_momentum_predictor, momentum.cpp:55-85,
- * 157-502): u, v (their BCs applied), H_prev (hu_prev, hv_prev) and the face surface forces (fxu, fyv) in;
- * u_star, v_star out, with the handle's rho_mid, eta and eta_prev.  DEVICE Field2D buffers; uses the
- * handle's fields as work space. */
+ * 157-502): u, v (their BCs applied), H_prev (hu_prev, hv_prev), the face surface forces (fxu, fyv) and the
+ * materials rho_mid, eta, eta_prev (scalar BCs applied) in; u_star, v_star and this step's convection H
+ * (hu, hv: the next step's H_prev) out.  DEVICE Field2D buffers; uses the handle's fields as work space. */
 dn_status dn_momentum_map(dn_handle *h, int step, const double *u, const double *v, const double *hu_prev,
-                          const double *hv_prev, const double *fxu, const double *fyv, double *u_star, double *v_star,
-                          int *iterations, double *residual);
-/* No counterpart in the reference.  Vector-Jacobian product of dn_momentum_map at (u, v), rho_mid, eta and
- * eta_prev held fixed: cotangents of the interior values of u_star, v_star in; cotangents of the interior
- * values of u, v, hu_prev, hv_prev, fxu, fyv out (ghosts 0).  The transposed coupled system M^T is solved by
+                          const double *hv_prev, const double *fxu, const double *fyv, const double *rho_mid,
+                          const double *eta, const double *eta_prev, double *u_star, double *v_star, double *hu,
+                          double *hv, int *iterations, double *residual);
+/* No counterpart in the reference.  Vector-Jacobian product of dn_momentum_map at its forward point (the same
+ * u, v, hu_prev, hv_prev, rho_mid, eta, eta_prev, and the forward's u_star, v_star): cotangents of the
+ * interior values of u_star, v_star, hu, hv in; cotangents of the interior values of u, v, hu_prev,
+ * hv_prev, fxu, fyv, rho_mid, eta, eta_prev out (ghosts 0).  The transposed coupled system M^T is solved by
  * the same Jacobi-BiCGSTAB to a relative residual of 1e-14; its iterations and relative residual are
  * reported.  DEVICE buffers. */
-dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const double *v, const double *gu_star,
-                              const double *gv_star, double *au, double *av, double *ahu, double *ahv, double *afu,
-                              double *afv, int *iterations, double *residual);
+dn_status dn_momentum_adjoint(dn_handle *h, int step, const double *u, const double *v, const double *hu_prev,
+                              const double *hv_prev, const double *rho_mid, const double *eta, const double *eta_prev,
+                              const double *u_star, const double *v_star, const double *gu_star,
+                              const double *gv_star, const double *ghu, const double *ghv, double *au, double *av,
+                              double *ahu, double *ahv, double *afu, double *afv, double *arho, double *aeta,
+                              double *aeta_prev, int *iterations, double *residual);
+/* The face surface forces as a map (update_surface_tension_force, phase_field.cpp:179-256): c_old, c_new
+ * (scalar BCs applied) in; fxu, fyv out (face BCs and smoothing passes applied).  DEVICE buffers. */
+dn_status dn_surface_force_map(dn_handle *h, const double *c_old, const double *c_new, double *fxu, double *fyv);
+/* No counterpart in the reference.  Vector-Jacobian product of dn_surface_force_map at (c_old, c_new):
+ * cotangents of the interior face forces in; cotangents of the interior values of c_old and c_new out.
+ * DN_ERR_UNSUPPORTED with smoothing passes.  DEVICE buffers. */
+dn_status dn_surface_force_adjoint(dn_handle *h, const double *c_old, const double *c_new, const double *gfxu,
+                                   const double *gfyv, double *ac_old, double *ac_new);
 
 /* The CH advective term -div(u c) with WENO5 face values, as build_phase_advection_fluxes
  * (phase_field.cpp:283-311) computes it, on caller DEVICE buffers: c (cell field), u, v (face fields) in,

@@ -1,8 +1,9 @@
 """The momentum predictor's hand-written adjoint (dn_momentum_adjoint) against central finite differences.
 
-The map (u, v, H_prev, f) -> (u*, v*) of the momentum predictor at fixed materials is quadratic in (u, v)
-(centred convection) and linear in H_prev and f, so central differences are exact up to the forward
-solve's tolerance, which these cases set to 1e-14 (absolute).  For random directions d and cotangents w,
+The map (u, v, H_prev, f, rho_mid, eta, eta_prev) -> (u*, v*, H) of the momentum predictor is quadratic in
+(u, v) (centred convection) and linear in H_prev and f, so central differences in those are exact up to the
+forward solve's tolerance (1e-14 absolute here); in the materials (which enter the solved operator) the
+O(eps^2) term is below the bar at eps = 1e-4 with perturbations of relative size 1e-4.  For random directions d and cotangents w,
 <w, J d> by central differences must equal <J^T w, d> from the adjoint to 1e-6 relative, on walls with
 Dirichlet and Neumann velocity sides, a periodic-x shear channel and a doubly periodic box, on step 0 (the
 convection term alone) and step 1 (AB2 with H_prev).  The composition with the projection
@@ -45,7 +46,7 @@ def _setup(dn, name):
     t = lambda a: torch.tensor(np.ascontiguousarray(a[g:a.shape[0] - g, g:a.shape[1] - g]), dtype=torch.float64,
                                device="cuda")
     rng = np.random.default_rng(5)
-    state = {n: t(gpu.get_field(n)) for n in ("u", "v")}
+    state = {n: t(gpu.get_field(n)) for n in ("u", "v", "rho_mid", "eta", "eta_prev")}
     for n, like in (("hu_prev", "u"), ("hv_prev", "v"), ("fxu", "u"), ("fyv", "v")):
         state[n] = torch.tensor(0.3 * rng.standard_normal(tuple(state[like].shape)), device="cuda")
     return cfg, gpu, state, rng
@@ -55,7 +56,8 @@ def _dirs(state, rng):
     return {n: torch.tensor(rng.standard_normal(tuple(a.shape)), device="cuda") for n, a in state.items()}
 
 
-ORDER = ("u", "v", "hu_prev", "hv_prev", "fxu", "fyv")
+ORDER = ("u", "v", "hu_prev", "hv_prev", "fxu", "fyv", "rho_mid", "eta", "eta_prev")
+VEL = ORDER[:6]
 
 
 @pytest.mark.parametrize("step", [0, 1])
@@ -64,11 +66,12 @@ def test_momentum_adjoint_matches_central_differences(dn, name, step):
     from ding_nsch_core_solver_b200 import autograd as ag
 
     cfg, gpu, state, rng = _setup(dn, name)
-    w = {n: torch.tensor(rng.standard_normal(tuple(state[k].shape)), device="cuda") for n, k in (("u", "u"), ("v", "v"))}
+    w = {n: torch.tensor(rng.standard_normal(tuple(state[k].shape)), device="cuda")
+         for n, k in (("u", "u"), ("v", "v"), ("hu", "u"), ("hv", "v"))}
 
     def loss(st):
-        us, vs = ag.momentum_predictor(gpu, step, *(st[n] for n in ORDER))
-        return (w["u"] * us).sum() + (w["v"] * vs).sum()
+        us, vs, hu, hv = ag.momentum_predictor(gpu, step, *(st[n] for n in ORDER))
+        return (w["u"] * us).sum() + (w["v"] * vs).sum() + (w["hu"] * hu).sum() + (w["hv"] * hv).sum()
 
     x = {n: a.clone().requires_grad_(True) for n, a in state.items()}
     grads = torch.autograd.grad(loss(x), [x[n] for n in ORDER])
@@ -105,14 +108,14 @@ def test_velocity_step_and_sigma_gradient(dn, name):
     x = {n: a.clone().requires_grad_(True) for n, a in state.items()}
     sigma = torch.tensor(1.3, dtype=torch.float64, device="cuda", requires_grad=True)
     out = loss(x, sigma)
-    grads = torch.autograd.grad(out, [x[n] for n in ORDER] + [sigma])
+    grads = torch.autograd.grad(out, [x[n] for n in VEL] + [sigma])
     d = _dirs(state, rng)
-    adj = sum(float((gr * d[n]).sum()) for gr, n in zip(grads[:-1], ORDER))
+    adj = sum(float((gr * d[n]).sum()) for gr, n in zip(grads[:-1], VEL))
     eps = 1e-4
     with torch.no_grad():
         s0 = torch.tensor(1.3, dtype=torch.float64, device="cuda")
-        fd = (float(loss({n: state[n] + eps * d[n] for n in ORDER}, s0)) -
-              float(loss({n: state[n] - eps * d[n] for n in ORDER}, s0))) / (2 * eps)
+        fd = (float(loss({n: state[n] + eps * d[n] for n in VEL}, s0)) -
+              float(loss({n: state[n] - eps * d[n] for n in VEL}, s0))) / (2 * eps)
         fd_s = (float(loss(state, s0 + eps)) - float(loss(state, s0 - eps))) / (2 * eps)
     print(name, f"state fd {fd:.12e} adjoint {adj:.12e}; sigma fd {fd_s:.12e} adjoint {float(grads[-1]):.12e}")
     assert abs(fd - adj) <= 1e-6 * max(abs(fd), 1e-3), (fd, adj)
