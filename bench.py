@@ -312,12 +312,15 @@ def run_ours(args):
             msolver.set_field(n, a)
         msolver.refresh_derived()
         msolver.set_initial_mass(msolver.compute_mass("c"))
+        if args.step_graph:  # from the second step of index >= 1 on, each step is one graph launch
+            msolver.set_step_graph(True)
         mstream = torch.cuda.ExternalStream(msolver.stream(), device=device)
         mstep = 0
         for _ in range(step - args.steps * 2):  # as many untimed steps as the plain run took
             msolver.step(mstep)
             mstep += 1
         mtimes, mreps, mphases = [], [], []
+        mlaunch0 = msolver.kernel_launches()
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -337,8 +340,11 @@ def run_ours(args):
             got = msolver.get_field(n)[g:-g, g:-g]
             ref = ref[g:-g, g:-g]
             errs[n] = float(np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-300))
+        mlaunches = msolver.kernel_launches() - mlaunch0
         mtotal = reduce_max(dist, sum(mtimes))
         mvalue = n_cells * args.steps * world / (mtotal * 1e-3) / 1e6
+        phase_keys = ("ch", "momentum", "pressure", "correction") + (
+            () if args.step_graph else ("pressure_inner_solves", "ch_inner_solves", "bicgstab_kernel"))
         mixed = {"value": round(mvalue, 4), "unit": "Mcell-steps/s", "ms_per_step": round(mtotal / args.steps, 4),
                  "vs_plain": round(mvalue / value, 4),
                  "pressure_iterations_mean": statistics.mean(r["pressure_iterations"] for r in mreps),
@@ -349,9 +355,11 @@ def run_ours(args):
                  # the plain FP64 step is the oracle's to rel-L2 <= 1e-10 (tests/test_gpu_configs.py)
                  "rel_l2_vs_plain_fp64": {k: float(f"{v:.3e}") for k, v in errs.items()},
                  "ch_iterations_mean": statistics.mean(r["ch_iterations"] for r in mreps),
-                 "phase_ms_mean": {k: round(statistics.mean(p[i] for p in mphases), 4) for i, k in enumerate(
-                     ("ch", "momentum", "pressure", "correction", "pressure_inner_solves", "ch_inner_solves",
-                      "bicgstab_kernel"))},
+                 # with captured steps the phases are timed by the graph's event nodes
+                 "phase_ms_mean": {k: round(statistics.mean(p[i] for p in mphases), 4)
+                                   for i, k in enumerate(phase_keys)},
+                 "step_graph": bool(args.step_graph),
+                 "gpu_launches": mlaunches,
                  "ch_solver": ("FP32 CG, (K + s I)^-2 V-cycles, FP64 defect correction"
                                if all(r["ch_preconditioner"] == 3 for r in mreps) else "FP64 ILDLT-PCG"),
                  "compared_after_steps": mstep}
@@ -371,6 +379,8 @@ def run_ours(args):
                 s.set_field(n, a)
             s.refresh_derived()
             s.set_initial_mass(s.compute_mass("c"))
+            if args.step_graph:
+                s.set_step_graph(True)
             members.append(s)
         bstep = 0
         for _ in range(args.warmup):
@@ -394,7 +404,9 @@ def run_ours(args):
         batched = {"instances": len(members), "value": round(bvalue, 4), "unit": "Mcell-steps/s",
                    "ms_per_batch_step": round(btotal / args.steps, 4), "vs_single": round(bvalue / value, 4),
                    "gpu_launches": blaunches,
-                   "entry_point": "dn_step_batch (one stream and host worker per instance)"}
+                   "entry_point": ("dn_step_batch: one CUDA graph launch per batch step, every instance's "
+                                   "step a branch of it" if args.step_graph and args.warmup >= 2 else
+                                   "dn_step_batch (one stream and host worker per instance)")}
         for s in members:
             s.close()
 
@@ -409,7 +421,8 @@ def run_ours(args):
         cells = sum(c["nx"] * c["ny"] for c in cfgs)
         shard, err, etimes, ereps = None, "", [], []
         try:
-            shard = ShardedEnsemble(cfgs, rank, world, device, proportional=not args.ensemble_equal)
+            shard = ShardedEnsemble(cfgs, rank, world, device, proportional=not args.ensemble_equal,
+                                    step_graph=args.step_graph)
             shard.initialize()
             estep = 0
             for _ in range(args.warmup):
@@ -457,7 +470,8 @@ def run_ours(args):
                         "workload": "uneven droplets: grids {64..256}^2, periodic both ways, split_icpcg, mixed, "
                                     "Pe = 1/Cn, each instance at half its tightest step limit (capillary, explicit "
                                     "CH, advective), seed 4; whole instances sharded over the ranks by LPT on cells x "
-                                    "max(nx, ny), each rank's share stepped together by dn_step_batch",
+                                    "max(nx, ny), each rank's share stepped together by dn_step_batch" +
+                                    (" as one CUDA graph launch per batch step" if args.step_graph else ""),
                         "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                         "sm_share": "equal (1/instances)" if args.ensemble_equal else "in proportion to cells"}
         if shard is not None:
@@ -573,6 +587,8 @@ def main():
                     help="keep the default launch shape instead of picking the pressure PCG's with "
                          "dn_autotune_pressure before the timed steps")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
+    ap.add_argument("--no-step-graph", dest="step_graph", action="store_false",
+                    help="step the mixed, batched and ensemble arms eagerly instead of replaying captured steps")
     ap.add_argument("--batch", type=int, default=8, help="instances of the batched-ensemble arm (0 skips it)")
     ap.add_argument("--ensemble", type=int, default=64, help="uneven droplet instances of the ensemble arm (0 skips)")
     ap.add_argument("--ensemble-equal", action="store_true",

@@ -131,6 +131,7 @@ def load():
         "dn_set_pressure_monitor": (I, [H, I]),
         "dn_pressure_monitor": (I, [H, DP, I, C.POINTER(C.c_int)]),
         "dn_autotune_pressure": (I, [H, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+        "dn_set_step_graph": (I, [H, I]),
         "dn_pressure_analysis": (I, [H, I, C.c_char_p]),
         "dn_history_csv_header": (C.c_size_t, [C.c_char_p, C.c_size_t]),
         "dn_history_csv_row": (I, [H, I, D, C.POINTER(Report), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -311,6 +312,11 @@ class Solver:
         """Solver::run_pressure_analysis_from_snapshot on the current state (step index `step`): the analysis
         files under output_dir/name/pressure_analysis/."""
         self._check(self._lib.dn_pressure_analysis(self._h, int(step), source_mode.encode()))
+
+    def set_step_graph(self, enable: bool = True) -> None:
+        """Replay captured steps (dn_set_step_graph): from the second eager step of index >= 1 on, each step
+        is one CUDA graph launch whose solves loop on the device; results equal the eager steps'."""
+        self._check(self._lib.dn_set_step_graph(self._h, 1 if enable else 0))
 
     def autotune_pressure(self) -> dict:
         """Time the pressure solve of the current state over the launch shapes (rows per CTA x sweep warps

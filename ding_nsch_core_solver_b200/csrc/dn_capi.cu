@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <functional>
 #include <mutex>
 #include <set>
 #include <string>
@@ -36,6 +37,8 @@ namespace {
 
 constexpr double kSqrt2 = 1.4142135623730950488;
 constexpr int kHostScal = 8192;  // pinned host scratch (doubles): scalars and reduction partials
+constexpr int kCapDepth = 4;     // conditional graph nodes nested at most this deep
+constexpr int kDiagParts = 128;  // CTAs of the diagnostics reduction
 // Sweep warps per CTA: one per SM sub-partition (scheduler).  A fifth warp shares a scheduler with the
 // first and slows both; fewer warps per CTA put more hand-overs across CTAs (measured 81.9 ms per pressure
 // solve with 4, 87.8 with 5, 92.6 with 1 on the 192 x 384 bench workload).
@@ -161,14 +164,6 @@ __global__ void k_finish3(const double *partials, int nparts, double *out) {
     out[2] = s2;
   }
 }
-// right-hand side of an inner solve: the projected FP64 residual rounded to FP32; the correction starts at 0
-__global__ void k_inner_rhs(const double *r, double mean, float *rf, float *ef, long long n) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) {
-    rf[t] = (float)(r[t] - mean);
-    ef[t] = 0.0f;
-  }
-}
 __global__ void k_add_correction(double *x, const float *e, long long n) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) x[t] += (double)e[t];
@@ -189,6 +184,117 @@ __global__ void k_add_correction_norms(double *x, const float *e, long long n, d
     partials[3 * blockIdx.x + 1] = v[1];
     partials[3 * blockIdx.x + 2] = 0.0;
   }
+}
+
+// ---- the defect-correction loop's decisions on the device (the record layout is DcSlot)
+constexpr int kDcMaxCycles = 40;  // outer cycles of one mixed-precision solve at most
+constexpr int kRecPressure = 0;   // offsets of the records in h->rec
+constexpr int kRecCh = 16;
+constexpr int kRecCount = 64;
+
+struct DcParams {
+  double tol;          // the reference's stopping tolerance, on the relative or the absolute FP64 residual
+  double n;            // cells (the projected norms of a singular system)
+  int max_it;          // inner iterations of the whole solve at most
+  int max_cycles;      // outer cycles at most
+  int project;         // singular pressure system: the residual is projected (its mean removed)
+  int ch;              // CH rules: multigrid inner solves only, a cycle that does not reduce the residual ends
+  const int *mg_flag;  // the coarsest level's inverse status of the inner hierarchy (0: usable); null: none
+};
+
+// max with std::max's semantics (a NaN first argument is kept, so a non-finite residual never reads as
+// converged)
+__device__ __forceinline__ double smax(double a, double b) { return a < b ? b : a; }
+
+// right-hand side of an inner solve: the FP64 residual less its mean (R[kDcMean]) rounded to FP32; the
+// correction starts at 0
+__global__ void k_inner_rhs_dev(const double *r, const double *R, float *rf, float *ef, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double mean = R[kDcMean];
+  if (t < n) {
+    rf[t] = (float)(r[t] - mean);
+    ef[t] = 0.0f;
+  }
+}
+
+// The check after each FP64 residual (sums = r, r^2, b^2 from k_outer_residual / k_finish3): the stopping
+// rule of the reference (rel < tol or abs < tol), the cycle and iteration budgets, and the stall rule (a
+// multigrid cycle that did not reduce the residual hands the pressure solve to the IC inner solver; any
+// other stalled cycle ends the solve).  Sets the outer while node's condition.
+__global__ void k_dc_decide(const double *sums, double *R, DcParams P, cudaGraphConditionalHandle loop) {
+  if (threadIdx.x != 0) return;
+  if (R[kDcStarted] == 0.0) {
+    R[kDcStarted] = 1.0;
+    R[kDcPrev] = INFINITY;
+    R[kDcUseMg] = (P.mg_flag != nullptr && *P.mg_flag == 0) ? 1.0 : 0.0;
+    R[kDcUsedMg0] = R[kDcUseMg];
+  }
+  bool more = true;
+  if (R[kDcErr] != 0.0 || R[kDcIcZero] != 0.0) {
+    more = false;  // a failed inner solve, or an IC inner solve that could not move (x unchanged)
+  } else {
+    const double s0 = sums[0], s1 = sums[1], s2 = sums[2];
+    const double mean = P.project ? s0 / P.n : 0.0;
+    const double rn2 = P.project ? smax(s1 - s0 * s0 / P.n, 0.0) : (P.ch ? smax(s1, 0.0) : s1);
+    const double absr = sqrt(rn2);
+    const double relr = absr / smax(sqrt(smax(s2, 0.0)), 1.0e-30);
+    R[kDcAbs] = absr;
+    R[kDcRel] = relr;
+    R[kDcMean] = mean;
+    if (relr < P.tol || absr < P.tol) {
+      more = false;
+    } else if (R[kDcCycles] >= (double)P.max_cycles || R[kDcTotal] >= (double)P.max_it) {
+      more = false;
+    } else if (!(absr < R[kDcPrev])) {
+      if (P.ch || R[kDcUseMg] == 0.0) more = false;
+      else R[kDcUseMg] = 0.0;
+    }
+    if (more) R[kDcPrev] = absr;
+  }
+  cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
+
+// the inner solver of this cycle: multigrid CG (has_mg: the graph holds that branch) or the IC persistent PCG
+__global__ void k_dc_branch(const double *R, int has_mg, cudaGraphConditionalHandle mg,
+                            cudaGraphConditionalHandle ic) {
+  if (threadIdx.x != 0) return;
+  const bool use_mg = R[kDcUseMg] != 0.0;
+  if (has_mg) cudaGraphSetConditional(mg, use_mg ? 1u : 0u);
+  cudaGraphSetConditional(ic, use_mg ? 0u : 1u);
+}
+
+// end of a cycle: counted; with the CH's norms (|e|^2, |x|^2 after the update) the iterate residual
+__global__ void k_dc_cycle_end(const double *norms, double *R) {
+  if (threadIdx.x != 0) return;
+  R[kDcCycles] += 1.0;
+  if (norms) R[kDcIres] = sqrt(smax(norms[0], 0.0) / smax(norms[1], 1.0e-30));
+}
+
+// the IC inner solver's factor is made once per solve: `make` on its first use, `go` once it exists
+__global__ void k_ic_need(const double *R, cudaGraphConditionalHandle make, cudaGraphConditionalHandle go) {
+  if (threadIdx.x != 0) return;
+  const bool ready = R[kDcIcReady] != 0.0;
+  cudaGraphSetConditional(make, ready ? 0u : 1u);
+  cudaGraphSetConditional(go, ready ? 1u : 0u);
+}
+// after the factor: a failed one is recorded (and the inner solve skipped), else it is ready
+__global__ void k_ic_gate(const int *status, double *R, cudaGraphConditionalHandle go) {
+  if (threadIdx.x != 0) return;
+  const bool failed = *status == kDevFactorFailed;
+  if (failed) R[kDcErr] = (double)kDevFactorFailed;
+  else R[kDcIcReady] = 1.0;
+  cudaGraphSetConditional(go, failed ? 0u : 1u);
+}
+// after the IC inner solve (its out[0] = iterations, status): iterations counted, a failure recorded
+__global__ void k_ic_done(const double *out, const int *status, double *R) {
+  if (threadIdx.x != 0) return;
+  if (*status != kDevOk) {
+    R[kDcErr] = (double)*status;
+    return;
+  }
+  R[kDcTotal] += out[0];
+  R[kDcIcCycles] += 1.0;
+  if (out[0] == 0.0) R[kDcIcZero] = 1.0;
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -405,6 +511,13 @@ struct MgHier {
   int levels() const { return (int)lv.size(); }
 };
 
+// Kernel launches recorded per region of a solve graph, so that a replay can count the launches it ran:
+// once, per outer cycle, per multigrid inner iteration, per IC inner solve.
+struct DcNodes {
+  long long fixed = 0, cycle = 0, iter = 0, ic = 0;
+  long long make = 0;  // the IC inner solver's factor branch, run once in a solve that uses it
+};
+
 struct dn_handle {
   dn_config cfg;
   int device = 0;
@@ -494,13 +607,45 @@ struct dn_handle {
     long long nodes;
   };
   std::vector<MgGraph> mg_graphs;
+  // graph capture: side streams for conditional node bodies, nested up to kCapDepth deep; `capturing` while
+  // the handle's work is being recorded into a graph (no read-backs then: results go to `rec`)
+  cudaStream_t cap_streams[kCapDepth] = {};
+  int cap_depth = 0;
+  bool capturing = false;
+  double *rec = nullptr;  // device records of the recorded solves and steps (kRecCount doubles)
+  long long graph_epoch = 0;  // bumped when a launch shape changes: recorded graphs are made again
+  // the eager mixed solves, each captured once with its loops on the device: [0] pressure, [1] CH
+  struct SolveGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long epoch = -1;
+    DcNodes nodes;
+  };
+  SolveGraph dc_graph[2];
+  bool ch_mg_ok = false;  // the (K + s I) hierarchy built for ch_mg_alpha0 is usable
+  // captured steps (dn_set_step_graph): the step recorded once into a graph and replayed
+  bool graph_steps = false;  // replay captured steps where the step allows it
+  bool steady = false;       // an eager step with step >= 1 has made every operator, factor and hierarchy
+  cudaGraphExec_t step_exec = nullptr;
+  long long step_epoch = -1;
+  dn_report step_rep{};      // the report fields fixed at capture (preconditioner kinds)
+  long long step_nodes = 0;  // kernel launches of one replay outside the mixed solves' loops
+  DcNodes step_dcn[2];       // the mixed solves' loops: [0] pressure, [1] CH
+  long long step_retry = 0;  // kernel launches of the CH solve's retry branch (run after a breakdown only)
+  cudaEvent_t cap_ev = nullptr;  // joins this handle's branch of a batch capture
+  long long uid = 0;             // unique among the process's handles (a batch graph names its handles by it)
+  // the batch graph this handle leads (dn_step_batch with it first): every handle's step in one graph
+  struct BatchGraph {
+    std::vector<long long> uids, epochs;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+  } batch;
   // mixed CH solve: FP32 13-point operator and CG vectors; the alpha0 its operator and hierarchy were built for
   float *fa13 = nullptr, *cx32 = nullptr, *cr32 = nullptr, *cz32 = nullptr, *cp32 = nullptr, *cq32 = nullptr,
         *ct32 = nullptr, *cb32 = nullptr;
   double ch_mg_alpha0 = -1.0;
   bool ch_mg = false;  // the CH solve runs the mixed form (FP64 defect correction around the FP32 inner CG)
-  bool ic32_ready = false;  // FP32 copies of the IC/ILDLT factor made for this solve
-  bool mgp_split_ready = false, mgp_usable = false;  // the split operator's FP32 copy and hierarchy exist
+  bool mgp_split_ready = false;  // the split operator's FP32 copy and hierarchy exist
   bool mixed_used_mg = false;  // the last mixed pressure solve started with the multigrid inner solver
   int refinement_cycles = 0;  // outer cycles of the last mixed-precision pressure solve
   dn_diag last_diag{};        // diagnostics at the end of the last dn_step (compute_diagnostics, solver.cpp:276)
@@ -749,15 +894,69 @@ dn_status pcg_launch_args(dn_handle *h, const double *a, const double *l, const 
   return DN_OK;
 }
 
+// results of a persistent solve (out[0..count) and its status word) into a record block: [0, count) and
+// [count] = the status
+__global__ void k_rec_copy(const double *out, int count, const int *status, double *dst) {
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < count; ++k) dst[k] = out[k];
+  dst[count] = (double)*status;
+}
+
+// 1 into a record slot (a branch that ran)
+__global__ void k_rec_flag(double *dst) {
+  if (threadIdx.x == 0) *dst = 1.0;
+}
+// the condition of the CH solve's retry with the diagonal preconditioner: the PCG broke down
+__global__ void k_cond_breakdown(const int *status, cudaGraphConditionalHandle hd) {
+  if (threadIdx.x != 0) return;
+  const int st = *status;
+  cudaGraphSetConditional(hd, (st == kDevPcgBreakdownRz0 || st == kDevPcgBreakdownPap || st == kDevPcgBreakdownRz)
+                                  ? 1u : 0u);
+}
+// sqrt(sum r^2 / sum b^2) of per-CTA pairs (k_residual_partials), added in a fixed order by one warp
+__global__ void k_eq_residual(const double *partials, int nb, double *dst) {
+  double rs = 0.0, bs = 0.0;
+  for (int k = threadIdx.x; k < nb; k += 32) {
+    rs += partials[2 * k];
+    bs += partials[2 * k + 1];
+  }
+  rs = warp_sum(rs);
+  bs = warp_sum(bs);
+  if (threadIdx.x == 0) *dst = sqrt(rs / (bs < 1.0e-30 ? 1.0e-30 : bs));
+}
+
+// Slots of a step's record (h->rec + kRecStep): the persistent solves' out[0..4) and status, and the rest
+// of what dn_step reports, so that a step recorded into a graph is read back once.
+constexpr int kRecStep = 32;
+enum StepSlot {
+  kSChPcg = 0,     // CH PCG: iterations, abs, rel, iterate residual; [4] status
+  kSChRetry = 5,   // the CH PCG broke down and was retried with the diagonal preconditioner
+  kSChEq = 6,      // CH equation residual |b - A x| / |b|
+  kSMom = 8,       // BiCGSTAB: iterations, residual, ...; [12] status
+  kSP = 16,        // pressure PCG: iterations, abs, rel, iterate residual; [20] status
+  kSPFactor = 21,  // the pressure factor's status (variable operator)
+};
+
+// rec: where a solve recorded into a graph (h->capturing) leaves its out[0..4) and status (k_rec_copy);
+// nothing is read back then
 template <int S, int SWEEP>
 dn_status run_pcg(dn_handle *h, const double *a, const double *l, const double *dinv, int prec, int project, int max_it,
-                  double tol, double out[4]) {
+                  double tol, double out[4], double *rec = nullptr) {
   PcgArgs P{};
   size_t dyn_smem = 0;
   int blocks = 1;
   DN_TRY((pcg_launch_args<S, SWEEP>(h, a, l, dinv, prec, project, max_it, tol, P, dyn_smem, blocks)));
   DN_TRY(reset_sync(h));
   void *args[] = {&P};
+  if (h->capturing) {
+    if (!rec) return fail(h, DN_ERR_UNSUPPORTED, "a recorded PCG solve needs a record");
+    DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_pcg<S, SWEEP>, dim3(blocks), dim3(kBlock), args, dyn_smem,
+                                           h->stream));
+    h->launches++;
+    k_rec_copy<<<1, 32, 0, h->stream>>>(h->scal + 8, 4, h->status, rec);
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    return check_launch(h, "k_rec_copy");
+  }
   cudaEventRecord(h->kev[0], h->stream);
   DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_pcg<S, SWEEP>, dim3(blocks), dim3(kBlock), args, dyn_smem,
                                          h->stream));
@@ -860,11 +1059,17 @@ dn_status run_pcg32(dn_handle *h, int prec, int project, int max_it, double tol,
   }
   DN_TRY(reset_sync(h));
   void *args[] = {&P};
+  const void *kern = !staged ? (const void *)k_pcg<5, 0, float>
+                     : h->G.px ? (const void *)k_pcg<5, 4, float>
+                               : (const void *)k_pcg<5, 3, float>;
+  if (h->capturing) {  // recorded into a graph: status and results stay on the device (h->status, h->scal + 8)
+    DN_CUDA(h, cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kBlock), args, dyn_smem, h->stream));
+    h->launches++;
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    return DN_OK;
+  }
   cudaEventRecord(h->kev[0], h->stream);
-  DN_CUDA(h, cudaLaunchCooperativeKernel(!staged ? (const void *)k_pcg<5, 0, float>
-                                         : h->G.px ? (const void *)k_pcg<5, 4, float>
-                                                   : (const void *)k_pcg<5, 3, float>,
-                                         dim3(blocks), dim3(kBlock), args, dyn_smem, h->stream));
+  DN_CUDA(h, cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kBlock), args, dyn_smem, h->stream));
   cudaEventRecord(h->kev[1], h->stream);
   h->launches++;
   int st = 0;
@@ -939,10 +1144,11 @@ dn_status mg_alloc(dn_handle *h, MgHier &H, int nx, int ny, const BCSide *sides)
   return DN_OK;
 }
 
-// Coarse operators of H's current level-0 operator and the inverse of the coarsest one.  *usable = false when
-// the coarsest matrix has a non-positive pivot (the caller then does not use the hierarchy).
-dn_status mg_setup(dn_handle *h, MgHier &H, bool *usable) {
-  *usable = false;
+// Coarse operators of H's current level-0 operator and the inverse of the coarsest one; H.flag (device) is
+// set when the coarsest matrix has a non-positive pivot.
+dn_status mg_setup_launch(dn_handle *h, MgHier &H) {
+  if (H.levels() > 0 && (!H.lv[0].a64 || !H.lv[0].a || !H.lv[0].r))
+    return fail(h, DN_ERR_INVALID_ARGUMENT, "multigrid level 0 has no operator");
   double mass = H.mass;
   for (int l = 1; l < H.levels(); ++l) {
     const MgHier::Lv &f = H.lv[l - 1];
@@ -956,7 +1162,14 @@ dn_status mg_setup(dn_handle *h, MgHier &H, bool *usable) {
   const int nc = c.nx * c.ny;
   k_mg_coarse_inverse<<<1, 256, sizeof(double) * nc * nc, h->stream>>>(c.a64, c.nx, c.ny, h->G.px, h->G.py,
                                                                          H.singular, H.inv, H.flag);
-  DN_TRY(check_launch(h, "k_mg_coarse_inverse"));
+  return check_launch(h, "k_mg_coarse_inverse");
+}
+
+// mg_setup_launch, then its flag read back: *usable = false when the coarsest matrix has a non-positive pivot
+// (the caller then does not use the hierarchy).
+dn_status mg_setup(dn_handle *h, MgHier &H, bool *usable) {
+  *usable = false;
+  DN_TRY(mg_setup_launch(h, H));
   int flag = 0;
   DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 33, H.flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1013,6 +1226,7 @@ dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
 // (hierarchy, b0, x0): the kernels' arguments are the level buffers' pointers, which never change, and the
 // operators are rewritten in place by mg_setup.
 dn_status mg_vcycle(dn_handle *h, MgHier &H, float *b0, float *x0) {
+  if (h->capturing) return mg_vcycle_launch(h, H, b0, x0);  // recorded into the enclosing graph
   for (const dn_handle::MgGraph &g : h->mg_graphs)
     if (g.H == &H && g.b0 == b0 && g.x0 == x0) {
       DN_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
@@ -1040,13 +1254,92 @@ dn_status mg_vcycle(dn_handle *h, MgHier &H, float *b0, float *x0) {
   return DN_OK;
 }
 
+// ---------------------------------------------------------------------------------------------------
+// CUDA graphs with device-side loop control.  A conditional node (while / if) is recorded into the stream
+// capture in progress on h->stream: its handle is created on the graph being captured, the node follows
+// the capture's current dependencies, and its body is captured into the node's body graph on a side
+// stream (h->stream points there while `body` runs).  Kernels inside the graph set the conditions
+// (cudaGraphSetConditional), so a whole solve -- its iterations and its stopping decisions -- runs without
+// the host.
+// ---------------------------------------------------------------------------------------------------
+dn_status cap_info(dn_handle *h, cudaGraph_t *g, const cudaGraphNode_t **deps, size_t *nd) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  DN_CUDA(h, cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, g, deps, nd));
+  if (cs != cudaStreamCaptureStatusActive) return fail(h, DN_ERR_CUDA, "conditional node outside a stream capture");
+  return DN_OK;
+}
+
+// a condition handle on the graph being captured; 0 at every launch of the graph until a kernel sets it
+dn_status cond_create(dn_handle *h, cudaGraphConditionalHandle *hd) {
+  cudaGraph_t g = nullptr;
+  DN_TRY(cap_info(h, &g, nullptr, nullptr));
+  DN_CUDA(h, cudaGraphConditionalHandleCreate(hd, g, 0, cudaGraphCondAssignDefault));
+  return DN_OK;
+}
+
+template <class Body>
+dn_status cond_node(dn_handle *h, cudaGraphConditionalHandle hd, cudaGraphConditionalNodeType type, Body &&body) {
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  DN_TRY(cap_info(h, &g, &deps, &nd));
+  if (h->cap_depth >= kCapDepth) return fail(h, DN_ERR_UNSUPPORTED, "conditional graph nodes nested too deeply");
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = hd;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  DN_CUDA(h, cudaGraphAddNode(&node, g, deps, nd, &p));
+  cudaStream_t outer = h->stream, side = h->cap_streams[h->cap_depth];
+  DN_CUDA(h, cudaStreamBeginCaptureToGraph(side, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+  h->stream = side;
+  ++h->cap_depth;
+  const dn_status st = body();
+  --h->cap_depth;
+  h->stream = outer;
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(side, &captured);
+  DN_TRY(st);
+  if (ce != cudaSuccess) return fail(h, DN_ERR_CUDA, std::string("conditional body capture: ") + cudaGetErrorString(ce));
+  DN_CUDA(h, cudaStreamUpdateCaptureDependencies(outer, &node, 1, cudaStreamSetCaptureDependencies));
+  return DN_OK;
+}
+
+// `record` captured into an executable graph (nothing runs); h->capturing is set meanwhile, so the step
+// pieces record their results on the device instead of reading them back
+template <class Record>
+dn_status capture_exec(dn_handle *h, cudaGraphExec_t *exec, Record &&record) {
+  *exec = nullptr;
+  DN_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  h->capturing = true;
+  const dn_status st = record();
+  h->capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+  if (st != DN_OK || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return st != DN_OK ? st : fail(h, DN_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  }
+  const cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    *exec = nullptr;
+    return fail(h, DN_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(ie));
+  }
+  return DN_OK;
+}
+
 // One FP32 inner solve A e = b by CG preconditioned with `vcycles` V-cycles of H applied in sequence (1 for
-// the pressure operator; 2 for the CH operator, preconditioned by (K + s I)^-2), to the relative residual tol
-// of |b| = bnorm.  V: the operator and the vectors (V.x is e, zero on entry; b is copied into V.r);
-// tmp: a level-0 buffer for the output of the first of two V-cycles.  out: [0] iterations.
+// the pressure operator; 2 for the CH operator, preconditioned by (K + s I)^-2), recorded into the capture:
+// r = b, then a while node whose body is one iteration (precondition, r.z, direction, A p, p.q, update,
+// r.r) ending in k_mgcg_ctrl, which stops at |r| < tol |b| (|b| = R[kDcAbs]), a breakdown or the inner
+// iteration budget left in R.  V: the operator and the vectors (V.x is e, zero on entry); tmp: a level-0
+// buffer for the output of the first of two V-cycles.
 template <int S>
-dn_status run_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tmp, int vcycles, int project,
-                     int max_it, double tol, double bnorm, double out[4]) {
+dn_status rec_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tmp, int vcycles, int project,
+                     int max_it, double tol, double *R, DcNodes *nodes) {
   const long long n = V.A.n;
   V.part = h->mg_part;
   V.scal = h->mg_scal;
@@ -1056,172 +1349,312 @@ dn_status run_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tm
     k_mgp_scalars<<<1, 32, 0, h->stream>>>(h->mg_part, nb, h->mg_scal, mode, first, project, dn_);
     return check_launch(h, "k_mgp_scalars");
   };
-  auto precondition = [&]() -> dn_status {
+  DN_CUDA(h, cudaMemcpyAsync(V.r, b, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  cudaGraphConditionalHandle loop = 0;
+  DN_TRY(cond_create(h, &loop));
+  k_mgcg_init<<<1, 32, 0, h->stream>>>(h->mg_scal, R, max_it, loop);
+  DN_TRY(check_launch(h, "k_mgcg_init"));
+  return cond_node(h, loop, cudaGraphCondTypeWhile, [&]() -> dn_status {
+    const long long before = h->launches;
     if (vcycles == 2) {
       DN_TRY(mg_vcycle(h, H, V.r, tmp));
-      return mg_vcycle(h, H, tmp, V.z);
+      DN_TRY(mg_vcycle(h, H, tmp, V.z));
+    } else {
+      DN_TRY(mg_vcycle(h, H, V.r, V.z));
     }
-    return mg_vcycle(h, H, V.r, V.z);
-  };
-  DN_CUDA(h, cudaMemsetAsync(h->mg_scal, 0, 16 * sizeof(double), h->stream));
-  DN_CUDA(h, cudaMemcpyAsync(V.r, b, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  DN_TRY(precondition());
-  k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
-  DN_TRY(check_launch(h, "k_mgp_rz"));
-  DN_TRY(finish(2, 1));
-  k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, 1);
-  DN_TRY(check_launch(h, "k_mgp_direction"));
-  int it = 0;
-  const int cap = std::max(1, max_it);
-  while (it < cap) {
+    k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
+    DN_TRY(check_launch(h, "k_mgp_rz"));
+    DN_TRY(finish(2, -1));
+    k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, -1);
+    DN_TRY(check_launch(h, "k_mgp_direction"));
     k_mgp_apply<S><<<nb, 256, 0, h->stream>>>(V);
     DN_TRY(check_launch(h, "k_mgp_apply"));
     DN_TRY(finish(0, 0));
     k_mgp_update<<<nb, 256, 0, h->stream>>>(V);
     DN_TRY(check_launch(h, "k_mgp_update"));
     DN_TRY(finish(1, 0));
-    ++it;
-    DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 40, h->mg_scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    DN_CUDA(h, cudaStreamSynchronize(h->stream));
-    double sc[8];
-    std::memcpy(sc, h->host_scal + 40, sizeof sc);
-    if (sc[kMgBad] != 0.0) break;  // breakdown: the outer FP64 loop judges the iterate
-    const double rel = std::sqrt(std::max(sc[kMgRr], 0.0)) / std::max(bnorm, 1.0e-300);
-    if (!(rel >= tol)) break;  // converged (or non-finite: the outer loop stops on its own residual)
-    DN_TRY(precondition());
-    k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
-    DN_TRY(check_launch(h, "k_mgp_rz"));
-    DN_TRY(finish(2, 0));
-    k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, 0);
-    DN_TRY(check_launch(h, "k_mgp_direction"));
-  }
-  out[0] = (double)it;
-  out[1] = out[2] = out[3] = 0.0;
-  return DN_OK;
+    k_mgcg_ctrl<<<1, 32, 0, h->stream>>>(h->mg_scal, R, tol, loop);
+    DN_TRY(check_launch(h, "k_mgcg_ctrl"));
+    if (nodes) nodes->iter = h->launches - before;
+    return DN_OK;
+  });
 }
 
 dn_status pressure_factor(dn_handle *h, bool split, bool icc);
 
-// FP32 copies of the FP64 IC/ILDLT factor for the IC inner solver (built on first use within a solve)
-dn_status ensure_ic32(dn_handle *h, bool split, int kind) {
-  if (h->ic32_ready) return DN_OK;
-  DN_TRY(pressure_factor(h, split, kind == kPrecICC));
+// The FP64 IC/ILDLT factor of the pressure operator (unless the constant split operator's is already
+// valid) and its FP32 copies for the IC inner solver, recorded into the capture; a failed factor is
+// recorded in R[kDcErr] and *gate is left 0.
+dn_status rec_ic32_factor(dn_handle *h, bool split, int kind, double *R, cudaGraphConditionalHandle gate) {
   const long long n = h->n;
+  if (!(split && h->p_factor_valid && h->p_factor_kind == kind)) {
+    DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    Factor F{h->l5, h->d5, h->dinv5, 0.0};
+    k_factor<5><<<1, 1024, 0, h->stream>>>(SpOp{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py}, F, kind,
+                                            h->status);
+    DN_TRY(check_launch(h, "k_factor<5>"));
+  } else {
+    DN_CUDA(h, cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+  }
   if (h->G.px) {  // the global-memory wavefront reads the L slots
     k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->l5, h->fl5, 5 * n);
     DN_TRY(check_launch(h, "k_to_float"));
   }
   k_to_float<<<blocks_for(n), 256, 0, h->stream>>>(h->dinv5, h->fdinv5, n);
   DN_TRY(check_launch(h, "k_to_float"));
-  h->ic32_ready = true;
-  return DN_OK;
+  k_ic_gate<<<1, 32, 0, h->stream>>>(h->status, R, gate);
+  return check_launch(h, "k_ic_gate");
 }
 
-// Mixed-precision pressure solve: x = 0; repeat r = b - A x (FP64, projected when the system is singular),
-// stop on the reference's rule (rel < tol or abs < tol on the FP64 residual), else solve A e = r in FP32 to
-// the relative tolerance mixed_inner_tolerance and add e to x in FP64.  The inner solver is CG with the
-// multigrid V-cycle (when the grid has a hierarchy and mixed_preconditioner allows it) or the persistent
-// PCG with the scheme's IC/ILDLT factor rounded to FP32.  An inner multigrid solve after which the FP64
-// residual does not decrease hands the rest of the solve to the IC inner solver.  The operator is the FP64
-// one rounded to FP32.  out: [0] inner iterations in total, [1] abs and [2] rel FP64 residual, [3] 0.
-dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
+// The FP32 copy of the pressure operator and the coarse operators of its hierarchy (kernels only: the
+// coarsest inverse's usability flag stays on the device, where the solve's first check reads it).
+dn_status mg_setup_launch(dn_handle *h, MgHier &H);
+
+// Mixed-precision pressure solve, recorded into the capture: x = 0 on entry; repeat r = b - A x (FP64,
+// projected when the system is singular), stop on the reference's rule (rel < tol or abs < tol on the FP64
+// residual), else solve A e = r in FP32 to the relative tolerance mixed_inner_tolerance and add e to x in
+// FP64.  The inner solver is CG with the multigrid V-cycle (when the grid has a usable hierarchy and
+// mixed_preconditioner allows it) or the persistent PCG with the scheme's IC/ILDLT factor rounded to FP32;
+// a multigrid cycle after which the FP64 residual does not decrease hands the rest of the solve to the IC
+// inner solver.  The operator is the FP64 one rounded to FP32.  Every decision is k_dc_decide's, on the
+// device; the result is the record R = h->rec + kRecPressure.
+dn_status rec_mixed_pressure(dn_handle *h, bool split, int kind, DcNodes *nodes) {
   const dn_config &cfg = h->cfg;
   const long long n = h->n;
   const int project = h->has_dirichlet ? 0 : 1;
-  h->ic32_ready = false;
-  bool use_mg = false;
-  // the split operator is the same every step: its FP32 copy and hierarchy are built once
-  if (!(split && h->mgp_split_ready)) {
+  double *R = h->rec + kRecPressure;
+  const long long start = h->launches;
+  if (!split) {  // the variable operator changes every step: its FP32 copy and hierarchy are made here
     k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
     DN_TRY(check_launch(h, "k_to_float"));
-    if (h->mgp.levels() > 0) {
-      h->mgp.lv[0].a64 = h->a5;
-      h->mgp.lv[0].a = h->fa5;
-      h->mgp.lv[0].r = h->fy;
-      DN_TRY(mg_setup(h, h->mgp, &use_mg));
-    }
-    h->mgp_split_ready = split;
-    h->mgp_usable = use_mg;
+    if (h->mgp.levels() > 0) DN_TRY(mg_setup_launch(h, h->mgp));
   }
-  use_mg = h->mgp_usable;
-  h->mixed_used_mg = use_mg;
-  if (!use_mg) DN_TRY(ensure_ic32(h, split, kind));
+  DcParams P{};
+  P.tol = cfg.pressure_tolerance;
+  P.n = (double)n;
+  P.max_it = cfg.poisson_iterations;
+  P.max_cycles = kDcMaxCycles;
+  P.project = project;
+  P.ch = 0;
+  P.mg_flag = h->mgp.levels() > 0 ? h->mgp.flag : nullptr;
   const SpOp A{h->a5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
-  h->phase_ms[4] = 0.0;
-  h->pcg_split_ms[0] = h->pcg_split_ms[1] = h->pcg_split_ms[2] = 0.0;
-  constexpr int kMaxCycles = 40;
-  int total = 0, cycles = 0;
-  double absr = 0.0, relr = 0.0, prev = INFINITY;
-  for (;;) {
-    const int nb = 128;
+  const int nb = 128;
+  DN_CUDA(h, cudaMemsetAsync(R, 0, kDcSize * sizeof(double), h->stream));
+  cudaGraphConditionalHandle loop = 0;
+  DN_TRY(cond_create(h, &loop));
+  auto check = [&]() -> dn_status {
     k_outer_residual<5><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
     DN_TRY(check_launch(h, "k_outer_residual"));
     k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
     DN_TRY(check_launch(h, "k_finish3"));
-    double sums[3];
-    DN_TRY(read_scalars(h, 3, sums));
-    const double mean = project ? sums[0] / (double)n : 0.0;
-    const double rn2 = project ? std::max(sums[1] - sums[0] * sums[0] / (double)n, 0.0) : sums[1];
-    absr = std::sqrt(rn2);
-    relr = absr / std::max(std::sqrt(std::max(sums[2], 0.0)), 1.0e-30);
-    if (relr < cfg.pressure_tolerance || absr < cfg.pressure_tolerance) break;
-    // the iteration budget is shared by the inner solves; a cycle that no longer reduces the residual ends it
-    if (cycles >= kMaxCycles || total >= cfg.poisson_iterations) break;
-    if (!(absr < prev)) {
-      if (!use_mg) break;
-      use_mg = false;  // the multigrid inner solve stalled: continue from this iterate with the IC inner solver
-      DN_TRY(ensure_ic32(h, split, kind));
-    }
-    prev = absr;
-    k_inner_rhs<<<blocks_for(n), 256, 0, h->stream>>>(h->r, mean, h->fb, h->fx, n);
+    k_dc_decide<<<1, 32, 0, h->stream>>>(h->scal + 8, R, P, loop);
+    return check_launch(h, "k_dc_decide");
+  };
+  DN_TRY(check());
+  if (nodes) nodes->fixed = h->launches - start;
+  return cond_node(h, loop, cudaGraphCondTypeWhile, [&]() -> dn_status {
+    const long long c0 = h->launches;
+    // every condition handle belongs to a node of the graph: the multigrid branch exists with a hierarchy
+    const bool has_mg = h->mgp.levels() > 0;
+    cudaGraphConditionalHandle use_mg = 0, use_ic = 0;
+    if (has_mg) DN_TRY(cond_create(h, &use_mg));
+    DN_TRY(cond_create(h, &use_ic));
+    k_dc_branch<<<1, 32, 0, h->stream>>>(R, has_mg ? 1 : 0, use_mg, use_ic);
+    DN_TRY(check_launch(h, "k_dc_branch"));
+    k_inner_rhs_dev<<<blocks_for(n), 256, 0, h->stream>>>(h->r, R, h->fb, h->fx, n);
     DN_TRY(check_launch(h, "k_inner_rhs"));
-    double o[4];
-    if (use_mg) {
-      MgVec V{};
-      V.A = SpOpT<float>{h->fa5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
-      V.x = h->fx;
-      V.r = h->fr;
-      V.z = h->fz;
-      V.p = h->fp0;
-      V.q = h->fap;
-      cudaEventRecord(h->kev[0], h->stream);
-      DN_TRY(run_mgcg32<5>(h, h->mgp, V, h->fb, nullptr, 1, project, cfg.poisson_iterations - total,
-                           cfg.mixed_inner_tolerance, absr, o));
-      cudaEventRecord(h->kev[1], h->stream);
-      DN_CUDA(h, cudaEventSynchronize(h->kev[1]));
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
-      h->phase_ms[4] += ms;
-    } else
-      DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations - total, cfg.mixed_inner_tolerance, o));
-    total += (int)o[0];
+    if (has_mg) {
+      DN_TRY(cond_node(h, use_mg, cudaGraphCondTypeIf, [&]() -> dn_status {
+        MgVec V{};
+        V.A = SpOpT<float>{h->fa5, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+        V.x = h->fx;
+        V.r = h->fr;
+        V.z = h->fz;
+        V.p = h->fp0;
+        V.q = h->fap;
+        return rec_mgcg32<5>(h, h->mgp, V, h->fb, nullptr, 1, project, cfg.poisson_iterations,
+                             cfg.mixed_inner_tolerance, R, nodes);
+      }));
+    }
+    DN_TRY(cond_node(h, use_ic, cudaGraphCondTypeIf, [&]() -> dn_status {
+      const long long i0 = h->launches;
+      cudaGraphConditionalHandle make = 0, go = 0;
+      DN_TRY(cond_create(h, &make));
+      DN_TRY(cond_create(h, &go));
+      k_ic_need<<<1, 32, 0, h->stream>>>(R, make, go);  // the factor once per solve
+      DN_TRY(check_launch(h, "k_ic_need"));
+      const long long m0 = h->launches;
+      DN_TRY(cond_node(h, make, cudaGraphCondTypeIf, [&]() { return rec_ic32_factor(h, split, kind, R, go); }));
+      if (nodes) nodes->make = h->launches - m0;
+      DN_TRY(cond_node(h, go, cudaGraphCondTypeIf, [&]() -> dn_status {
+        double unused[4];  // the results stay on the device (h->capturing)
+        DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations, cfg.mixed_inner_tolerance, unused));
+        k_ic_done<<<1, 32, 0, h->stream>>>(h->scal + 8, h->status, R);
+        return check_launch(h, "k_ic_done");
+      }));
+      if (nodes) nodes->ic = h->launches - i0 - nodes->make;
+      return DN_OK;
+    }));
     k_add_correction<<<blocks_for(n), 256, 0, h->stream>>>(h->x, h->fx, n);
     DN_TRY(check_launch(h, "k_add_correction"));
-    ++cycles;
-    if ((int)o[0] == 0 && !use_mg) break;
+    k_dc_cycle_end<<<1, 32, 0, h->stream>>>(nullptr, R);
+    DN_TRY(check_launch(h, "k_dc_cycle_end"));
+    DN_TRY(check());
+    if (nodes) nodes->cycle = h->launches - c0 - nodes->iter - nodes->ic - nodes->make;
+    return DN_OK;
+  });
+}
+
+// kernel launches a solve graph's loops ran, from its record: per outer cycle, per multigrid inner
+// iteration, per IC inner solve, and the IC factor branch once
+long long dc_launches(const DcNodes &d, const double *R) {
+  return (long long)R[kDcCycles] * d.cycle + (long long)R[kDcMgIts] * d.iter + (long long)R[kDcIcCycles] * d.ic +
+         (R[kDcIcCycles] > 0.0 ? d.make : 0);
+}
+
+// The eager form of a recorded solve: captured once per handle (and again after a launch-shape change),
+// replayed, and its record read back with one synchronisation.
+dn_status replay_solve(dn_handle *h, dn_handle::SolveGraph &g, const std::function<dn_status(DcNodes *)> &record,
+                       double *R, double host[kDcSize], float *ms) {
+  if (!g.exec || g.epoch != h->graph_epoch) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    DcNodes nodes;
+    const long long before = h->launches;
+    DN_TRY(capture_exec(h, &g.exec, [&]() { return record(&nodes); }));
+    h->launches = before;
+    g.nodes = nodes;
+    g.epoch = h->graph_epoch;
   }
-  h->refinement_cycles = cycles;
-  out[0] = (double)total;
-  out[1] = absr;
-  out[2] = relr;
-  out[3] = 0.0;
+  cudaEventRecord(h->kev[0], h->stream);
+  DN_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+  cudaEventRecord(h->kev[1], h->stream);
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 96, R, kDcSize * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(host, h->host_scal + 96, kDcSize * sizeof(double));
+  *ms = 0.0f;
+  cudaEventElapsedTime(ms, h->kev[0], h->kev[1]);
+  h->launches += g.nodes.fixed + dc_launches(g.nodes, host);
+  return DN_OK;
+}
+
+dn_status dc_error(dn_handle *h, const double R[kDcSize], int kind) {
+  const int st = (int)R[kDcErr];
+  if (st == 0) return DN_OK;
+  if (st == kDevFactorFailed)
+    return fail(h, kind == kPrecICC ? DN_ERR_ICC_FAILED : DN_ERR_ILDLT_FAILED,
+                kind == kPrecICC ? "ICC preconditioner construction failed" : "ILDLT preconditioner construction failed");
+  return dev_status_to_dn(h, st);
+}
+
+// Mixed-precision pressure solve (rec_mixed_pressure), eager or recorded into a step graph.  The split
+// operator is the same every step: its FP32 copy and hierarchy are made once, here.  out: [0] inner
+// iterations in total, [1] abs and [2] rel FP64 residual, [3] 0.
+dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
+  const long long n = h->n;
+  if (split && !h->mgp_split_ready) {
+    if (h->capturing) return fail(h, DN_ERR_UNSUPPORTED, "the split operator's hierarchy is made by an eager step");
+    k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
+    DN_TRY(check_launch(h, "k_to_float"));
+    if (h->mgp.levels() > 0) {
+      bool usable = false;
+      DN_TRY(mg_setup(h, h->mgp, &usable));
+      if (!usable) DN_TRY(pressure_factor(h, true, kind == kPrecICC));
+    } else {
+      DN_TRY(pressure_factor(h, true, kind == kPrecICC));  // the IC inner solver's factor, made once
+    }
+    h->mgp_split_ready = true;
+  }
+  h->phase_ms[4] = 0.0;
+  h->pcg_split_ms[0] = h->pcg_split_ms[1] = h->pcg_split_ms[2] = 0.0;
+  out[0] = out[1] = out[2] = out[3] = 0.0;
+  if (h->capturing) return rec_mixed_pressure(h, split, kind, &h->step_dcn[0]);
+  double R[kDcSize];
+  float ms = 0.0f;
+  DN_TRY(replay_solve(h, h->dc_graph[0], [&](DcNodes *nd) { return rec_mixed_pressure(h, split, kind, nd); },
+                      h->rec + kRecPressure, R, &ms));
+  h->phase_ms[4] = ms;
+  DN_TRY(dc_error(h, R, kind));
+  h->refinement_cycles = (int)R[kDcCycles];
+  h->mixed_used_mg = R[kDcUsedMg0] != 0.0;
+  out[0] = R[kDcTotal];
+  out[1] = R[kDcAbs];
+  out[2] = R[kDcRel];
   return DN_OK;
 }
 
 // Mixed-precision CH solve (precision = mixed, multigrid hierarchy present): the FP64 defect-correction loop
-// of mixed_pressure around FP32 inner CG solves of the 13-point operator A = alpha0 I + beta1 K + beta2 K^2
+// of rec_mixed_pressure around FP32 inner CG solves of the 13-point operator A = alpha0 I + beta1 K + beta2 K^2
 // (K = -L, build_cahn_hilliard_operator, ch_sparse_krylov.hpp:205-233), preconditioned by two V-cycles of
 // K + s I with s = sqrt(alpha0 / beta2).  beta2 (K + s I)^2 has A's K^2 and constant terms, and on every
 // eigenvector of K (eigenvalue k >= 0) the ratio (alpha0 + beta1 k + beta2 k^2) / (beta2 (k + s)^2) lies
 // between 1/2 + beta1 / (4 beta2 s) (at k = s) and 1, so the preconditioned condition number stays below 2
 // on every grid.  Stops on the reference's rule (relative or absolute FP64 residual below ch_tolerance,
-// solve_preconditioned_cg, ch_sparse_krylov.hpp:545-560); x starts at the state (h->x).  *iter_res: the last
-// correction's size relative to the iterate, the analogue of the PCG's iterate residual.
+// solve_preconditioned_cg, ch_sparse_krylov.hpp:545-560), or when a cycle does not reduce the residual; x
+// starts at the state (h->x).  Recorded into the capture; the record is R = h->rec + kRecCh, with the last
+// correction's size relative to the iterate (the analogue of the PCG's iterate residual) in R[kDcIres].
+dn_status rec_mixed_ch(dn_handle *h, DcNodes *nodes) {
+  const dn_config &cfg = h->cfg;
+  const long long n = h->n;
+  double *R = h->rec + kRecCh;
+  const long long start = h->launches;
+  DcParams P{};
+  P.tol = cfg.ch_tolerance;
+  P.n = (double)n;
+  P.max_it = cfg.ch_inner_iterations;
+  P.max_cycles = kDcMaxCycles;
+  P.project = 0;
+  P.ch = 1;
+  P.mg_flag = h->mgc.flag;
+  const SpOp A{h->a13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+  const int nb = 128;
+  DN_CUDA(h, cudaMemsetAsync(R, 0, kDcSize * sizeof(double), h->stream));
+  cudaGraphConditionalHandle loop = 0;
+  DN_TRY(cond_create(h, &loop));
+  auto check = [&]() -> dn_status {
+    k_outer_residual<13><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
+    DN_TRY(check_launch(h, "k_outer_residual"));
+    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
+    DN_TRY(check_launch(h, "k_finish3"));
+    k_dc_decide<<<1, 32, 0, h->stream>>>(h->scal + 8, R, P, loop);
+    return check_launch(h, "k_dc_decide");
+  };
+  DN_TRY(check());
+  if (nodes) nodes->fixed = h->launches - start;
+  return cond_node(h, loop, cudaGraphCondTypeWhile, [&]() -> dn_status {
+    const long long c0 = h->launches;
+    k_inner_rhs_dev<<<blocks_for(n), 256, 0, h->stream>>>(h->r, R, h->cb32, h->cx32, n);
+    DN_TRY(check_launch(h, "k_inner_rhs"));
+    MgVec V{};
+    V.A = SpOpT<float>{h->fa13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
+    V.x = h->cx32;
+    V.r = h->cr32;
+    V.z = h->cz32;
+    V.p = h->cp32;
+    V.q = h->cq32;
+    DN_TRY(rec_mgcg32<13>(h, h->mgc, V, h->cb32, h->ct32, 2, 0, cfg.ch_inner_iterations, cfg.mixed_inner_tolerance,
+                          R, nodes));
+    k_add_correction_norms<<<nb, 256, 0, h->stream>>>(h->x, h->cx32, n, h->partials);
+    DN_TRY(check_launch(h, "k_add_correction_norms"));
+    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
+    DN_TRY(check_launch(h, "k_finish3"));
+    k_dc_cycle_end<<<1, 32, 0, h->stream>>>(h->scal + 8, R);
+    DN_TRY(check_launch(h, "k_dc_cycle_end"));
+    DN_TRY(check());
+    if (nodes) nodes->cycle = h->launches - c0 - nodes->iter;
+    return DN_OK;
+  });
+}
+
+// The mixed CH solve (rec_mixed_ch), eager or recorded into a step graph.  The FP32 operator and the
+// (K + s I) hierarchy are made when alpha0 changes (an eager step).  *used = false when the hierarchy is
+// unusable (the caller then runs the FP64 ILDLT PCG).
 dn_status mixed_ch(dn_handle *h, double alpha0, dn_report *rep, double *iter_res, bool *used) {
   const dn_config &cfg = h->cfg;
   const long long n = h->n;
   *used = false;
   if (h->ch_mg_alpha0 != alpha0) {
+    if (h->capturing) return fail(h, DN_ERR_UNSUPPORTED, "the CH hierarchy is made by an eager step");
     const double a2 = cfg.cn > 0.0 ? (3.0 * kSqrt2 * cfg.cn / 4.0) : 0.0;
     const double beta2 = a2 / cfg.pe;
     if (!(beta2 > 0.0) || !(alpha0 > 0.0)) return DN_OK;
@@ -1235,59 +1668,26 @@ dn_status mixed_ch(dn_handle *h, double alpha0, dn_report *rep, double *iter_res
     h->mgc.singular = 0;
     bool ok = false;
     DN_TRY(mg_setup(h, h->mgc, &ok));
-    if (!ok) return DN_OK;
+    h->ch_mg_ok = ok;
     h->ch_mg_alpha0 = alpha0;
   }
+  if (!h->ch_mg_ok) return DN_OK;
   *used = true;
-  const SpOp A{h->a13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
-  constexpr int kMaxCycles = 40;
-  int total = 0, cycles = 0;
-  double absr = 0.0, relr = 0.0, prev = INFINITY, ires = 0.0;
-  for (;;) {
-    const int nb = 128;
-    k_outer_residual<13><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
-    DN_TRY(check_launch(h, "k_outer_residual"));
-    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
-    DN_TRY(check_launch(h, "k_finish3"));
-    double sums[3];
-    DN_TRY(read_scalars(h, 3, sums));
-    absr = std::sqrt(std::max(sums[1], 0.0));
-    relr = absr / std::max(std::sqrt(std::max(sums[2], 0.0)), 1.0e-30);
-    if (relr < cfg.ch_tolerance || absr < cfg.ch_tolerance) break;
-    if (cycles >= kMaxCycles || total >= cfg.ch_inner_iterations || !(absr < prev)) break;
-    prev = absr;
-    k_inner_rhs<<<blocks_for(n), 256, 0, h->stream>>>(h->r, 0.0, h->cb32, h->cx32, n);
-    DN_TRY(check_launch(h, "k_inner_rhs"));
-    MgVec V{};
-    V.A = SpOpT<float>{h->fa13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
-    V.x = h->cx32;
-    V.r = h->cr32;
-    V.z = h->cz32;
-    V.p = h->cp32;
-    V.q = h->cq32;
-    double o[4];
-    DN_TRY(run_mgcg32<13>(h, h->mgc, V, h->cb32, h->ct32, 2, 0, cfg.ch_inner_iterations - total,
-                          cfg.mixed_inner_tolerance, absr, o));
-    total += (int)o[0];
-    k_add_correction_norms<<<nb, 256, 0, h->stream>>>(h->x, h->cx32, n, h->partials);
-    DN_TRY(check_launch(h, "k_add_correction_norms"));
-    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
-    DN_TRY(check_launch(h, "k_finish3"));
-    double en[3];
-    DN_TRY(read_scalars(h, 3, en));
-    ires = std::sqrt(std::max(en[0], 0.0) / std::max(en[1], 1.0e-30));
-    ++cycles;
-  }
-  rep->ch_iterations = total;
   rep->ch_preconditioner = 3;
-  *iter_res = ires;
+  if (h->capturing) return rec_mixed_ch(h, &h->step_dcn[1]);
+  double R[kDcSize];
+  float ms = 0.0f;
+  DN_TRY(replay_solve(h, h->dc_graph[1], [&](DcNodes *nd) { return rec_mixed_ch(h, nd); }, h->rec + kRecCh, R, &ms));
+  h->phase_ms[5] += ms;
+  rep->ch_iterations = (int)R[kDcTotal];
+  *iter_res = R[kDcIres];
   return DN_OK;
 }
 
 // Jacobi-BiCGSTAB on the momentum system (the handle's M, or another operator in the same row format --
 // the adjoint's M^T -- with its own stopping rule: relative when use_rel, else the reference's absolute one).
 dn_status run_bicgstab(dn_handle *h, double out[4], const double *coef = nullptr, const int *tgt = nullptr,
-                       int use_rel = 0, double tol = -1.0, int max_it = -1) {
+                       int use_rel = 0, double tol = -1.0, int max_it = -1, double *rec = nullptr) {
   BicgArgs P;
   P.n = h->nm;
   P.coef = coef ? coef : h->mcoef;
@@ -1321,6 +1721,14 @@ dn_status run_bicgstab(dn_handle *h, double out[4], const double *coef = nullptr
   int blocks = (int)std::min<long long>((long long)h->bicg_occ * h->cta_cap, std::max<long long>(1, h->nm / 1024));
   blocks = std::max(1, std::min(blocks, kMaxBlocks));
   void *args[] = {&P};
+  if (h->capturing) {  // recorded into a graph: out and status into rec (k_rec_copy)
+    if (!rec) return fail(h, DN_ERR_UNSUPPORTED, "a recorded BiCGSTAB solve needs a record");
+    DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(blocks), dim3(kBlock), args, 0, h->stream));
+    h->launches++;
+    k_rec_copy<<<1, 32, 0, h->stream>>>(h->scal + 8, 4, h->status, rec);
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    return check_launch(h, "k_rec_copy");
+  }
   cudaEventRecord(h->kev[0], h->stream);
   DN_CUDA(h, cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(blocks), dim3(kBlock), args, 0, h->stream));
   cudaEventRecord(h->kev[1], h->stream);
@@ -1481,17 +1889,35 @@ dn_status ch_linear_solve(dn_handle *h, double alpha0, dn_report *rep, double *i
   DN_TRY(ensure_ch_system(h, alpha0));
   double out[4];
   bool mixed_done = false;
-  if (h->ch_mg && h->cfg.precision == DN_PRECISION_MIXED) {
-    cudaEventRecord(h->kev[0], h->stream);
-    DN_TRY(mixed_ch(h, alpha0, rep, iter_res, &mixed_done));
-    cudaEventRecord(h->kev[1], h->stream);
-    DN_CUDA(h, cudaEventSynchronize(h->kev[1]));
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
-    h->phase_ms[5] += ms;
-  }
+  if (h->ch_mg && h->cfg.precision == DN_PRECISION_MIXED) DN_TRY(mixed_ch(h, alpha0, rep, iter_res, &mixed_done));
   rep->ch_preconditioner = mixed_done ? 3 : (h->ch_prec == kPrecLDLT) ? 1 : 0;
-  if (!mixed_done) {
+  if (!mixed_done && h->capturing) {
+    // recorded: results in the step record; a breakdown retries with the diagonal preconditioner
+    // (phase_field.cpp:468-473) in a conditional branch
+    double *R = h->rec + kRecStep;
+    if (h->ch_prec == kPrecLDLT) {
+      DN_TRY((run_pcg<13, 1>(h, h->a13, h->l13, h->dinv13, kPrecLDLT, 0, h->cfg.ch_inner_iterations,
+                             h->cfg.ch_tolerance, out, R + kSChPcg)));
+      cudaGraphConditionalHandle retry = 0;
+      DN_TRY(cond_create(h, &retry));
+      k_cond_breakdown<<<1, 32, 0, h->stream>>>(h->status, retry);
+      DN_TRY(check_launch(h, "k_cond_breakdown"));
+      const long long r0 = h->launches;
+      DN_TRY(cond_node(h, retry, cudaGraphCondTypeIf, [&]() -> dn_status {
+        k_diag_inverse<13><<<blocks_for(h->n), 256, 0, h->stream>>>(
+            SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, h->dinv13);
+        DN_TRY(check_launch(h, "k_diag_inverse"));
+        DN_TRY((run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations,
+                               h->cfg.ch_tolerance, out, R + kSChPcg)));
+        k_rec_flag<<<1, 32, 0, h->stream>>>(R + kSChRetry);
+        return check_launch(h, "k_rec_flag");
+      }));
+      h->step_retry = h->launches - r0;
+    } else {
+      DN_TRY((run_pcg<13, 2>(h, h->a13, h->l13, h->dinv13, kPrecDiag, 0, h->cfg.ch_inner_iterations,
+                             h->cfg.ch_tolerance, out, R + kSChPcg)));
+    }
+  } else if (!mixed_done) {
     dn_status s;
     if (h->ch_prec == kPrecLDLT)
       s = run_pcg<13, 1>(h, h->a13, h->l13, h->dinv13, kPrecLDLT, 0, h->cfg.ch_inner_iterations, h->cfg.ch_tolerance,
@@ -1518,15 +1944,14 @@ dn_status ch_linear_solve(dn_handle *h, double alpha0, dn_report *rep, double *i
   k_residual_partials<13><<<nb, 256, 0, h->stream>>>(SpOp{h->a13, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, h->b,
                                                       h->x, h->partials);
   DN_TRY(check_launch(h, "k_residual_partials"));
-  std::vector<double> part(2 * nb);
-  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 64, h->partials, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  double *eq = h->rec + kRecStep + kSChEq;
+  k_eq_residual<<<1, 32, 0, h->stream>>>(h->partials, nb, eq);
+  DN_TRY(check_launch(h, "k_eq_residual"));
+  *eq_res = 0.0;
+  if (h->capturing) return DN_OK;
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + 64, eq, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
-  double rs = 0.0, bs = 0.0;
-  for (int k = 0; k < nb; ++k) {
-    rs += h->host_scal[64 + 2 * k];
-    bs += h->host_scal[64 + 2 * k + 1];
-  }
-  *eq_res = std::sqrt(rs / std::max(bs, 1.0e-30));
+  *eq_res = h->host_scal[64];
   return DN_OK;
 }
 
@@ -1598,7 +2023,7 @@ dn_status momentum(dn_handle *h, int step, dn_report *rep) {
                                                            h->mx);
   DN_TRY(check_launch(h, "k_mom_assemble"));
   double out[4];
-  DN_TRY(run_bicgstab(h, out));
+  DN_TRY(run_bicgstab(h, out, nullptr, nullptr, 0, -1.0, -1, h->rec + kRecStep + kSMom));
   rep->momentum_iterations = (int)out[0];
   rep->momentum_residual = out[1];
   DN_TRY(copy_field(h, f[DN_F_U_STAR], f[DN_F_U]));
@@ -2297,6 +2722,10 @@ dn_status pressure_factor(dn_handle *h, bool split, bool icc) {
     k_factor<5><<<1, 1024, 0, h->stream>>>(SpOp{h->a5, (int)h->n, h->G.nx, h->G.ny, h->G.px, h->G.py}, F, kind,
                                             h->status);
     DN_TRY(check_launch(h, "k_factor<5>"));
+    if (h->capturing) {  // recorded: the status goes to the step record (a failed factor is reported after)
+      k_rec_copy<<<1, 32, 0, h->stream>>>(nullptr, 0, h->status, h->rec + kRecStep + kSPFactor);
+      return check_launch(h, "k_rec_copy");
+    }
     int st = 0;
     DN_TRY(read_status(h, &st));
     if (st == kDevFactorFailed) {
@@ -2325,13 +2754,13 @@ dn_status pressure_factor_solve(dn_handle *h, bool split, bool icc, dn_report *r
     rep->mixed_inner_multigrid = h->mixed_used_mg ? 1 : 0;
   } else if (h->sw5 > 0 && h->G.px) {
     DN_TRY((run_pcg<5, 4>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
-                          cfg.pressure_tolerance, out)));
+                          cfg.pressure_tolerance, out, h->rec + kRecStep + kSP)));
   } else if (h->sw5 > 0) {
     DN_TRY((run_pcg<5, 3>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
-                          cfg.pressure_tolerance, out)));
+                          cfg.pressure_tolerance, out, h->rec + kRecStep + kSP)));
   } else {
     DN_TRY((run_pcg<5, 0>(h, h->a5, h->l5, h->dinv5, kind, h->has_dirichlet ? 0 : 1, cfg.poisson_iterations,
-                          cfg.pressure_tolerance, out)));
+                          cfg.pressure_tolerance, out, h->rec + kRecStep + kSP)));
   }
   rep->pressure_iterations = (int)out[0];
   rep->pressure_residual = out[2];
@@ -2361,6 +2790,7 @@ dn_status correct(dn_handle *h, int step, dn_report *rep) {
   LAUNCH_INTERIOR(k_copy_interior, f[DN_F_P], f[DN_F_P], f[DN_F_P_CORR]);
   if (!h->has_dirichlet) DN_TRY(subtract_mean(h, f[DN_F_P]));
   DN_TRY(bc(h, f[DN_F_P], kBCPressure));
+  if (h->capturing) return DN_OK;  // the boundary speeds are read with the step record
   double bs[2];
   DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->scal + 16, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -2380,6 +2810,281 @@ dn_status begin_step(dn_handle *h) {
   return copy_field(h, f[DN_F_V_PREV], f[DN_F_V]);
 }
 
+dn_status diag_launch(dn_handle *h) {
+  Fv *f = h->f;
+  k_diag_partials<<<kDiagParts, 256, 0, h->stream>>>(f[DN_F_C], f[DN_F_U], f[DN_F_V], f[DN_F_MU], f[DN_F_RHO],
+                                                     f[DN_F_ETA], h->G, h->cfg.cn, h->partials);
+  return check_launch(h, "k_diag_partials");
+}
+
+// compute_diagnostics (diagnostics.cpp:114-167) from k_diag_partials' per-CTA values (host copy `part`)
+dn_status diag_finish(dn_handle *h, const double *part, dn_diag *d) {
+  const int nb = kDiagParts;
+  const int ops[kNDiag] = {0, 0, 1, 1, 1, 0, 2, 1, 2, 1, 0, 1, 1, 1};
+  double a[kNDiag];
+  for (int k = 0; k < kNDiag; ++k) {
+    a[k] = ops[k] == 0 ? 0.0 : (ops[k] == 1 ? -INFINITY : INFINITY);
+    for (int b = 0; b < nb; ++b) {
+      const double v = part[b * kNDiag + k];
+      a[k] = ops[k] == 0 ? a[k] + v : (ops[k] == 1 ? std::max(a[k], v) : std::min(a[k], v));
+    }
+  }
+  const dn_config &c = h->cfg;
+  std::memset(d, 0, sizeof(*d));
+  d->mass = a[0];
+  d->mass_drift = std::fabs(a[0] - h->initial_mass);
+  d->divergence_l2 = std::sqrt(a[1] / (double)(c.nx * c.ny));
+  d->max_divergence = std::max(0.0, a[2]);
+  d->max_abs_mu = std::max(0.0, a[3]);
+  d->max_velocity = std::max(0.0, a[4]);
+  d->kinetic_energy = a[5];
+  d->rho_min = a[6];
+  d->rho_max = std::max(0.0, a[7]);
+  d->eta_min = a[8];
+  d->eta_max = std::max(0.0, a[9]);
+  d->total_free_energy = a[10];
+  // populate_timestep_limits, diagnostics.cpp:48-112
+  const double h_ = std::min(h->G.dx, h->G.dy), tiny = 1.0e-30;
+  const double mar = std::max(0.0, a[11]);
+  d->dt_limit_advective = mar > tiny ? 0.5 / mar : INFINITY;
+  d->dt_limit_capillary = INFINITY;
+  d->dt_limit_ch_explicit = INFINITY;
+  if (solve_ch(c)) {
+    const double rs = std::max(d->rho_max, tiny);
+    d->dt_limit_capillary = 0.5 * std::sqrt(std::max(c.re * c.ca * h_ * h_ * h_ / rs, 0.0));
+    const double mob = std::max(0.0, a[12]), wpp = std::max(0.0, a[13]);
+    if (mob > tiny) {
+      const double coeff = 6.0 * kSqrt2 * mob * wpp / std::max(c.pe * c.cn, tiny);
+      d->dt_limit_ch_explicit = coeff > tiny ? 0.25 * h_ * h_ / coeff : INFINITY;
+    }
+  }
+  d->dt_limit_active = d->dt_limit_advective;
+  if (d->dt_limit_capillary < d->dt_limit_active) d->dt_limit_active = d->dt_limit_capillary;
+  if (d->dt_limit_ch_explicit < d->dt_limit_active) d->dt_limit_active = d->dt_limit_ch_explicit;
+  d->dt_limit_ratio = (!std::isfinite(d->dt_limit_active) || d->dt_limit_active <= tiny) ? 0.0 : c.dt / d->dt_limit_active;
+  if (!std::isfinite(d->mass_drift) || !std::isfinite(d->divergence_l2) || !std::isfinite(d->max_velocity) ||
+      !std::isfinite(d->max_abs_mu))
+    return fail(h, DN_ERR_NONFINITE, "non-finite diagnostic detected");
+  return DN_OK;
+}
+
+
+// ---- captured steps
+// A step with no host decision left -- the CH operator and its factor or hierarchy made for this alpha0, the
+// split operator's factor or hierarchy made, no pressure analysis, monitor or DCDM / Jacobi scheme -- is
+// recorded once into a CUDA graph: the solves' loops are conditional nodes, every result lands in h->rec
+// (read back once per step), the phase boundaries are event nodes.  Every kernel that depends on the step
+// index tests step == 0 only, so one recording serves every step >= 1.
+constexpr int kHostRec = 4096;   // pinned host copies of a replayed step: the record and boundary speeds,
+constexpr int kHostDiag = 4352;  // and the diagnostics partials
+
+bool step_capturable(const dn_handle *h, int step) {
+  const dn_config &c = h->cfg;
+  if (!h->graph_steps || !h->steady || step < 1) return false;
+  if (c.mode == DN_MODE_ADVECTION_ONLY || c.analysis_enabled || h->mon_cap > 0) return false;
+  if (c.pressure_scheme == DN_P_JACOBI || c.pressure_scheme == DN_P_SPLIT_DCDM_ICPCG) return false;
+  if (solve_ch(c)) {
+    const double alpha0 = 3.0 / (2.0 * c.dt);
+    if (!(std::fabs(alpha0 - h->ch_alpha0) <= 1.0e-14 * std::max(1.0, std::fabs(alpha0)))) return false;
+    if (h->ch_mg && c.precision == DN_PRECISION_MIXED && h->ch_mg_alpha0 != alpha0) return false;
+  }
+  if (use_split(c)) {
+    const int kind = c.pressure_scheme == DN_P_SPLIT_ICPCG ? kPrecICC : kPrecLDLT;
+    if (c.precision == DN_PRECISION_MIXED ? !h->mgp_split_ready : !(h->p_factor_valid && h->p_factor_kind == kind))
+      return false;
+  }
+  return true;
+}
+
+// dn_step's work with h->capturing set (nothing read back); rep receives the fields fixed at capture
+dn_status record_step(dn_handle *h, int step, dn_report *rep) {
+  std::memset(rep, 0, sizeof(*rep));
+  rep->ch_preconditioner = -1;
+  const long long before = h->launches;
+  h->step_dcn[0] = h->step_dcn[1] = DcNodes{};
+  h->step_retry = 0;
+  h->step = step;
+  DN_CUDA(h, cudaEventRecordWithFlags(h->ev[0], h->stream, cudaEventRecordExternal));
+  DN_TRY(begin_step(h));
+  DN_TRY(phase(h, step, rep));
+  DN_CUDA(h, cudaEventRecordWithFlags(h->ev[1], h->stream, cudaEventRecordExternal));
+  DN_TRY(momentum(h, step, rep));
+  DN_CUDA(h, cudaEventRecordWithFlags(h->ev[2], h->stream, cudaEventRecordExternal));
+  DN_TRY(pressure(h, step, rep));
+  DN_CUDA(h, cudaEventRecordWithFlags(h->ev[3], h->stream, cudaEventRecordExternal));
+  DN_TRY(correct(h, step, rep));
+  DN_CUDA(h, cudaEventRecordWithFlags(h->ev[4], h->stream, cudaEventRecordExternal));
+  DN_TRY(diag_launch(h));
+  // launches of one replay outside the loops (each loop body was recorded once)
+  long long bodies = 0;
+  for (const DcNodes &d : h->step_dcn) bodies += d.cycle + d.iter + d.ic + d.make;
+  bodies += h->step_retry;
+  h->step_nodes = h->launches - before - bodies;
+  h->launches = before;
+  return DN_OK;
+}
+
+dn_status ensure_step_graph(dn_handle *h, int step) {
+  if (h->step_exec && h->step_epoch == h->graph_epoch) return DN_OK;
+  if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  h->step_exec = nullptr;
+  DN_TRY(capture_exec(h, &h->step_exec, [&]() { return record_step(h, step, &h->step_rep); }));
+  h->step_epoch = h->graph_epoch;
+  return DN_OK;
+}
+
+// the copies a replayed step's results need, issued on `st` after the replay
+dn_status step_readback(dn_handle *h, cudaStream_t st) {
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + kHostRec, h->rec, kRecCount * sizeof(double), cudaMemcpyDeviceToHost, st));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + kHostRec + kRecCount, h->scal + 16, 2 * sizeof(double),
+                             cudaMemcpyDeviceToHost, st));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal + kHostDiag, h->partials, (size_t)kDiagParts * kNDiag * sizeof(double),
+                             cudaMemcpyDeviceToHost, st));
+  return DN_OK;
+}
+
+
+// The report, statuses and diagnostics of a replayed step from its record (after step_readback and a
+// synchronisation), as dn_step reports them.
+dn_status step_complete(dn_handle *h, int step, dn_report *rep) {
+  const dn_config &c = h->cfg;
+  const double *R = h->host_scal + kHostRec;
+  const double *S = R + kRecStep;
+  *rep = h->step_rep;
+  h->step = step;
+  for (int k = 0; k < 4; ++k) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, h->ev[k], h->ev[k + 1]);
+    h->phase_ms[k] = ms;
+  }
+  for (int k = 4; k < 8; ++k) h->phase_ms[k] = 0.0;
+  long long launches = h->step_nodes;
+  if (solve_ch(c)) {
+    if (rep->ch_preconditioner == 3) {
+      const double *C = R + kRecCh;
+      rep->ch_iterations = (int)C[kDcTotal];
+      rep->ch_residual = C[kDcIres];
+      launches += dc_launches(h->step_dcn[1], C);
+    } else {
+      const int st = (int)S[kSChPcg + 4];
+      if (st != kDevOk) return dev_status_to_dn(h, st);
+      rep->ch_iterations = (int)S[kSChPcg];
+      rep->ch_residual = S[kSChPcg + 3];
+      if (S[kSChRetry] != 0.0) {  // phase_field.cpp:468-473: the diagonal preconditioner from now on
+        launches += h->step_retry;
+        rep->ch_preconditioner = 2;
+        h->ch_prec = kPrecDiag;
+        ++h->graph_epoch;
+      }
+    }
+    rep->ch_equation_residual = S[kSChEq];
+  }
+  {
+    const int st = (int)S[kSMom + 4];
+    if (st != kDevOk) return dev_status_to_dn(h, st);
+    rep->momentum_iterations = (int)S[kSMom];
+    rep->momentum_residual = S[kSMom + 1];
+  }
+  const bool split = use_split(c);
+  const bool icc = c.pressure_scheme == DN_P_ICPCG || c.pressure_scheme == DN_P_SPLIT_ICPCG;
+  if (c.precision == DN_PRECISION_MIXED) {
+    const double *P = R + kRecPressure;
+    DN_TRY(dc_error(h, P, icc ? kPrecICC : kPrecLDLT));
+    rep->pressure_iterations = (int)P[kDcTotal];
+    rep->pressure_residual = P[kDcRel];
+    rep->refinement_cycles = (int)P[kDcCycles];
+    rep->mixed_inner_multigrid = P[kDcUsedMg0] != 0.0 ? 1 : 0;
+    h->refinement_cycles = rep->refinement_cycles;
+    h->mixed_used_mg = rep->mixed_inner_multigrid != 0;
+    launches += dc_launches(h->step_dcn[0], P);
+  } else {
+    if (!split && (int)S[kSPFactor] == kDevFactorFailed)
+      return fail(h, icc ? DN_ERR_ICC_FAILED : DN_ERR_ILDLT_FAILED,
+                  icc ? "ICC preconditioner construction failed" : "ILDLT preconditioner construction failed");
+    const int st = (int)S[kSP + 4];
+    if (st != kDevOk) return dev_status_to_dn(h, st);
+    rep->pressure_iterations = (int)S[kSP];
+    rep->pressure_residual = S[kSP + 2];
+  }
+  h->phase_ms[7] = rep->pressure_iterations;
+  rep->boundary_speed_pre = R[kRecCount];
+  rep->boundary_speed_post = R[kRecCount + 1];
+  h->launches += launches;
+  return diag_finish(h, h->host_scal + kHostDiag, &h->last_diag);
+}
+
+// one step replayed from the handle's graph (recorded on first use)
+dn_status graph_step(dn_handle *h, int step, dn_report *rep) {
+  DN_TRY(ensure_step_graph(h, step));
+  DN_CUDA(h, cudaGraphLaunch(h->step_exec, h->stream));
+  DN_TRY(step_readback(h, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));
+  return step_complete(h, step, rep);
+}
+
+// One step of every handle as one launch: each handle's step recorded as a branch of one graph (the handle's
+// stream joins the capture of the batch stream, records its step, and is joined back), captured once for
+// this list of handles and replayed; the results of every handle are read back with one synchronisation.
+dn_status batch_graph_step(dn_handle *const *hs, int count, const int *steps, dn_report *reports) {
+  dn_handle *o = hs[0];
+  dn_handle::BatchGraph &B = o->batch;
+  bool fresh = B.exec != nullptr && (int)B.uids.size() == count;
+  for (int a = 0; fresh && a < count; ++a)
+    fresh = B.uids[(size_t)a] == hs[a]->uid && B.epochs[(size_t)a] == hs[a]->graph_epoch;
+  if (!fresh) {
+    if (B.exec) cudaGraphExecDestroy(B.exec);
+    B.exec = nullptr;
+    if (!B.stream) DN_CUDA(o, cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking));
+    if (!B.fork) DN_CUDA(o, cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming));
+    DN_CUDA(o, cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+    dn_status st = DN_OK;
+    if (cudaEventRecord(B.fork, B.stream) != cudaSuccess) st = fail(o, DN_ERR_CUDA, "batch capture fork");
+    int joined = 0;
+    for (int a = 0; a < count && st == DN_OK; ++a) {
+      dn_handle *h = hs[a];
+      if (cudaStreamWaitEvent(h->stream, B.fork, 0) != cudaSuccess) {
+        st = fail(o, DN_ERR_CUDA, "batch capture join");
+        break;
+      }
+      h->capturing = true;
+      st = record_step(h, steps[a], &h->step_rep);
+      h->capturing = false;
+      if (cudaEventRecord(h->cap_ev, h->stream) != cudaSuccess || cudaStreamWaitEvent(B.stream, h->cap_ev, 0) != cudaSuccess)
+        if (st == DN_OK) st = fail(o, DN_ERR_CUDA, "batch capture rejoin");
+      ++joined;
+      if (st != DN_OK && h != o) o->err = h->err;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(B.stream, &g);
+    if (st != DN_OK || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return st != DN_OK ? st : fail(o, DN_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&B.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      B.exec = nullptr;
+      return fail(o, DN_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(ie));
+    }
+    (void)joined;
+    B.uids.assign((size_t)count, 0);
+    B.epochs.assign((size_t)count, 0);
+    for (int a = 0; a < count; ++a) {
+      B.uids[(size_t)a] = hs[a]->uid;
+      B.epochs[(size_t)a] = hs[a]->graph_epoch;
+    }
+  }
+  DN_CUDA(o, cudaGraphLaunch(B.exec, B.stream));
+  for (int a = 0; a < count; ++a) DN_TRY(step_readback(hs[a], B.stream));
+  DN_CUDA(o, cudaStreamSynchronize(B.stream));
+  dn_status first = DN_OK;
+  for (int a = 0; a < count; ++a) {
+    dn_report local{};
+    const dn_status st = step_complete(hs[a], steps[a], reports ? &reports[a] : &local);
+    if (st != DN_OK && first == DN_OK) first = st;
+  }
+  return first;
+}
 }  // namespace
 
 // ===================================================================================================
@@ -2448,8 +3153,15 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   h->cta_cap = std::max(1, h->num_sms / std::max(1, cfg->device_share));
   h->rows_per_cta = cfg->pcg_rows_per_cta > 0 ? cfg->pcg_rows_per_cta : kPcgRowsPerCta;
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
+  for (cudaStream_t &cs : h->cap_streams)
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
   for (auto &e : h->ev) cudaEventCreate(&e);
   for (auto &e : h->kev) cudaEventCreate(&e);
+  cudaEventCreateWithFlags(&h->cap_ev, cudaEventDisableTiming);
+  {
+    static std::atomic<long long> next_uid{0};
+    h->uid = ++next_uid;
+  }
 
   // grid and effective BCs (operators.cpp:36-112)
   h->G.nx = c.nx;
@@ -2527,6 +3239,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   A(dalloc(h, &h->prog, 2 * (size_t)kMaxBlocks * 8));
   A(dalloc(h, &h->partials, 2 * (size_t)kMaxBlocks * 8));
   A(dalloc(h, &h->scal, 64));
+  A(dalloc(h, &h->rec, kRecCount));
   A(dalloc(h, &h->prof, 64));
   if (s == DN_OK && cudaMallocHost(&h->host_scal, kHostScal * sizeof(double)) != cudaSuccess) s = DN_ERR_CUDA;
   if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
@@ -2598,6 +3311,11 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
     if (c.mixed_preconditioner == DN_MIXED_PREC_MULTIGRID) {
       A(mg_alloc(h, h->mgp, h->G.nx, h->G.ny, h->bc.p));
+      if (h->mgp.levels() > 0) {  // level 0 is the FP32 pressure operator, its CG's vectors and residual fy
+        h->mgp.lv[0].a64 = h->a5;
+        h->mgp.lv[0].a = h->fa5;
+        h->mgp.lv[0].r = h->fy;
+      }
       h->mgp.singular = h->has_dirichlet ? 0 : 1;
       A(dalloc(h, &h->mg_scal, 16));
       A(dalloc(h, &h->mg_part, 3 * (size_t)kMgParts));
@@ -2671,6 +3389,13 @@ dn_status dn_destroy(dn_handle *h) {
   if (!h) return DN_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (const dn_handle::MgGraph &g : h->mg_graphs) cudaGraphExecDestroy(g.exec);
+  for (dn_handle::SolveGraph &g : h->dc_graph)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  if (h->cap_ev) cudaEventDestroy(h->cap_ev);
+  if (h->batch.exec) cudaGraphExecDestroy(h->batch.exec);
+  if (h->batch.fork) cudaEventDestroy(h->batch.fork);
+  if (h->batch.stream) cudaStreamDestroy(h->batch.stream);
   for (void *p : h->allocations) cudaFree(p);
   if (h->mon) cudaFree(h->mon);
   if (h->host_scal) cudaFreeHost(h->host_scal);
@@ -2678,6 +3403,8 @@ dn_status dn_destroy(dn_handle *h) {
     if (e) cudaEventDestroy(e);
   for (auto &e : h->kev)
     if (e) cudaEventDestroy(e);
+  for (cudaStream_t cs : h->cap_streams)
+    if (cs) cudaStreamDestroy(cs);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return DN_OK;
@@ -3008,6 +3735,7 @@ dn_status dn_autotune_pressure(dn_handle *h, int *rows_per_cta, int *sweep_warps
       for (int sw : sws) {
         h->rows_per_cta = rows;
         h->sw5 = sw;
+        ++h->graph_epoch;  // recorded solves hold launch shapes
         dn_report rep{};
         cudaEventRecord(e0, h->stream);
         st = pressure(h, h->step, &rep);
@@ -3026,6 +3754,7 @@ dn_status dn_autotune_pressure(dn_handle *h, int *rows_per_cta, int *sweep_warps
   cudaEventDestroy(e1);
   h->rows_per_cta = st == DN_OK ? best_rows : rows0;
   h->sw5 = st == DN_OK ? best_sw : sw0;
+  ++h->graph_epoch;
   if (st != DN_OK) return st;
   if (rows_per_cta) *rows_per_cta = (int)best_rows;
   if (sweep_warps_per_cta) *sweep_warps_per_cta = best_sw;
@@ -3174,6 +3903,7 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
   if (!h) return DN_ERR_INVALID_ARGUMENT;
   dn_report local;
   if (!rep) rep = &local;
+  if (step_capturable(h, step)) return graph_step(h, step, rep);
   std::memset(rep, 0, sizeof(*rep));
   rep->ch_preconditioner = -1;
   h->step = step;
@@ -3210,7 +3940,15 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep) {
   }
   // the step ends with compute_diagnostics (solver.cpp:276); the reference's run loop aborts on a
   // non-finite one (solver.cpp:355-364), which here is the step's status DN_ERR_NONFINITE
-  return dn_diagnostics(h, &h->last_diag);
+  const dn_status ds = dn_diagnostics(h, &h->last_diag);
+  if (ds == DN_OK && step >= 1) h->steady = true;  // every operator, factor and hierarchy of a step >= 1 exists
+  return ds;
+}
+
+dn_status dn_set_step_graph(dn_handle *h, int enable) {
+  if (!h) return DN_ERR_INVALID_ARGUMENT;
+  h->graph_steps = enable != 0;
+  return DN_OK;
 }
 
 dn_status dn_last_diagnostics(dn_handle *h, dn_diag *d) {
@@ -3229,6 +3967,14 @@ dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, 
     if (!handles[a]) return DN_ERR_INVALID_ARGUMENT;
     for (int b2 = 0; b2 < a; ++b2)
       if (handles[b2] == handles[a]) return DN_ERR_INVALID_ARGUMENT;  // one handle twice would race with itself
+  }
+  // every handle replays captured steps and the step allows it: the whole batch is one graph launch
+  bool one_graph = count > 0 && steps != nullptr;
+  for (int a = 0; one_graph && a < count; ++a)
+    one_graph = step_capturable(handles[a], steps[a]) && handles[a]->device == handles[0]->device;
+  if (one_graph) {
+    if (cudaSetDevice(handles[0]->device) != cudaSuccess) return fail(handles[0], DN_ERR_CUDA, "cudaSetDevice failed");
+    return batch_graph_step(handles, count, steps, reports);
   }
   std::vector<dn_status> st;
   try {
@@ -3753,60 +4499,11 @@ dn_status dn_compute_mass(dn_handle *h, int field, double *mass) {
 
 dn_status dn_diagnostics(dn_handle *h, dn_diag *d) {
   if (!h || !d) return DN_ERR_INVALID_ARGUMENT;
-  const int nb = 128;
-  Fv *f = h->f;
-  k_diag_partials<<<nb, 256, 0, h->stream>>>(f[DN_F_C], f[DN_F_U], f[DN_F_V], f[DN_F_MU], f[DN_F_RHO], f[DN_F_ETA], h->G,
-                                             h->cfg.cn, h->partials);
-  DN_TRY(check_launch(h, "k_diag_partials"));
-  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->partials, (size_t)nb * kNDiag * sizeof(double), cudaMemcpyDeviceToHost,
-                             h->stream));
+  DN_TRY(diag_launch(h));
+  DN_CUDA(h, cudaMemcpyAsync(h->host_scal, h->partials, (size_t)kDiagParts * kNDiag * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
   DN_CUDA(h, cudaStreamSynchronize(h->stream));
-  const int ops[kNDiag] = {0, 0, 1, 1, 1, 0, 2, 1, 2, 1, 0, 1, 1, 1};
-  double a[kNDiag];
-  for (int k = 0; k < kNDiag; ++k) {
-    a[k] = ops[k] == 0 ? 0.0 : (ops[k] == 1 ? -INFINITY : INFINITY);
-    for (int b = 0; b < nb; ++b) {
-      const double v = h->host_scal[b * kNDiag + k];
-      a[k] = ops[k] == 0 ? a[k] + v : (ops[k] == 1 ? std::max(a[k], v) : std::min(a[k], v));
-    }
-  }
-  const dn_config &c = h->cfg;
-  std::memset(d, 0, sizeof(*d));
-  d->mass = a[0];
-  d->mass_drift = std::fabs(a[0] - h->initial_mass);
-  d->divergence_l2 = std::sqrt(a[1] / (double)(c.nx * c.ny));
-  d->max_divergence = std::max(0.0, a[2]);
-  d->max_abs_mu = std::max(0.0, a[3]);
-  d->max_velocity = std::max(0.0, a[4]);
-  d->kinetic_energy = a[5];
-  d->rho_min = a[6];
-  d->rho_max = std::max(0.0, a[7]);
-  d->eta_min = a[8];
-  d->eta_max = std::max(0.0, a[9]);
-  d->total_free_energy = a[10];
-  // populate_timestep_limits, diagnostics.cpp:48-112
-  const double h_ = std::min(h->G.dx, h->G.dy), tiny = 1.0e-30;
-  const double mar = std::max(0.0, a[11]);
-  d->dt_limit_advective = mar > tiny ? 0.5 / mar : INFINITY;
-  d->dt_limit_capillary = INFINITY;
-  d->dt_limit_ch_explicit = INFINITY;
-  if (solve_ch(c)) {
-    const double rs = std::max(d->rho_max, tiny);
-    d->dt_limit_capillary = 0.5 * std::sqrt(std::max(c.re * c.ca * h_ * h_ * h_ / rs, 0.0));
-    const double mob = std::max(0.0, a[12]), wpp = std::max(0.0, a[13]);
-    if (mob > tiny) {
-      const double coeff = 6.0 * kSqrt2 * mob * wpp / std::max(c.pe * c.cn, tiny);
-      d->dt_limit_ch_explicit = coeff > tiny ? 0.25 * h_ * h_ / coeff : INFINITY;
-    }
-  }
-  d->dt_limit_active = d->dt_limit_advective;
-  if (d->dt_limit_capillary < d->dt_limit_active) d->dt_limit_active = d->dt_limit_capillary;
-  if (d->dt_limit_ch_explicit < d->dt_limit_active) d->dt_limit_active = d->dt_limit_ch_explicit;
-  d->dt_limit_ratio = (!std::isfinite(d->dt_limit_active) || d->dt_limit_active <= tiny) ? 0.0 : c.dt / d->dt_limit_active;
-  if (!std::isfinite(d->mass_drift) || !std::isfinite(d->divergence_l2) || !std::isfinite(d->max_velocity) ||
-      !std::isfinite(d->max_abs_mu))
-    return fail(h, DN_ERR_NONFINITE, "non-finite diagnostic detected");
-  return DN_OK;
+  return diag_finish(h, h->host_scal, d);
 }
 
 dn_status dn_synchronize(dn_handle *h) {

@@ -342,10 +342,37 @@ __global__ void k_mg_coarse_inverse(const double *a, int nx, int ny, int px, int
 }
 
 // ---------------------------------------------------------------------------------------------------
-// CG on the FP32 operator of level 0.  Scalars live on the device (slots below); the host reads only the
-// residual norm of each iteration to decide when to stop.
+// CG on the FP32 operator of level 0.  Scalars and the loop control live on the device (slots below): the
+// iterations run inside a CUDA graph's conditional while node whose condition k_mgcg_ctrl sets, so the host
+// reads nothing until the whole solve has ended.
 // ---------------------------------------------------------------------------------------------------
-enum MgScal { kMgRz = 0, kMgPq = 1, kMgRr = 2, kMgAlpha = 3, kMgBeta = 4, kMgMeanZ = 5, kMgBad = 6 };
+enum MgScal {
+  kMgRz = 0, kMgPq = 1, kMgRr = 2, kMgAlpha = 3, kMgBeta = 4, kMgMeanZ = 5, kMgBad = 6,
+  kMgIt = 7,   // iterations of this inner solve
+  kMgCap = 8,  // its iteration limit
+  kMgScalCount = 16
+};
+
+// The record of one defect-correction solve (FP64 outer loop around FP32 inner solves), kDcSize doubles on
+// the device: what the host reads once the solve's graph has run, and the outer loop's own state.
+enum DcSlot {
+  kDcTotal = 0,    // inner iterations, all cycles
+  kDcCycles = 1,   // outer cycles
+  kDcAbs = 2,      // FP64 residual |b - A x| (projected when singular) of the last check
+  kDcRel = 3,      // the same relative to |b|
+  kDcPrev = 4,     // the residual of the previous cycle (a cycle that does not reduce it ends the multigrid)
+  kDcUseMg = 5,    // the next inner solve is the multigrid CG (else the IC/ILDLT persistent PCG)
+  kDcIres = 6,     // CH: the last correction's size relative to the iterate
+  kDcMean = 7,     // mean of the residual removed before the inner solve (singular systems)
+  kDcErr = 8,      // device status of a failed inner solve or factor (0: none)
+  kDcIcZero = 9,   // the IC inner solve returned without an iteration
+  kDcIcReady = 10, // the FP32 IC/ILDLT factor has been made in this solve
+  kDcStarted = 11, // the first check has run
+  kDcUsedMg0 = 12, // the solve started with the multigrid inner solver
+  kDcIcCycles = 13,// cycles run by the IC inner solver
+  kDcMgIts = 14,   // iterations run by the multigrid inner solver
+  kDcSize = 16
+};
 
 struct MgVec {
   SpOpT<float> A;
@@ -402,9 +429,10 @@ __global__ void k_mgp_rz(MgVec V) {
     V.part[3 * blockIdx.x + 2] = v[2];
   }
 }
-// p = (z - mean z) + beta p (first: p = z - mean z)
+// p = (z - mean z) + beta p (first: p = z - mean z; first < 0: the first iteration of the solve)
 __global__ void k_mgp_direction(MgVec V, int first) {
   const float beta = (float)V.scal[kMgBeta], mz = (float)V.scal[kMgMeanZ];
+  if (first < 0) first = V.scal[kMgIt] == 0.0 ? 1 : 0;
   const unsigned n = (unsigned)V.A.n;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
     V.p[t] = first ? V.z[t] - mz : (V.z[t] - mz) + beta * V.p[t];
@@ -413,10 +441,12 @@ __global__ void k_mgp_direction(MgVec V, int first) {
 //   mode 0 (after k_mgp_apply):  pq, alpha = rz / pq
 //   mode 1 (after k_mgp_update): rr
 //   mode 2 (after k_mgp_rz):     mean z, rz' (projected when singular), beta = rz' / rz (0 when first), rz = rz'
-// A non-positive or non-finite pq or rz' sets kMgBad (the host ends the inner solve).
+// A non-positive or non-finite pq or rz' sets kMgBad (k_mgcg_ctrl then ends the inner solve).  first < 0:
+// the first iteration of the solve.
 __global__ void k_mgp_scalars(const double *part, int nparts, double *scal, int mode, int first, int project,
                               double n) {
   const int lane = threadIdx.x;
+  if (first < 0) first = scal[kMgIt] == 0.0 ? 1 : 0;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int p = lane; p < nparts; p += 32) {
     s0 += part[3 * p];
@@ -443,6 +473,35 @@ __global__ void k_mgp_scalars(const double *part, int nparts, double *scal, int 
     scal[kMgBeta] = first ? 0.0 : rz / scal[kMgRz];
     scal[kMgRz] = rz;
   }
+}
+
+// Start of an inner solve: its scalars cleared and its iteration limit, the outer loop's budget left
+// (max(1, max_it - inner iterations so far)).  Sets the while node's condition.
+__global__ void k_mgcg_init(double *scal, const double *rec, int max_it, cudaGraphConditionalHandle loop) {
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < kMgScalCount; ++k) scal[k] = 0.0;
+  scal[kMgCap] = (double)max(1, max_it - (int)rec[kDcTotal]);
+  cudaGraphSetConditional(loop, 1u);
+}
+
+// End of one inner iteration (after the r.r reduction): counts it, and continues while no breakdown was
+// flagged, |r| / |b| >= tol (|b| = the outer residual the inner right-hand side was made from; a NaN ends
+// it) and the iteration limit is not reached.
+__global__ void k_mgcg_ctrl(double *scal, double *rec, double tol, cudaGraphConditionalHandle loop) {
+  if (threadIdx.x != 0) return;
+  const double it = scal[kMgIt] + 1.0;
+  scal[kMgIt] = it;
+  rec[kDcTotal] += 1.0;
+  rec[kDcMgIts] += 1.0;
+  bool more = it < scal[kMgCap];
+  if (scal[kMgBad] != 0.0) {
+    more = false;
+  } else {
+    const double rr = scal[kMgRr], b = rec[kDcAbs];  // std::max semantics: a NaN stays a NaN
+    const double rel = sqrt(rr < 0.0 ? 0.0 : rr) / (b < 1.0e-300 ? 1.0e-300 : b);
+    if (!(rel >= tol)) more = false;
+  }
+  cudaGraphSetConditional(loop, more ? 1u : 0u);
 }
 
 }  // namespace dn

@@ -103,9 +103,12 @@ def gather_records(dist, mine, records) -> list:
 class ShardedEnsemble:
     """This rank's share of a ragged batch: one handle per instance, stepped together by dn_step_batch.
     Within the rank each handle's persistent grids take SMs in proportion to its cells (device_share =
-    the rank's cells / its cells), or an equal share with `proportional=False`."""
+    the rank's cells / its cells), or an equal share with `proportional=False`.  With `step_graph` every
+    handle replays captured steps, so that from the second step of index >= 1 on a batch step is one CUDA
+    graph launch holding every instance's step (dn_step_batch)."""
 
-    def __init__(self, cfgs: list, rank: int = 0, world: int = 1, device: int = 0, proportional: bool = True):
+    def __init__(self, cfgs: list, rank: int = 0, world: int = 1, device: int = 0, proportional: bool = True,
+                 step_graph: bool = False):
         self.cfgs = list(cfgs)
         self.parts = lpt_partition([estimated_cost(c) for c in self.cfgs], world)
         self.mine = self.parts[rank]
@@ -116,6 +119,8 @@ class ShardedEnsemble:
             for i, n in zip(self.mine, cells):
                 share = max(1, round(total / n)) if proportional else max(1, len(self.mine))
                 self.members.append(capi.Solver(dict(self.cfgs[i], device_share=share), device=device))
+                if step_graph:
+                    self.members[-1].set_step_graph(True)
         except Exception:
             self.close()
             raise

@@ -178,8 +178,20 @@ dn_status dn_step(dn_handle *h, int step, dn_report *rep);
  * reports (NULL allowed) receives one dn_report per handle.  Each handle's result equals its dn_step alone.
  * Returns the first failing handle's status (its message via dn_last_error).  The CUDA runtime maps streams
  * onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 unless the environment sets it before the process
- * creates its CUDA context; up to 32), and streams that share a queue serialise. */
+ * creates its CUDA context; up to 32), and streams that share a queue serialise.  When every handle has
+ * captured steps enabled (dn_set_step_graph) and its step can be captured, the batch is instead one CUDA
+ * graph holding every handle's step as a branch, recorded on the first such call for this list of handles
+ * and launched once per call. */
 dn_status dn_step_batch(dn_handle *const *handles, int count, const int *steps, dn_report *reports);
+/* Captured steps (no reference counterpart): with enable != 0, a step of index >= 1 that follows an eager
+ * step of index >= 1 is recorded once into a CUDA graph and replayed from then on.  The graph holds every
+ * launch of the step; the loops of the solves run on the device as conditional graph nodes, whose
+ * conditions kernels set from the same residual checks as the eager step.  The host reads the step's
+ * results once, after the replay.  Results, iteration counts and reports equal the eager step's.  Steps
+ * that need host decisions run eagerly: step 0; a changed CH operator; the DCDM and Jacobi schemes; the
+ * pressure analysis; an active pressure monitor.  A launch-shape change (dn_autotune_pressure) records the
+ * step again. */
+dn_status dn_set_step_graph(dn_handle *h, int enable);
 /* history copies at the start of advance_one_timestep (solver.cpp:225-231) */
 dn_status dn_begin_step(dn_handle *h, int step);
 /* Solver::advance_phase_state (phase_field.cpp:258-281): CH solve, materials, surface force */
