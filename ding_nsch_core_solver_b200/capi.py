@@ -51,6 +51,7 @@ class Config(C.Structure):
         ("mixed_inner_tolerance", C.c_double), ("device_share", C.c_int), ("dcdm_direction_mode", C.c_int),
         ("dcdm_history_size", C.c_int), ("dcdm_max_stored_directions", C.c_int), ("dcdm_restart_interval", C.c_int),
         ("pcg_rows_per_cta", C.c_int), ("sweep_warps_per_cta", C.c_int), ("device_wait_limit", C.c_int), ("mixed_preconditioner", C.c_int),
+        ("mg_cluster_cells", C.c_int),
         ("analysis_enabled", C.c_int), ("analysis_mode", C.c_int), ("analysis_trigger_step", C.c_int),
         ("analysis_interface_band_multiplier", C.c_double), ("name", C.c_char * 128), ("output_dir", C.c_char * 512),
         ("analysis_case_group", C.c_char * 128), ("analysis_initial_guess", C.c_char * 64),

@@ -505,6 +505,7 @@ struct MgHier {
   std::vector<Lv> lv;
   float *inv = nullptr;  // the coarsest level's inverse
   int *flag = nullptr;
+  MgChain *dchain = nullptr;  // the levels as one device record (the cluster inner solve reads it)
   MgFold fold{};
   double mass = 0.0;  // uniform diagonal term of level 0 (CH: the shift s)
   int singular = 0;   // pure-Neumann / periodic pressure: shift the coarsest matrix's null space away
@@ -622,6 +623,7 @@ struct dn_handle {
   };
   SolveGraph dc_graph[2];
   bool ch_mg_ok = false;  // the (K + s I) hierarchy built for ch_mg_alpha0 is usable
+  long long mg_cluster_cells = kMgClusterCells;  // level-0 grids this small: each inner CG is one cluster launch
   // captured steps (dn_set_step_graph): the step recorded once into a graph and replayed
   bool graph_steps = false;  // replay captured steps where the step allows it
   bool steady = false;       // an eager step with step >= 1 has made every operator, factor and hierarchy
@@ -1095,6 +1097,21 @@ MgLevel mg_level(const MgHier &H, int l) {
   return MgLevel{m.a, m.x, m.b, m.r, m.nx, m.ny};
 }
 
+// H's levels (fixed once its level 0 is set) as one device record, for the cluster inner solve
+dn_status mg_upload_chain(dn_handle *h, MgHier &H) {
+  if (H.levels() == 0) return DN_OK;
+  MgChain ch{};
+  for (int l = 0; l < H.levels(); ++l) ch.lv[l] = mg_level(H, l);
+  ch.first = 0;
+  ch.last = H.levels() - 1;
+  ch.fold = H.fold;
+  ch.inv = H.inv;
+  DN_TRY(dalloc(h, &H.dchain, 1));
+  DN_CUDA(h, cudaMemcpyAsync(H.dchain, &ch, sizeof(ch), cudaMemcpyHostToDevice, h->stream));
+  DN_CUDA(h, cudaStreamSynchronize(h->stream));  // `ch` lives on this stack frame
+  return DN_OK;
+}
+
 // Levels 1.. of a hierarchy whose level 0 is an nx x ny grid: halve both extents while they are even and >= 4
 // and the level is larger than the direct coarse solve.  Leaves H empty when the grid never gets there.
 dn_status mg_alloc(dn_handle *h, MgHier &H, int nx, int ny, const BCSide *sides) {
@@ -1341,6 +1358,47 @@ template <int S>
 dn_status rec_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tmp, int vcycles, int project,
                      int max_it, double tol, double *R, DcNodes *nodes) {
   const long long n = V.A.n;
+  // the bottom levels (the first of at most kMgBottomCells cells and the coarser ones) of the cluster form, in
+  // shared memory: 3 floats per cell
+  int bottom = H.levels() - 1;
+  while (bottom > 0 && (long long)H.lv[bottom - 1].nx * H.lv[bottom - 1].ny <= kMgBottomCells) --bottom;
+  size_t bottom_smem = 0;
+  for (int l = bottom; l < H.levels(); ++l) bottom_smem += 3 * sizeof(float) * (size_t)H.lv[l].nx * H.lv[l].ny;
+  if (n <= h->mg_cluster_cells && bottom_smem <= (size_t)kMgClusterSmemMax) {  // one cluster launch
+    if (!H.dchain) return fail(h, DN_ERR_INVALID_ARGUMENT, "multigrid levels not uploaded");
+    MgClusterArgs P{};
+    P.bottom = bottom;
+    P.ch = H.dchain;
+    P.A = V.A;
+    P.x = V.x;
+    P.r = V.r;
+    P.z = V.z;
+    P.p = V.p;
+    P.q = V.q;
+    P.tmp = tmp;
+    P.b = b;
+    P.vcycles = vcycles;
+    P.project = project;
+    P.max_it = max_it;
+    P.tol = tol;
+    P.R = R;
+    // about 4 cells per thread on level 0, at most the portable cluster size
+    const unsigned cs = (unsigned)std::min<long long>(kMgClusterMax, std::max<long long>(1, (n + 4095) / 4096));
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(cs);
+    lc.blockDim = dim3(kMgClusterThreads);
+    lc.dynamicSmemBytes = bottom_smem;
+    lc.stream = h->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    DN_CUDA(h, cudaLaunchKernelEx(&lc, k_mgcg_cluster<S>, P));
+    return check_launch(h, "k_mgcg_cluster");
+  }
   V.part = h->mg_part;
   V.scal = h->mg_scal;
   const int nb = (int)std::min<long long>({(long long)kMgParts, 4LL * h->num_sms, (long long)blocks_for(n)});
@@ -3152,6 +3210,7 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
   h->num_sms = prop.multiProcessorCount;
   h->cta_cap = std::max(1, h->num_sms / std::max(1, cfg->device_share));
   h->rows_per_cta = cfg->pcg_rows_per_cta > 0 ? cfg->pcg_rows_per_cta : kPcgRowsPerCta;
+  h->mg_cluster_cells = cfg->mg_cluster_cells > 0 ? cfg->mg_cluster_cells : kMgClusterCells;
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
   for (cudaStream_t &cs : h->cap_streams)
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return bad(DN_ERR_CUDA, "stream");
@@ -3297,6 +3356,9 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
     A(dalloc(h, &h->dcdm_adirs, (size_t)h->dcdm_keep * h->n));
     if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
   }
+  // the cluster form of the multigrid inner CG keeps its bottom levels in shared memory
+  for (const void *k : {(const void *)k_mgcg_cluster<5>, (const void *)k_mgcg_cluster<13>})
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMgClusterSmemMax);
   // the preconditioner-only kernel (DCDM directions, the pressure analysis) may use shared memory as k_pcg does
   for (const void *k : {(const void *)k_prec_apply<3>, (const void *)k_prec_apply<4>}) {
     cudaFuncAttributes fa{};
@@ -3339,6 +3401,9 @@ dn_status dn_create(const dn_config *cfg, int device, dn_handle **out) {
           h->ch_mg = true;
         }
       }
+      if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
+      A(mg_upload_chain(h, h->mgp));
+      A(mg_upload_chain(h, h->mgc));
       if (s != DN_OK) return bad(s, "device allocation failed: " + h->err);
     }
     const int optin = h->smem_optin;

@@ -111,6 +111,7 @@ extern "C" void dn_config_default(dn_config *c) {
   c->pcg_rows_per_cta = 0;     // 512
   c->sweep_warps_per_cta = 0;  // as many as the shared memory holds, up to 4
   c->device_wait_limit = 0;    // kSpinLimit polls
+  c->mg_cluster_cells = 0;     // off
   c->mixed_preconditioner = DN_MIXED_PREC_MULTIGRID;
   c->analysis_enabled = 0;     // config.hpp:53-133
   c->analysis_mode = DN_ANALYSIS_OFF;
@@ -260,6 +261,7 @@ extern "C" dn_status dn_config_parse(const char *text, dn_config *cfg, char *err
     geti("pcg_rows_per_cta", cfg->pcg_rows_per_cta);
     geti("sweep_warps_per_cta", cfg->sweep_warps_per_cta);
     geti("device_wait_limit", cfg->device_wait_limit);
+    geti("mg_cluster_cells", cfg->mg_cluster_cells);
     if (cfg->device_wait_limit < 0) throw std::runtime_error("device_wait_limit must be non-negative (0: the default)");
     if (kv.count("dcdm_direction_mode")) {  // pressure.cpp:383-395
       const std::string m = lower(kv["dcdm_direction_mode"]);

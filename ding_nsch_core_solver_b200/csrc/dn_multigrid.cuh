@@ -25,6 +25,8 @@
 // SpMV accumulate in FP32; the CG dot products and norms accumulate in FP64.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "dn_common.cuh"
 #include "dn_krylov.cuh"
 
@@ -502,6 +504,340 @@ __global__ void k_mgcg_ctrl(double *scal, double *rec, double tol, cudaGraphCond
     if (!(rel >= tol)) more = false;
   }
   cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// The inner CG as one thread-block cluster (level-0 grids up to mg_cluster_cells cells).  Small grids leave a
+// full-device launch per phase latency-bound: a V-cycle is about 11 launches per level, each a few
+// microseconds for a few thousand cells.  Here 1-8 CTAs of 1024 threads, which the hardware schedules
+// together, run every iteration of the solve: V-cycles, r.z, direction, A p, p.q and the update as phases
+// separated by cluster barriers (barrier.cluster with release / acquire, which orders the global memory the
+// phases exchange), dot products reduced through distributed shared memory in rank order, so every CTA holds
+// the same scalars and takes the same stopping decision.  One launch per inner solve; nothing waits on
+// another launch or spins.  The cell arithmetic is the per-phase kernels' (mg_*_at), phase for phase.
+// ---------------------------------------------------------------------------------------------------
+constexpr int kMgClusterThreads = 1024;
+constexpr int kMgClusterMax = 8;              // CTAs per cluster at most (the portable cluster size)
+constexpr long long kMgClusterCells = 0;  // default: off (set from measurements)
+constexpr int kMgClusterSmemMax = 160 * 1024;  // dynamic shared memory of the bottom levels at most
+
+struct MgClusterArgs {
+  const MgChain *ch;     // levels 0 .. last of the preconditioner's hierarchy, in device memory (lv[0].b / .x
+                         // are replaced per V-cycle)
+  SpOpT<float> A;        // the CG operator on level 0 (the 5-point pressure or the 13-point CH operator)
+  float *x, *r, *z, *p, *q, *tmp;
+  const float *b;        // the inner right-hand side (x is zero on entry)
+  int vcycles, project, max_it;
+  int bottom;            // the first level of at most kMgBottomCells cells: it and the coarser ones run on CTA 0
+                         // in shared memory (3 floats per cell of those levels, dynamic)
+  double tol;            // relative to |b| = R[kDcAbs]
+  double *R;             // the defect-correction record: iterations added to kDcTotal and kDcMgIts
+};
+
+__device__ __forceinline__ void mgc_sync() { cooperative_groups::this_cluster().sync(); }
+
+// K sums over the cluster: the CTA's sums, then every CTA adds the CTAs' sums in rank order (warp 0 reads
+// them from distributed shared memory), so all threads of all CTAs hold the same bits.  `slot` alternates
+// by `par` so that a CTA writing the next reduction never overwrites sums another CTA is still reading.
+template <int K>
+__device__ __forceinline__ void mgc_sum(double (&v)[K], double *sh, double (*slot)[4], double *bc, int &par) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  block_sum<K>(v, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) slot[par][k] = v[k];
+  }
+  cl.sync();
+  if (threadIdx.x == 0) {
+    const unsigned cs = cl.num_blocks();
+#pragma unroll
+    for (int k = 0; k < K; ++k) bc[k] = 0.0;
+    for (unsigned j = 0; j < cs; ++j) {
+      const double *o = cl.map_shared_rank(&slot[par][0], j);
+#pragma unroll
+      for (int k = 0; k < K; ++k) bc[k] += o[k];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = bc[k];
+  __syncthreads();
+  par ^= 1;
+}
+
+// The off-diagonal sum of mg_row_sum for up to kMgBatch cells at once: every load of the batch is issued
+// before any sum is formed (the neighbours' x values do not wait for the coefficients), then each cell's sum
+// is taken in slot order over its non-zero coefficients, as mg_row_sum takes it.
+constexpr int kMgBatch = 4;
+__device__ __forceinline__ void mg_row_sums(const MgLevel &L, const float *x, const int (&ci)[kMgBatch],
+                                            const int (&cj)[kMgBatch], const bool (&on)[kMgBatch], long long n,
+                                            int px, int py, float (&out)[kMgBatch]) {
+  constexpr int ks[4] = {0, 1, 3, 4};
+  float av[kMgBatch][4], xv[kMgBatch][4];
+#pragma unroll
+  for (int u = 0; u < kMgBatch; ++u) {
+    const long long r = (long long)ci[u] * L.ny + cj[u];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      av[u][q] = 0.0f;
+      xv[u][q] = 0.0f;
+      if (on[u]) {
+        const long long c = slot_col<5>(ci[u], cj[u], ks[q], L.nx, L.ny, px, py);
+        av[u][q] = __ldg(&L.a[(size_t)ks[q] * n + r]);
+        if (c >= 0) xv[u][q] = x[c];
+        else av[u][q] = 0.0f;  // mg_row_sum skips a missing neighbour
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kMgBatch; ++u) {
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (av[u][q] != 0.0f) s += av[u][q] * xv[u][q];
+    out[u] = s;
+  }
+}
+
+// mg_smooth_at for the cells t0, t0 + st, ... (kMgBatch of them, those below lim): one colour, so no cell of
+// the batch reads another's x, and all loads go before the stores.  The arithmetic is mg_smooth_at's.
+__device__ __forceinline__ void mg_smooth_batch(const MgLevel &L, int color, int first, int px, int py, unsigned t0,
+                                                unsigned st, unsigned lim) {
+  const int half = L.ny >> 1;
+  const long long n = (long long)L.nx * L.ny;
+  int ci[kMgBatch], cj[kMgBatch];
+  bool on[kMgBatch];
+  float bv[kMgBatch], dv[kMgBatch], rs[kMgBatch];
+#pragma unroll
+  for (int u = 0; u < kMgBatch; ++u) {
+    const unsigned t = t0 + (unsigned)u * st;
+    on[u] = t < lim;
+    const unsigned tt = on[u] ? t : 0u;
+    ci[u] = (int)(tt / (unsigned)half);
+    cj[u] = 2 * (int)(tt - (unsigned)ci[u] * (unsigned)half) + ((ci[u] + color) & 1);
+    const long long r = (long long)ci[u] * L.ny + cj[u];
+    bv[u] = on[u] ? L.b[r] : 0.0f;
+    dv[u] = on[u] ? __ldg(&L.a[2 * n + r]) : 1.0f;
+  }
+  if (!first) mg_row_sums(L, L.x, ci, cj, on, n, px, py, rs);
+#pragma unroll
+  for (int u = 0; u < kMgBatch; ++u) {
+    if (!on[u]) continue;
+    const long long r = (long long)ci[u] * L.ny + cj[u];
+    float s = bv[u];
+    if (!first) s -= rs[u];
+    L.x[r] = s / dv[u];
+    if (first) L.x[(long long)ci[u] * L.ny + (cj[u] ^ 1)] = 0.0f;
+  }
+}
+
+// mg_residual_at for a batch of cells, loads before stores (r is written, x only read)
+__device__ __forceinline__ void mg_residual_batch(const MgLevel &L, int px, int py, unsigned t0, unsigned st,
+                                                  unsigned lim) {
+  const long long n = (long long)L.nx * L.ny;
+  int ci[kMgBatch], cj[kMgBatch];
+  bool on[kMgBatch];
+  float bv[kMgBatch], dv[kMgBatch], xc[kMgBatch], rs[kMgBatch];
+#pragma unroll
+  for (int u = 0; u < kMgBatch; ++u) {
+    const unsigned t = t0 + (unsigned)u * st;
+    on[u] = t < lim;
+    const unsigned tt = on[u] ? t : 0u;
+    ci[u] = (int)(tt / (unsigned)L.ny);
+    cj[u] = (int)(tt - (unsigned)ci[u] * (unsigned)L.ny);
+    bv[u] = on[u] ? L.b[tt] : 0.0f;
+    dv[u] = on[u] ? __ldg(&L.a[2 * n + tt]) : 0.0f;
+    xc[u] = on[u] ? L.x[tt] : 0.0f;
+  }
+  mg_row_sums(L, L.x, ci, cj, on, n, px, py, rs);
+#pragma unroll
+  for (int u = 0; u < kMgBatch; ++u)
+    if (on[u]) L.r[t0 + (unsigned)u * st] = bv[u] - (dv[u] * xc[u] + rs[u]);
+}
+
+// Levels `first` .. last of C in one CTA with __syncthreads between phases (k_mg_bottom's order of phases);
+// lv: the levels with their x, b, r (in shared memory for the cluster form).
+__device__ void mg_bottom_cta(const MgChain &C, const MgLevel *lv, int first) {
+  const unsigned tid = threadIdx.x, nt = blockDim.x;
+  const int px = C.fold.px, py = C.fold.py, last = C.last;
+  for (int l = first; l < last; ++l) {
+    const MgLevel &F = lv[l], &Cl = lv[l + 1];
+    const unsigned nf = (unsigned)F.nx * (unsigned)F.ny, nh = nf >> 1, nc = (unsigned)Cl.nx * (unsigned)Cl.ny;
+    for (int k = 0; k < kMgSweeps; ++k) {
+      for (unsigned t = tid; t < nh; t += kMgBatch * nt) mg_smooth_batch(F, 0, k == 0, px, py, t, nt, nh);
+      __syncthreads();
+      for (unsigned t = tid; t < nh; t += kMgBatch * nt) mg_smooth_batch(F, 1, 0, px, py, t, nt, nh);
+      __syncthreads();
+    }
+    for (unsigned t = tid; t < nf; t += kMgBatch * nt) mg_residual_batch(F, px, py, t, nt, nf);
+    __syncthreads();
+    for (unsigned t = tid; t < nc; t += nt) mg_restrict_at(F, Cl, C.fold, t);
+    __syncthreads();
+  }
+  {
+    const MgLevel &L = lv[last];
+    const int n = L.nx * L.ny;
+    for (int i = (int)tid; i < n; i += (int)nt) {  // inv is symmetric: thread i reads column i
+      float s = 0.0f;
+      for (int k = 0; k < n; ++k) s += __ldg(&C.inv[(size_t)k * n + i]) * L.b[k];
+      L.x[i] = s;
+    }
+    __syncthreads();
+  }
+  for (int l = last - 1; l >= first; --l) {
+    const MgLevel &F = lv[l], &Cl = lv[l + 1];
+    const unsigned nf = (unsigned)F.nx * (unsigned)F.ny, nh = nf >> 1;
+    for (unsigned t = tid; t < nf; t += nt) mg_prolong_at(Cl, F, C.fold, t);
+    __syncthreads();
+    for (int k = 0; k < kMgSweeps; ++k) {
+      for (unsigned t = tid; t < nh; t += kMgBatch * nt) mg_smooth_batch(F, 1, 0, px, py, t, nt, nh);
+      __syncthreads();
+      for (unsigned t = tid; t < nh; t += kMgBatch * nt) mg_smooth_batch(F, 0, 0, px, py, t, nt, nh);
+      __syncthreads();
+    }
+  }
+}
+
+// One V-cycle x0 = B b0 over every level of `C`.  The levels above `bf` (the first of at most kMgBottomCells
+// cells) run on the whole cluster, its threads striding over each phase's cells in batches, with a cluster
+// barrier between phases.  The levels from bf down run on CTA 0 alone with their x, b, r in shared memory
+// (`smem`, 3 x their cells floats), entered with level bf's b and left with its x through global memory.
+__device__ void mgc_vcycle(const MgChain &C, int bf, float *smem, MgLevel *s_lv, float *b0, float *x0, unsigned gt,
+                           unsigned GT) {
+  const int px = C.fold.px, py = C.fold.py, last = C.last;
+  auto level = [&](int l) {
+    MgLevel L = C.lv[l];
+    if (l == 0) {
+      L.b = b0;
+      L.x = x0;
+    }
+    return L;
+  };
+  for (int l = 0; l < bf; ++l) {
+    const MgLevel F = level(l), Cl = level(l + 1);
+    const unsigned nf = (unsigned)F.nx * (unsigned)F.ny, nh = nf >> 1, nc = (unsigned)Cl.nx * (unsigned)Cl.ny;
+    for (int k = 0; k < kMgSweeps; ++k) {
+      for (unsigned t = gt; t < nh; t += kMgBatch * GT) mg_smooth_batch(F, 0, k == 0, px, py, t, GT, nh);
+      mgc_sync();
+      for (unsigned t = gt; t < nh; t += kMgBatch * GT) mg_smooth_batch(F, 1, 0, px, py, t, GT, nh);
+      mgc_sync();
+    }
+    for (unsigned t = gt; t < nf; t += kMgBatch * GT) mg_residual_batch(F, px, py, t, GT, nf);
+    mgc_sync();
+    for (unsigned t = gt; t < nc; t += GT) mg_restrict_at(F, Cl, C.fold, t);
+    mgc_sync();
+  }
+  if (cooperative_groups::this_cluster().block_rank() == 0) {
+    if (threadIdx.x == 0) {  // the bottom levels' table, their vectors in shared memory
+      float *q = smem;
+      for (int l = bf; l <= last; ++l) {
+        MgLevel L = C.lv[l];
+        const unsigned nl = (unsigned)L.nx * (unsigned)L.ny;
+        L.x = q;
+        L.b = q + nl;
+        L.r = q + 2 * nl;
+        q += 3 * nl;
+        s_lv[l] = L;
+      }
+    }
+    __syncthreads();
+    const MgLevel E = level(bf);  // the entry level's global b and x
+    const unsigned ne = (unsigned)E.nx * (unsigned)E.ny;
+    float *eb = s_lv[bf].b;
+    for (unsigned t = threadIdx.x; t < ne; t += blockDim.x) eb[t] = E.b[t];
+    __syncthreads();
+    mg_bottom_cta(C, s_lv, bf);
+    const float *ex = s_lv[bf].x;
+    for (unsigned t = threadIdx.x; t < ne; t += blockDim.x) E.x[t] = ex[t];
+  }
+  mgc_sync();
+  for (int l = bf - 1; l >= 0; --l) {
+    const MgLevel F = level(l), Cl = level(l + 1);
+    const unsigned nf = (unsigned)F.nx * (unsigned)F.ny, nh = nf >> 1;
+    for (unsigned t = gt; t < nf; t += GT) mg_prolong_at(Cl, F, C.fold, t);
+    mgc_sync();
+    for (int k = 0; k < kMgSweeps; ++k) {
+      for (unsigned t = gt; t < nh; t += kMgBatch * GT) mg_smooth_batch(F, 1, 0, px, py, t, GT, nh);
+      mgc_sync();
+      for (unsigned t = gt; t < nh; t += kMgBatch * GT) mg_smooth_batch(F, 0, 0, px, py, t, GT, nh);
+      mgc_sync();
+    }
+  }
+}
+
+// The whole inner solve: r = b; per iteration z = M r (vcycles V-cycles, through tmp when two), r.z (the
+// mean of z removed when the system is singular), p = (z - mean z) + beta p, q = A p, alpha = r.z / p.q,
+// x += alpha p, r -= alpha q; it ends as k_mgcg_ctrl ends the per-phase form: a non-positive or non-finite
+// r.z or p.q, |r| < tol |b|, or the iteration budget left in R (at least one iteration).
+template <int S>
+__global__ void __launch_bounds__(kMgClusterThreads, 1) k_mgcg_cluster(const MgClusterArgs P) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned gt = cl.block_rank() * blockDim.x + threadIdx.x, GT = cl.num_blocks() * blockDim.x;
+  __shared__ double sh[3 * 32];
+  __shared__ double slot[2][4];
+  __shared__ double bc[4];
+  __shared__ MgLevel s_lv[kMgMaxLevels];
+  extern __shared__ float mgc_smem[];
+  int par = 0;
+  const unsigned n = (unsigned)P.A.n, ny = (unsigned)P.A.ny;
+  const double bnorm = P.R[kDcAbs];
+  const int cap = max(1, P.max_it - (int)P.R[kDcTotal]);
+  for (unsigned t = gt; t < n; t += GT) P.r[t] = P.b[t];
+  mgc_sync();
+  double rz_old = 0.0;
+  int it = 0;
+  for (;;) {
+    if (P.vcycles == 2) {
+      mgc_vcycle(*P.ch, P.bottom, mgc_smem, s_lv, P.r, P.tmp, gt, GT);
+      mgc_vcycle(*P.ch, P.bottom, mgc_smem, s_lv, P.tmp, P.z, gt, GT);
+    } else {
+      mgc_vcycle(*P.ch, P.bottom, mgc_smem, s_lv, P.r, P.z, gt, GT);
+    }
+    double v3[3] = {0.0, 0.0, 0.0};
+    for (unsigned t = gt; t < n; t += GT) {
+      const double z = P.z[t], r = P.r[t];
+      v3[0] += r * z;
+      v3[1] += z;
+      v3[2] += r;
+    }
+    mgc_sum<3>(v3, sh, slot, bc, par);
+    const double mz = P.project ? v3[1] / (double)n : 0.0;
+    const double rz = P.project ? v3[0] - mz * v3[2] : v3[0];
+    bool bad = !(rz > 0.0) || !isfinite(rz);
+    const float beta = it == 0 ? 0.0f : (float)(rz / rz_old), fmz = (float)mz;
+    rz_old = rz;
+    for (unsigned t = gt; t < n; t += GT) P.p[t] = it == 0 ? P.z[t] - fmz : (P.z[t] - fmz) + beta * P.p[t];
+    mgc_sync();
+    double v1[1] = {0.0};
+    for (unsigned t = gt; t < n; t += GT) {
+      const int i = (int)(t / ny), j = (int)(t - (unsigned)i * ny);
+      const float s = spmv_row<S>(P.A, P.p, i, j);
+      P.q[t] = s;
+      v1[0] += (double)P.p[t] * (double)s;
+    }
+    mgc_sum<1>(v1, sh, slot, bc, par);
+    if (!(v1[0] > 0.0) || !isfinite(v1[0])) bad = true;
+    const float alpha = (float)(rz / v1[0]);
+    double v2[1] = {0.0};
+    for (unsigned t = gt; t < n; t += GT) {
+      P.x[t] += alpha * P.p[t];
+      const float r = P.r[t] - alpha * P.q[t];
+      P.r[t] = r;
+      v2[0] += (double)r * (double)r;
+    }
+    mgc_sum<1>(v2, sh, slot, bc, par);
+    ++it;
+    // std::max semantics, as k_mgcg_ctrl: a NaN ends the solve
+    const double rr = v2[0], rel = sqrt(rr < 0.0 ? 0.0 : rr) / (bnorm < 1.0e-300 ? 1.0e-300 : bnorm);
+    if (bad || !(rel >= P.tol) || it >= cap) break;
+  }
+  if (gt == 0) {
+    P.R[kDcTotal] += (double)it;
+    P.R[kDcMgIts] += (double)it;
+  }
+  mgc_sync();  // no CTA leaves while another may still read its shared memory
 }
 
 }  // namespace dn

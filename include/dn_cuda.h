@@ -97,6 +97,9 @@ typedef struct {
                                       the CH solve also runs the mixed form (FP32 CG, two V-cycles of the
                                       shifted Laplacian K + sqrt(alpha0/beta2) I as preconditioner); with 1 it
                                       stays FP64 ILDLT-PCG */
+  int mg_cluster_cells;            /* level-0 grids up to this many cells run each multigrid inner CG solve as
+                                      one thread-block cluster launch (0 or negative: never, a launch per
+                                      phase recorded in the solve's graph) */
   /* pressure analysis (config.hpp:36-133; run_pressure_analysis_from_snapshot, pressure_analysis.cpp:156-328) */
   int analysis_enabled;            /* analysis_enabled */
   int analysis_mode;               /* dn_analysis_mode, from the analysis_mode string */

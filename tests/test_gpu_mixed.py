@@ -6,8 +6,11 @@ defect-correction loop that stops on the
 reference's rule applied to the FP64 residual.  Two inner solvers are covered: CG preconditioned by one
 geometric multigrid V-cycle (mixed_preconditioner = multigrid, the default where the grid coarsens to <= 128
 cells) and the persistent PCG with the scheme's IC/ILDLT factor rounded to FP32 (mixed_preconditioner = ic);
-both keep FP32 operators and vectors and FP64 dot products and norms.  c, mu, u and v after each step must match the FP64 reference to rel-L2 <= 1e-8 (the tolerance
-of the mixed form); the CH and momentum solves stay FP64.
+both keep FP32 operators and vectors and FP64 dot products and norms.  The multigrid CG runs either as one
+thread-block cluster launch per inner solve (mg_cluster_cells, off by default) or as a launch per phase
+recorded in the solve's graph (the default); both are checked on the same states.
+Fields after each step must match the FP64 reference to rel-L2 <= 1e-8 (the tolerance of the mixed form);
+with the IC inner solver the CH solve stays FP64, and the momentum solve stays FP64 in every form.
 
 Each step starts both solvers from the same state (the oracle's, copied into the GPU handle): the mixed
 form's inner solves end at a different iterate than the reference's IC-PCG, within the same residual, and
@@ -76,10 +79,13 @@ def assert_within_reference_error(orc, gpu, tight, where):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["multigrid", "ic"])
+@pytest.mark.parametrize("prec", ["multigrid", "multigrid_cluster", "ic"])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_mixed_step_matches_fp64_oracle(dn, name, prec):
-    cfg = dict(CASES[name], mixed_preconditioner=prec)
+    cfg = dict(CASES[name], mixed_preconditioner=prec.split("_")[0])
+    if prec == "multigrid_cluster":
+        cfg["mg_cluster_cells"] = 1 << 20
+    prec = cfg["mixed_preconditioner"]
     orc, gpu = seeded_pair(dn, cfg, seed=13)
     from ding_nsch_core_solver_b200.capi import FIELDS as GPU_FIELDS
 
