@@ -123,12 +123,14 @@ __global__ void k_p_assemble(Grid G, BCSet bc, Fv rm, Fv us, Fv vs, Fv pe, int s
 // Mixed-precision pressure solve: FP64 defect correction around FP32 inner PCG solves
 // ---------------------------------------------------------------------------------------------------
 __global__ void k_to_float(const double *src, float *dst, long long n) {
+  pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) dst[t] = (float)src[t];
 }
 // r = b - A x in FP64, with per-CTA sums of r, r^2 and b^2 (the outer residual and its stopping norms)
 template <int S>
 __global__ void k_outer_residual(SpOp A, const double *b, const double *x, double *r, double *partials) {
+  pdl_entry();
   __shared__ double sh[3 * 32];
   double v[3] = {0.0, 0.0, 0.0};
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < A.n; t += (long long)gridDim.x * blockDim.x) {
@@ -148,6 +150,7 @@ __global__ void k_outer_residual(SpOp A, const double *b, const double *x, doubl
 }
 // the three sums of k_outer_residual, added in a fixed order by one warp
 __global__ void k_finish3(const double *partials, int nparts, double *out) {
+  pdl_entry();
   const int lane = threadIdx.x;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int p = lane; p < nparts; p += 32) {
@@ -165,11 +168,13 @@ __global__ void k_finish3(const double *partials, int nparts, double *out) {
   }
 }
 __global__ void k_add_correction(double *x, const float *e, long long n) {
+  pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) x[t] += (double)e[t];
 }
 // x += e with per-CTA sums of e^2 and of the updated x^2 (the iterate residual |dx| / |x| of the CH report)
 __global__ void k_add_correction_norms(double *x, const float *e, long long n, double *partials) {
+  pdl_entry();
   __shared__ double sh[3 * 32];
   double v[3] = {0.0, 0.0, 0.0};
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -209,6 +214,7 @@ __device__ __forceinline__ double smax(double a, double b) { return a < b ? b : 
 // right-hand side of an inner solve: the FP64 residual less its mean (R[kDcMean]) rounded to FP32; the
 // correction starts at 0
 __global__ void k_inner_rhs_dev(const double *r, const double *R, float *rf, float *ef, long long n) {
+  pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const double mean = R[kDcMean];
   if (t < n) {
@@ -222,6 +228,7 @@ __global__ void k_inner_rhs_dev(const double *r, const double *R, float *rf, flo
 // multigrid cycle that did not reduce the residual hands the pressure solve to the IC inner solver; any
 // other stalled cycle ends the solve).  Sets the outer while node's condition.
 __global__ void k_dc_decide(const double *sums, double *R, DcParams P, cudaGraphConditionalHandle loop) {
+  pdl_entry();
   if (threadIdx.x != 0) return;
   if (R[kDcStarted] == 0.0) {
     R[kDcStarted] = 1.0;
@@ -257,6 +264,7 @@ __global__ void k_dc_decide(const double *sums, double *R, DcParams P, cudaGraph
 // the inner solver of this cycle: multigrid CG (has_mg: the graph holds that branch) or the IC persistent PCG
 __global__ void k_dc_branch(const double *R, int has_mg, cudaGraphConditionalHandle mg,
                             cudaGraphConditionalHandle ic) {
+  pdl_entry();
   if (threadIdx.x != 0) return;
   const bool use_mg = R[kDcUseMg] != 0.0;
   if (has_mg) cudaGraphSetConditional(mg, use_mg ? 1u : 0u);
@@ -265,6 +273,7 @@ __global__ void k_dc_branch(const double *R, int has_mg, cudaGraphConditionalHan
 
 // end of a cycle: counted; with the CH's norms (|e|^2, |x|^2 after the update) the iterate residual
 __global__ void k_dc_cycle_end(const double *norms, double *R) {
+  pdl_entry();
   if (threadIdx.x != 0) return;
   R[kDcCycles] += 1.0;
   if (norms) R[kDcIres] = sqrt(smax(norms[0], 0.0) / smax(norms[1], 1.0e-30));
@@ -287,6 +296,7 @@ __global__ void k_ic_gate(const int *status, double *R, cudaGraphConditionalHand
 }
 // after the IC inner solve (its out[0] = iterations, status): iterations counted, a failure recorded
 __global__ void k_ic_done(const double *out, const int *status, double *R) {
+  pdl_entry();
   if (threadIdx.x != 0) return;
   if (*status != kDevOk) {
     R[kDcErr] = (double)*status;
@@ -714,6 +724,26 @@ dn_status check_launch(dn_handle *h, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(h, DN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   return DN_OK;
+}
+
+// A launch with programmatic stream serialization: the kernel (which opens with pdl_entry) may be launched
+// while its predecessor in the stream is still finishing, and waits for it on the device.
+template <typename... KArgs, typename... Args>
+dn_status launch_pdl(dn_handle *h, const char *name, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                     Args &&...args) {
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = h->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&lc, kernel, std::forward<Args>(args)...);
+  if (e != cudaSuccess) return fail(h, DN_ERR_CUDA, std::string(name) + ": " + cudaGetErrorString(e));
+  return check_launch(h, name);
 }
 
 bool is_uish(int id) { return id == DN_F_U || id == DN_F_U_PREV || id == DN_F_U_STAR || id == DN_F_SFX_U || id == DN_F_HU_PREV; }
@@ -1205,8 +1235,7 @@ dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
   int bottom = L - 1;
   while (bottom > 0 && (long long)H.lv[bottom - 1].nx * H.lv[bottom - 1].ny <= kMgBottomCells) --bottom;
   auto smooth = [&](const MgLevel &M, int color, int first) -> dn_status {
-    k_mg_smooth<<<blocks_for((long long)M.nx * (M.ny / 2)), 256, 0, h->stream>>>(M, color, first, px, py);
-    return check_launch(h, "k_mg_smooth");
+    return launch_pdl(h, "k_mg_smooth", k_mg_smooth, dim3(blocks_for((long long)M.nx * (M.ny / 2))), dim3(256), 0, M, color, first, px, py);
   };
   for (int l = 0; l < bottom; ++l) {
     const MgLevel F = mg_level(H, l), C = mg_level(H, l + 1);
@@ -1214,10 +1243,8 @@ dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
       DN_TRY(smooth(F, 0, k == 0));
       DN_TRY(smooth(F, 1, 0));
     }
-    k_mg_residual<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(F, px, py);
-    DN_TRY(check_launch(h, "k_mg_residual"));
-    k_mg_restrict<<<blocks_for((long long)C.nx * C.ny), 256, 0, h->stream>>>(F, C, H.fold);
-    DN_TRY(check_launch(h, "k_mg_restrict"));
+    DN_TRY(launch_pdl(h, "k_mg_residual", k_mg_residual, dim3(blocks_for((long long)F.nx * F.ny)), dim3(256), 0, F, px, py));
+    DN_TRY(launch_pdl(h, "k_mg_restrict", k_mg_restrict, dim3(blocks_for((long long)C.nx * C.ny)), dim3(256), 0, F, C, H.fold));
   }
   MgChain ch{};
   for (int l = 0; l < L; ++l) ch.lv[l] = mg_level(H, l);
@@ -1225,12 +1252,10 @@ dn_status mg_vcycle_launch(dn_handle *h, MgHier &H, float *b0, float *x0) {
   ch.last = L - 1;
   ch.fold = H.fold;
   ch.inv = H.inv;
-  k_mg_bottom<<<1, 1024, 0, h->stream>>>(ch);
-  DN_TRY(check_launch(h, "k_mg_bottom"));
+  DN_TRY(launch_pdl(h, "k_mg_bottom", k_mg_bottom, dim3(1), dim3(1024), 0, ch));
   for (int l = bottom - 1; l >= 0; --l) {
     const MgLevel F = mg_level(H, l), C = mg_level(H, l + 1);
-    k_mg_prolong<<<blocks_for((long long)F.nx * F.ny), 256, 0, h->stream>>>(C, F, H.fold);
-    DN_TRY(check_launch(h, "k_mg_prolong"));
+    DN_TRY(launch_pdl(h, "k_mg_prolong", k_mg_prolong, dim3(blocks_for((long long)F.nx * F.ny)), dim3(256), 0, C, F, H.fold));
     for (int k = 0; k < kMgSweeps; ++k) {
       DN_TRY(smooth(F, 1, 0));
       DN_TRY(smooth(F, 0, 0));
@@ -1404,14 +1429,12 @@ dn_status rec_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tm
   const int nb = (int)std::min<long long>({(long long)kMgParts, 4LL * h->num_sms, (long long)blocks_for(n)});
   const double dn_ = (double)n;
   auto finish = [&](int mode, int first) -> dn_status {
-    k_mgp_scalars<<<1, 32, 0, h->stream>>>(h->mg_part, nb, h->mg_scal, mode, first, project, dn_);
-    return check_launch(h, "k_mgp_scalars");
+    return launch_pdl(h, "k_mgp_scalars", k_mgp_scalars, dim3(1), dim3(32), 0, h->mg_part, nb, h->mg_scal, mode, first, project, dn_);
   };
   DN_CUDA(h, cudaMemcpyAsync(V.r, b, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
   cudaGraphConditionalHandle loop = 0;
   DN_TRY(cond_create(h, &loop));
-  k_mgcg_init<<<1, 32, 0, h->stream>>>(h->mg_scal, R, max_it, loop);
-  DN_TRY(check_launch(h, "k_mgcg_init"));
+  DN_TRY(launch_pdl(h, "k_mgcg_init", k_mgcg_init, dim3(1), dim3(32), 0, h->mg_scal, R, max_it, loop));
   return cond_node(h, loop, cudaGraphCondTypeWhile, [&]() -> dn_status {
     const long long before = h->launches;
     if (vcycles == 2) {
@@ -1420,19 +1443,14 @@ dn_status rec_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tm
     } else {
       DN_TRY(mg_vcycle(h, H, V.r, V.z));
     }
-    k_mgp_rz<<<nb, 256, 0, h->stream>>>(V);
-    DN_TRY(check_launch(h, "k_mgp_rz"));
+    DN_TRY(launch_pdl(h, "k_mgp_rz", k_mgp_rz, dim3(nb), dim3(256), 0, V));
     DN_TRY(finish(2, -1));
-    k_mgp_direction<<<nb, 256, 0, h->stream>>>(V, -1);
-    DN_TRY(check_launch(h, "k_mgp_direction"));
-    k_mgp_apply<S><<<nb, 256, 0, h->stream>>>(V);
-    DN_TRY(check_launch(h, "k_mgp_apply"));
+    DN_TRY(launch_pdl(h, "k_mgp_direction", k_mgp_direction, dim3(nb), dim3(256), 0, V, -1));
+    DN_TRY(launch_pdl(h, "k_mgp_apply", k_mgp_apply<S>, dim3(nb), dim3(256), 0, V));
     DN_TRY(finish(0, 0));
-    k_mgp_update<<<nb, 256, 0, h->stream>>>(V);
-    DN_TRY(check_launch(h, "k_mgp_update"));
+    DN_TRY(launch_pdl(h, "k_mgp_update", k_mgp_update, dim3(nb), dim3(256), 0, V));
     DN_TRY(finish(1, 0));
-    k_mgcg_ctrl<<<1, 32, 0, h->stream>>>(h->mg_scal, R, tol, loop);
-    DN_TRY(check_launch(h, "k_mgcg_ctrl"));
+    DN_TRY(launch_pdl(h, "k_mgcg_ctrl", k_mgcg_ctrl, dim3(1), dim3(32), 0, h->mg_scal, R, tol, loop));
     if (nodes) nodes->iter = h->launches - before;
     return DN_OK;
   });
@@ -1483,8 +1501,7 @@ dn_status rec_mixed_pressure(dn_handle *h, bool split, int kind, DcNodes *nodes)
   double *R = h->rec + kRecPressure;
   const long long start = h->launches;
   if (!split) {  // the variable operator changes every step: its FP32 copy and hierarchy are made here
-    k_to_float<<<blocks_for(5 * n), 256, 0, h->stream>>>(h->a5, h->fa5, 5 * n);
-    DN_TRY(check_launch(h, "k_to_float"));
+    DN_TRY(launch_pdl(h, "k_to_float", k_to_float, dim3(blocks_for(5 * n)), dim3(256), 0, h->a5, h->fa5, 5 * n));
     if (h->mgp.levels() > 0) DN_TRY(mg_setup_launch(h, h->mgp));
   }
   DcParams P{};
@@ -1501,12 +1518,9 @@ dn_status rec_mixed_pressure(dn_handle *h, bool split, int kind, DcNodes *nodes)
   cudaGraphConditionalHandle loop = 0;
   DN_TRY(cond_create(h, &loop));
   auto check = [&]() -> dn_status {
-    k_outer_residual<5><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
-    DN_TRY(check_launch(h, "k_outer_residual"));
-    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
-    DN_TRY(check_launch(h, "k_finish3"));
-    k_dc_decide<<<1, 32, 0, h->stream>>>(h->scal + 8, R, P, loop);
-    return check_launch(h, "k_dc_decide");
+    DN_TRY(launch_pdl(h, "k_outer_residual", k_outer_residual<5>, dim3(nb), dim3(256), 0, A, h->b, h->x, h->r, h->partials));
+    DN_TRY(launch_pdl(h, "k_finish3", k_finish3, dim3(1), dim3(32), 0, h->partials, nb, h->scal + 8));
+    return launch_pdl(h, "k_dc_decide", k_dc_decide, dim3(1), dim3(32), 0, h->scal + 8, R, P, loop);
   };
   DN_TRY(check());
   if (nodes) nodes->fixed = h->launches - start;
@@ -1517,10 +1531,8 @@ dn_status rec_mixed_pressure(dn_handle *h, bool split, int kind, DcNodes *nodes)
     cudaGraphConditionalHandle use_mg = 0, use_ic = 0;
     if (has_mg) DN_TRY(cond_create(h, &use_mg));
     DN_TRY(cond_create(h, &use_ic));
-    k_dc_branch<<<1, 32, 0, h->stream>>>(R, has_mg ? 1 : 0, use_mg, use_ic);
-    DN_TRY(check_launch(h, "k_dc_branch"));
-    k_inner_rhs_dev<<<blocks_for(n), 256, 0, h->stream>>>(h->r, R, h->fb, h->fx, n);
-    DN_TRY(check_launch(h, "k_inner_rhs"));
+    DN_TRY(launch_pdl(h, "k_dc_branch", k_dc_branch, dim3(1), dim3(32), 0, R, has_mg ? 1 : 0, use_mg, use_ic));
+    DN_TRY(launch_pdl(h, "k_inner_rhs", k_inner_rhs_dev, dim3(blocks_for(n)), dim3(256), 0, h->r, R, h->fb, h->fx, n));
     if (has_mg) {
       DN_TRY(cond_node(h, use_mg, cudaGraphCondTypeIf, [&]() -> dn_status {
         MgVec V{};
@@ -1547,16 +1559,13 @@ dn_status rec_mixed_pressure(dn_handle *h, bool split, int kind, DcNodes *nodes)
       DN_TRY(cond_node(h, go, cudaGraphCondTypeIf, [&]() -> dn_status {
         double unused[4];  // the results stay on the device (h->capturing)
         DN_TRY(run_pcg32(h, kind, project, cfg.poisson_iterations, cfg.mixed_inner_tolerance, unused));
-        k_ic_done<<<1, 32, 0, h->stream>>>(h->scal + 8, h->status, R);
-        return check_launch(h, "k_ic_done");
+        return launch_pdl(h, "k_ic_done", k_ic_done, dim3(1), dim3(32), 0, h->scal + 8, h->status, R);
       }));
       if (nodes) nodes->ic = h->launches - i0 - nodes->make;
       return DN_OK;
     }));
-    k_add_correction<<<blocks_for(n), 256, 0, h->stream>>>(h->x, h->fx, n);
-    DN_TRY(check_launch(h, "k_add_correction"));
-    k_dc_cycle_end<<<1, 32, 0, h->stream>>>(nullptr, R);
-    DN_TRY(check_launch(h, "k_dc_cycle_end"));
+    DN_TRY(launch_pdl(h, "k_add_correction", k_add_correction, dim3(blocks_for(n)), dim3(256), 0, h->x, h->fx, n));
+    DN_TRY(launch_pdl(h, "k_dc_cycle_end", k_dc_cycle_end, dim3(1), dim3(32), 0, nullptr, R));
     DN_TRY(check());
     if (nodes) nodes->cycle = h->launches - c0 - nodes->iter - nodes->ic - nodes->make;
     return DN_OK;
@@ -1670,19 +1679,15 @@ dn_status rec_mixed_ch(dn_handle *h, DcNodes *nodes) {
   cudaGraphConditionalHandle loop = 0;
   DN_TRY(cond_create(h, &loop));
   auto check = [&]() -> dn_status {
-    k_outer_residual<13><<<nb, 256, 0, h->stream>>>(A, h->b, h->x, h->r, h->partials);
-    DN_TRY(check_launch(h, "k_outer_residual"));
-    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
-    DN_TRY(check_launch(h, "k_finish3"));
-    k_dc_decide<<<1, 32, 0, h->stream>>>(h->scal + 8, R, P, loop);
-    return check_launch(h, "k_dc_decide");
+    DN_TRY(launch_pdl(h, "k_outer_residual", k_outer_residual<13>, dim3(nb), dim3(256), 0, A, h->b, h->x, h->r, h->partials));
+    DN_TRY(launch_pdl(h, "k_finish3", k_finish3, dim3(1), dim3(32), 0, h->partials, nb, h->scal + 8));
+    return launch_pdl(h, "k_dc_decide", k_dc_decide, dim3(1), dim3(32), 0, h->scal + 8, R, P, loop);
   };
   DN_TRY(check());
   if (nodes) nodes->fixed = h->launches - start;
   return cond_node(h, loop, cudaGraphCondTypeWhile, [&]() -> dn_status {
     const long long c0 = h->launches;
-    k_inner_rhs_dev<<<blocks_for(n), 256, 0, h->stream>>>(h->r, R, h->cb32, h->cx32, n);
-    DN_TRY(check_launch(h, "k_inner_rhs"));
+    DN_TRY(launch_pdl(h, "k_inner_rhs", k_inner_rhs_dev, dim3(blocks_for(n)), dim3(256), 0, h->r, R, h->cb32, h->cx32, n));
     MgVec V{};
     V.A = SpOpT<float>{h->fa13, (int)n, h->G.nx, h->G.ny, h->G.px, h->G.py};
     V.x = h->cx32;
@@ -1692,12 +1697,9 @@ dn_status rec_mixed_ch(dn_handle *h, DcNodes *nodes) {
     V.q = h->cq32;
     DN_TRY(rec_mgcg32<13>(h, h->mgc, V, h->cb32, h->ct32, 2, 0, cfg.ch_inner_iterations, cfg.mixed_inner_tolerance,
                           R, nodes));
-    k_add_correction_norms<<<nb, 256, 0, h->stream>>>(h->x, h->cx32, n, h->partials);
-    DN_TRY(check_launch(h, "k_add_correction_norms"));
-    k_finish3<<<1, 32, 0, h->stream>>>(h->partials, nb, h->scal + 8);
-    DN_TRY(check_launch(h, "k_finish3"));
-    k_dc_cycle_end<<<1, 32, 0, h->stream>>>(h->scal + 8, R);
-    DN_TRY(check_launch(h, "k_dc_cycle_end"));
+    DN_TRY(launch_pdl(h, "k_add_correction_norms", k_add_correction_norms, dim3(nb), dim3(256), 0, h->x, h->cx32, n, h->partials));
+    DN_TRY(launch_pdl(h, "k_finish3", k_finish3, dim3(1), dim3(32), 0, h->partials, nb, h->scal + 8));
+    DN_TRY(launch_pdl(h, "k_dc_cycle_end", k_dc_cycle_end, dim3(1), dim3(32), 0, h->scal + 8, R));
     DN_TRY(check());
     if (nodes) nodes->cycle = h->launches - c0 - nodes->iter;
     return DN_OK;

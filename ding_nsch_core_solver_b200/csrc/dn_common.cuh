@@ -34,6 +34,15 @@ enum DevStatus : int {
 
 enum PrecKind { kPrecDiag = 0, kPrecLDLT = 1, kPrecICC = 2 };
 
+// Entry of a kernel launched with programmatic stream serialization (launch_pdl on the host): wait until the
+// grids it depends on have completed and their memory is visible, then let the next grid of the stream be
+// launched (its blocks wait here the same way), so that a launch overlaps its predecessor's tail instead of
+// following it.  Without that launch attribute both instructions return at once.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

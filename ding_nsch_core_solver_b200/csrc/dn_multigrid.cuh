@@ -174,18 +174,22 @@ __device__ __forceinline__ void mg_prolong_at(const MgLevel &C, const MgLevel &F
 
 // one launch per phase on the levels above kMgBottomCells cells
 __global__ void k_mg_smooth(MgLevel L, int color, int first, int px, int py) {
+  pdl_entry();
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < (unsigned)L.nx * (unsigned)(L.ny >> 1)) mg_smooth_at(L, color, first, px, py, t);
 }
 __global__ void k_mg_residual(MgLevel L, int px, int py) {
+  pdl_entry();
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < (unsigned)L.nx * (unsigned)L.ny) mg_residual_at(L, px, py, t);
 }
 __global__ void k_mg_restrict(MgLevel F, MgLevel C, MgFold fold) {
+  pdl_entry();
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < (unsigned)C.nx * (unsigned)C.ny) mg_restrict_at(F, C, fold, t);
 }
 __global__ void k_mg_prolong(MgLevel C, MgLevel F, MgFold fold) {
+  pdl_entry();
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < (unsigned)F.nx * (unsigned)F.ny) mg_prolong_at(C, F, fold, t);
 }
@@ -201,6 +205,7 @@ struct MgChain {
   const float *inv;
 };
 __global__ void __launch_bounds__(1024) k_mg_bottom(MgChain Ch) {
+  pdl_entry();
   const unsigned tid = threadIdx.x, nt = blockDim.x;
   const int px = Ch.fold.px, py = Ch.fold.py;
   for (int l = Ch.first; l < Ch.last; ++l) {
@@ -386,6 +391,7 @@ struct MgVec {
 // q = A p (the 5-point pressure or the 13-point CH operator), partial sums of p.q
 template <int S>
 __global__ void k_mgp_apply(MgVec V) {
+  pdl_entry();
   __shared__ double sh[32];
   double v[1] = {0.0};
   const unsigned n = (unsigned)V.A.n, ny = (unsigned)V.A.ny;
@@ -400,6 +406,7 @@ __global__ void k_mgp_apply(MgVec V) {
 }
 // x += alpha p, r -= alpha q, partial sums of r.r
 __global__ void k_mgp_update(MgVec V) {
+  pdl_entry();
   __shared__ double sh[32];
   double v[1] = {0.0};
   const float alpha = (float)V.scal[kMgAlpha];
@@ -415,6 +422,7 @@ __global__ void k_mgp_update(MgVec V) {
 }
 // partial sums of r.z, z and r (the projected r.z of a singular system needs the last two)
 __global__ void k_mgp_rz(MgVec V) {
+  pdl_entry();
   __shared__ double sh[3 * 32];
   double v[3] = {0.0, 0.0, 0.0};
   const unsigned n = (unsigned)V.A.n;
@@ -433,6 +441,7 @@ __global__ void k_mgp_rz(MgVec V) {
 }
 // p = (z - mean z) + beta p (first: p = z - mean z; first < 0: the first iteration of the solve)
 __global__ void k_mgp_direction(MgVec V, int first) {
+  pdl_entry();
   const float beta = (float)V.scal[kMgBeta], mz = (float)V.scal[kMgMeanZ];
   if (first < 0) first = V.scal[kMgIt] == 0.0 ? 1 : 0;
   const unsigned n = (unsigned)V.A.n;
@@ -447,6 +456,7 @@ __global__ void k_mgp_direction(MgVec V, int first) {
 // the first iteration of the solve.
 __global__ void k_mgp_scalars(const double *part, int nparts, double *scal, int mode, int first, int project,
                               double n) {
+  pdl_entry();
   const int lane = threadIdx.x;
   if (first < 0) first = scal[kMgIt] == 0.0 ? 1 : 0;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -480,6 +490,7 @@ __global__ void k_mgp_scalars(const double *part, int nparts, double *scal, int 
 // Start of an inner solve: its scalars cleared and its iteration limit, the outer loop's budget left
 // (max(1, max_it - inner iterations so far)).  Sets the while node's condition.
 __global__ void k_mgcg_init(double *scal, const double *rec, int max_it, cudaGraphConditionalHandle loop) {
+  pdl_entry();
   if (threadIdx.x != 0) return;
   for (int k = 0; k < kMgScalCount; ++k) scal[k] = 0.0;
   scal[kMgCap] = (double)max(1, max_it - (int)rec[kDcTotal]);
@@ -490,6 +501,7 @@ __global__ void k_mgcg_init(double *scal, const double *rec, int max_it, cudaGra
 // flagged, |r| / |b| >= tol (|b| = the outer residual the inner right-hand side was made from; a NaN ends
 // it) and the iteration limit is not reached.
 __global__ void k_mgcg_ctrl(double *scal, double *rec, double tol, cudaGraphConditionalHandle loop) {
+  pdl_entry();
   if (threadIdx.x != 0) return;
   const double it = scal[kMgIt] + 1.0;
   scal[kMgIt] = it;
