@@ -104,3 +104,34 @@ def test_one_launch_batch_equals_each_instance_alone():
     finally:
         for s in batch + alone:
             s.close()
+
+
+@pytest.mark.parametrize("name", ["plain_split_walls", "plain_variable_ildlt", "mixed_split_walls_mg"])
+def test_replayed_step_fails_like_the_eager_step(name):
+    """A NaN planted in c once the steps are replayed: the replayed step returns the eager step's status and
+    message.  In the plain form that is the CH PCG's breakdown after its retry with the diagonal
+    preconditioner (phase_field.cpp:468-473), which the graph runs as a conditional branch on the device
+    status; in the mixed form the first failing solve or the non-finite diagnostics (solver.cpp:355-364).
+    Every loop of the graph ends on its own on a NaN (breakdown checks, the decisions' std::max semantics,
+    the cycle and iteration caps)."""
+    cfg = CASES[name]
+    eager, graph = _seeded(cfg, 7), _seeded(cfg, 7)
+    graph.set_step_graph(True)
+    g = cfg["ghost"]
+    try:
+        for step in range(3):
+            assert eager.step(step) == graph.step(step)
+        for s in (eager, graph):
+            f = s.get_field("c")
+            f[g + 5, g + 5] = np.nan
+            s.set_field("c", f)
+        errors = []
+        for s in (eager, graph):
+            with pytest.raises(capi.DnError) as e:
+                s.step(3)
+            errors.append(e.value)
+        assert errors[0].status == errors[1].status, (str(errors[0]), str(errors[1]))
+        assert str(errors[0]) == str(errors[1])
+    finally:
+        eager.close()
+        graph.close()
