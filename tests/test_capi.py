@@ -106,3 +106,25 @@ def test_create_rejects_grids_below_eight_cells(lib):
     with pytest.raises(capi.DnError) as ei:
         capi.Solver("nx = 6\nny = 6\nperiodic_x = false\nperiodic_y = false\n")
     assert ei.value.status == 10 and "nx, ny >= 8" in str(ei.value)
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every structure capi.py mirrors (dn_bc, dn_config, dn_report, dn_diag) has the C header's size and field
+    offsets: a C program compiled against include/dn_cuda.h prints them.  A field added to the header but not
+    to the mirror (or in another place) would hand the library a shifted struct."""
+    mirrors = {"dn_bc": capi.BC, "dn_config": capi.Config, "dn_report": capi.Report, "dn_diag": capi.Diag}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "dn_cuda.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for n, _ in py._fields_:
+            lines.append(f'  printf("{cname}.{n} %zu\\n", offsetof({cname}, {n}));')
+    lines += ["  return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[cname]) == C.sizeof(py), (cname, got[cname], C.sizeof(py))
+        for n, _ in py._fields_:
+            assert int(got[f"{cname}.{n}"]) == getattr(py, n).offset, (cname, n)

@@ -353,3 +353,30 @@ def test_patched_reference_build_binds_the_c_abi():
     assert {"dn_create", "dn_pressure_solve", "dn_ch_linear_solve"} <= set(needed), needed
     for name in needed:
         assert re.search(r"\b" + name + r"\s*\(", header), name
+
+
+def test_oracle_ctypes_structs_match_its_header(tmp_path):
+    """oracle.py's ctypes mirrors have oracle/dn_oracle.h's sizes and field offsets (a C program compiled
+    against the header prints them), so the checker never reads a shifted struct."""
+    import ctypes as C
+    import subprocess
+
+    from oracle import oracle as o
+
+    mirrors = {"orc_bc": o.BC, "orc_config": o.Config, "orc_report": o.Report, "orc_diag": o.Diag}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "dn_oracle.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for n, _ in py._fields_:
+            lines.append(f'  printf("{cname}.{n} %zu\\n", offsetof({cname}, {n}));')
+    lines += ["  return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")
+    subprocess.run(["gcc", "-std=c99", "-I", here, "-o", str(exe), str(src)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[cname]) == C.sizeof(py), (cname, got[cname], C.sizeof(py))
+        for n, _ in py._fields_:
+            assert int(got[f"{cname}.{n}"]) == getattr(py, n).offset, (cname, n)
