@@ -1377,8 +1377,9 @@ dn_status capture_exec(dn_handle *h, cudaGraphExec_t *exec, Record &&record) {
 // the pressure operator; 2 for the CH operator, preconditioned by (K + s I)^-2), recorded into the capture:
 // r = b, then a while node whose body is one iteration (precondition, r.z, direction, A p, p.q, update,
 // r.r) ending in k_mgcg_ctrl, which stops at |r| < tol |b| (|b| = R[kDcAbs]), a breakdown or the inner
-// iteration budget left in R.  V: the operator and the vectors (V.x is e, zero on entry); tmp: a level-0
-// buffer for the output of the first of two V-cycles.
+// iteration budget left in R.  Grids of at most mg_cluster_cells cells run the same solve as one
+// thread-block cluster launch instead (k_mgcg_cluster).  V: the operator and the vectors (V.x is e, zero on
+// entry); tmp: a level-0 buffer for the output of the first of two V-cycles.
 template <int S>
 dn_status rec_mgcg32(dn_handle *h, MgHier &H, MgVec V, const float *b, float *tmp, int vcycles, int project,
                      int max_it, double tol, double *R, DcNodes *nodes) {
@@ -1460,7 +1461,7 @@ dn_status pressure_factor(dn_handle *h, bool split, bool icc);
 
 // The FP64 IC/ILDLT factor of the pressure operator (unless the constant split operator's is already
 // valid) and its FP32 copies for the IC inner solver, recorded into the capture; a failed factor is
-// recorded in R[kDcErr] and *gate is left 0.
+// recorded in R[kDcErr] and leaves the condition `gate` (the IC inner solve's branch) at 0.
 dn_status rec_ic32_factor(dn_handle *h, bool split, int kind, double *R, cudaGraphConditionalHandle gate) {
   const long long n = h->n;
   if (!(split && h->p_factor_valid && h->p_factor_kind == kind)) {
@@ -1482,8 +1483,8 @@ dn_status rec_ic32_factor(dn_handle *h, bool split, int kind, double *R, cudaGra
   return check_launch(h, "k_ic_gate");
 }
 
-// The FP32 copy of the pressure operator and the coarse operators of its hierarchy (kernels only: the
-// coarsest inverse's usability flag stays on the device, where the solve's first check reads it).
+// The coarse operators of a hierarchy and the coarsest level's inverse (kernels only: the inverse's
+// usability flag stays on the device, where the solve's first check reads it).
 dn_status mg_setup_launch(dn_handle *h, MgHier &H);
 
 // Mixed-precision pressure solve, recorded into the capture: x = 0 on entry; repeat r = b - A x (FP64,
@@ -1615,8 +1616,9 @@ dn_status dc_error(dn_handle *h, const double R[kDcSize], int kind) {
 }
 
 // Mixed-precision pressure solve (rec_mixed_pressure), eager or recorded into a step graph.  The split
-// operator is the same every step: its FP32 copy and hierarchy are made once, here.  out: [0] inner
-// iterations in total, [1] abs and [2] rel FP64 residual, [3] 0.
+// operator is the same every step: its FP32 copy and hierarchy are made once, here, and so is its IC/ILDLT
+// factor where the IC inner solver runs from the start (no usable hierarchy).  out: [0] inner iterations in
+// total, [1] abs and [2] rel FP64 residual, [3] 0.
 dn_status mixed_pressure(dn_handle *h, bool split, int kind, double out[4]) {
   const long long n = h->n;
   if (split && !h->mgp_split_ready) {
